@@ -1,0 +1,370 @@
+"""Benchmark of the coagulation step (mc_coag) on B200.
+
+Workload: 1e6 computational particles, 20 species with per-particle
+Dirichlet(1) mass fractions and densities U(1000, 2000) kg/m^3, three
+log-normal modes (D_g 0.02 / 0.1 / 0.5 um), nummass weighting, Brownian
+kernel at 288 K and 1e5 Pa, del_t = 60 s.  A step is one mc_coag call on that
+population; the metric is pair tests per second (the reference's tot_n_samp
+counter) and simulated seconds per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank advances its own population (weak scaling, no
+data-path collective); rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+B_TEST = 56  # algorithmic bytes per pair test (indices, two records, k_max entry)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-part", type=int, default=1_000_000)
+    ap.add_argument("--del-t", type=float, default=60.0)
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return ws, rank, local
+
+
+def allreduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload(n_part, seed):
+    from partmc_b200 import aero_dist
+    return aero_dist.brown_20spec(n_part, seed=seed)
+
+
+def cpu_baseline(n_part, del_t, budget_s=20.0):
+    """The oracle (C restatement of the reference's mc_coag), one thread, on
+    a bounded sample of the same workload: as many steps as fit in budget_s."""
+    from oracle import oracle as O
+    pop = workload(n_part, seed=11)
+    orc = O.Oracle(pop.aero_data.density, (pop.awa.type, pop.awa.magnitude, pop.awa.exponent), seed=5)
+    orc.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
+    orc.set_next_id(pop.n_part + 1)
+    orc.mc_coag(4, 288.0, 1e5, 0.0, del_t)  # first step builds the k_max table: untimed
+    steps, samp, t0 = 0, 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and steps < 1000:
+        a, _ = orc.mc_coag(4, 288.0, 1e5, 0.0, del_t)
+        samp += a
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": samp / dt, "unit": "pair-tests/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} steps of the 1e6-particle workload after one untimed step ({dt:.1f} s)",
+            "sim_s_per_s": steps * del_t / dt}
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference's CPU algorithm (the oracle port, since
+    the Fortran reference cannot be built here) on all host threads, one
+    independent population per thread, same workload and metric."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    n_thr = min(os.cpu_count() or 1, 32)
+    orcs = []
+    for k in range(n_thr):
+        pop = workload(args.n_part, seed=100 + k)
+        o = O.Oracle(pop.aero_data.density, (pop.awa.type, pop.awa.magnitude, pop.awa.exponent), seed=7 + k)
+        o.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
+        o.set_next_id(pop.n_part + 1)
+        orcs.append(o)
+    temps = np.full(n_thr, 288.0)
+    press = np.full(n_thr, 1e5)
+    O.step_many(orcs, n_thr, 4, temps, press, 0.0, args.del_t, max(1, args.warmup))
+    per_step = []
+    tot = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        a, _ = O.step_many(orcs, n_thr, 4, temps, press, 0.0, args.del_t, 1)
+        per_step.append(time.perf_counter() - t0)
+        tot += a
+    dt = sum(per_step)
+    v = tot / dt
+    line = {"metric": "coag pair-tests/s at 1e6 particles", "value": v, "unit": "pair-tests/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "brown_20spec_1e6_nummass", "n_part": args.n_part, "n_spec": 20,
+                       "kernel": "brown", "del_t": args.del_t, "populations": n_thr,
+                       "l2": "populations larger than L2"},
+            "cpu_baseline": {"value": v, "unit": "pair-tests/s", "cores": n_thr, "kind": "port",
+                             "sample": f"{n_thr} independent 1e6-particle populations, one per thread"},
+            "e2e": {"value": v, "unit": "pair-tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "sim_s_per_s": args.steps * args.del_t * n_thr / dt}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            barrier(ws)
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    from partmc_b200 import build
+    build.build()
+    import partmc_b200 as pm
+    from partmc_b200 import _lib
+
+    L = _lib.lib()
+    mode = pm.MODE_MIXED if args.mode == "mixed" else pm.MODE_FP64
+    pop = workload(args.n_part, seed=1 + rank)
+    env = pm.EnvState(288.0, 1e5)
+
+    def new_state(m):
+        st = pm.AeroState(pop.aero_data, pop.awa, seed=1000 + rank, mode=m)
+        st.add_particles(pop.vol, pop.group)
+        return st
+
+    # L2 flush buffer (larger than the 126 MB L2), written between timed steps
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed_steps(st, k, w):
+        for _ in range(w):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, args.del_t)
+        L.pmc_coag_gpu_profile(st.ctx, 1)
+        n0 = ctypes.c_int64()
+        L.pmc_coag_gpu_launch_count(ctypes.byref(n0))
+        barrier(ws)
+        torch.cuda.synchronize()
+        samp = 0
+        ms = 0.0
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, args.del_t)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            samp += a
+        n1 = ctypes.c_int64()
+        L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
+        prof = {}
+        for which, name in ((0, "test"), (1, "scatter"), (2, "hist"), (3, "step")):
+            t, nl, u = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
+            L.pmc_coag_gpu_profile_read(st.ctx, which, ctypes.byref(t), ctypes.byref(nl), ctypes.byref(u))
+            prof[name] = (t.value, nl.value, u.value)
+        L.pmc_coag_gpu_profile(st.ctx, 0)
+        return ms, samp, n1.value - n0.value, prof
+
+    clocks = ClockSampler(local)
+    st = new_state(mode)
+    clocks.start()
+    ms, samp, launches, prof = timed_steps(st, args.steps, args.warmup)
+    clk = clocks.stop()
+    # plain FP64 form of the same step, for the precision comparison
+    st64 = new_state(pm.MODE_FP64)
+    ms64, samp64, _, _ = timed_steps(st64, max(3, args.steps // 2), args.warmup)
+    del st64
+
+    # end to end through the C ABI with host buffers: upload, step, download
+    host_vol = torch.from_numpy(pop.vol).pin_memory().numpy()
+    host_grp = torch.from_numpy(pop.group).pin_memory().numpy()
+    ste = new_state(mode)
+    for _ in range(2):
+        ste.add_particles(host_vol, host_grp)
+        pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, ste, args.del_t)
+        out = ste.particles()
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_samp = 0
+    h2d = d2h = 0
+    for _ in range(args.e2e_steps):
+        ste.add_particles(host_vol, host_grp)
+        a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, ste, args.del_t)
+        out = ste.particles()
+        e2e_samp += a
+        h2d = host_vol.nbytes + host_grp.nbytes
+        d2h = sum(v.nbytes for v in out.values())
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+
+    # whole-job aggregates: max time over ranks, summed work
+    t_max = allreduce_max(ms / 1e3, ws)
+    samp_all = allreduce_sum(samp, ws)
+    e2e_t = allreduce_max(e2e_s, ws)
+    e2e_all = allreduce_sum(e2e_samp, ws)
+    t64 = allreduce_max(ms64 / 1e3, ws)
+    samp64_all = allreduce_sum(samp64, ws)
+
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        ttest, ntest, utest = prof["test"]
+        tsc, nsc, usc = prof["scatter"]
+        # dominant kernel by measured time
+        if tsc >= ttest:
+            dom, t_tot, n_l, units, bpu = "k_sort_scatter (sort pass 3 + pair-test records)", tsc, nsc, usc, 8 * 20 + 16
+        else:
+            dom, t_tot, n_l, units, bpu = "k_test (pair tests)", ttest, ntest, utest, B_TEST
+        avg_ms = t_tot / max(n_l, 1)
+        bytes_per_launch = units / max(n_l, 1) * bpu
+        achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(args.n_part, args.del_t)
+        line = {
+            "metric": "coag pair-tests/s at 1e6 particles",
+            "value": samp_all / t_max,
+            "unit": "pair-tests/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if args.mode == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": "brown_20spec_1e6_nummass", "n_part": args.n_part, "n_spec": 20,
+                       "kernel": "brown", "weighting": "nummass", "del_t": args.del_t,
+                       "precision": "FP32 kernel eval/accept, FP64 k_max/merge/sums" if args.mode == "mixed"
+                       else "FP64", "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"replicas x{ws}"},
+            "sim_s_per_s": args.steps * args.del_t * ws / t_max,
+            "fp64_plain": {"value": samp64_all / t64, "unit": "pair-tests/s",
+                           "ms_per_step": ms64 / max(3, args.steps // 2)},
+            "e2e": {"value": e2e_all / e2e_t, "unit": "pair-tests/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "avg_launch_ms": avg_ms, "launches": n_l,
+                         "bytes_per_unit": bpu, "units_per_launch": units / max(n_l, 1)},
+            "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "units": v[2]} for k, v in prof.items()},
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if ws > 1:
+        barrier(ws)
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

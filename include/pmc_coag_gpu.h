@@ -1,0 +1,203 @@
+/*
+ * pmc_coag_gpu.h -- C ABI of the B200 coagulation library (libpmc_coag_gpu.so).
+ *
+ * This is the drop-in boundary for PartMC's particle-resolved coagulation
+ * step.  The reference calls
+ *     mc_coag(coag_kernel_type, env_state, aero_data, aero_state, del_t,
+ *             tot_n_samp, tot_n_coag)                (src/coagulation.F90:43-59)
+ * from run_part_timestep (src/run_part.F90:917-931).  A Fortran module with
+ * bind(c) interfaces maps that call onto
+ * pmc_coag_gpu_step(); the particle state lives on the GPU between calls and
+ * is synchronised with aero_state_t only when another process needs it.
+ *
+ * Conventions
+ *  - Every function returns a status code (PMC_OK = 0), following the int
+ *    status pattern of the reference's C RNG wrapper (src/rand_gsl.c:80-152,
+ *    checked by rand_check_gsl in src/rand.F90:38-58).  The reference instead
+ *    stops the program (die_msg / assert, src/util.F90:103-143).
+ *  - Species volumes are passed as the reference stores them: n_spec values
+ *    per particle, particle-major (Fortran vol(n_spec) per particle), i.e.
+ *    vol[i * n_spec + s].
+ *  - Groups and classes are 1-based, as in aero_particle_t (aero_particle.F90:34-36).
+ *  - Weights are n_group x n_class arrays, entry (g, c) at (g-1) + n_group*(c-1),
+ *    the layout of aero_weight_array_t%weight (aero_weight_array.F90:35-39).
+ *  - No entry point takes ownership of caller memory.  All pointers are host
+ *    pointers unless a name says _dev.
+ */
+#ifndef PMC_COAG_GPU_H
+#define PMC_COAG_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PMC_OK 0
+#define PMC_ERR_INVALID_ARG 1
+#define PMC_ERR_OUT_OF_GRID 2     /* die_msg(765620746 / 134572570), coagulation.F90:561-565 */
+#define PMC_ERR_CAPACITY 3        /* particle capacity or bin limit exceeded */
+#define PMC_ERR_CUDA 4            /* a CUDA runtime call failed */
+#define PMC_ERR_TIMEOUT 5         /* a bounded device loop ran out of iterations */
+#define PMC_ERR_RNG_EXHAUSTED 6   /* replay stream shorter than the draws needed */
+#define PMC_ERR_ASSERT 7          /* a reference assert() condition failed */
+#define PMC_ERR_NO_DEVICE 8
+
+/* kernel types, coag_kernel.F90:29-45 */
+#define PMC_KERNEL_SEDI 1
+#define PMC_KERNEL_ADDITIVE 2
+#define PMC_KERNEL_CONSTANT 3
+#define PMC_KERNEL_BROWN 4
+#define PMC_KERNEL_ZERO 5
+
+/* weight types, aero_weight.F90:24-30 */
+#define PMC_WEIGHT_NONE 1
+#define PMC_WEIGHT_POWER 2
+#define PMC_WEIGHT_MFA 3
+
+/* execution modes */
+#define PMC_MODE_FP64 0   /* parallel pair tests in FP64 */
+#define PMC_MODE_MIXED 1  /* FP32 kernel evaluation and accept test; FP64 k_max, merges, sums */
+#define PMC_MODE_REPLAY 2 /* one device thread runs the reference's sequential order on a given uniform stream */
+
+typedef struct pmc_coag_gpu_ctx pmc_coag_gpu_ctx;
+
+/* Create a context holding one particle population.  Replaces the state
+ * set-up the reference does with aero_data_t (density, aero_data.F90), the
+ * weight array (aero_state_set_weight, aero_state.F90:184-235) and the RNG
+ * seed (pmc_srand, rand.F90:66-113).  i_water is the 1-based water species
+ * (0 if none), used only when merging frozen particles. */
+int pmc_coag_gpu_init(int n_spec, const double *density, int i_water,
+                      int n_group, int n_class, const int *w_type,
+                      const double *w_mag, const double *w_exp, uint64_t seed,
+                      pmc_coag_gpu_ctx **ctx);
+
+/* Create a context holding n_pop independent populations that share species,
+ * weights' shape and kernel, and advance together (batched mode). */
+int pmc_coag_gpu_init_batch(int n_pop, int n_spec, const double *density,
+                            int i_water, int n_group, int n_class,
+                            const int *w_type, const double *w_mag,
+                            const double *w_exp, const uint64_t *seeds,
+                            pmc_coag_gpu_ctx **ctx);
+
+int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx *ctx);
+
+/* Replace the whole particle list of population `pop` (0-based; 0 for a
+ * one-population context).  Equivalent to filling aero_state%apa and
+ * clearing aero_state%valid_sort (aero_state.F90:69-84).  Optional arrays may
+ * be NULL: group/cls default to 1, id to consecutive values from the
+ * context's next id, n_primary to 1.  Components default to one component
+ * with source 1 and create time 0 (aero_particle_set_component,
+ * aero_particle.F90:186-200). */
+int pmc_coag_gpu_upload(pmc_coag_gpu_ctx *ctx, int pop, int n_part,
+                        const double *vol, const int *group, const int *cls,
+                        const int64_t *id, const int *n_primary);
+
+/* Components of the uploaded particles: n_comp[i] <= 20, comp_source and
+ * comp_create_time are 20 entries per particle (aero_particle_t%component,
+ * aero_particle.F90:54). */
+int pmc_coag_gpu_upload_components(pmc_coag_gpu_ctx *ctx, int pop, int n_part,
+                                   const int *n_comp, const int *comp_source,
+                                   const double *comp_create_time);
+
+/* The mc_coag drop-in (coagulation.F90:43-96): advance the population(s) by
+ * one coagulation step of length del_t.  tot_n_samp / tot_n_coag receive the
+ * reference's counters (summed over populations in a batched context). */
+int pmc_coag_gpu_step(pmc_coag_gpu_ctx *ctx, int kernel_type, double temp,
+                      double pressure, double additive_coeff, double del_t,
+                      int *tot_n_samp, int *tot_n_coag);
+
+/* Batched form: temp[pop], pressure[pop] per population, n_steps steps, the
+ * counters summed over populations and steps. */
+int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx *ctx, int kernel_type,
+                            const double *temp, const double *pressure,
+                            double additive_coeff, double del_t, int n_steps,
+                            int64_t *tot_n_samp, int64_t *tot_n_coag);
+
+/* Number of particles of population `pop` (aero_state_n_part). */
+int pmc_coag_gpu_n_part(pmc_coag_gpu_ctx *ctx, int pop, int *n_part);
+
+/* Copy population `pop` back to the host (aero_state%apa).  Arrays sized for
+ * max_part particles; any pointer may be NULL. */
+int pmc_coag_gpu_download(pmc_coag_gpu_ctx *ctx, int pop, int max_part,
+                          double *vol, int *group, int *cls, int64_t *id,
+                          int *n_primary, int *n_part);
+int pmc_coag_gpu_download_components(pmc_coag_gpu_ctx *ctx, int pop,
+                                     int max_part, int *n_comp,
+                                     int *comp_source,
+                                     double *comp_create_time);
+
+/* New weight magnitudes/exponents, e.g. after aero_state_rebalance doubles or
+ * halves a group (aero_state.F90:1722-1852).  Invalidates the sort. */
+int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx *ctx, const int *w_type,
+                            const double *w_mag, const double *w_exp);
+
+/* The ID counter (next_id, aero_particle.F90:72, new_id :157-165). */
+int pmc_coag_gpu_set_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t next_id);
+int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t *next_id);
+
+/* PMC_MODE_FP64 (default), PMC_MODE_MIXED or PMC_MODE_REPLAY. */
+int pmc_coag_gpu_set_mode(pmc_coag_gpu_ctx *ctx, int mode);
+
+/* Replay stream: uniforms in [0, 1) consumed in the reference's order
+ * (pmc_random, rand.F90:138-167).  Copied to the device. */
+int pmc_coag_gpu_replay_set(pmc_coag_gpu_ctx *ctx, const double *u, int64_t n);
+/* Same, read from a file of little-endian float64 values. */
+int pmc_coag_gpu_replay_open(pmc_coag_gpu_ctx *ctx, const char *path);
+/* Uniforms consumed so far from the replay stream. */
+int pmc_coag_gpu_replay_used(pmc_coag_gpu_ctx *ctx, int64_t *n_used);
+
+/* Counters of the last step: kernel-bound violations (warn_assert_msg
+ * 532446093, coagulation.F90:749-751), conflict redraws, sub-rounds. */
+int pmc_coag_gpu_stats(pmc_coag_gpu_ctx *ctx, int64_t *kmax_violations,
+                       int64_t *redraws, int64_t *rounds);
+
+/* ---- measurement ---- */
+
+/* Time, with CUDA events on the library's own stream, every launch of the
+ * pair-test kernel (which = 0; units = samples tested), of the sort scatter
+ * and record build (1; units = slots), of the sort histogram (2; units =
+ * slots) and whole steps (3).  enable = 0 turns timing off; either call
+ * clears the totals.  No counterpart in the reference. */
+int pmc_coag_gpu_profile(pmc_coag_gpu_ctx *ctx, int enable);
+int pmc_coag_gpu_profile_read(pmc_coag_gpu_ctx *ctx, int which,
+                              double *total_ms, int64_t *launches,
+                              int64_t *units);
+/* Kernel launches issued by this library since it was loaded. */
+int pmc_coag_gpu_launch_count(int64_t *n);
+
+/* ---- inspection entry points used by the parity tests ---- */
+
+/* Sort population `pop` (aero_state_sort, aero_state.F90:3291-3307) and
+ * return the bin grid edges (n_bin+1, radius in m), the per-(bin, class)
+ * counts (n_bin x n_class, bin fastest) and each particle's 1-based bin in
+ * upload order.  Any output may be NULL. */
+int pmc_coag_gpu_sort(pmc_coag_gpu_ctx *ctx, int pop, int *n_bin,
+                      double *edges, int max_bin, int *counts, int *bins);
+
+/* k_max table of the current grid (est_k_minmax_binned_unweighted,
+ * coag_kernel.F90:253-280), n_bin x n_bin column-major. */
+int pmc_coag_gpu_kmax_table(pmc_coag_gpu_ctx *ctx, int kernel_type,
+                            double temp, double pressure,
+                            double additive_coeff, double *kmax, int max_bin);
+
+/* Weighted kernel (num_conc_weighted_kernel, coag_kernel.F90:175-209)
+ * evaluated on the device for n_pairs particle pairs given by species
+ * volumes (particle-major) and 1-based classes, in FP64 (mode FP64) or FP32
+ * (mode MIXED).  c_ij is the destination class of each pair. */
+int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx *ctx, int kernel_type,
+                             double temp, double pressure,
+                             double additive_coeff, int n_pairs,
+                             const double *vol1, const int *c1,
+                             const double *vol2, const int *c2,
+                             const int *c_ij, double *k_out);
+
+/* Human-readable name of a status code. */
+const char *pmc_coag_gpu_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,280 @@
+"""Host-side mirror of the reference's coagulation interface over the C ABI.
+
+The names follow the reference: ``mc_coag(coag_kernel_type, env_state,
+aero_data, aero_state, del_t) -> (tot_n_samp, tot_n_coag)``
+(coagulation.F90:43-59), with ``AeroData``, ``AeroWeightArray``,
+``EnvState`` and ``AeroState`` standing for aero_data_t, aero_weight_array_t,
+env_state_t and aero_state_t.  An ``AeroState`` keeps its particles on the
+GPU between calls; ``particles()`` copies them back.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import MODE_FP64, MODE_MIXED, MODE_REPLAY, check, dp, ip, lp
+
+# coag_kernel.F90:29-45
+COAG_KERNEL_TYPE_SEDI = 1
+COAG_KERNEL_TYPE_ADDITIVE = 2
+COAG_KERNEL_TYPE_CONSTANT = 3
+COAG_KERNEL_TYPE_BROWN = 4
+COAG_KERNEL_TYPE_ZERO = 5
+KERNEL_NAMES = {"sedi": 1, "additive": 2, "constant": 3, "brown": 4, "zero": 5}
+
+# aero_weight.F90:24-30
+AERO_WEIGHT_TYPE_NONE = 1
+AERO_WEIGHT_TYPE_POWER = 2
+AERO_WEIGHT_TYPE_MFA = 3
+
+MAX_AERO_COMPONENT_SIZE = 20
+
+
+class AeroData:
+    """Species densities (kg/m^3) and the water species index (1-based, 0 = none)."""
+
+    def __init__(self, density, i_water=0, names=None):
+        self.density = np.ascontiguousarray(np.atleast_1d(density), dtype=np.float64)
+        self.i_water = int(i_water)
+        self.names = names
+
+    @property
+    def n_spec(self):
+        return self.density.size
+
+
+class AeroWeightArray:
+    """weight(n_group, n_class) of (type, magnitude, exponent)
+    (aero_weight_array.F90:35-39)."""
+
+    def __init__(self, w_type, magnitude, exponent):
+        self.type = np.asfortranarray(np.atleast_2d(w_type), dtype=np.int32)
+        self.magnitude = np.asfortranarray(np.atleast_2d(magnitude), dtype=np.float64)
+        self.exponent = np.asfortranarray(np.atleast_2d(exponent), dtype=np.float64)
+
+    @property
+    def n_group(self):
+        return self.type.shape[0]
+
+    @property
+    def n_class(self):
+        return self.type.shape[1]
+
+    # aero_weight_array_set_flat / _set_power / _set_nummass, aero_weight_array.F90:66-118
+    @classmethod
+    def flat(cls, n_class=1, magnitude=1.0):
+        return cls(np.full((1, n_class), AERO_WEIGHT_TYPE_NONE), np.full((1, n_class), magnitude),
+                   np.zeros((1, n_class)))
+
+    @classmethod
+    def power(cls, exponent, n_class=1, magnitude=1.0):
+        return cls(np.full((1, n_class), AERO_WEIGHT_TYPE_POWER), np.full((1, n_class), magnitude),
+                   np.full((1, n_class), float(exponent)))
+
+    @classmethod
+    def nummass(cls, n_class=1, magnitudes=(1.0, 1.0)):
+        t = np.array([[AERO_WEIGHT_TYPE_NONE] * n_class, [AERO_WEIGHT_TYPE_POWER] * n_class])
+        m = np.array([[magnitudes[0]] * n_class, [magnitudes[1]] * n_class], dtype=np.float64)
+        e = np.array([[0.0] * n_class, [-3.0] * n_class])
+        return cls(t, m, e)
+
+    def flat_arrays(self):
+        return (np.ascontiguousarray(self.type.ravel(order="F")),
+                np.ascontiguousarray(self.magnitude.ravel(order="F")),
+                np.ascontiguousarray(self.exponent.ravel(order="F")))
+
+    def num_conc_at_radius(self, i_class, radius):
+        """aero_weight_array_num_conc_at_radius (aero_weight_array.F90:232-252),
+        i_class 1-based, vectorised over radius."""
+        r = np.asarray(radius, dtype=np.float64)
+        inv = np.zeros_like(r)
+        for g in range(self.n_group):
+            t, m, e = self.type[g, i_class - 1], self.magnitude[g, i_class - 1], self.exponent[g, i_class - 1]
+            nc = np.full_like(r, m) if t == AERO_WEIGHT_TYPE_NONE else m * r ** e
+            inv = inv + 1.0 / nc
+        return 1.0 / inv
+
+
+class EnvState:
+    def __init__(self, temp=288.0, pressure=1e5, additive_kernel_coefficient=1000.0):
+        self.temp = float(temp)
+        self.pressure = float(pressure)
+        self.additive_kernel_coefficient = float(additive_kernel_coefficient)
+
+
+class AeroState:
+    """Particle population(s) resident on the GPU (aero_state_t).
+
+    ``n_pop > 1`` makes a batched state: independent populations with their
+    own seeds that advance together in one step.
+    """
+
+    def __init__(self, aero_data, aero_weight_array, seed=1, mode=MODE_FP64, n_pop=1, seeds=None):
+        self.aero_data = aero_data
+        self.awa = aero_weight_array
+        self.n_pop = int(n_pop)
+        t, m, e = aero_weight_array.flat_arrays()
+        L = _lib.lib()
+        ctx = ctypes.c_void_p()
+        if self.n_pop == 1 and seeds is None:
+            rc = L.pmc_coag_gpu_init(aero_data.n_spec, dp(aero_data.density), aero_data.i_water,
+                                     aero_weight_array.n_group, aero_weight_array.n_class, ip(t), dp(m), dp(e),
+                                     int(seed), ctypes.byref(ctx))
+        else:
+            sd = np.ascontiguousarray(seeds if seeds is not None else np.arange(1, self.n_pop + 1) + int(seed) * 1000003,
+                                      dtype=np.uint64)
+            rc = L.pmc_coag_gpu_init_batch(self.n_pop, aero_data.n_spec, dp(aero_data.density), aero_data.i_water,
+                                           aero_weight_array.n_group, aero_weight_array.n_class, ip(t), dp(m), dp(e),
+                                           sd.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), ctypes.byref(ctx))
+        check(rc, "pmc_coag_gpu_init")
+        self.ctx = ctx
+        self.set_mode(mode)
+
+    def __del__(self):
+        if getattr(self, "ctx", None):
+            _lib.lib().pmc_coag_gpu_destroy(self.ctx)
+            self.ctx = None
+
+    def close(self):
+        self.__del__()
+
+    def set_mode(self, mode):
+        check(_lib.lib().pmc_coag_gpu_set_mode(self.ctx, mode), "pmc_coag_gpu_set_mode")
+        self.mode = mode
+
+    def set_weight(self, aero_weight_array):
+        self.awa = aero_weight_array
+        t, m, e = aero_weight_array.flat_arrays()
+        check(_lib.lib().pmc_coag_gpu_set_weight(self.ctx, ip(t), dp(m), dp(e)), "pmc_coag_gpu_set_weight")
+
+    def add_particles(self, vol, weight_group=None, weight_class=None, ids=None, n_primary_parts=None,
+                      n_comp=None, comp_source=None, comp_create_time=None, pop=0):
+        """Replace population ``pop`` by these particles.  vol: (n_part, n_spec)."""
+        vol = np.ascontiguousarray(vol, dtype=np.float64)
+        if vol.ndim == 1:
+            vol = vol[:, None]
+        n = vol.shape[0]
+        as32 = lambda a: None if a is None else np.ascontiguousarray(np.broadcast_to(a, (n,)), dtype=np.int32)
+        g, c, npp = as32(weight_group), as32(weight_class), as32(n_primary_parts)
+        ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.int64)
+        rc = _lib.lib().pmc_coag_gpu_upload(self.ctx, pop, n, dp(vol), ip(g), ip(c), lp(ids), ip(npp))
+        check(rc, "pmc_coag_gpu_upload")
+        if n_comp is not None:
+            nc = as32(n_comp)
+            cs = np.ascontiguousarray(comp_source, dtype=np.int32).reshape(n, MAX_AERO_COMPONENT_SIZE)
+            ct = np.ascontiguousarray(comp_create_time, dtype=np.float64).reshape(n, MAX_AERO_COMPONENT_SIZE)
+            rc = _lib.lib().pmc_coag_gpu_upload_components(self.ctx, pop, n, ip(nc), ip(cs), dp(ct))
+            check(rc, "pmc_coag_gpu_upload_components")
+
+    def n_part(self, pop=0):
+        n = ctypes.c_int()
+        check(_lib.lib().pmc_coag_gpu_n_part(self.ctx, pop, ctypes.byref(n)), "pmc_coag_gpu_n_part")
+        return n.value
+
+    def particles(self, pop=0, components=False):
+        n = self.n_part(pop)
+        out = {
+            "vol": np.empty((n, self.aero_data.n_spec), dtype=np.float64),
+            "weight_group": np.empty(n, dtype=np.int32),
+            "weight_class": np.empty(n, dtype=np.int32),
+            "id": np.empty(n, dtype=np.int64),
+            "n_primary_parts": np.empty(n, dtype=np.int32),
+        }
+        got = ctypes.c_int()
+        rc = _lib.lib().pmc_coag_gpu_download(self.ctx, pop, n, dp(out["vol"]), ip(out["weight_group"]),
+                                              ip(out["weight_class"]), lp(out["id"]), ip(out["n_primary_parts"]),
+                                              ctypes.byref(got))
+        check(rc, "pmc_coag_gpu_download")
+        if components:
+            out["n_comp"] = np.empty(n, dtype=np.int32)
+            out["comp_source"] = np.empty((n, MAX_AERO_COMPONENT_SIZE), dtype=np.int32)
+            out["comp_create_time"] = np.empty((n, MAX_AERO_COMPONENT_SIZE), dtype=np.float64)
+            rc = _lib.lib().pmc_coag_gpu_download_components(self.ctx, pop, n, ip(out["n_comp"]),
+                                                             ip(out["comp_source"]), dp(out["comp_create_time"]))
+            check(rc, "pmc_coag_gpu_download_components")
+        return out
+
+    def set_next_id(self, next_id, pop=0):
+        check(_lib.lib().pmc_coag_gpu_set_next_id(self.ctx, pop, int(next_id)), "pmc_coag_gpu_set_next_id")
+
+    def next_id(self, pop=0):
+        v = ctypes.c_int64()
+        check(_lib.lib().pmc_coag_gpu_get_next_id(self.ctx, pop, ctypes.byref(v)), "pmc_coag_gpu_get_next_id")
+        return v.value
+
+    def set_replay(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        check(_lib.lib().pmc_coag_gpu_replay_set(self.ctx, dp(u), u.size), "pmc_coag_gpu_replay_set")
+
+    def replay_used(self):
+        v = ctypes.c_int64()
+        check(_lib.lib().pmc_coag_gpu_replay_used(self.ctx, ctypes.byref(v)), "pmc_coag_gpu_replay_used")
+        return v.value
+
+    def stats(self):
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(_lib.lib().pmc_coag_gpu_stats(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+              "pmc_coag_gpu_stats")
+        return {"kmax_violations": a.value, "redraws": b.value, "rounds": c.value}
+
+    def sort(self, pop=0, max_bin=256):
+        n = self.n_part(pop)
+        nb = ctypes.c_int()
+        edges = np.zeros(max_bin + 1)
+        counts = np.zeros(max_bin * self.awa.n_class, dtype=np.int32)
+        bins = np.zeros(max(n, 1), dtype=np.int32)
+        rc = _lib.lib().pmc_coag_gpu_sort(self.ctx, pop, ctypes.byref(nb), dp(edges), max_bin, ip(counts), ip(bins))
+        check(rc, "pmc_coag_gpu_sort")
+        k = nb.value
+        return edges[:k + 1], counts[:k * self.awa.n_class].reshape(self.awa.n_class, k).T, bins[:n]
+
+    def kmax_table(self, coag_kernel_type, env_state, max_bin=256):
+        out = np.zeros(max_bin * max_bin)
+        rc = _lib.lib().pmc_coag_gpu_kmax_table(self.ctx, coag_kernel_type, env_state.temp, env_state.pressure,
+                                                env_state.additive_kernel_coefficient, dp(out), max_bin)
+        check(rc, "pmc_coag_gpu_kmax_table")
+        return out
+
+    def eval_kernel(self, coag_kernel_type, env_state, vol1, c1, vol2, c2, c_ij):
+        vol1 = np.ascontiguousarray(vol1, dtype=np.float64)
+        vol2 = np.ascontiguousarray(vol2, dtype=np.float64)
+        n = vol1.shape[0]
+        c1 = np.ascontiguousarray(np.broadcast_to(c1, (n,)), dtype=np.int32)
+        c2 = np.ascontiguousarray(np.broadcast_to(c2, (n,)), dtype=np.int32)
+        cij = np.ascontiguousarray(np.broadcast_to(c_ij, (n,)), dtype=np.int32)
+        out = np.zeros(n)
+        rc = _lib.lib().pmc_coag_gpu_eval_kernel(self.ctx, coag_kernel_type, env_state.temp, env_state.pressure,
+                                                 env_state.additive_kernel_coefficient, n, dp(vol1), ip(c1),
+                                                 dp(vol2), ip(c2), ip(cij), dp(out))
+        check(rc, "pmc_coag_gpu_eval_kernel")
+        return out
+
+
+def mc_coag(coag_kernel_type, env_state, aero_data, aero_state, del_t):
+    """Do coagulation for time del_t (coagulation.F90:43-96).
+
+    Returns (tot_n_samp, tot_n_coag), the reference's counters of samples
+    tested and coagulation events.  Raises PmcError where the reference would
+    stop (e.g. a coagulated particle outside the bin grid).
+    """
+    if aero_data is not aero_state.aero_data and aero_data.n_spec != aero_state.aero_data.n_spec:
+        raise ValueError("aero_data does not match aero_state")
+    a, b = ctypes.c_int(), ctypes.c_int()
+    rc = _lib.lib().pmc_coag_gpu_step(aero_state.ctx, int(coag_kernel_type), env_state.temp, env_state.pressure,
+                                      env_state.additive_kernel_coefficient, float(del_t), ctypes.byref(a),
+                                      ctypes.byref(b))
+    check(rc, "mc_coag")
+    return a.value, b.value
+
+
+def mc_coag_batch(coag_kernel_type, temps, pressures, additive_kernel_coefficient, aero_state, del_t, n_steps=1):
+    """Advance every population of a batched AeroState by n_steps steps.
+    Returns (tot_n_samp, tot_n_coag) summed over populations and steps."""
+    t = np.ascontiguousarray(np.broadcast_to(temps, (aero_state.n_pop,)), dtype=np.float64)
+    p = np.ascontiguousarray(np.broadcast_to(pressures, (aero_state.n_pop,)), dtype=np.float64)
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    rc = _lib.lib().pmc_coag_gpu_step_batch(aero_state.ctx, int(coag_kernel_type), dp(t), dp(p),
+                                            float(additive_kernel_coefficient), float(del_t), int(n_steps),
+                                            ctypes.byref(a), ctypes.byref(b))
+    check(rc, "mc_coag_batch")
+    return a.value, b.value

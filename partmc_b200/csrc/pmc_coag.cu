@@ -1,0 +1,1725 @@
+// pmc_coag.cu -- host orchestration and C ABI of the B200 coagulation step.
+//
+// The C ABI (include/pmc_coag_gpu.h) is the drop-in for mc_coag
+// (coagulation.F90:43-96).  A context owns one or more particle
+// populations resident in HBM; a step runs the rounds described in
+// pmc_kernels.cuh over all populations at once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/pmc_coag_gpu.h"
+#include "pmc_kernels.cuh"
+#include "pmc_merge.cuh"
+#include "pmc_replay.cuh"
+
+using namespace pmc;
+
+namespace {
+
+inline void note_launch();
+
+// ---------------------------------------------------------------------------
+// exclusive scan of n values into out[0..n] (out[n] = total), three kernels
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <class T>
+__global__ void k_scan_reduce(const T* in, long long n, long long* bsum) {
+  long long base = (long long)blockIdx.x * kScanTile;
+  long long s = 0;
+  for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
+    long long i = base + k;
+    if (i < n) s += (long long)in[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ long long ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += ws[k];
+    bsum[blockIdx.x] = t;
+  }
+}
+
+__device__ long long block_excl_scan_ll(long long v, long long* total) {
+  __shared__ long long ws[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  long long x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[wid] = x;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  if (wid == 0) {
+    long long s = lane < nw ? ws[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    ws[lane] = s;
+  }
+  __syncthreads();
+  long long pre = (wid > 0 ? ws[wid - 1] : 0) + x - v;
+  if (total) *total = ws[nw - 1];
+  __syncthreads();
+  return pre;
+}
+
+// exclusive scan of the block sums, in place (single block, any count)
+__global__ void k_scan_bsum(long long* bsum, int nb, long long* out_total) {
+  long long carry = 0;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    long long v = i < nb ? bsum[i] : 0;
+    long long tot;
+    long long pre = block_excl_scan_ll(v, &tot);
+    if (i < nb) bsum[i] = carry + pre;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *out_total = carry;
+}
+
+template <class T>
+__global__ void k_scan_final(const T* in, long long n, const long long* bsum, long long* out) {
+  long long base = (long long)blockIdx.x * kScanTile;
+  long long v[kScanItems];
+  long long s = 0;
+  for (int k = 0; k < kScanItems; k++) {
+    long long i = base + (long long)threadIdx.x * kScanItems + k;
+    v[k] = i < n ? (long long)in[i] : 0;
+    s += v[k];
+  }
+  long long pre = block_excl_scan_ll(s, nullptr) + bsum[blockIdx.x];
+  for (int k = 0; k < kScanItems; k++) {
+    long long i = base + (long long)threadIdx.x * kScanItems + k;
+    if (i < n) out[i] = pre;
+    pre += v[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// small helper kernels
+
+__global__ void k_fill_u32(unsigned* p, long long n, unsigned v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void k_compact_flags(const uint8_t* flag, const long long* off, long long n,
+                                long long* outw) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    if (flag[i]) outw[off[i]] = i;
+}
+
+// target operations of round 0, in the reference's backwards target order
+// (coagulation.F90:220-237)
+__global__ void k_build_ops(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
+                            const long long* pp_off, const long long* prio_off, int n_gpairs,
+                            int* op_pop, int* op_pair, int* op_slot, int* op_k, unsigned* op_prio) {
+  int gp = blockIdx.x;
+  if (gp >= n_gpairs) return;
+  long long n = pp_off[gp + 1] - pp_off[gp];
+  if (n == 0) return;
+  int pop = gpair_pop[gp];
+  const PopDev& P = pops[pop];
+  int p = gpair_local[gp];
+  const PairState& S = P.pair[p];
+  int tcell = S.bt + P.grid->n_bin * S.ct;
+  int start = P.cell_start[tcell];
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    long long q = pp_off[gp] + k;
+    op_pop[q] = pop;
+    op_pair[q] = p;
+    op_slot[q] = P.list[start + (int)(n - 1 - k)];
+    op_k[q] = (int)k;
+    op_prio[q] = (unsigned)(prio_off[gp] + k);
+  }
+}
+
+// redo list of lost target operations (order of q kept)
+__global__ void k_build_redo(const int* op_pop, const int* op_pair, const int* op_slot,
+                             const int* op_k, const int* lost, const long long* lost_off,
+                             long long Q, int* r_pop, int* r_pair, int* r_slot, int* r_k,
+                             unsigned* r_prio, unsigned prio_base) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
+       q += (long long)gridDim.x * blockDim.x) {
+    if (!lost[q]) continue;
+    long long j = lost_off[q];
+    r_pop[j] = op_pop[q];
+    r_pair[j] = op_pair[q];
+    r_slot[j] = op_slot[q];
+    r_k[j] = op_k[q] + (1 << 24);  // fresh random stream for the redo
+    r_prio[j] = prio_base + (unsigned)j;
+  }
+}
+
+// per-population bases of the allocations of one round: events are ordered
+// by population, so a global exclusive rank minus the count of earlier
+// populations is the rank inside the population.
+__global__ void k_alloc_bases(const PopDev* pops, int n_pop, const int* set_slots,
+                              const int* set_ids, const int* pp_slots, const int* pp_ids,
+                              int* set_slot_base, long long* set_id_base, int* pp_slot_base,
+                              long long* pp_id_base) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  long long cs = 0, ci = 0, ps = 0, pi = 0;
+  for (int k = 0; k < n_pop; k++) {
+    PopCtr* c = pops[k].ctr;
+    set_slot_base[k] = c->n_slots - (int)cs;
+    set_id_base[k] = c->next_id - ci;
+    pp_slot_base[k] = c->n_slots + set_slots[k] - (int)ps;
+    pp_id_base[k] = c->next_id + set_ids[k] - pi;
+    cs += set_slots[k];
+    ci += set_ids[k];
+    ps += pp_slots[k];
+    pi += pp_ids[k];
+  }
+}
+
+__global__ void k_count_per_pop(const int* need, const long long* n_items, const int* item_pop_of,
+                                const long long* ev_w, const long long* work_off, int n_gpairs,
+                                const int* gpair_pop, int* per_pop) {
+  // need[e] summed per population; population of item e is item_pop_of[e]
+  // when given, else found through ev_w/work_off (per-set events)
+  long long n = *n_items;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (!need[e]) continue;
+    int pop;
+    if (item_pop_of) pop = item_pop_of[e];
+    else pop = gpair_pop[find_pair(work_off, n_gpairs, ev_w[e])];
+    atomicAdd(&per_pop[pop], need[e]);
+  }
+}
+
+__global__ void k_alloc_finish(const PopDev* pops, int n_pop, const int* set_slots,
+                               const int* set_ids, const int* pp_slots, const int* pp_ids) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pop) return;
+  PopCtr* c = pops[k].ctr;
+  c->n_slots += set_slots[k] + pp_slots[k];
+  c->next_id += set_ids[k] + pp_ids[k];
+}
+
+// particle upload: transpose particle-major volumes into species-major slots
+__global__ void k_upload(PopDev P, int n, const double* vol_pm, const int* grp, const int* cls,
+                         const long long* id, const int* nprim, long long id0) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double vt = 0.0, ms = 0.0;
+    for (int s = 0; s < P.n_spec; s++) {
+      double v = vol_pm[(size_t)i * P.n_spec + s];
+      P.vol[(size_t)s * P.cap + i] = v;
+      vt = vt + v;
+    }
+    for (int s = 0; s < P.n_spec; s++) ms = ms + P.vol[(size_t)s * P.cap + i] * P.density[s];
+    P.vtot[i] = vt;
+    P.mass[i] = ms;
+    P.grp[i] = grp ? grp[i] : 1;
+    P.cls[i] = cls ? cls[i] : 1;
+    P.id[i] = id ? id[i] : id0 + i;
+    P.nprim[i] = nprim ? nprim[i] : 1;
+    P.ncomp[i] = 1;
+    P.csrc[i] = 1;
+    P.ctime[i] = 0.0;
+    P.lct[i] = 0.0;
+    P.gct[i] = 0.0;
+    P.imf[i] = 0.0;
+    P.den_ice[i] = __longlong_as_double(0x7ff8000000000000LL);
+    P.phi[i] = __longlong_as_double(0x7ff8000000000000LL);
+    P.hyst[i] = 0;
+    P.frozen[i] = 0;
+    P.alive[i] = 1;
+  }
+}
+
+// gather live slots in slot order into the particle-major output
+__global__ void k_download(PopDev P, const long long* live_off, int n_slots, double* vol_pm,
+                           int* grp, int* cls, long long* id, int* nprim, int* ncomp, int* csrc,
+                           double* ctime) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += gridDim.x * blockDim.x) {
+    if (!P.alive[i]) continue;
+    long long j = live_off[i];
+    for (int s = 0; s < P.n_spec; s++) vol_pm[j * P.n_spec + s] = P.vol[(size_t)s * P.cap + i];
+    grp[j] = P.grp[i];
+    cls[j] = P.cls[i];
+    id[j] = P.id[i];
+    nprim[j] = P.nprim[i];
+    ncomp[j] = P.ncomp[i];
+    for (int k = 0; k < kMaxComponent; k++) {
+      csrc[j * kMaxComponent + k] = k < P.ncomp[i] ? P.csrc[(size_t)k * P.cap + i] : 0;
+      ctime[j * kMaxComponent + k] = k < P.ncomp[i] ? P.ctime[(size_t)k * P.cap + i] : 0.0;
+    }
+  }
+}
+
+// move live slots of src into dst compactly (relayout)
+__global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_slots,
+                           int compact) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += gridDim.x * blockDim.x) {
+    if (compact && !S.alive[i]) continue;
+    int j = compact ? (int)live_off[i] : i;
+    for (int s = 0; s < S.n_spec; s++) D.vol[(size_t)s * D.cap + j] = S.vol[(size_t)s * S.cap + i];
+    D.vtot[j] = S.vtot[i];
+    D.mass[j] = S.mass[i];
+    D.rad[j] = S.rad[i];
+    D.grp[j] = S.grp[i];
+    D.cls[j] = S.cls[i];
+    D.id[j] = S.id[i];
+    D.nprim[j] = S.nprim[i];
+    D.ncomp[j] = S.ncomp[i];
+    for (int k = 0; k < S.ncomp[i]; k++) {
+      D.csrc[(size_t)k * D.cap + j] = S.csrc[(size_t)k * S.cap + i];
+      D.ctime[(size_t)k * D.cap + j] = S.ctime[(size_t)k * S.cap + i];
+    }
+    D.lct[j] = S.lct[i];
+    D.gct[j] = S.gct[i];
+    D.imf[j] = S.imf[i];
+    D.den_ice[j] = S.den_ice[i];
+    D.phi[j] = S.phi[i];
+    D.hyst[j] = S.hyst[i];
+    D.frozen[j] = S.frozen[i];
+    D.alive[j] = S.alive[i];
+    D.bin[j] = S.bin[i];
+    D.claim[j] = S.claim[i];
+  }
+}
+
+__global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, const double* v2,
+                              const int* c2, const int* cij, double* out, int precision) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // records of the two particles, built as the sort pass builds them
+  double vt1 = 0.0, vt2 = 0.0, m1 = 0.0, m2 = 0.0;
+  for (int s = 0; s < P.n_spec; s++) {
+    vt1 = vt1 + v1[(size_t)i * P.n_spec + s];
+    vt2 = vt2 + v2[(size_t)i * P.n_spec + s];
+  }
+  for (int s = 0; s < P.n_spec; s++) {
+    m1 = m1 + v1[(size_t)i * P.n_spec + s] * P.density[s];
+    m2 = m2 + v2[(size_t)i * P.n_spec + s] * P.density[s];
+  }
+  RecD q[2];
+  double vt[2] = {vt1, vt2}, ms[2] = {m1, m2};
+  int cl[2] = {c1[i] - 1, c2[i] - 1};
+  for (int k = 0; k < 2; k++) {
+    double r = vol2rad(vt[k]);
+    q[k].r = r;
+    q[k].rv = rad2vol(r);
+    q[k].nc = num_conc_at_radius<double>(P.w, cl[k], r);
+    q[k].a = q[k].b = q[k].c = 0.0;
+    if (P.kernel_type == kKernelAdditive) q[k].a = vt[k];
+    if (P.kernel_type == kKernelBrown) {
+      BrownPart bp = brown_part(P.benv, vt[k], ms[k] / vt[k]);
+      q[k].a = bp.diffus;
+      q[k].b = bp.speedsq;
+      q[k].c = bp.deltasq;
+    }
+    if (P.kernel_type == kKernelSedi) q[k].a = fall_g(vol2rad(vt[k]));
+  }
+  int cc = cij[i] - 1;
+  double k;
+  if (precision == 0) {
+    const double* a = (const double*)&q[0];
+    const double* b = (const double*)&q[1];
+    switch (P.kernel_type) {
+      case kKernelAdditive: k = pair_kernel<kKernelAdditive, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
+      case kKernelConstant: k = pair_kernel<kKernelConstant, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
+      case kKernelBrown: k = pair_kernel<kKernelBrown, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
+      case kKernelSedi: k = pair_kernel<kKernelSedi, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
+      default: k = 0.0;
+    }
+  } else {
+    float a[6], b[6];
+    const double* qa = (const double*)&q[0];
+    const double* qb = (const double*)&q[1];
+    for (int j = 0; j < 6; j++) {
+      a[j] = (float)qa[j];
+      b[j] = (float)qb[j];
+    }
+    float kf;
+    switch (P.kernel_type) {
+      case kKernelAdditive: kf = pair_kernel<kKernelAdditive, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
+      case kKernelConstant: kf = pair_kernel<kKernelConstant, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
+      case kKernelBrown: kf = pair_kernel<kKernelBrown, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
+      case kKernelSedi: kf = pair_kernel<kKernelSedi, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
+      default: kf = 0.f;
+    }
+    k = kf;
+  }
+  out[i] = k;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+#define CK(x)                                                          \
+  do {                                                                 \
+    cudaError_t e_ = (x);                                              \
+    if (e_ != cudaSuccess) {                                           \
+      snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", #x, \
+               cudaGetErrorString(e_), __FILE__, __LINE__);            \
+      throw Fail(PMC_ERR_CUDA);                                        \
+    }                                                                  \
+  } while (0)
+
+char g_last_error[512];
+// kernel launches issued by this library (for the benchmark's launch count)
+long long g_launches = 0;
+inline void note_launch() { ++g_launches; }
+
+struct Fail {
+  int code;
+  explicit Fail(int c) : code(c) {}
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void reserve(size_t m) {
+    if (m <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t want = std::max<size_t>(m, 1024);
+    if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) {
+      p = nullptr;
+      throw Fail(PMC_ERR_CAPACITY);
+    }
+    n = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct PopHost {
+  PopDev h{};
+  bool valid_sort = false;
+  int n_bin = 0;
+  std::vector<double> edges, centers;
+  std::vector<PairDesc> pair_desc;
+  // owned allocations (freed on relayout / destroy)
+  std::vector<void*> slot_allocs;
+  std::vector<void*> sort_allocs;
+  std::vector<void*> fixed_allocs;
+  uint64_t seed = 1;
+  uint32_t step = 0;
+  int kmax_kt = 0;  // kernel type of the current k_max table
+  int chunk_hist_cap = 0;
+};
+
+struct Ctx {
+  int n_pop = 1, n_spec = 1, n_group = 1, n_class = 1, i_water = 0;
+  std::vector<double> density;
+  Weights w{};
+  int mode = PMC_MODE_FP64;
+  std::vector<PopHost> pops;
+  PopDev* d_pops = nullptr;
+  PopCtr* d_ctrs = nullptr;  // one counter block per population
+  std::vector<PopCtr> h_ctrs;
+  cudaStream_t stream = nullptr;
+  int max_rounds = 32;
+  // per-round buffers
+  DevBuf<int> gpair_pop, gpair_local;
+  DevBuf<long long> pop_pair_base;
+  DevBuf<long long> nwork_set, nwork_pp, nprio, work_off, pp_off, prio_off;
+  DevBuf<int> pair_losers;
+  DevBuf<uint8_t> flag, win_set, win_pp;
+  DevBuf<int2> ev;
+  DevBuf<long long> flag_off, ev_w;
+  DevBuf<int> need_slot_set, need_id_set, need_slot_pp, need_id_pp, lost_pp;
+  DevBuf<long long> rank_slot_set, rank_id_set, rank_slot_pp, rank_id_pp, lost_off;
+  DevBuf<int> op_pop, op_pair, op_slot, op_k, r_pop, r_pair, r_slot, r_k;
+  DevBuf<unsigned> op_prio, r_prio;
+  DevBuf<PPResult> pp_res;
+  DevBuf<double> pp_vol;
+  DevBuf<int> per_pop_i;  // 4 x n_pop counters
+  DevBuf<int> slot_base_set, slot_base_pp;
+  DevBuf<long long> id_base_set, id_base_pp;
+  DevBuf<long long> scan_bsum, scan_total;
+  DevBuf<long long> n_dev;  // device scalars
+  long long h_total = 0;
+  // stats of the last step
+  long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
+  // optional per-kernel timing with CUDA events on the library's stream:
+  // 0 pair tests, 1 sort scatter + record build, 2 sort histogram,
+  // 3 whole steps
+  bool prof = false;
+  cudaEvent_t prof_ev[2] = {nullptr, nullptr};
+  double prof_ms[4] = {0, 0, 0, 0};
+  long long prof_launch[4] = {0, 0, 0, 0}, prof_units[4] = {0, 0, 0, 0};
+  // replay
+  DevBuf<double> replay_u;
+  long long replay_n = 0, replay_used = 0;
+  ReplayBuffers replay;
+};
+
+void free_list(std::vector<void*>& v) {
+  for (void* p : v) cudaFree(p);
+  v.clear();
+}
+
+template <class T>
+T* dalloc(std::vector<void*>& owner, size_t n) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) throw Fail(PMC_ERR_CAPACITY);
+  owner.push_back(p);
+  return (T*)p;
+}
+
+int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return (int)b;
+}
+
+// times the launches issued inside its scope when profiling is on
+struct ProfScope {
+  Ctx& c;
+  int id;
+  long long units;
+  ProfScope(Ctx& c_, int id_, long long units_) : c(c_), id(id_), units(units_) {
+    if (c.prof) cudaEventRecord(c.prof_ev[0], c.stream);
+  }
+  ~ProfScope() {
+    if (!c.prof) return;
+    cudaEventRecord(c.prof_ev[1], c.stream);
+    cudaEventSynchronize(c.prof_ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c.prof_ev[0], c.prof_ev[1]);
+    c.prof_ms[id] += ms;
+    c.prof_launch[id] += 1;
+    c.prof_units[id] += units;
+  }
+};
+
+template <class T>
+long long scan(Ctx& c, const T* in, long long n, long long* out, bool read_total) {
+  int nb = (int)((n + kScanTile - 1) / kScanTile);
+  if (nb < 1) nb = 1;
+  c.scan_bsum.reserve(nb + 1);
+  c.scan_total.reserve(2);
+  k_scan_reduce<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_bsum.p); note_launch();
+  k_scan_bsum<<<1, kScanThreads, 0, c.stream>>>(c.scan_bsum.p, nb, out + n); note_launch();
+  k_scan_final<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_bsum.p, out); note_launch();
+  if (!read_total) return -1;
+  long long t = 0;
+  CK(cudaMemcpyAsync(&t, out + n, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return t;
+}
+
+void push_pops(Ctx& c) {
+  std::vector<PopDev> v(c.n_pop);
+  for (int k = 0; k < c.n_pop; k++) v[k] = c.pops[k].h;
+  CK(cudaMemcpyAsync(c.d_pops, v.data(), sizeof(PopDev) * c.n_pop, cudaMemcpyHostToDevice, c.stream));
+}
+
+// counters of every population in one copy
+std::vector<PopCtr>& read_ctrs(Ctx& c) {
+  c.h_ctrs.resize(c.n_pop);
+  CK(cudaMemcpyAsync(c.h_ctrs.data(), c.d_ctrs, sizeof(PopCtr) * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return c.h_ctrs;
+}
+
+void write_ctrs(Ctx& c) {
+  CK(cudaMemcpyAsync(c.d_ctrs, c.h_ctrs.data(), sizeof(PopCtr) * c.n_pop, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+}
+
+PopCtr read_ctr(Ctx& c, int k) { return read_ctrs(c)[k]; }
+
+void write_ctr(Ctx& c, int k, const PopCtr& r) {
+  CK(cudaMemcpyAsync(c.d_ctrs + k, &r, sizeof(PopCtr), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+}
+
+// allocate the slot arrays of a population with capacity cap
+void alloc_slots(Ctx& c, PopHost& ph, int cap) {
+  PopDev& h = ph.h;
+  std::vector<void*>& o = ph.slot_allocs;
+  h.cap = cap;
+  h.vol = dalloc<double>(o, (size_t)cap * c.n_spec);
+  h.vtot = dalloc<double>(o, cap);
+  h.mass = dalloc<double>(o, cap);
+  h.rad = dalloc<double>(o, cap);
+  h.grp = dalloc<int>(o, cap);
+  h.cls = dalloc<int>(o, cap);
+  h.id = dalloc<long long>(o, cap);
+  h.nprim = dalloc<int>(o, cap);
+  h.ncomp = dalloc<int>(o, cap);
+  h.csrc = dalloc<int>(o, (size_t)cap * kMaxComponent);
+  h.ctime = dalloc<double>(o, (size_t)cap * kMaxComponent);
+  h.lct = dalloc<double>(o, cap);
+  h.gct = dalloc<double>(o, cap);
+  h.imf = dalloc<double>(o, cap);
+  h.den_ice = dalloc<double>(o, cap);
+  h.phi = dalloc<double>(o, cap);
+  h.hyst = dalloc<int>(o, cap);
+  h.frozen = dalloc<int>(o, cap);
+  h.alive = dalloc<uint8_t>(o, cap);
+  h.bin = dalloc<int>(o, cap);
+  h.list = dalloc<int>(o, cap);
+  h.recd = dalloc<RecD>(o, cap);
+  h.recf = dalloc<RecF>(o, cap);
+  h.claim = dalloc<unsigned>(o, cap);
+  CK(cudaMemsetAsync(h.alive, 0, cap, c.stream));
+}
+
+// sort structures that depend on the grid and the slot count
+void alloc_sort(Ctx& c, PopHost& ph) {
+  PopDev& h = ph.h;
+  free_list(ph.sort_allocs);
+  std::vector<void*>& o = ph.sort_allocs;
+  int nb = std::max(ph.n_bin, 1);
+  h.n_cells = nb * c.n_class;
+  ph.chunk_hist_cap = 0;  // reallocated by the sort when needed
+  h.chunk_hist = nullptr;
+  h.cell_count = dalloc<int>(o, h.n_cells);
+  h.cell_start = dalloc<int>(o, h.n_cells + 1);
+  h.kmax_tab = dalloc<double>(o, (size_t)nb * nb);
+  // pairs in the reference's loop order (coagulation.F90:74-94)
+  ph.pair_desc.clear();
+  for (int c1 = 0; c1 < c.n_class; c1++)
+    for (int c2 = 0; c2 <= c1; c2++)
+      for (int b1 = 0; b1 < ph.n_bin; b1++)
+        for (int b2 = (c1 == c2 ? b1 : 0); b2 < ph.n_bin; b2++) {
+          PairDesc d;
+          d.b1 = (int16_t)b1;
+          d.b2 = (int16_t)b2;
+          d.c1 = (int8_t)c1;
+          d.c2 = (int8_t)c2;
+          d.pad0 = d.pad1 = 0;
+          ph.pair_desc.push_back(d);
+        }
+  h.n_pairs = (int)ph.pair_desc.size();
+  PairDesc* pd = dalloc<PairDesc>(o, std::max<size_t>(ph.pair_desc.size(), 1));
+  if (!ph.pair_desc.empty())
+    CK(cudaMemcpyAsync(pd, ph.pair_desc.data(), sizeof(PairDesc) * ph.pair_desc.size(),
+                       cudaMemcpyHostToDevice, c.stream));
+  h.pair_desc = pd;
+  h.pair = dalloc<PairState>(o, std::max<size_t>(ph.pair_desc.size(), 1));
+  h.kmax_valid = 0;
+}
+
+// bin_grid_make (log) on the host, with glibc's log/exp like the reference
+void make_grid(Ctx& c, PopHost& ph, int n_bin, double rmin, double rmax) {
+  ph.n_bin = n_bin;
+  ph.edges.assign(n_bin + 1, 0.0);
+  ph.centers.assign(std::max(n_bin, 1), 0.0);
+  if (n_bin > 0) {
+    auto linspace = [](double a, double b, int n, double* out) {
+      for (int i = 2; i <= n - 1; i++) {
+        double t = (double)(i - 1) / (double)(n - 1);
+        out[i - 1] = (1.0 - t) * a + t * b;
+      }
+      if (n > 0) {
+        out[0] = a;
+        out[n - 1] = b;
+      }
+    };
+    auto logspace = [&](double a, double b, int n, double* out) {
+      if (n == 0) return;
+      linspace(log(a), log(b), n, out);
+      for (int i = 0; i < n; i++) out[i] = exp(out[i]);
+      out[0] = a;
+      out[n - 1] = b;
+    };
+    logspace(rmin, rmax, n_bin + 1, ph.edges.data());
+    double c1 = exp(interp_linear_disc(log(rmin), log(rmax), 2 * n_bin + 1, 2));
+    double c2 = exp(interp_linear_disc(log(rmin), log(rmax), 2 * n_bin + 1, 2 * n_bin));
+    logspace(c1, c2, n_bin, ph.centers.data());
+  }
+  GridDev g{};
+  g.n_bin = n_bin;
+  if (n_bin > 0) {
+    g.log_lo = log(ph.edges[0]);
+    g.log_hi = log(ph.edges[n_bin]);
+    for (int i = 0; i <= n_bin; i++) g.edges[i] = ph.edges[i];
+    for (int i = 0; i < n_bin; i++) g.centers[i] = ph.centers[i];
+  }
+  CK(cudaMemcpyAsync(ph.h.grid, &g, sizeof(GridDev), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  alloc_sort(c, ph);
+}
+
+void set_params(Ctx& c, PopHost& ph) {
+  PopDev& h = ph.h;
+  h.n_spec = c.n_spec;
+  h.n_group = c.n_group;
+  h.n_class = c.n_class;
+  h.i_water = c.i_water;
+  h.w = c.w;
+  h.flat = weights_flat(c.w);
+  bool inc, dec;
+  weight_monotonicity(c.w, &inc, &dec);
+  h.mono_dec = dec;
+  h.dmin = *std::min_element(c.density.begin(), c.density.end());
+  h.dmax = *std::max_element(c.density.begin(), c.density.end());
+  h.seed = ph.seed;
+}
+
+void init_pop(Ctx& c, PopHost& ph, int cap) {
+  std::vector<void*>& o = ph.fixed_allocs;
+  ph.h.ctr = c.d_ctrs + (&ph - c.pops.data());
+  ph.h.grid = dalloc<GridDev>(o, 1);
+  double* dens = dalloc<double>(o, c.n_spec);
+  CK(cudaMemcpy(dens, c.density.data(), sizeof(double) * c.n_spec, cudaMemcpyHostToDevice));
+  ph.h.density = dens;
+  set_params(c, ph);
+  alloc_slots(c, ph, cap);
+  PopCtr z{};
+  z.next_id = 1;
+  z.bmin = 1 << 30;
+  z.bmax = -1;
+  write_ctr(c, (int)(&ph - c.pops.data()), z);
+  ph.n_bin = 0;
+  GridDev g{};
+  CK(cudaMemcpyAsync(ph.h.grid, &g, sizeof(GridDev), cudaMemcpyHostToDevice, c.stream));
+  alloc_sort(c, ph);
+}
+
+// grow (compact = false, slot numbers kept) or compact (slot order kept)
+void relayout(Ctx& c, int k, int new_cap, bool compact) {
+  PopHost& ph = c.pops[k];
+  PopCtr r = read_ctr(c, k);
+  PopDev old = ph.h;
+  std::vector<void*> old_allocs;
+  old_allocs.swap(ph.slot_allocs);
+  alloc_slots(c, ph, new_cap);
+  DevBuf<long long> off;
+  off.reserve((size_t)r.n_slots + 1);
+  long long n_live = r.n_slots;
+  if (compact) n_live = scan(c, old.alive, r.n_slots, off.p, true);
+  if (r.n_slots > 0)
+    k_relayout<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(old, ph.h, off.p, r.n_slots,
+                                                               compact ? 1 : 0); note_launch();
+  CK(cudaStreamSynchronize(c.stream));
+  off.release();
+  free_list(old_allocs);
+  if (compact) r.n_slots = (int)n_live;
+  write_ctr(c, k, r);
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+}
+
+// ---------------------------------------------------------------------------
+// sort, with the grid decision of aero_sorted_remake_if_needed
+// (aero_sorted.F90:214-373)
+
+__global__ void k_radius_minmax_masked(const PopDev* pops, const uint8_t* on) {
+  if (!on[blockIdx.y]) return;
+  const PopDev& P = pops[blockIdx.y];
+  int n = P.ctr->n_slots;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!P.alive[i]) continue;
+    double r = vol2rad(P.vtot[i]);
+    unsigned long long b = (unsigned long long)__double_as_longlong(r);
+    atomicMin(&P.ctr->rmin_bits, b);
+    atomicMax(&P.ctr->rmax_bits, b);
+  }
+}
+
+void prepare_chunks(Ctx& c) {
+  std::vector<PopCtr>& r = read_ctrs(c);
+  for (int k = 0; k < c.n_pop; k++) {
+    PopHost& ph = c.pops[k];
+    ph.h.n_chunks = (r[k].n_slots + kChunk - 1) / kChunk;
+    int need = std::max(ph.h.n_chunks, 1) * ph.h.n_cells;
+    if (need > ph.chunk_hist_cap) {
+      int want = std::max(need, 1024);
+      ph.h.chunk_hist = dalloc<int>(ph.sort_allocs, want);
+      ph.chunk_hist_cap = want;
+    }
+  }
+}
+
+// histogram + scan of every population with its current grid
+void run_hist_scan(Ctx& c) {
+  prepare_chunks(c);
+  std::vector<PopCtr>& r = read_ctrs(c);
+  for (int k = 0; k < c.n_pop; k++) {
+    r[k].bmin = 1 << 30;
+    r[k].bmax = -1;
+    r[k].out_of_grid = 0;
+  }
+  write_ctrs(c);
+  push_pops(c);
+  int max_chunks = 1, max_cells = 1;
+  for (int k = 0; k < c.n_pop; k++) {
+    max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
+    max_cells = std::max(max_cells, c.pops[k].h.n_cells);
+  }
+  dim3 g(max_chunks, c.n_pop);
+  {
+    long long units = 0;
+    for (int k = 0; k < c.n_pop; k++) units += (long long)r[k].n_slots;
+    ProfScope ps(c, 2, units);
+    k_sort_hist<<<g, kSortThreads, sizeof(int) * max_cells, c.stream>>>(c.d_pops); note_launch();
+  }
+  k_sort_scan<<<c.n_pop, 1024, 0, c.stream>>>(c.d_pops); note_launch();
+}
+
+// aero_state_sort: grid decision (remake_if_needed) then the sort itself
+void sort_pops(Ctx& c, bool decide_grid) {
+  bool hist_current = false;
+  if (decide_grid) {
+    // radius range of populations without a valid sort
+    std::vector<uint8_t> on(c.n_pop, 0);
+    bool any = false;
+    std::vector<PopCtr>& r = read_ctrs(c);
+    int max_slots = 1;
+    for (int k = 0; k < c.n_pop; k++) {
+      if (!c.pops[k].valid_sort) {
+        on[k] = 1;
+        any = true;
+        r[k].rmin_bits = 0x7ff0000000000000ULL;
+        r[k].rmax_bits = 0;
+        max_slots = std::max(max_slots, r[k].n_slots);
+      }
+    }
+    if (any) {
+      write_ctrs(c);
+      DevBuf<uint8_t> don;
+      don.reserve(c.n_pop);
+      CK(cudaMemcpyAsync(don.p, on.data(), c.n_pop, cudaMemcpyHostToDevice, c.stream));
+      dim3 g(grid_for(max_slots, 256), c.n_pop);
+      k_radius_minmax_masked<<<g, 256, 0, c.stream>>>(c.d_pops, don.p); note_launch();
+      CK(cudaStreamSynchronize(c.stream));
+      don.release();
+    }
+    // occupied bin range of the others
+    run_hist_scan(c);
+    hist_current = true;
+    std::vector<PopCtr>& q = read_ctrs(c);
+    for (int k = 0; k < c.n_pop; k++) {
+      PopHost& ph = c.pops[k];
+      double rmin = 0.0, rmax = 0.0;
+      if (!ph.valid_sort) {
+        if (q[k].n_live > 0) {
+          memcpy(&rmin, &q[k].rmin_bits, 8);
+          memcpy(&rmax, &q[k].rmax_bits, 8);
+        }
+      } else if (q[k].bmax < 0) {
+        if (ph.n_bin > 0) {
+          rmin = ph.edges[ph.n_bin];
+          rmax = ph.edges[0];
+        }
+      } else {
+        rmin = ph.edges[q[k].bmin];
+        rmax = ph.edges[q[k].bmax + 1];
+      }
+      bool need = false;
+      if (rmax == 0.0) {
+        if (!ph.valid_sort && ph.n_bin != 0) {
+          make_grid(c, ph, 0, 0.0, 0.0);
+          hist_current = false;
+        }
+      } else if (ph.n_bin < 1) {
+        need = true;
+      } else {
+        double gmin = ph.edges[0], gmax = ph.edges[ph.n_bin];
+        if (rmin / gmin < 3.0 || gmax / rmax < 3.0) need = true;
+      }
+      if (need) {
+        double gmin = rmin / 10.0, gmax = rmax * 10.0;
+        int n_bin = (int)ceil((log10(gmax) - log10(gmin)) * 10.0);
+        if (n_bin > kMaxBin) throw Fail(PMC_ERR_CAPACITY);
+        make_grid(c, ph, n_bin, gmin, gmax);
+        hist_current = false;
+      }
+      // a population uploaded without a sort is sorted now even when its
+      // grid is kept
+      if (!ph.valid_sort) hist_current = hist_current && true;
+      ph.valid_sort = true;
+    }
+  }
+  if (!hist_current) run_hist_scan(c);
+  int max_chunks = 1, max_cells = 1;
+  for (int k = 0; k < c.n_pop; k++) {
+    max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
+    max_cells = std::max(max_cells, c.pops[k].h.n_cells);
+  }
+  dim3 g(max_chunks, c.n_pop);
+  int prec = c.mode == PMC_MODE_MIXED ? 1 : 0;
+  long long units = 0;
+  if (c.prof) {
+    std::vector<PopCtr>& r = read_ctrs(c);
+    for (int k = 0; k < c.n_pop; k++) units += (long long)r[k].n_slots;
+  }
+  ProfScope ps(c, 1, units);
+  k_sort_scatter<<<g, kSortThreads, sizeof(int) * kSortWarps * max_cells, c.stream>>>(c.d_pops, prec); note_launch();
+}
+
+// ---------------------------------------------------------------------------
+// one step over all populations
+
+template <int KT, class T>
+void launch_test(Ctx& c, bool flat, int n_gpairs) {
+  int blocks = 148 * 8;
+  if (flat)
+    k_test<KT, T, true><<<blocks, 256, 0, c.stream>>>(
+        c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
+        c.work_off.p + n_gpairs, c.flag.p, c.ev.p);
+  else
+    k_test<KT, T, false><<<blocks, 256, 0, c.stream>>>(
+        c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
+        c.work_off.p + n_gpairs, c.flag.p, c.ev.p);
+  note_launch();
+}
+
+void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs) {
+  bool f32 = c.mode == PMC_MODE_MIXED;
+  switch (kt) {
+    case kKernelAdditive:
+      f32 ? launch_test<kKernelAdditive, float>(c, flat, n_gpairs)
+          : launch_test<kKernelAdditive, double>(c, flat, n_gpairs);
+      break;
+    case kKernelConstant:
+      f32 ? launch_test<kKernelConstant, float>(c, flat, n_gpairs)
+          : launch_test<kKernelConstant, double>(c, flat, n_gpairs);
+      break;
+    case kKernelBrown:
+      f32 ? launch_test<kKernelBrown, float>(c, flat, n_gpairs)
+          : launch_test<kKernelBrown, double>(c, flat, n_gpairs);
+      break;
+    case kKernelSedi:
+      f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs)
+          : launch_test<kKernelSedi, double>(c, flat, n_gpairs);
+      break;
+    default:
+      launch_test<kKernelZero, double>(c, flat, n_gpairs);
+  }
+}
+
+void launch_pp(Ctx& c, int kt, long long Q) {
+  int blocks = grid_for(Q, 128);
+  switch (kt) {
+    case kKernelAdditive:
+      k_pp_ops<kKernelAdditive><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+      break;
+    case kKernelConstant:
+      k_pp_ops<kKernelConstant><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+      break;
+    case kKernelBrown:
+      k_pp_ops<kKernelBrown><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+      break;
+    case kKernelSedi:
+      k_pp_ops<kKernelSedi><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+      break;
+    default:
+      k_pp_ops<kKernelZero><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+  }
+}
+
+void set_n_dev(Ctx& c, long long v) {
+  CK(cudaMemcpyAsync(c.n_dev.p, &v, sizeof(long long), cudaMemcpyHostToDevice, c.stream));
+}
+
+void step_parallel(Ctx& c, int kt) {
+  // counters of this step
+  for (int k = 0; k < c.n_pop; k++) {
+    PopCtr r = read_ctr(c, k);
+    r.tot_samp = r.tot_coag = r.kmax_warn = r.redraws = 0;
+    r.status = 0;
+    write_ctr(c, k, r);
+  }
+  push_pops(c);
+  sort_pops(c, true);
+  // global pair list
+  std::vector<long long> base(c.n_pop + 1, 0);
+  for (int k = 0; k < c.n_pop; k++) base[k + 1] = base[k] + c.pops[k].h.n_pairs;
+  int n_gpairs = (int)base[c.n_pop];
+  {
+    std::vector<int> gp_pop(std::max(n_gpairs, 1)), gp_loc(std::max(n_gpairs, 1));
+    for (int k = 0; k < c.n_pop; k++)
+      for (int p = 0; p < c.pops[k].h.n_pairs; p++) {
+        gp_pop[base[k] + p] = k;
+        gp_loc[base[k] + p] = p;
+      }
+    c.gpair_pop.reserve(gp_pop.size());
+    c.gpair_local.reserve(gp_loc.size());
+    c.pop_pair_base.reserve(base.size());
+    CK(cudaMemcpyAsync(c.gpair_pop.p, gp_pop.data(), sizeof(int) * gp_pop.size(), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.gpair_local.p, gp_loc.data(), sizeof(int) * gp_loc.size(), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.pop_pair_base.p, base.data(), sizeof(long long) * base.size(), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+  }
+  size_t ng = (size_t)n_gpairs + 1;
+  c.nwork_set.reserve(ng);
+  c.nwork_pp.reserve(ng);
+  c.nprio.reserve(ng);
+  c.work_off.reserve(ng);
+  c.pp_off.reserve(ng);
+  c.prio_off.reserve(ng);
+  c.pair_losers.reserve(ng);
+  c.per_pop_i.reserve(4 * (size_t)c.n_pop);
+  c.slot_base_set.reserve(c.n_pop);
+  c.slot_base_pp.reserve(c.n_pop);
+  c.id_base_set.reserve(c.n_pop);
+  c.id_base_pp.reserve(c.n_pop);
+  c.n_dev.reserve(4);
+  int max_pairs = 1;
+  for (int k = 0; k < c.n_pop; k++) max_pairs = std::max(max_pairs, c.pops[k].h.n_pairs);
+  int nb_max = 1;
+  for (int k = 0; k < c.n_pop; k++) nb_max = std::max(nb_max, c.pops[k].n_bin);
+  bool flat = weights_flat(c.w);
+  float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
+  long long redraws = 0;
+  long long Qprev = 0;
+  int round = 0;
+  for (;;) {
+    for (int k = 0; k < c.n_pop; k++) c.pops[k].h.round = (uint32_t)round;
+    push_pops(c);
+    if (round > 0) sort_pops(c, false);
+    {
+      dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
+      if (round == 0) {
+        k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
+        note_launch();
+      }
+      dim3 gp((max_pairs + 127) / 128, c.n_pop);
+      k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p,
+                                        c.nprio.p, c.pair_losers.p, 1, inflate); note_launch();
+    }
+    if (round == 0) {
+      for (int k = 0; k < c.n_pop; k++) c.pops[k].h.kmax_valid = 1;
+      push_pops(c);
+    }
+    long long W = scan(c, c.nwork_set.p, n_gpairs, c.work_off.p, true);
+    long long Q0 = scan(c, c.nwork_pp.p, n_gpairs, c.pp_off.p, true);
+    long long Ptot = scan(c, c.nprio.p, n_gpairs, c.prio_off.p, true);
+    long long Q = round == 0 ? Q0 : Qprev;
+    if (Ptot + Q + 1 >= 0xffffffffLL) throw Fail(PMC_ERR_CAPACITY);
+    // buffers
+    c.flag.reserve((size_t)W + 1);
+    c.ev.reserve((size_t)W + 1);
+    c.flag_off.reserve((size_t)W + 1);
+    // reset claims and per-pair losers
+    for (int k = 0; k < c.n_pop; k++) {
+      PopHost& ph = c.pops[k];
+      k_fill_u32<<<grid_for(ph.h.cap, 256), 256, 0, c.stream>>>(ph.h.claim, ph.h.cap, 0xffffffffu); note_launch();
+    }
+    CK(cudaMemsetAsync(c.pair_losers.p, 0, sizeof(int) * ng, c.stream));
+    if (W > 0) {
+      ProfScope ps(c, 0, W);
+      launch_test_kt(c, kt, flat, n_gpairs);
+    }
+    // target operations of the per-particle path
+    if (Q > 0) {
+      if (round == 0) {
+        c.op_pop.reserve(Q); c.op_pair.reserve(Q); c.op_slot.reserve(Q); c.op_k.reserve(Q); c.op_prio.reserve(Q);
+        k_build_ops<<<n_gpairs, 128, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pp_off.p,
+                                                    c.prio_off.p, n_gpairs, c.op_pop.p, c.op_pair.p,
+                                                    c.op_slot.p, c.op_k.p, c.op_prio.p); note_launch();
+      }
+      c.pp_res.reserve(Q);
+      c.pp_vol.reserve((size_t)Q * c.n_spec);
+      set_n_dev(c, Q);
+      launch_pp(c, kt, Q);
+    }
+    // events of the per-set tests, in sample order
+    long long E = 0;
+    if (W > 0) {
+      E = scan(c, c.flag.p, W, c.flag_off.p, true);
+      c.ev_w.reserve((size_t)E + 1);
+      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, W, c.ev_w.p); note_launch();
+    }
+    c.need_slot_set.reserve(E + 1); c.need_id_set.reserve(E + 1); c.win_set.reserve(E + 1);
+    c.rank_slot_set.reserve(E + 2); c.rank_id_set.reserve(E + 2);
+    c.need_slot_pp.reserve(Q + 1); c.need_id_pp.reserve(Q + 1); c.win_pp.reserve(Q + 1);
+    c.lost_pp.reserve(Q + 1); c.lost_off.reserve(Q + 2);
+    c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
+    CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
+    if (E > 0) {
+      set_n_dev(c, E);
+      k_resolve_set<<<grid_for(E, 256), 256, 0, c.stream>>>(
+          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
+          c.n_dev.p, c.ev_w.p, c.ev.p, c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p,
+          c.win_set.p); note_launch();
+      scan(c, c.need_slot_set.p, E, c.rank_slot_set.p, false);
+      scan(c, c.need_id_set.p, E, c.rank_id_set.p, false);
+      k_count_per_pop<<<grid_for(E, 256), 256, 0, c.stream>>>(c.need_slot_set.p, c.n_dev.p, nullptr, c.ev_w.p, c.work_off.p, n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 0 * c.n_pop); note_launch();
+      k_count_per_pop<<<grid_for(E, 256), 256, 0, c.stream>>>(c.need_id_set.p, c.n_dev.p, nullptr, c.ev_w.p, c.work_off.p, n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 1 * c.n_pop); note_launch();
+    }
+    if (Q > 0) {
+      set_n_dev(c, Q);
+      k_pp_resolve<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_prio.p, c.n_dev.p,
+                                                           c.pp_res.p, c.win_pp.p, c.need_slot_pp.p,
+                                                           c.need_id_pp.p, c.lost_pp.p); note_launch();
+      scan(c, c.need_slot_pp.p, Q, c.rank_slot_pp.p, false);
+      scan(c, c.need_id_pp.p, Q, c.rank_id_pp.p, false);
+      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p, nullptr, nullptr, 0, nullptr, c.per_pop_i.p + 2 * c.n_pop); note_launch();
+      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p, nullptr, nullptr, 0, nullptr, c.per_pop_i.p + 3 * c.n_pop); note_launch();
+    }
+    // capacity for the new slots
+    {
+      std::vector<int> pp(4 * c.n_pop);
+      CK(cudaMemcpyAsync(pp.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+      for (int k = 0; k < c.n_pop; k++) {
+        PopCtr r = read_ctr(c, k);
+        long long need = (long long)r.n_slots + pp[0 * c.n_pop + k] + pp[2 * c.n_pop + k];
+        if (need > c.pops[k].h.cap) {
+          // grow keeping slot numbers (the round's claims refer to them)
+          int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
+          relayout(c, k, nc, false);
+        }
+      }
+    }
+    k_alloc_bases<<<1, 1, 0, c.stream>>>(c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop,
+                                         c.per_pop_i.p + 1 * c.n_pop, c.per_pop_i.p + 2 * c.n_pop,
+                                         c.per_pop_i.p + 3 * c.n_pop, c.slot_base_set.p,
+                                         c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p); note_launch();
+    if (E > 0) {
+      set_n_dev(c, E);
+      k_apply_set<<<grid_for(E, 256), 256, 0, c.stream>>>(
+          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs, c.n_dev.p, c.ev_w.p,
+          c.ev.p, c.win_set.p, c.rank_slot_set.p, c.rank_id_set.p, c.slot_base_set.p,
+          c.id_base_set.p); note_launch();
+    }
+    if (Q > 0) {
+      set_n_dev(c, Q);
+      k_pp_apply<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p,
+                                                         c.pp_vol.p, c.win_pp.p, c.rank_slot_pp.p,
+                                                         c.rank_id_pp.p, c.slot_base_pp.p,
+                                                         c.id_base_pp.p); note_launch();
+    }
+    k_alloc_finish<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(
+        c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop, c.per_pop_i.p + 1 * c.n_pop,
+        c.per_pop_i.p + 2 * c.n_pop, c.per_pop_i.p + 3 * c.n_pop); note_launch();
+    // losers
+    long long set_losers = 0;
+    if (E > 0) {
+      long long nw = 0;
+      std::vector<int> pl(ng);
+      CK(cudaMemcpyAsync(pl.data(), c.pair_losers.p, sizeof(int) * ng, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+      for (size_t i = 0; i < (size_t)n_gpairs; i++) nw += pl[i];
+      set_losers = nw;
+    }
+    long long pp_lost = 0;
+    if (Q > 0) pp_lost = scan(c, c.lost_pp.p, Q, c.lost_off.p, true);
+    redraws += set_losers + pp_lost;
+    round++;
+    if (set_losers + pp_lost == 0) break;
+    if (round >= c.max_rounds) {
+      for (int k = 0; k < c.n_pop; k++) {
+        PopCtr r = read_ctr(c, k);
+        if (r.status == 0) r.status = PMC_ERR_TIMEOUT;
+        write_ctr(c, k, r);
+      }
+      break;
+    }
+    // redo list of lost target operations
+    if (pp_lost > 0) {
+      c.r_pop.reserve(pp_lost); c.r_pair.reserve(pp_lost); c.r_slot.reserve(pp_lost); c.r_k.reserve(pp_lost); c.r_prio.reserve(pp_lost);
+      k_build_redo<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.lost_pp.p, c.lost_off.p, Q,
+                                                           c.r_pop.p, c.r_pair.p, c.r_slot.p, c.r_k.p, c.r_prio.p, 0x80000000u); note_launch();
+      std::swap(c.op_pop, c.r_pop); std::swap(c.op_pair, c.r_pair); std::swap(c.op_slot, c.r_slot);
+      std::swap(c.op_k, c.r_k); std::swap(c.op_prio, c.r_prio);
+    }
+    Qprev = pp_lost;
+  }
+  c.last_redraws = redraws;
+  c.last_rounds = round;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+struct pmc_coag_gpu_ctx {
+  Ctx c;
+};
+
+extern "C" {
+
+const char* pmc_coag_gpu_status_string(int s) {
+  switch (s) {
+    case PMC_OK: return "ok";
+    case PMC_ERR_INVALID_ARG: return "invalid argument";
+    case PMC_ERR_OUT_OF_GRID: return "particle outside of bin_grid: try reducing the timestep del_t";
+    case PMC_ERR_CAPACITY: return "capacity exceeded";
+    case PMC_ERR_CUDA: return g_last_error[0] ? g_last_error : "CUDA error";
+    case PMC_ERR_TIMEOUT: return "bounded device loop ran out of iterations";
+    case PMC_ERR_RNG_EXHAUSTED: return "replay stream exhausted";
+    case PMC_ERR_ASSERT: return "reference assertion failed";
+    case PMC_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+#define GUARD_BEGIN try {
+#define GUARD_END                 \
+  }                               \
+  catch (Fail & f) {              \
+    return f.code;                \
+  }                               \
+  catch (...) {                   \
+    return PMC_ERR_CAPACITY;      \
+  }
+
+static int do_init(int n_pop, int n_spec, const double* density, int i_water, int n_group, int n_class,
+                   const int* w_type, const double* w_mag, const double* w_exp, const uint64_t* seeds,
+                   pmc_coag_gpu_ctx** out) {
+  if (!out || n_pop < 1 || n_spec < 1 || n_spec > kMaxSpec || n_group < 1 || n_group > kMaxGroup ||
+      n_class < 1 || n_class > kMaxClass || !density || !w_type || !w_mag || !w_exp)
+    return PMC_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return PMC_ERR_NO_DEVICE;
+  std::unique_ptr<pmc_coag_gpu_ctx> x(new pmc_coag_gpu_ctx());
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  c.n_pop = n_pop;
+  c.n_spec = n_spec;
+  c.n_group = n_group;
+  c.n_class = n_class;
+  c.i_water = i_water;
+  c.density.assign(density, density + n_spec);
+  memset(&c.w, 0, sizeof(c.w));
+  c.w.n_group = n_group;
+  c.w.n_class = n_class;
+  for (int cl = 0; cl < n_class; cl++)
+    for (int g = 0; g < n_group; g++) {
+      int src = g + n_group * cl;
+      int dst = g + kMaxGroup * cl;
+      if (w_type[src] < 1 || w_type[src] > 3) return PMC_ERR_INVALID_ARG;
+      c.w.type[dst] = w_type[src];
+      c.w.mag[dst] = w_mag[src];
+      c.w.expo[dst] = w_exp[src];
+    }
+  CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  c.pops.resize(n_pop);
+  CK(cudaMalloc(&c.d_pops, sizeof(PopDev) * n_pop));
+  CK(cudaMalloc(&c.d_ctrs, sizeof(PopCtr) * n_pop));
+  CK(cudaMemset(c.d_ctrs, 0, sizeof(PopCtr) * n_pop));
+  for (int k = 0; k < n_pop; k++) {
+    c.pops[k].seed = seeds ? seeds[k] : (uint64_t)(k + 1);
+    init_pop(c, c.pops[k], 1024);
+  }
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  *out = x.release();
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_init(int n_spec, const double* density, int i_water, int n_group, int n_class,
+                      const int* w_type, const double* w_mag, const double* w_exp, uint64_t seed,
+                      pmc_coag_gpu_ctx** ctx) {
+  return do_init(1, n_spec, density, i_water, n_group, n_class, w_type, w_mag, w_exp, &seed, ctx);
+}
+
+int pmc_coag_gpu_init_batch(int n_pop, int n_spec, const double* density, int i_water, int n_group,
+                            int n_class, const int* w_type, const double* w_mag, const double* w_exp,
+                            const uint64_t* seeds, pmc_coag_gpu_ctx** ctx) {
+  return do_init(n_pop, n_spec, density, i_water, n_group, n_class, w_type, w_mag, w_exp, seeds, ctx);
+}
+
+int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
+  if (!x) return PMC_OK;
+  Ctx& c = x->c;
+  cudaStreamSynchronize(c.stream);
+  for (auto& ph : c.pops) {
+    free_list(ph.slot_allocs);
+    free_list(ph.sort_allocs);
+    free_list(ph.fixed_allocs);
+  }
+  cudaFree(c.d_pops);
+  cudaFree(c.d_ctrs);
+  DevBuf<int>* bi[] = {&c.gpair_pop, &c.gpair_local, &c.pair_losers, &c.need_slot_set, &c.need_id_set,
+                       &c.need_slot_pp, &c.need_id_pp, &c.lost_pp, &c.op_pop, &c.op_pair, &c.op_slot,
+                       &c.op_k, &c.r_pop, &c.r_pair, &c.r_slot, &c.r_k, &c.per_pop_i,
+                       &c.slot_base_set, &c.slot_base_pp};
+  for (auto* b : bi) b->release();
+  DevBuf<long long>* bl[] = {&c.pop_pair_base, &c.nwork_set, &c.nwork_pp, &c.nprio, &c.work_off, &c.pp_off,
+                             &c.prio_off, &c.flag_off, &c.ev_w, &c.rank_slot_set, &c.rank_id_set,
+                             &c.rank_slot_pp, &c.rank_id_pp, &c.lost_off, &c.id_base_set, &c.id_base_pp,
+                             &c.scan_bsum, &c.scan_total, &c.n_dev};
+  for (auto* b : bl) b->release();
+  c.flag.release();
+  c.win_set.release();
+  c.win_pp.release();
+  c.ev.release();
+  c.op_prio.release();
+  c.r_prio.release();
+  c.pp_res.release();
+  c.pp_vol.release();
+  c.replay_u.release();
+  replay_free(c.replay);
+  cudaStreamDestroy(c.stream);
+  delete x;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* vol, const int* group,
+                        const int* cls, const int64_t* id, const int* n_primary) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || n_part < 0 || (n_part > 0 && !vol)) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  int cap = std::max(1024, n_part + n_part / 2 + 64);
+  if (cap > ph.h.cap || cap < ph.h.cap / 4) {
+    free_list(ph.slot_allocs);
+    alloc_slots(c, ph, cap);
+  }
+  PopCtr r = read_ctr(c, pop);
+  if (n_part > 0) {
+    std::vector<void*> tmp;
+    double* dv = dalloc<double>(tmp, (size_t)n_part * c.n_spec);
+    int* dg = group ? dalloc<int>(tmp, n_part) : nullptr;
+    int* dc = cls ? dalloc<int>(tmp, n_part) : nullptr;
+    long long* di = id ? dalloc<long long>(tmp, n_part) : nullptr;
+    int* dn = n_primary ? dalloc<int>(tmp, n_part) : nullptr;
+    CK(cudaMemcpyAsync(dv, vol, sizeof(double) * n_part * c.n_spec, cudaMemcpyHostToDevice, c.stream));
+    if (dg) CK(cudaMemcpyAsync(dg, group, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
+    if (dc) CK(cudaMemcpyAsync(dc, cls, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
+    if (di) CK(cudaMemcpyAsync(di, id, sizeof(long long) * n_part, cudaMemcpyHostToDevice, c.stream));
+    if (dn) CK(cudaMemcpyAsync(dn, n_primary, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
+    long long id0 = r.next_id;
+    CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
+    k_upload<<<grid_for(n_part, 256), 256, 0, c.stream>>>(ph.h, n_part, dv, dg, dc, di, dn, id0); note_launch();
+    CK(cudaStreamSynchronize(c.stream));
+    free_list(tmp);
+    if (group)
+      for (int i = 0; i < n_part; i++)
+        if (group[i] < 1 || group[i] > c.n_group) return PMC_ERR_INVALID_ARG;
+    if (cls)
+      for (int i = 0; i < n_part; i++)
+        if (cls[i] < 1 || cls[i] > c.n_class) return PMC_ERR_INVALID_ARG;
+    if (id) {
+      long long mx = 0;
+      for (int i = 0; i < n_part; i++) mx = std::max<long long>(mx, id[i]);
+      r.next_id = std::max<long long>(r.next_id, mx + 1);
+    } else {
+      r.next_id = id0 + n_part;
+    }
+  } else {
+    CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
+  }
+  r.n_slots = n_part;
+  r.n_live = n_part;
+  write_ctr(c, pop, r);
+  ph.valid_sort = false;
+  ph.n_bin = 0;
+  {
+    GridDev g{};
+    CK(cudaMemcpyAsync(ph.h.grid, &g, sizeof(GridDev), cudaMemcpyHostToDevice, c.stream));
+  }
+  alloc_sort(c, ph);
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_upload_components(pmc_coag_gpu_ctx* x, int pop, int n_part, const int* n_comp,
+                                   const int* comp_source, const double* comp_create_time) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || !n_comp || !comp_source || !comp_create_time)
+    return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  PopCtr r = read_ctr(c, pop);
+  if (n_part != r.n_slots) return PMC_ERR_INVALID_ARG;
+  std::vector<int> src((size_t)kMaxComponent * ph.h.cap, 0);
+  std::vector<double> tim((size_t)kMaxComponent * ph.h.cap, 0.0);
+  std::vector<double> lct(n_part), gct(n_part);
+  for (int i = 0; i < n_part; i++) {
+    if (n_comp[i] < 0 || n_comp[i] > kMaxComponent) return PMC_ERR_INVALID_ARG;
+    double lo = 0.0, hi = 0.0;
+    for (int k = 0; k < n_comp[i]; k++) {
+      src[(size_t)k * ph.h.cap + i] = comp_source[(size_t)i * kMaxComponent + k];
+      double t = comp_create_time[(size_t)i * kMaxComponent + k];
+      tim[(size_t)k * ph.h.cap + i] = t;
+      if (k == 0 || t < lo) lo = t;
+      if (k == 0 || t > hi) hi = t;
+    }
+    lct[i] = lo;
+    gct[i] = hi;
+  }
+  CK(cudaMemcpyAsync(ph.h.ncomp, n_comp, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(ph.h.csrc, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(ph.h.ctime, tim.data(), sizeof(double) * tim.size(), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(ph.h.lct, lct.data(), sizeof(double) * n_part, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(ph.h.gct, gct.data(), sizeof(double) * n_part, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
+static int finish_step(Ctx& c, long long* samp, long long* coag) {
+  long long s = 0, k = 0, warn = 0;
+  int status = 0;
+  for (int p = 0; p < c.n_pop; p++) {
+    PopCtr r = read_ctr(c, p);
+    s += r.tot_samp;
+    k += r.tot_coag;
+    warn += r.kmax_warn;
+    if (r.status && !status) status = r.status;
+    // compact when more than half of the used slots are dead
+    if (r.n_slots > 4096 && r.n_live < r.n_slots / 2) relayout(c, p, c.pops[p].h.cap, true);
+  }
+  c.last_kmax_warn = warn;
+  *samp = s;
+  *coag = k;
+  return status;
+}
+
+int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* temp,
+                            const double* pressure, double additive_coeff, double del_t, int n_steps,
+                            int64_t* tot_n_samp, int64_t* tot_n_coag) {
+  if (!x || kernel_type < 1 || kernel_type > 5 || !temp || !pressure || n_steps < 0)
+    return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  long long S = 0, K = 0;
+  for (int st = 0; st < n_steps; st++) {
+    for (int k = 0; k < c.n_pop; k++) {
+      PopHost& ph = c.pops[k];
+      ph.h.kernel_type = kernel_type;
+      ph.h.temp = temp[k];
+      ph.h.pressure = pressure[k];
+      ph.h.coeff = additive_coeff;
+      ph.h.del_t = del_t;
+      ph.h.benv = brown_env(temp[k], pressure[k]);
+      ph.h.step = ++ph.step;
+      // the reference keeps its bounds until the grid changes
+      // (coag_kernel_bounds_valid, aero_sorted.F90:55); a new kernel type
+      // would make them meaningless, so that case recomputes them
+      if (ph.kmax_kt != kernel_type) {
+        ph.h.kmax_valid = 0;
+        ph.kmax_kt = kernel_type;
+      }
+    }
+    push_pops(c);
+    long long s = 0, k = 0;
+    int status;
+    if (c.mode == PMC_MODE_REPLAY) {
+      status = replay_step(c.n_pop, c.d_pops, c.stream, c.replay, c.replay_u.p, c.replay_n,
+                           &c.replay_used, kernel_type, &s, &k);
+      for (int p = 0; p < c.n_pop; p++) c.pops[p].valid_sort = true;
+    } else {
+      ProfScope ps(c, 3, 1);
+      step_parallel(c, kernel_type);
+      status = finish_step(c, &s, &k);
+    }
+    S += s;
+    K += k;
+    if (status) {
+      if (tot_n_samp) *tot_n_samp = S;
+      if (tot_n_coag) *tot_n_coag = K;
+      return status;
+    }
+  }
+  if (tot_n_samp) *tot_n_samp = S;
+  if (tot_n_coag) *tot_n_coag = K;
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_step(pmc_coag_gpu_ctx* x, int kernel_type, double temp, double pressure,
+                      double additive_coeff, double del_t, int* tot_n_samp, int* tot_n_coag) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  std::vector<double> t(x->c.n_pop, temp), p(x->c.n_pop, pressure);
+  int64_t s = 0, k = 0;
+  int rc = pmc_coag_gpu_step_batch(x, kernel_type, t.data(), p.data(), additive_coeff, del_t, 1, &s, &k);
+  if (tot_n_samp) *tot_n_samp = (int)s;
+  if (tot_n_coag) *tot_n_coag = (int)k;
+  return rc;
+}
+
+int pmc_coag_gpu_n_part(pmc_coag_gpu_ctx* x, int pop, int* n_part) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || !n_part) return PMC_ERR_INVALID_ARG;
+  GUARD_BEGIN
+  PopCtr r = read_ctr(x->c, pop);
+  *n_part = r.n_live;
+  return PMC_OK;
+  GUARD_END
+}
+
+static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, int* cls, int64_t* id,
+                       int* n_primary, int* n_comp, int* comp_source, double* comp_time, int* n_part) {
+  PopHost& ph = c.pops[pop];
+  PopCtr r = read_ctr(c, pop);
+  if (n_part) *n_part = r.n_live;
+  if (r.n_live > max_part) return PMC_ERR_CAPACITY;
+  std::vector<void*> tmp;
+  long long* off = dalloc<long long>(tmp, (size_t)r.n_slots + 1);
+  long long nl = scan(c, ph.h.alive, r.n_slots, off, true);
+  if (nl != r.n_live) return PMC_ERR_ASSERT;
+  size_t n = std::max<long long>(nl, 1);
+  double* dv = dalloc<double>(tmp, n * c.n_spec);
+  int* dg = dalloc<int>(tmp, n);
+  int* dc = dalloc<int>(tmp, n);
+  long long* di = dalloc<long long>(tmp, n);
+  int* dn = dalloc<int>(tmp, n);
+  int* dnc = dalloc<int>(tmp, n);
+  int* dcs = dalloc<int>(tmp, n * kMaxComponent);
+  double* dct = dalloc<double>(tmp, n * kMaxComponent);
+  if (r.n_slots > 0)
+    k_download<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(ph.h, off, r.n_slots, dv, dg, dc, di, dn,
+                                                                dnc, dcs, dct); note_launch();
+  if (nl > 0) {
+    if (vol) CK(cudaMemcpyAsync(vol, dv, sizeof(double) * nl * c.n_spec, cudaMemcpyDeviceToHost, c.stream));
+    if (group) CK(cudaMemcpyAsync(group, dg, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (cls) CK(cudaMemcpyAsync(cls, dc, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (id) CK(cudaMemcpyAsync(id, di, sizeof(long long) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (n_primary) CK(cudaMemcpyAsync(n_primary, dn, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (n_comp) CK(cudaMemcpyAsync(n_comp, dnc, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (comp_source) CK(cudaMemcpyAsync(comp_source, dcs, sizeof(int) * nl * kMaxComponent, cudaMemcpyDeviceToHost, c.stream));
+    if (comp_time) CK(cudaMemcpyAsync(comp_time, dct, sizeof(double) * nl * kMaxComponent, cudaMemcpyDeviceToHost, c.stream));
+  }
+  CK(cudaStreamSynchronize(c.stream));
+  free_list(tmp);
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_download(pmc_coag_gpu_ctx* x, int pop, int max_part, double* vol, int* group, int* cls,
+                          int64_t* id, int* n_primary, int* n_part) {
+  if (!x || pop < 0 || pop >= x->c.n_pop) return PMC_ERR_INVALID_ARG;
+  GUARD_BEGIN
+  return do_download(x->c, pop, max_part, vol, group, cls, id, n_primary, nullptr, nullptr, nullptr, n_part);
+  GUARD_END
+}
+
+int pmc_coag_gpu_download_components(pmc_coag_gpu_ctx* x, int pop, int max_part, int* n_comp,
+                                     int* comp_source, double* comp_create_time) {
+  if (!x || pop < 0 || pop >= x->c.n_pop) return PMC_ERR_INVALID_ARG;
+  GUARD_BEGIN
+  return do_download(x->c, pop, max_part, nullptr, nullptr, nullptr, nullptr, nullptr, n_comp,
+                     comp_source, comp_create_time, nullptr);
+  GUARD_END
+}
+
+int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx* x, const int* w_type, const double* w_mag,
+                            const double* w_exp) {
+  if (!x || !w_type || !w_mag || !w_exp) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  for (int cl = 0; cl < c.n_class; cl++)
+    for (int g = 0; g < c.n_group; g++) {
+      int src = g + c.n_group * cl, dst = g + kMaxGroup * cl;
+      if (w_type[src] < 1 || w_type[src] > 3) return PMC_ERR_INVALID_ARG;
+      c.w.type[dst] = w_type[src];
+      c.w.mag[dst] = w_mag[src];
+      c.w.expo[dst] = w_exp[src];
+    }
+  for (auto& ph : c.pops) {
+    set_params(c, ph);
+    ph.valid_sort = false;  // aero_state_set_weight clears valid_sort
+  }
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_set_next_id(pmc_coag_gpu_ctx* x, int pop, int64_t next_id) {
+  if (!x || pop < 0 || pop >= x->c.n_pop) return PMC_ERR_INVALID_ARG;
+  GUARD_BEGIN
+  PopCtr r = read_ctr(x->c, pop);
+  r.next_id = next_id;
+  write_ctr(x->c, pop, r);
+  CK(cudaStreamSynchronize(x->c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx* x, int pop, int64_t* next_id) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || !next_id) return PMC_ERR_INVALID_ARG;
+  GUARD_BEGIN
+  *next_id = read_ctr(x->c, pop).next_id;
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_set_mode(pmc_coag_gpu_ctx* x, int mode) {
+  if (!x || mode < PMC_MODE_FP64 || mode > PMC_MODE_REPLAY) return PMC_ERR_INVALID_ARG;
+  x->c.mode = mode;
+  for (auto& ph : x->c.pops) ph.valid_sort = ph.valid_sort && mode != PMC_MODE_REPLAY;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_replay_set(pmc_coag_gpu_ctx* x, const double* u, int64_t n) {
+  if (!x || (n > 0 && !u) || n < 0) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  c.replay_u.reserve((size_t)std::max<int64_t>(n, 1));
+  if (n > 0) CK(cudaMemcpy(c.replay_u.p, u, sizeof(double) * n, cudaMemcpyHostToDevice));
+  c.replay_n = n;
+  c.replay_used = 0;
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_replay_open(pmc_coag_gpu_ctx* x, const char* path) {
+  if (!x || !path) return PMC_ERR_INVALID_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return PMC_ERR_INVALID_ARG;
+  std::vector<double> u;
+  double buf[4096];
+  size_t m;
+  while ((m = fread(buf, sizeof(double), 4096, f)) > 0) u.insert(u.end(), buf, buf + m);
+  fclose(f);
+  return pmc_coag_gpu_replay_set(x, u.data(), (int64_t)u.size());
+}
+
+int pmc_coag_gpu_replay_used(pmc_coag_gpu_ctx* x, int64_t* n_used) {
+  if (!x || !n_used) return PMC_ERR_INVALID_ARG;
+  *n_used = x->c.replay_used;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_stats(pmc_coag_gpu_ctx* x, int64_t* kmax_violations, int64_t* redraws, int64_t* rounds) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  if (kmax_violations) *kmax_violations = x->c.last_kmax_warn;
+  if (redraws) *redraws = x->c.last_redraws;
+  if (rounds) *rounds = x->c.last_rounds;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_profile(pmc_coag_gpu_ctx* x, int enable) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  if (enable && !c.prof_ev[0]) {
+    CK(cudaEventCreate(&c.prof_ev[0]));
+    CK(cudaEventCreate(&c.prof_ev[1]));
+  }
+  c.prof = enable != 0;
+  for (int i = 0; i < 4; i++) {
+    c.prof_ms[i] = 0.0;
+    c.prof_launch[i] = c.prof_units[i] = 0;
+  }
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_profile_read(pmc_coag_gpu_ctx* x, int which, double* total_ms, int64_t* launches,
+                              int64_t* units) {
+  if (!x || which < 0 || which > 3) return PMC_ERR_INVALID_ARG;
+  if (total_ms) *total_ms = x->c.prof_ms[which];
+  if (launches) *launches = x->c.prof_launch[which];
+  if (units) *units = x->c.prof_units[which];
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_launch_count(int64_t* n) {
+  if (!n) return PMC_ERR_INVALID_ARG;
+  *n = g_launches;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_sort(pmc_coag_gpu_ctx* x, int pop, int* n_bin, double* edges, int max_bin, int* counts,
+                      int* bins) {
+  if (!x || pop < 0 || pop >= x->c.n_pop) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  sort_pops(c, true);
+  CK(cudaStreamSynchronize(c.stream));
+  PopHost& ph = c.pops[pop];
+  if (n_bin) *n_bin = ph.n_bin;
+  if (ph.n_bin > max_bin) return PMC_ERR_CAPACITY;
+  if (edges && ph.n_bin > 0) memcpy(edges, ph.edges.data(), sizeof(double) * (ph.n_bin + 1));
+  if (counts && ph.n_bin > 0)
+    CK(cudaMemcpy(counts, ph.h.cell_count, sizeof(int) * ph.n_bin * c.n_class, cudaMemcpyDeviceToHost));
+  if (bins) {
+    PopCtr r = read_ctr(c, pop);
+    std::vector<int> b(std::max(r.n_slots, 1));
+    std::vector<uint8_t> a(std::max(r.n_slots, 1));
+    if (r.n_slots > 0) {
+      CK(cudaMemcpy(b.data(), ph.h.bin, sizeof(int) * r.n_slots, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(a.data(), ph.h.alive, r.n_slots, cudaMemcpyDeviceToHost));
+    }
+    int j = 0;
+    for (int i = 0; i < r.n_slots; i++)
+      if (a[i]) bins[j++] = b[i] >= 0 ? b[i] + 1 : 0;
+  }
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_kmax_table(pmc_coag_gpu_ctx* x, int kernel_type, double temp, double pressure,
+                            double additive_coeff, double* kmax, int max_bin) {
+  if (!x || !kmax) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[0];
+  if (ph.n_bin > max_bin) return PMC_ERR_CAPACITY;
+  ph.h.kernel_type = kernel_type;
+  ph.h.temp = temp;
+  ph.h.pressure = pressure;
+  ph.h.coeff = additive_coeff;
+  ph.h.benv = brown_env(temp, pressure);
+  ph.h.kmax_valid = 0;
+  push_pops(c);
+  int nb = std::max(ph.n_bin, 1);
+  dim3 g((nb * nb + 255) / 256, c.n_pop);
+  k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops); note_launch();
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaGetLastError());
+  if (ph.n_bin > 0) CK(cudaMemcpy(kmax, ph.h.kmax_tab, sizeof(double) * ph.n_bin * ph.n_bin, cudaMemcpyDeviceToHost));
+  ph.h.kmax_valid = 1;
+  push_pops(c);
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx* x, int kernel_type, double temp, double pressure,
+                             double additive_coeff, int n_pairs, const double* vol1, const int* c1,
+                             const double* vol2, const int* c2, const int* c_ij, double* k_out) {
+  if (!x || n_pairs < 0 || (n_pairs > 0 && (!vol1 || !vol2 || !c1 || !c2 || !c_ij || !k_out)))
+    return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  if (n_pairs == 0) return PMC_OK;
+  PopDev P = c.pops[0].h;
+  P.kernel_type = kernel_type;
+  P.temp = temp;
+  P.pressure = pressure;
+  P.coeff = additive_coeff;
+  P.benv = brown_env(temp, pressure);
+  std::vector<void*> tmp;
+  size_t nv = (size_t)n_pairs * c.n_spec;
+  double* d1 = dalloc<double>(tmp, nv);
+  double* d2 = dalloc<double>(tmp, nv);
+  int* e1 = dalloc<int>(tmp, n_pairs);
+  int* e2 = dalloc<int>(tmp, n_pairs);
+  int* e3 = dalloc<int>(tmp, n_pairs);
+  double* out = dalloc<double>(tmp, n_pairs);
+  CK(cudaMemcpy(d1, vol1, sizeof(double) * nv, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d2, vol2, sizeof(double) * nv, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e1, c1, sizeof(int) * n_pairs, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e2, c2, sizeof(int) * n_pairs, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e3, c_ij, sizeof(int) * n_pairs, cudaMemcpyHostToDevice));
+  k_eval_kernel<<<(n_pairs + 127) / 128, 128, 0, c.stream>>>(P, n_pairs, d1, e1, d2, e2, e3, out,
+                                                             c.mode == PMC_MODE_MIXED ? 1 : 0); note_launch();
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(k_out, out, sizeof(double) * n_pairs, cudaMemcpyDeviceToHost));
+  free_list(tmp);
+  return PMC_OK;
+  GUARD_END
+}
+
+}  // extern "C"

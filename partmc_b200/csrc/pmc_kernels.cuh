@@ -1,0 +1,486 @@
+// pmc_kernels.cuh -- kernels of the parallel coagulation step.
+//
+// One step of mc_coag (coagulation.F90:43-96) runs as rounds.  Round 0:
+//   sort      stable counting sort of live slots into (bin, class) cells,
+//             with each particle's pair-test record written in cell order
+//             (aero_state_sort / aero_sorted_sort_particles,
+//             aero_sorted.F90:185-373);
+//   k bounds  the n_bin x n_bin k_max table when the grid changed
+//             (est_k_minmax_binned_unweighted, coag_kernel.F90:253-280);
+//   pairs     one thread per bin pair: destination class, f_max, k_max,
+//             path choice and the Poisson number of samples
+//             (mc_coag_for_bin / compute_n_samp, coagulation.F90:101-145,
+//             648-702);
+//   tests     one thread per sample: random pair, weighted kernel, accept
+//             (maybe_coag_pair / find_rand_pair, coagulation.F90:712-803);
+//             an accepted sample claims both particles with atomicMin of its
+//             priority (its position in the reference's loop order);
+//   resolve   an accepted sample that holds both claims is applied
+//             (coagulate / coagulate_weighting, coagulation.F90:810-985);
+//             one that lost a claim is redrawn in the next round.
+// Later rounds re-sort and redraw only the lost samples, so a particle can
+// take part in several coagulations per step, as in the sequential loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pmc_physics.cuh"
+#include "pmc_state.cuh"
+
+namespace pmc {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kChunk = 2048;  // slots per sort block
+constexpr int kWarpSlots = kChunk / kSortWarps;
+
+enum Stream : uint32_t {
+  kStreamPair = 1,
+  kStreamTest = 2,
+  kStreamMerge = 3,
+  kStreamPart = 4,
+};
+
+// Status codes shared with the C ABI.
+enum : int {
+  kOk = 0,
+  kErrArg = 1,
+  kErrOutOfGrid = 2,
+  kErrCapacity = 3,
+  kErrCuda = 4,
+  kErrTimeout = 5,
+  kErrRng = 6,
+  kErrAssert = 7,
+};
+
+__device__ __forceinline__ void set_status(PopCtr* c, int code) { atomicCAS(&c->status, 0, code); }
+
+__device__ __forceinline__ void add_ll(long long* p, long long v) {
+  atomicAdd((unsigned long long*)p, (unsigned long long)v);
+}
+__device__ __forceinline__ void add_ll(int* p, long long v) { atomicAdd(p, (int)v); }
+
+__device__ __forceinline__ Rng make_rng(const PopDev& P, uint32_t stream, uint32_t p, uint32_t s) {
+  return Rng(P.seed, P.step, (p << 12) | ((P.round & 0xffu) << 4) | stream, s);
+}
+
+// ---------------------------------------------------------------------------
+// radius range of live particles (remake_if_needed without a valid sort,
+// aero_sorted.F90:293-306)
+__global__ void k_radius_minmax(const PopDev* pops, int n_pop) {
+  const PopDev& P = pops[blockIdx.y];
+  int n = P.ctr->n_slots;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!P.alive[i]) continue;
+    double r = vol2rad(P.vtot[i]);
+    unsigned long long b = (unsigned long long)__double_as_longlong(r);
+    atomicMin(&P.ctr->rmin_bits, b);
+    atomicMax(&P.ctr->rmax_bits, b);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sort pass 1: radius, bin and per-chunk cell histogram
+__global__ void k_sort_hist(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  int chunk = blockIdx.x;
+  if (chunk >= P.n_chunks) return;
+  extern __shared__ int sh[];
+  int nc = P.n_cells;
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) sh[c] = 0;
+  __syncthreads();
+  const GridDev& G = *P.grid;
+  int n = P.ctr->n_slots;
+  int base = chunk * kChunk;
+  for (int k = threadIdx.x; k < kChunk; k += blockDim.x) {
+    int i = base + k;
+    if (i >= n) break;
+    if (!P.alive[i]) {
+      P.bin[i] = -1;
+      continue;
+    }
+    double r = vol2rad(P.vtot[i]);
+    P.rad[i] = r;
+    int b = bin_find(G.n_bin, G.log_lo, G.log_hi, r);
+    if (b < 1 || b > G.n_bin) {
+      P.bin[i] = -1;
+      add_ll(&P.ctr->out_of_grid, (long long)(1));
+      continue;
+    }
+    P.bin[i] = b - 1;
+    atomicAdd(&sh[(b - 1) + G.n_bin * (P.cls[i] - 1)], 1);
+  }
+  __syncthreads();
+  int* out = P.chunk_hist + (size_t)chunk * nc;
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) out[c] = sh[c];
+}
+
+// block-wide exclusive scan of one int per thread (blockDim <= 1024)
+__device__ int block_excl_scan(int v, int* total) {
+  __shared__ int ws[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[wid] = x;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  if (wid == 0) {
+    int s = lane < nw ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    ws[lane] = s;
+  }
+  __syncthreads();
+  int pre = (wid > 0 ? ws[wid - 1] : 0) + x - v;
+  if (total) *total = ws[nw - 1];
+  __syncthreads();
+  return pre;
+}
+
+// sort pass 2: cell totals, cell starts, per-chunk offsets (one block per
+// population, one thread per cell)
+__global__ void k_sort_scan(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.x];
+  int nc = P.n_cells;
+  int c = threadIdx.x;
+  int tot = 0;
+  if (c < nc)
+    for (int k = 0; k < P.n_chunks; k++) tot += P.chunk_hist[(size_t)k * nc + c];
+  int all;
+  int start = block_excl_scan(c < nc ? tot : 0, &all);
+  if (c < nc) {
+    P.cell_count[c] = tot;
+    P.cell_start[c] = start;
+    int run = start;
+    for (int k = 0; k < P.n_chunks; k++) {
+      int h = P.chunk_hist[(size_t)k * nc + c];
+      P.chunk_hist[(size_t)k * nc + c] = run;
+      run += h;
+    }
+    if (tot > 0) {
+      int b = c % P.grid->n_bin;
+      atomicMin(&P.ctr->bmin, b);
+      atomicMax(&P.ctr->bmax, b);
+    }
+  }
+  if (c == 0) P.cell_start[nc] = all;
+}
+
+// pair-test record of slot i (see RecD)
+__device__ __forceinline__ RecD make_rec(const PopDev& P, int i) {
+  RecD q;
+  double r = P.rad[i];
+  q.r = r;
+  q.rv = rad2vol(r);
+  q.nc = num_conc_at_radius<double>(P.w, P.cls[i] - 1, r);
+  q.a = q.b = q.c = 0.0;
+  switch (P.kernel_type) {
+    case kKernelAdditive: q.a = P.vtot[i]; break;
+    case kKernelBrown: {
+      double v = P.vtot[i];
+      BrownPart bp = brown_part(P.benv, v, P.mass[i] / v);
+      q.a = bp.diffus;
+      q.b = bp.speedsq;
+      q.c = bp.deltasq;
+      break;
+    }
+    case kKernelSedi: q.a = fall_g(vol2rad(P.vtot[i])); break;
+    default: break;
+  }
+  return q;
+}
+
+// sort pass 3: deterministic stable scatter (slot order within each cell)
+// and record build.  Warp w of a block owns slots [w*256, (w+1)*256) of the
+// chunk; ranks inside a 32-slot tile come from __match_any_sync.
+__global__ void k_sort_scatter(const PopDev* pops, int precision) {
+  const PopDev& P = pops[blockIdx.y];
+  int chunk = blockIdx.x;
+  if (chunk >= P.n_chunks) return;
+  extern __shared__ int wc[];  // [kSortWarps][n_cells]
+  int nc = P.n_cells;
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int k = threadIdx.x; k < kSortWarps * nc; k += blockDim.x) wc[k] = 0;
+  __syncthreads();
+  int n = P.ctr->n_slots;
+  int nb = P.grid->n_bin;
+  int base = chunk * kChunk + w * kWarpSlots;
+  for (int t = 0; t < kWarpSlots; t += 32) {
+    int i = base + t + lane;
+    int key = -1;
+    if (i < n && P.bin[i] >= 0) key = P.bin[i] + nb * (P.cls[i] - 1);
+    unsigned peers = __match_any_sync(0xffffffffu, key);
+    int leader = __ffs(peers) - 1;
+    if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
+  }
+  __syncthreads();
+  const int* off = P.chunk_hist + (size_t)chunk * nc;
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    int run = off[c];
+    for (int q = 0; q < kSortWarps; q++) {
+      int x = wc[q * nc + c];
+      wc[q * nc + c] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  unsigned lt = (1u << lane) - 1u;
+  for (int t = 0; t < kWarpSlots; t += 32) {
+    int i = base + t + lane;
+    int key = -1;
+    if (i < n && P.bin[i] >= 0) key = P.bin[i] + nb * (P.cls[i] - 1);
+    unsigned peers = __match_any_sync(0xffffffffu, key);
+    int leader = __ffs(peers) - 1;
+    int pos = 0;
+    if (key >= 0) pos = wc[w * nc + key] + __popc(peers & lt);
+    __syncwarp();
+    if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
+    __syncwarp();
+    if (key >= 0) {
+      P.list[pos] = i;
+      RecD q = make_rec(P, i);
+      if (precision == 0) {
+        P.recd[pos] = q;
+      } else {
+        RecF f;
+        f.r = (float)q.r;
+        f.rv = (float)q.rv;
+        f.nc = (float)q.nc;
+        f.a = (float)q.a;
+        f.b = (float)q.b;
+        f.c = (float)q.c;
+        f.pad0 = f.pad1 = 0.f;
+        P.recf[pos] = f;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_max table, est_k_minmax_binned_unweighted (coag_kernel.F90:253-280)
+__global__ void k_kmax_table(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  if (P.kmax_valid) return;
+  int nb = P.grid->n_bin;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb * nb) return;
+  int b1 = t % nb, b2 = t / nb;
+  double kmin, kmax;
+  bool ok = kminmax_for_bin(P.kernel_type, P.grid->edges, b1, b2, P.benv, P.coeff, P.dmin, P.dmax,
+                            &kmin, &kmax);
+  if (!ok) set_status(P.ctr, kErrAssert);
+  P.kmax_tab[b1 + nb * b2] = kmax;
+}
+
+// ---------------------------------------------------------------------------
+// pair set-up for round 0: mc_coag_for_bin, try_per_particle_coag's
+// eligibility tests and compute_n_samp (coagulation.F90:101-241, 648-702).
+// nwork_set[gp] = samples of a per-set pair; nwork_pp[gp] = targets of a
+// per-particle pair; nprio[gp] = both (priority space in loop order).
+__global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long long* nwork_set,
+                        long long* nwork_pp, long long* nprio, const int* pair_losers,
+                        int use_particle_path, float kmax_inflate) {
+  const PopDev& P = pops[blockIdx.y];
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n_pairs) return;
+  long long gp = pop_pair_base[blockIdx.y] + p;
+  PairDesc d = P.pair_desc[p];
+  int nb = P.grid->n_bin;
+  int b1 = d.b1, b2 = d.b2, c1 = d.c1, c2 = d.c2;
+  int cell1 = b1 + nb * c1, cell2 = b2 + nb * c2;
+  PairState& S = P.pair[p];
+  int n1 = P.cell_count[cell1], n2 = P.cell_count[cell2];
+  S.n1 = n1;
+  S.n2 = n2;
+  S.start1 = P.cell_start[cell1];
+  S.start2 = P.cell_start[cell2];
+  bool same = (b1 == b2) && (c1 == c2);
+  if (P.round > 0) {
+    // redraws of lost samples; a per-particle pair is not redone
+    long long nl = S.path == kPathSet ? pair_losers[gp] : 0;
+    if ((same && n1 < 2) || n1 < 1 || n2 < 1) nl = 0;
+    nwork_set[gp] = nl;
+    nwork_pp[gp] = 0;
+    nprio[gp] = nl;
+    return;
+  }
+  if (n1 == 0 || n2 == 0) {
+    S.path = kPathSkip;
+    nwork_set[gp] = nwork_pp[gp] = nprio[gp] = 0;
+    return;
+  }
+  const GridDev& G = *P.grid;
+  int cc = coag_dest_class(P.w, G.centers, b1, b2, c1, c2);
+  double f_max = max_num_conc_factor(P.w, G.edges, b1, b2, c1, c2, cc);
+  double k_max = P.kmax_tab[b1 + nb * b2] * f_max;
+  if (kmax_inflate != 0.f) k_max = k_max * (1.0 + (double)kmax_inflate);
+  S.cc = cc;
+  S.k_max = k_max;
+  S.inv_k_max = 1.0 / k_max;
+  {
+    double ri = G.centers[b1], rj = G.centers[b2];
+    S.fflat = P.flat ? num_conc_factor(P.w, ri, rj, c1, c2, cc) : 1.0;
+  }
+  // try_per_particle_coag eligibility (coagulation.F90:191-217)
+  if (use_particle_path && P.mono_dec) {
+    double n1min, n1max, n2min, n2max;
+    {
+      double a = num_conc_at_radius<double>(P.w, c1, G.edges[b1]);
+      double b = num_conc_at_radius<double>(P.w, c1, G.edges[b1 + 1]);
+      n1min = a < b ? a : b;
+      n1max = a > b ? a : b;
+      a = num_conc_at_radius<double>(P.w, c2, G.edges[b2]);
+      b = num_conc_at_radius<double>(P.w, c2, G.edges[b2 + 1]);
+      n2min = a < b ? a : b;
+      n2max = a > b ? a : b;
+    }
+    bool ok = false;
+    int bt = 0, bs = 0, ct = 0, cs = 0;
+    if (n1max < n2min && cc == c1) {
+      bt = b1; bs = b2; ct = c1; cs = c2; ok = true;
+    }
+    if (n2max < n1min && cc == c2) {
+      bt = b2; bs = b1; ct = c2; cs = c1; ok = true;
+    }
+    if (ok) {
+      int ns = P.cell_count[bs + nb * cs];
+      double nspt = k_max * P.del_t * (double)ns;
+      double min_tv = rad2vol(G.edges[bt]);
+      double max_sv = rad2vol(G.edges[bs + 1]);
+      double max_new = min_tv + max_sv * nspt;
+      if (nspt >= 1.0 && !(max_new / min_tv > 1.5)) {
+        S.path = kPathParticle;
+        S.bt = bt; S.bs = bs; S.ct = ct; S.cs = cs;
+        S.nspt = nspt;
+        int nt = P.cell_count[bt + nb * ct];
+        nwork_set[gp] = 0;
+        nwork_pp[gp] = nt;
+        nprio[gp] = nt;
+        return;
+      }
+    }
+  }
+  // per_set_coag / compute_n_samp
+  double n_possible = same ? (double)n1 * ((double)n2 - 1.0) / 2.0 : (double)n1 * (double)n2;
+  double mean = k_max * P.del_t * n_possible;
+  Rng g = make_rng(P, kStreamPair, (uint32_t)p, 0);
+  int ns = rand_poisson(g, mean);
+  if (ns < 0) {
+    set_status(P.ctr, kErrTimeout);
+    ns = 0;
+  }
+  S.path = kPathSet;
+  add_ll(&P.ctr->tot_samp, (long long)((long long)ns));
+  if ((same && n1 < 2) || n1 < 1 || n2 < 1) ns = 0;
+  nwork_set[gp] = ns;
+  nwork_pp[gp] = 0;
+  nprio[gp] = ns;
+}
+
+// ---------------------------------------------------------------------------
+// weighted kernel of a pair of records (num_conc_weighted_kernel,
+// coag_kernel.F90:175-209)
+template <int KT, class T, bool FLAT>
+__device__ __forceinline__ T pair_kernel(const PopDev& P, const T* q1, const T* q2, int c1, int c2,
+                                         int cc, T fflat, T coeff) {
+  // q = {r, rv, nc, a, b, c}
+  T k;
+  if (KT == kKernelAdditive) {
+    k = coeff * (q1[3] + q2[3]);
+  } else if (KT == kKernelConstant) {
+    k = (T)kBeta0;
+  } else if (KT == kKernelBrown) {
+    k = brown_pair<T>(q1[0], q1[3], q1[4], q1[5], q2[0], q2[3], q2[4], q2[5]);
+  } else if (KT == kKernelSedi) {
+    k = sedi_pair<T>(q1[0], q1[3], q2[0], q2[3]);
+  } else {
+    k = T(0);
+  }
+  if (FLAT) return k * fflat;
+  T rij = vol2rad(q1[1] + q2[1]);
+  T ncij = num_conc_at_radius<T>(P.w, cc, rij);
+  T nci = q1[2], ncj = q2[2];
+  T mn = nci;
+  if (ncj < mn) mn = ncj;
+  if (ncij < mn) mn = ncij;
+  return k * (nci * ncj / mn);
+}
+
+__device__ __forceinline__ int find_pair(const long long* off, int n, long long w) {
+  // largest gp with off[gp] <= w (off is an exclusive scan, off[n] = total)
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (off[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per-set pair tests (maybe_coag_pair, coagulation.F90:712-759).  One thread
+// per sample w of the flattened (population, pair, sample) space.
+template <int KT, class T, bool FLAT>
+__global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpair_pop,
+                                              const int* gpair_local, const long long* work_off,
+                                              const long long* prio_off, int n_gpairs,
+                                              const long long* total, uint8_t* flag, int2* ev) {
+  long long W = *total;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < W;
+       w += (long long)gridDim.x * blockDim.x) {
+    int gp = find_pair(work_off, n_gpairs, w);
+    const PopDev& P = pops[gpair_pop[gp]];
+    int p = gpair_local[gp];
+    long long s = w - work_off[gp];
+    const PairState& S = P.pair[p];
+    PairDesc d = P.pair_desc[p];
+    U4 rnd = philox4x32_10(U4{P.step, (uint32_t)(p << 12) | ((P.round & 0xffu) << 4) | kStreamTest,
+                              (uint32_t)s, 0u},
+                           (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+    // find_rand_pair (coagulation.F90:766-803), 0-based entries
+    int n1 = S.n1, n2 = S.n2;
+    int i1 = (int)(u32d(rnd.x) * (double)n1);
+    if (i1 >= n1) i1 = n1 - 1;
+    int i2;
+    bool same = (d.b1 == d.b2) && (d.c1 == d.c2);
+    if (same) {
+      i2 = (int)(u32d(rnd.y) * (double)(n2 - 1));
+      if (i2 >= n2 - 1) i2 = n2 - 2;
+      if (i2 == i1) i2 = n2 - 1;
+    } else {
+      i2 = (int)(u32d(rnd.y) * (double)n2);
+      if (i2 >= n2) i2 = n2 - 1;
+    }
+    int e1 = S.start1 + i1, e2 = S.start2 + i2;
+    T k;
+    if constexpr (sizeof(T) == 8) {
+      const double* q1 = (const double*)&P.recd[e1];
+      const double* q2 = (const double*)&P.recd[e2];
+      k = (T)pair_kernel<KT, double, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, S.fflat, P.coeff);
+    } else {
+      const float* q1 = (const float*)&P.recf[e1];
+      const float* q2 = (const float*)&P.recf[e2];
+      k = (T)pair_kernel<KT, float, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, (float)S.fflat,
+                                          (float)P.coeff);
+    }
+    T prob = k * (T)S.inv_k_max;
+    if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, (long long)(1LL));
+    bool acc = (T)u53(rnd.z, rnd.w) < prob;
+    flag[w] = acc ? 1 : 0;
+    if (acc) {
+      int s1 = P.list[e1], s2 = P.list[e2];
+      unsigned prio = (unsigned)(prio_off[gp] + s);
+      atomicMin(&P.claim[s1], prio);
+      atomicMin(&P.claim[s2], prio);
+      ev[w] = make_int2(s1, s2);
+    }
+  }
+}
+
+}  // namespace pmc

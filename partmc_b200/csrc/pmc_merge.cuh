@@ -1,0 +1,569 @@
+// pmc_merge.cuh -- applying accepted coagulation events on the device.
+//
+// Per-set events: coagulate_weighting + coagulate (coagulation.F90:810-985).
+// Per-particle (accelerated) path: sample_source_particle +
+// coag_target_with_source (coagulation.F90:333-582), one thread per target.
+// Every write to a particle slot is guarded by the slot's claim word: an
+// event or target operation is applied only if it holds the lowest priority
+// on every slot it writes or removes; otherwise it is redone in the next
+// round against the re-sorted state.
+#pragma once
+
+#include "pmc_kernels.cuh"
+
+namespace pmc {
+
+// Metadata of one particle (the non-volume fields of aero_particle_t,
+// aero_particle.F90:30-69, without optical properties).
+struct PMeta {
+  int grp, cls;
+  long long id;
+  int nprim, ncomp;
+  int csrc[kMaxComponent];
+  double ctime[kMaxComponent];
+  double lct, gct, imf, den_ice, phi;
+  int hyst, frozen;
+};
+
+__device__ __forceinline__ void load_meta(const PopDev& P, int i, PMeta& m) {
+  m.grp = P.grp[i];
+  m.cls = P.cls[i];
+  m.id = P.id[i];
+  m.nprim = P.nprim[i];
+  m.ncomp = P.ncomp[i];
+  for (int k = 0; k < m.ncomp; k++) {
+    m.csrc[k] = P.csrc[(size_t)k * P.cap + i];
+    m.ctime[k] = P.ctime[(size_t)k * P.cap + i];
+  }
+  m.lct = P.lct[i];
+  m.gct = P.gct[i];
+  m.imf = P.imf[i];
+  m.den_ice = P.den_ice[i];
+  m.phi = P.phi[i];
+  m.hyst = P.hyst[i];
+  m.frozen = P.frozen[i];
+}
+
+__device__ __forceinline__ void store_particle(const PopDev& P, int i, const double* v,
+                                               const PMeta& m) {
+  double vt = 0.0, ms = 0.0;
+  for (int s = 0; s < P.n_spec; s++) {
+    P.vol[(size_t)s * P.cap + i] = v[s];
+    vt = vt + v[s];
+  }
+  for (int s = 0; s < P.n_spec; s++) ms = ms + v[s] * P.density[s];
+  P.vtot[i] = vt;
+  P.mass[i] = ms;
+  P.grp[i] = m.grp;
+  P.cls[i] = m.cls;
+  P.id[i] = m.id;
+  P.nprim[i] = m.nprim;
+  P.ncomp[i] = m.ncomp;
+  for (int k = 0; k < m.ncomp; k++) {
+    P.csrc[(size_t)k * P.cap + i] = m.csrc[k];
+    P.ctime[(size_t)k * P.cap + i] = m.ctime[k];
+  }
+  P.lct[i] = m.lct;
+  P.gct[i] = m.gct;
+  P.imf[i] = m.imf;
+  P.den_ice[i] = m.den_ice;
+  P.phi[i] = m.phi;
+  P.hyst[i] = m.hyst;
+  P.frozen[i] = m.frozen;
+  P.alive[i] = 1;
+}
+
+__device__ __forceinline__ void zero_meta(PMeta& m) {
+  m.grp = m.cls = 0;
+  m.id = 0;
+  m.nprim = m.ncomp = 0;
+  m.lct = m.gct = m.imf = 0.0;
+  m.den_ice = __longlong_as_double(0x7ff8000000000000LL);
+  m.phi = m.den_ice;
+  m.hyst = m.frozen = 0;
+}
+
+// aero_particle_coagulate, aero_particle.F90:917-1033 (metadata part; the
+// caller adds the volumes).  out may alias a: inputs are read first.
+template <class R>
+__device__ void coag_meta(R& g, const PMeta& a, double ice_a, const PMeta& b, double ice_b,
+                          PMeta& out) {
+  PMeta r;
+  r.grp = 0;
+  r.cls = 0;
+  r.hyst = (a.hyst == 1 && b.hyst == 1) ? 1 : 0;
+  r.id = 0;
+  int n1 = a.ncomp, n2 = b.ncomp;
+  if (n1 + n2 > kMaxComponent) {
+    int n1_new = prob_round(g, (double)a.nprim / (double)(a.nprim + b.nprim) * (double)kMaxComponent);
+    if (n1_new > n1) n1_new = n1;  // cannot sample more than exist
+    int n2_new = kMaxComponent - n1_new;
+    if (n2_new > n2) n2_new = n2;
+    int sample[kMaxComponent];
+    sample_wo_replacement(g, n1_new, n1, sample);
+    for (int i = 0; i < n1_new; i++) {
+      r.csrc[i] = a.csrc[sample[i] - 1];
+      r.ctime[i] = a.ctime[sample[i] - 1];
+    }
+    sample_wo_replacement(g, n2_new, n2, sample);
+    for (int i = 0; i < n2_new; i++) {
+      r.csrc[n1_new + i] = b.csrc[sample[i] - 1];
+      r.ctime[n1_new + i] = b.ctime[sample[i] - 1];
+    }
+    r.ncomp = n1_new + n2_new;
+  } else {
+    for (int i = 0; i < n1; i++) {
+      r.csrc[i] = a.csrc[i];
+      r.ctime[i] = a.ctime[i];
+    }
+    for (int i = 0; i < n2; i++) {
+      r.csrc[n1 + i] = b.csrc[i];
+      r.ctime[n1 + i] = b.ctime[i];
+    }
+    r.ncomp = n1 + n2;
+  }
+  r.lct = a.lct < b.lct ? a.lct : b.lct;
+  r.gct = a.gct > b.gct ? a.gct : b.gct;
+  r.frozen = (a.frozen || b.frozen) ? 1 : 0;
+  r.imf = a.imf > b.imf ? a.imf : b.imf;
+  if (r.frozen) {
+    if (a.frozen && b.frozen) {
+      double i1 = ice_a * kWaterDensity / a.den_ice;
+      double i2 = ice_b * kWaterDensity / b.den_ice;
+      r.den_ice = (a.den_ice * i1 + b.den_ice * i2) / (i1 + i2);
+    } else if (a.frozen) {
+      r.den_ice = a.den_ice;
+    } else {
+      r.den_ice = b.den_ice;
+    }
+    r.phi = 1.0;
+  } else {
+    r.den_ice = __longlong_as_double(0x7ff8000000000000LL);
+    r.phi = a.phi;
+  }
+  r.nprim = a.nprim + b.nprim;
+  out = r;
+}
+
+// Decisions of coagulate_weighting (coagulation.F90:855-892).
+struct MergeDecision {
+  bool rm1, rm2, create, lost1, lost2;
+  int new_group;  // 1-based
+};
+
+template <class R>
+__device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int c1, int c2, int cc) {
+  MergeDecision d;
+  double r1 = P.rad[s1], r2 = P.rad[s2];
+  double rc = vol2rad(rad2vol(r1) + rad2vol(r2));
+  double nc1 = num_conc_at_radius<double>(P.w, c1, r1);
+  double nc2 = num_conc_at_radius<double>(P.w, c2, r2);
+  double ncc = num_conc_at_radius<double>(P.w, cc, rc);
+  d.new_group = rand_group(g, P.w, cc, rc);
+  double mn = nc1;
+  if (nc2 < mn) mn = nc2;
+  if (ncc < mn) mn = ncc;
+  d.rm1 = g.next() < mn / nc1;
+  d.rm2 = g.next() < mn / nc2;
+  d.create = g.next() < mn / ncc;
+  if (d.create) {
+    d.lost1 = d.lost2 = false;
+    if (d.rm1 && d.rm2) {
+      if (P.vtot[s1] > P.vtot[s2]) d.lost2 = true;
+      else d.lost1 = true;
+    }
+  } else {
+    d.lost1 = d.rm1;
+    d.lost2 = d.rm2;
+  }
+  return d;
+}
+
+// Resolve accepted per-set samples: winner test, slot/id needs.
+// ev_w[e] = sample index w of event e (in w order).
+__global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
+                              const long long* work_off, const long long* prio_off, int n_gpairs,
+                              const long long* n_events, const long long* ev_w, const int2* ev,
+                              int* pair_losers, int* need_slot, int* need_id, uint8_t* win) {
+  long long E = *n_events;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long w = ev_w[e];
+    int gp = find_pair(work_off, n_gpairs, w);
+    const PopDev& P = pops[gpair_pop[gp]];
+    int p = gpair_local[gp];
+    long long s = w - work_off[gp];
+    unsigned prio = (unsigned)(prio_off[gp] + s);
+    int2 sl = ev[w];
+    bool winner = P.claim[sl.x] == prio && P.claim[sl.y] == prio;
+    win[e] = winner ? 1 : 0;
+    need_slot[e] = 0;
+    need_id[e] = 0;
+    if (!winner) {
+      atomicAdd(&pair_losers[gp], 1);
+      continue;
+    }
+    PairDesc d = P.pair_desc[p];
+    const PairState& S = P.pair[p];
+    Rng g = make_rng(P, kStreamMerge, (uint32_t)p, (uint32_t)s);
+    MergeDecision m = merge_decide(P, g, sl.x, sl.y, d.c1, d.c2, S.cc);
+    if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+    if (m.create) {
+      need_slot[e] = (!m.rm1 && !m.rm2) ? 1 : 0;
+      bool keep1 = m.rm1 && !m.lost1, keep2 = m.rm2 && !m.lost2;
+      need_id[e] = (!keep1 && !keep2) ? 1 : 0;
+    }
+  }
+}
+
+// Apply winning per-set events (coagulate, coagulation.F90:928-985).
+__global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
+                            const long long* work_off, int n_gpairs, const long long* n_events,
+                            const long long* ev_w, const int2* ev, const uint8_t* win,
+                            const long long* slot_rank, const long long* id_rank,
+                            const int* slot_base, const long long* id_base) {
+  long long E = *n_events;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (!win[e]) continue;
+    long long w = ev_w[e];
+    int gp = find_pair(work_off, n_gpairs, w);
+    int pop = gpair_pop[gp];
+    const PopDev& P = pops[pop];
+    int p = gpair_local[gp];
+    long long s = w - work_off[gp];
+    int2 sl = ev[w];
+    int s1 = sl.x, s2 = sl.y;
+    PairDesc d = P.pair_desc[p];
+    const PairState& S = P.pair[p];
+    Rng g = make_rng(P, kStreamMerge, (uint32_t)p, (uint32_t)s);
+    MergeDecision m = merge_decide(P, g, s1, s2, d.c1, d.c2, S.cc);
+    add_ll(&P.ctr->tot_coag, (long long)(1LL));
+    int dlive = 0;
+    if (m.create) {
+      double v[kMaxSpec];
+      PMeta a, b;
+      load_meta(P, s1, a);
+      load_meta(P, s2, b);
+      double ice_a = 0.0, ice_b = 0.0;
+      if (P.i_water > 0) {
+        ice_a = P.vol[(size_t)(P.i_water - 1) * P.cap + s1];
+        ice_b = P.vol[(size_t)(P.i_water - 1) * P.cap + s2];
+      }
+      for (int q = 0; q < P.n_spec; q++)
+        v[q] = P.vol[(size_t)q * P.cap + s1] + P.vol[(size_t)q * P.cap + s2];
+      PMeta c;
+      coag_meta(g, a, ice_a, b, ice_b, c);
+      c.grp = m.new_group;
+      c.cls = S.cc + 1;
+      int dest;
+      if (m.rm1) dest = s1;
+      else if (m.rm2) dest = s2;
+      else dest = slot_base[pop] + (int)slot_rank[e];
+      if (m.rm1 && !m.lost1) c.id = a.id;
+      else if (m.rm2 && !m.lost2) c.id = b.id;
+      else c.id = id_base[pop] + id_rank[e];
+      if (dest >= P.cap) {
+        set_status(P.ctr, kErrCapacity);
+        continue;
+      }
+      store_particle(P, dest, v, c);
+      // the coagulated particle must lie on the grid (aero_state_add_particle
+      // with allow_resort=.false., aero_sorted.F90:427-440)
+      double r = vol2rad(P.vtot[dest]);
+      int nbin = bin_find(P.grid->n_bin, P.grid->log_lo, P.grid->log_hi, r);
+      if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
+      if (m.rm1 && dest != s1) P.alive[s1] = 0;
+      if (m.rm2 && dest != s2) P.alive[s2] = 0;
+      dlive = 1 - (int)m.rm1 - (int)m.rm2;
+    } else {
+      if (m.rm1) P.alive[s1] = 0;
+      if (m.rm2) P.alive[s2] = 0;
+      dlive = -(int)m.rm1 - (int)m.rm2;
+    }
+    if (dlive) add_ll(&P.ctr->n_live, (long long)(dlive));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per-particle (accelerated) path, phase 1: run sample_source_particle and
+// the target update of coag_target_with_source for one target, store the
+// result, and claim the target and every removed source.
+constexpr int kMaxRemove = 64;  // removals stored per target operation
+constexpr int kMaxCopies = 8;   // dup copies per target operation
+
+struct PPResult {
+  int target, p;        // target slot, pair (local)
+  int merged;           // n_coag > 0
+  int n_copies;         // prob_round(old_nc / new_nc); 0 removes the target
+  int n_rm;
+  int copy_group[kMaxCopies];
+  int rm[kMaxRemove];
+  PMeta meta;           // new target metadata
+};
+
+template <int KT>
+__device__ double pp_kernel(const PopDev& P, const RecD& qs, const RecD& qt, int cs, int ct) {
+  const double* a = (const double*)&qs;
+  const double* b = (const double*)&qt;
+  return pair_kernel<KT, double, false>(P, a, b, cs, ct, ct, 0.0, P.coeff);
+}
+
+template <int KT>
+__global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pair,
+                         const int* op_slot, const int* op_k, const unsigned* op_prio,
+                         const long long* n_ops, PPResult* res, double* res_vol) {
+  long long Q = *n_ops;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
+       q += (long long)gridDim.x * blockDim.x) {
+    const PopDev& P = pops[op_pop[q]];
+    int p = op_pair[q], t = op_slot[q];
+    unsigned prio = op_prio[q];
+    PPResult& R = res[q];
+    R.target = t;
+    R.p = p;
+    R.merged = 0;
+    R.n_copies = 1;
+    R.n_rm = 0;
+    if (!P.alive[t]) continue;
+    const PairState& S = P.pair[p];
+    const GridDev& G = *P.grid;
+    int nb = G.n_bin;
+    int cs = S.cs, ct = S.ct;
+    int src_cell = S.bs + nb * cs;
+    int n_src = P.cell_count[src_cell];
+    int src_start = P.cell_start[src_cell];
+    if (n_src == 0) continue;
+    RecD qt = make_rec(P, t);
+    double nc_target = qt.nc;
+    double nc_src_min = num_conc_at_radius<double>(P.w, cs, G.edges[S.bs]);
+    double prm_max = nc_target / nc_src_min;
+    if (!(prm_max <= 1.0)) {
+      set_status(P.ctr, kErrAssert);
+      continue;
+    }
+    Rng g = make_rng(P, kStreamPart, (uint32_t)p, (uint32_t)op_k[q]);
+    int n_remove = rand_poisson(g, prm_max * S.nspt);
+    int n_extra = rand_poisson(g, (1.0 - prm_max) * S.nspt);
+    if (n_remove < 0 || n_extra < 0) {
+      set_status(P.ctr, kErrTimeout);
+      continue;
+    }
+    int n_total = n_remove + n_extra;
+    int ns = P.n_spec;
+    double* acc = res_vol + (size_t)q * ns;  // accumulated source volumes
+    double vol_sq[kMaxSpec], vol_cv[kMaxSpec];
+    for (int k = 0; k < ns; k++) {
+      acc[k] = 0.0;
+      vol_sq[k] = 0.0;
+      vol_cv[k] = 0.0;
+    }
+    PMeta src;
+    zero_meta(src);
+    int n_avg = 0, n_samp = 0;
+    double pc_tot = 0.0;
+    for (int i_samp = 1; i_samp <= n_total; i_samp++) {
+      if (n_samp > n_remove && n_avg >= 2) {
+        double cv_max = 0.0;
+        bool found = false;
+        for (int k = 0; k < ns; k++) {
+          double mean = acc[k] / (double)n_avg;
+          if (mean > 0.0) vol_cv[k] = sqrt(vol_sq[k] / (double)n_avg - mean * mean) / mean;
+        }
+        for (int k = 0; k < ns; k++) {
+          if (isnan(vol_cv[k])) continue;
+          if (!found || vol_cv[k] > cv_max) cv_max = vol_cv[k];
+          found = true;
+        }
+        if (!found) cv_max = __longlong_as_double(0x7ff8000000000000LL);
+        double conf = cv_max / sqrt((double)n_avg) * student_t_95(n_avg);
+        if (conf < 0.1) break;
+      }
+      n_samp++;
+      int ie = rand_int(g, n_src);
+      int e = src_start + ie - 1;
+      int si = P.list[e];
+      RecD qs = P.recd[e];
+      double k = pp_kernel<KT>(P, qs, qt, cs, ct);
+      double pc = k * S.inv_k_max;
+      pc_tot = pc_tot + pc;
+      if (g.next() < pc) {
+        n_avg++;
+        PMeta sm;
+        load_meta(P, si, sm);
+        double ice_a = 0.0, ice_b = 0.0;
+        if (P.i_water > 0) {
+          ice_a = acc[P.i_water - 1];
+          ice_b = P.vol[(size_t)(P.i_water - 1) * P.cap + si];
+        }
+        coag_meta(g, src, ice_a, sm, ice_b, src);
+        for (int k2 = 0; k2 < ns; k2++) {
+          double vi = P.vol[(size_t)k2 * P.cap + si];
+          acc[k2] = acc[k2] + vi;
+          vol_sq[k2] = vol_sq[k2] + vi * vi;
+        }
+        if (i_samp <= n_remove) {
+          double pri = nc_target / qs.nc;
+          if (g.next() < pri / prm_max) {
+            bool dup = false;
+            for (int z = 0; z < R.n_rm; z++) dup = dup || (R.rm[z] == si);
+            if (!dup) {
+              if (R.n_rm < kMaxRemove) {
+                R.rm[R.n_rm++] = si;
+                atomicMin(&P.claim[si], prio);
+              } else {
+                set_status(P.ctr, kErrCapacity);
+              }
+            }
+          }
+        }
+      }
+    }
+    add_ll(&P.ctr->tot_samp, (long long)((long long)n_samp));
+    if (n_avg == 0) continue;
+    double pc_mean = pc_tot / (double)n_samp;
+    if (!(pc_mean <= 1.0)) add_ll(&P.ctr->kmax_warn, (long long)(1LL));
+    int n_coag = rand_binomial(g, n_total, pc_mean);
+    double scale = (double)n_coag / (double)n_avg;
+    for (int k = 0; k < ns; k++) acc[k] = acc[k] * scale;
+    src.nprim = prob_round(g, (double)src.nprim * scale);
+    {
+      int n_comp = src.ncomp;
+      int n_new = src.nprim < kMaxComponent ? src.nprim : kMaxComponent;
+      int sample[kMaxComponent];
+      if (n_new < n_comp) {
+        PMeta m = src;
+        sample_wo_replacement(g, n_new, n_comp, sample);
+        for (int i = 0; i < n_new; i++) {
+          m.csrc[i] = src.csrc[sample[i] - 1];
+          m.ctime[i] = src.ctime[sample[i] - 1];
+        }
+        m.ncomp = n_new;
+        src = m;
+      } else if (n_comp < kMaxComponent && n_comp > 0) {
+        PMeta m = src;
+        int i_comp = 1;
+        while (i_comp <= n_new) {
+          if (i_comp + n_comp <= n_new) {
+            for (int i = 1; i <= n_comp; i++) {
+              m.csrc[i_comp + i - 2] = src.csrc[i - 1];
+              m.ctime[i_comp + i - 2] = src.ctime[i - 1];
+            }
+            i_comp += n_comp;
+          } else {
+            int size = n_new - i_comp + 1;
+            sample_wo_replacement(g, size, n_comp, sample);
+            for (int i = 1; i <= size; i++) {
+              m.csrc[i_comp + i - 2] = src.csrc[sample[i - 1] - 1];
+              m.ctime[i_comp + i - 2] = src.ctime[sample[i - 1] - 1];
+            }
+            i_comp = n_new + 1;
+          }
+        }
+        m.ncomp = n_new;
+        src = m;
+      }
+    }
+    add_ll(&P.ctr->tot_coag, (long long)((long long)n_coag));
+    if (n_coag == 0) continue;
+    // coag_target_with_source (coagulation.F90:522-582): new target
+    PMeta tm;
+    load_meta(P, t, tm);
+    double ice_t = 0.0;
+    if (P.i_water > 0) ice_t = P.vol[(size_t)(P.i_water - 1) * P.cap + t];
+    double ice_s = P.i_water > 0 ? acc[P.i_water - 1] : 0.0;
+    long long tid = tm.id;
+    double old_nc = nc_target;
+    PMeta nm;
+    coag_meta(g, tm, ice_t, src, ice_s, nm);
+    nm.id = tid;
+    double vt = 0.0;
+    for (int k = 0; k < ns; k++) {
+      acc[k] = P.vol[(size_t)k * P.cap + t] + acc[k];  // now the new target volumes
+      vt = vt + acc[k];
+    }
+    double rnew = vol2rad(vt);
+    int cc = S.cc;
+    nm.grp = rand_group(g, P.w, cc, rnew);
+    nm.cls = cc + 1;
+    int b = bin_find(nb, G.log_lo, G.log_hi, rnew);
+    if (b < 1 || b > nb) set_status(P.ctr, kErrOutOfGrid);
+    double new_nc = num_conc_at_radius<double>(P.w, cc, rnew);
+    int n_copies = prob_round(g, old_nc / new_nc);
+    if (n_copies > kMaxCopies) {
+      set_status(P.ctr, kErrCapacity);
+      n_copies = kMaxCopies;
+    }
+    for (int z = 1; z < n_copies; z++) R.copy_group[z] = rand_group(g, P.w, cc, rnew);
+    R.merged = 1;
+    R.n_copies = n_copies;
+    R.meta = nm;
+    atomicMin(&P.claim[t], prio);
+  }
+}
+
+// phase 2a: winners and allocation needs of the target operations
+__global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsigned* op_prio,
+                             const long long* n_ops, const PPResult* res, uint8_t* win,
+                             int* need_slot, int* need_id, int* lost) {
+  long long Q = *n_ops;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
+       q += (long long)gridDim.x * blockDim.x) {
+    const PopDev& P = pops[op_pop[q]];
+    const PPResult& R = res[q];
+    unsigned prio = op_prio[q];
+    bool ok = true;
+    if (R.merged) ok = ok && P.claim[R.target] == prio;
+    for (int z = 0; z < R.n_rm; z++) ok = ok && P.claim[R.rm[z]] == prio;
+    win[q] = ok ? 1 : 0;
+    lost[q] = ok ? 0 : 1;
+    int extra = (ok && R.merged && R.n_copies > 1) ? R.n_copies - 1 : 0;
+    need_slot[q] = extra;
+    need_id[q] = extra;
+  }
+}
+
+// phase 2b: apply the winning target operations
+__global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long long* n_ops,
+                           const PPResult* res, const double* res_vol, const uint8_t* win,
+                           const long long* slot_rank, const long long* id_rank,
+                           const int* slot_base, const long long* id_base) {
+  long long Q = *n_ops;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
+       q += (long long)gridDim.x * blockDim.x) {
+    if (!win[q]) continue;
+    int pop = op_pop[q];
+    const PopDev& P = pops[pop];
+    const PPResult& R = res[q];
+    int dlive = 0;
+    for (int z = 0; z < R.n_rm; z++) {
+      P.alive[R.rm[z]] = 0;
+      dlive--;
+    }
+    if (R.merged) {
+      const double* v = res_vol + (size_t)q * P.n_spec;
+      int t = R.target;
+      if (R.n_copies == 0) {
+        P.alive[t] = 0;
+        dlive--;
+      } else {
+        store_particle(P, t, v, R.meta);
+        for (int z = 1; z < R.n_copies; z++) {
+          int dest = slot_base[pop] + (int)slot_rank[q] + (z - 1);
+          if (dest >= P.cap) {
+            set_status(P.ctr, kErrCapacity);
+            break;
+          }
+          PMeta cm = R.meta;
+          cm.grp = R.copy_group[z];
+          cm.id = id_base[pop] + id_rank[q] + (z - 1);
+          store_particle(P, dest, v, cm);
+          dlive++;
+        }
+      }
+    }
+    if (dlive) add_ll(&P.ctr->n_live, (long long)(dlive));
+  }
+}
+
+}  // namespace pmc

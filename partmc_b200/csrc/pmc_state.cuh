@@ -1,0 +1,140 @@
+// pmc_state.cuh -- device-resident layout of particle populations.
+//
+// A population is the GPU form of aero_state_t (aero_state.F90:69-84):
+//  - particle slots, structure-of-arrays, slot i of species s at
+//    vol[s * cap + i] (species-major, so a pass over one species is
+//    coalesced); per-slot caches vtot = sum(vol) and mass = sum(vol*density)
+//    are kept exact (recomputed in the reference's summation order on every
+//    change);
+//  - the aero_sorted_t equivalent (aero_sorted.F90:47-66): bin grid, one
+//    list of slot numbers per (bin, class) cell in CSR form, and a
+//    bin-ordered array of pair-test records;
+//  - the k_max table per bin pair (coag_kernel_max) and per-pair state.
+#pragma once
+
+#include <cstdint>
+
+#include "pmc_physics.cuh"
+
+namespace pmc {
+
+// Pair-test record of one particle, stored in cell order so that a test
+// reads two records.  r: radius; rv: rad2vol(r) (for the coagulated radius
+// of coag_num_conc_factor); nc: number concentration of the particle's class
+// at r; a/b/c: per-particle kernel terms (additive: total volume; Brownian:
+// diffusivity, squared thermal speed, delta^2; sedimentation: terminal
+// velocity).
+struct __align__(16) RecD {
+  double r, rv, nc, a, b, c;
+};
+struct __align__(32) RecF {
+  float r, rv, nc, a, b, c, pad0, pad1;
+};
+
+struct GridDev {
+  int n_bin;
+  double log_lo, log_hi;  // log(edges[0]), log(edges[n_bin])
+  double edges[kMaxBin + 1];
+  double centers[kMaxBin];
+};
+
+// (b1, c1, b2, c2) of pair p, in the reference's loop order
+// (coagulation.F90:74-94).  0-based.
+struct PairDesc {
+  int16_t b1, b2;
+  int8_t c1, c2, pad0, pad1;
+};
+
+enum PairPath : int { kPathSkip = 0, kPathSet = 1, kPathParticle = 2 };
+
+struct PairState {
+  double k_max;      // coag_kernel_max(b1,b2) * f_max (FP32 mode: inflated)
+  double inv_k_max;  // accept_factor = 1 / k_max
+  double fflat;      // constant weight factor when every weight is flat
+  double nspt;       // n_source_per_target (per-particle path)
+  int path;
+  int cc;            // destination class (0-based)
+  int n1, n2;        // cell sizes at round start
+  int start1, start2;
+  int bt, bs, ct, cs;  // per-particle path target/source cells (0-based)
+};
+
+// Per-population counters and scalars that kernels update.
+struct PopCtr {
+  int n_slots;       // slots in use (high-water mark)
+  int n_live;
+  long long next_id;
+  long long tot_samp, tot_coag;
+  long long kmax_warn;
+  long long redraws;
+  int status;        // first error code seen
+  int out_of_grid;
+  int bmin, bmax;    // occupied bin range after a sort (-1 if empty)
+  unsigned long long rmin_bits, rmax_bits;  // radius range (positive doubles)
+  int new_slots, new_ids;  // allocations in the current apply phase
+  int losers;
+  int n_events;
+  long long rng_used;      // replay: uniforms consumed
+};
+
+// One population as the kernels see it (kept in device memory).
+struct PopDev {
+  int cap, n_spec, n_group, n_class, i_water;
+  int n_cells;  // n_bin * n_class
+  int n_chunks; // sort chunks covering n_slots
+  int n_pairs;
+  uint64_t seed;
+  uint32_t step, round;
+  int kernel_type;
+  double temp, pressure, coeff, del_t;
+  BrownEnv benv;
+  double dmin, dmax;  // min/max species density
+  Weights w;
+  bool flat;
+  bool mono_dec;
+
+  // slots
+  double* vol;
+  double* vtot;
+  double* mass;
+  double* rad;
+  int* grp;  // 1-based
+  int* cls;  // 1-based
+  long long* id;
+  int* nprim;
+  int* ncomp;
+  int* csrc;      // [kMaxComponent][cap]
+  double* ctime;  // [kMaxComponent][cap]
+  double* lct;
+  double* gct;
+  double* imf;
+  double* den_ice;
+  double* phi;
+  int* hyst;
+  int* frozen;
+  uint8_t* alive;
+  int* bin;  // 0-based bin of each slot (after the sort), -1 dead
+
+  const double* density;  // [n_spec]
+
+  // sort
+  GridDev* grid;
+  int* chunk_hist;  // [n_chunks][n_cells]
+  int* cell_count;  // [n_cells]
+  int* cell_start;  // [n_cells + 1]
+  int* list;        // [cap] slot numbers in cell order
+  RecD* recd;       // [cap]
+  RecF* recf;       // [cap]
+
+  double* kmax_tab;  // [n_bin * n_bin], (b1, b2) at b1 + n_bin * b2
+  int kmax_valid;
+
+  const PairDesc* pair_desc;  // [n_pairs]
+  PairState* pair;            // [n_pairs]
+
+  unsigned* claim;  // [cap] lowest priority that claimed the slot this round
+
+  PopCtr* ctr;
+};
+
+}  // namespace pmc

@@ -1,0 +1,96 @@
+"""The parallel CUDA step against the reference's invariants and the oracle's
+statistics, through the C ABI."""
+import numpy as np
+import pytest
+
+import partmc_b200 as pm
+from partmc_b200 import aero_dist
+from oracle import exact as E
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def test_flat_weights_conserve_volume_and_count(gpu_lib):
+    pop = aero_dist.additive_exp(20000, seed=1)
+    st = pm.AeroState(pop.aero_data, pop.awa, seed=3)
+    st.add_particles(pop.vol, pop.group)
+    env = pm.EnvState(288.0, 1e5, 1000.0)
+    v0 = pop.vol.sum()
+    n = pop.n_part
+    for _ in range(50):
+        ns, nc = pm.mc_coag(pm.COAG_KERNEL_TYPE_ADDITIVE, env, pop.aero_data, st, 1.0)
+        assert ns >= nc >= 0
+        n -= nc  # flat weights: every event removes both and creates one
+        assert st.n_part() == n
+    p = st.particles()
+    assert abs(p["vol"].sum() / v0 - 1) < 1e-12
+    assert len(np.unique(p["id"])) == len(p["id"])
+
+
+@pytest.mark.parametrize("mode", [pm.MODE_FP64, pm.MODE_MIXED])
+def test_additive_matches_exact_solution(gpu_lib, mode):
+    N0, R, n_part = 1e9, 1e-5, 20000
+    times = [60.0, 180.0, 300.0]
+    hs = {t: [] for t in times}
+    for k in range(6):
+        pop = aero_dist.additive_exp(n_part, seed=100 + k, num_conc=N0, radius_at_mean_vol=R)
+        st = pm.AeroState(pop.aero_data, pop.awa, seed=11 + k, mode=mode)
+        st.add_particles(pop.vol, pop.group)
+        env = pm.EnvState(288.0, 1e5, 1000.0)
+        for step in range(1, 301):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_ADDITIVE, env, pop.aero_data, st, 1.0)
+            if float(step) in hs:
+                p = st.particles()
+                d = 2 * E.vol2rad(p["vol"].sum(1))
+                h, dc = E.size_histogram(d, np.full(len(d), pop.awa.magnitude[0, 0]))
+                hs[float(step)].append(h)
+    for t in times:
+        ex = E.soln_additive_exp(dc / 2, t, N0, R, 1000.0)
+        err = E.rel_err_by_col(ex, np.mean(hs[t], axis=0))[0]
+        assert err < 0.05, (t, err)
+
+
+def test_brownian_matches_oracle_ensemble(gpu_lib):
+    """Number and mass distributions of a power-weighted Brownian run agree
+    with the oracle's ensemble within 3 sigma of the Monte Carlo error."""
+    n_part, n_runs, n_steps = 4000, 8, 30
+    env = pm.EnvState(288.0, 1e5)
+    hist = {"gpu": [], "cpu": []}
+    for k in range(n_runs):
+        pop = aero_dist.brown_bimodal(n_part, seed=200 + k)
+        st = pm.AeroState(pop.aero_data, pop.awa, seed=300 + k)
+        st.add_particles(pop.vol, pop.group)
+        orc = O.Oracle(pop.aero_data.density, (pop.awa.type, pop.awa.magnitude, pop.awa.exponent), seed=400 + k)
+        orc.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
+        orc.set_next_id(pop.n_part + 1)
+        for _ in range(n_steps):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, 600.0)
+            orc.mc_coag(O.KERNEL_BROWN, 288.0, 1e5, 0.0, 600.0)
+        for key, vol in (("gpu", st.particles()["vol"]), ("cpu", orc.particles()[0])):
+            r = E.vol2rad(vol.sum(1))
+            nc = pop.awa.num_conc_at_radius(1, r)
+            h, dc = E.size_histogram(2 * r, nc, n_bin=40, dmin=1e-8, dmax=1e-6)
+            hist[key].append(h)
+    g, c = np.array(hist["gpu"]), np.array(hist["cpu"])
+    se = np.sqrt(g.var(0, ddof=1) / n_runs + c.var(0, ddof=1) / n_runs)
+    ok = se > 0
+    z = (g.mean(0) - c.mean(0))[ok] / se[ok]
+    assert np.abs(z).max() < 4.0, np.abs(z).max()
+    tot_g, tot_c = g.sum(1), c.sum(1)
+    se_t = np.sqrt(tot_g.var(ddof=1) / n_runs + tot_c.var(ddof=1) / n_runs)
+    assert abs(tot_g.mean() - tot_c.mean()) < 3 * se_t + 1e-9 * tot_c.mean()
+
+
+def test_step_is_deterministic(gpu_lib):
+    pop = aero_dist.brown_bimodal(20000, seed=7)
+    env = pm.EnvState(288.0, 1e5)
+    outs = []
+    for _ in range(2):
+        st = pm.AeroState(pop.aero_data, pop.awa, seed=5)
+        st.add_particles(pop.vol, pop.group)
+        for _ in range(5):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, 600.0)
+        outs.append(st.particles())
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
