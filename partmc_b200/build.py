@@ -20,7 +20,8 @@ UNITS = [
     ("pmc_coag.cu", []),
     ("pmc_replay.cu", ["-fmad=false"]),
 ]
-HEADERS = ["pmc_physics.cuh", "pmc_state.cuh", "pmc_kernels.cuh", "pmc_merge.cuh", "pmc_replay.cuh"]
+HEADERS = ["pmc_physics.cuh", "pmc_state.cuh", "pmc_kernels.cuh", "pmc_merge.cuh", "pmc_particle.cuh",
+           "pmc_replay.cuh"]
 
 
 def _nvcc():

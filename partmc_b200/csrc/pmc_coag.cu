@@ -460,7 +460,7 @@ struct Ctx {
   // 0 pair tests, 1 sort scatter + record build, 2 sort histogram,
   // 3 whole steps
   bool prof = false;
-  cudaEvent_t prof_ev[2] = {nullptr, nullptr};
+  cudaEvent_t prof_ev[4][2] = {};
   double prof_ms[4] = {0, 0, 0, 0};
   long long prof_launch[4] = {0, 0, 0, 0}, prof_units[4] = {0, 0, 0, 0};
   // replay
@@ -495,14 +495,14 @@ struct ProfScope {
   int id;
   long long units;
   ProfScope(Ctx& c_, int id_, long long units_) : c(c_), id(id_), units(units_) {
-    if (c.prof) cudaEventRecord(c.prof_ev[0], c.stream);
+    if (c.prof) cudaEventRecord(c.prof_ev[id][0], c.stream);
   }
   ~ProfScope() {
     if (!c.prof) return;
-    cudaEventRecord(c.prof_ev[1], c.stream);
-    cudaEventSynchronize(c.prof_ev[1]);
+    cudaEventRecord(c.prof_ev[id][1], c.stream);
+    cudaEventSynchronize(c.prof_ev[id][1]);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, c.prof_ev[0], c.prof_ev[1]);
+    cudaEventElapsedTime(&ms, c.prof_ev[id][0], c.prof_ev[id][1]);
     c.prof_ms[id] += ms;
     c.prof_launch[id] += 1;
     c.prof_units[id] += units;
@@ -933,6 +933,133 @@ void set_n_dev(Ctx& c, long long v) {
   CK(cudaMemcpyAsync(c.n_dev.p, &v, sizeof(long long), cudaMemcpyHostToDevice, c.stream));
 }
 
+// One mc_coag call in replay mode: the grid decision of
+// aero_sorted_remake_if_needed on the host (glibc log/exp, as the reference),
+// then one device thread runs the reference's loop on the persisted inverse
+// maps.  One population only.
+int replay_step_host(Ctx& c, long long* s_out, long long* k_out) {
+  if (c.n_pop != 1) return PMC_ERR_INVALID_ARG;
+  PopHost& ph = c.pops[0];
+  ReplayBuffers& rb = c.replay;
+  PopCtr r = read_ctr(c, 0);
+  if (r.n_live != r.n_slots) {
+    relayout(c, 0, ph.h.cap, true);  // dense slots, order kept
+    r = read_ctr(c, 0);
+    rb.valid = false;
+  }
+  if (ph.h.cap < 2 * r.n_slots + 1024) {
+    relayout(c, 0, 2 * r.n_slots + 1024, false);
+    rb.valid = false;
+  }
+  // radius range: from the inverse maps while they are valid, else from the
+  // particles (aero_sorted.F90:263-306)
+  double rmin = 0.0, rmax = 0.0;
+  if (!rb.valid || ph.n_bin < 1) {
+    r.rmin_bits = 0x7ff0000000000000ULL;
+    r.rmax_bits = 0;
+    write_ctr(c, 0, r);
+    push_pops(c);
+    DevBuf<uint8_t> on;
+    on.reserve(1);
+    uint8_t one = 1;
+    CK(cudaMemcpyAsync(on.p, &one, 1, cudaMemcpyHostToDevice, c.stream));
+    dim3 g(grid_for(std::max(r.n_slots, 1), 256), 1);
+    k_radius_minmax_masked<<<g, 256, 0, c.stream>>>(c.d_pops, on.p);
+    note_launch();
+    PopCtr q = read_ctr(c, 0);
+    on.release();
+    if (q.n_live > 0) {
+      memcpy(&rmin, &q.rmin_bits, 8);
+      memcpy(&rmax, &q.rmax_bits, 8);
+    }
+  } else {
+    std::vector<int> cnt(ph.n_bin * c.n_class);
+    DevBuf<int> d;
+    d.reserve(cnt.size());
+    replay_cell_counts(rb.dev, d.p, c.stream);
+    note_launch();
+    CK(cudaMemcpyAsync(cnt.data(), d.p, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    d.release();
+    int bmin = 0, bmax = 0;
+    for (int b = 1; b <= ph.n_bin; b++) {
+      int s = 0;
+      for (int cl = 0; cl < c.n_class; cl++) s += cnt[(b - 1) + ph.n_bin * cl];
+      if (s > 0) {
+        if (bmin == 0) bmin = b;
+        bmax = b;
+      }
+    }
+    if (bmin == 0) {
+      rmin = ph.edges[ph.n_bin];
+      rmax = ph.edges[0];
+    } else {
+      rmin = ph.edges[bmin - 1];
+      rmax = ph.edges[bmax];
+    }
+  }
+  bool rebuild = !rb.valid;
+  if (rmax == 0.0) {
+    if (!rb.valid) make_grid(c, ph, 0, 0.0, 0.0);
+  } else {
+    bool need = ph.n_bin < 1;
+    if (!need) {
+      double gmin = ph.edges[0], gmax = ph.edges[ph.n_bin];
+      need = rmin / gmin < 3.0 || gmax / rmax < 3.0;
+    }
+    if (need) {
+      double gmin = rmin / 10.0, gmax = rmax * 10.0;
+      int n_bin = (int)ceil((log10(gmax) - log10(gmin)) * 10.0);
+      if (n_bin > kMaxBin) return PMC_ERR_CAPACITY;
+      make_grid(c, ph, n_bin, gmin, gmax);
+      rebuild = true;
+    }
+  }
+  ph.valid_sort = true;
+  int nb = std::max(ph.n_bin, 1);
+  if (!replay_reserve(rb, ph.h.cap, nb * c.n_class, c.n_group * c.n_class, nb, c.n_class, c.n_group))
+    return PMC_ERR_CAPACITY;
+  if (rb.n_cells != nb * c.n_class || !rb.valid) rebuild = true;
+  push_pops(c);
+  if (!ph.h.kmax_valid && ph.n_bin > 0) {
+    dim3 g((ph.n_bin * ph.n_bin + 255) / 256, 1);
+    k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
+    note_launch();
+    ph.h.kmax_valid = 1;
+    push_pops(c);
+  }
+  long long hv[4] = {c.replay_used, 0, 0, r.next_id};
+  CK(cudaMemcpyAsync(rb.dev.used, hv, sizeof(long long) * 4, cudaMemcpyHostToDevice, c.stream));
+  int hi[2] = {0, r.n_slots};
+  CK(cudaMemcpyAsync(rb.dev.status, hi, sizeof(int) * 2, cudaMemcpyHostToDevice, c.stream));
+  ReplayDev rd = rb.dev;
+  rd.u = c.replay_u.p;
+  rd.n_u = c.replay_n;
+  rd.rebuild = rebuild ? 1 : 0;
+  size_t stack = 0;
+  cudaDeviceGetLimit(&stack, cudaLimitStackSize);
+  if (stack < 16384) CK(cudaDeviceSetLimit(cudaLimitStackSize, 16384));
+  replay_launch(c.d_pops, 0, rd, c.stream);
+  note_launch();
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(hv, rb.dev.used, sizeof(long long) * 4, cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaMemcpyAsync(hi, rb.dev.status, sizeof(int) * 2, cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  c.replay_used = hv[0];
+  *s_out = hv[1];
+  *k_out = hv[2];
+  r = read_ctr(c, 0);
+  r.n_slots = r.n_live = hi[1];
+  r.next_id = hv[3];
+  r.tot_samp = hv[1];
+  r.tot_coag = hv[2];
+  write_ctr(c, 0, r);
+  rb.valid = hi[0] == 0;
+  static const int map[] = {PMC_OK, PMC_ERR_INVALID_ARG, PMC_ERR_OUT_OF_GRID, PMC_ERR_CAPACITY,
+                            PMC_ERR_CUDA, PMC_ERR_TIMEOUT, PMC_ERR_RNG_EXHAUSTED, PMC_ERR_ASSERT};
+  return (hi[0] >= 0 && hi[0] <= 7) ? map[hi[0]] : PMC_ERR_ASSERT;
+}
+
 void step_parallel(Ctx& c, int kt) {
   // counters of this step
   for (int k = 0; k < c.n_pop; k++) {
@@ -1320,6 +1447,7 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
   r.n_live = n_part;
   write_ctr(c, pop, r);
   ph.valid_sort = false;
+  c.replay.valid = false;
   ph.n_bin = 0;
   {
     GridDev g{};
@@ -1415,11 +1543,10 @@ int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* 
     long long s = 0, k = 0;
     int status;
     if (c.mode == PMC_MODE_REPLAY) {
-      status = replay_step(c.n_pop, c.d_pops, c.stream, c.replay, c.replay_u.p, c.replay_n,
-                           &c.replay_used, kernel_type, &s, &k);
-      for (int p = 0; p < c.n_pop; p++) c.pops[p].valid_sort = true;
+      status = replay_step_host(c, &s, &k);
     } else {
       ProfScope ps(c, 3, 1);
+      c.replay.valid = false;  // the parallel step reorders and rewrites slots
       step_parallel(c, kernel_type);
       status = finish_step(c, &s, &k);
     }
@@ -1528,6 +1655,7 @@ int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx* x, const int* w_type, const double
     set_params(c, ph);
     ph.valid_sort = false;  // aero_state_set_weight clears valid_sort
   }
+  c.replay.valid = false;
   push_pops(c);
   CK(cudaStreamSynchronize(c.stream));
   return PMC_OK;
@@ -1602,9 +1730,11 @@ int pmc_coag_gpu_profile(pmc_coag_gpu_ctx* x, int enable) {
   if (!x) return PMC_ERR_INVALID_ARG;
   Ctx& c = x->c;
   GUARD_BEGIN
-  if (enable && !c.prof_ev[0]) {
-    CK(cudaEventCreate(&c.prof_ev[0]));
-    CK(cudaEventCreate(&c.prof_ev[1]));
+  if (enable && !c.prof_ev[0][0]) {
+    for (int i = 0; i < 4; i++) {
+      CK(cudaEventCreate(&c.prof_ev[i][0]));
+      CK(cudaEventCreate(&c.prof_ev[i][1]));
+    }
   }
   c.prof = enable != 0;
   for (int i = 0; i < 4; i++) {

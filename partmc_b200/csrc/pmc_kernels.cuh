@@ -41,18 +41,6 @@ enum Stream : uint32_t {
   kStreamPart = 4,
 };
 
-// Status codes shared with the C ABI.
-enum : int {
-  kOk = 0,
-  kErrArg = 1,
-  kErrOutOfGrid = 2,
-  kErrCapacity = 3,
-  kErrCuda = 4,
-  kErrTimeout = 5,
-  kErrRng = 6,
-  kErrAssert = 7,
-};
-
 __device__ __forceinline__ void set_status(PopCtr* c, int code) { atomicCAS(&c->status, 0, code); }
 
 __device__ __forceinline__ void add_ll(long long* p, long long v) {

@@ -7,7 +7,7 @@
 // the routine it restates.
 #include "pmc_replay.cuh"
 
-#include "pmc_merge.cuh"
+#include "pmc_particle.cuh"
 #include "pmc_physics.cuh"
 
 namespace pmc {

@@ -18,6 +18,18 @@
 
 namespace pmc {
 
+// Status codes shared with the C ABI.
+enum : int {
+  kOk = 0,
+  kErrArg = 1,
+  kErrOutOfGrid = 2,
+  kErrCapacity = 3,
+  kErrCuda = 4,
+  kErrTimeout = 5,
+  kErrRng = 6,
+  kErrAssert = 7,
+};
+
 // Pair-test record of one particle, stored in cell order so that a test
 // reads two records.  r: radius; rv: rad2vol(r) (for the coagulated radius
 // of coag_num_conc_factor); nc: number concentration of the particle's class
