@@ -250,6 +250,7 @@ def main():
         torch.cuda.synchronize()
         samp = 0
         ms = 0.0
+        rounds = redraws = 0
         for _ in range(k):
             flush.zero_()
             torch.cuda.synchronize()
@@ -260,6 +261,9 @@ def main():
             torch.cuda.synchronize()
             ms += e0.elapsed_time(e1)
             samp += a
+            stt = st.stats()
+            rounds += stt["rounds"]
+            redraws += stt["redraws"]
         n1 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
         prof = {}
@@ -268,6 +272,8 @@ def main():
             L.pmc_coag_gpu_profile_read(st.ctx, which, ctypes.byref(t), ctypes.byref(nl), ctypes.byref(u))
             prof[name] = (t.value, nl.value, u.value)
         L.pmc_coag_gpu_profile(st.ctx, 0)
+        prof["rounds_per_step"] = rounds / max(k, 1)
+        prof["redraws_per_step"] = redraws / max(k, 1)
         return ms, samp, n1.value - n0.value, prof
 
     clocks = ClockSampler(local)
@@ -354,7 +360,10 @@ def main():
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "avg_launch_ms": avg_ms, "launches": n_l,
                          "bytes_per_unit": bpu, "units_per_launch": units / max(n_l, 1)},
-            "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "units": v[2]} for k, v in prof.items()},
+            "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "units": v[2]} for k, v in prof.items()
+                          if isinstance(v, tuple)},
+            "rounds_per_step": prof["rounds_per_step"],
+            "redraws_per_step": prof["redraws_per_step"],
             "clocks": clk,
         }
         if cpu is not None:
