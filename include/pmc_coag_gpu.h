@@ -193,6 +193,38 @@ int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx *ctx, int kernel_type,
                              const double *vol2, const int *c2,
                              const int *c_ij, double *k_out);
 
+/* Size-bin sort that allocates nothing.  No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory on the call path,
+ * such as code being captured into a CUDA graph (where cudaMalloc is not
+ * allowed) or a host model whose device memory is all handed out up front by
+ * its own allocator.
+ *
+ * Same result as the sort inside a context (aero_sorted_sort_particles on a
+ * log grid of n_bin bins from edge_min to edge_max, bin_grid.F90:143-167):
+ *   bin_dev[i]        1-based bin of particle i (0 below the grid, n_bin+1 above)
+ *   cell_count_dev    n_bin x n_class entries, bin fastest
+ *   cell_start_dev    n_bin*n_class + 1 exclusive offsets into list_dev
+ *   list_dev          0-based particle numbers grouped by (bin, class), in
+ *                     increasing particle order inside each group
+ * from vtot_dev[i] (total particle volume, m^3) and 1-based cls_dev[i].
+ * All pointers are caller-owned device buffers; work is queued on `stream`
+ * (a cudaStream_t, NULL for the legacy default stream) and the call returns
+ * without waiting for it.
+ *
+ * Limits: n_part <= 2,097,152 and n_bin * n_class <= 1024 (n_bin <= 256);
+ * larger sizes return PMC_ERR_CAPACITY.  The scratch is one 4 MiB static
+ * device array per GPU, held until the process exits and shared by every
+ * call: calls whose work overlaps on the GPU (different streams, or other
+ * threads) race on it and must be serialised by the caller.  The first call
+ * on each device looks up that array's address and should therefore come
+ * before any stream capture. */
+int pmc_coag_gpu_bin_sort_noalloc(int n_part, const double *vtot_dev,
+                                  const int *cls_dev, int n_bin, int n_class,
+                                  double edge_min, double edge_max,
+                                  int *bin_dev, int *cell_count_dev,
+                                  int *cell_start_dev, int *list_dev,
+                                  void *stream);
+
 /* Human-readable name of a status code. */
 const char *pmc_coag_gpu_status_string(int status);
 

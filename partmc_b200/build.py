@@ -19,6 +19,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("pmc_coag.cu", []),
     ("pmc_replay.cu", ["-fmad=false"]),
+    ("pmc_noalloc.cu", []),
 ]
 HEADERS = ["pmc_physics.cuh", "pmc_state.cuh", "pmc_kernels.cuh", "pmc_merge.cuh", "pmc_particle.cuh",
            "pmc_replay.cuh"]
