@@ -251,6 +251,7 @@ def main():
         samp = 0
         ms = 0.0
         rounds = redraws = 0
+        conf = {"events": 0, "event_losers": 0, "target_ops": 0, "target_op_losers": 0}
         for _ in range(k):
             flush.zero_()
             torch.cuda.synchronize()
@@ -264,6 +265,8 @@ def main():
             stt = st.stats()
             rounds += stt["rounds"]
             redraws += stt["redraws"]
+            for kk, vv in st.conflicts().items():
+                conf[kk] += vv
         n1 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
         prof = {}
@@ -274,6 +277,7 @@ def main():
         L.pmc_coag_gpu_profile(st.ctx, 0)
         prof["rounds_per_step"] = rounds / max(k, 1)
         prof["redraws_per_step"] = redraws / max(k, 1)
+        prof["conflicts_per_step"] = {kk: vv / max(k, 1) for kk, vv in conf.items()}
         return ms, samp, n1.value - n0.value, prof
 
     clocks = ClockSampler(local)
@@ -364,6 +368,7 @@ def main():
                           if isinstance(v, tuple)},
             "rounds_per_step": prof["rounds_per_step"],
             "redraws_per_step": prof["redraws_per_step"],
+            "conflicts_per_step": prof["conflicts_per_step"],
             "clocks": clk,
         }
         if cpu is not None:

@@ -153,6 +153,14 @@ int pmc_coag_gpu_replay_used(pmc_coag_gpu_ctx *ctx, int64_t *n_used);
 int pmc_coag_gpu_stats(pmc_coag_gpu_ctx *ctx, int64_t *kmax_violations,
                        int64_t *redraws, int64_t *rounds);
 
+/* Conflicts of the last step, summed over its rounds: accepted per-set
+ * events and how many lost a claim, per-particle target operations and how
+ * many lost a claim (each loser is redone in a later round).  No counterpart
+ * in the reference, which applies events one at a time. */
+int pmc_coag_gpu_conflicts(pmc_coag_gpu_ctx *ctx, int64_t *events,
+                           int64_t *event_losers, int64_t *target_ops,
+                           int64_t *target_op_losers);
+
 /* ---- measurement ---- */
 
 /* Time, with CUDA events on the library's own stream, every launch of the

@@ -217,6 +217,12 @@ class AeroState:
               "pmc_coag_gpu_stats")
         return {"kmax_violations": a.value, "redraws": b.value, "rounds": c.value}
 
+    def conflicts(self):
+        v = [ctypes.c_int64() for _ in range(4)]
+        check(_lib.lib().pmc_coag_gpu_conflicts(self.ctx, *[ctypes.byref(x) for x in v]), "pmc_coag_gpu_conflicts")
+        return {"events": v[0].value, "event_losers": v[1].value, "target_ops": v[2].value,
+                "target_op_losers": v[3].value}
+
     def sort(self, pop=0, max_bin=256):
         n = self.n_part(pop)
         nb = ctypes.c_int()

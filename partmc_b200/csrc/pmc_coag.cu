@@ -31,8 +31,17 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
+// the element count is n, or *nd when nd is given (a count that only the
+// device knows; n is then its upper bound)
+__device__ __forceinline__ long long scan_n(long long n, const long long* nd) {
+  if (!nd) return n;
+  long long m = *nd;
+  return m < n ? m : n;
+}
+
 template <class T>
-__global__ void k_scan_reduce(const T* in, long long n, long long* bsum) {
+__global__ void k_scan_reduce(const T* in, long long n_max, const long long* nd, long long* bsum) {
+  long long n = scan_n(n_max, nd);
   long long base = (long long)blockIdx.x * kScanTile;
   long long s = 0;
   for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
@@ -76,8 +85,10 @@ __device__ long long block_excl_scan_ll(long long v, long long* total) {
   return pre;
 }
 
-// exclusive scan of the block sums, in place (single block, any count)
-__global__ void k_scan_bsum(long long* bsum, int nb, long long* out_total) {
+// exclusive scan of the block sums, in place (single block, any count);
+// the total goes to out[n]
+__global__ void k_scan_bsum(long long* bsum, int nb, long long* out, long long n_max, const long long* nd) {
+  long long* out_total = out + scan_n(n_max, nd);
   long long carry = 0;
   for (int base = 0; base < nb; base += blockDim.x) {
     int i = base + threadIdx.x;
@@ -91,7 +102,9 @@ __global__ void k_scan_bsum(long long* bsum, int nb, long long* out_total) {
 }
 
 template <class T>
-__global__ void k_scan_final(const T* in, long long n, const long long* bsum, long long* out) {
+__global__ void k_scan_final(const T* in, long long n_max, const long long* nd, const long long* bsum,
+                             long long* out) {
+  long long n = scan_n(n_max, nd);
   long long base = (long long)blockIdx.x * kScanTile;
   long long v[kScanItems];
   long long s = 0;
@@ -241,6 +254,7 @@ __global__ void k_upload(PopDev P, int n, const double* vol_pm, const int* grp, 
     P.hyst[i] = 0;
     P.frozen[i] = 0;
     P.alive[i] = 1;
+    P.bin[i] = -1;  // set by the first refresh after the grid decision
   }
 }
 
@@ -293,6 +307,8 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.alive[j] = S.alive[i];
     D.bin[j] = S.bin[i];
     D.claim[j] = S.claim[i];
+    D.recd[j] = S.recd[i];
+    D.recf[j] = S.recf[i];
   }
 }
 
@@ -421,12 +437,18 @@ struct PopHost {
   uint32_t step = 0;
   int kmax_kt = 0;  // kernel type of the current k_max table
   int chunk_hist_cap = 0;
+  // per-slot radius/bin/record caches are valid for this grid, kernel,
+  // environment and weights
+  bool caches_valid = false;
+  int key_kt = 0, key_wver = -1;
+  double key_temp = 0, key_press = 0, key_coeff = 0;
 };
 
 struct Ctx {
   int n_pop = 1, n_spec = 1, n_group = 1, n_class = 1, i_water = 0;
   std::vector<double> density;
   Weights w{};
+  int wver = 0;  // bumped on every weight change
   int mode = PMC_MODE_FP64;
   std::vector<PopHost> pops;
   PopDev* d_pops = nullptr;
@@ -456,11 +478,24 @@ struct Ctx {
   long long h_total = 0;
   // stats of the last step
   long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
+  long long last_set_losers = 0, last_pp_lost = 0, last_events = 0, last_ops = 0;
   // optional per-kernel timing with CUDA events on the library's stream:
   // 0 pair tests, 1 sort scatter + record build, 2 sort histogram,
   // 3 whole steps
   bool prof = false;
-  cudaEvent_t prof_ev[4][2] = {};
+  struct ProfPair {
+    int id;
+    long long units;
+    cudaEvent_t e0, e1;
+  };
+  std::vector<ProfPair> prof_pending;
+  std::vector<cudaEvent_t> prof_free;
+  // host copy of each population's slot count, kept current after every
+  // round so the sort can size itself without reading the device
+  std::vector<int> n_slots_host;
+  // device scalars of a round: [0] per-set losers; [1..3] spare
+  DevBuf<long long> round_dev;
+  std::vector<long long> base_cached;  // pair-list layout last uploaded
   double prof_ms[4] = {0, 0, 0, 0};
   long long prof_launch[4] = {0, 0, 0, 0}, prof_units[4] = {0, 0, 0, 0};
   // replay
@@ -489,35 +524,68 @@ int grid_for(long long n, int threads) {
   return (int)b;
 }
 
-// times the launches issued inside its scope when profiling is on
+// Times the launches issued inside its scope when profiling is on: a pair
+// of CUDA events on the library's stream, read back only when the totals
+// are asked for, so timing adds no synchronisation to the step.
 struct ProfScope {
   Ctx& c;
   int id;
   long long units;
+  cudaEvent_t e0 = nullptr;
   ProfScope(Ctx& c_, int id_, long long units_) : c(c_), id(id_), units(units_) {
-    if (c.prof) cudaEventRecord(c.prof_ev[id][0], c.stream);
+    if (!c.prof) return;
+    e0 = prof_event(c);
+    cudaEventRecord(e0, c.stream);
   }
   ~ProfScope() {
-    if (!c.prof) return;
-    cudaEventRecord(c.prof_ev[id][1], c.stream);
-    cudaEventSynchronize(c.prof_ev[id][1]);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, c.prof_ev[id][0], c.prof_ev[id][1]);
-    c.prof_ms[id] += ms;
-    c.prof_launch[id] += 1;
-    c.prof_units[id] += units;
+    if (!c.prof || !e0) return;
+    cudaEvent_t e1 = prof_event(c);
+    cudaEventRecord(e1, c.stream);
+    c.prof_pending.push_back({id, units, e0, e1});
+  }
+  static cudaEvent_t prof_event(Ctx& c) {
+    if (!c.prof_free.empty()) {
+      cudaEvent_t e = c.prof_free.back();
+      c.prof_free.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
   }
 };
 
+// fold the recorded event pairs into the per-kernel totals
+void prof_collect(Ctx& c) {
+  if (c.prof_pending.empty()) return;
+  cudaStreamSynchronize(c.stream);
+  for (auto& p : c.prof_pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.e0, p.e1);
+    c.prof_ms[p.id] += ms;
+    c.prof_launch[p.id] += 1;
+    c.prof_units[p.id] += p.units;
+    c.prof_free.push_back(p.e0);
+    c.prof_free.push_back(p.e1);
+  }
+  c.prof_pending.clear();
+}
+
+// exclusive scan of in[0..n) into out[0..n] (out[n] = total).  With nd, the
+// count is *nd (device memory) and n only bounds it.
 template <class T>
-long long scan(Ctx& c, const T* in, long long n, long long* out, bool read_total) {
+void scan_dev(Ctx& c, const T* in, long long n, const long long* nd, long long* out) {
   int nb = (int)((n + kScanTile - 1) / kScanTile);
   if (nb < 1) nb = 1;
   c.scan_bsum.reserve(nb + 1);
-  c.scan_total.reserve(2);
-  k_scan_reduce<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_bsum.p); note_launch();
-  k_scan_bsum<<<1, kScanThreads, 0, c.stream>>>(c.scan_bsum.p, nb, out + n); note_launch();
-  k_scan_final<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, c.scan_bsum.p, out); note_launch();
+  k_scan_reduce<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, nd, c.scan_bsum.p); note_launch();
+  k_scan_bsum<<<1, kScanThreads, 0, c.stream>>>(c.scan_bsum.p, nb, out, n, nd); note_launch();
+  k_scan_final<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, nd, c.scan_bsum.p, out); note_launch();
+}
+
+template <class T>
+long long scan(Ctx& c, const T* in, long long n, long long* out, bool read_total) {
+  scan_dev(c, in, n, (const long long*)nullptr, out);
   if (!read_total) return -1;
   long long t = 0;
   CK(cudaMemcpyAsync(&t, out + n, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
@@ -728,20 +796,53 @@ __global__ void k_radius_minmax_masked(const PopDev* pops, const uint8_t* on) {
   if (!on[blockIdx.y]) return;
   const PopDev& P = pops[blockIdx.y];
   int n = P.ctr->n_slots;
+  // positive doubles order like their bit patterns: reduce the bits in the
+  // block, then one atomic per block
+  unsigned long long lo = ~0ULL, hi = 0ULL;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (!P.alive[i]) continue;
-    double r = vol2rad(P.vtot[i]);
-    unsigned long long b = (unsigned long long)__double_as_longlong(r);
-    atomicMin(&P.ctr->rmin_bits, b);
-    atomicMax(&P.ctr->rmax_bits, b);
+    unsigned long long b = (unsigned long long)__double_as_longlong(vol2rad(P.vtot[i]));
+    lo = b < lo ? b : lo;
+    hi = b > hi ? b : hi;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long l2 = __shfl_down_sync(0xffffffffu, lo, o);
+    unsigned long long h2 = __shfl_down_sync(0xffffffffu, hi, o);
+    lo = l2 < lo ? l2 : lo;
+    hi = h2 > hi ? h2 : hi;
+  }
+  __shared__ unsigned long long slo[32], shi[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    slo[wid] = lo;
+    shi[wid] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+      lo = slo[k] < lo ? slo[k] : lo;
+      hi = shi[k] > hi ? shi[k] : hi;
+    }
+    if (hi > 0ULL) {
+      atomicMin(&P.ctr->rmin_bits, lo);
+      atomicMax(&P.ctr->rmax_bits, hi);
+    }
   }
 }
 
+__global__ void k_reset_ranges(PopCtr* ctrs, int n_pop) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pop) return;
+  ctrs[k].bmin = 1 << 30;
+  ctrs[k].bmax = -1;
+  ctrs[k].out_of_grid = 0;
+}
+
+// chunk counts from the host's copy of the slot counts
 void prepare_chunks(Ctx& c) {
-  std::vector<PopCtr>& r = read_ctrs(c);
   for (int k = 0; k < c.n_pop; k++) {
     PopHost& ph = c.pops[k];
-    ph.h.n_chunks = (r[k].n_slots + kChunk - 1) / kChunk;
+    ph.h.n_chunks = (c.n_slots_host[k] + kChunk - 1) / kChunk;
     int need = std::max(ph.h.n_chunks, 1) * ph.h.n_cells;
     if (need > ph.chunk_hist_cap) {
       int want = std::max(need, 1024);
@@ -754,13 +855,8 @@ void prepare_chunks(Ctx& c) {
 // histogram + scan of every population with its current grid
 void run_hist_scan(Ctx& c) {
   prepare_chunks(c);
-  std::vector<PopCtr>& r = read_ctrs(c);
-  for (int k = 0; k < c.n_pop; k++) {
-    r[k].bmin = 1 << 30;
-    r[k].bmax = -1;
-    r[k].out_of_grid = 0;
-  }
-  write_ctrs(c);
+  k_reset_ranges<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_ctrs, c.n_pop);
+  note_launch();
   push_pops(c);
   int max_chunks = 1, max_cells = 1;
   for (int k = 0; k < c.n_pop; k++) {
@@ -770,19 +866,66 @@ void run_hist_scan(Ctx& c) {
   dim3 g(max_chunks, c.n_pop);
   {
     long long units = 0;
-    for (int k = 0; k < c.n_pop; k++) units += (long long)r[k].n_slots;
+    for (int k = 0; k < c.n_pop; k++) units += (long long)c.n_slots_host[k];
     ProfScope ps(c, 2, units);
     k_sort_hist<<<g, kSortThreads, sizeof(int) * max_cells, c.stream>>>(c.d_pops); note_launch();
   }
-  k_sort_scan<<<c.n_pop, 1024, 0, c.stream>>>(c.d_pops); note_launch();
+  {
+    dim3 gc(max_cells, c.n_pop);
+    k_sort_count<<<gc, 256, 0, c.stream>>>(c.d_pops);
+    note_launch();
+    k_sort_offsets<<<gc, 256, 0, c.stream>>>(c.d_pops);
+    note_launch();
+  }
+}
+
+bool caches_current(const Ctx& c, const PopHost& ph) {
+  return ph.caches_valid && ph.key_kt == ph.h.kernel_type && ph.key_temp == ph.h.temp &&
+         ph.key_press == ph.h.pressure && ph.key_coeff == ph.h.coeff && ph.key_wver == c.wver;
+}
+
+// recompute radius, bin and records of every live slot of the marked
+// populations (after a grid, environment, kernel or weight change)
+void refresh_caches(Ctx& c, const std::vector<uint8_t>& on) {
+  bool any = false;
+  int max_slots = 1;
+  std::vector<PopCtr>& r = read_ctrs(c);
+  for (int k = 0; k < c.n_pop; k++)
+    if (on[k]) {
+      any = true;
+      max_slots = std::max(max_slots, r[k].n_slots);
+    }
+  if (!any) return;
+  push_pops(c);
+  DevBuf<uint8_t> don;
+  don.reserve(c.n_pop);
+  CK(cudaMemcpyAsync(don.p, on.data(), c.n_pop, cudaMemcpyHostToDevice, c.stream));
+  dim3 g(grid_for(max_slots, 256), c.n_pop);
+  k_refresh_all<<<g, 256, 0, c.stream>>>(c.d_pops, don.p);
+  note_launch();
+  CK(cudaStreamSynchronize(c.stream));
+  don.release();
+  for (int k = 0; k < c.n_pop; k++)
+    if (on[k]) {
+      PopHost& ph = c.pops[k];
+      ph.caches_valid = true;
+      ph.key_kt = ph.h.kernel_type;
+      ph.key_temp = ph.h.temp;
+      ph.key_press = ph.h.pressure;
+      ph.key_coeff = ph.h.coeff;
+      ph.key_wver = c.wver;
+    }
 }
 
 // aero_state_sort: grid decision (remake_if_needed) then the sort itself
 void sort_pops(Ctx& c, bool decide_grid) {
   bool hist_current = false;
   if (decide_grid) {
+    std::vector<PopCtr>& r0 = read_ctrs(c);
+    c.n_slots_host.resize(c.n_pop);
+    for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] = r0[k].n_slots;
     // radius range of populations without a valid sort
-    std::vector<uint8_t> on(c.n_pop, 0);
+    std::vector<uint8_t> on(c.n_pop, 0), fresh(c.n_pop, 0);
     bool any = false;
     std::vector<PopCtr>& r = read_ctrs(c);
     int max_slots = 1;
@@ -793,6 +936,8 @@ void sort_pops(Ctx& c, bool decide_grid) {
         r[k].rmin_bits = 0x7ff0000000000000ULL;
         r[k].rmax_bits = 0;
         max_slots = std::max(max_slots, r[k].n_slots);
+      } else if (!caches_current(c, c.pops[k])) {
+        fresh[k] = 1;  // current grid, stale caches
       }
     }
     if (any) {
@@ -801,14 +946,17 @@ void sort_pops(Ctx& c, bool decide_grid) {
       don.reserve(c.n_pop);
       CK(cudaMemcpyAsync(don.p, on.data(), c.n_pop, cudaMemcpyHostToDevice, c.stream));
       dim3 g(grid_for(max_slots, 256), c.n_pop);
-      k_radius_minmax_masked<<<g, 256, 0, c.stream>>>(c.d_pops, don.p); note_launch();
+      k_radius_minmax_masked<<<g, 256, 0, c.stream>>>(c.d_pops, don.p);
+      note_launch();
       CK(cudaStreamSynchronize(c.stream));
       don.release();
     }
-    // occupied bin range of the others
+    refresh_caches(c, fresh);
+    // occupied bin range of the populations with a valid sort
     run_hist_scan(c);
     hist_current = true;
     std::vector<PopCtr>& q = read_ctrs(c);
+    std::vector<uint8_t> regrid(c.n_pop, 0);
     for (int k = 0; k < c.n_pop; k++) {
       PopHost& ph = c.pops[k];
       double rmin = 0.0, rmax = 0.0;
@@ -828,10 +976,7 @@ void sort_pops(Ctx& c, bool decide_grid) {
       }
       bool need = false;
       if (rmax == 0.0) {
-        if (!ph.valid_sort && ph.n_bin != 0) {
-          make_grid(c, ph, 0, 0.0, 0.0);
-          hist_current = false;
-        }
+        if (!ph.valid_sort && ph.n_bin != 0) make_grid(c, ph, 0, 0.0, 0.0);
       } else if (ph.n_bin < 1) {
         need = true;
       } else {
@@ -843,13 +988,16 @@ void sort_pops(Ctx& c, bool decide_grid) {
         int n_bin = (int)ceil((log10(gmax) - log10(gmin)) * 10.0);
         if (n_bin > kMaxBin) throw Fail(PMC_ERR_CAPACITY);
         make_grid(c, ph, n_bin, gmin, gmax);
+      }
+      // a new grid or a population without a valid sort: all bins change
+      if (need || !ph.valid_sort) {
+        regrid[k] = 1;
+        ph.caches_valid = false;
         hist_current = false;
       }
-      // a population uploaded without a sort is sorted now even when its
-      // grid is kept
-      if (!ph.valid_sort) hist_current = hist_current && true;
       ph.valid_sort = true;
     }
+    refresh_caches(c, regrid);
   }
   if (!hist_current) run_hist_scan(c);
   int max_chunks = 1, max_cells = 1;
@@ -858,14 +1006,10 @@ void sort_pops(Ctx& c, bool decide_grid) {
     max_cells = std::max(max_cells, c.pops[k].h.n_cells);
   }
   dim3 g(max_chunks, c.n_pop);
-  int prec = c.mode == PMC_MODE_MIXED ? 1 : 0;
   long long units = 0;
-  if (c.prof) {
-    std::vector<PopCtr>& r = read_ctrs(c);
-    for (int k = 0; k < c.n_pop; k++) units += (long long)r[k].n_slots;
-  }
+  for (int k = 0; k < c.n_pop; k++) units += (long long)c.n_slots_host[k];
   ProfScope ps(c, 1, units);
-  k_sort_scatter<<<g, kSortThreads, sizeof(int) * kSortWarps * max_cells, c.stream>>>(c.d_pops, prec); note_launch();
+  k_sort_scatter<<<g, kSortThreads, sizeof(int) * kSortWarps * max_cells, c.stream>>>(c.d_pops); note_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -1055,26 +1199,47 @@ int replay_step_host(Ctx& c, long long* s_out, long long* k_out) {
   r.tot_coag = hv[2];
   write_ctr(c, 0, r);
   rb.valid = hi[0] == 0;
+  ph.caches_valid = false;  // the replay rewrote slots without the caches
   static const int map[] = {PMC_OK, PMC_ERR_INVALID_ARG, PMC_ERR_OUT_OF_GRID, PMC_ERR_CAPACITY,
                             PMC_ERR_CUDA, PMC_ERR_TIMEOUT, PMC_ERR_RNG_EXHAUSTED, PMC_ERR_ASSERT};
   return (hi[0] >= 0 && hi[0] <= 7) ? map[hi[0]] : PMC_ERR_ASSERT;
 }
 
+__global__ void k_step_reset(PopCtr* ctrs, int n_pop) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pop) return;
+  ctrs[k].tot_samp = ctrs[k].tot_coag = ctrs[k].kmax_warn = ctrs[k].redraws = 0;
+  ctrs[k].status = 0;
+}
+
+__global__ void k_fill_claims(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  int n = P.ctr->n_slots;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    P.claim[i] = 0xffffffffu;
+}
+
+// per-population work of a round: samples and target operations
+__global__ void k_pop_work(const long long* pop_pair_base, int n_pop, const long long* work_off,
+                           const long long* pp_off, long long* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_pop) return;
+  long long a = pop_pair_base[k], b = pop_pair_base[k + 1];
+  out[2 * k] = work_off[b] - work_off[a];
+  out[2 * k + 1] = pp_off[b] - pp_off[a];
+}
+
 void step_parallel(Ctx& c, int kt) {
-  // counters of this step
-  for (int k = 0; k < c.n_pop; k++) {
-    PopCtr r = read_ctr(c, k);
-    r.tot_samp = r.tot_coag = r.kmax_warn = r.redraws = 0;
-    r.status = 0;
-    write_ctr(c, k, r);
-  }
+  k_step_reset<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_ctrs, c.n_pop);
+  note_launch();
   push_pops(c);
   sort_pops(c, true);
-  // global pair list
+  // global pair list, uploaded when its layout changes
   std::vector<long long> base(c.n_pop + 1, 0);
   for (int k = 0; k < c.n_pop; k++) base[k + 1] = base[k] + c.pops[k].h.n_pairs;
   int n_gpairs = (int)base[c.n_pop];
-  {
+  size_t ng = (size_t)n_gpairs + 1;
+  if (base != c.base_cached) {
     std::vector<int> gp_pop(std::max(n_gpairs, 1)), gp_loc(std::max(n_gpairs, 1));
     for (int k = 0; k < c.n_pop; k++)
       for (int p = 0; p < c.pops[k].h.n_pairs; p++) {
@@ -1088,8 +1253,8 @@ void step_parallel(Ctx& c, int kt) {
     CK(cudaMemcpyAsync(c.gpair_local.p, gp_loc.data(), sizeof(int) * gp_loc.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(c.pop_pair_base.p, base.data(), sizeof(long long) * base.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    c.base_cached = base;
   }
-  size_t ng = (size_t)n_gpairs + 1;
   c.nwork_set.reserve(ng);
   c.nwork_pp.reserve(ng);
   c.nprio.reserve(ng);
@@ -1102,164 +1267,192 @@ void step_parallel(Ctx& c, int kt) {
   c.slot_base_pp.reserve(c.n_pop);
   c.id_base_set.reserve(c.n_pop);
   c.id_base_pp.reserve(c.n_pop);
-  c.n_dev.reserve(4);
-  int max_pairs = 1;
-  for (int k = 0; k < c.n_pop; k++) max_pairs = std::max(max_pairs, c.pops[k].h.n_pairs);
-  int nb_max = 1;
-  for (int k = 0; k < c.n_pop; k++) nb_max = std::max(nb_max, c.pops[k].n_bin);
+  c.n_dev.reserve(4 + 2 * (size_t)c.n_pop);
+  c.round_dev.reserve(4);
+  int max_pairs = 1, nb_max = 1, max_cap = 1;
+  for (int k = 0; k < c.n_pop; k++) {
+    max_pairs = std::max(max_pairs, c.pops[k].h.n_pairs);
+    nb_max = std::max(nb_max, c.pops[k].n_bin);
+    max_cap = std::max(max_cap, c.pops[k].h.cap);
+  }
   bool flat = weights_flat(c.w);
   float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
-  long long redraws = 0;
-  long long Qprev = 0;
+  long long redraws = 0, Qprev = 0;
+  c.last_set_losers = c.last_pp_lost = c.last_events = c.last_ops = 0;
+  std::vector<long long> hw(3 + 2 * (size_t)c.n_pop);
+  std::vector<int> per_pop(4 * (size_t)c.n_pop);
   int round = 0;
   for (;;) {
     for (int k = 0; k < c.n_pop; k++) c.pops[k].h.round = (uint32_t)round;
     push_pops(c);
     if (round > 0) sort_pops(c, false);
-    {
+    if (round == 0) {
       dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
-      if (round == 0) {
-        k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
-        note_launch();
-      }
+      k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
+      note_launch();
+    }
+    {
       dim3 gp((max_pairs + 127) / 128, c.n_pop);
-      k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p,
-                                        c.nprio.p, c.pair_losers.p, 1, inflate); note_launch();
+      k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, c.nprio.p,
+                                        c.pair_losers.p, 1, inflate);
+      note_launch();
     }
     if (round == 0) {
       for (int k = 0; k < c.n_pop; k++) c.pops[k].h.kmax_valid = 1;
       push_pops(c);
     }
-    long long W = scan(c, c.nwork_set.p, n_gpairs, c.work_off.p, true);
-    long long Q0 = scan(c, c.nwork_pp.p, n_gpairs, c.pp_off.p, true);
-    long long Ptot = scan(c, c.nprio.p, n_gpairs, c.prio_off.p, true);
+    scan_dev(c, c.nwork_set.p, n_gpairs, nullptr, c.work_off.p);
+    scan_dev(c, c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p);
+    scan_dev(c, c.nprio.p, n_gpairs, nullptr, c.prio_off.p);
+    long long* popw = c.n_dev.p + 4;
+    k_pop_work<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.pop_pair_base.p, c.n_pop, c.work_off.p, c.pp_off.p,
+                                                            popw);
+    note_launch();
+    // one read-back: totals and per-population work
+    CK(cudaMemcpyAsync(&hw[0], c.work_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&hw[1], c.pp_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&hw[2], c.prio_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&hw[3], popw, sizeof(long long) * 2 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    long long W = hw[0], Q0 = hw[1], Ptot = hw[2];
     long long Q = round == 0 ? Q0 : Qprev;
-    if (Ptot + Q + 1 >= 0xffffffffLL) throw Fail(PMC_ERR_CAPACITY);
-    // buffers
+    if (Ptot + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
+    // capacity for the worst case of this round: every sample creates a
+    // particle and every target operation makes kMaxCopies - 1 copies
+    for (int k = 0; k < c.n_pop; k++) {
+      long long qk = round == 0 ? hw[3 + 2 * k + 1] : Q;
+      long long need = (long long)c.n_slots_host[k] + hw[3 + 2 * k] + (kMaxCopies - 1) * qk;
+      if (need > c.pops[k].h.cap) {
+        int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
+        relayout(c, k, nc, false);  // slot numbers kept
+      }
+    }
     c.flag.reserve((size_t)W + 1);
     c.ev.reserve((size_t)W + 1);
-    c.flag_off.reserve((size_t)W + 1);
-    // reset claims and per-pair losers
-    for (int k = 0; k < c.n_pop; k++) {
-      PopHost& ph = c.pops[k];
-      k_fill_u32<<<grid_for(ph.h.cap, 256), 256, 0, c.stream>>>(ph.h.claim, ph.h.cap, 0xffffffffu); note_launch();
+    c.flag_off.reserve((size_t)W + 2);
+    c.ev_w.reserve((size_t)W + 1);
+    c.need_slot_set.reserve(W + 1);
+    c.need_id_set.reserve(W + 1);
+    c.win_set.reserve(W + 1);
+    c.rank_slot_set.reserve(W + 2);
+    c.rank_id_set.reserve(W + 2);
+    c.need_slot_pp.reserve(Q + 1);
+    c.need_id_pp.reserve(Q + 1);
+    c.win_pp.reserve(Q + 1);
+    c.lost_pp.reserve(Q + 1);
+    c.lost_off.reserve(Q + 2);
+    c.rank_slot_pp.reserve(Q + 2);
+    c.rank_id_pp.reserve(Q + 2);
+    {
+      dim3 g(grid_for(max_cap, 256), c.n_pop);
+      k_fill_claims<<<g, 256, 0, c.stream>>>(c.d_pops);
+      note_launch();
     }
     CK(cudaMemsetAsync(c.pair_losers.p, 0, sizeof(int) * ng, c.stream));
+    CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 4, c.stream));
+    CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
     if (W > 0) {
       ProfScope ps(c, 0, W);
       launch_test_kt(c, kt, flat, n_gpairs);
     }
-    // target operations of the per-particle path
     if (Q > 0) {
       if (round == 0) {
         c.op_pop.reserve(Q); c.op_pair.reserve(Q); c.op_slot.reserve(Q); c.op_k.reserve(Q); c.op_prio.reserve(Q);
         k_build_ops<<<n_gpairs, 128, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pp_off.p,
                                                     c.prio_off.p, n_gpairs, c.op_pop.p, c.op_pair.p,
-                                                    c.op_slot.p, c.op_k.p, c.op_prio.p); note_launch();
+                                                    c.op_slot.p, c.op_k.p, c.op_prio.p);
+        note_launch();
       }
       c.pp_res.reserve(Q);
       c.pp_vol.reserve((size_t)Q * c.n_spec);
       set_n_dev(c, Q);
       launch_pp(c, kt, Q);
     }
-    // events of the per-set tests, in sample order
-    long long E = 0;
+    // accepted per-set samples in sample order; their count E stays on the
+    // device (flag_off[W])
+    const long long* Ed = c.flag_off.p + W;
     if (W > 0) {
-      E = scan(c, c.flag.p, W, c.flag_off.p, true);
-      c.ev_w.reserve((size_t)E + 1);
-      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, W, c.ev_w.p); note_launch();
-    }
-    c.need_slot_set.reserve(E + 1); c.need_id_set.reserve(E + 1); c.win_set.reserve(E + 1);
-    c.rank_slot_set.reserve(E + 2); c.rank_id_set.reserve(E + 2);
-    c.need_slot_pp.reserve(Q + 1); c.need_id_pp.reserve(Q + 1); c.win_pp.reserve(Q + 1);
-    c.lost_pp.reserve(Q + 1); c.lost_off.reserve(Q + 2);
-    c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
-    CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
-    if (E > 0) {
-      set_n_dev(c, E);
-      k_resolve_set<<<grid_for(E, 256), 256, 0, c.stream>>>(
-          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
-          c.n_dev.p, c.ev_w.p, c.ev.p, c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p,
-          c.win_set.p); note_launch();
-      scan(c, c.need_slot_set.p, E, c.rank_slot_set.p, false);
-      scan(c, c.need_id_set.p, E, c.rank_id_set.p, false);
-      k_count_per_pop<<<grid_for(E, 256), 256, 0, c.stream>>>(c.need_slot_set.p, c.n_dev.p, nullptr, c.ev_w.p, c.work_off.p, n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 0 * c.n_pop); note_launch();
-      k_count_per_pop<<<grid_for(E, 256), 256, 0, c.stream>>>(c.need_id_set.p, c.n_dev.p, nullptr, c.ev_w.p, c.work_off.p, n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 1 * c.n_pop); note_launch();
+      scan_dev(c, c.flag.p, W, nullptr, c.flag_off.p);
+      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, W, c.ev_w.p);
+      note_launch();
+      k_resolve_set<<<grid_for(W, 256), 256, 0, c.stream>>>(
+          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs, Ed, c.ev_w.p, c.ev.p,
+          c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.round_dev.p);
+      note_launch();
+      scan_dev(c, c.need_slot_set.p, W, Ed, c.rank_slot_set.p);
+      scan_dev(c, c.need_id_set.p, W, Ed, c.rank_id_set.p);
+      k_count_per_pop<<<grid_for(W, 256), 256, 0, c.stream>>>(c.need_slot_set.p, Ed, nullptr, c.ev_w.p, c.work_off.p,
+                                                             n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 0 * c.n_pop);
+      note_launch();
+      k_count_per_pop<<<grid_for(W, 256), 256, 0, c.stream>>>(c.need_id_set.p, Ed, nullptr, c.ev_w.p, c.work_off.p,
+                                                             n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 1 * c.n_pop);
+      note_launch();
     }
     if (Q > 0) {
       set_n_dev(c, Q);
-      k_pp_resolve<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_prio.p, c.n_dev.p,
-                                                           c.pp_res.p, c.win_pp.p, c.need_slot_pp.p,
-                                                           c.need_id_pp.p, c.lost_pp.p); note_launch();
-      scan(c, c.need_slot_pp.p, Q, c.rank_slot_pp.p, false);
-      scan(c, c.need_id_pp.p, Q, c.rank_id_pp.p, false);
-      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p, nullptr, nullptr, 0, nullptr, c.per_pop_i.p + 2 * c.n_pop); note_launch();
-      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p, nullptr, nullptr, 0, nullptr, c.per_pop_i.p + 3 * c.n_pop); note_launch();
+      k_pp_resolve<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_prio.p, c.n_dev.p, c.pp_res.p,
+                                                           c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
+      note_launch();
+      scan_dev(c, c.need_slot_pp.p, Q, nullptr, c.rank_slot_pp.p);
+      scan_dev(c, c.need_id_pp.p, Q, nullptr, c.rank_id_pp.p);
+      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p, nullptr,
+                                                             nullptr, 0, nullptr, c.per_pop_i.p + 2 * c.n_pop);
+      note_launch();
+      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p, nullptr, nullptr,
+                                                             0, nullptr, c.per_pop_i.p + 3 * c.n_pop);
+      note_launch();
     }
-    // capacity for the new slots
-    {
-      std::vector<int> pp(4 * c.n_pop);
-      CK(cudaMemcpyAsync(pp.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaStreamSynchronize(c.stream));
-      for (int k = 0; k < c.n_pop; k++) {
-        PopCtr r = read_ctr(c, k);
-        long long need = (long long)r.n_slots + pp[0 * c.n_pop + k] + pp[2 * c.n_pop + k];
-        if (need > c.pops[k].h.cap) {
-          // grow keeping slot numbers (the round's claims refer to them)
-          int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
-          relayout(c, k, nc, false);
-        }
-      }
-    }
-    k_alloc_bases<<<1, 1, 0, c.stream>>>(c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop,
-                                         c.per_pop_i.p + 1 * c.n_pop, c.per_pop_i.p + 2 * c.n_pop,
-                                         c.per_pop_i.p + 3 * c.n_pop, c.slot_base_set.p,
-                                         c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p); note_launch();
-    if (E > 0) {
-      set_n_dev(c, E);
-      k_apply_set<<<grid_for(E, 256), 256, 0, c.stream>>>(
-          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs, c.n_dev.p, c.ev_w.p,
-          c.ev.p, c.win_set.p, c.rank_slot_set.p, c.rank_id_set.p, c.slot_base_set.p,
-          c.id_base_set.p); note_launch();
+    k_alloc_bases<<<1, 1, 0, c.stream>>>(c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop, c.per_pop_i.p + 1 * c.n_pop,
+                                         c.per_pop_i.p + 2 * c.n_pop, c.per_pop_i.p + 3 * c.n_pop, c.slot_base_set.p,
+                                         c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p);
+    note_launch();
+    if (W > 0) {
+      k_apply_set<<<grid_for(W, 256), 256, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p,
+                                                          n_gpairs, Ed, c.ev_w.p, c.ev.p, c.win_set.p,
+                                                          c.rank_slot_set.p, c.rank_id_set.p, c.slot_base_set.p,
+                                                          c.id_base_set.p);
+      note_launch();
     }
     if (Q > 0) {
-      set_n_dev(c, Q);
-      k_pp_apply<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p,
-                                                         c.pp_vol.p, c.win_pp.p, c.rank_slot_pp.p,
-                                                         c.rank_id_pp.p, c.slot_base_pp.p,
-                                                         c.id_base_pp.p); note_launch();
+      k_pp_apply<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
+                                                         c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p,
+                                                         c.slot_base_pp.p, c.id_base_pp.p);
+      note_launch();
+      scan_dev(c, c.lost_pp.p, Q, nullptr, c.lost_off.p);
     }
-    k_alloc_finish<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(
-        c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop, c.per_pop_i.p + 1 * c.n_pop,
-        c.per_pop_i.p + 2 * c.n_pop, c.per_pop_i.p + 3 * c.n_pop); note_launch();
-    // losers
-    long long set_losers = 0;
-    if (E > 0) {
-      long long nw = 0;
-      std::vector<int> pl(ng);
-      CK(cudaMemcpyAsync(pl.data(), c.pair_losers.p, sizeof(int) * ng, cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaStreamSynchronize(c.stream));
-      for (size_t i = 0; i < (size_t)n_gpairs; i++) nw += pl[i];
-      set_losers = nw;
-    }
-    long long pp_lost = 0;
-    if (Q > 0) pp_lost = scan(c, c.lost_pp.p, Q, c.lost_off.p, true);
+    k_alloc_finish<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop,
+                                                                c.per_pop_i.p + 1 * c.n_pop, c.per_pop_i.p + 2 * c.n_pop,
+                                                                c.per_pop_i.p + 3 * c.n_pop);
+    note_launch();
+    // one read-back at the end of the round
+    long long set_losers = 0, pp_lost = 0, E = 0;
+    CK(cudaMemcpyAsync(&set_losers, c.round_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    if (W > 0) CK(cudaMemcpyAsync(&E, Ed, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    if (Q > 0) CK(cudaMemcpyAsync(&pp_lost, c.lost_off.p + Q, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] += per_pop[0 * c.n_pop + k] + per_pop[2 * c.n_pop + k];
     redraws += set_losers + pp_lost;
+    c.last_set_losers += set_losers;
+    c.last_pp_lost += pp_lost;
+    c.last_events += E;
+    c.last_ops += Q;
     round++;
     if (set_losers + pp_lost == 0) break;
     if (round >= c.max_rounds) {
-      for (int k = 0; k < c.n_pop; k++) {
-        PopCtr r = read_ctr(c, k);
-        if (r.status == 0) r.status = PMC_ERR_TIMEOUT;
-        write_ctr(c, k, r);
-      }
+      std::vector<PopCtr>& r = read_ctrs(c);
+      for (int k = 0; k < c.n_pop; k++)
+        if (r[k].status == 0) r[k].status = PMC_ERR_TIMEOUT;
+      write_ctrs(c);
       break;
     }
-    // redo list of lost target operations
     if (pp_lost > 0) {
-      c.r_pop.reserve(pp_lost); c.r_pair.reserve(pp_lost); c.r_slot.reserve(pp_lost); c.r_k.reserve(pp_lost); c.r_prio.reserve(pp_lost);
-      k_build_redo<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.lost_pp.p, c.lost_off.p, Q,
-                                                           c.r_pop.p, c.r_pair.p, c.r_slot.p, c.r_k.p, c.r_prio.p, 0x80000000u); note_launch();
+      c.r_pop.reserve(pp_lost); c.r_pair.reserve(pp_lost); c.r_slot.reserve(pp_lost); c.r_k.reserve(pp_lost);
+      c.r_prio.reserve(pp_lost);
+      k_build_redo<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.lost_pp.p,
+                                                           c.lost_off.p, Q, c.r_pop.p, c.r_pair.p, c.r_slot.p, c.r_k.p,
+                                                           c.r_prio.p, 0x40000000u);
+      note_launch();
       std::swap(c.op_pop, c.r_pop); std::swap(c.op_pair, c.r_pair); std::swap(c.op_slot, c.r_slot);
       std::swap(c.op_k, c.r_k); std::swap(c.op_prio, c.r_prio);
     }
@@ -1447,6 +1640,7 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
   r.n_live = n_part;
   write_ctr(c, pop, r);
   ph.valid_sort = false;
+  ph.caches_valid = false;
   c.replay.valid = false;
   ph.n_bin = 0;
   {
@@ -1651,6 +1845,7 @@ int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx* x, const int* w_type, const double
       c.w.mag[dst] = w_mag[src];
       c.w.expo[dst] = w_exp[src];
     }
+  c.wver++;
   for (auto& ph : c.pops) {
     set_params(c, ph);
     ph.valid_sort = false;  // aero_state_set_weight clears valid_sort
@@ -1730,12 +1925,7 @@ int pmc_coag_gpu_profile(pmc_coag_gpu_ctx* x, int enable) {
   if (!x) return PMC_ERR_INVALID_ARG;
   Ctx& c = x->c;
   GUARD_BEGIN
-  if (enable && !c.prof_ev[0][0]) {
-    for (int i = 0; i < 4; i++) {
-      CK(cudaEventCreate(&c.prof_ev[i][0]));
-      CK(cudaEventCreate(&c.prof_ev[i][1]));
-    }
-  }
+  prof_collect(c);
   c.prof = enable != 0;
   for (int i = 0; i < 4; i++) {
     c.prof_ms[i] = 0.0;
@@ -1748,6 +1938,7 @@ int pmc_coag_gpu_profile(pmc_coag_gpu_ctx* x, int enable) {
 int pmc_coag_gpu_profile_read(pmc_coag_gpu_ctx* x, int which, double* total_ms, int64_t* launches,
                               int64_t* units) {
   if (!x || which < 0 || which > 3) return PMC_ERR_INVALID_ARG;
+  prof_collect(x->c);
   if (total_ms) *total_ms = x->c.prof_ms[which];
   if (launches) *launches = x->c.prof_launch[which];
   if (units) *units = x->c.prof_units[which];
@@ -1757,6 +1948,16 @@ int pmc_coag_gpu_profile_read(pmc_coag_gpu_ctx* x, int which, double* total_ms, 
 int pmc_coag_gpu_launch_count(int64_t* n) {
   if (!n) return PMC_ERR_INVALID_ARG;
   *n = g_launches;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_conflicts(pmc_coag_gpu_ctx* x, int64_t* events, int64_t* event_losers,
+                           int64_t* target_ops, int64_t* target_op_losers) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  if (events) *events = x->c.last_events;
+  if (event_losers) *event_losers = x->c.last_set_losers;
+  if (target_ops) *target_ops = x->c.last_ops;
+  if (target_op_losers) *target_op_losers = x->c.last_pp_lost;
   return PMC_OK;
 }
 

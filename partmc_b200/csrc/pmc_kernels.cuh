@@ -53,22 +53,10 @@ __device__ __forceinline__ Rng make_rng(const PopDev& P, uint32_t stream, uint32
 }
 
 // ---------------------------------------------------------------------------
-// radius range of live particles (remake_if_needed without a valid sort,
-// aero_sorted.F90:293-306)
-__global__ void k_radius_minmax(const PopDev* pops, int n_pop) {
-  const PopDev& P = pops[blockIdx.y];
-  int n = P.ctr->n_slots;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (!P.alive[i]) continue;
-    double r = vol2rad(P.vtot[i]);
-    unsigned long long b = (unsigned long long)__double_as_longlong(r);
-    atomicMin(&P.ctr->rmin_bits, b);
-    atomicMax(&P.ctr->rmax_bits, b);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// sort pass 1: radius, bin and per-chunk cell histogram
+// sort pass 1: per-chunk histogram of the cached (bin, class) of each live
+// slot.  Bins are kept current per slot: every write of a particle refreshes
+// its radius, bin and record (refresh_slot), and a grid change refreshes
+// them all (k_refresh_all).
 __global__ void k_sort_hist(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int chunk = blockIdx.x;
@@ -77,26 +65,20 @@ __global__ void k_sort_hist(const PopDev* pops) {
   int nc = P.n_cells;
   for (int c = threadIdx.x; c < nc; c += blockDim.x) sh[c] = 0;
   __syncthreads();
-  const GridDev& G = *P.grid;
+  int nb = P.grid->n_bin;
   int n = P.ctr->n_slots;
   int base = chunk * kChunk;
   for (int k = threadIdx.x; k < kChunk; k += blockDim.x) {
     int i = base + k;
     if (i >= n) break;
-    if (!P.alive[i]) {
-      P.bin[i] = -1;
+    if (!P.alive[i]) continue;
+    int b = P.bin[i], cl = P.cls[i] - 1;
+    // a slot whose cached bin does not fit the current grid is not sorted
+    if (b < 0 || b >= nb || cl < 0 || cl >= P.n_class) {
+      add_ll(&P.ctr->out_of_grid, 1);
       continue;
     }
-    double r = vol2rad(P.vtot[i]);
-    P.rad[i] = r;
-    int b = bin_find(G.n_bin, G.log_lo, G.log_hi, r);
-    if (b < 1 || b > G.n_bin) {
-      P.bin[i] = -1;
-      add_ll(&P.ctr->out_of_grid, (long long)(1));
-      continue;
-    }
-    P.bin[i] = b - 1;
-    atomicAdd(&sh[(b - 1) + G.n_bin * (P.cls[i] - 1)], 1);
+    atomicAdd(&sh[b + nb * cl], 1);
   }
   __syncthreads();
   int* out = P.chunk_hist + (size_t)chunk * nc;
@@ -132,33 +114,50 @@ __device__ int block_excl_scan(int v, int* total) {
   return pre;
 }
 
-// sort pass 2: cell totals, cell starts, per-chunk offsets (one block per
-// population, one thread per cell)
-__global__ void k_sort_scan(const PopDev* pops) {
-  const PopDev& P = pops[blockIdx.x];
+// sort pass 2a: total of each cell over the chunks (one block per cell)
+__global__ void k_sort_count(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  int c = blockIdx.x;
+  if (c >= P.n_cells) return;
   int nc = P.n_cells;
-  int c = threadIdx.x;
-  int tot = 0;
-  if (c < nc)
-    for (int k = 0; k < P.n_chunks; k++) tot += P.chunk_hist[(size_t)k * nc + c];
-  int all;
-  int start = block_excl_scan(c < nc ? tot : 0, &all);
-  if (c < nc) {
+  int s = 0;
+  for (int k = threadIdx.x; k < P.n_chunks; k += blockDim.x) s += P.chunk_hist[(size_t)k * nc + c];
+  int tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) {
     P.cell_count[c] = tot;
-    P.cell_start[c] = start;
-    int run = start;
-    for (int k = 0; k < P.n_chunks; k++) {
-      int h = P.chunk_hist[(size_t)k * nc + c];
-      P.chunk_hist[(size_t)k * nc + c] = run;
-      run += h;
-    }
     if (tot > 0) {
       int b = c % P.grid->n_bin;
       atomicMin(&P.ctr->bmin, b);
       atomicMax(&P.ctr->bmax, b);
     }
   }
-  if (c == 0) P.cell_start[nc] = all;
+}
+
+// sort pass 2b: start of each cell and the offset of every chunk inside it
+// (one block per cell; chunk offsets by a block scan over the chunks)
+__global__ void k_sort_offsets(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  int c = blockIdx.x;
+  if (c >= P.n_cells) return;
+  int nc = P.n_cells;
+  int s = 0;
+  for (int q = threadIdx.x; q < c; q += blockDim.x) s += P.cell_count[q];
+  int start;
+  block_excl_scan(s, &start);
+  if (threadIdx.x == 0) {
+    P.cell_start[c] = start;
+    if (c == nc - 1) P.cell_start[nc] = start + P.cell_count[c];
+  }
+  int run = start;
+  for (int base = 0; base < P.n_chunks; base += blockDim.x) {
+    int k = base + threadIdx.x;
+    int h = k < P.n_chunks ? P.chunk_hist[(size_t)k * nc + c] : 0;
+    int tot;
+    int pre = block_excl_scan(h, &tot);
+    if (k < P.n_chunks) P.chunk_hist[(size_t)k * nc + c] = run + pre;
+    run += tot;
+  }
 }
 
 // pair-test record of slot i (see RecD)
@@ -185,10 +184,46 @@ __device__ __forceinline__ RecD make_rec(const PopDev& P, int i) {
   return q;
 }
 
-// sort pass 3: deterministic stable scatter (slot order within each cell)
-// and record build.  Warp w of a block owns slots [w*256, (w+1)*256) of the
+__device__ __forceinline__ RecF to_f32(const RecD& q) {
+  RecF f;
+  f.r = (float)q.r;
+  f.rv = (float)q.rv;
+  f.nc = (float)q.nc;
+  f.a = (float)q.a;
+  f.b = (float)q.b;
+  f.c = (float)q.c;
+  f.pad0 = f.pad1 = 0.f;
+  return f;
+}
+
+// radius, bin (aero_sorted_particle_in_bin, aero_sorted.F90:378-391) and
+// pair-test records of live slot i; returns the 1-based bin (0 or n_bin+1
+// off the grid, which leaves the slot unsorted)
+__device__ __forceinline__ int refresh_slot(const PopDev& P, int i) {
+  const GridDev& G = *P.grid;
+  double r = vol2rad(P.vtot[i]);
+  P.rad[i] = r;
+  int b = bin_find(G.n_bin, G.log_lo, G.log_hi, r);
+  P.bin[i] = (b >= 1 && b <= G.n_bin) ? b - 1 : -1;
+  RecD q = make_rec(P, i);
+  P.recd[i] = q;
+  P.recf[i] = to_f32(q);
+  return b;
+}
+
+__global__ void k_refresh_all(const PopDev* pops, const uint8_t* on) {
+  if (!on[blockIdx.y]) return;
+  const PopDev& P = pops[blockIdx.y];
+  int n = P.ctr->n_slots;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (P.alive[i]) refresh_slot(P, i);
+    else P.bin[i] = -1;
+  }
+}
+
+// sort pass 3: deterministic stable scatter (slot order within each cell).  Warp w of a block owns slots [w*256, (w+1)*256) of the
 // chunk; ranks inside a 32-slot tile come from __match_any_sync.
-__global__ void k_sort_scatter(const PopDev* pops, int precision) {
+__global__ void k_sort_scatter(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int chunk = blockIdx.x;
   if (chunk >= P.n_chunks) return;
@@ -203,7 +238,8 @@ __global__ void k_sort_scatter(const PopDev* pops, int precision) {
   for (int t = 0; t < kWarpSlots; t += 32) {
     int i = base + t + lane;
     int key = -1;
-    if (i < n && P.bin[i] >= 0) key = P.bin[i] + nb * (P.cls[i] - 1);
+    if (i < n && P.alive[i] && P.bin[i] >= 0 && P.bin[i] < nb && P.cls[i] >= 1 && P.cls[i] <= P.n_class)
+      key = P.bin[i] + nb * (P.cls[i] - 1);
     unsigned peers = __match_any_sync(0xffffffffu, key);
     int leader = __ffs(peers) - 1;
     if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
@@ -223,7 +259,8 @@ __global__ void k_sort_scatter(const PopDev* pops, int precision) {
   for (int t = 0; t < kWarpSlots; t += 32) {
     int i = base + t + lane;
     int key = -1;
-    if (i < n && P.bin[i] >= 0) key = P.bin[i] + nb * (P.cls[i] - 1);
+    if (i < n && P.alive[i] && P.bin[i] >= 0 && P.bin[i] < nb && P.cls[i] >= 1 && P.cls[i] <= P.n_class)
+      key = P.bin[i] + nb * (P.cls[i] - 1);
     unsigned peers = __match_any_sync(0xffffffffu, key);
     int leader = __ffs(peers) - 1;
     int pos = 0;
@@ -231,23 +268,7 @@ __global__ void k_sort_scatter(const PopDev* pops, int precision) {
     __syncwarp();
     if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
     __syncwarp();
-    if (key >= 0) {
-      P.list[pos] = i;
-      RecD q = make_rec(P, i);
-      if (precision == 0) {
-        P.recd[pos] = q;
-      } else {
-        RecF f;
-        f.r = (float)q.r;
-        f.rv = (float)q.rv;
-        f.nc = (float)q.nc;
-        f.a = (float)q.a;
-        f.b = (float)q.b;
-        f.c = (float)q.c;
-        f.pad0 = f.pad1 = 0.f;
-        P.recf[pos] = f;
-      }
-    }
+    if (key >= 0) P.list[pos] = i;
   }
 }
 
@@ -446,14 +467,15 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
       if (i2 >= n2) i2 = n2 - 1;
     }
     int e1 = S.start1 + i1, e2 = S.start2 + i2;
+    int s1 = P.list[e1], s2 = P.list[e2];
     T k;
     if constexpr (sizeof(T) == 8) {
-      const double* q1 = (const double*)&P.recd[e1];
-      const double* q2 = (const double*)&P.recd[e2];
+      const double* q1 = (const double*)&P.recd[s1];
+      const double* q2 = (const double*)&P.recd[s2];
       k = (T)pair_kernel<KT, double, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, S.fflat, P.coeff);
     } else {
-      const float* q1 = (const float*)&P.recf[e1];
-      const float* q2 = (const float*)&P.recf[e2];
+      const float* q1 = (const float*)&P.recf[s1];
+      const float* q2 = (const float*)&P.recf[s2];
       k = (T)pair_kernel<KT, float, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, (float)S.fflat,
                                           (float)P.coeff);
     }
@@ -462,7 +484,6 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
     bool acc = (T)u53(rnd.z, rnd.w) < prob;
     flag[w] = acc ? 1 : 0;
     if (acc) {
-      int s1 = P.list[e1], s2 = P.list[e2];
       unsigned prio = (unsigned)(prio_off[gp] + s);
       atomicMin(&P.claim[s1], prio);
       atomicMin(&P.claim[s2], prio);

@@ -14,6 +14,11 @@
 
 namespace pmc {
 
+__device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
+  P.alive[i] = 0;
+  P.bin[i] = -1;
+}
+
 // Decisions of coagulate_weighting (coagulation.F90:855-892).
 struct MergeDecision {
   bool rm1, rm2, create, lost1, lost2;
@@ -53,7 +58,8 @@ __device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int
 __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
                               const long long* work_off, const long long* prio_off, int n_gpairs,
                               const long long* n_events, const long long* ev_w, const int2* ev,
-                              int* pair_losers, int* need_slot, int* need_id, uint8_t* win) {
+                              int* pair_losers, int* need_slot, int* need_id, uint8_t* win,
+                              long long* n_losers) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
@@ -70,6 +76,7 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const in
     need_id[e] = 0;
     if (!winner) {
       atomicAdd(&pair_losers[gp], 1);
+      add_ll(n_losers, 1);
       continue;
     }
     PairDesc d = P.pair_desc[p];
@@ -139,15 +146,14 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int*
       store_particle(P, dest, v, c);
       // the coagulated particle must lie on the grid (aero_state_add_particle
       // with allow_resort=.false., aero_sorted.F90:427-440)
-      double r = vol2rad(P.vtot[dest]);
-      int nbin = bin_find(P.grid->n_bin, P.grid->log_lo, P.grid->log_hi, r);
+      int nbin = refresh_slot(P, dest);
       if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
-      if (m.rm1 && dest != s1) P.alive[s1] = 0;
-      if (m.rm2 && dest != s2) P.alive[s2] = 0;
+      if (m.rm1 && dest != s1) kill_slot(P, s1);
+      if (m.rm2 && dest != s2) kill_slot(P, s2);
       dlive = 1 - (int)m.rm1 - (int)m.rm2;
     } else {
-      if (m.rm1) P.alive[s1] = 0;
-      if (m.rm2) P.alive[s2] = 0;
+      if (m.rm1) kill_slot(P, s1);
+      if (m.rm2) kill_slot(P, s2);
       dlive = -(int)m.rm1 - (int)m.rm2;
     }
     if (dlive) add_ll(&P.ctr->n_live, (long long)(dlive));
@@ -203,7 +209,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     int n_src = P.cell_count[src_cell];
     int src_start = P.cell_start[src_cell];
     if (n_src == 0) continue;
-    RecD qt = make_rec(P, t);
+    RecD qt = P.recd[t];
     double nc_target = qt.nc;
     double nc_src_min = num_conc_at_radius<double>(P.w, cs, G.edges[S.bs]);
     double prm_max = nc_target / nc_src_min;
@@ -252,7 +258,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
       int ie = rand_int(g, n_src);
       int e = src_start + ie - 1;
       int si = P.list[e];
-      RecD qs = P.recd[e];
+      RecD qs = P.recd[si];
       double k = pp_kernel<KT>(P, qs, qt, cs, ct);
       double pc = k * S.inv_k_max;
       pc_tot = pc_tot + pc;
@@ -406,17 +412,18 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
     const PPResult& R = res[q];
     int dlive = 0;
     for (int z = 0; z < R.n_rm; z++) {
-      P.alive[R.rm[z]] = 0;
+      kill_slot(P, R.rm[z]);
       dlive--;
     }
     if (R.merged) {
       const double* v = res_vol + (size_t)q * P.n_spec;
       int t = R.target;
       if (R.n_copies == 0) {
-        P.alive[t] = 0;
+        kill_slot(P, t);
         dlive--;
       } else {
         store_particle(P, t, v, R.meta);
+        refresh_slot(P, t);
         for (int z = 1; z < R.n_copies; z++) {
           int dest = slot_base[pop] + (int)slot_rank[q] + (z - 1);
           if (dest >= P.cap) {
@@ -427,6 +434,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
           cm.grp = R.copy_group[z];
           cm.id = id_base[pop] + id_rank[q] + (z - 1);
           store_particle(P, dest, v, cm);
+          refresh_slot(P, dest);
           dlive++;
         }
       }

@@ -125,7 +125,7 @@ struct PopDev {
   int* hyst;
   int* frozen;
   uint8_t* alive;
-  int* bin;  // 0-based bin of each slot (after the sort), -1 dead
+  int* bin;  // 0-based bin of each live slot, -1 dead or off the grid
 
   const double* density;  // [n_spec]
 
@@ -135,8 +135,8 @@ struct PopDev {
   int* cell_count;  // [n_cells]
   int* cell_start;  // [n_cells + 1]
   int* list;        // [cap] slot numbers in cell order
-  RecD* recd;       // [cap]
-  RecF* recf;       // [cap]
+  RecD* recd;       // [cap] pair-test record of each slot (FP64)
+  RecF* recf;       // [cap] the same in FP32
 
   double* kmax_tab;  // [n_bin * n_bin], (b1, b2) at b1 + n_bin * b2
   int kmax_valid;
