@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--batch-pops", type=int, default=256)
+    ap.add_argument("--batch-same", type=int, default=8)
     return ap.parse_args()
 
 
@@ -149,6 +151,58 @@ def measured_peak_hbm():
 def workload(n_part, seed):
     from partmc_b200 import aero_dist
     return aero_dist.brown_20spec(n_part, seed=seed)
+
+
+def run_batched(pm, n_pop, steps, warmup, del_t, mode, seed=5):
+    """Batched form: n_pop independent populations (log-uniform 1e3..1e5
+    particles, per-population T, p and mode parameters, power weighting) in
+    one context; every launch covers all populations.  Returns aggregate
+    pair tests per second and simulated seconds per second."""
+    import torch
+    from partmc_b200 import aero_dist
+    pops, temps, press = aero_dist.batched_bimodal(n_pop=n_pop, seed=seed)
+    ad = pops[0].aero_data
+    st = pm.AeroState(ad, pops[0].awa, mode=mode, n_pop=n_pop)
+    for k, p in enumerate(pops):
+        st.set_weight_pop(k, p.awa)
+        st.add_particles(p.vol, p.group, pop=k)
+    for _ in range(warmup):
+        pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, st, del_t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    samp, _ = pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, st, del_t, n_steps=steps)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    n_part = int(sum(p.n_part for p in pops))
+    return {"value": samp / sec, "unit": "pair-tests/s", "populations": n_pop, "particles": n_part,
+            "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec,
+            "rounds_last_step": st.stats()["rounds"]}
+
+
+def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode):
+    """n_pop independent copies (different seeds and samples) of the 1e6
+    particle workload advanced together in one batched context."""
+    import torch
+    pops = [workload(n_part, seed=200 + k) for k in range(n_pop)]
+    st = pm.AeroState(pops[0].aero_data, pops[0].awa, mode=mode, n_pop=n_pop)
+    for k, p in enumerate(pops):
+        # same densities (seeded); the weights depend on the sample
+        st.set_weight_pop(k, p.awa)
+        st.add_particles(p.vol, p.group, pop=k)
+    temps, press = np.full(n_pop, 288.0), np.full(n_pop, 1e5)
+    for _ in range(warmup):
+        pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, st, del_t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    samp, _ = pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, st, del_t, n_steps=steps)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    return {"value": samp / sec, "unit": "pair-tests/s", "populations": n_pop, "particles_each": n_part,
+            "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec}
 
 
 def cpu_baseline(n_part, del_t, budget_s=20.0):
@@ -289,6 +343,10 @@ def main():
     st64 = new_state(pm.MODE_FP64)
     ms64, samp64, _, _ = timed_steps(st64, max(3, args.steps // 2), args.warmup)
     del st64
+    del st
+    batched = run_batched(pm, args.batch_pops, max(3, args.steps // 2), args.warmup, args.del_t, mode)
+    batched_1e6 = run_batched_same(pm, args.batch_same, args.n_part, max(3, args.steps // 2), args.warmup,
+                                   args.del_t, mode)
 
     # end to end through the C ABI with host buffers: upload, step, download
     host_vol = torch.from_numpy(pop.vol).pin_memory().numpy()
@@ -357,6 +415,8 @@ def main():
             "sim_s_per_s": args.steps * args.del_t * ws / t_max,
             "fp64_plain": {"value": samp64_all / t64, "unit": "pair-tests/s",
                            "ms_per_step": ms64 / max(3, args.steps // 2)},
+            "batched": batched,
+            "batched_1e6": batched_1e6,
             "e2e": {"value": e2e_all / e2e_t, "unit": "pair-tests/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),

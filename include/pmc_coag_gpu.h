@@ -133,6 +133,13 @@ int pmc_coag_gpu_download_components(pmc_coag_gpu_ctx *ctx, int pop,
 int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx *ctx, const int *w_type,
                             const double *w_mag, const double *w_exp);
 
+/* Weights of one population of a batched context (same shape as the
+ * context's weights); each population keeps its own magnitudes, as separate
+ * aero_state_t instances do. */
+int pmc_coag_gpu_set_weight_pop(pmc_coag_gpu_ctx *ctx, int pop,
+                                const int *w_type, const double *w_mag,
+                                const double *w_exp);
+
 /* The ID counter (next_id, aero_particle.F90:72, new_id :157-165). */
 int pmc_coag_gpu_set_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t next_id);
 int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t *next_id);

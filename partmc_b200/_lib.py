@@ -45,6 +45,7 @@ SIGNATURES = {
     "pmc_coag_gpu_download": (_I, [_P, _I, _I, _DP, _IP, _IP, _LP, _IP, _IP]),
     "pmc_coag_gpu_download_components": (_I, [_P, _I, _I, _IP, _IP, _DP]),
     "pmc_coag_gpu_set_weight": (_I, [_P, _IP, _DP, _DP]),
+    "pmc_coag_gpu_set_weight_pop": (_I, [_P, _I, _IP, _DP, _DP]),
     "pmc_coag_gpu_set_next_id": (_I, [_P, _I, ctypes.c_int64]),
     "pmc_coag_gpu_get_next_id": (_I, [_P, _I, _LP]),
     "pmc_coag_gpu_set_mode": (_I, [_P, _I]),

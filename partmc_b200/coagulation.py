@@ -147,6 +147,12 @@ class AeroState:
         t, m, e = aero_weight_array.flat_arrays()
         check(_lib.lib().pmc_coag_gpu_set_weight(self.ctx, ip(t), dp(m), dp(e)), "pmc_coag_gpu_set_weight")
 
+    def set_weight_pop(self, pop, aero_weight_array):
+        """Weights of one population of a batched state."""
+        t, m, e = aero_weight_array.flat_arrays()
+        check(_lib.lib().pmc_coag_gpu_set_weight_pop(self.ctx, pop, ip(t), dp(m), dp(e)),
+              "pmc_coag_gpu_set_weight_pop")
+
     def add_particles(self, vol, weight_group=None, weight_class=None, ids=None, n_primary_parts=None,
                       n_comp=None, comp_source=None, comp_create_time=None, pop=0):
         """Replace population ``pop`` by these particles.  vol: (n_part, n_spec)."""

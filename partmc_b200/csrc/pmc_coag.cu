@@ -436,6 +436,8 @@ struct PopHost {
   uint64_t seed = 1;
   uint32_t step = 0;
   int kmax_kt = 0;  // kernel type of the current k_max table
+  bool own_w = false;  // weights set for this population alone
+  Weights w{};
   int chunk_hist_cap = 0;
   // per-slot radius/bin/record caches are valid for this grid, kernel,
   // environment and weights
@@ -453,6 +455,8 @@ struct Ctx {
   std::vector<PopHost> pops;
   PopDev* d_pops = nullptr;
   PopCtr* d_ctrs = nullptr;  // one counter block per population
+  uint32_t* d_round = nullptr;  // round of the current step, read by the kernels
+  bool dirty = true;            // host PopDev copies changed since the last push
   std::vector<PopCtr> h_ctrs;
   cudaStream_t stream = nullptr;
   int max_rounds = 32;
@@ -595,8 +599,12 @@ long long scan(Ctx& c, const T* in, long long n, long long* out, bool read_total
 
 void push_pops(Ctx& c) {
   std::vector<PopDev> v(c.n_pop);
-  for (int k = 0; k < c.n_pop; k++) v[k] = c.pops[k].h;
+  for (int k = 0; k < c.n_pop; k++) {
+    v[k] = c.pops[k].h;
+    v[k].round_p = c.d_round;
+  }
   CK(cudaMemcpyAsync(c.d_pops, v.data(), sizeof(PopDev) * c.n_pop, cudaMemcpyHostToDevice, c.stream));
+  c.dirty = false;
 }
 
 // counters of every population in one copy
@@ -649,6 +657,7 @@ void alloc_slots(Ctx& c, PopHost& ph, int cap) {
   h.recf = dalloc<RecF>(o, cap);
   h.claim = dalloc<unsigned>(o, cap);
   CK(cudaMemsetAsync(h.alive, 0, cap, c.stream));
+  c.dirty = true;
 }
 
 // sort structures that depend on the grid and the slot count
@@ -685,6 +694,7 @@ void alloc_sort(Ctx& c, PopHost& ph) {
   h.pair_desc = pd;
   h.pair = dalloc<PairState>(o, std::max<size_t>(ph.pair_desc.size(), 1));
   h.kmax_valid = 0;
+  c.dirty = true;
 }
 
 // bin_grid_make (log) on the host, with glibc's log/exp like the reference
@@ -734,14 +744,15 @@ void set_params(Ctx& c, PopHost& ph) {
   h.n_group = c.n_group;
   h.n_class = c.n_class;
   h.i_water = c.i_water;
-  h.w = c.w;
-  h.flat = weights_flat(c.w);
+  h.w = ph.own_w ? ph.w : c.w;
+  h.flat = weights_flat(h.w);
   bool inc, dec;
-  weight_monotonicity(c.w, &inc, &dec);
+  weight_monotonicity(h.w, &inc, &dec);
   h.mono_dec = dec;
   h.dmin = *std::min_element(c.density.begin(), c.density.end());
   h.dmax = *std::max_element(c.density.begin(), c.density.end());
   h.seed = ph.seed;
+  c.dirty = true;
 }
 
 void init_pop(Ctx& c, PopHost& ph, int cap) {
@@ -845,9 +856,10 @@ void prepare_chunks(Ctx& c) {
     ph.h.n_chunks = (c.n_slots_host[k] + kChunk - 1) / kChunk;
     int need = std::max(ph.h.n_chunks, 1) * ph.h.n_cells;
     if (need > ph.chunk_hist_cap) {
-      int want = std::max(need, 1024);
+      int want = std::max(need * 2, 1024);  // headroom: slots grow inside a step
       ph.h.chunk_hist = dalloc<int>(ph.sort_allocs, want);
       ph.chunk_hist_cap = want;
+      c.dirty = true;
     }
   }
 }
@@ -857,7 +869,7 @@ void run_hist_scan(Ctx& c) {
   prepare_chunks(c);
   k_reset_ranges<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_ctrs, c.n_pop);
   note_launch();
-  push_pops(c);
+  if (c.dirty) push_pops(c);
   int max_chunks = 1, max_cells = 1;
   for (int k = 0; k < c.n_pop; k++) {
     max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
@@ -1275,7 +1287,8 @@ void step_parallel(Ctx& c, int kt) {
     nb_max = std::max(nb_max, c.pops[k].n_bin);
     max_cap = std::max(max_cap, c.pops[k].h.cap);
   }
-  bool flat = weights_flat(c.w);
+  bool flat = true;
+  for (int k = 0; k < c.n_pop; k++) flat = flat && c.pops[k].h.flat;
   float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
   long long redraws = 0, Qprev = 0;
   c.last_set_losers = c.last_pp_lost = c.last_events = c.last_ops = 0;
@@ -1283,8 +1296,11 @@ void step_parallel(Ctx& c, int kt) {
   std::vector<int> per_pop(4 * (size_t)c.n_pop);
   int round = 0;
   for (;;) {
-    for (int k = 0; k < c.n_pop; k++) c.pops[k].h.round = (uint32_t)round;
-    push_pops(c);
+    {
+      uint32_t r32 = (uint32_t)round;  // staged before the call returns
+      CK(cudaMemcpyAsync(c.d_round, &r32, sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+    }
+    if (c.dirty) push_pops(c);
     if (round > 0) sort_pops(c, false);
     if (round == 0) {
       dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
@@ -1298,8 +1314,9 @@ void step_parallel(Ctx& c, int kt) {
       note_launch();
     }
     if (round == 0) {
+      // the device copies learn this with the next push
       for (int k = 0; k < c.n_pop; k++) c.pops[k].h.kmax_valid = 1;
-      push_pops(c);
+      c.dirty = true;
     }
     scan_dev(c, c.nwork_set.p, n_gpairs, nullptr, c.work_off.p);
     scan_dev(c, c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p);
@@ -1531,6 +1548,8 @@ static int do_init(int n_pop, int n_spec, const double* density, int i_water, in
   c.pops.resize(n_pop);
   CK(cudaMalloc(&c.d_pops, sizeof(PopDev) * n_pop));
   CK(cudaMalloc(&c.d_ctrs, sizeof(PopCtr) * n_pop));
+  CK(cudaMalloc(&c.d_round, sizeof(uint32_t)));
+  CK(cudaMemset(c.d_round, 0, sizeof(uint32_t)));
   CK(cudaMemset(c.d_ctrs, 0, sizeof(PopCtr) * n_pop));
   for (int k = 0; k < n_pop; k++) {
     c.pops[k].seed = seeds ? seeds[k] : (uint64_t)(k + 1);
@@ -1566,6 +1585,7 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   }
   cudaFree(c.d_pops);
   cudaFree(c.d_ctrs);
+  cudaFree(c.d_round);
   DevBuf<int>* bi[] = {&c.gpair_pop, &c.gpair_local, &c.pair_losers, &c.need_slot_set, &c.need_id_set,
                        &c.need_slot_pp, &c.need_id_pp, &c.lost_pp, &c.op_pop, &c.op_pair, &c.op_slot,
                        &c.op_k, &c.r_pop, &c.r_pair, &c.r_slot, &c.r_k, &c.per_pop_i,
@@ -1850,6 +1870,33 @@ int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx* x, const int* w_type, const double
     set_params(c, ph);
     ph.valid_sort = false;  // aero_state_set_weight clears valid_sort
   }
+  c.replay.valid = false;
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_set_weight_pop(pmc_coag_gpu_ctx* x, int pop, const int* w_type, const double* w_mag,
+                                const double* w_exp) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || !w_type || !w_mag || !w_exp) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  Weights w = c.w;
+  for (int cl = 0; cl < c.n_class; cl++)
+    for (int g = 0; g < c.n_group; g++) {
+      int src = g + c.n_group * cl, dst = g + kMaxGroup * cl;
+      if (w_type[src] < 1 || w_type[src] > 3) return PMC_ERR_INVALID_ARG;
+      w.type[dst] = w_type[src];
+      w.mag[dst] = w_mag[src];
+      w.expo[dst] = w_exp[src];
+    }
+  ph.w = w;
+  ph.own_w = true;
+  c.wver++;
+  set_params(c, ph);
+  ph.valid_sort = false;
   c.replay.valid = false;
   push_pops(c);
   CK(cudaStreamSynchronize(c.stream));

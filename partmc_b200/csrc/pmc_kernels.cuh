@@ -48,8 +48,14 @@ __device__ __forceinline__ void add_ll(long long* p, long long v) {
 }
 __device__ __forceinline__ void add_ll(int* p, long long v) { atomicAdd(p, (int)v); }
 
+// sort chunks covering the population's slots (the slot count lives on the
+// device and grows inside a step)
+__device__ __forceinline__ int n_chunks_of(const PopDev& P) {
+  return (P.ctr->n_slots + kChunk - 1) / kChunk;
+}
+
 __device__ __forceinline__ Rng make_rng(const PopDev& P, uint32_t stream, uint32_t p, uint32_t s) {
-  return Rng(P.seed, P.step, (p << 12) | ((P.round & 0xffu) << 4) | stream, s);
+  return Rng(P.seed, P.step, (p << 12) | ((*P.round_p & 0xffu) << 4) | stream, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -60,7 +66,7 @@ __device__ __forceinline__ Rng make_rng(const PopDev& P, uint32_t stream, uint32
 __global__ void k_sort_hist(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int chunk = blockIdx.x;
-  if (chunk >= P.n_chunks) return;
+  if (chunk >= n_chunks_of(P)) return;
   extern __shared__ int sh[];
   int nc = P.n_cells;
   for (int c = threadIdx.x; c < nc; c += blockDim.x) sh[c] = 0;
@@ -121,7 +127,8 @@ __global__ void k_sort_count(const PopDev* pops) {
   if (c >= P.n_cells) return;
   int nc = P.n_cells;
   int s = 0;
-  for (int k = threadIdx.x; k < P.n_chunks; k += blockDim.x) s += P.chunk_hist[(size_t)k * nc + c];
+  int n_chunks = n_chunks_of(P);
+  for (int k = threadIdx.x; k < n_chunks; k += blockDim.x) s += P.chunk_hist[(size_t)k * nc + c];
   int tot;
   block_excl_scan(s, &tot);
   if (threadIdx.x == 0) {
@@ -150,12 +157,13 @@ __global__ void k_sort_offsets(const PopDev* pops) {
     if (c == nc - 1) P.cell_start[nc] = start + P.cell_count[c];
   }
   int run = start;
-  for (int base = 0; base < P.n_chunks; base += blockDim.x) {
+  int n_chunks = n_chunks_of(P);
+  for (int base = 0; base < n_chunks; base += blockDim.x) {
     int k = base + threadIdx.x;
-    int h = k < P.n_chunks ? P.chunk_hist[(size_t)k * nc + c] : 0;
+    int h = k < n_chunks ? P.chunk_hist[(size_t)k * nc + c] : 0;
     int tot;
     int pre = block_excl_scan(h, &tot);
-    if (k < P.n_chunks) P.chunk_hist[(size_t)k * nc + c] = run + pre;
+    if (k < n_chunks) P.chunk_hist[(size_t)k * nc + c] = run + pre;
     run += tot;
   }
 }
@@ -221,12 +229,13 @@ __global__ void k_refresh_all(const PopDev* pops, const uint8_t* on) {
   }
 }
 
-// sort pass 3: deterministic stable scatter (slot order within each cell).  Warp w of a block owns slots [w*256, (w+1)*256) of the
-// chunk; ranks inside a 32-slot tile come from __match_any_sync.
+// sort pass 3: deterministic stable scatter (slot order within each cell).
+// Warp w of a block owns slots [w*256, (w+1)*256) of the chunk; ranks
+// inside a 32-slot tile come from __match_any_sync.
 __global__ void k_sort_scatter(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int chunk = blockIdx.x;
-  if (chunk >= P.n_chunks) return;
+  if (chunk >= n_chunks_of(P)) return;
   extern __shared__ int wc[];  // [kSortWarps][n_cells]
   int nc = P.n_cells;
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -311,7 +320,7 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
   S.start1 = P.cell_start[cell1];
   S.start2 = P.cell_start[cell2];
   bool same = (b1 == b2) && (c1 == c2);
-  if (P.round > 0) {
+  if (*P.round_p > 0) {
     // redraws of lost samples; a per-particle pair is not redone
     long long nl = S.path == kPathSet ? pair_losers[gp] : 0;
     if ((same && n1 < 2) || n1 < 1 || n2 < 1) nl = 0;
@@ -449,7 +458,7 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
     long long s = w - work_off[gp];
     const PairState& S = P.pair[p];
     PairDesc d = P.pair_desc[p];
-    U4 rnd = philox4x32_10(U4{P.step, (uint32_t)(p << 12) | ((P.round & 0xffu) << 4) | kStreamTest,
+    U4 rnd = philox4x32_10(U4{P.step, (uint32_t)(p << 12) | ((*P.round_p & 0xffu) << 4) | kStreamTest,
                               (uint32_t)s, 0u},
                            (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
     // find_rand_pair (coagulation.F90:766-803), 0-based entries

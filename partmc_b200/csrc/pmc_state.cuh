@@ -96,7 +96,8 @@ struct PopDev {
   int n_chunks; // sort chunks covering n_slots
   int n_pairs;
   uint64_t seed;
-  uint32_t step, round;
+  uint32_t step;
+  const uint32_t* round_p;  // the current round of the step (one device word for all populations)
   int kernel_type;
   double temp, pressure, coeff, del_t;
   BrownEnv benv;
