@@ -26,7 +26,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-B_TEST = 56  # algorithmic bytes per pair test (indices, two records, k_max entry)
+B_TEST = 56  # algorithmic bytes per pair test: two cell-list entries and two 24-byte records
+B_SCATTER = 13  # per slot: alive flag, bin and class read, one cell-list entry written
 
 
 def parse():
@@ -42,6 +43,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batch-pops", type=int, default=256)
     ap.add_argument("--batch-same", type=int, default=8)
+    ap.add_argument("--headline-only", action="store_true",
+                    help="measure the headline step only (no FP64, batched or end-to-end lines)")
     return ap.parse_args()
 
 
@@ -176,9 +179,9 @@ def run_batched(pm, n_pop, steps, warmup, del_t, mode, seed=5):
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     n_part = int(sum(p.n_part for p in pops))
-    return {"value": samp / sec, "unit": "pair-tests/s", "populations": n_pop, "particles": n_part,
-            "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec,
-            "rounds_last_step": st.stats()["rounds"]}
+    return ({"unit": "pair-tests/s", "populations": n_pop, "particles": n_part,
+             "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec,
+             "rounds_last_step": st.stats()["rounds"]}, samp, sec)
 
 
 def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode):
@@ -201,8 +204,8 @@ def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode):
     e1.record()
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
-    return {"value": samp / sec, "unit": "pair-tests/s", "populations": n_pop, "particles_each": n_part,
-            "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec}
+    return ({"unit": "pair-tests/s", "populations": n_pop, "particles_each": n_part,
+             "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec}, samp, sec)
 
 
 def cpu_baseline(n_part, del_t, budget_s=20.0):
@@ -263,6 +266,102 @@ def run_reference(args, ws, rank):
             "e2e": {"value": v, "unit": "pair-tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "sim_s_per_s": args.steps * args.del_t * n_thr / dt}
     print(json.dumps(line))
+
+
+def aggregate(d, samp, sec, ws):
+    """Whole-job form of a per-rank measurement: summed work over the
+    slowest rank's time."""
+    t = allreduce_max(sec, ws)
+    d["value"] = allreduce_sum(samp, ws) / t
+    return d
+
+
+def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
+    """Secondary lines: the plain FP64 step, the batched forms and the two
+    end-to-end measurements through the C ABI."""
+    out = {}
+    # plain FP64 form of the same step, for the precision comparison
+    k64 = max(3, args.steps // 2)
+    st64 = new_state(pm.MODE_FP64)
+    ms64, samp64, _, _ = timed_steps(st64, k64, args.warmup)
+    del st64
+    out["fp64_plain"] = aggregate({"unit": "pair-tests/s", "ms_per_step": ms64 / k64}, samp64, ms64 / 1e3, ws)
+    kb = max(3, args.steps // 2)
+    b, samp_b, sec_b = run_batched(pm, args.batch_pops, kb, args.warmup, args.del_t, mode)
+    out["batched"] = aggregate(b, samp_b, sec_b, ws)
+    b, samp_b, sec_b = run_batched_same(pm, args.batch_same, args.n_part, kb, args.warmup, args.del_t, mode)
+    out["batched_1e6"] = aggregate(b, samp_b, sec_b, ws)
+
+    # end to end through the C ABI with host buffers, the way a drop-in
+    # mc_coag sees them: the population lives in pinned host memory; every
+    # step uploads it, steps it and downloads it into the same buffers.
+    def pinned(shape, dt):
+        return torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+
+    cap_h = pop.n_part + pop.n_part // 2
+    hb = {"vol": pinned((cap_h, pop.aero_data.n_spec), torch.float64),
+          "weight_group": pinned((cap_h,), torch.int32), "weight_class": pinned((cap_h,), torch.int32),
+          "id": pinned((cap_h,), torch.int64), "n_primary_parts": pinned((cap_h,), torch.int32)}
+    n_h = pop.n_part
+    hb["vol"][:n_h] = pop.vol
+    hb["weight_group"][:n_h] = pop.group
+    hb["weight_class"][:n_h] = 1
+    hb["id"][:n_h] = np.arange(1, n_h + 1)
+    hb["n_primary_parts"][:n_h] = 1
+    ste = new_state(mode)
+
+    def e2e_step():
+        nonlocal n_h
+        ste.add_particles(hb["vol"][:n_h], hb["weight_group"][:n_h], hb["weight_class"][:n_h], ids=hb["id"][:n_h],
+                          n_primary_parts=hb["n_primary_parts"][:n_h])
+        a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, ste, args.del_t)
+        got = ste.particles(out=hb)
+        n_in = n_h
+        n_h = got["id"].shape[0]
+        return a, n_in, n_h
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e2e_samp, h2d, d2h = 0, 0, 0
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        a, n_in, n_out = e2e_step()
+        e2e_samp += a
+        h2d += n_in * (8 * pop.aero_data.n_spec + 4 + 4 + 8 + 4)
+        d2h += n_out * (8 * pop.aero_data.n_spec + 4 + 4 + 8 + 4)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    del ste
+
+    # the same API with the population kept in HBM between calls (a
+    # coagulation-only run): per step the host passes temperature and
+    # pressure and reads back the two counters
+    str_ = new_state(mode)
+    for _ in range(args.warmup):
+        pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, str_, args.del_t)
+    barrier(ws)
+    torch.cuda.synchronize()
+    res_samp = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, str_, args.del_t)
+        res_samp += a
+    torch.cuda.synchronize()
+    res_s = time.perf_counter() - t0
+    del str_
+
+    out["e2e"] = aggregate({"unit": "pair-tests/s",
+                            "h2d_bytes_per_step": int(h2d / max(args.e2e_steps, 1)),
+                            "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1)),
+                            "path": "upload (pinned host) + mc_coag + download (pinned host) every step "
+                                    "through the C ABI",
+                            "ms_per_step": 1e3 * e2e_s / max(args.e2e_steps, 1)}, e2e_samp, e2e_s, ws)
+    out["e2e_resident"] = aggregate({"unit": "pair-tests/s", "h2d_bytes_per_step": 16, "d2h_bytes_per_step": 8,
+                                     "path": "mc_coag through the C ABI, population resident in HBM between calls",
+                                     "ms_per_step": 1e3 * res_s / max(args.steps, 1)}, res_samp, res_s, ws)
+    return out
 
 
 def main():
@@ -339,45 +438,13 @@ def main():
     clocks.start()
     ms, samp, launches, prof = timed_steps(st, args.steps, args.warmup)
     clk = clocks.stop()
-    # plain FP64 form of the same step, for the precision comparison
-    st64 = new_state(pm.MODE_FP64)
-    ms64, samp64, _, _ = timed_steps(st64, max(3, args.steps // 2), args.warmup)
-    del st64
     del st
-    batched = run_batched(pm, args.batch_pops, max(3, args.steps // 2), args.warmup, args.del_t, mode)
-    batched_1e6 = run_batched_same(pm, args.batch_same, args.n_part, max(3, args.steps // 2), args.warmup,
-                                   args.del_t, mode)
-
-    # end to end through the C ABI with host buffers: upload, step, download
-    host_vol = torch.from_numpy(pop.vol).pin_memory().numpy()
-    host_grp = torch.from_numpy(pop.group).pin_memory().numpy()
-    ste = new_state(mode)
-    for _ in range(2):
-        ste.add_particles(host_vol, host_grp)
-        pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, ste, args.del_t)
-        out = ste.particles()
-    barrier(ws)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e2e_samp = 0
-    h2d = d2h = 0
-    for _ in range(args.e2e_steps):
-        ste.add_particles(host_vol, host_grp)
-        a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, ste, args.del_t)
-        out = ste.particles()
-        e2e_samp += a
-        h2d = host_vol.nbytes + host_grp.nbytes
-        d2h = sum(v.nbytes for v in out.values())
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-
     # whole-job aggregates: max time over ranks, summed work
     t_max = allreduce_max(ms / 1e3, ws)
     samp_all = allreduce_sum(samp, ws)
-    e2e_t = allreduce_max(e2e_s, ws)
-    e2e_all = allreduce_sum(e2e_samp, ws)
-    t64 = allreduce_max(ms64 / 1e3, ws)
-    samp64_all = allreduce_sum(samp64, ws)
+    extra = {}
+    if not args.headline_only:
+        extra = run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws)
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -385,7 +452,7 @@ def main():
         tsc, nsc, usc = prof["scatter"]
         # dominant kernel by measured time
         if tsc >= ttest:
-            dom, t_tot, n_l, units, bpu = "k_sort_scatter (sort pass 3 + pair-test records)", tsc, nsc, usc, 8 * 20 + 16
+            dom, t_tot, n_l, units, bpu = "k_sort_scatter (counting-sort scatter)", tsc, nsc, usc, B_SCATTER
         else:
             dom, t_tot, n_l, units, bpu = "k_test (pair tests)", ttest, ntest, utest, B_TEST
         avg_ms = t_tot / max(n_l, 1)
@@ -413,12 +480,6 @@ def main():
                        else "FP64", "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": f"replicas x{ws}"},
             "sim_s_per_s": args.steps * args.del_t * ws / t_max,
-            "fp64_plain": {"value": samp64_all / t64, "unit": "pair-tests/s",
-                           "ms_per_step": ms64 / max(3, args.steps // 2)},
-            "batched": batched,
-            "batched_1e6": batched_1e6,
-            "e2e": {"value": e2e_all / e2e_t, "unit": "pair-tests/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
@@ -431,6 +492,7 @@ def main():
             "conflicts_per_step": prof["conflicts_per_step"],
             "clocks": clk,
         }
+        line.update(extra)
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))

@@ -177,15 +177,28 @@ class AeroState:
         check(_lib.lib().pmc_coag_gpu_n_part(self.ctx, pop, ctypes.byref(n)), "pmc_coag_gpu_n_part")
         return n.value
 
-    def particles(self, pop=0, components=False):
+    def particles(self, pop=0, components=False, out=None):
+        """The particles of population ``pop`` (aero_state.F90 particle
+        arrays, in slot order).  ``out``: optional dict of preallocated
+        arrays (e.g. in pinned host memory) with room for every particle;
+        the result then holds views of their first n_part rows."""
         n = self.n_part(pop)
-        out = {
-            "vol": np.empty((n, self.aero_data.n_spec), dtype=np.float64),
-            "weight_group": np.empty(n, dtype=np.int32),
-            "weight_class": np.empty(n, dtype=np.int32),
-            "id": np.empty(n, dtype=np.int64),
-            "n_primary_parts": np.empty(n, dtype=np.int32),
-        }
+        if out is None:
+            out = {
+                "vol": np.empty((n, self.aero_data.n_spec), dtype=np.float64),
+                "weight_group": np.empty(n, dtype=np.int32),
+                "weight_class": np.empty(n, dtype=np.int32),
+                "id": np.empty(n, dtype=np.int64),
+                "n_primary_parts": np.empty(n, dtype=np.int32),
+            }
+        else:
+            for key, dt in (("vol", np.float64), ("weight_group", np.int32), ("weight_class", np.int32),
+                            ("id", np.int64), ("n_primary_parts", np.int32)):
+                a = out[key]
+                if a.dtype != dt or not a.flags.c_contiguous or a.shape[0] < n:
+                    raise ValueError(f"out[{key!r}] must be a C-contiguous {np.dtype(dt).name} array "
+                                     f"with at least {n} rows")
+            out = {k: v[:n] for k, v in out.items()}
         got = ctypes.c_int()
         rc = _lib.lib().pmc_coag_gpu_download(self.ctx, pop, n, dp(out["vol"]), ip(out["weight_group"]),
                                               ip(out["weight_class"]), lp(out["id"]), ip(out["n_primary_parts"]),

@@ -310,6 +310,12 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.recd[j] = S.recd[i];
     D.recf[j] = S.recf[i];
   }
+  // growth keeps slot numbers, so the current cell list (positions below
+  // n_slots) stays valid and is carried over; compaction renumbers slots
+  // and the next sort rebuilds the list
+  if (!compact)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += gridDim.x * blockDim.x)
+      D.list[i] = S.list[i];
 }
 
 __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, const double* v2,
@@ -391,6 +397,7 @@ __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, 
   } while (0)
 
 char g_last_error[512];
+char g_last_assert[256];  // site and index of the last failed device bounds check
 // kernel launches issued by this library (for the benchmark's launch count)
 long long g_launches = 0;
 inline void note_launch() { ++g_launches; }
@@ -479,6 +486,11 @@ struct Ctx {
   DevBuf<long long> id_base_set, id_base_pp;
   DevBuf<long long> scan_bsum, scan_total;
   DevBuf<long long> n_dev;  // device scalars
+  // staging for upload / download (shared by all populations; every call
+  // synchronises before it returns)
+  DevBuf<double> st_d;
+  DevBuf<int> st_i;
+  DevBuf<long long> st_l;
   long long h_total = 0;
   // stats of the last step
   long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
@@ -669,6 +681,7 @@ void alloc_sort(Ctx& c, PopHost& ph) {
   h.n_cells = nb * c.n_class;
   ph.chunk_hist_cap = 0;  // reallocated by the sort when needed
   h.chunk_hist = nullptr;
+  h.chunk_hist_len = 0;
   h.cell_count = dalloc<int>(o, h.n_cells);
   h.cell_start = dalloc<int>(o, h.n_cells + 1);
   h.kmax_tab = dalloc<double>(o, (size_t)nb * nb);
@@ -858,6 +871,7 @@ void prepare_chunks(Ctx& c) {
     if (need > ph.chunk_hist_cap) {
       int want = std::max(need * 2, 1024);  // headroom: slots grow inside a step
       ph.h.chunk_hist = dalloc<int>(ph.sort_allocs, want);
+      ph.h.chunk_hist_len = want;
       ph.chunk_hist_cap = want;
       c.dirty = true;
     }
@@ -1222,11 +1236,17 @@ __global__ void k_step_reset(PopCtr* ctrs, int n_pop) {
   if (k >= n_pop) return;
   ctrs[k].tot_samp = ctrs[k].tot_coag = ctrs[k].kmax_warn = ctrs[k].redraws = 0;
   ctrs[k].status = 0;
+  ctrs[k].bad_site = 0;
+  ctrs[k].bad_index = 0;
 }
 
 __global__ void k_fill_claims(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int n = P.ctr->n_slots;
+  if (n > P.cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) bad_index(P.ctr, kBadSlotCount, n);
+    n = P.cap;
+  }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     P.claim[i] = 0xffffffffu;
 }
@@ -1499,7 +1519,7 @@ const char* pmc_coag_gpu_status_string(int s) {
     case PMC_ERR_CUDA: return g_last_error[0] ? g_last_error : "CUDA error";
     case PMC_ERR_TIMEOUT: return "bounded device loop ran out of iterations";
     case PMC_ERR_RNG_EXHAUSTED: return "replay stream exhausted";
-    case PMC_ERR_ASSERT: return "reference assertion failed";
+    case PMC_ERR_ASSERT: return g_last_assert[0] ? g_last_assert : "reference assertion failed";
     case PMC_ERR_NO_DEVICE: return "no CUDA device";
   }
   return "unknown status";
@@ -1605,6 +1625,9 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.pp_res.release();
   c.pp_vol.release();
   c.replay_u.release();
+  c.st_d.release();
+  c.st_i.release();
+  c.st_l.release();
   replay_free(c.replay);
   cudaStreamDestroy(c.stream);
   delete x;
@@ -1617,35 +1640,36 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
   Ctx& c = x->c;
   GUARD_BEGIN
   PopHost& ph = c.pops[pop];
+  if (group)
+    for (int i = 0; i < n_part; i++)
+      if (group[i] < 1 || group[i] > c.n_group) return PMC_ERR_INVALID_ARG;
+  if (cls)
+    for (int i = 0; i < n_part; i++)
+      if (cls[i] < 1 || cls[i] > c.n_class) return PMC_ERR_INVALID_ARG;
   int cap = std::max(1024, n_part + n_part / 2 + 64);
   if (cap > ph.h.cap || cap < ph.h.cap / 4) {
     free_list(ph.slot_allocs);
     alloc_slots(c, ph, cap);
   }
   PopCtr r = read_ctr(c, pop);
+  CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
   if (n_part > 0) {
-    std::vector<void*> tmp;
-    double* dv = dalloc<double>(tmp, (size_t)n_part * c.n_spec);
-    int* dg = group ? dalloc<int>(tmp, n_part) : nullptr;
-    int* dc = cls ? dalloc<int>(tmp, n_part) : nullptr;
-    long long* di = id ? dalloc<long long>(tmp, n_part) : nullptr;
-    int* dn = n_primary ? dalloc<int>(tmp, n_part) : nullptr;
-    CK(cudaMemcpyAsync(dv, vol, sizeof(double) * n_part * c.n_spec, cudaMemcpyHostToDevice, c.stream));
-    if (dg) CK(cudaMemcpyAsync(dg, group, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
-    if (dc) CK(cudaMemcpyAsync(dc, cls, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
-    if (di) CK(cudaMemcpyAsync(di, id, sizeof(long long) * n_part, cudaMemcpyHostToDevice, c.stream));
-    if (dn) CK(cudaMemcpyAsync(dn, n_primary, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
+    size_t n = (size_t)n_part;
+    c.st_d.reserve(n * c.n_spec);
+    c.st_i.reserve(3 * n);
+    c.st_l.reserve(n);
+    double* dv = c.st_d.p;
+    int* dg = group ? c.st_i.p : nullptr;
+    int* dc = cls ? c.st_i.p + n : nullptr;
+    int* dn = n_primary ? c.st_i.p + 2 * n : nullptr;
+    long long* di = id ? c.st_l.p : nullptr;
+    CK(cudaMemcpyAsync(dv, vol, sizeof(double) * n * c.n_spec, cudaMemcpyHostToDevice, c.stream));
+    if (dg) CK(cudaMemcpyAsync(dg, group, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+    if (dc) CK(cudaMemcpyAsync(dc, cls, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+    if (di) CK(cudaMemcpyAsync(di, id, sizeof(long long) * n, cudaMemcpyHostToDevice, c.stream));
+    if (dn) CK(cudaMemcpyAsync(dn, n_primary, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
     long long id0 = r.next_id;
-    CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
     k_upload<<<grid_for(n_part, 256), 256, 0, c.stream>>>(ph.h, n_part, dv, dg, dc, di, dn, id0); note_launch();
-    CK(cudaStreamSynchronize(c.stream));
-    free_list(tmp);
-    if (group)
-      for (int i = 0; i < n_part; i++)
-        if (group[i] < 1 || group[i] > c.n_group) return PMC_ERR_INVALID_ARG;
-    if (cls)
-      for (int i = 0; i < n_part; i++)
-        if (cls[i] < 1 || cls[i] > c.n_class) return PMC_ERR_INVALID_ARG;
     if (id) {
       long long mx = 0;
       for (int i = 0; i < n_part; i++) mx = std::max<long long>(mx, id[i]);
@@ -1653,8 +1677,6 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
     } else {
       r.next_id = id0 + n_part;
     }
-  } else {
-    CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
   }
   r.n_slots = n_part;
   r.n_live = n_part;
@@ -1718,6 +1740,17 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
     k += r.tot_coag;
     warn += r.kmax_warn;
     if (r.status && !status) status = r.status;
+    if (r.bad_site) {
+      static const char* site[] = {"", "pair test: list position", "pair test: slot", "event: slot",
+                                   "sort scatter: list position", "sort: chunk histogram size",
+                                   "pair set-up: cell range", "slot count above capacity",
+                                   "event: destination slot"};
+      snprintf(g_last_assert, sizeof(g_last_assert),
+               "device bounds check failed (%s, population %d, index %lld)",
+               r.bad_site < 9 ? site[r.bad_site] : "?", p, r.bad_index);
+      status = PMC_ERR_ASSERT;
+      continue;  // no compaction of a population in this state
+    }
     // compact when more than half of the used slots are dead
     if (r.n_slots > 4096 && r.n_live < r.n_slots / 2) relayout(c, p, c.pops[p].h.cap, true);
   }
@@ -1804,19 +1837,22 @@ static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, i
   PopCtr r = read_ctr(c, pop);
   if (n_part) *n_part = r.n_live;
   if (r.n_live > max_part) return PMC_ERR_CAPACITY;
-  std::vector<void*> tmp;
-  long long* off = dalloc<long long>(tmp, (size_t)r.n_slots + 1);
+  size_t ns = (size_t)r.n_slots + 1;
+  size_t n = std::max(r.n_live, 1);
+  c.st_l.reserve(ns + n);
+  c.st_d.reserve(n * (c.n_spec + kMaxComponent));
+  c.st_i.reserve(n * (4 + kMaxComponent));
+  long long* off = c.st_l.p;
   long long nl = scan(c, ph.h.alive, r.n_slots, off, true);
   if (nl != r.n_live) return PMC_ERR_ASSERT;
-  size_t n = std::max<long long>(nl, 1);
-  double* dv = dalloc<double>(tmp, n * c.n_spec);
-  int* dg = dalloc<int>(tmp, n);
-  int* dc = dalloc<int>(tmp, n);
-  long long* di = dalloc<long long>(tmp, n);
-  int* dn = dalloc<int>(tmp, n);
-  int* dnc = dalloc<int>(tmp, n);
-  int* dcs = dalloc<int>(tmp, n * kMaxComponent);
-  double* dct = dalloc<double>(tmp, n * kMaxComponent);
+  long long* di = c.st_l.p + ns;
+  double* dv = c.st_d.p;
+  double* dct = c.st_d.p + n * c.n_spec;
+  int* dg = c.st_i.p;
+  int* dc = dg + n;
+  int* dn = dc + n;
+  int* dnc = dn + n;
+  int* dcs = dnc + n;
   if (r.n_slots > 0)
     k_download<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(ph.h, off, r.n_slots, dv, dg, dc, di, dn,
                                                                 dnc, dcs, dct); note_launch();
@@ -1831,7 +1867,6 @@ static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, i
     if (comp_time) CK(cudaMemcpyAsync(comp_time, dct, sizeof(double) * nl * kMaxComponent, cudaMemcpyDeviceToHost, c.stream));
   }
   CK(cudaStreamSynchronize(c.stream));
-  free_list(tmp);
   return PMC_OK;
 }
 

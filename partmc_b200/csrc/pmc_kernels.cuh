@@ -43,6 +43,19 @@ enum Stream : uint32_t {
 
 __device__ __forceinline__ void set_status(PopCtr* c, int code) { atomicCAS(&c->status, 0, code); }
 
+// a failed bounds check: record the first site and index, flag the step
+__device__ __noinline__ void bad_index(PopCtr* c, int site, long long idx) {
+  if (atomicCAS(&c->bad_site, 0, site) == 0) c->bad_index = idx;
+  set_status(c, kErrAssert);
+}
+
+// the chunk histogram of the current slot count fits its allocation
+__device__ __forceinline__ bool chunk_hist_fits(const PopDev& P, int n_chunks) {
+  if ((long long)n_chunks * P.n_cells <= (long long)P.chunk_hist_len) return true;
+  bad_index(P.ctr, kBadChunkHist, (long long)n_chunks * P.n_cells);
+  return false;
+}
+
 __device__ __forceinline__ void add_ll(long long* p, long long v) {
   atomicAdd((unsigned long long*)p, (unsigned long long)v);
 }
@@ -66,7 +79,9 @@ __device__ __forceinline__ Rng make_rng(const PopDev& P, uint32_t stream, uint32
 __global__ void k_sort_hist(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int chunk = blockIdx.x;
-  if (chunk >= n_chunks_of(P)) return;
+  int n_chunks = n_chunks_of(P);
+  if (chunk >= n_chunks) return;
+  if (!chunk_hist_fits(P, n_chunks)) return;
   extern __shared__ int sh[];
   int nc = P.n_cells;
   for (int c = threadIdx.x; c < nc; c += blockDim.x) sh[c] = 0;
@@ -128,6 +143,7 @@ __global__ void k_sort_count(const PopDev* pops) {
   int nc = P.n_cells;
   int s = 0;
   int n_chunks = n_chunks_of(P);
+  if (!chunk_hist_fits(P, n_chunks)) return;
   for (int k = threadIdx.x; k < n_chunks; k += blockDim.x) s += P.chunk_hist[(size_t)k * nc + c];
   int tot;
   block_excl_scan(s, &tot);
@@ -158,6 +174,7 @@ __global__ void k_sort_offsets(const PopDev* pops) {
   }
   int run = start;
   int n_chunks = n_chunks_of(P);
+  if (!chunk_hist_fits(P, n_chunks)) return;
   for (int base = 0; base < n_chunks; base += blockDim.x) {
     int k = base + threadIdx.x;
     int h = k < n_chunks ? P.chunk_hist[(size_t)k * nc + c] : 0;
@@ -235,7 +252,9 @@ __global__ void k_refresh_all(const PopDev* pops, const uint8_t* on) {
 __global__ void k_sort_scatter(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int chunk = blockIdx.x;
-  if (chunk >= n_chunks_of(P)) return;
+  int n_chunks = n_chunks_of(P);
+  if (chunk >= n_chunks) return;
+  if (!chunk_hist_fits(P, n_chunks)) return;
   extern __shared__ int wc[];  // [kSortWarps][n_cells]
   int nc = P.n_cells;
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -277,7 +296,10 @@ __global__ void k_sort_scatter(const PopDev* pops) {
     __syncwarp();
     if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
     __syncwarp();
-    if (key >= 0) P.list[pos] = i;
+    if (key >= 0) {
+      if (pos >= 0 && pos < P.cap) P.list[pos] = i;
+      else bad_index(P.ctr, kBadScatterPos, pos);
+    }
   }
 }
 
@@ -319,6 +341,10 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
   S.n2 = n2;
   S.start1 = P.cell_start[cell1];
   S.start2 = P.cell_start[cell2];
+  if (S.start1 < 0 || (long long)S.start1 + n1 > P.cap || S.start2 < 0 || (long long)S.start2 + n2 > P.cap) {
+    bad_index(P.ctr, kBadPairCells, p);
+    S.n1 = S.n2 = n1 = n2 = 0;
+  }
   bool same = (b1 == b2) && (c1 == c2);
   if (*P.round_p > 0) {
     // redraws of lost samples; a per-particle pair is not redone
@@ -476,7 +502,17 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
       if (i2 >= n2) i2 = n2 - 1;
     }
     int e1 = S.start1 + i1, e2 = S.start2 + i2;
+    if (e1 < 0 || e1 >= P.cap || e2 < 0 || e2 >= P.cap) {
+      bad_index(P.ctr, kBadTestPos, e1 < 0 || e1 >= P.cap ? e1 : e2);
+      flag[w] = 0;
+      continue;
+    }
     int s1 = P.list[e1], s2 = P.list[e2];
+    if (s1 < 0 || s1 >= P.cap || s2 < 0 || s2 >= P.cap) {
+      bad_index(P.ctr, kBadTestSlot, s1 < 0 || s1 >= P.cap ? s1 : s2);
+      flag[w] = 0;
+      continue;
+    }
     T k;
     if constexpr (sizeof(T) == 8) {
       const double* q1 = (const double*)&P.recd[s1];

@@ -70,6 +70,13 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const in
     long long s = w - work_off[gp];
     unsigned prio = (unsigned)(prio_off[gp] + s);
     int2 sl = ev[w];
+    if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
+      bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+      win[e] = 0;
+      need_slot[e] = 0;
+      need_id[e] = 0;
+      continue;
+    }
     bool winner = P.claim[sl.x] == prio && P.claim[sl.y] == prio;
     win[e] = winner ? 1 : 0;
     need_slot[e] = 0;
@@ -141,6 +148,10 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int*
       else c.id = id_base[pop] + id_rank[e];
       if (dest >= P.cap) {
         set_status(P.ctr, kErrCapacity);
+        continue;
+      }
+      if (dest < 0) {
+        bad_index(P.ctr, kBadDest, dest);
         continue;
       }
       store_particle(P, dest, v, c);

@@ -87,6 +87,21 @@ struct PopCtr {
   int losers;
   int n_events;
   long long rng_used;      // replay: uniforms consumed
+  int bad_site;            // first failed bounds check (kBad*), 0 if none
+  long long bad_index;     // the index that failed it
+};
+
+// sites of the device bounds checks (PopCtr::bad_site)
+enum : int {
+  kBadNone = 0,
+  kBadTestPos = 1,     // pair test: cell-list position outside the list
+  kBadTestSlot = 2,    // pair test: slot number outside the slots
+  kBadEventSlot = 3,   // accepted event names a slot outside the slots
+  kBadScatterPos = 4,  // sort scatter: list position outside the list
+  kBadChunkHist = 5,   // sort: chunk histogram larger than its allocation
+  kBadPairCells = 6,   // pair set-up: a cell runs past the list
+  kBadSlotCount = 7,   // slot count above the capacity
+  kBadDest = 8,        // event destination slot outside the slots
 };
 
 // One population as the kernels see it (kept in device memory).
@@ -133,6 +148,7 @@ struct PopDev {
   // sort
   GridDev* grid;
   int* chunk_hist;  // [n_chunks][n_cells]
+  int chunk_hist_len;  // ints allocated at chunk_hist
   int* cell_count;  // [n_cells]
   int* cell_start;  // [n_cells + 1]
   int* list;        // [cap] slot numbers in cell order
