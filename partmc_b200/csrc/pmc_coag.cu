@@ -26,10 +26,14 @@ namespace {
 inline void note_launch();
 
 // ---------------------------------------------------------------------------
-// exclusive scan of n values into out[0..n] (out[n] = total), three kernels
-constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 4;
+// exclusive scan of n values into out[0..n] (out[n] = total): one
+// single-pass launch with decoupled look-back, for up to kScanMaxJobs arrays
+// of the same element type at once (blockIdx.y selects the array)
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kScanMaxJobs = 4;
+constexpr int kScanSpinLimit = 1 << 20;  // bounded wait on a predecessor tile
 
 // the element count is n, or *nd when nd is given (a count that only the
 // device knows; n is then its upper bound)
@@ -37,26 +41,6 @@ __device__ __forceinline__ long long scan_n(long long n, const long long* nd) {
   if (!nd) return n;
   long long m = *nd;
   return m < n ? m : n;
-}
-
-template <class T>
-__global__ void k_scan_reduce(const T* in, long long n_max, const long long* nd, long long* bsum) {
-  long long n = scan_n(n_max, nd);
-  long long base = (long long)blockIdx.x * kScanTile;
-  long long s = 0;
-  for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
-    long long i = base + k;
-    if (i < n) s += (long long)in[i];
-  }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  __shared__ long long ws[32];
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += ws[k];
-    bsum[blockIdx.x] = t;
-  }
 }
 
 __device__ long long block_excl_scan_ll(long long v, long long* total) {
@@ -85,40 +69,95 @@ __device__ long long block_excl_scan_ll(long long v, long long* total) {
   return pre;
 }
 
-// exclusive scan of the block sums, in place (single block, any count);
-// the total goes to out[n]
-__global__ void k_scan_bsum(long long* bsum, int nb, long long* out, long long n_max, const long long* nd) {
-  long long* out_total = out + scan_n(n_max, nd);
-  long long carry = 0;
-  for (int base = 0; base < nb; base += blockDim.x) {
-    int i = base + threadIdx.x;
-    long long v = i < nb ? bsum[i] : 0;
-    long long tot;
-    long long pre = block_excl_scan_ll(v, &tot);
-    if (i < nb) bsum[i] = carry + pre;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) *out_total = carry;
+struct ScanJob {
+  const void* in;
+  long long* out;
+  long long n_max;
+  const long long* nd;
+};
+struct ScanJobs {
+  ScanJob j[kScanMaxJobs];
+};
+
+// tile status word: epoch (20 bits) | flag (2 bits: 1 aggregate, 2 inclusive
+// prefix) | value (42 bits).  A word from another launch has another epoch,
+// so the status array needs no reset between launches.
+__device__ __forceinline__ unsigned long long scan_word(uint32_t epoch, unsigned flag, long long v) {
+  return ((unsigned long long)(epoch & 0xFFFFFu) << 44) | ((unsigned long long)flag << 42) |
+         ((unsigned long long)v & ((1ULL << 42) - 1));
 }
 
 template <class T>
-__global__ void k_scan_final(const T* in, long long n_max, const long long* nd, const long long* bsum,
-                             long long* out) {
-  long long n = scan_n(n_max, nd);
-  long long base = (long long)blockIdx.x * kScanTile;
+__global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigned long long* status,
+                                                          int status_stride, unsigned* tile_ctr,
+                                                          uint32_t epoch, unsigned long long* err) {
+  const ScanJob J = jobs.j[blockIdx.y];
+  __shared__ unsigned tile_sh;
+  __shared__ long long carry_sh;
+  if (threadIdx.x == 0) {
+    // tiles in the order blocks start, so a tile only waits on running blocks
+    unsigned t = atomicAdd(&tile_ctr[blockIdx.y], 1u);
+    if (t == gridDim.x - 1) tile_ctr[blockIdx.y] = 0;  // the last claimant re-arms the counter
+    tile_sh = t;
+  }
+  __syncthreads();
+  long long tile = tile_sh;
+  long long n = scan_n(J.n_max, J.nd);
+  long long nb = (n + kScanTile - 1) / kScanTile;
+  if (n <= 0) {
+    if (tile == 0 && threadIdx.x == 0) J.out[0] = 0;
+    return;
+  }
+  if (tile >= nb) return;
+  const T* in = (const T*)J.in;
+  long long base = tile * kScanTile + (long long)threadIdx.x * kScanItems;
   long long v[kScanItems];
   long long s = 0;
+#pragma unroll
   for (int k = 0; k < kScanItems; k++) {
-    long long i = base + (long long)threadIdx.x * kScanItems + k;
+    long long i = base + k;
     v[k] = i < n ? (long long)in[i] : 0;
     s += v[k];
   }
-  long long pre = block_excl_scan_ll(s, nullptr) + bsum[blockIdx.x];
-  for (int k = 0; k < kScanItems; k++) {
-    long long i = base + (long long)threadIdx.x * kScanItems + k;
-    if (i < n) out[i] = pre;
-    pre += v[k];
+  long long agg;
+  long long pre = block_excl_scan_ll(s, &agg);
+  unsigned long long* st = status + (size_t)blockIdx.y * status_stride;
+  if (threadIdx.x == 0) {
+    long long excl = 0;
+    if (tile == 0) {
+      atomicExch(&st[0], scan_word(epoch, 2u, agg));
+    } else {
+      atomicExch(&st[tile], scan_word(epoch, 1u, agg));
+      long long look = tile - 1;
+      int spins = 0;
+      while (look >= 0) {
+        unsigned long long w = *(volatile unsigned long long*)&st[look];
+        unsigned flag = (unsigned)((w >> 42) & 3u);
+        if ((uint32_t)(w >> 44) != (epoch & 0xFFFFFu) || flag == 0) {
+          if (++spins > kScanSpinLimit) {
+            atomicAdd(err, 1ULL);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        excl += (long long)(w & ((1ULL << 42) - 1));
+        if (flag == 2u) break;
+        look--;
+      }
+      atomicExch(&st[tile], scan_word(epoch, 2u, excl + agg));
+    }
+    carry_sh = excl;
   }
+  __syncthreads();
+  long long off = carry_sh + pre;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    long long i = base + k;
+    if (i < n) J.out[i] = off;
+    off += v[k];
+  }
+  if (tile == nb - 1 && threadIdx.x == 0) J.out[n] = carry_sh + agg;
 }
 
 // ---------------------------------------------------------------------------
@@ -130,11 +169,19 @@ __global__ void k_fill_u32(unsigned* p, long long n, unsigned v) {
     p[i] = v;
 }
 
+// accepted samples in sample order: event e gets its sample index, its two
+// slots and its global pair
 __global__ void k_compact_flags(const uint8_t* flag, const long long* off, long long n,
-                                long long* outw) {
+                                long long* outw, const int2* ev, const int* ev_gp, int2* ev_c,
+                                int* gp_c) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
-    if (flag[i]) outw[off[i]] = i;
+    if (flag[i]) {
+      long long e = off[i];
+      outw[e] = i;
+      ev_c[e] = ev[i];
+      gp_c[e] = ev_gp[i];
+    }
 }
 
 // target operations of round 0, in the reference's backwards target order
@@ -179,73 +226,80 @@ __global__ void k_build_redo(const int* op_pop, const int* op_pair, const int* o
   }
 }
 
-// per-population bases of the allocations of one round: events are ordered
-// by population, so a global exclusive rank minus the count of earlier
-// populations is the rank inside the population.
-__global__ void k_alloc_bases(const PopDev* pops, int n_pop, const int* set_slots,
-                              const int* set_ids, const int* pp_slots, const int* pp_ids,
+// Per-population bases of the allocations of one round.  Events and target
+// operations are ordered by population, so a global exclusive rank minus the
+// count of earlier populations is the rank inside the population.  Per-set
+// counts come from the rank scans at the population boundaries (and are
+// stored in per_pop for the host); per-particle counts were summed into
+// per_pop by k_count_per_pop.  The slot and ID counters of each population
+// advance here by the round's allocations: the apply kernels read only the
+// bases.  One block; populations in tiles of blockDim.x.
+__global__ void k_alloc_bases(const PopDev* pops, int n_pop, const long long* pop_pair_base,
+                              const long long* work_off, const long long* flag_off, int has_set,
+                              const long long* rank_slot_set, const long long* rank_id_set, int* per_pop,
                               int* set_slot_base, long long* set_id_base, int* pp_slot_base,
                               long long* pp_id_base) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  long long cs = 0, ci = 0, ps = 0, pi = 0;
-  for (int k = 0; k < n_pop; k++) {
-    PopCtr* c = pops[k].ctr;
-    set_slot_base[k] = c->n_slots - (int)cs;
-    set_id_base[k] = c->next_id - ci;
-    pp_slot_base[k] = c->n_slots + set_slots[k] - (int)ps;
-    pp_id_base[k] = c->next_id + set_ids[k] - pi;
-    cs += set_slots[k];
-    ci += set_ids[k];
-    ps += pp_slots[k];
-    pi += pp_ids[k];
+  long long carry[4] = {0, 0, 0, 0};
+  for (int base = 0; base < n_pop; base += blockDim.x) {
+    int k = base + threadIdx.x;
+    long long cnt[4] = {0, 0, 0, 0};
+    if (k < n_pop) {
+      if (has_set) {
+        long long e_lo = flag_off[work_off[pop_pair_base[k]]];
+        long long e_hi = flag_off[work_off[pop_pair_base[k + 1]]];
+        cnt[0] = rank_slot_set[e_hi] - rank_slot_set[e_lo];
+        cnt[1] = rank_id_set[e_hi] - rank_id_set[e_lo];
+        per_pop[k] = (int)cnt[0];
+        per_pop[n_pop + k] = (int)cnt[1];
+      }
+      cnt[2] = per_pop[2 * n_pop + k];
+      cnt[3] = per_pop[3 * n_pop + k];
+    }
+    long long pre[4], tot[4];
+    for (int j = 0; j < 4; j++) pre[j] = block_excl_scan_ll(cnt[j], &tot[j]);
+    if (k < n_pop) {
+      PopCtr* c = pops[k].ctr;
+      long long cs = carry[0] + pre[0], ci = carry[1] + pre[1], ps = carry[2] + pre[2], pi = carry[3] + pre[3];
+      set_slot_base[k] = c->n_slots - (int)cs;
+      set_id_base[k] = c->next_id - ci;
+      pp_slot_base[k] = c->n_slots + (int)cnt[0] - (int)ps;
+      pp_id_base[k] = c->next_id + cnt[1] - pi;
+      c->n_slots += (int)(cnt[0] + cnt[2]);
+      c->next_id += cnt[1] + cnt[3];
+    }
+    for (int j = 0; j < 4; j++) carry[j] += tot[j];
   }
 }
 
+// need[q] of target operation q summed per population (op_pop[q])
 __global__ void k_count_per_pop(const int* need, const long long* n_items, const int* item_pop_of,
-                                const long long* ev_w, const long long* work_off, int n_gpairs,
-                                const int* gpair_pop, int* per_pop) {
-  // need[e] summed per population; population of item e is item_pop_of[e]
-  // when given, else found through ev_w/work_off (per-set events)
+                                int* per_pop) {
   long long n = *n_items;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
     if (!need[e]) continue;
-    int pop;
-    if (item_pop_of) pop = item_pop_of[e];
-    else pop = gpair_pop[find_pair(work_off, n_gpairs, ev_w[e])];
-    atomicAdd(&per_pop[pop], need[e]);
+    atomicAdd(&per_pop[item_pop_of[e]], need[e]);
   }
 }
 
-__global__ void k_alloc_finish(const PopDev* pops, int n_pop, const int* set_slots,
-                               const int* set_ids, const int* pp_slots, const int* pp_ids) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_pop) return;
-  PopCtr* c = pops[k].ctr;
-  c->n_slots += set_slots[k] + pp_slots[k];
-  c->next_id += set_ids[k] + pp_ids[k];
-}
-
-// particle upload: transpose particle-major volumes into species-major slots
-__global__ void k_upload(PopDev P, int n, const double* vol_pm, const int* grp, const int* cls,
-                         const long long* id, const int* nprim, long long id0) {
+// particle upload: the caller's arrays were copied straight into slots
+// 0..n-1 (same particle-major layout); fill the caches and the fields the
+// caller did not give
+__global__ void k_upload(PopDev P, int n, int have_grp, int have_cls, int have_id, int have_nprim,
+                         long long id0) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double vt = 0.0, ms = 0.0;
-    for (int s = 0; s < P.n_spec; s++) {
-      double v = vol_pm[(size_t)i * P.n_spec + s];
-      P.vol[(size_t)s * P.cap + i] = v;
-      vt = vt + v;
-    }
-    for (int s = 0; s < P.n_spec; s++) ms = ms + P.vol[(size_t)s * P.cap + i] * P.density[s];
+    for (int s = 0; s < P.n_spec; s++) vt = vt + P.vol[vol_at(P, i, s)];
+    for (int s = 0; s < P.n_spec; s++) ms = ms + P.vol[vol_at(P, i, s)] * P.density[s];
     P.vtot[i] = vt;
     P.mass[i] = ms;
-    P.grp[i] = grp ? grp[i] : 1;
-    P.cls[i] = cls ? cls[i] : 1;
-    P.id[i] = id ? id[i] : id0 + i;
-    P.nprim[i] = nprim ? nprim[i] : 1;
+    if (!have_grp) P.grp[i] = 1;
+    if (!have_cls) P.cls[i] = 1;
+    if (!have_id) P.id[i] = id0 + i;
+    if (!have_nprim) P.nprim[i] = 1;
     P.ncomp[i] = 1;
-    P.csrc[i] = 1;
-    P.ctime[i] = 0.0;
+    P.csrc[comp_at(i, 0)] = 1;
+    P.ctime[comp_at(i, 0)] = 0.0;
     P.lct[i] = 0.0;
     P.gct[i] = 0.0;
     P.imf[i] = 0.0;
@@ -258,23 +312,26 @@ __global__ void k_upload(PopDev P, int n, const double* vol_pm, const int* grp, 
   }
 }
 
-// gather live slots in slot order into the particle-major output
 __global__ void k_download(PopDev P, const long long* live_off, int n_slots, double* vol_pm,
                            int* grp, int* cls, long long* id, int* nprim, int* ncomp, int* csrc,
                            double* ctime) {
+  // only the fields asked for (non-null outputs) are gathered
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += gridDim.x * blockDim.x) {
     if (!P.alive[i]) continue;
     long long j = live_off[i];
-    for (int s = 0; s < P.n_spec; s++) vol_pm[j * P.n_spec + s] = P.vol[(size_t)s * P.cap + i];
-    grp[j] = P.grp[i];
-    cls[j] = P.cls[i];
-    id[j] = P.id[i];
-    nprim[j] = P.nprim[i];
-    ncomp[j] = P.ncomp[i];
-    for (int k = 0; k < kMaxComponent; k++) {
-      csrc[j * kMaxComponent + k] = k < P.ncomp[i] ? P.csrc[(size_t)k * P.cap + i] : 0;
-      ctime[j * kMaxComponent + k] = k < P.ncomp[i] ? P.ctime[(size_t)k * P.cap + i] : 0.0;
-    }
+    if (vol_pm)
+      for (int s = 0; s < P.n_spec; s++) vol_pm[j * P.n_spec + s] = P.vol[vol_at(P, i, s)];
+    if (grp) grp[j] = P.grp[i];
+    if (cls) cls[j] = P.cls[i];
+    if (id) id[j] = P.id[i];
+    if (nprim) nprim[j] = P.nprim[i];
+    if (ncomp) ncomp[j] = P.ncomp[i];
+    if (csrc)
+      for (int k = 0; k < kMaxComponent; k++)
+        csrc[j * kMaxComponent + k] = k < P.ncomp[i] ? P.csrc[comp_at(i, k)] : 0;
+    if (ctime)
+      for (int k = 0; k < kMaxComponent; k++)
+        ctime[j * kMaxComponent + k] = k < P.ncomp[i] ? P.ctime[comp_at(i, k)] : 0.0;
   }
 }
 
@@ -284,7 +341,7 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += gridDim.x * blockDim.x) {
     if (compact && !S.alive[i]) continue;
     int j = compact ? (int)live_off[i] : i;
-    for (int s = 0; s < S.n_spec; s++) D.vol[(size_t)s * D.cap + j] = S.vol[(size_t)s * S.cap + i];
+    for (int s = 0; s < S.n_spec; s++) D.vol[vol_at(D, j, s)] = S.vol[vol_at(S, i, s)];
     D.vtot[j] = S.vtot[i];
     D.mass[j] = S.mass[i];
     D.rad[j] = S.rad[i];
@@ -294,8 +351,8 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.nprim[j] = S.nprim[i];
     D.ncomp[j] = S.ncomp[i];
     for (int k = 0; k < S.ncomp[i]; k++) {
-      D.csrc[(size_t)k * D.cap + j] = S.csrc[(size_t)k * S.cap + i];
-      D.ctime[(size_t)k * D.cap + j] = S.ctime[(size_t)k * S.cap + i];
+      D.csrc[comp_at(j, k)] = S.csrc[comp_at(i, k)];
+      D.ctime[comp_at(j, k)] = S.ctime[comp_at(i, k)];
     }
     D.lct[j] = S.lct[i];
     D.gct[j] = S.gct[i];
@@ -462,7 +519,8 @@ struct Ctx {
   std::vector<PopHost> pops;
   PopDev* d_pops = nullptr;
   PopCtr* d_ctrs = nullptr;  // one counter block per population
-  uint32_t* d_round = nullptr;  // round of the current step, read by the kernels
+  uint32_t* d_round = nullptr;  // [round of the current step, claim generation], read by the kernels
+  uint32_t claim_gen = 0;
   bool dirty = true;            // host PopDev copies changed since the last push
   std::vector<PopCtr> h_ctrs;
   cudaStream_t stream = nullptr;
@@ -473,6 +531,10 @@ struct Ctx {
   DevBuf<long long> nwork_set, nwork_pp, nprio, work_off, pp_off, prio_off;
   DevBuf<int> pair_losers;
   DevBuf<uint8_t> flag, win_set, win_pp;
+  DevBuf<uint32_t> dec_set;  // merge decision of each accepted per-set event
+  DevBuf<int> ev_gp, gp_c;   // global pair of each accepted sample / event
+  DevBuf<int2> ev_c;         // slots of each event
+  DevBuf<double2> ice_set;   // water volumes of the sources of each event
   DevBuf<int2> ev;
   DevBuf<long long> flag_off, ev_w;
   DevBuf<int> need_slot_set, need_id_set, need_slot_pp, need_id_pp, lost_pp;
@@ -484,7 +546,11 @@ struct Ctx {
   DevBuf<int> per_pop_i;  // 4 x n_pop counters
   DevBuf<int> slot_base_set, slot_base_pp;
   DevBuf<long long> id_base_set, id_base_pp;
-  DevBuf<long long> scan_bsum, scan_total;
+  DevBuf<unsigned long long> scan_status;  // look-back tile words
+  size_t scan_status_n = 0;                // words cleared so far
+  DevBuf<unsigned> scan_ctr;               // per-job tile counters (re-armed by the kernel)
+  DevBuf<unsigned long long> scan_err;     // look-backs that gave up
+  uint32_t scan_epoch = 0;
   DevBuf<long long> n_dev;  // device scalars
   // staging for upload / download (shared by all populations; every call
   // synchronises before it returns)
@@ -587,16 +653,63 @@ void prof_collect(Ctx& c) {
   c.prof_pending.clear();
 }
 
-// exclusive scan of in[0..n) into out[0..n] (out[n] = total).  With nd, the
+// exclusive scans of in[0..n) into out[0..n] (out[n] = total), up to
+// kScanMaxJobs arrays of one element type in one launch.  With nd, a job's
 // count is *nd (device memory) and n only bounds it.
 template <class T>
+struct ScanArg {
+  const T* in;
+  long long n;
+  const long long* nd;
+  long long* out;
+};
+
+template <class T>
+void scan_multi(Ctx& c, std::initializer_list<ScanArg<T>> args) {
+  ScanJobs jobs{};
+  int k = 0;
+  long long nb = 1;
+  for (const auto& a : args) {
+    jobs.j[k].in = a.in;
+    jobs.j[k].out = a.out;
+    jobs.j[k].n_max = a.n;
+    jobs.j[k].nd = a.nd;
+    nb = std::max(nb, (a.n + kScanTile - 1) / kScanTile);
+    k++;
+  }
+  if (k == 0) return;
+  if (nb > (1LL << 30)) throw Fail(PMC_ERR_CAPACITY);
+  c.scan_status.reserve((size_t)kScanMaxJobs * nb);
+  if (c.scan_status.n > c.scan_status_n) {  // fresh memory: clear it once
+    CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, c.stream));
+    c.scan_status_n = c.scan_status.n;
+  }
+  c.scan_epoch = (c.scan_epoch + 1) & 0xFFFFFu;
+  if (c.scan_epoch == 0) {
+    // the epoch wrapped: old words could match again, so clear them
+    CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, c.stream));
+    c.scan_epoch = 1;
+  }
+  dim3 g((unsigned)nb, (unsigned)k);
+  k_scan_lb<T><<<g, kScanThreads, 0, c.stream>>>(jobs, c.scan_status.p, (int)nb, c.scan_ctr.p, c.scan_epoch,
+                                                  c.scan_err.p);
+  note_launch();
+}
+
+template <class T>
 void scan_dev(Ctx& c, const T* in, long long n, const long long* nd, long long* out) {
-  int nb = (int)((n + kScanTile - 1) / kScanTile);
-  if (nb < 1) nb = 1;
-  c.scan_bsum.reserve(nb + 1);
-  k_scan_reduce<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, nd, c.scan_bsum.p); note_launch();
-  k_scan_bsum<<<1, kScanThreads, 0, c.stream>>>(c.scan_bsum.p, nb, out, n, nd); note_launch();
-  k_scan_final<T><<<nb, kScanThreads, 0, c.stream>>>(in, n, nd, c.scan_bsum.p, out); note_launch();
+  scan_multi<T>(c, {ScanArg<T>{in, n, nd, out}});
+}
+
+// a look-back that gave up is reported as a timed-out step
+void check_scan_err(Ctx& c) {
+  unsigned long long e = 0;
+  CK(cudaMemcpyAsync(&e, c.scan_err.p, sizeof(e), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  if (e) {
+    CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(e), c.stream));
+    throw Fail(PMC_ERR_TIMEOUT);
+  }
 }
 
 template <class T>
@@ -606,6 +719,7 @@ long long scan(Ctx& c, const T* in, long long n, long long* out, bool read_total
   long long t = 0;
   CK(cudaMemcpyAsync(&t, out + n, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
+  check_scan_err(c);
   return t;
 }
 
@@ -614,6 +728,7 @@ void push_pops(Ctx& c) {
   for (int k = 0; k < c.n_pop; k++) {
     v[k] = c.pops[k].h;
     v[k].round_p = c.d_round;
+    v[k].gen_p = c.d_round + 1;
   }
   CK(cudaMemcpyAsync(c.d_pops, v.data(), sizeof(PopDev) * c.n_pop, cudaMemcpyHostToDevice, c.stream));
   c.dirty = false;
@@ -667,8 +782,9 @@ void alloc_slots(Ctx& c, PopHost& ph, int cap) {
   h.list = dalloc<int>(o, cap);
   h.recd = dalloc<RecD>(o, cap);
   h.recf = dalloc<RecF>(o, cap);
-  h.claim = dalloc<unsigned>(o, cap);
+  h.claim = dalloc<unsigned long long>(o, cap);
   CK(cudaMemsetAsync(h.alive, 0, cap, c.stream));
+  CK(cudaMemsetAsync(h.claim, 0xff, sizeof(unsigned long long) * cap, c.stream));  // no claim
   c.dirty = true;
 }
 
@@ -707,6 +823,7 @@ void alloc_sort(Ctx& c, PopHost& ph) {
   h.pair_desc = pd;
   h.pair = dalloc<PairState>(o, std::max<size_t>(ph.pair_desc.size(), 1));
   h.kmax_valid = 0;
+  h.pair_setup_valid = 0;
   c.dirty = true;
 }
 
@@ -765,6 +882,7 @@ void set_params(Ctx& c, PopHost& ph) {
   h.dmin = *std::min_element(c.density.begin(), c.density.end());
   h.dmax = *std::max_element(c.density.begin(), c.density.end());
   h.seed = ph.seed;
+  h.pair_setup_valid = 0;  // the per-pair weight factors depend on the weights
   c.dirty = true;
 }
 
@@ -1042,40 +1160,41 @@ void sort_pops(Ctx& c, bool decide_grid) {
 // one step over all populations
 
 template <int KT, class T>
-void launch_test(Ctx& c, bool flat, int n_gpairs) {
-  int blocks = 148 * 8;
+void launch_test(Ctx& c, bool flat, int n_gpairs, long long W) {
+  // sized from the round's sample count: redraw rounds are small
+  int blocks = (int)std::min<long long>(148 * 8, std::max<long long>(1, (W + 255) / 256));
   if (flat)
     k_test<KT, T, true><<<blocks, 256, 0, c.stream>>>(
         c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
-        c.work_off.p + n_gpairs, c.flag.p, c.ev.p);
+        c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
   else
     k_test<KT, T, false><<<blocks, 256, 0, c.stream>>>(
         c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
-        c.work_off.p + n_gpairs, c.flag.p, c.ev.p);
+        c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
   note_launch();
 }
 
-void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs) {
+void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W) {
   bool f32 = c.mode == PMC_MODE_MIXED;
   switch (kt) {
     case kKernelAdditive:
-      f32 ? launch_test<kKernelAdditive, float>(c, flat, n_gpairs)
-          : launch_test<kKernelAdditive, double>(c, flat, n_gpairs);
+      f32 ? launch_test<kKernelAdditive, float>(c, flat, n_gpairs, W)
+          : launch_test<kKernelAdditive, double>(c, flat, n_gpairs, W);
       break;
     case kKernelConstant:
-      f32 ? launch_test<kKernelConstant, float>(c, flat, n_gpairs)
-          : launch_test<kKernelConstant, double>(c, flat, n_gpairs);
+      f32 ? launch_test<kKernelConstant, float>(c, flat, n_gpairs, W)
+          : launch_test<kKernelConstant, double>(c, flat, n_gpairs, W);
       break;
     case kKernelBrown:
-      f32 ? launch_test<kKernelBrown, float>(c, flat, n_gpairs)
-          : launch_test<kKernelBrown, double>(c, flat, n_gpairs);
+      f32 ? launch_test<kKernelBrown, float>(c, flat, n_gpairs, W)
+          : launch_test<kKernelBrown, double>(c, flat, n_gpairs, W);
       break;
     case kKernelSedi:
-      f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs)
-          : launch_test<kKernelSedi, double>(c, flat, n_gpairs);
+      f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs, W)
+          : launch_test<kKernelSedi, double>(c, flat, n_gpairs, W);
       break;
     default:
-      launch_test<kKernelZero, double>(c, flat, n_gpairs);
+      launch_test<kKernelZero, double>(c, flat, n_gpairs, W);
   }
 }
 
@@ -1248,7 +1367,7 @@ __global__ void k_fill_claims(const PopDev* pops) {
     n = P.cap;
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    P.claim[i] = 0xffffffffu;
+    P.claim[i] = ~0ULL;
 }
 
 // per-population work of a round: samples and target operations
@@ -1316,16 +1435,36 @@ void step_parallel(Ctx& c, int kt) {
   std::vector<int> per_pop(4 * (size_t)c.n_pop);
   int round = 0;
   for (;;) {
+    bool claims_wrapped = false;
     {
-      uint32_t r32 = (uint32_t)round;  // staged before the call returns
-      CK(cudaMemcpyAsync(c.d_round, &r32, sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+      // every round gets a new claim generation; when the counter wraps,
+      // the claim words are cleared once
+      c.claim_gen++;
+      if (c.claim_gen == 0xffffffffu) {
+        c.claim_gen = 0;
+        claims_wrapped = true;
+      }
+      uint32_t rg[2] = {(uint32_t)round, c.claim_gen};  // staged before the call returns
+      CK(cudaMemcpyAsync(c.d_round, rg, sizeof(rg), cudaMemcpyHostToDevice, c.stream));
     }
     if (c.dirty) push_pops(c);
     if (round > 0) sort_pops(c, false);
     if (round == 0) {
-      dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
-      k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
-      note_launch();
+      bool need_kmax = false, need_setup = false;
+      for (int k = 0; k < c.n_pop; k++) {
+        need_kmax = need_kmax || !c.pops[k].h.kmax_valid;
+        need_setup = need_setup || !c.pops[k].h.pair_setup_valid;
+      }
+      if (need_kmax) {
+        dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
+        k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
+        note_launch();
+      }
+      if (need_setup) {
+        dim3 g((unsigned)(((long long)max_pairs * 32 + 255) / 256), c.n_pop);
+        k_pair_setup<<<g, 256, 0, c.stream>>>(c.d_pops);
+        note_launch();
+      }
     }
     {
       dim3 gp((max_pairs + 127) / 128, c.n_pop);
@@ -1335,12 +1474,15 @@ void step_parallel(Ctx& c, int kt) {
     }
     if (round == 0) {
       // the device copies learn this with the next push
-      for (int k = 0; k < c.n_pop; k++) c.pops[k].h.kmax_valid = 1;
+      for (int k = 0; k < c.n_pop; k++) {
+        c.pops[k].h.kmax_valid = 1;
+        c.pops[k].h.pair_setup_valid = 1;
+      }
       c.dirty = true;
     }
-    scan_dev(c, c.nwork_set.p, n_gpairs, nullptr, c.work_off.p);
-    scan_dev(c, c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p);
-    scan_dev(c, c.nprio.p, n_gpairs, nullptr, c.prio_off.p);
+    scan_multi<long long>(c, {{c.nwork_set.p, n_gpairs, nullptr, c.work_off.p},
+                              {c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p},
+                              {c.nprio.p, n_gpairs, nullptr, c.prio_off.p}});
     long long* popw = c.n_dev.p + 4;
     k_pop_work<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.pop_pair_base.p, c.n_pop, c.work_off.p, c.pp_off.p,
                                                             popw);
@@ -1350,7 +1492,13 @@ void step_parallel(Ctx& c, int kt) {
     CK(cudaMemcpyAsync(&hw[1], c.pp_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(&hw[2], c.prio_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(&hw[3], popw, sizeof(long long) * 2 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+    unsigned long long pair_scan_err = 0;
+    CK(cudaMemcpyAsync(&pair_scan_err, c.scan_err.p, sizeof(pair_scan_err), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    if (pair_scan_err) {
+      CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(pair_scan_err), c.stream));
+      throw Fail(PMC_ERR_TIMEOUT);
+    }
     long long W = hw[0], Q0 = hw[1], Ptot = hw[2];
     long long Q = round == 0 ? Q0 : Qprev;
     if (Ptot + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
@@ -1371,6 +1519,11 @@ void step_parallel(Ctx& c, int kt) {
     c.need_slot_set.reserve(W + 1);
     c.need_id_set.reserve(W + 1);
     c.win_set.reserve(W + 1);
+    c.dec_set.reserve(W + 1);
+    c.ev_gp.reserve(W + 1);
+    c.gp_c.reserve(W + 1);
+    c.ev_c.reserve(W + 1);
+    c.ice_set.reserve(W + 1);
     c.rank_slot_set.reserve(W + 2);
     c.rank_id_set.reserve(W + 2);
     c.need_slot_pp.reserve(Q + 1);
@@ -1380,7 +1533,7 @@ void step_parallel(Ctx& c, int kt) {
     c.lost_off.reserve(Q + 2);
     c.rank_slot_pp.reserve(Q + 2);
     c.rank_id_pp.reserve(Q + 2);
-    {
+    if (claims_wrapped) {
       dim3 g(grid_for(max_cap, 256), c.n_pop);
       k_fill_claims<<<g, 256, 0, c.stream>>>(c.d_pops);
       note_launch();
@@ -1390,7 +1543,7 @@ void step_parallel(Ctx& c, int kt) {
     CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
     if (W > 0) {
       ProfScope ps(c, 0, W);
-      launch_test_kt(c, kt, flat, n_gpairs);
+      launch_test_kt(c, kt, flat, n_gpairs, W);
     }
     if (Q > 0) {
       if (round == 0) {
@@ -1410,44 +1563,43 @@ void step_parallel(Ctx& c, int kt) {
     const long long* Ed = c.flag_off.p + W;
     if (W > 0) {
       scan_dev(c, c.flag.p, W, nullptr, c.flag_off.p);
-      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, W, c.ev_w.p);
+      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, W, c.ev_w.p, c.ev.p,
+                                                             c.ev_gp.p, c.ev_c.p, c.gp_c.p);
       note_launch();
       k_resolve_set<<<grid_for(W, 256), 256, 0, c.stream>>>(
-          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs, Ed, c.ev_w.p, c.ev.p,
-          c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.round_dev.p);
+          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p,
+          c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p, c.round_dev.p);
       note_launch();
-      scan_dev(c, c.need_slot_set.p, W, Ed, c.rank_slot_set.p);
-      scan_dev(c, c.need_id_set.p, W, Ed, c.rank_id_set.p);
-      k_count_per_pop<<<grid_for(W, 256), 256, 0, c.stream>>>(c.need_slot_set.p, Ed, nullptr, c.ev_w.p, c.work_off.p,
-                                                             n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 0 * c.n_pop);
-      note_launch();
-      k_count_per_pop<<<grid_for(W, 256), 256, 0, c.stream>>>(c.need_id_set.p, Ed, nullptr, c.ev_w.p, c.work_off.p,
-                                                             n_gpairs, c.gpair_pop.p, c.per_pop_i.p + 1 * c.n_pop);
-      note_launch();
+      scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}});
     }
     if (Q > 0) {
       set_n_dev(c, Q);
       k_pp_resolve<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_prio.p, c.n_dev.p, c.pp_res.p,
                                                            c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
       note_launch();
-      scan_dev(c, c.need_slot_pp.p, Q, nullptr, c.rank_slot_pp.p);
-      scan_dev(c, c.need_id_pp.p, Q, nullptr, c.rank_id_pp.p);
-      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p, nullptr,
-                                                             nullptr, 0, nullptr, c.per_pop_i.p + 2 * c.n_pop);
+      scan_multi<int>(c, {{c.need_slot_pp.p, Q, nullptr, c.rank_slot_pp.p},
+                          {c.need_id_pp.p, Q, nullptr, c.rank_id_pp.p}});
+      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p,
+                                                             c.per_pop_i.p + 2 * c.n_pop);
       note_launch();
-      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p, nullptr, nullptr,
-                                                             0, nullptr, c.per_pop_i.p + 3 * c.n_pop);
+      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p,
+                                                             c.per_pop_i.p + 3 * c.n_pop);
       note_launch();
     }
-    k_alloc_bases<<<1, 1, 0, c.stream>>>(c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop, c.per_pop_i.p + 1 * c.n_pop,
-                                         c.per_pop_i.p + 2 * c.n_pop, c.per_pop_i.p + 3 * c.n_pop, c.slot_base_set.p,
-                                         c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p);
+    k_alloc_bases<<<1, 256, 0, c.stream>>>(c.d_pops, c.n_pop, c.pop_pair_base.p, c.work_off.p, c.flag_off.p,
+                                           W > 0 ? 1 : 0, c.rank_slot_set.p, c.rank_id_set.p, c.per_pop_i.p,
+                                           c.slot_base_set.p, c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p);
     note_launch();
     if (W > 0) {
-      k_apply_set<<<grid_for(W, 256), 256, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p,
-                                                          n_gpairs, Ed, c.ev_w.p, c.ev.p, c.win_set.p,
-                                                          c.rank_slot_set.p, c.rank_id_set.p, c.slot_base_set.p,
-                                                          c.id_base_set.p);
+      // part 1, one warp per event: species and components
+      k_apply_move<<<grid_for(W * 32, 256), 256, 0, c.stream>>>(
+          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p, c.win_set.p,
+          c.dec_set.p, c.rank_slot_set.p, c.slot_base_set.p, c.ice_set.p);
+      note_launch();
+      // part 2, one thread per event: removals, scalar fields, caches
+      k_apply_set<<<grid_for(W, 256), 256, 0, c.stream>>>(
+          c.d_pops, c.gpair_pop.p, c.gpair_local.p, Ed, c.ev_c.p, c.gp_c.p, c.win_set.p, c.dec_set.p,
+          c.rank_slot_set.p, c.rank_id_set.p, c.slot_base_set.p, c.id_base_set.p, c.ice_set.p);
       note_launch();
     }
     if (Q > 0) {
@@ -1457,17 +1609,19 @@ void step_parallel(Ctx& c, int kt) {
       note_launch();
       scan_dev(c, c.lost_pp.p, Q, nullptr, c.lost_off.p);
     }
-    k_alloc_finish<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_pops, c.n_pop, c.per_pop_i.p + 0 * c.n_pop,
-                                                                c.per_pop_i.p + 1 * c.n_pop, c.per_pop_i.p + 2 * c.n_pop,
-                                                                c.per_pop_i.p + 3 * c.n_pop);
-    note_launch();
     // one read-back at the end of the round
     long long set_losers = 0, pp_lost = 0, E = 0;
     CK(cudaMemcpyAsync(&set_losers, c.round_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     if (W > 0) CK(cudaMemcpyAsync(&E, Ed, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     if (Q > 0) CK(cudaMemcpyAsync(&pp_lost, c.lost_off.p + Q, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+    unsigned long long scan_err = 0;
+    CK(cudaMemcpyAsync(&scan_err, c.scan_err.p, sizeof(scan_err), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    if (scan_err) {
+      CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(scan_err), c.stream));
+      throw Fail(PMC_ERR_TIMEOUT);
+    }
     for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] += per_pop[0 * c.n_pop + k] + per_pop[2 * c.n_pop + k];
     redraws += set_losers + pp_lost;
     c.last_set_losers += set_losers;
@@ -1568,8 +1722,12 @@ static int do_init(int n_pop, int n_spec, const double* density, int i_water, in
   c.pops.resize(n_pop);
   CK(cudaMalloc(&c.d_pops, sizeof(PopDev) * n_pop));
   CK(cudaMalloc(&c.d_ctrs, sizeof(PopCtr) * n_pop));
-  CK(cudaMalloc(&c.d_round, sizeof(uint32_t)));
-  CK(cudaMemset(c.d_round, 0, sizeof(uint32_t)));
+  CK(cudaMalloc(&c.d_round, 2 * sizeof(uint32_t)));  // round of the step, claim generation
+  CK(cudaMemset(c.d_round, 0, 2 * sizeof(uint32_t)));
+  c.scan_ctr.reserve(kScanMaxJobs);
+  CK(cudaMemset(c.scan_ctr.p, 0, sizeof(unsigned) * c.scan_ctr.n));
+  c.scan_err.reserve(1);
+  CK(cudaMemset(c.scan_err.p, 0, sizeof(unsigned long long) * c.scan_err.n));
   CK(cudaMemset(c.d_ctrs, 0, sizeof(PopCtr) * n_pop));
   for (int k = 0; k < n_pop; k++) {
     c.pops[k].seed = seeds ? seeds[k] : (uint64_t)(k + 1);
@@ -1614,10 +1772,18 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   DevBuf<long long>* bl[] = {&c.pop_pair_base, &c.nwork_set, &c.nwork_pp, &c.nprio, &c.work_off, &c.pp_off,
                              &c.prio_off, &c.flag_off, &c.ev_w, &c.rank_slot_set, &c.rank_id_set,
                              &c.rank_slot_pp, &c.rank_id_pp, &c.lost_off, &c.id_base_set, &c.id_base_pp,
-                             &c.scan_bsum, &c.scan_total, &c.n_dev};
+                             &c.n_dev};
   for (auto* b : bl) b->release();
   c.flag.release();
   c.win_set.release();
+  c.dec_set.release();
+  c.ev_gp.release();
+  c.gp_c.release();
+  c.ev_c.release();
+  c.ice_set.release();
+  c.scan_status.release();
+  c.scan_ctr.release();
+  c.scan_err.release();
   c.win_pp.release();
   c.ev.release();
   c.op_prio.release();
@@ -1655,21 +1821,15 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
   CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
   if (n_part > 0) {
     size_t n = (size_t)n_part;
-    c.st_d.reserve(n * c.n_spec);
-    c.st_i.reserve(3 * n);
-    c.st_l.reserve(n);
-    double* dv = c.st_d.p;
-    int* dg = group ? c.st_i.p : nullptr;
-    int* dc = cls ? c.st_i.p + n : nullptr;
-    int* dn = n_primary ? c.st_i.p + 2 * n : nullptr;
-    long long* di = id ? c.st_l.p : nullptr;
-    CK(cudaMemcpyAsync(dv, vol, sizeof(double) * n * c.n_spec, cudaMemcpyHostToDevice, c.stream));
-    if (dg) CK(cudaMemcpyAsync(dg, group, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
-    if (dc) CK(cudaMemcpyAsync(dc, cls, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
-    if (di) CK(cudaMemcpyAsync(di, id, sizeof(long long) * n, cudaMemcpyHostToDevice, c.stream));
-    if (dn) CK(cudaMemcpyAsync(dn, n_primary, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(ph.h.vol, vol, sizeof(double) * n * c.n_spec, cudaMemcpyHostToDevice, c.stream));
+    if (group) CK(cudaMemcpyAsync(ph.h.grp, group, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+    if (cls) CK(cudaMemcpyAsync(ph.h.cls, cls, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+    if (id) CK(cudaMemcpyAsync(ph.h.id, id, sizeof(long long) * n, cudaMemcpyHostToDevice, c.stream));
+    if (n_primary) CK(cudaMemcpyAsync(ph.h.nprim, n_primary, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
     long long id0 = r.next_id;
-    k_upload<<<grid_for(n_part, 256), 256, 0, c.stream>>>(ph.h, n_part, dv, dg, dc, di, dn, id0); note_launch();
+    k_upload<<<grid_for(n_part, 256), 256, 0, c.stream>>>(ph.h, n_part, group != nullptr, cls != nullptr,
+                                                          id != nullptr, n_primary != nullptr, id0);
+    note_launch();
     if (id) {
       long long mx = 0;
       for (int i = 0; i < n_part; i++) mx = std::max<long long>(mx, id[i]);
@@ -1705,25 +1865,23 @@ int pmc_coag_gpu_upload_components(pmc_coag_gpu_ctx* x, int pop, int n_part, con
   PopHost& ph = c.pops[pop];
   PopCtr r = read_ctr(c, pop);
   if (n_part != r.n_slots) return PMC_ERR_INVALID_ARG;
-  std::vector<int> src((size_t)kMaxComponent * ph.h.cap, 0);
-  std::vector<double> tim((size_t)kMaxComponent * ph.h.cap, 0.0);
+  // the slot arrays hold components particle-major, as the caller passes them
   std::vector<double> lct(n_part), gct(n_part);
   for (int i = 0; i < n_part; i++) {
     if (n_comp[i] < 0 || n_comp[i] > kMaxComponent) return PMC_ERR_INVALID_ARG;
     double lo = 0.0, hi = 0.0;
     for (int k = 0; k < n_comp[i]; k++) {
-      src[(size_t)k * ph.h.cap + i] = comp_source[(size_t)i * kMaxComponent + k];
-      double t = comp_create_time[(size_t)i * kMaxComponent + k];
-      tim[(size_t)k * ph.h.cap + i] = t;
+      double t = comp_create_time[comp_at(i, k)];
       if (k == 0 || t < lo) lo = t;
       if (k == 0 || t > hi) hi = t;
     }
     lct[i] = lo;
     gct[i] = hi;
   }
+  size_t nc = (size_t)n_part * kMaxComponent;
   CK(cudaMemcpyAsync(ph.h.ncomp, n_comp, sizeof(int) * n_part, cudaMemcpyHostToDevice, c.stream));
-  CK(cudaMemcpyAsync(ph.h.csrc, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice, c.stream));
-  CK(cudaMemcpyAsync(ph.h.ctime, tim.data(), sizeof(double) * tim.size(), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(ph.h.csrc, comp_source, sizeof(int) * nc, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(ph.h.ctime, comp_create_time, sizeof(double) * nc, cudaMemcpyHostToDevice, c.stream));
   CK(cudaMemcpyAsync(ph.h.lct, lct.data(), sizeof(double) * n_part, cudaMemcpyHostToDevice, c.stream));
   CK(cudaMemcpyAsync(ph.h.gct, gct.data(), sizeof(double) * n_part, cudaMemcpyHostToDevice, c.stream));
   CK(cudaStreamSynchronize(c.stream));
@@ -1840,11 +1998,23 @@ static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, i
   size_t ns = (size_t)r.n_slots + 1;
   size_t n = std::max(r.n_live, 1);
   c.st_l.reserve(ns + n);
-  c.st_d.reserve(n * (c.n_spec + kMaxComponent));
-  c.st_i.reserve(n * (4 + kMaxComponent));
   long long* off = c.st_l.p;
   long long nl = scan(c, ph.h.alive, r.n_slots, off, true);
   if (nl != r.n_live) return PMC_ERR_ASSERT;
+  if (nl > 0 && nl == r.n_slots && !comp_source && !comp_time) {
+    // no dead slots: the slot arrays already hold the particles in order,
+    // in the caller's particle-major layout
+    if (vol) CK(cudaMemcpyAsync(vol, ph.h.vol, sizeof(double) * nl * c.n_spec, cudaMemcpyDeviceToHost, c.stream));
+    if (group) CK(cudaMemcpyAsync(group, ph.h.grp, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (cls) CK(cudaMemcpyAsync(cls, ph.h.cls, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (id) CK(cudaMemcpyAsync(id, ph.h.id, sizeof(long long) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (n_primary) CK(cudaMemcpyAsync(n_primary, ph.h.nprim, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    if (n_comp) CK(cudaMemcpyAsync(n_comp, ph.h.ncomp, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return PMC_OK;
+  }
+  c.st_d.reserve(n * (c.n_spec + kMaxComponent));
+  c.st_i.reserve(n * (4 + kMaxComponent));
   long long* di = c.st_l.p + ns;
   double* dv = c.st_d.p;
   double* dct = c.st_d.p + n * c.n_spec;
@@ -1854,8 +2024,11 @@ static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, i
   int* dnc = dn + n;
   int* dcs = dnc + n;
   if (r.n_slots > 0)
-    k_download<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(ph.h, off, r.n_slots, dv, dg, dc, di, dn,
-                                                                dnc, dcs, dct); note_launch();
+    k_download<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(
+        ph.h, off, r.n_slots, vol ? dv : nullptr, group ? dg : nullptr, cls ? dc : nullptr, id ? di : nullptr,
+        n_primary ? dn : nullptr, n_comp ? dnc : nullptr, comp_source ? dcs : nullptr,
+        comp_time ? dct : nullptr);
+  note_launch();
   if (nl > 0) {
     if (vol) CK(cudaMemcpyAsync(vol, dv, sizeof(double) * nl * c.n_spec, cudaMemcpyDeviceToHost, c.stream));
     if (group) CK(cudaMemcpyAsync(group, dg, sizeof(int) * nl, cudaMemcpyDeviceToHost, c.stream));

@@ -320,6 +320,65 @@ __global__ void k_kmax_table(const PopDev* pops) {
 }
 
 // ---------------------------------------------------------------------------
+// Grid- and weight-dependent fields of every bin pair: the destination class
+// (coag_dest_class, coag_kernel.F90:382-416), max_coag_num_conc_factor
+// (coag_kernel.F90:422-465), the flat-weight factor, and the weight
+// conditions of try_per_particle_coag (coagulation.F90:191-217).  One warp
+// per pair; lane (a-1)*5 + (b-1) takes radius sample (a, b) of the 5x5 grid.
+__global__ void k_pair_setup(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  if (P.pair_setup_valid) return;
+  int lane = threadIdx.x & 31;
+  int p = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (p >= P.n_pairs) return;  // the whole warp
+  PairDesc d = P.pair_desc[p];
+  int b1 = d.b1, b2 = d.b2, c1 = d.c1, c2 = d.c2;
+  const GridDev& G = *P.grid;
+  int cc = coag_dest_class(P.w, G.centers, b1, b2, c1, c2);
+  double f = 0.0;
+  if (lane < 25) {
+    double ri = interp_linear_disc(G.edges[b1], G.edges[b1 + 1], 5, lane / 5 + 1);
+    double rj = interp_linear_disc(G.edges[b2], G.edges[b2 + 1], 5, lane % 5 + 1);
+    f = num_conc_factor(P.w, ri, rj, c1, c2, cc);
+  }
+  // the factors are positive: the maximum does not depend on the order
+  for (int o = 16; o > 0; o >>= 1) {
+    double g = __shfl_xor_sync(0xffffffffu, f, o);
+    if (g > f) f = g;
+  }
+  if (lane != 0) return;
+  PairState& S = P.pair[p];
+  S.cc = cc;
+  S.f_max = f;
+  S.fflat = P.flat ? num_conc_factor(P.w, G.centers[b1], G.centers[b2], c1, c2, cc) : 1.0;
+  S.pp_ok = 0;
+  if (P.mono_dec) {
+    double n1min, n1max, n2min, n2max;
+    {
+      double a = num_conc_at_radius<double>(P.w, c1, G.edges[b1]);
+      double b = num_conc_at_radius<double>(P.w, c1, G.edges[b1 + 1]);
+      n1min = a < b ? a : b;
+      n1max = a > b ? a : b;
+      a = num_conc_at_radius<double>(P.w, c2, G.edges[b2]);
+      b = num_conc_at_radius<double>(P.w, c2, G.edges[b2 + 1]);
+      n2min = a < b ? a : b;
+      n2max = a > b ? a : b;
+    }
+    int ok = 0, bt = 0, bs = 0, ct = 0, cs = 0;
+    if (n1max < n2min && cc == c1) {
+      bt = b1; bs = b2; ct = c1; cs = c2; ok = 1;
+    }
+    if (n2max < n1min && cc == c2) {
+      bt = b2; bs = b1; ct = c2; cs = c1; ok = 1;
+    }
+    S.pp_ok = ok;
+    S.bt = bt; S.bs = bs; S.ct = ct; S.cs = cs;
+    S.pp_min_tv = rad2vol(G.edges[bt]);
+    S.pp_max_sv = rad2vol(G.edges[bs + 1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pair set-up for round 0: mc_coag_for_bin, try_per_particle_coag's
 // eligibility tests and compute_n_samp (coagulation.F90:101-241, 648-702).
 // nwork_set[gp] = samples of a per-set pair; nwork_pp[gp] = targets of a
@@ -360,55 +419,24 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
     nwork_set[gp] = nwork_pp[gp] = nprio[gp] = 0;
     return;
   }
-  const GridDev& G = *P.grid;
-  int cc = coag_dest_class(P.w, G.centers, b1, b2, c1, c2);
-  double f_max = max_num_conc_factor(P.w, G.edges, b1, b2, c1, c2, cc);
-  double k_max = P.kmax_tab[b1 + nb * b2] * f_max;
+  double k_max = P.kmax_tab[b1 + nb * b2] * S.f_max;
   if (kmax_inflate != 0.f) k_max = k_max * (1.0 + (double)kmax_inflate);
-  S.cc = cc;
   S.k_max = k_max;
   S.inv_k_max = 1.0 / k_max;
-  {
-    double ri = G.centers[b1], rj = G.centers[b2];
-    S.fflat = P.flat ? num_conc_factor(P.w, ri, rj, c1, c2, cc) : 1.0;
-  }
-  // try_per_particle_coag eligibility (coagulation.F90:191-217)
-  if (use_particle_path && P.mono_dec) {
-    double n1min, n1max, n2min, n2max;
-    {
-      double a = num_conc_at_radius<double>(P.w, c1, G.edges[b1]);
-      double b = num_conc_at_radius<double>(P.w, c1, G.edges[b1 + 1]);
-      n1min = a < b ? a : b;
-      n1max = a > b ? a : b;
-      a = num_conc_at_radius<double>(P.w, c2, G.edges[b2]);
-      b = num_conc_at_radius<double>(P.w, c2, G.edges[b2 + 1]);
-      n2min = a < b ? a : b;
-      n2max = a > b ? a : b;
-    }
-    bool ok = false;
-    int bt = 0, bs = 0, ct = 0, cs = 0;
-    if (n1max < n2min && cc == c1) {
-      bt = b1; bs = b2; ct = c1; cs = c2; ok = true;
-    }
-    if (n2max < n1min && cc == c2) {
-      bt = b2; bs = b1; ct = c2; cs = c1; ok = true;
-    }
-    if (ok) {
-      int ns = P.cell_count[bs + nb * cs];
-      double nspt = k_max * P.del_t * (double)ns;
-      double min_tv = rad2vol(G.edges[bt]);
-      double max_sv = rad2vol(G.edges[bs + 1]);
-      double max_new = min_tv + max_sv * nspt;
-      if (nspt >= 1.0 && !(max_new / min_tv > 1.5)) {
-        S.path = kPathParticle;
-        S.bt = bt; S.bs = bs; S.ct = ct; S.cs = cs;
-        S.nspt = nspt;
-        int nt = P.cell_count[bt + nb * ct];
-        nwork_set[gp] = 0;
-        nwork_pp[gp] = nt;
-        nprio[gp] = nt;
-        return;
-      }
+  // try_per_particle_coag eligibility (coagulation.F90:191-217): the weight
+  // conditions were settled by k_pair_setup; the cell-count ones are here
+  if (use_particle_path && P.mono_dec && S.pp_ok) {
+    int ns = P.cell_count[S.bs + nb * S.cs];
+    double nspt = k_max * P.del_t * (double)ns;
+    double max_new = S.pp_min_tv + S.pp_max_sv * nspt;
+    if (nspt >= 1.0 && !(max_new / S.pp_min_tv > 1.5)) {
+      S.path = kPathParticle;
+      S.nspt = nspt;
+      int nt = P.cell_count[S.bt + nb * S.ct];
+      nwork_set[gp] = 0;
+      nwork_pp[gp] = nt;
+      nprio[gp] = nt;
+      return;
     }
   }
   // per_set_coag / compute_n_samp
@@ -474,7 +502,8 @@ template <int KT, class T, bool FLAT>
 __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpair_pop,
                                               const int* gpair_local, const long long* work_off,
                                               const long long* prio_off, int n_gpairs,
-                                              const long long* total, uint8_t* flag, int2* ev) {
+                                              const long long* total, uint8_t* flag, int2* ev,
+                                              int* ev_gp) {
   long long W = *total;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < W;
        w += (long long)gridDim.x * blockDim.x) {
@@ -530,9 +559,10 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
     flag[w] = acc ? 1 : 0;
     if (acc) {
       unsigned prio = (unsigned)(prio_off[gp] + s);
-      atomicMin(&P.claim[s1], prio);
-      atomicMin(&P.claim[s2], prio);
+      atomicMin(&P.claim[s1], claim_key(P, prio));
+      atomicMin(&P.claim[s2], claim_key(P, prio));
       ev[w] = make_int2(s1, s2);
+      ev_gp[w] = gp;
     }
   }
 }

@@ -53,23 +53,43 @@ __device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int
   return d;
 }
 
-// Resolve accepted per-set samples: winner test, slot/id needs.
-// ev_w[e] = sample index w of event e (in w order).
+// A merge decision and the number of uniforms its stream had used, in one
+// word: bits 0-4 rm1, rm2, create, lost1, lost2; bits 5-7 the new weight
+// group; bits 8-31 the uniforms used.
+__device__ __forceinline__ uint32_t pack_decision(const MergeDecision& m, uint32_t used) {
+  return (m.rm1 ? 1u : 0u) | (m.rm2 ? 2u : 0u) | (m.create ? 4u : 0u) | (m.lost1 ? 8u : 0u) |
+         (m.lost2 ? 16u : 0u) | ((uint32_t)(m.new_group & 7) << 5) | (used << 8);
+}
+__device__ __forceinline__ MergeDecision unpack_decision(uint32_t x, uint32_t* used) {
+  MergeDecision m;
+  m.rm1 = x & 1u;
+  m.rm2 = x & 2u;
+  m.create = x & 4u;
+  m.lost1 = x & 8u;
+  m.lost2 = x & 16u;
+  m.new_group = (int)((x >> 5) & 7u);
+  *used = x >> 8;
+  return m;
+}
+
+// Resolve accepted per-set samples: winner test, slot/id needs.  Event e
+// has sample index ev_w[e], slots ev[e] and global pair ev_gp[e] (in sample
+// order, compacted from the pair tests).
 __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
-                              const long long* work_off, const long long* prio_off, int n_gpairs,
+                              const long long* work_off, const long long* prio_off,
                               const long long* n_events, const long long* ev_w, const int2* ev,
-                              int* pair_losers, int* need_slot, int* need_id, uint8_t* win,
-                              long long* n_losers) {
+                              const int* ev_gp, int* pair_losers, int* need_slot, int* need_id,
+                              uint8_t* win, uint32_t* dec, long long* n_losers) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
     long long w = ev_w[e];
-    int gp = find_pair(work_off, n_gpairs, w);
+    int gp = ev_gp[e];
     const PopDev& P = pops[gpair_pop[gp]];
     int p = gpair_local[gp];
     long long s = w - work_off[gp];
     unsigned prio = (unsigned)(prio_off[gp] + s);
-    int2 sl = ev[w];
+    int2 sl = ev[e];
     if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
       bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
       win[e] = 0;
@@ -77,7 +97,8 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const in
       need_id[e] = 0;
       continue;
     }
-    bool winner = P.claim[sl.x] == prio && P.claim[sl.y] == prio;
+    unsigned long long key = claim_key(P, prio);
+    bool winner = P.claim[sl.x] == key && P.claim[sl.y] == key;
     win[e] = winner ? 1 : 0;
     need_slot[e] = 0;
     need_id[e] = 0;
@@ -91,6 +112,7 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const in
     Rng g = make_rng(P, kStreamMerge, (uint32_t)p, (uint32_t)s);
     MergeDecision m = merge_decide(P, g, sl.x, sl.y, d.c1, d.c2, S.cc);
     if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+    dec[e] = pack_decision(m, g.used());
     if (m.create) {
       need_slot[e] = (!m.rm1 && !m.rm2) ? 1 : 0;
       bool keep1 = m.rm1 && !m.lost1, keep2 = m.rm2 && !m.lost2;
@@ -99,75 +121,179 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const in
   }
 }
 
-// Apply winning per-set events (coagulate, coagulation.F90:928-985).
+// destination slot of a winning event that creates a particle (-1: none)
+__device__ __forceinline__ int event_dest(const MergeDecision& m, int s1, int s2, int slot_base,
+                                          long long slot_rank) {
+  if (!m.create) return -1;
+  if (m.rm1) return s1;
+  if (m.rm2) return s2;
+  return slot_base + (int)slot_rank;
+}
+
+// Apply winning per-set events (coagulate, coagulation.F90:928-985), part 1:
+// the per-particle vectors.  One warp per event: lane q adds species q of the
+// two sources (particle-major, so each source is a few cache lines) and lane
+// k places component k; the random component selection is computed by every
+// lane alike from the stream position k_resolve_set stored.  The summed
+// volume and mass go to the destination's caches for part 2; the water
+// volumes of the sources, which part 2 needs after the destination may have
+// been overwritten, go to ice[e].
+__global__ void __launch_bounds__(256) k_apply_move(const PopDev* pops, const int* gpair_pop,
+                                                    const int* gpair_local, const long long* work_off,
+                                                    const long long* n_events, const long long* ev_w,
+                                                    const int2* ev, const int* ev_gp, const uint8_t* win,
+                                                    const uint32_t* dec, const long long* slot_rank,
+                                                    const int* slot_base, double2* ice) {
+  constexpr unsigned kFull = 0xffffffffu;
+  long long E = *n_events;
+  int lane = threadIdx.x & 31;
+  long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long e = warp; e < E; e += n_warps) {
+    if (!win[e]) continue;  // the same e for the whole warp
+    uint32_t used;
+    MergeDecision m = unpack_decision(dec[e], &used);
+    if (!m.create) continue;
+    int gp = ev_gp[e];
+    int pop = gpair_pop[gp];
+    const PopDev& P = pops[pop];
+    int2 sl = ev[e];
+    int s1 = sl.x, s2 = sl.y;
+    int dest = event_dest(m, s1, s2, slot_base[pop], m.rm1 || m.rm2 ? 0 : slot_rank[e]);
+    if (dest < 0 || dest >= P.cap) continue;  // reported by part 2
+    // every read of the two sources comes before the first write to dest
+    int na = P.ncomp[s1], nb = P.ncomp[s2];
+    if (P.i_water > 0 && lane == 0)
+      ice[e] = make_double2(P.vol[vol_at(P, s1, P.i_water - 1)], P.vol[vol_at(P, s2, P.i_water - 1)]);
+    int ca = 0, cb = 0;
+    double ta = 0.0, tb = 0.0;
+    if (lane < na && lane < kMaxComponent) {
+      ca = P.csrc[comp_at(s1, lane)];
+      ta = P.ctime[comp_at(s1, lane)];
+    }
+    if (lane < nb && lane < kMaxComponent) {
+      cb = P.csrc[comp_at(s2, lane)];
+      tb = P.ctime[comp_at(s2, lane)];
+    }
+    const int ns = P.n_spec;
+    double v_lo = 0.0, v_hi = 0.0;  // species lane and lane + 32
+    if (lane < ns) v_lo = P.vol[vol_at(P, s1, lane)] + P.vol[vol_at(P, s2, lane)];
+    if (lane + 32 < ns) v_hi = P.vol[vol_at(P, s1, lane + 32)] + P.vol[vol_at(P, s2, lane + 32)];
+    int n1_new = na, n2_new = nb;
+    int k_src = lane < na ? lane : lane - na;
+    bool from_a = lane < na;
+    if (na + nb > kMaxComponent) {
+      int np1 = P.nprim[s1], np2 = P.nprim[s2];
+      Rng g = make_rng(P, kStreamMerge, (uint32_t)gpair_local[gp], (uint32_t)(ev_w[e] - work_off[gp]));
+      g.seek(used);
+      int sa[kMaxComponent], sb[kMaxComponent];
+      coag_components(g, na, np1, nb, np2, &n1_new, &n2_new, sa, sb);
+      from_a = lane < n1_new;
+      k_src = 0;
+      if (from_a) k_src = sa[lane] - 1;
+      else if (lane - n1_new < n2_new) k_src = sb[lane - n1_new] - 1;
+    }
+    k_src &= 31;
+    int xa = __shfl_sync(kFull, ca, k_src), xb = __shfl_sync(kFull, cb, k_src);
+    double ya = __shfl_sync(kFull, ta, k_src), yb = __shfl_sync(kFull, tb, k_src);
+    // totals in the reference's order (species 1..n)
+    double vt = 0.0, ms = 0.0;
+    for (int q = 0; q < ns && q < 64; q++) {
+      double v = __shfl_sync(kFull, q < 32 ? v_lo : v_hi, q & 31);
+      vt = vt + v;
+      ms = ms + v * P.density[q];
+    }
+    __syncwarp();
+    if (lane < ns) P.vol[vol_at(P, dest, lane)] = v_lo;
+    if (lane + 32 < ns) P.vol[vol_at(P, dest, lane + 32)] = v_hi;
+    int n_out = n1_new + n2_new;
+    if (lane < n_out) {
+      P.csrc[comp_at(dest, lane)] = from_a ? xa : xb;
+      P.ctime[comp_at(dest, lane)] = from_a ? ya : yb;
+    }
+    if (lane == 0) {
+      P.vtot[dest] = vt;
+      P.mass[dest] = ms;
+      P.ncomp[dest] = n_out;
+    }
+  }
+}
+
+// particle fields that coag_scalars reads (component lists excluded)
+__device__ __forceinline__ void load_scalars(const PopDev& P, int i, PMeta& m) {
+  m.id = P.id[i];
+  m.nprim = P.nprim[i];
+  m.lct = P.lct[i];
+  m.gct = P.gct[i];
+  m.imf = P.imf[i];
+  m.den_ice = P.den_ice[i];
+  m.phi = P.phi[i];
+  m.hyst = P.hyst[i];
+  m.frozen = P.frozen[i];
+}
+
+// Part 2, one thread per event: removals, the scalar fields of the
+// coagulated particle, its radius, bin and pair-test record.
 __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
-                            const long long* work_off, int n_gpairs, const long long* n_events,
-                            const long long* ev_w, const int2* ev, const uint8_t* win,
-                            const long long* slot_rank, const long long* id_rank,
-                            const int* slot_base, const long long* id_base) {
+                            const long long* n_events, const int2* ev, const int* ev_gp, const uint8_t* win,
+                            const uint32_t* dec, const long long* slot_rank, const long long* id_rank,
+                            const int* slot_base, const long long* id_base, const double2* ice) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
     if (!win[e]) continue;
-    long long w = ev_w[e];
-    int gp = find_pair(work_off, n_gpairs, w);
+    int gp = ev_gp[e];
     int pop = gpair_pop[gp];
     const PopDev& P = pops[pop];
     int p = gpair_local[gp];
-    long long s = w - work_off[gp];
-    int2 sl = ev[w];
+    int2 sl = ev[e];
     int s1 = sl.x, s2 = sl.y;
-    PairDesc d = P.pair_desc[p];
-    const PairState& S = P.pair[p];
-    Rng g = make_rng(P, kStreamMerge, (uint32_t)p, (uint32_t)s);
-    MergeDecision m = merge_decide(P, g, s1, s2, d.c1, d.c2, S.cc);
+    uint32_t used;
+    MergeDecision m = unpack_decision(dec[e], &used);
     add_ll(&P.ctr->tot_coag, (long long)(1LL));
-    int dlive = 0;
-    if (m.create) {
-      double v[kMaxSpec];
-      PMeta a, b;
-      load_meta(P, s1, a);
-      load_meta(P, s2, b);
-      double ice_a = 0.0, ice_b = 0.0;
-      if (P.i_water > 0) {
-        ice_a = P.vol[(size_t)(P.i_water - 1) * P.cap + s1];
-        ice_b = P.vol[(size_t)(P.i_water - 1) * P.cap + s2];
-      }
-      for (int q = 0; q < P.n_spec; q++)
-        v[q] = P.vol[(size_t)q * P.cap + s1] + P.vol[(size_t)q * P.cap + s2];
-      PMeta c;
-      coag_meta(g, a, ice_a, b, ice_b, c);
-      c.grp = m.new_group;
-      c.cls = S.cc + 1;
-      int dest;
-      if (m.rm1) dest = s1;
-      else if (m.rm2) dest = s2;
-      else dest = slot_base[pop] + (int)slot_rank[e];
-      if (m.rm1 && !m.lost1) c.id = a.id;
-      else if (m.rm2 && !m.lost2) c.id = b.id;
-      else c.id = id_base[pop] + id_rank[e];
-      if (dest >= P.cap) {
-        set_status(P.ctr, kErrCapacity);
-        continue;
-      }
-      if (dest < 0) {
-        bad_index(P.ctr, kBadDest, dest);
-        continue;
-      }
-      store_particle(P, dest, v, c);
-      // the coagulated particle must lie on the grid (aero_state_add_particle
-      // with allow_resort=.false., aero_sorted.F90:427-440)
-      int nbin = refresh_slot(P, dest);
-      if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
-      if (m.rm1 && dest != s1) kill_slot(P, s1);
-      if (m.rm2 && dest != s2) kill_slot(P, s2);
-      dlive = 1 - (int)m.rm1 - (int)m.rm2;
-    } else {
+    if (!m.create) {
       if (m.rm1) kill_slot(P, s1);
       if (m.rm2) kill_slot(P, s2);
-      dlive = -(int)m.rm1 - (int)m.rm2;
+      int dlive = -(int)m.rm1 - (int)m.rm2;
+      if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
+      continue;
     }
-    if (dlive) add_ll(&P.ctr->n_live, (long long)(dlive));
+    int dest = event_dest(m, s1, s2, slot_base[pop], m.rm1 || m.rm2 ? 0 : slot_rank[e]);
+    if (dest >= P.cap) {
+      set_status(P.ctr, kErrCapacity);
+      continue;
+    }
+    if (dest < 0) {
+      bad_index(P.ctr, kBadDest, dest);
+      continue;
+    }
+    PMeta a, b, c;
+    load_scalars(P, s1, a);
+    load_scalars(P, s2, b);
+    double2 wi = P.i_water > 0 ? ice[e] : make_double2(0.0, 0.0);
+    coag_scalars(a, wi.x, b, wi.y, c);
+    P.grp[dest] = m.new_group;
+    P.cls[dest] = P.pair[p].cc + 1;
+    if (m.rm1 && !m.lost1) P.id[dest] = a.id;
+    else if (m.rm2 && !m.lost2) P.id[dest] = b.id;
+    else P.id[dest] = id_base[pop] + id_rank[e];
+    P.nprim[dest] = c.nprim;
+    P.lct[dest] = c.lct;
+    P.gct[dest] = c.gct;
+    P.imf[dest] = c.imf;
+    P.den_ice[dest] = c.den_ice;
+    P.phi[dest] = c.phi;
+    P.hyst[dest] = c.hyst;
+    P.frozen[dest] = c.frozen;
+    P.alive[dest] = 1;
+    // the coagulated particle must lie on the grid (aero_state_add_particle
+    // with allow_resort=.false., aero_sorted.F90:427-440)
+    int nbin = refresh_slot(P, dest);
+    if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
+    if (m.rm1 && dest != s1) kill_slot(P, s1);
+    if (m.rm2 && dest != s2) kill_slot(P, s2);
+    int dlive = 1 - (int)m.rm1 - (int)m.rm2;
+    if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
   }
 }
 
@@ -280,11 +406,11 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
         double ice_a = 0.0, ice_b = 0.0;
         if (P.i_water > 0) {
           ice_a = acc[P.i_water - 1];
-          ice_b = P.vol[(size_t)(P.i_water - 1) * P.cap + si];
+          ice_b = P.vol[vol_at(P, si, P.i_water - 1)];
         }
         coag_meta(g, src, ice_a, sm, ice_b, src);
         for (int k2 = 0; k2 < ns; k2++) {
-          double vi = P.vol[(size_t)k2 * P.cap + si];
+          double vi = P.vol[vol_at(P, si, k2)];
           acc[k2] = acc[k2] + vi;
           vol_sq[k2] = vol_sq[k2] + vi * vi;
         }
@@ -296,7 +422,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
             if (!dup) {
               if (R.n_rm < kMaxRemove) {
                 R.rm[R.n_rm++] = si;
-                atomicMin(&P.claim[si], prio);
+                atomicMin(&P.claim[si], claim_key(P, prio));
               } else {
                 set_status(P.ctr, kErrCapacity);
               }
@@ -356,7 +482,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     PMeta tm;
     load_meta(P, t, tm);
     double ice_t = 0.0;
-    if (P.i_water > 0) ice_t = P.vol[(size_t)(P.i_water - 1) * P.cap + t];
+    if (P.i_water > 0) ice_t = P.vol[vol_at(P, t, P.i_water - 1)];
     double ice_s = P.i_water > 0 ? acc[P.i_water - 1] : 0.0;
     long long tid = tm.id;
     double old_nc = nc_target;
@@ -365,7 +491,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     nm.id = tid;
     double vt = 0.0;
     for (int k = 0; k < ns; k++) {
-      acc[k] = P.vol[(size_t)k * P.cap + t] + acc[k];  // now the new target volumes
+      acc[k] = P.vol[vol_at(P, t, k)] + acc[k];  // now the new target volumes
       vt = vt + acc[k];
     }
     double rnew = vol2rad(vt);
@@ -384,7 +510,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     R.merged = 1;
     R.n_copies = n_copies;
     R.meta = nm;
-    atomicMin(&P.claim[t], prio);
+    atomicMin(&P.claim[t], claim_key(P, prio));
   }
 }
 
@@ -399,8 +525,8 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
     const PPResult& R = res[q];
     unsigned prio = op_prio[q];
     bool ok = true;
-    if (R.merged) ok = ok && P.claim[R.target] == prio;
-    for (int z = 0; z < R.n_rm; z++) ok = ok && P.claim[R.rm[z]] == prio;
+    if (R.merged) ok = ok && P.claim[R.target] == claim_key(P, prio);
+    for (int z = 0; z < R.n_rm; z++) ok = ok && P.claim[R.rm[z]] == claim_key(P, prio);
     win[q] = ok ? 1 : 0;
     lost[q] = ok ? 0 : 1;
     int extra = (ok && R.merged && R.n_copies > 1) ? R.n_copies - 1 : 0;

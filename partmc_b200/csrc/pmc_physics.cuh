@@ -536,6 +536,17 @@ struct Rng {
     have = 0;
     return u53(buf.z, buf.w);
   }
+  // uniforms drawn so far, and the state after exactly u draws
+  PMC_HD uint32_t used() const { return 2 * n - (have ? 1u : 0u); }
+  PMC_HD void seek(uint32_t u) {
+    n = (u + 1) / 2;
+    if (u & 1u) {
+      buf = philox4x32_10(U4{c0, c1, c2, n - 1}, k0, k1);
+      have = 2;
+    } else {
+      have = 0;
+    }
+  }
 };
 
 // Samplers with the reference's methods (rand.F90), drawing from an Rng.

@@ -51,7 +51,7 @@ struct Seq {
   __device__ double vtot(int i) { return P->vtot[i - 1]; }
   __device__ double radius(int i) { return vol2rad(P->vtot[i - 1]); }
   __device__ void load(int i, Tp& t) {
-    for (int s = 0; s < P->n_spec; s++) t.vol[s] = P->vol[(size_t)s * P->cap + (i - 1)];
+    for (int s = 0; s < P->n_spec; s++) t.vol[s] = P->vol[vol_at(*P, i - 1, s)];
     load_meta(*P, i - 1, t.m);
   }
   __device__ void copy_slot(int dst, int src) {
@@ -244,7 +244,7 @@ struct Seq {
     return true;
   }
   __device__ void slot_vol(int i, double* v) {
-    for (int s = 0; s < P->n_spec; s++) v[s] = P->vol[(size_t)s * P->cap + (i - 1)];
+    for (int s = 0; s < P->n_spec; s++) v[s] = P->vol[vol_at(*P, i - 1, s)];
   }
 
   // coagulate_weighting + coagulate (coagulation.F90:810-985)

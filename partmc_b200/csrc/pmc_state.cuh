@@ -1,11 +1,13 @@
 // pmc_state.cuh -- device-resident layout of particle populations.
 //
 // A population is the GPU form of aero_state_t (aero_state.F90:69-84):
-//  - particle slots, structure-of-arrays, slot i of species s at
-//    vol[s * cap + i] (species-major, so a pass over one species is
-//    coalesced); per-slot caches vtot = sum(vol) and mass = sum(vol*density)
-//    are kept exact (recomputed in the reference's summation order on every
-//    change);
+//  - particle slots, one array per field; the per-particle vectors are
+//    particle-major (species s of slot i at vol[i * n_spec + s], component k
+//    at csrc/ctime[i * kMaxComponent + k]) because the step only ever reads
+//    or writes whole particles: a warp moves one particle's 20 species in one
+//    or two cache lines.  Per-slot caches vtot = sum(vol) and
+//    mass = sum(vol*density) are recomputed in the reference's summation
+//    order on every change;
 //  - the aero_sorted_t equivalent (aero_sorted.F90:47-66): bin grid, one
 //    list of slot numbers per (bin, class) cell in CSR form, and a
 //    bin-ordered array of pair-test records;
@@ -43,6 +45,14 @@ struct __align__(32) RecF {
   float r, rv, nc, a, b, c, pad0, pad1;
 };
 
+struct PopDev;
+
+// index of species s of slot i, and of component k of slot i
+#define PMC_VOL_AT(n_spec, i, s) ((size_t)(i) * (size_t)(n_spec) + (size_t)(s))
+__host__ __device__ __forceinline__ size_t comp_at(long long i, int k) {
+  return (size_t)i * kMaxComponent + (size_t)k;
+}
+
 struct GridDev {
   int n_bin;
   double log_lo, log_hi;  // log(edges[0]), log(edges[n_bin])
@@ -60,14 +70,19 @@ struct PairDesc {
 enum PairPath : int { kPathSkip = 0, kPathSet = 1, kPathParticle = 2 };
 
 struct PairState {
+  // set per step
   double k_max;      // coag_kernel_max(b1,b2) * f_max (FP32 mode: inflated)
   double inv_k_max;  // accept_factor = 1 / k_max
-  double fflat;      // constant weight factor when every weight is flat
   double nspt;       // n_source_per_target (per-particle path)
   int path;
-  int cc;            // destination class (0-based)
   int n1, n2;        // cell sizes at round start
   int start1, start2;
+  // set when the grid or the weights change (k_pair_setup)
+  double f_max;      // max_coag_num_conc_factor
+  double fflat;      // constant weight factor when every weight is flat
+  double pp_min_tv, pp_max_sv;  // rad2vol of the target bin's lower and the source bin's upper edge
+  int cc;            // destination class (0-based)
+  int pp_ok;         // the weights make the per-particle path possible
   int bt, bs, ct, cs;  // per-particle path target/source cells (0-based)
 };
 
@@ -113,6 +128,7 @@ struct PopDev {
   uint64_t seed;
   uint32_t step;
   const uint32_t* round_p;  // the current round of the step (one device word for all populations)
+  const uint32_t* gen_p;    // rounds since the context was made (claim generation)
   int kernel_type;
   double temp, pressure, coeff, del_t;
   BrownEnv benv;
@@ -157,13 +173,28 @@ struct PopDev {
 
   double* kmax_tab;  // [n_bin * n_bin], (b1, b2) at b1 + n_bin * b2
   int kmax_valid;
+  int pair_setup_valid;  // the grid/weight-dependent fields of pair[] are current
 
   const PairDesc* pair_desc;  // [n_pairs]
   PairState* pair;            // [n_pairs]
 
-  unsigned* claim;  // [cap] lowest priority that claimed the slot this round
+  // [cap] lowest claim key of the current round: (~generation << 32) |
+  // priority, so a key from any earlier round is larger and is replaced by
+  // the first claim of this round; no per-round reset is needed
+  unsigned long long* claim;
 
   PopCtr* ctr;
 };
+
+__host__ __device__ __forceinline__ size_t vol_at(const PopDev& P, long long i, int s) {
+  return PMC_VOL_AT(P.n_spec, i, s);
+}
+
+#ifdef __CUDACC__
+// claim key of priority prio in the current round
+__device__ __forceinline__ unsigned long long claim_key(const PopDev& P, unsigned prio) {
+  return ((unsigned long long)(~*P.gen_p) << 32) | (unsigned long long)prio;
+}
+#endif
 
 }  // namespace pmc
