@@ -27,7 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 B_TEST = 56  # algorithmic bytes per pair test: two cell-list entries and two 24-byte records
-B_SCATTER = 13  # per slot: alive flag, bin and class read, one cell-list entry written
+B_SORT = 8  # per slot: its cell key read, its cell-list entry written
 
 
 def parse():
@@ -423,7 +423,7 @@ def main():
         n1 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
         prof = {}
-        for which, name in ((0, "test"), (1, "scatter"), (2, "hist"), (3, "step")):
+        for which, name in ((0, "test"), (1, "sort"), (3, "step")):
             t, nl, u = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
             L.pmc_coag_gpu_profile_read(st.ctx, which, ctypes.byref(t), ctypes.byref(nl), ctypes.byref(u))
             prof[name] = (t.value, nl.value, u.value)
@@ -449,10 +449,10 @@ def main():
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         ttest, ntest, utest = prof["test"]
-        tsc, nsc, usc = prof["scatter"]
+        tsc, nsc, usc = prof["sort"]
         # dominant kernel by measured time
         if tsc >= ttest:
-            dom, t_tot, n_l, units, bpu = "k_sort_scatter (counting-sort scatter)", tsc, nsc, usc, B_SCATTER
+            dom, t_tot, n_l, units, bpu = "k_sort_all (cell counting sort)", tsc, nsc, usc, B_SORT
         else:
             dom, t_tot, n_l, units, bpu = "k_test (pair tests)", ttest, ntest, utest, B_TEST
         avg_ms = t_tot / max(n_l, 1)

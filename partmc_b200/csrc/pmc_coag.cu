@@ -163,11 +163,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
 // ---------------------------------------------------------------------------
 // small helper kernels
 
-__global__ void k_fill_u32(unsigned* p, long long n, unsigned v) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    p[i] = v;
-}
 
 // accepted samples in sample order: event e gets its sample index, its two
 // slots and its global pair
@@ -308,7 +303,7 @@ __global__ void k_upload(PopDev P, int n, int have_grp, int have_cls, int have_i
     P.hyst[i] = 0;
     P.frozen[i] = 0;
     P.alive[i] = 1;
-    P.bin[i] = -1;  // set by the first refresh after the grid decision
+    P.cell[i] = -1;  // set by the first refresh after the grid decision
   }
 }
 
@@ -362,7 +357,7 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.hyst[j] = S.hyst[i];
     D.frozen[j] = S.frozen[i];
     D.alive[j] = S.alive[i];
-    D.bin[j] = S.bin[i];
+    D.cell[j] = S.cell[i];
     D.claim[j] = S.claim[i];
     D.recd[j] = S.recd[i];
     D.recf[j] = S.recf[i];
@@ -525,6 +520,9 @@ struct Ctx {
   std::vector<PopCtr> h_ctrs;
   cudaStream_t stream = nullptr;
   int max_rounds = 32;
+  int n_sm = 148;        // multiprocessors of the device
+  size_t sort_smem = 0;  // dynamic shared memory the sort grid was sized for
+  int sort_blocks = 0;   // co-resident sort blocks at that size
   // per-round buffers
   DevBuf<int> gpair_pop, gpair_local;
   DevBuf<long long> pop_pair_base;
@@ -562,8 +560,7 @@ struct Ctx {
   long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
   long long last_set_losers = 0, last_pp_lost = 0, last_events = 0, last_ops = 0;
   // optional per-kernel timing with CUDA events on the library's stream:
-  // 0 pair tests, 1 sort scatter + record build, 2 sort histogram,
-  // 3 whole steps
+  // 0 pair tests, 1 sorts (k_sort_all), 2 unused, 3 whole steps
   bool prof = false;
   struct ProfPair {
     int id;
@@ -778,7 +775,7 @@ void alloc_slots(Ctx& c, PopHost& ph, int cap) {
   h.hyst = dalloc<int>(o, cap);
   h.frozen = dalloc<int>(o, cap);
   h.alive = dalloc<uint8_t>(o, cap);
-  h.bin = dalloc<int>(o, cap);
+  h.cell = dalloc<int>(o, cap);
   h.list = dalloc<int>(o, cap);
   h.recd = dalloc<RecD>(o, cap);
   h.recf = dalloc<RecF>(o, cap);
@@ -972,13 +969,6 @@ __global__ void k_radius_minmax_masked(const PopDev* pops, const uint8_t* on) {
   }
 }
 
-__global__ void k_reset_ranges(PopCtr* ctrs, int n_pop) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_pop) return;
-  ctrs[k].bmin = 1 << 30;
-  ctrs[k].bmax = -1;
-  ctrs[k].out_of_grid = 0;
-}
 
 // chunk counts from the host's copy of the slot counts
 void prepare_chunks(Ctx& c) {
@@ -996,31 +986,34 @@ void prepare_chunks(Ctx& c) {
   }
 }
 
-// histogram + scan of every population with its current grid
-void run_hist_scan(Ctx& c) {
+// the full sort of every population with its current grid: one cooperative
+// launch of k_sort_all on a persistent grid of co-resident blocks
+void run_sort(Ctx& c) {
   prepare_chunks(c);
-  k_reset_ranges<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_ctrs, c.n_pop);
-  note_launch();
   if (c.dirty) push_pops(c);
   int max_chunks = 1, max_cells = 1;
+  long long units = 0;
   for (int k = 0; k < c.n_pop; k++) {
     max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
     max_cells = std::max(max_cells, c.pops[k].h.n_cells);
+    units += (long long)c.n_slots_host[k];
   }
-  dim3 g(max_chunks, c.n_pop);
-  {
-    long long units = 0;
-    for (int k = 0; k < c.n_pop; k++) units += (long long)c.n_slots_host[k];
-    ProfScope ps(c, 2, units);
-    k_sort_hist<<<g, kSortThreads, sizeof(int) * max_cells, c.stream>>>(c.d_pops); note_launch();
+  size_t smem = sizeof(int) * kSortWarps * (size_t)max_cells;
+  if (smem != c.sort_smem) {
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_all, kSortThreads, smem));
+    if (per_sm < 1) throw Fail(PMC_ERR_CAPACITY);
+    c.sort_blocks = per_sm * c.n_sm;
+    c.sort_smem = smem;
   }
-  {
-    dim3 gc(max_cells, c.n_pop);
-    k_sort_count<<<gc, 256, 0, c.stream>>>(c.d_pops);
-    note_launch();
-    k_sort_offsets<<<gc, 256, 0, c.stream>>>(c.d_pops);
-    note_launch();
-  }
+  long long items = (long long)c.n_pop * max_chunks;
+  int blocks = (int)std::min<long long>(c.sort_blocks, std::max<long long>(items, 1));
+  int n_pop = c.n_pop;
+  const PopDev* pops = c.d_pops;
+  void* args[] = {(void*)&pops, (void*)&n_pop, (void*)&max_chunks, (void*)&max_cells};
+  ProfScope ps(c, 1, units);
+  CK(cudaLaunchCooperativeKernel((const void*)k_sort_all, dim3(blocks), dim3(kSortThreads), args, smem, c.stream));
+  note_launch();
 }
 
 bool caches_current(const Ctx& c, const PopHost& ph) {
@@ -1071,7 +1064,7 @@ void sort_pops(Ctx& c, bool decide_grid) {
     // radius range of populations without a valid sort
     std::vector<uint8_t> on(c.n_pop, 0), fresh(c.n_pop, 0);
     bool any = false;
-    std::vector<PopCtr>& r = read_ctrs(c);
+    std::vector<PopCtr>& r = r0;
     int max_slots = 1;
     for (int k = 0; k < c.n_pop; k++) {
       if (!c.pops[k].valid_sort) {
@@ -1096,8 +1089,9 @@ void sort_pops(Ctx& c, bool decide_grid) {
       don.release();
     }
     refresh_caches(c, fresh);
-    // occupied bin range of the populations with a valid sort
-    run_hist_scan(c);
+    // sort with the current grid; the occupied bin range decides whether the
+    // grid is kept
+    run_sort(c);
     hist_current = true;
     std::vector<PopCtr>& q = read_ctrs(c);
     std::vector<uint8_t> regrid(c.n_pop, 0);
@@ -1143,17 +1137,7 @@ void sort_pops(Ctx& c, bool decide_grid) {
     }
     refresh_caches(c, regrid);
   }
-  if (!hist_current) run_hist_scan(c);
-  int max_chunks = 1, max_cells = 1;
-  for (int k = 0; k < c.n_pop; k++) {
-    max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
-    max_cells = std::max(max_cells, c.pops[k].h.n_cells);
-  }
-  dim3 g(max_chunks, c.n_pop);
-  long long units = 0;
-  for (int k = 0; k < c.n_pop; k++) units += (long long)c.n_slots_host[k];
-  ProfScope ps(c, 1, units);
-  k_sort_scatter<<<g, kSortThreads, sizeof(int) * kSortWarps * max_cells, c.stream>>>(c.d_pops); note_launch();
+  if (!hist_current) run_sort(c);
 }
 
 // ---------------------------------------------------------------------------
@@ -1719,6 +1703,14 @@ static int do_init(int n_pop, int n_spec, const double* density, int i_water, in
       c.w.expo[dst] = w_exp[src];
     }
   CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  {
+    int dev = 0, n_sm = 0, coop = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) throw Fail(PMC_ERR_NO_DEVICE);  // the sort needs cooperative launches
+    c.n_sm = n_sm;
+  }
   c.pops.resize(n_pop);
   CK(cudaMalloc(&c.d_pops, sizeof(PopDev) * n_pop));
   CK(cudaMalloc(&c.d_ctrs, sizeof(PopCtr) * n_pop));
@@ -2234,12 +2226,12 @@ int pmc_coag_gpu_sort(pmc_coag_gpu_ctx* x, int pop, int* n_bin, double* edges, i
     std::vector<int> b(std::max(r.n_slots, 1));
     std::vector<uint8_t> a(std::max(r.n_slots, 1));
     if (r.n_slots > 0) {
-      CK(cudaMemcpy(b.data(), ph.h.bin, sizeof(int) * r.n_slots, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(b.data(), ph.h.cell, sizeof(int) * r.n_slots, cudaMemcpyDeviceToHost));
       CK(cudaMemcpy(a.data(), ph.h.alive, r.n_slots, cudaMemcpyDeviceToHost));
     }
     int j = 0;
     for (int i = 0; i < r.n_slots; i++)
-      if (a[i]) bins[j++] = b[i] >= 0 ? b[i] + 1 : 0;
+      if (a[i]) bins[j++] = (b[i] >= 0 && ph.n_bin > 0) ? b[i] % ph.n_bin + 1 : 0;
   }
   return PMC_OK;
   GUARD_END

@@ -25,6 +25,8 @@
 #include <cuda_runtime.h>
 
 #include "pmc_physics.cuh"
+#include <cooperative_groups.h>
+
 #include "pmc_state.cuh"
 
 namespace pmc {
@@ -72,40 +74,6 @@ __device__ __forceinline__ Rng make_rng(const PopDev& P, uint32_t stream, uint32
 }
 
 // ---------------------------------------------------------------------------
-// sort pass 1: per-chunk histogram of the cached (bin, class) of each live
-// slot.  Bins are kept current per slot: every write of a particle refreshes
-// its radius, bin and record (refresh_slot), and a grid change refreshes
-// them all (k_refresh_all).
-__global__ void k_sort_hist(const PopDev* pops) {
-  const PopDev& P = pops[blockIdx.y];
-  int chunk = blockIdx.x;
-  int n_chunks = n_chunks_of(P);
-  if (chunk >= n_chunks) return;
-  if (!chunk_hist_fits(P, n_chunks)) return;
-  extern __shared__ int sh[];
-  int nc = P.n_cells;
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) sh[c] = 0;
-  __syncthreads();
-  int nb = P.grid->n_bin;
-  int n = P.ctr->n_slots;
-  int base = chunk * kChunk;
-  for (int k = threadIdx.x; k < kChunk; k += blockDim.x) {
-    int i = base + k;
-    if (i >= n) break;
-    if (!P.alive[i]) continue;
-    int b = P.bin[i], cl = P.cls[i] - 1;
-    // a slot whose cached bin does not fit the current grid is not sorted
-    if (b < 0 || b >= nb || cl < 0 || cl >= P.n_class) {
-      add_ll(&P.ctr->out_of_grid, 1);
-      continue;
-    }
-    atomicAdd(&sh[b + nb * cl], 1);
-  }
-  __syncthreads();
-  int* out = P.chunk_hist + (size_t)chunk * nc;
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) out[c] = sh[c];
-}
-
 // block-wide exclusive scan of one int per thread (blockDim <= 1024)
 __device__ int block_excl_scan(int v, int* total) {
   __shared__ int ws[32];
@@ -133,56 +101,6 @@ __device__ int block_excl_scan(int v, int* total) {
   if (total) *total = ws[nw - 1];
   __syncthreads();
   return pre;
-}
-
-// sort pass 2a: total of each cell over the chunks (one block per cell)
-__global__ void k_sort_count(const PopDev* pops) {
-  const PopDev& P = pops[blockIdx.y];
-  int c = blockIdx.x;
-  if (c >= P.n_cells) return;
-  int nc = P.n_cells;
-  int s = 0;
-  int n_chunks = n_chunks_of(P);
-  if (!chunk_hist_fits(P, n_chunks)) return;
-  for (int k = threadIdx.x; k < n_chunks; k += blockDim.x) s += P.chunk_hist[(size_t)k * nc + c];
-  int tot;
-  block_excl_scan(s, &tot);
-  if (threadIdx.x == 0) {
-    P.cell_count[c] = tot;
-    if (tot > 0) {
-      int b = c % P.grid->n_bin;
-      atomicMin(&P.ctr->bmin, b);
-      atomicMax(&P.ctr->bmax, b);
-    }
-  }
-}
-
-// sort pass 2b: start of each cell and the offset of every chunk inside it
-// (one block per cell; chunk offsets by a block scan over the chunks)
-__global__ void k_sort_offsets(const PopDev* pops) {
-  const PopDev& P = pops[blockIdx.y];
-  int c = blockIdx.x;
-  if (c >= P.n_cells) return;
-  int nc = P.n_cells;
-  int s = 0;
-  for (int q = threadIdx.x; q < c; q += blockDim.x) s += P.cell_count[q];
-  int start;
-  block_excl_scan(s, &start);
-  if (threadIdx.x == 0) {
-    P.cell_start[c] = start;
-    if (c == nc - 1) P.cell_start[nc] = start + P.cell_count[c];
-  }
-  int run = start;
-  int n_chunks = n_chunks_of(P);
-  if (!chunk_hist_fits(P, n_chunks)) return;
-  for (int base = 0; base < n_chunks; base += blockDim.x) {
-    int k = base + threadIdx.x;
-    int h = k < n_chunks ? P.chunk_hist[(size_t)k * nc + c] : 0;
-    int tot;
-    int pre = block_excl_scan(h, &tot);
-    if (k < n_chunks) P.chunk_hist[(size_t)k * nc + c] = run + pre;
-    run += tot;
-  }
 }
 
 // pair-test record of slot i (see RecD)
@@ -229,7 +147,8 @@ __device__ __forceinline__ int refresh_slot(const PopDev& P, int i) {
   double r = vol2rad(P.vtot[i]);
   P.rad[i] = r;
   int b = bin_find(G.n_bin, G.log_lo, G.log_hi, r);
-  P.bin[i] = (b >= 1 && b <= G.n_bin) ? b - 1 : -1;
+  int cl = P.cls[i] - 1;
+  P.cell[i] = (b >= 1 && b <= G.n_bin && cl >= 0 && cl < P.n_class) ? (b - 1) + G.n_bin * cl : -1;
   RecD q = make_rec(P, i);
   P.recd[i] = q;
   P.recf[i] = to_f32(q);
@@ -242,64 +161,164 @@ __global__ void k_refresh_all(const PopDev* pops, const uint8_t* on) {
   int n = P.ctr->n_slots;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (P.alive[i]) refresh_slot(P, i);
-    else P.bin[i] = -1;
+    else P.cell[i] = -1;
   }
 }
 
-// sort pass 3: deterministic stable scatter (slot order within each cell).
-// Warp w of a block owns slots [w*256, (w+1)*256) of the chunk; ranks
-// inside a 32-slot tile come from __match_any_sync.
-__global__ void k_sort_scatter(const PopDev* pops) {
-  const PopDev& P = pops[blockIdx.y];
-  int chunk = blockIdx.x;
-  int n_chunks = n_chunks_of(P);
-  if (chunk >= n_chunks) return;
-  if (!chunk_hist_fits(P, n_chunks)) return;
-  extern __shared__ int wc[];  // [kSortWarps][n_cells]
-  int nc = P.n_cells;
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int k = threadIdx.x; k < kSortWarps * nc; k += blockDim.x) wc[k] = 0;
-  __syncthreads();
-  int n = P.ctr->n_slots;
-  int nb = P.grid->n_bin;
-  int base = chunk * kChunk + w * kWarpSlots;
-  for (int t = 0; t < kWarpSlots; t += 32) {
-    int i = base + t + lane;
-    int key = -1;
-    if (i < n && P.alive[i] && P.bin[i] >= 0 && P.bin[i] < nb && P.cls[i] >= 1 && P.cls[i] <= P.n_class)
-      key = P.bin[i] + nb * (P.cls[i] - 1);
-    unsigned peers = __match_any_sync(0xffffffffu, key);
-    int leader = __ffs(peers) - 1;
-    if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
+// ---------------------------------------------------------------------------
+// aero_sorted's bin lists rebuilt as one deterministic, stable counting sort
+// of the slots by cell (slot order within each cell), for every population in
+// one cooperative launch.  The grid is persistent (co-resident blocks looping
+// over work items) and the phases are separated by grid-wide barriers:
+//   1. per-chunk histograms of the cell keys (kChunk slots per item; warp-
+//      aggregated shared-memory counts), stored cell-major:
+//      chunk_hist[cell * n_chunks + chunk]; the occupied bin range is reset
+//   2. per cell (one warp): total over the chunks, occupied bin range
+//   3. per cell (one warp): start of the cell and the exclusive scan of its
+//      chunk column (the chunk's first position inside the cell)
+//   4. per chunk: scatter; warp w of the block owns slots
+//      [w * kWarpSlots, (w + 1) * kWarpSlots) of the chunk and ranks slots of
+//      one cell inside a 32-slot tile with __match_any_sync
+__device__ __forceinline__ int warp_sum_int(int v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, int n_pop, int max_chunks,
+                                                           int max_cells) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ int sm[];  // [kSortWarps][max_cells]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long n_chunk_items = (long long)n_pop * max_chunks;
+  // phase 1
+  if (blockIdx.x == 0)
+    for (int k = threadIdx.x; k < n_pop; k += blockDim.x) {
+      pops[k].ctr->bmin = 1 << 30;
+      pops[k].ctr->bmax = -1;
+    }
+  for (long long item = blockIdx.x; item < n_chunk_items; item += gridDim.x) {
+    const PopDev& P = pops[item / max_chunks];
+    int chunk = (int)(item % max_chunks);
+    int n_chunks = n_chunks_of(P);
+    if (chunk >= n_chunks || !chunk_hist_fits(P, n_chunks)) continue;  // the same for the whole block
+    int nc = P.n_cells;
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) sm[c] = 0;
+    __syncthreads();
+    int n = P.ctr->n_slots;
+    for (int k = threadIdx.x; k < kChunk; k += blockDim.x) {
+      int i = chunk * kChunk + k;
+      int key = i < n ? P.cell[i] : -1;
+      if (key >= nc) key = -1;
+      unsigned peers = __match_any_sync(0xffffffffu, key);
+      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&sm[key], __popc(peers));
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) P.chunk_hist[(size_t)c * n_chunks + chunk] = sm[c];
+    __syncthreads();
   }
-  __syncthreads();
-  const int* off = P.chunk_hist + (size_t)chunk * nc;
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-    int run = off[c];
-    for (int q = 0; q < kSortWarps; q++) {
-      int x = wc[q * nc + c];
-      wc[q * nc + c] = run;
-      run += x;
+  grid.sync();
+  // phase 2
+  const long long warp_id = (long long)blockIdx.x * kSortWarps + w;
+  const long long n_warps = (long long)gridDim.x * kSortWarps;
+  const long long n_cell_items = (long long)n_pop * max_cells;
+  for (long long item = warp_id; item < n_cell_items; item += n_warps) {
+    const PopDev& P = pops[item / max_cells];
+    int c = (int)(item % max_cells);
+    int n_chunks = n_chunks_of(P);
+    if (c >= P.n_cells) continue;
+    int s = 0;
+    if (n_chunks > 0 && chunk_hist_fits(P, n_chunks)) {
+      const int* col = P.chunk_hist + (size_t)c * n_chunks;
+      for (int k = lane; k < n_chunks; k += 32) s += col[k];
+    }
+    s = warp_sum_int(s);
+    if (lane == 0) {
+      P.cell_count[c] = s;
+      if (s > 0 && P.grid->n_bin > 0) {
+        int b = c % P.grid->n_bin;
+        atomicMin(&P.ctr->bmin, b);
+        atomicMax(&P.ctr->bmax, b);
+      }
     }
   }
-  __syncthreads();
-  unsigned lt = (1u << lane) - 1u;
-  for (int t = 0; t < kWarpSlots; t += 32) {
-    int i = base + t + lane;
-    int key = -1;
-    if (i < n && P.alive[i] && P.bin[i] >= 0 && P.bin[i] < nb && P.cls[i] >= 1 && P.cls[i] <= P.n_class)
-      key = P.bin[i] + nb * (P.cls[i] - 1);
-    unsigned peers = __match_any_sync(0xffffffffu, key);
-    int leader = __ffs(peers) - 1;
-    int pos = 0;
-    if (key >= 0) pos = wc[w * nc + key] + __popc(peers & lt);
-    __syncwarp();
-    if (key >= 0 && lane == leader) wc[w * nc + key] += __popc(peers);
-    __syncwarp();
-    if (key >= 0) {
-      if (pos >= 0 && pos < P.cap) P.list[pos] = i;
-      else bad_index(P.ctr, kBadScatterPos, pos);
+  grid.sync();
+  // phase 3
+  for (long long item = warp_id; item < n_cell_items; item += n_warps) {
+    const PopDev& P = pops[item / max_cells];
+    int c = (int)(item % max_cells);
+    int n_chunks = n_chunks_of(P);
+    int nc = P.n_cells;
+    if (c >= nc) continue;
+    int start = 0;
+    for (int q = lane; q < c; q += 32) start += P.cell_count[q];
+    start = warp_sum_int(start);
+    if (lane == 0) {
+      P.cell_start[c] = start;
+      if (c == nc - 1) P.cell_start[nc] = start + P.cell_count[c];
     }
+    if (n_chunks == 0 || !chunk_hist_fits(P, n_chunks)) continue;
+    int* col = P.chunk_hist + (size_t)c * n_chunks;
+    int run = start;
+    for (int base = 0; base < n_chunks; base += 32) {
+      int k = base + lane;
+      int h = k < n_chunks ? col[k] : 0;
+      int x = h;
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (k < n_chunks) col[k] = run + x - h;
+      run += __shfl_sync(0xffffffffu, x, 31);
+    }
+  }
+  grid.sync();
+  // phase 4
+  for (long long item = blockIdx.x; item < n_chunk_items; item += gridDim.x) {
+    const PopDev& P = pops[item / max_chunks];
+    int chunk = (int)(item % max_chunks);
+    int n_chunks = n_chunks_of(P);
+    if (chunk >= n_chunks || !chunk_hist_fits(P, n_chunks)) continue;
+    int nc = P.n_cells;
+    for (int k = threadIdx.x; k < kSortWarps * nc; k += blockDim.x) sm[k] = 0;
+    __syncthreads();
+    int n = P.ctr->n_slots;
+    int base = chunk * kChunk + w * kWarpSlots;
+    for (int t = 0; t < kWarpSlots; t += 32) {
+      int i = base + t + lane;
+      int key = i < n ? P.cell[i] : -1;
+      if (key >= nc) key = -1;
+      unsigned peers = __match_any_sync(0xffffffffu, key);
+      if (key >= 0 && lane == __ffs(peers) - 1) sm[w * nc + key] += __popc(peers);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+      int run = P.chunk_hist[(size_t)c * n_chunks + chunk];
+      for (int q = 0; q < kSortWarps; q++) {
+        int x = sm[q * nc + c];
+        sm[q * nc + c] = run;
+        run += x;
+      }
+    }
+    __syncthreads();
+    unsigned lt = (1u << lane) - 1u;
+    for (int t = 0; t < kWarpSlots; t += 32) {
+      int i = base + t + lane;
+      int key = i < n ? P.cell[i] : -1;
+      if (key >= nc) key = -1;
+      unsigned peers = __match_any_sync(0xffffffffu, key);
+      int leader = __ffs(peers) - 1;
+      int pos = 0;
+      if (key >= 0) pos = sm[w * nc + key] + __popc(peers & lt);
+      __syncwarp();
+      if (key >= 0 && lane == leader) sm[w * nc + key] += __popc(peers);
+      __syncwarp();
+      if (key >= 0) {
+        if (pos >= 0 && pos < P.cap) P.list[pos] = i;
+        else bad_index(P.ctr, kBadScatterPos, pos);
+      }
+    }
+    __syncthreads();
   }
 }
 

@@ -16,7 +16,7 @@ namespace pmc {
 
 __device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
   P.alive[i] = 0;
-  P.bin[i] = -1;
+  P.cell[i] = -1;
 }
 
 // Decisions of coagulate_weighting (coagulation.F90:855-892).

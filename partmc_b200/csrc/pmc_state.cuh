@@ -95,7 +95,7 @@ struct PopCtr {
   long long kmax_warn;
   long long redraws;
   int status;        // first error code seen
-  int out_of_grid;
+  int out_of_grid;   // unused (kept for the layout of the counter block)
   int bmin, bmax;    // occupied bin range after a sort (-1 if empty)
   unsigned long long rmin_bits, rmax_bits;  // radius range (positive doubles)
   int new_slots, new_ids;  // allocations in the current apply phase
@@ -157,7 +157,10 @@ struct PopDev {
   int* hyst;
   int* frozen;
   uint8_t* alive;
-  int* bin;  // 0-based bin of each live slot, -1 dead or off the grid
+  // sort key of each slot: the (bin, class) cell bin + n_bin * class
+  // (0-based) of a live particle on the grid, -1 for a dead slot or a
+  // particle off the grid
+  int* cell;
 
   const double* density;  // [n_spec]
 
