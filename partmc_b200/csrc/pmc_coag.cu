@@ -998,7 +998,7 @@ void run_sort(Ctx& c) {
     max_cells = std::max(max_cells, c.pops[k].h.n_cells);
     units += (long long)c.n_slots_host[k];
   }
-  size_t smem = sizeof(int) * kSortWarps * (size_t)max_cells;
+  size_t smem = sizeof(int) * (kSortWarps + 1) * (size_t)max_cells;
   if (smem != c.sort_smem) {
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_all, kSortThreads, smem));

@@ -169,28 +169,38 @@ __global__ void k_refresh_all(const PopDev* pops, const uint8_t* on) {
 // aero_sorted's bin lists rebuilt as one deterministic, stable counting sort
 // of the slots by cell (slot order within each cell), for every population in
 // one cooperative launch.  The grid is persistent (co-resident blocks looping
-// over work items) and the phases are separated by grid-wide barriers:
-//   1. per-chunk histograms of the cell keys (kChunk slots per item; warp-
-//      aggregated shared-memory counts), stored cell-major:
-//      chunk_hist[cell * n_chunks + chunk]; the occupied bin range is reset
-//   2. per cell (one warp): total over the chunks, occupied bin range
-//   3. per cell (one warp): start of the cell and the exclusive scan of its
-//      chunk column (the chunk's first position inside the cell)
-//   4. per chunk: scatter; warp w of the block owns slots
-//      [w * kWarpSlots, (w + 1) * kWarpSlots) of the chunk and ranks slots of
-//      one cell inside a 32-slot tile with __match_any_sync
-__device__ __forceinline__ int warp_sum_int(int v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
+// over work items); two grid-wide barriers separate three phases:
+//   1. per chunk of kChunk slots: the cell keys go to registers (thread
+//      (w, lane) holds slots w * kWarpSlots + j * 32 + lane, j < kKeysPerThread)
+//      and a warp-aggregated histogram to chunk_hist, cell-major
+//      (chunk_hist[cell * n_chunks + chunk]); the occupied bin range is reset
+//   2. per cell (one warp): exclusive scan of its chunk column in place and
+//      the cell total; the occupied bin range
+//   3. per chunk: the cell starts (a block scan of the totals; the chunk-0
+//      block of each population stores them), then the scatter, ranking the
+//      slots of one cell inside a 32-slot tile with __match_any_sync.  A block
+//      reuses the keys it loaded in phase 1 for the same chunk.
+constexpr int kKeysPerThread = kWarpSlots / 32;
+
+__device__ __forceinline__ void sort_load_keys(const PopDev& P, int chunk, int n, int nc, int w, int lane,
+                                               int* keys) {
+#pragma unroll
+  for (int j = 0; j < kKeysPerThread; j++) {
+    int i = chunk * kChunk + w * kWarpSlots + j * 32 + lane;
+    int key = i < n ? P.cell[i] : -1;
+    keys[j] = key < nc ? key : -1;
+  }
 }
 
 __global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, int n_pop, int max_chunks,
                                                            int max_cells) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  extern __shared__ int sm[];  // [kSortWarps][max_cells]
+  extern __shared__ int sm[];  // [kSortWarps][max_cells] counters, then [max_cells] cell starts
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long long n_chunk_items = (long long)n_pop * max_chunks;
+  int keys[kKeysPerThread];
+  long long kept = -1;  // chunk item whose keys are in registers
   // phase 1
   if (blockIdx.x == 0)
     for (int k = threadIdx.x; k < n_pop; k += blockDim.x) {
@@ -203,15 +213,14 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, i
     int n_chunks = n_chunks_of(P);
     if (chunk >= n_chunks || !chunk_hist_fits(P, n_chunks)) continue;  // the same for the whole block
     int nc = P.n_cells;
+    sort_load_keys(P, chunk, P.ctr->n_slots, nc, w, lane, keys);
+    kept = item;
     for (int c = threadIdx.x; c < nc; c += blockDim.x) sm[c] = 0;
     __syncthreads();
-    int n = P.ctr->n_slots;
-    for (int k = threadIdx.x; k < kChunk; k += blockDim.x) {
-      int i = chunk * kChunk + k;
-      int key = i < n ? P.cell[i] : -1;
-      if (key >= nc) key = -1;
-      unsigned peers = __match_any_sync(0xffffffffu, key);
-      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&sm[key], __popc(peers));
+#pragma unroll
+    for (int j = 0; j < kKeysPerThread; j++) {
+      unsigned peers = __match_any_sync(0xffffffffu, keys[j]);
+      if (keys[j] >= 0 && lane == __ffs(peers) - 1) atomicAdd(&sm[keys[j]], __popc(peers));
     }
     __syncthreads();
     for (int c = threadIdx.x; c < nc; c += blockDim.x) P.chunk_hist[(size_t)c * n_chunks + chunk] = sm[c];
@@ -221,21 +230,37 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, i
   // phase 2
   const long long warp_id = (long long)blockIdx.x * kSortWarps + w;
   const long long n_warps = (long long)gridDim.x * kSortWarps;
-  const long long n_cell_items = (long long)n_pop * max_cells;
-  for (long long item = warp_id; item < n_cell_items; item += n_warps) {
+  for (long long item = warp_id; item < (long long)n_pop * max_cells; item += n_warps) {
     const PopDev& P = pops[item / max_cells];
     int c = (int)(item % max_cells);
-    int n_chunks = n_chunks_of(P);
     if (c >= P.n_cells) continue;
-    int s = 0;
+    int n_chunks = n_chunks_of(P);
+    int run = 0;
     if (n_chunks > 0 && chunk_hist_fits(P, n_chunks)) {
-      const int* col = P.chunk_hist + (size_t)c * n_chunks;
-      for (int k = lane; k < n_chunks; k += 32) s += col[k];
+      int* col = P.chunk_hist + (size_t)c * n_chunks;
+      for (int base = 0; base < n_chunks; base += 128) {
+        int h[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          int k = base + u * 32 + lane;
+          h[u] = k < n_chunks ? col[k] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          int x = h[u];
+          for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+          }
+          int k = base + u * 32 + lane;
+          if (k < n_chunks) col[k] = run + x - h[u];
+          run += __shfl_sync(0xffffffffu, x, 31);
+        }
+      }
     }
-    s = warp_sum_int(s);
     if (lane == 0) {
-      P.cell_count[c] = s;
-      if (s > 0 && P.grid->n_bin > 0) {
+      P.cell_count[c] = run;
+      if (run > 0 && P.grid->n_bin > 0) {
         int b = c % P.grid->n_bin;
         atomicMin(&P.ctr->bmin, b);
         atomicMax(&P.ctr->bmax, b);
@@ -244,56 +269,43 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, i
   }
   grid.sync();
   // phase 3
-  for (long long item = warp_id; item < n_cell_items; item += n_warps) {
-    const PopDev& P = pops[item / max_cells];
-    int c = (int)(item % max_cells);
-    int n_chunks = n_chunks_of(P);
-    int nc = P.n_cells;
-    if (c >= nc) continue;
-    int start = 0;
-    for (int q = lane; q < c; q += 32) start += P.cell_count[q];
-    start = warp_sum_int(start);
-    if (lane == 0) {
-      P.cell_start[c] = start;
-      if (c == nc - 1) P.cell_start[nc] = start + P.cell_count[c];
-    }
-    if (n_chunks == 0 || !chunk_hist_fits(P, n_chunks)) continue;
-    int* col = P.chunk_hist + (size_t)c * n_chunks;
-    int run = start;
-    for (int base = 0; base < n_chunks; base += 32) {
-      int k = base + lane;
-      int h = k < n_chunks ? col[k] : 0;
-      int x = h;
-      for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      if (k < n_chunks) col[k] = run + x - h;
-      run += __shfl_sync(0xffffffffu, x, 31);
-    }
-  }
-  grid.sync();
-  // phase 4
+  int* starts = sm + kSortWarps * max_cells;
   for (long long item = blockIdx.x; item < n_chunk_items; item += gridDim.x) {
     const PopDev& P = pops[item / max_chunks];
     int chunk = (int)(item % max_chunks);
     int n_chunks = n_chunks_of(P);
-    if (chunk >= n_chunks || !chunk_hist_fits(P, n_chunks)) continue;
     int nc = P.n_cells;
+    if (chunk == 0 && n_chunks == 0) {  // an empty population still gets its (zero) cell starts
+      for (int c = threadIdx.x; c <= nc; c += blockDim.x) P.cell_start[c] = 0;
+      continue;
+    }
+    if (chunk >= n_chunks || !chunk_hist_fits(P, n_chunks)) continue;
+    int n = P.ctr->n_slots;
+    if (item != kept) sort_load_keys(P, chunk, n, nc, w, lane, keys);
+    // cell starts
+    int carry = 0;
+    for (int base = 0; base < nc; base += blockDim.x) {
+      int c = base + threadIdx.x;
+      int v = c < nc ? P.cell_count[c] : 0;
+      int tot;
+      int pre = block_excl_scan(v, &tot);
+      if (c < nc) starts[c] = carry + pre;
+      carry += tot;
+    }
+    if (chunk == 0) {
+      for (int c = threadIdx.x; c < nc; c += blockDim.x) P.cell_start[c] = starts[c];
+      if (threadIdx.x == 0) P.cell_start[nc] = carry;
+    }
     for (int k = threadIdx.x; k < kSortWarps * nc; k += blockDim.x) sm[k] = 0;
     __syncthreads();
-    int n = P.ctr->n_slots;
-    int base = chunk * kChunk + w * kWarpSlots;
-    for (int t = 0; t < kWarpSlots; t += 32) {
-      int i = base + t + lane;
-      int key = i < n ? P.cell[i] : -1;
-      if (key >= nc) key = -1;
-      unsigned peers = __match_any_sync(0xffffffffu, key);
-      if (key >= 0 && lane == __ffs(peers) - 1) sm[w * nc + key] += __popc(peers);
+#pragma unroll
+    for (int j = 0; j < kKeysPerThread; j++) {
+      unsigned peers = __match_any_sync(0xffffffffu, keys[j]);
+      if (keys[j] >= 0 && lane == __ffs(peers) - 1) sm[w * nc + keys[j]] += __popc(peers);
     }
     __syncthreads();
     for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-      int run = P.chunk_hist[(size_t)c * n_chunks + chunk];
+      int run = starts[c] + P.chunk_hist[(size_t)c * n_chunks + chunk];
       for (int q = 0; q < kSortWarps; q++) {
         int x = sm[q * nc + c];
         sm[q * nc + c] = run;
@@ -302,10 +314,10 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, i
     }
     __syncthreads();
     unsigned lt = (1u << lane) - 1u;
-    for (int t = 0; t < kWarpSlots; t += 32) {
-      int i = base + t + lane;
-      int key = i < n ? P.cell[i] : -1;
-      if (key >= nc) key = -1;
+#pragma unroll
+    for (int j = 0; j < kKeysPerThread; j++) {
+      int key = keys[j];
+      int i = chunk * kChunk + w * kWarpSlots + j * 32 + lane;
       unsigned peers = __match_any_sync(0xffffffffu, key);
       int leader = __ffs(peers) - 1;
       int pos = 0;
