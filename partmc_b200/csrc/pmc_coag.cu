@@ -74,6 +74,7 @@ struct ScanJob {
   long long* out;
   long long n_max;
   const long long* nd;
+  long long* total_out;  // optional second copy of the total at a fixed address
 };
 struct ScanJobs {
   ScanJob j[kScanMaxJobs];
@@ -105,7 +106,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
   long long n = scan_n(J.n_max, J.nd);
   long long nb = (n + kScanTile - 1) / kScanTile;
   if (n <= 0) {
-    if (tile == 0 && threadIdx.x == 0) J.out[0] = 0;
+    if (tile == 0 && threadIdx.x == 0) {
+      J.out[0] = 0;
+      if (J.total_out) *J.total_out = 0;
+    }
     return;
   }
   if (tile >= nb) return;
@@ -157,7 +161,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
     if (i < n) J.out[i] = off;
     off += v[k];
   }
-  if (tile == nb - 1 && threadIdx.x == 0) J.out[n] = carry_sh + agg;
+  if (tile == nb - 1 && threadIdx.x == 0) {
+    J.out[n] = carry_sh + agg;
+    if (J.total_out) *J.total_out = carry_sh + agg;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -166,9 +173,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
 
 // accepted samples in sample order: event e gets its sample index, its two
 // slots and its global pair
-__global__ void k_compact_flags(const uint8_t* flag, const long long* off, long long n,
+__global__ void k_compact_flags(const uint8_t* flag, const long long* off, const long long* n_samples,
                                 long long* outw, const int2* ev, const int* ev_gp, int2* ev_c,
                                 int* gp_c) {
+  long long n = *n_samples;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     if (flag[i]) {
@@ -659,6 +667,7 @@ struct ScanArg {
   long long n;
   const long long* nd;
   long long* out;
+  long long* total_out = nullptr;
 };
 
 template <class T>
@@ -671,6 +680,7 @@ void scan_multi(Ctx& c, std::initializer_list<ScanArg<T>> args) {
     jobs.j[k].out = a.out;
     jobs.j[k].n_max = a.n;
     jobs.j[k].nd = a.nd;
+    jobs.j[k].total_out = a.total_out;
     nb = std::max(nb, (a.n + kScanTile - 1) / kScanTile);
     k++;
   }
@@ -1413,7 +1423,7 @@ void step_parallel(Ctx& c, int kt) {
   bool flat = true;
   for (int k = 0; k < c.n_pop; k++) flat = flat && c.pops[k].h.flat;
   float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
-  long long redraws = 0, Qprev = 0;
+  long long redraws = 0, Qprev = 0, last_set_losers = 0;
   c.last_set_losers = c.last_pp_lost = c.last_events = c.last_ops = 0;
   std::vector<long long> hw(3 + 2 * (size_t)c.n_pop);
   std::vector<int> per_pop(4 * (size_t)c.n_pop);
@@ -1467,30 +1477,49 @@ void step_parallel(Ctx& c, int kt) {
     scan_multi<long long>(c, {{c.nwork_set.p, n_gpairs, nullptr, c.work_off.p},
                               {c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p},
                               {c.nprio.p, n_gpairs, nullptr, c.prio_off.p}});
-    long long* popw = c.n_dev.p + 4;
-    k_pop_work<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.pop_pair_base.p, c.n_pop, c.work_off.p, c.pp_off.p,
-                                                            popw);
-    note_launch();
-    // one read-back: totals and per-population work
-    CK(cudaMemcpyAsync(&hw[0], c.work_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(&hw[1], c.pp_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(&hw[2], c.prio_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(&hw[3], popw, sizeof(long long) * 2 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
-    unsigned long long pair_scan_err = 0;
-    CK(cudaMemcpyAsync(&pair_scan_err, c.scan_err.p, sizeof(pair_scan_err), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
-    if (pair_scan_err) {
-      CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(pair_scan_err), c.stream));
-      throw Fail(PMC_ERR_TIMEOUT);
+    long long W, Q;
+    if (round == 0) {
+      long long* popw = c.n_dev.p + 4;
+      if (c.n_pop > 1) {
+        k_pop_work<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.pop_pair_base.p, c.n_pop, c.work_off.p,
+                                                                c.pp_off.p, popw);
+        note_launch();
+      }
+      // one read-back: totals and per-population work
+      CK(cudaMemcpyAsync(&hw[0], c.work_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(&hw[1], c.pp_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(&hw[2], c.prio_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+      if (c.n_pop > 1)
+        CK(cudaMemcpyAsync(&hw[3], popw, sizeof(long long) * 2 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+      unsigned long long pair_scan_err = 0;
+      CK(cudaMemcpyAsync(&pair_scan_err, c.scan_err.p, sizeof(pair_scan_err), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+      if (pair_scan_err) {
+        CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(pair_scan_err), c.stream));
+        throw Fail(PMC_ERR_TIMEOUT);
+      }
+      W = hw[0];
+      Q = hw[1];
+      if (c.n_pop == 1) {
+        hw[3] = W;
+        hw[4] = Q;
+      }
+      if (hw[2] + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
+    } else {
+      // later rounds redraw the losers of the previous round: their count
+      // bounds this round's samples, and every kernel reads the exact count
+      // from the device, so the round needs no read-back before its launches
+      W = last_set_losers;
+      Q = Qprev;
+      for (int k = 0; k < c.n_pop; k++) {
+        hw[3 + 2 * k] = W;
+        hw[3 + 2 * k + 1] = Q;
+      }
     }
-    long long W = hw[0], Q0 = hw[1], Ptot = hw[2];
-    long long Q = round == 0 ? Q0 : Qprev;
-    if (Ptot + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
     // capacity for the worst case of this round: every sample creates a
     // particle and every target operation makes kMaxCopies - 1 copies
     for (int k = 0; k < c.n_pop; k++) {
-      long long qk = round == 0 ? hw[3 + 2 * k + 1] : Q;
-      long long need = (long long)c.n_slots_host[k] + hw[3 + 2 * k] + (kMaxCopies - 1) * qk;
+      long long need = (long long)c.n_slots_host[k] + hw[3 + 2 * k] + (kMaxCopies - 1) * hw[3 + 2 * k + 1];
       if (need > c.pops[k].h.cap) {
         int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
         relayout(c, k, nc, false);  // slot numbers kept
@@ -1542,12 +1571,14 @@ void step_parallel(Ctx& c, int kt) {
       set_n_dev(c, Q);
       launch_pp(c, kt, Q);
     }
-    // accepted per-set samples in sample order; their count E stays on the
-    // device (flag_off[W])
-    const long long* Ed = c.flag_off.p + W;
+    // accepted per-set samples in sample order; the sample count is
+    // work_off[n_gpairs] and the event count E goes to round_dev[1], both on
+    // the device
+    const long long* Wd = c.work_off.p + n_gpairs;
+    long long* Ed = c.round_dev.p + 1;
     if (W > 0) {
-      scan_dev(c, c.flag.p, W, nullptr, c.flag_off.p);
-      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, W, c.ev_w.p, c.ev.p,
+      scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, Ed}});
+      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, Wd, c.ev_w.p, c.ev.p,
                                                              c.ev_gp.p, c.ev_c.p, c.gp_c.p);
       note_launch();
       k_resolve_set<<<grid_for(W, 256), 256, 0, c.stream>>>(
@@ -1597,6 +1628,7 @@ void step_parallel(Ctx& c, int kt) {
     long long set_losers = 0, pp_lost = 0, E = 0;
     CK(cudaMemcpyAsync(&set_losers, c.round_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     if (W > 0) CK(cudaMemcpyAsync(&E, Ed, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    last_set_losers = set_losers;
     if (Q > 0) CK(cudaMemcpyAsync(&pp_lost, c.lost_off.p + Q, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
     unsigned long long scan_err = 0;
