@@ -147,6 +147,13 @@ int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t *next_id);
 /* PMC_MODE_FP64 (default), PMC_MODE_MIXED or PMC_MODE_REPLAY. */
 int pmc_coag_gpu_set_mode(pmc_coag_gpu_ctx *ctx, int mode);
 
+/* Run the redraw rounds of a step (every round after the first) as one CUDA
+ * graph whose loop condition is set on the device (enable = 1, the default),
+ * or from a host loop (enable = 0).  Both give the same particles, bit for
+ * bit.  A step with per-particle (accelerated) work always uses the host
+ * loop.  No counterpart in the reference (an execution choice). */
+int pmc_coag_gpu_set_graphs(pmc_coag_gpu_ctx *ctx, int enable);
+
 /* Replay stream: uniforms in [0, 1) consumed in the reference's order
  * (pmc_random, rand.F90:138-167).  Copied to the device. */
 int pmc_coag_gpu_replay_set(pmc_coag_gpu_ctx *ctx, const double *u, int64_t n);

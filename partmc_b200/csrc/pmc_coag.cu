@@ -80,21 +80,22 @@ struct ScanJobs {
   ScanJob j[kScanMaxJobs];
 };
 
-// tile status word: epoch (20 bits) | flag (2 bits: 1 aggregate, 2 inclusive
-// prefix) | value (42 bits).  A word from another launch has another epoch,
-// so the status array needs no reset between launches.
-__device__ __forceinline__ unsigned long long scan_word(uint32_t epoch, unsigned flag, long long v) {
-  return ((unsigned long long)(epoch & 0xFFFFFu) << 44) | ((unsigned long long)flag << 42) |
-         ((unsigned long long)v & ((1ULL << 42) - 1));
+// tile status word: flag (2 bits: 1 aggregate, 2 inclusive prefix) | value
+// (62 bits); 0 = not published.  The last block of a launch to finish
+// clears the launch's words, so the array is all zero between launches and
+// a launch can be replayed (CUDA graphs) without host bookkeeping.
+__device__ __forceinline__ unsigned long long scan_word(unsigned flag, long long v) {
+  return ((unsigned long long)flag << 62) | ((unsigned long long)v & ((1ULL << 62) - 1));
 }
 
 template <class T>
 __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigned long long* status,
                                                           int status_stride, unsigned* tile_ctr,
-                                                          uint32_t epoch, unsigned long long* err) {
+                                                          unsigned* done_ctr, unsigned long long* err) {
   const ScanJob J = jobs.j[blockIdx.y];
   __shared__ unsigned tile_sh;
   __shared__ long long carry_sh;
+  unsigned long long* st = status + (size_t)blockIdx.y * status_stride;
   if (threadIdx.x == 0) {
     // tiles in the order blocks start, so a tile only waits on running blocks
     unsigned t = atomicAdd(&tile_ctr[blockIdx.y], 1u);
@@ -110,60 +111,68 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
       J.out[0] = 0;
       if (J.total_out) *J.total_out = 0;
     }
-    return;
-  }
-  if (tile >= nb) return;
-  const T* in = (const T*)J.in;
-  long long base = tile * kScanTile + (long long)threadIdx.x * kScanItems;
-  long long v[kScanItems];
-  long long s = 0;
+  } else if (tile < nb) {
+    const T* in = (const T*)J.in;
+    long long base = tile * kScanTile + (long long)threadIdx.x * kScanItems;
+    long long v[kScanItems];
+    long long s = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; k++) {
-    long long i = base + k;
-    v[k] = i < n ? (long long)in[i] : 0;
-    s += v[k];
-  }
-  long long agg;
-  long long pre = block_excl_scan_ll(s, &agg);
-  unsigned long long* st = status + (size_t)blockIdx.y * status_stride;
-  if (threadIdx.x == 0) {
-    long long excl = 0;
-    if (tile == 0) {
-      atomicExch(&st[0], scan_word(epoch, 2u, agg));
-    } else {
-      atomicExch(&st[tile], scan_word(epoch, 1u, agg));
-      long long look = tile - 1;
-      int spins = 0;
-      while (look >= 0) {
-        unsigned long long w = *(volatile unsigned long long*)&st[look];
-        unsigned flag = (unsigned)((w >> 42) & 3u);
-        if ((uint32_t)(w >> 44) != (epoch & 0xFFFFFu) || flag == 0) {
-          if (++spins > kScanSpinLimit) {
-            atomicAdd(err, 1ULL);
-            break;
-          }
-          __nanosleep(32);
-          continue;
-        }
-        excl += (long long)(w & ((1ULL << 42) - 1));
-        if (flag == 2u) break;
-        look--;
-      }
-      atomicExch(&st[tile], scan_word(epoch, 2u, excl + agg));
+    for (int k = 0; k < kScanItems; k++) {
+      long long i = base + k;
+      v[k] = i < n ? (long long)in[i] : 0;
+      s += v[k];
     }
-    carry_sh = excl;
-  }
-  __syncthreads();
-  long long off = carry_sh + pre;
+    long long agg;
+    long long pre = block_excl_scan_ll(s, &agg);
+    if (threadIdx.x == 0) {
+      long long excl = 0;
+      if (tile == 0) {
+        atomicExch(&st[0], scan_word(2u, agg));
+      } else {
+        atomicExch(&st[tile], scan_word(1u, agg));
+        long long look = tile - 1;
+        int spins = 0;
+        while (look >= 0) {
+          unsigned long long w = *(volatile unsigned long long*)&st[look];
+          unsigned flag = (unsigned)(w >> 62);
+          if (flag == 0) {
+            if (++spins > kScanSpinLimit) {
+              atomicAdd(err, 1ULL);
+              break;
+            }
+            __nanosleep(32);
+            continue;
+          }
+          excl += (long long)(w & ((1ULL << 62) - 1));
+          if (flag == 2u) break;
+          look--;
+        }
+        atomicExch(&st[tile], scan_word(2u, excl + agg));
+      }
+      carry_sh = excl;
+    }
+    __syncthreads();
+    long long off = carry_sh + pre;
 #pragma unroll
-  for (int k = 0; k < kScanItems; k++) {
-    long long i = base + k;
-    if (i < n) J.out[i] = off;
-    off += v[k];
+    for (int k = 0; k < kScanItems; k++) {
+      long long i = base + k;
+      if (i < n) J.out[i] = off;
+      off += v[k];
+    }
+    if (tile == nb - 1 && threadIdx.x == 0) {
+      J.out[n] = carry_sh + agg;
+      if (J.total_out) *J.total_out = carry_sh + agg;
+    }
   }
-  if (tile == nb - 1 && threadIdx.x == 0) {
-    J.out[n] = carry_sh + agg;
-    if (J.total_out) *J.total_out = carry_sh + agg;
+  // the last block of this job to finish clears the job's status words
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned d = atomicAdd(&done_ctr[blockIdx.y], 1u);
+    if (d == gridDim.x - 1) {
+      for (unsigned k = 0; k < gridDim.x; k++) st[k] = 0ULL;
+      done_ctr[blockIdx.y] = 0;
+      __threadfence();
+    }
   }
 }
 
@@ -529,6 +538,14 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   int max_rounds = 32;
   int n_sm = 148;        // multiprocessors of the device
+  // redraw rounds as a CUDA graph
+  bool use_graph = true;
+  cudaStream_t cap_stream = nullptr;  // capture stream
+  cudaGraph_t rg_graph = nullptr;
+  cudaGraphExec_t rg_exec = nullptr;
+  std::vector<long long> rg_key;
+  long long rg_nodes = 0, rg_builds = 0;
+  DevBuf<long long> graph_stats;
   size_t sort_smem = 0;  // dynamic shared memory the sort grid was sized for
   int sort_blocks = 0;   // co-resident sort blocks at that size
   // per-round buffers
@@ -554,9 +571,8 @@ struct Ctx {
   DevBuf<long long> id_base_set, id_base_pp;
   DevBuf<unsigned long long> scan_status;  // look-back tile words
   size_t scan_status_n = 0;                // words cleared so far
-  DevBuf<unsigned> scan_ctr;               // per-job tile counters (re-armed by the kernel)
+  DevBuf<unsigned> scan_ctr;               // per-job tile and finished-block counters (re-armed by the kernel)
   DevBuf<unsigned long long> scan_err;     // look-backs that gave up
-  uint32_t scan_epoch = 0;
   DevBuf<long long> n_dev;  // device scalars
   // staging for upload / download (shared by all populations; every call
   // synchronises before it returns)
@@ -671,7 +687,8 @@ struct ScanArg {
 };
 
 template <class T>
-void scan_multi(Ctx& c, std::initializer_list<ScanArg<T>> args) {
+void scan_multi(Ctx& c, std::initializer_list<ScanArg<T>> args, cudaStream_t st = nullptr) {
+  if (!st) st = c.stream;
   ScanJobs jobs{};
   int k = 0;
   long long nb = 1;
@@ -688,18 +705,12 @@ void scan_multi(Ctx& c, std::initializer_list<ScanArg<T>> args) {
   if (nb > (1LL << 30)) throw Fail(PMC_ERR_CAPACITY);
   c.scan_status.reserve((size_t)kScanMaxJobs * nb);
   if (c.scan_status.n > c.scan_status_n) {  // fresh memory: clear it once
-    CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, c.stream));
+    CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, st));
     c.scan_status_n = c.scan_status.n;
   }
-  c.scan_epoch = (c.scan_epoch + 1) & 0xFFFFFu;
-  if (c.scan_epoch == 0) {
-    // the epoch wrapped: old words could match again, so clear them
-    CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, c.stream));
-    c.scan_epoch = 1;
-  }
   dim3 g((unsigned)nb, (unsigned)k);
-  k_scan_lb<T><<<g, kScanThreads, 0, c.stream>>>(jobs, c.scan_status.p, (int)nb, c.scan_ctr.p, c.scan_epoch,
-                                                  c.scan_err.p);
+  k_scan_lb<T><<<g, kScanThreads, 0, st>>>(jobs, c.scan_status.p, (int)nb, c.scan_ctr.p, c.scan_ctr.p + kScanMaxJobs,
+                                           c.scan_err.p);
   note_launch();
 }
 
@@ -981,10 +992,12 @@ __global__ void k_radius_minmax_masked(const PopDev* pops, const uint8_t* on) {
 
 
 // chunk counts from the host's copy of the slot counts
-void prepare_chunks(Ctx& c) {
+// chunk histograms for the current slot counts plus extra slots per
+// population (the growth a device-driven loop may add before the host looks)
+void prepare_chunks(Ctx& c, long long extra = 0) {
   for (int k = 0; k < c.n_pop; k++) {
     PopHost& ph = c.pops[k];
-    ph.h.n_chunks = (c.n_slots_host[k] + kChunk - 1) / kChunk;
+    ph.h.n_chunks = (int)((c.n_slots_host[k] + extra + kChunk - 1) / kChunk);
     int need = std::max(ph.h.n_chunks, 1) * ph.h.n_cells;
     if (need > ph.chunk_hist_cap) {
       int want = std::max(need * 2, 1024);  // headroom: slots grow inside a step
@@ -996,18 +1009,10 @@ void prepare_chunks(Ctx& c) {
   }
 }
 
-// the full sort of every population with its current grid: one cooperative
-// launch of k_sort_all on a persistent grid of co-resident blocks
-void run_sort(Ctx& c) {
-  prepare_chunks(c);
-  if (c.dirty) push_pops(c);
-  int max_chunks = 1, max_cells = 1;
-  long long units = 0;
-  for (int k = 0; k < c.n_pop; k++) {
-    max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
-    max_cells = std::max(max_cells, c.pops[k].h.n_cells);
-    units += (long long)c.n_slots_host[k];
-  }
+// one cooperative launch of k_sort_all on a persistent grid of co-resident
+// blocks, for chunk and cell counts up to max_chunks and max_cells
+// co-resident blocks of the sort for max_cells cells (its shared memory)
+size_t size_sort(Ctx& c, int max_cells) {
   size_t smem = sizeof(int) * (kSortWarps + 1) * (size_t)max_cells;
   if (smem != c.sort_smem) {
     int per_sm = 0;
@@ -1016,14 +1021,46 @@ void run_sort(Ctx& c) {
     c.sort_blocks = per_sm * c.n_sm;
     c.sort_smem = smem;
   }
+  return smem;
+}
+
+void launch_sort(Ctx& c, cudaStream_t st, int max_chunks, int max_cells) {
+  size_t smem = size_sort(c, max_cells);
   long long items = (long long)c.n_pop * max_chunks;
   int blocks = (int)std::min<long long>(c.sort_blocks, std::max<long long>(items, 1));
-  int n_pop = c.n_pop;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kSortThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   const PopDev* pops = c.d_pops;
-  void* args[] = {(void*)&pops, (void*)&n_pop, (void*)&max_chunks, (void*)&max_cells};
-  ProfScope ps(c, 1, units);
-  CK(cudaLaunchCooperativeKernel((const void*)k_sort_all, dim3(blocks), dim3(kSortThreads), args, smem, c.stream));
+  CK(cudaLaunchKernelEx(&cfg, k_sort_all, pops, c.n_pop, max_chunks, max_cells));
   note_launch();
+}
+
+int max_cells_of(const Ctx& c) {
+  int m = 1;
+  for (int k = 0; k < c.n_pop; k++) m = std::max(m, c.pops[k].h.n_cells);
+  return m;
+}
+
+// the full sort of every population with its current grid
+void run_sort(Ctx& c) {
+  prepare_chunks(c);
+  if (c.dirty) push_pops(c);
+  int max_chunks = 1;
+  long long units = 0;
+  for (int k = 0; k < c.n_pop; k++) {
+    max_chunks = std::max(max_chunks, c.pops[k].h.n_chunks);
+    units += (long long)c.n_slots_host[k];
+  }
+  ProfScope ps(c, 1, units);
+  launch_sort(c, c.stream, max_chunks, max_cells_of(c));
 }
 
 bool caches_current(const Ctx& c, const PopHost& ph) {
@@ -1154,41 +1191,41 @@ void sort_pops(Ctx& c, bool decide_grid) {
 // one step over all populations
 
 template <int KT, class T>
-void launch_test(Ctx& c, bool flat, int n_gpairs, long long W) {
+void launch_test(Ctx& c, bool flat, int n_gpairs, long long W, cudaStream_t st) {
   // sized from the round's sample count: redraw rounds are small
   int blocks = (int)std::min<long long>(148 * 8, std::max<long long>(1, (W + 255) / 256));
   if (flat)
-    k_test<KT, T, true><<<blocks, 256, 0, c.stream>>>(
+    k_test<KT, T, true><<<blocks, 256, 0, st>>>(
         c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
         c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
   else
-    k_test<KT, T, false><<<blocks, 256, 0, c.stream>>>(
+    k_test<KT, T, false><<<blocks, 256, 0, st>>>(
         c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
         c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
   note_launch();
 }
 
-void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W) {
+void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaStream_t st) {
   bool f32 = c.mode == PMC_MODE_MIXED;
   switch (kt) {
     case kKernelAdditive:
-      f32 ? launch_test<kKernelAdditive, float>(c, flat, n_gpairs, W)
-          : launch_test<kKernelAdditive, double>(c, flat, n_gpairs, W);
+      f32 ? launch_test<kKernelAdditive, float>(c, flat, n_gpairs, W, st)
+          : launch_test<kKernelAdditive, double>(c, flat, n_gpairs, W, st);
       break;
     case kKernelConstant:
-      f32 ? launch_test<kKernelConstant, float>(c, flat, n_gpairs, W)
-          : launch_test<kKernelConstant, double>(c, flat, n_gpairs, W);
+      f32 ? launch_test<kKernelConstant, float>(c, flat, n_gpairs, W, st)
+          : launch_test<kKernelConstant, double>(c, flat, n_gpairs, W, st);
       break;
     case kKernelBrown:
-      f32 ? launch_test<kKernelBrown, float>(c, flat, n_gpairs, W)
-          : launch_test<kKernelBrown, double>(c, flat, n_gpairs, W);
+      f32 ? launch_test<kKernelBrown, float>(c, flat, n_gpairs, W, st)
+          : launch_test<kKernelBrown, double>(c, flat, n_gpairs, W, st);
       break;
     case kKernelSedi:
-      f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs, W)
-          : launch_test<kKernelSedi, double>(c, flat, n_gpairs, W);
+      f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs, W, st)
+          : launch_test<kKernelSedi, double>(c, flat, n_gpairs, W, st);
       break;
     default:
-      launch_test<kKernelZero, double>(c, flat, n_gpairs, W);
+      launch_test<kKernelZero, double>(c, flat, n_gpairs, W, st);
   }
 }
 
@@ -1374,6 +1411,213 @@ __global__ void k_pop_work(const long long* pop_pair_base, int n_pop, const long
   out[2 * k + 1] = pp_off[b] - pp_off[a];
 }
 
+// ---------------------------------------------------------------------------
+// Redraw rounds as one CUDA graph.  After round 0 the host knows a bound on
+// the samples of every later round (round 0's losers) and every kernel of a
+// round reads its exact counts from the device, so the rounds up to the
+// step's end run as the body of a conditional WHILE node: k_round_begin
+// advances the round and the claim generation and clears the round's
+// scalars; k_round_end accumulates the step's statistics and sets the loop
+// condition (losers left and fewer than max_rounds rounds).  Only per-set
+// rounds run this way; a step with per-particle work keeps the host loop.
+
+__global__ void k_round_begin(uint32_t* d_round, long long* round_dev, int* per_pop, int n_per_pop) {
+  if (blockIdx.x != 0) return;
+  if (threadIdx.x == 0) {
+    d_round[0] += 1u;
+    d_round[1] += 1u;
+  }
+  for (int k = threadIdx.x; k < 4; k += blockDim.x) round_dev[k] = 0;
+  for (int k = threadIdx.x; k < n_per_pop; k += blockDim.x) per_pop[k] = 0;
+}
+
+// stats: [0] per-set losers (redraws), [1] events, [2] rounds
+__global__ void k_round_end(const long long* round_dev, long long* stats, const uint32_t* d_round, int max_rounds,
+                            PopCtr* ctrs, int n_pop, cudaGraphConditionalHandle cond) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  long long losers = round_dev[0];
+  stats[0] += losers;
+  stats[1] += round_dev[1];
+  stats[2] += 1;
+  bool more = losers > 0 && (int)d_round[0] + 1 < max_rounds;
+  if (losers > 0 && !more)
+    for (int k = 0; k < n_pop; k++)
+      if (ctrs[k].status == 0) ctrs[k].status = kErrTimeout;
+  cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
+struct RedrawBounds {
+  int kt;
+  bool flat;
+  int n_gpairs, max_pairs;
+  long long W;     // samples per round, at most
+  int max_chunks;  // sort chunks per population, at most
+  int max_cells;
+  float inflate;
+};
+
+// the kernels of one redraw round on stream st (per-set path only)
+void enqueue_redraw_round(Ctx& c, cudaStream_t st, const RedrawBounds& b, cudaGraphConditionalHandle cond) {
+  size_t ng = (size_t)b.n_gpairs + 1;
+  long long W = b.W;
+  k_round_begin<<<1, 128, 0, st>>>(c.d_round, c.round_dev.p, c.per_pop_i.p, 4 * c.n_pop);
+  note_launch();
+  launch_sort(c, st, b.max_chunks, b.max_cells);
+  {
+    dim3 gp((b.max_pairs + 127) / 128, c.n_pop);
+    k_pairs<<<gp, 128, 0, st>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, c.nprio.p,
+                                c.pair_losers.p, 1, b.inflate);
+    note_launch();
+  }
+  scan_multi<long long>(c, {{c.nwork_set.p, b.n_gpairs, nullptr, c.work_off.p},
+                            {c.nwork_pp.p, b.n_gpairs, nullptr, c.pp_off.p},
+                            {c.nprio.p, b.n_gpairs, nullptr, c.prio_off.p}}, st);
+  CK(cudaMemsetAsync(c.pair_losers.p, 0, sizeof(int) * ng, st));
+  launch_test_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
+  const long long* Wd = c.work_off.p + b.n_gpairs;
+  long long* Ed = c.round_dev.p + 1;
+  scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, Ed}}, st);
+  k_compact_flags<<<grid_for(W, 256), 256, 0, st>>>(c.flag.p, c.flag_off.p, Wd, c.ev_w.p, c.ev.p, c.ev_gp.p,
+                                                    c.ev_c.p, c.gp_c.p);
+  note_launch();
+  k_resolve_set<<<grid_for(W, 256), 256, 0, st>>>(
+      c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p,
+      c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p, c.round_dev.p);
+  note_launch();
+  scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}},
+                  st);
+  k_alloc_bases<<<1, 256, 0, st>>>(c.d_pops, c.n_pop, c.pop_pair_base.p, c.work_off.p, c.flag_off.p, 1,
+                                   c.rank_slot_set.p, c.rank_id_set.p, c.per_pop_i.p, c.slot_base_set.p,
+                                   c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p);
+  note_launch();
+  k_apply_move<<<grid_for(W * 32, 256), 256, 0, st>>>(
+      c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p, c.win_set.p,
+      c.dec_set.p, c.rank_slot_set.p, c.slot_base_set.p, c.ice_set.p);
+  note_launch();
+  k_apply_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, Ed, c.ev_c.p, c.gp_c.p,
+                                                c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
+                                                c.slot_base_set.p, c.id_base_set.p, c.ice_set.p);
+  note_launch();
+  k_round_end<<<1, 32, 0, st>>>(c.round_dev.p, c.graph_stats.p, c.d_round, c.max_rounds, c.d_ctrs, c.n_pop, cond);
+  note_launch();
+}
+
+// everything the captured launches depend on: sizes and device addresses
+std::vector<long long> redraw_key(const Ctx& c, const RedrawBounds& b) {
+  return {c.n_pop, b.kt, b.flat, b.n_gpairs, b.max_pairs, b.W, b.max_chunks, b.max_cells,
+          (long long)(b.inflate * 1e9f), c.max_rounds, c.sort_blocks, (long long)c.sort_smem,
+          (long long)c.d_pops, (long long)c.d_round, (long long)c.d_ctrs, (long long)c.round_dev.p,
+          (long long)c.per_pop_i.p, (long long)c.pop_pair_base.p, (long long)c.gpair_pop.p,
+          (long long)c.gpair_local.p, (long long)c.nwork_set.p, (long long)c.nwork_pp.p, (long long)c.nprio.p,
+          (long long)c.pair_losers.p, (long long)c.work_off.p, (long long)c.pp_off.p, (long long)c.prio_off.p,
+          (long long)c.flag.p, (long long)c.flag_off.p, (long long)c.ev.p, (long long)c.ev_gp.p,
+          (long long)c.ev_w.p, (long long)c.ev_c.p, (long long)c.gp_c.p, (long long)c.need_slot_set.p,
+          (long long)c.need_id_set.p, (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p,
+          (long long)c.rank_id_set.p, (long long)c.slot_base_set.p, (long long)c.id_base_set.p,
+          (long long)c.slot_base_pp.p, (long long)c.id_base_pp.p, (long long)c.ice_set.p,
+          (long long)c.scan_status.p, (long long)c.scan_ctr.p, (long long)c.scan_err.p,
+          (long long)c.graph_stats.p, c.mode};
+}
+
+void free_redraw_graph(Ctx& c) {
+  if (c.rg_exec) cudaGraphExecDestroy(c.rg_exec);
+  if (c.rg_graph) cudaGraphDestroy(c.rg_graph);
+  c.rg_exec = nullptr;
+  c.rg_graph = nullptr;
+  c.rg_key.clear();
+}
+
+// Run the redraw rounds of this step as the graph (captured again when a
+// bound or an address changed).  losers0: round 0's per-set losers.
+// Returns the rounds run.
+long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pairs, long long losers0,
+                           float inflate, long long* redraws, long long* events) {
+  RedrawBounds b;
+  b.kt = kt;
+  b.flat = flat;
+  b.n_gpairs = n_gpairs;
+  b.max_pairs = max_pairs;
+  // bounds rounded up so that the graph survives ordinary step-to-step changes
+  b.W = 4096;
+  while (b.W < losers0) b.W *= 2;
+  long long slots = 0;
+  for (int k = 0; k < c.n_pop; k++) slots = std::max<long long>(slots, c.n_slots_host[k]);
+  b.max_chunks = (int)((slots + b.W + kChunk - 1) / kChunk);
+  b.max_chunks = (b.max_chunks + 15) / 16 * 16;
+  b.max_cells = max_cells_of(c);
+  b.inflate = inflate;
+  // every buffer at its final size before the addresses are taken
+  prepare_chunks(c, (long long)b.max_chunks * kChunk - slots);
+  size_t w = (size_t)b.W;
+  c.flag.reserve(w + 1); c.ev.reserve(w + 1); c.flag_off.reserve(w + 2); c.ev_w.reserve(w + 1);
+  c.need_slot_set.reserve(w + 1); c.need_id_set.reserve(w + 1); c.win_set.reserve(w + 1);
+  c.dec_set.reserve(w + 1); c.ev_gp.reserve(w + 1); c.gp_c.reserve(w + 1); c.ev_c.reserve(w + 1);
+  c.ice_set.reserve(w + 1); c.rank_slot_set.reserve(w + 2); c.rank_id_set.reserve(w + 2);
+  c.graph_stats.reserve(4);
+  {
+    long long nb = std::max<long long>((b.W + kScanTile - 1) / kScanTile, (n_gpairs + kScanTile) / kScanTile);
+    c.scan_status.reserve((size_t)kScanMaxJobs * nb);
+    if (c.scan_status.n > c.scan_status_n) {
+      CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, c.stream));
+      c.scan_status_n = c.scan_status.n;
+    }
+  }
+  size_sort(c, b.max_cells);
+  if (c.dirty) push_pops(c);
+  std::vector<long long> key = redraw_key(c, b);
+  if (key != c.rg_key) {
+    free_redraw_graph(c);
+    CK(cudaGraphCreate(&c.rg_graph, 0));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, c.rg_graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, c.rg_graph, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    bool prof = c.prof;
+    c.prof = false;  // no event records inside the body
+    long long n0 = g_launches;
+    CK(cudaStreamBeginCaptureToGraph(c.cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    try {
+      enqueue_redraw_round(c, c.cap_stream, b, cond);
+    } catch (...) {
+      cudaGraph_t dummy;
+      cudaStreamEndCapture(c.cap_stream, &dummy);
+      c.prof = prof;
+      free_redraw_graph(c);
+      throw;
+    }
+    cudaGraph_t captured = nullptr;
+    CK(cudaStreamEndCapture(c.cap_stream, &captured));
+    c.prof = prof;
+    c.rg_nodes = g_launches - n0;
+    g_launches = n0;  // counted when they run
+    CK(cudaGraphInstantiate(&c.rg_exec, c.rg_graph, 0));
+    c.rg_key = key;
+    c.rg_builds++;
+  }
+  CK(cudaMemsetAsync(c.graph_stats.p, 0, sizeof(long long) * 4, c.stream));
+  CK(cudaGraphLaunch(c.rg_exec, c.stream));
+  long long st[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(st, c.graph_stats.p, sizeof(st), cudaMemcpyDeviceToHost, c.stream));
+  unsigned long long scan_err = 0;
+  CK(cudaMemcpyAsync(&scan_err, c.scan_err.p, sizeof(scan_err), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  if (scan_err) {
+    CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(scan_err), c.stream));
+    throw Fail(PMC_ERR_TIMEOUT);
+  }
+  g_launches += c.rg_nodes * st[2];
+  *redraws = st[0];
+  *events = st[1];
+  c.claim_gen += (uint32_t)st[2];
+  return st[2];
+}
+
 void step_parallel(Ctx& c, int kt) {
   k_step_reset<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.d_ctrs, c.n_pop);
   note_launch();
@@ -1424,6 +1668,7 @@ void step_parallel(Ctx& c, int kt) {
   for (int k = 0; k < c.n_pop; k++) flat = flat && c.pops[k].h.flat;
   float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
   long long redraws = 0, Qprev = 0, last_set_losers = 0;
+  bool any_pp = false;
   c.last_set_losers = c.last_pp_lost = c.last_events = c.last_ops = 0;
   std::vector<long long> hw(3 + 2 * (size_t)c.n_pop);
   std::vector<int> per_pop(4 * (size_t)c.n_pop);
@@ -1434,7 +1679,7 @@ void step_parallel(Ctx& c, int kt) {
       // every round gets a new claim generation; when the counter wraps,
       // the claim words are cleared once
       c.claim_gen++;
-      if (c.claim_gen == 0xffffffffu) {
+      if (c.claim_gen >= 0xffffffffu - 4u * (uint32_t)c.max_rounds) {  // room for a graph's rounds
         c.claim_gen = 0;
         claims_wrapped = true;
       }
@@ -1556,7 +1801,7 @@ void step_parallel(Ctx& c, int kt) {
     CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
     if (W > 0) {
       ProfScope ps(c, 0, W);
-      launch_test_kt(c, kt, flat, n_gpairs, W);
+      launch_test_kt(c, kt, flat, n_gpairs, W, c.stream);
     }
     if (Q > 0) {
       if (round == 0) {
@@ -1644,8 +1889,19 @@ void step_parallel(Ctx& c, int kt) {
     c.last_pp_lost += pp_lost;
     c.last_events += E;
     c.last_ops += Q;
+    if (Q > 0) any_pp = true;
     round++;
     if (set_losers + pp_lost == 0) break;
+    if (round == 1 && c.use_graph && !any_pp && pp_lost == 0 && round < c.max_rounds) {
+      // the redraw rounds, device-driven
+      long long g_redraws = 0, g_events = 0;
+      long long n = run_redraw_graph(c, kt, flat, n_gpairs, max_pairs, set_losers, inflate, &g_redraws, &g_events);
+      redraws += g_redraws;
+      c.last_set_losers += g_redraws;
+      c.last_events += g_events;
+      round += (int)n;
+      break;
+    }
     if (round >= c.max_rounds) {
       std::vector<PopCtr>& r = read_ctrs(c);
       for (int k = 0; k < c.n_pop; k++)
@@ -1735,6 +1991,7 @@ static int do_init(int n_pop, int n_spec, const double* density, int i_water, in
       c.w.expo[dst] = w_exp[src];
     }
   CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c.cap_stream, cudaStreamNonBlocking));
   {
     int dev = 0, n_sm = 0, coop = 0;
     CK(cudaGetDevice(&dev));
@@ -1748,7 +2005,7 @@ static int do_init(int n_pop, int n_spec, const double* density, int i_water, in
   CK(cudaMalloc(&c.d_ctrs, sizeof(PopCtr) * n_pop));
   CK(cudaMalloc(&c.d_round, 2 * sizeof(uint32_t)));  // round of the step, claim generation
   CK(cudaMemset(c.d_round, 0, 2 * sizeof(uint32_t)));
-  c.scan_ctr.reserve(kScanMaxJobs);
+  c.scan_ctr.reserve(2 * kScanMaxJobs);  // tile counters, then finished-block counters
   CK(cudaMemset(c.scan_ctr.p, 0, sizeof(unsigned) * c.scan_ctr.n));
   c.scan_err.reserve(1);
   CK(cudaMemset(c.scan_err.p, 0, sizeof(unsigned long long) * c.scan_err.n));
@@ -1819,6 +2076,9 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.st_i.release();
   c.st_l.release();
   replay_free(c.replay);
+  free_redraw_graph(c);
+  c.graph_stats.release();
+  cudaStreamDestroy(c.cap_stream);
   cudaStreamDestroy(c.stream);
   delete x;
   return PMC_OK;
@@ -2153,6 +2413,12 @@ int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx* x, int pop, int64_t* next_id) {
   *next_id = read_ctr(x->c, pop).next_id;
   return PMC_OK;
   GUARD_END
+}
+
+int pmc_coag_gpu_set_graphs(pmc_coag_gpu_ctx* x, int enable) {
+  if (!x || (enable != 0 && enable != 1)) return PMC_ERR_INVALID_ARG;
+  x->c.use_graph = enable == 1;
+  return PMC_OK;
 }
 
 int pmc_coag_gpu_set_mode(pmc_coag_gpu_ctx* x, int mode) {
