@@ -140,12 +140,12 @@ class AeroState:
 
     def set_mode(self, mode):
         check(_lib.lib().pmc_coag_gpu_set_mode(self.ctx, mode), "pmc_coag_gpu_set_mode")
+        self.mode = mode
 
     def set_graphs(self, enable):
         """Redraw rounds as one device-driven CUDA graph (default) or from a
         host loop; the particles are the same either way."""
         check(_lib.lib().pmc_coag_gpu_set_graphs(self.ctx, 1 if enable else 0), "pmc_coag_gpu_set_graphs")
-        self.mode = mode
 
     def set_weight(self, aero_weight_array):
         self.awa = aero_weight_array
