@@ -238,8 +238,8 @@ int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx *ctx, int kernel_type,
  * device array per GPU, held until the process exits and shared by every
  * call: calls whose work overlaps on the GPU (different streams, or other
  * threads) race on it and must be serialised by the caller.  The first call
- * on each device looks up that array's address and should therefore come
- * before any stream capture. */
+ * on each device looks up that array's address (a runtime call, made once
+ * per device). */
 int pmc_coag_gpu_bin_sort_noalloc(int n_part, const double *vtot_dev,
                                   const int *cls_dev, int n_bin, int n_class,
                                   double edge_min, double edge_max,

@@ -79,6 +79,8 @@ def lib():
                                   ctypes.c_double, ip, ip]
         L.orc_kmax_warnings.restype = ctypes.c_int64
         L.orc_kmax_warnings.argtypes = [P]
+        L.orc_pp_targets.restype = ctypes.c_int64
+        L.orc_pp_targets.argtypes = [P]
         L.orc_sort.argtypes = [P]
         L.orc_n_bin.argtypes = [P]
         L.orc_bin_edges.argtypes = [P, dp]
@@ -240,6 +242,10 @@ class Oracle:
 
     def kmax_warnings(self):
         return lib().orc_kmax_warnings(self.ptr)
+
+    def pp_targets(self):
+        """Targets the per-particle (accelerated) path has handled."""
+        return lib().orc_pp_targets(self.ptr)
 
     def sort(self):
         rc = lib().orc_sort(self.ptr)

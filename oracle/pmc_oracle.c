@@ -82,6 +82,7 @@ struct orc_state {
 
   int64_t next_id;
   int64_t kmax_warn;
+  int64_t pp_targets; /* targets handled by the per-particle path (a counter for tests) */
 
   jmp_buf *fail;
   int fail_code;
@@ -1586,6 +1587,7 @@ static int try_per_particle_coag(orc_state *st, const coag_env *env,
     tpart target, src;
     tpart_from(st, &target, tp);
     int n_samp, n_coag;
+    st->pp_targets++;
     sample_source_particle(st, env, bs, cs, &target, nspt, af, &n_samp,
                            &n_coag, &src);
     if (n_coag > 0) coag_target_with_source(st, bt, ct, e, &src, cc);
@@ -1649,6 +1651,7 @@ int orc_mc_coag(orc_state *st, int kt, double temp, double pressure,
 }
 
 int64_t orc_kmax_warnings(const orc_state *st) { return st->kmax_warn; }
+int64_t orc_pp_targets(const orc_state *st) { return st->pp_targets; }
 
 /* ---------------------------------------------------------------------- */
 /* creation / IO                                                           */

@@ -112,6 +112,8 @@ int orc_mc_coag(orc_state *st, int kernel_type, double temp, double pressure,
                 int *tot_n_coag);
 /* count of k/k_max > 1 warnings (warn_assert_msg 532446093 / 383983415) */
 int64_t orc_kmax_warnings(const orc_state *st);
+/* target particles the per-particle path has handled since creation */
+int64_t orc_pp_targets(const orc_state *st);
 
 /* aero_state_sort: (re)make the bin grid and the inverse maps. */
 int orc_sort(orc_state *st);

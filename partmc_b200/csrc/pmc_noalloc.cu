@@ -5,8 +5,7 @@
 // inside a context (bin + per-chunk histogram, scan, stable scatter) on
 // caller-owned device buffers.  Its only scratch, the per-chunk cell
 // histogram, lives in the file-scope array below instead of coming from
-// cudaMalloc, so the call allocates nothing and can run where allocating is
-// not allowed: inside a CUDA graph capture, or in a host program whose device
+// cudaMalloc, so the call allocates nothing: for a host program whose device
 // memory is all handed out up front by another allocator.
 #include <cuda_runtime.h>
 

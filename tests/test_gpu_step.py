@@ -133,3 +133,43 @@ def test_host_round_trip_each_step(gpu_lib):
     assert hb["n_primary_parts"][:n].sum() == pop.n_part
     with pytest.raises(ValueError):
         st.particles(out={**hb, "id": np.zeros(3, np.int64)})
+
+
+def test_per_particle_path_matches_oracle_ensemble(gpu_lib):
+    """A bimodal population of many 10 nm particles and few 0.5 um particles
+    under power weights: the large-target / small-source bin pairs take the
+    per-particle (accelerated) path of try_per_particle_coag
+    (coagulation.F90:150-241).  The GPU's target operations must run, and the
+    number distribution and total number must agree with the oracle's
+    ensemble within the Monte Carlo error."""
+    modes = [(1e11, 0.01e-6, np.log10(1.5)), (1e8, 0.5e-6, np.log10(1.5))]
+    n_part, n_runs, n_steps = 8000, 8, 4
+    env = pm.EnvState(288.0, 1e5)
+    hist = {"gpu": [], "cpu": []}
+    ops = pp_cpu = 0
+    for k in range(n_runs):
+        pop = aero_dist.brown_bimodal(n_part, seed=500 + k, modes=modes)
+        st = pm.AeroState(pop.aero_data, pop.awa, seed=600 + k)
+        st.add_particles(pop.vol, pop.group)
+        orc = O.Oracle(pop.aero_data.density, (pop.awa.type, pop.awa.magnitude, pop.awa.exponent), seed=700 + k)
+        orc.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
+        orc.set_next_id(pop.n_part + 1)
+        for _ in range(n_steps):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, 600.0)
+            ops += st.conflicts()["target_ops"]
+            orc.mc_coag(O.KERNEL_BROWN, 288.0, 1e5, 0.0, 600.0)
+        pp_cpu += orc.pp_targets()
+        for key, vol in (("gpu", st.particles()["vol"]), ("cpu", orc.particles()[0])):
+            r = E.vol2rad(vol.sum(1))
+            nc = pop.awa.num_conc_at_radius(1, r)
+            h, dc = E.size_histogram(2 * r, nc, n_bin=30, dmin=5e-9, dmax=5e-6)
+            hist[key].append(h)
+    assert pp_cpu > 0 and ops > 0, (pp_cpu, ops)
+    g, c = np.array(hist["gpu"]), np.array(hist["cpu"])
+    se = np.sqrt(g.var(0, ddof=1) / n_runs + c.var(0, ddof=1) / n_runs)
+    ok = se > 0
+    z = (g.mean(0) - c.mean(0))[ok] / se[ok]
+    assert np.abs(z).max() < 4.5, np.abs(z).max()
+    tot_g, tot_c = g.sum(1), c.sum(1)
+    se_t = np.sqrt(tot_g.var(ddof=1) / n_runs + tot_c.var(ddof=1) / n_runs)
+    assert abs(tot_g.mean() - tot_c.mean()) < 3 * se_t + 1e-9 * tot_c.mean()

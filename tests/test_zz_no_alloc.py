@@ -1,8 +1,8 @@
 """pmc_coag_gpu_bin_sort_noalloc against the context's sort.
 
 The no-alloc entry point serves callers that cannot allocate device memory
-while they call us (a CUDA graph being captured, or a host model whose device
-memory is all pre-assigned by its own allocator).  It must give the same
+while they call us (a host model whose device memory is all pre-assigned by
+its own allocator).  It must give the same
 bins and per-cell counts as pmc_coag_gpu_sort, which allocates its scratch,
 and keep doing so on consecutive calls that reuse its static scratch array.
 This file is collected last so a failure here does not hide other results."""
