@@ -306,6 +306,7 @@ constexpr int kMaxCopies = 8;   // dup copies per target operation
 
 struct PPResult {
   int target, p;        // target slot, pair (local)
+  int n_samp, n_coag;   // counted into tot_n_samp / tot_n_coag when the operation is applied
   int merged;           // n_coag > 0
   int n_copies;         // prob_round(old_nc / new_nc); 0 removes the target
   int n_rm;
@@ -334,6 +335,8 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     PPResult& R = res[q];
     R.target = t;
     R.p = p;
+    R.n_samp = 0;
+    R.n_coag = 0;
     R.merged = 0;
     R.n_copies = 1;
     R.n_rm = 0;
@@ -431,7 +434,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
         }
       }
     }
-    add_ll(&P.ctr->tot_samp, (long long)((long long)n_samp));
+    R.n_samp = n_samp;
     if (n_avg == 0) continue;
     double pc_mean = pc_tot / (double)n_samp;
     if (!(pc_mean <= 1.0)) add_ll(&P.ctr->kmax_warn, (long long)(1LL));
@@ -476,7 +479,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
         src = m;
       }
     }
-    add_ll(&P.ctr->tot_coag, (long long)((long long)n_coag));
+    R.n_coag = n_coag;
     if (n_coag == 0) continue;
     // coag_target_with_source (coagulation.F90:522-582): new target
     PMeta tm;
@@ -547,6 +550,10 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
     int pop = op_pop[q];
     const PopDev& P = pops[pop];
     const PPResult& R = res[q];
+    // an operation that lost a claim is redone from scratch, so only applied
+    // operations count their samples and coagulations
+    if (R.n_samp) add_ll(&P.ctr->tot_samp, (long long)R.n_samp);
+    if (R.n_coag) add_ll(&P.ctr->tot_coag, (long long)R.n_coag);
     int dlive = 0;
     for (int z = 0; z < R.n_rm; z++) {
       kill_slot(P, R.rm[z]);
