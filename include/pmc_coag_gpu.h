@@ -6,7 +6,7 @@
  *     mc_coag(coag_kernel_type, env_state, aero_data, aero_state, del_t,
  *             tot_n_samp, tot_n_coag)                (src/coagulation.F90:43-59)
  * from run_part_timestep (src/run_part.F90:917-931).  A Fortran module with
- * bind(c) interfaces (see INTEGRATION.md) maps that call onto
+ * bind(c) interfaces maps that call onto
  * pmc_coag_gpu_step(); the particle state lives on the GPU between calls and
  * is synchronised with aero_state_t only when another process needs it.
  *

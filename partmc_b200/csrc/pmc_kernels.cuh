@@ -281,7 +281,10 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_all(const PopDev* pops, i
     }
     if (chunk >= n_chunks || !chunk_hist_fits(P, n_chunks)) continue;
     int n = P.ctr->n_slots;
-    if (item != kept) sort_load_keys(P, chunk, n, nc, w, lane, keys);
+    if (item != kept) {
+      sort_load_keys(P, chunk, n, nc, w, lane, keys);
+      kept = item;
+    }
     // cell starts
     int carry = 0;
     for (int base = 0; base < nc; base += blockDim.x) {

@@ -46,3 +46,29 @@ def test_batch_counters_sum_over_populations(gpu_lib):
     s, c = pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, batch, 600.0, n_steps=2)
     assert s >= c >= 0
     assert all(batch.n_part(pop=k) > 0 for k in range(3))
+
+
+def test_many_chunks_per_sort_block(gpu_lib):
+    """48 populations of 60 000 particles: more sort chunks (30 each, 1440 in
+    all) than the sort's co-resident blocks, so blocks sort several chunks.
+    Selected populations still match their runs alone bit for bit."""
+    n_pop, n = 48, 60000
+    pops = [aero_dist.brown_bimodal(n, seed=900 + k) for k in range(n_pop)]
+    assert all(p.n_part >= n for p in pops)  # trimmed to exactly n below
+    ad = pops[0].aero_data
+    seeds = np.arange(1, n_pop + 1, dtype=np.uint64)
+    batch = pm.AeroState(ad, pops[0].awa, n_pop=n_pop, seeds=seeds)
+    for k, p in enumerate(pops):
+        batch.set_weight_pop(k, p.awa)
+        batch.add_particles(p.vol[:n], p.group[:n], pop=k)
+    temps, press = np.full(n_pop, 288.0), np.full(n_pop, 1e5)
+    pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, batch, 600.0, n_steps=2)
+    for k in (0, 17, 47):
+        p = pops[k]
+        alone = pm.AeroState(ad, p.awa, seed=int(seeds[k]))
+        alone.add_particles(p.vol[:n], p.group[:n])
+        for _ in range(2):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, pm.EnvState(288.0, 1e5), ad, alone, 600.0)
+        a, b = alone.particles(), batch.particles(pop=k)
+        for key in a:
+            assert np.array_equal(a[key], b[key]), (k, key)
