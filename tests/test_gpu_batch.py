@@ -53,7 +53,7 @@ def test_many_chunks_per_sort_block(gpu_lib):
     all) than the sort's co-resident blocks, so blocks sort several chunks.
     Selected populations still match their runs alone bit for bit."""
     n_pop, n = 48, 60000
-    pops = [aero_dist.brown_bimodal(n, seed=900 + k) for k in range(n_pop)]
+    pops = [aero_dist.brown_bimodal(int(n * 1.05), seed=900 + k) for k in range(n_pop)]
     assert all(p.n_part >= n for p in pops)  # trimmed to exactly n below
     ad = pops[0].aero_data
     seeds = np.arange(1, n_pop + 1, dtype=np.uint64)
