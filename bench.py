@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batch-pops", type=int, default=256)
     ap.add_argument("--batch-same", type=int, default=8)
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="redraw rounds from the host loop instead of the CUDA graph (for launch lists)")
     ap.add_argument("--headline-only", action="store_true",
                     help="measure the headline step only (no FP64, batched or end-to-end lines)")
     return ap.parse_args()
@@ -335,32 +337,43 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     e2e_s = time.perf_counter() - t0
     del ste
 
-    # the same API with the population kept in HBM between calls (a
-    # coagulation-only run): per step the host passes temperature and
-    # pressure and reads back the two counters
+    # the drop-in for a coagulation-only run: the population stays in HBM and
+    # the host's copy of it (slot by slot, in pinned memory) is brought up to
+    # date after every step with the slots that step wrote; per step the host
+    # passes temperature and pressure in and reads the counters and the
+    # changed particles back
     str_ = new_state(mode)
+    mirror = pm.HostMirror(str_, alloc=lambda shape, dt: pinned(shape, torch.from_numpy(np.empty(0, dt)).dtype))
+    mirror.sync()  # the first, full copy: before the timed region
+    rec = 8 * pop.aero_data.n_spec + 4 + 4 + 8 + 4 + 4 + 4  # vol, group, class, id, n_primary, slot, alive
     for _ in range(args.warmup):
         pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, str_, args.del_t)
+        mirror.sync()
     barrier(ws)
     torch.cuda.synchronize()
-    res_samp = 0
+    res_samp, res_d2h = 0, 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
         a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, str_, args.del_t)
+        n_changed, _ = mirror.sync()
         res_samp += a
+        res_d2h += 8 + n_changed * rec
     torch.cuda.synchronize()
     res_s = time.perf_counter() - t0
-    del str_
+    del mirror, str_
 
-    out["e2e"] = aggregate({"unit": "pair-tests/s",
-                            "h2d_bytes_per_step": int(h2d / max(args.e2e_steps, 1)),
-                            "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1)),
-                            "path": "upload (pinned host) + mc_coag + download (pinned host) every step "
-                                    "through the C ABI",
-                            "ms_per_step": 1e3 * e2e_s / max(args.e2e_steps, 1)}, e2e_samp, e2e_s, ws)
-    out["e2e_resident"] = aggregate({"unit": "pair-tests/s", "h2d_bytes_per_step": 16, "d2h_bytes_per_step": 8,
-                                     "path": "mc_coag through the C ABI, population resident in HBM between calls",
-                                     "ms_per_step": 1e3 * res_s / max(args.steps, 1)}, res_samp, res_s, ws)
+    out["e2e"] = aggregate({"unit": "pair-tests/s", "h2d_bytes_per_step": 16,
+                            "d2h_bytes_per_step": int(res_d2h / max(args.steps, 1)),
+                            "path": "mc_coag through the C ABI with the population resident in HBM; after every "
+                                    "step the host copy (pinned, slot-indexed) is brought up to date with the "
+                                    "slots the step wrote (pmc_coag_gpu_sync_host)",
+                            "ms_per_step": 1e3 * res_s / max(args.steps, 1)}, res_samp, res_s, ws)
+    out["e2e_full_sync"] = aggregate({"unit": "pair-tests/s",
+                                      "h2d_bytes_per_step": int(h2d / max(args.e2e_steps, 1)),
+                                      "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1)),
+                                      "path": "upload (pinned host) + mc_coag + download (pinned host) of the "
+                                              "whole population every step through the C ABI",
+                                      "ms_per_step": 1e3 * e2e_s / max(args.e2e_steps, 1)}, e2e_samp, e2e_s, ws)
     return out
 
 
@@ -387,6 +400,7 @@ def main():
 
     def new_state(m):
         st = pm.AeroState(pop.aero_data, pop.awa, seed=1000 + rank, mode=m)
+        st.set_graphs(not args.no_graphs)
         st.add_particles(pop.vol, pop.group)
         return st
 
@@ -423,7 +437,7 @@ def main():
         n1 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
         prof = {}
-        for which, name in ((0, "test"), (1, "sort"), (3, "step")):
+        for which, name in ((0, "test"), (1, "sort"), (2, "redraw_graph"), (3, "step")):
             t, nl, u = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
             L.pmc_coag_gpu_profile_read(st.ctx, which, ctypes.byref(t), ctypes.byref(nl), ctypes.byref(u))
             prof[name] = (t.value, nl.value, u.value)

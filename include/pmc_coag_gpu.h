@@ -128,6 +128,23 @@ int pmc_coag_gpu_download_components(pmc_coag_gpu_ctx *ctx, int pop,
                                      int *comp_source,
                                      double *comp_create_time);
 
+/* Keep a host copy of population `pop` current, slot by slot.  The host
+ * arrays have room for `cap` slots (vol: cap x n_spec, particle-major; the
+ * others: cap entries); alive[] marks the live slots, and the live slots in
+ * increasing order are the particles, in the order pmc_coag_gpu_download
+ * returns them.  Only slots written since the previous call are copied (and
+ * scattered into the arrays by the library).  Every slot is copied when *full
+ * is nonzero on entry (new or regrown host arrays), and on the first call
+ * after an upload or after the library compacted its slots; *full is 1 on
+ * return when that happened.  *n_slots: slots in use (PMC_ERR_CAPACITY,
+ * nothing copied, if above cap); *n_changed: slots copied.  This serves the reference's ownership of aero_state
+ * (aero_state.F90:69-84: the host reads the particle list after mc_coag)
+ * without moving the unchanged particles across the bus every step. */
+int pmc_coag_gpu_sync_host(pmc_coag_gpu_ctx *ctx, int pop, int cap,
+                           double *vol, int *group, int *cls, int64_t *id,
+                           int *n_primary, uint8_t *alive, int *n_slots,
+                           int *n_changed, int *full);
+
 /* New weight magnitudes/exponents, e.g. after aero_state_rebalance doubles or
  * halves a group (aero_state.F90:1722-1852).  Invalidates the sort. */
 int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx *ctx, const int *w_type,

@@ -9,6 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpmc_coag_gpu.so")
 
 PMC_OK = 0
+PMC_ERR_CAPACITY = 3
 STATUS_NAMES = {
     0: "PMC_OK",
     1: "PMC_ERR_INVALID_ARG",
@@ -44,6 +45,8 @@ SIGNATURES = {
     "pmc_coag_gpu_n_part": (_I, [_P, _I, _IP]),
     "pmc_coag_gpu_download": (_I, [_P, _I, _I, _DP, _IP, _IP, _LP, _IP, _IP]),
     "pmc_coag_gpu_download_components": (_I, [_P, _I, _I, _IP, _IP, _DP]),
+    "pmc_coag_gpu_sync_host": (_I, [_P, _I, _I, _DP, _IP, _IP, _LP, _IP, ctypes.POINTER(ctypes.c_uint8), _IP, _IP,
+                                    _IP]),
     "pmc_coag_gpu_set_weight": (_I, [_P, _IP, _DP, _DP]),
     "pmc_coag_gpu_set_weight_pop": (_I, [_P, _I, _IP, _DP, _DP]),
     "pmc_coag_gpu_set_next_id": (_I, [_P, _I, ctypes.c_int64]),

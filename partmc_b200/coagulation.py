@@ -280,6 +280,57 @@ class AeroState:
         return out
 
 
+class HostMirror:
+    """A host copy of one population kept slot by slot and brought up to date
+    by copying only the slots written since the previous sync
+    (pmc_coag_gpu_sync_host).  particles() gives the same arrays, in the same
+    order, as AeroState.particles().  ``alloc`` makes the arrays (default
+    numpy.empty; pass an allocator of page-locked memory to speed the first,
+    full copy)."""
+
+    def __init__(self, aero_state, pop=0, cap=None, alloc=None):
+        self.st, self.pop = aero_state, pop
+        self.alloc = alloc or (lambda shape, dtype: np.empty(shape, dtype=dtype))
+        self.n_slots = 0
+        self._make(cap if cap is not None else max(1024, 2 * aero_state.n_part(pop)))
+
+    def _make(self, cap):
+        ns = self.st.aero_data.n_spec
+        self.cap = int(cap)
+        self.vol = self.alloc((self.cap, ns), np.float64)
+        self.group = self.alloc((self.cap,), np.int32)
+        self.cls = self.alloc((self.cap,), np.int32)
+        self.id = self.alloc((self.cap,), np.int64)
+        self.n_primary = self.alloc((self.cap,), np.int32)
+        self.alive = self.alloc((self.cap,), np.uint8)
+        self.alive[:] = 0
+        self._fresh = True
+
+    def sync(self):
+        """Bring the copy up to date; returns (slots copied, full copy?)."""
+        ns, nc = ctypes.c_int(), ctypes.c_int()
+        u8 = ctypes.POINTER(ctypes.c_uint8)
+        while True:
+            full = ctypes.c_int(1 if self._fresh else 0)
+            rc = _lib.lib().pmc_coag_gpu_sync_host(
+                self.st.ctx, self.pop, self.cap, dp(self.vol), ip(self.group), ip(self.cls), lp(self.id),
+                ip(self.n_primary), self.alive.ctypes.data_as(u8), ctypes.byref(ns), ctypes.byref(nc),
+                ctypes.byref(full))
+            if rc == _lib.PMC_ERR_CAPACITY and ns.value > self.cap:
+                self._make(2 * ns.value)  # regrown arrays: the next call copies every slot
+                continue
+            break
+        check(rc, "pmc_coag_gpu_sync_host")
+        self._fresh = False
+        self.n_slots = ns.value
+        return nc.value, bool(full.value)
+
+    def particles(self):
+        live = np.flatnonzero(self.alive[:self.n_slots])
+        return {"vol": self.vol[live], "weight_group": self.group[live], "weight_class": self.cls[live],
+                "id": self.id[live], "n_primary_parts": self.n_primary[live]}
+
+
 def mc_coag(coag_kernel_type, env_state, aero_data, aero_state, del_t):
     """Do coagulation for time del_t (coagulation.F90:43-96).
 

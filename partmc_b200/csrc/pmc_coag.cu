@@ -13,6 +13,7 @@
 #include <memory>
 #include <string>
 #include <vector>
+#include <thread>
 
 #include "../../include/pmc_coag_gpu.h"
 #include "pmc_kernels.cuh"
@@ -298,8 +299,13 @@ __global__ void k_count_per_pop(const int* need, const long long* n_items, const
 // 0..n-1 (same particle-major layout); fill the caches and the fields the
 // caller did not give
 __global__ void k_upload(PopDev P, int n, int have_grp, int have_cls, int have_id, int have_nprim,
-                         long long id0) {
+                         long long id0, int* bad, unsigned long long* max_id) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // the caller's groups and classes are checked here, on the device
+    if (have_grp && (P.grp[i] < 1 || P.grp[i] > P.n_group)) atomicOr(bad, 1);
+    if (have_cls && (P.cls[i] < 1 || P.cls[i] > P.n_class)) atomicOr(bad, 2);
+    if (have_id && P.id[i] >= 0) atomicMax(max_id, (unsigned long long)P.id[i]);
+    P.changed[i] = 0;
     double vt = 0.0, ms = 0.0;
     for (int s = 0; s < P.n_spec; s++) vt = vt + P.vol[vol_at(P, i, s)];
     for (int s = 0; s < P.n_spec; s++) ms = ms + P.vol[vol_at(P, i, s)] * P.density[s];
@@ -347,6 +353,27 @@ __global__ void k_download(PopDev P, const long long* live_off, int n_slots, dou
   }
 }
 
+// the slots written since the last host sync, compacted in slot order
+// (off: exclusive scan of changed over the slots); their flags are cleared
+__global__ void k_gather_changed(PopDev P, const long long* off, int n_range, int* slot, int* alive, double* vol,
+                                 int* grp, int* cls, long long* id, int* nprim) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_range; i += gridDim.x * blockDim.x) {
+    if (!P.changed[i]) continue;
+    long long j = off[i];
+    slot[j] = i;
+    int a = P.alive[i];
+    alive[j] = a;
+    if (a) {
+      for (int s = 0; s < P.n_spec; s++) vol[j * P.n_spec + s] = P.vol[vol_at(P, i, s)];
+      grp[j] = P.grp[i];
+      cls[j] = P.cls[i];
+      id[j] = P.id[i];
+      nprim[j] = P.nprim[i];
+    }
+    P.changed[i] = 0;
+  }
+}
+
 // move live slots of src into dst compactly (relayout)
 __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_slots,
                            int compact) {
@@ -374,6 +401,7 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.hyst[j] = S.hyst[i];
     D.frozen[j] = S.frozen[i];
     D.alive[j] = S.alive[i];
+    D.changed[j] = S.changed[i];
     D.cell[j] = S.cell[i];
     D.claim[j] = S.claim[i];
     D.recd[j] = S.recd[i];
@@ -499,6 +527,29 @@ struct DevBuf {
   }
 };
 
+// page-locked host staging (cudaHostAlloc), grown on demand
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t b) {
+    if (b <= bytes) return;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(b + b / 4, 1 << 20);
+    if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) {
+      p = nullptr;
+      throw Fail(PMC_ERR_CAPACITY);
+    }
+    bytes = want;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
 struct PopHost {
   PopDev h{};
   bool valid_sort = false;
@@ -513,6 +564,10 @@ struct PopHost {
   uint32_t step = 0;
   int kmax_kt = 0;  // kernel type of the current k_max table
   bool own_w = false;  // weights set for this population alone
+  // host copy kept slot by slot (pmc_coag_gpu_sync_host): refreshed in full
+  // after an upload or a compaction, else by the slots written since
+  bool mirror_full = true;
+  int mirror_slots = 0;
   Weights w{};
   int chunk_hist_cap = 0;
   // per-slot radius/bin/record caches are valid for this grid, kernel,
@@ -579,12 +634,14 @@ struct Ctx {
   DevBuf<double> st_d;
   DevBuf<int> st_i;
   DevBuf<long long> st_l;
+  PinnedBuf pin;  // host staging of the changed slots
   long long h_total = 0;
   // stats of the last step
   long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
   long long last_set_losers = 0, last_pp_lost = 0, last_events = 0, last_ops = 0;
   // optional per-kernel timing with CUDA events on the library's stream:
-  // 0 pair tests, 1 sorts (k_sort_all), 2 unused, 3 whole steps
+  // 0 pair tests, 1 sorts (k_sort_all), 2 redraw-round graph launches,
+  // 3 whole steps
   bool prof = false;
   struct ProfPair {
     int id;
@@ -796,12 +853,14 @@ void alloc_slots(Ctx& c, PopHost& ph, int cap) {
   h.hyst = dalloc<int>(o, cap);
   h.frozen = dalloc<int>(o, cap);
   h.alive = dalloc<uint8_t>(o, cap);
+  h.changed = dalloc<uint8_t>(o, cap);
   h.cell = dalloc<int>(o, cap);
   h.list = dalloc<int>(o, cap);
   h.recd = dalloc<RecD>(o, cap);
   h.recf = dalloc<RecF>(o, cap);
   h.claim = dalloc<unsigned long long>(o, cap);
   CK(cudaMemsetAsync(h.alive, 0, cap, c.stream));
+  CK(cudaMemsetAsync(h.changed, 0, cap, c.stream));
   CK(cudaMemsetAsync(h.claim, 0xff, sizeof(unsigned long long) * cap, c.stream));  // no claim
   c.dirty = true;
 }
@@ -942,7 +1001,10 @@ void relayout(Ctx& c, int k, int new_cap, bool compact) {
   CK(cudaStreamSynchronize(c.stream));
   off.release();
   free_list(old_allocs);
-  if (compact) r.n_slots = (int)n_live;
+  if (compact) {
+    r.n_slots = (int)n_live;
+    ph.mirror_full = true;  // slots renumbered
+  }
   write_ctr(c, k, r);
   push_pops(c);
   CK(cudaStreamSynchronize(c.stream));
@@ -1601,7 +1663,10 @@ long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pair
     c.rg_builds++;
   }
   CK(cudaMemsetAsync(c.graph_stats.p, 0, sizeof(long long) * 4, c.stream));
-  CK(cudaGraphLaunch(c.rg_exec, c.stream));
+  {
+    ProfScope ps(c, 2, 1);
+    CK(cudaGraphLaunch(c.rg_exec, c.stream));
+  }
   long long st[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(st, c.graph_stats.p, sizeof(st), cudaMemcpyDeviceToHost, c.stream));
   unsigned long long scan_err = 0;
@@ -2075,6 +2140,7 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.st_d.release();
   c.st_i.release();
   c.st_l.release();
+  c.pin.release();
   replay_free(c.replay);
   free_redraw_graph(c);
   c.graph_stats.release();
@@ -2090,12 +2156,6 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
   Ctx& c = x->c;
   GUARD_BEGIN
   PopHost& ph = c.pops[pop];
-  if (group)
-    for (int i = 0; i < n_part; i++)
-      if (group[i] < 1 || group[i] > c.n_group) return PMC_ERR_INVALID_ARG;
-  if (cls)
-    for (int i = 0; i < n_part; i++)
-      if (cls[i] < 1 || cls[i] > c.n_class) return PMC_ERR_INVALID_ARG;
   int cap = std::max(1024, n_part + n_part / 2 + 64);
   if (cap > ph.h.cap || cap < ph.h.cap / 4) {
     free_list(ph.slot_allocs);
@@ -2103,6 +2163,8 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
   }
   PopCtr r = read_ctr(c, pop);
   CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
+  CK(cudaMemsetAsync(ph.h.changed, 0, ph.h.cap, c.stream));
+  ph.mirror_full = true;  // a host copy kept slot by slot must be refreshed in full
   if (n_part > 0) {
     size_t n = (size_t)n_part;
     CK(cudaMemcpyAsync(ph.h.vol, vol, sizeof(double) * n * c.n_spec, cudaMemcpyHostToDevice, c.stream));
@@ -2111,16 +2173,28 @@ int pmc_coag_gpu_upload(pmc_coag_gpu_ctx* x, int pop, int n_part, const double* 
     if (id) CK(cudaMemcpyAsync(ph.h.id, id, sizeof(long long) * n, cudaMemcpyHostToDevice, c.stream));
     if (n_primary) CK(cudaMemcpyAsync(ph.h.nprim, n_primary, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
     long long id0 = r.next_id;
+    c.st_l.reserve(2);
+    CK(cudaMemsetAsync(c.st_l.p, 0, 2 * sizeof(long long), c.stream));
+    int* bad = (int*)c.st_l.p;
+    unsigned long long* max_id = (unsigned long long*)(c.st_l.p + 1);
     k_upload<<<grid_for(n_part, 256), 256, 0, c.stream>>>(ph.h, n_part, group != nullptr, cls != nullptr,
-                                                          id != nullptr, n_primary != nullptr, id0);
+                                                          id != nullptr, n_primary != nullptr, id0, bad, max_id);
     note_launch();
-    if (id) {
-      long long mx = 0;
-      for (int i = 0; i < n_part; i++) mx = std::max<long long>(mx, id[i]);
-      r.next_id = std::max<long long>(r.next_id, mx + 1);
-    } else {
-      r.next_id = id0 + n_part;
+    long long chk[2] = {0, 0};
+    CK(cudaMemcpyAsync(chk, c.st_l.p, sizeof(chk), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if ((int)chk[0] != 0) {
+      // invalid groups or classes: the population is left empty
+      CK(cudaMemsetAsync(ph.h.alive, 0, ph.h.cap, c.stream));
+      r.n_slots = r.n_live = 0;
+      write_ctr(c, pop, r);
+      ph.valid_sort = false;
+      ph.caches_valid = false;
+      c.replay.valid = false;
+      return PMC_ERR_INVALID_ARG;
     }
+    if (id) r.next_id = std::max<long long>(r.next_id, chk[1] + 1);
+    else r.next_id = id0 + n_part;
   }
   r.n_slots = n_part;
   r.n_live = n_part;
@@ -2325,6 +2399,103 @@ static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, i
   }
   CK(cudaStreamSynchronize(c.stream));
   return PMC_OK;
+}
+
+int pmc_coag_gpu_sync_host(pmc_coag_gpu_ctx* x, int pop, int cap, double* vol, int* group, int* cls,
+                           int64_t* id, int* n_primary, uint8_t* alive, int* n_slots, int* n_changed, int* full) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || cap < 0 || !vol || !group || !cls || !id || !n_primary || !alive)
+    return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  PopCtr r = read_ctr(c, pop);
+  if (n_slots) *n_slots = r.n_slots;
+  if (r.n_slots > cap) return PMC_ERR_CAPACITY;
+  int ns = c.n_spec;
+  if (full && *full) ph.mirror_full = true;  // the caller asks for every slot (new arrays)
+  if (ph.mirror_full) {
+    // every slot: the slot arrays already have the host layout
+    size_t n = (size_t)r.n_slots;
+    if (n > 0) {
+      CK(cudaMemcpyAsync(vol, ph.h.vol, sizeof(double) * n * ns, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(group, ph.h.grp, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(cls, ph.h.cls, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(id, ph.h.id, sizeof(long long) * n, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(n_primary, ph.h.nprim, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(alive, ph.h.alive, n, cudaMemcpyDeviceToHost, c.stream));
+    }
+    CK(cudaMemsetAsync(ph.h.changed, 0, ph.h.cap, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if ((size_t)cap > n) memset(alive + n, 0, (size_t)cap - n);
+    ph.mirror_full = false;
+    ph.mirror_slots = r.n_slots;
+    if (n_changed) *n_changed = r.n_slots;
+    if (full) *full = 1;
+    return PMC_OK;
+  }
+  int range = std::max(ph.mirror_slots, r.n_slots);
+  if (range > ph.h.cap) range = ph.h.cap;
+  size_t t = (size_t)std::max(range, 1);  // room for every slot of the range
+  c.st_l.reserve(2 * t + 2);
+  c.st_d.reserve(t * ns);
+  c.st_i.reserve(5 * t);
+  long long total = range > 0 ? scan(c, ph.h.changed, range, c.st_l.p, true) : 0;
+  if (range > 0) {
+    int* d_slot = c.st_i.p;
+    int* d_alive = d_slot + t;
+    int* d_grp = d_alive + t;
+    int* d_cls = d_grp + t;
+    int* d_np = d_cls + t;
+    long long* d_id = c.st_l.p + range + 1;
+    k_gather_changed<<<grid_for(range, 256), 256, 0, c.stream>>>(ph.h, c.st_l.p, range, d_slot, d_alive, c.st_d.p,
+                                                                d_grp, d_cls, d_id, d_np);
+    note_launch();
+    size_t tt = (size_t)std::max<long long>(total, 1);
+    size_t rec = sizeof(double) * ns + 5 * sizeof(int) + sizeof(long long);
+    c.pin.reserve(rec * tt);
+    double* h_vol = (double*)c.pin.p;
+    long long* h_id = (long long*)(h_vol + tt * ns);
+    int* h_i = (int*)(h_id + tt);
+    if (total > 0) {
+      CK(cudaMemcpyAsync(h_vol, c.st_d.p, sizeof(double) * total * ns, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(h_id, d_id, sizeof(long long) * total, cudaMemcpyDeviceToHost, c.stream));
+      for (int f = 0; f < 5; f++)
+        CK(cudaMemcpyAsync(h_i + (size_t)f * tt, c.st_i.p + (size_t)f * t, sizeof(int) * total,
+                           cudaMemcpyDeviceToHost, c.stream));
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    // scatter into the caller's slot-indexed arrays
+    const int* h_slot = h_i;
+    const int* h_alive = h_i + tt;
+    const int* h_grp = h_i + 2 * tt;
+    const int* h_cls = h_i + 3 * tt;
+    const int* h_np = h_i + 4 * tt;
+    auto work = [&](long long j0, long long j1) {
+      for (long long j = j0; j < j1; j++) {
+        int sl = h_slot[j];
+        alive[sl] = (uint8_t)h_alive[j];
+        if (!h_alive[j]) continue;
+        memcpy(vol + (size_t)sl * ns, h_vol + (size_t)j * ns, sizeof(double) * ns);
+        group[sl] = h_grp[j];
+        cls[sl] = h_cls[j];
+        id[sl] = h_id[j];
+        n_primary[sl] = h_np[j];
+      }
+    };
+    int n_thr = total > 32768 ? (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (n_thr <= 1) {
+      work(0, total);
+    } else {
+      std::vector<std::thread> th;
+      for (int q = 0; q < n_thr; q++) th.emplace_back(work, total * q / n_thr, total * (q + 1) / n_thr);
+      for (auto& w : th) w.join();
+    }
+  }
+  ph.mirror_slots = r.n_slots;
+  if (n_changed) *n_changed = (int)total;
+  if (full) *full = 0;
+  return PMC_OK;
+  GUARD_END
 }
 
 int pmc_coag_gpu_download(pmc_coag_gpu_ctx* x, int pop, int max_part, double* vol, int* group, int* cls,

@@ -16,6 +16,7 @@ namespace pmc {
 
 __device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
   P.alive[i] = 0;
+  P.changed[i] = 1;
   P.cell[i] = -1;
 }
 
@@ -286,6 +287,7 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int*
     P.hyst[dest] = c.hyst;
     P.frozen[dest] = c.frozen;
     P.alive[dest] = 1;
+    P.changed[dest] = 1;
     // the coagulated particle must lie on the grid (aero_state_add_particle
     // with allow_resort=.false., aero_sorted.F90:427-440)
     int nbin = refresh_slot(P, dest);

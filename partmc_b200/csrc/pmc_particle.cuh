@@ -65,6 +65,7 @@ __device__ __forceinline__ void store_particle(const PopDev& P, int i, const dou
   P.hyst[i] = m.hyst;
   P.frozen[i] = m.frozen;
   P.alive[i] = 1;
+  P.changed[i] = 1;
 }
 
 __device__ __forceinline__ void zero_meta(PMeta& m) {

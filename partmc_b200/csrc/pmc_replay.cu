@@ -63,6 +63,7 @@ struct Seq {
     if (i < 1 || i > n) return fail(kErrAssert);
     if (i < n) copy_slot(i, n);
     P->alive[n - 1] = 0;
+    P->changed[n - 1] = 1;
     n--;
     return true;
   }

@@ -157,6 +157,7 @@ struct PopDev {
   int* hyst;
   int* frozen;
   uint8_t* alive;
+  uint8_t* changed;  // slot written since the host copy was last brought up to date
   // sort key of each slot: the (bin, class) cell bin + n_bin * class
   // (0-based) of a live particle on the grid, -1 for a dead slot or a
   // particle off the grid

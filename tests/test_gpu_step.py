@@ -180,3 +180,45 @@ def test_per_particle_path_matches_oracle_ensemble(gpu_lib):
     tot_g, tot_c = g.sum(1), c.sum(1)
     se_t = np.sqrt(tot_g.var(ddof=1) / n_runs + tot_c.var(ddof=1) / n_runs)
     assert abs(tot_g.mean() - tot_c.mean()) < 3 * se_t + 1e-9 * tot_c.mean()
+
+
+def check_mirror_steps(st, pop, kt, env, del_t, n_steps):
+    mirror = pm.HostMirror(st, cap=256)  # too small: the first sync regrows it
+    n, full = mirror.sync()
+    assert full and n == pop.n_part
+    fulls = 0
+    for _ in range(n_steps):
+        pm.mc_coag(kt, env, pop.aero_data, st, del_t)
+        n, full = mirror.sync()
+        fulls += full
+        a, b = mirror.particles(), st.particles()
+        for key in b:
+            assert np.array_equal(a[key], b[key]), key
+    return fulls
+
+
+@pytest.mark.parametrize("mode", [pm.MODE_MIXED, pm.MODE_REPLAY])
+def test_host_mirror_tracks_every_step(gpu_lib, mode):
+    """A host copy kept slot by slot and updated with only the changed slots
+    equals a full download after every step: per-set events and the
+    per-particle path's removals and copies, and in replay mode the
+    reference's swap-last removals that shrink the slot count."""
+    modes = [(1e11, 0.01e-6, np.log10(1.5)), (1e8, 0.5e-6, np.log10(1.5))]
+    pop = aero_dist.brown_bimodal(6000, seed=31, modes=modes)
+    st = pm.AeroState(pop.aero_data, pop.awa, seed=4, mode=mode)
+    st.add_particles(pop.vol, pop.group)
+    if mode == pm.MODE_REPLAY:
+        st.set_replay(np.random.default_rng(5).random(20_000_000))
+    check_mirror_steps(st, pop, pm.COAG_KERNEL_TYPE_BROWN, pm.EnvState(288.0, 1e5), 600.0, 8)
+
+
+def test_host_mirror_after_compaction(gpu_lib):
+    """Flat-weight additive coagulation removing most particles: the library
+    compacts its slots, which renumbers them, and the next sync copies every
+    slot; the copy still equals a full download after every step."""
+    pop = aero_dist.additive_exp(20000, seed=6)
+    st = pm.AeroState(pop.aero_data, pop.awa, seed=2, mode=pm.MODE_MIXED)
+    st.add_particles(pop.vol, pop.group)
+    fulls = check_mirror_steps(st, pop, pm.COAG_KERNEL_TYPE_ADDITIVE, pm.EnvState(288.0, 1e5, 1000.0), 600.0, 6)
+    assert st.n_part() < pop.n_part // 2
+    assert fulls >= 1  # a compaction happened and forced one full copy
