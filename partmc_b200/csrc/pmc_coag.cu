@@ -512,8 +512,10 @@ struct DevBuf {
     if (m <= n) return;
     if (p) cudaFree(p);
     p = nullptr;
+    // geometric growth: sizes that creep up step by step (slot counts,
+    // sample counts) reallocate rarely
+    size_t want = std::max<size_t>(std::max<size_t>(m, n + n / 2), 1024);
     n = 0;
-    size_t want = std::max<size_t>(m, 1024);
     if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) {
       p = nullptr;
       throw Fail(PMC_ERR_CAPACITY);
