@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batch-pops", type=int, default=256)
     ap.add_argument("--batch-same", type=int, default=8)
+    ap.add_argument("--serve-jobs", type=int, default=200)
     ap.add_argument("--no-graphs", action="store_true",
                     help="redraw rounds from the host loop instead of the CUDA graph (for launch lists)")
     ap.add_argument("--headline-only", action="store_true",
@@ -361,6 +362,18 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     torch.cuda.synchronize()
     res_s = time.perf_counter() - t0
     del mirror, str_
+
+    # serving (cfg 5): Poisson arrivals at 50 jobs/s, 1e3..1e6 particles,
+    # additive / Brownian / sedimentation, 10..200 steps of del_t, continuous
+    # batching within a 150 GB HBM budget
+    from partmc_b200 import serve
+    jobs = serve.poisson_jobs(args.serve_jobs, rate=50.0, seed=5 + 1000 * (ws > 1))
+    srv = serve.Server([pm.COAG_KERNEL_TYPE_ADDITIVE, pm.COAG_KERNEL_TYPE_BROWN, pm.COAG_KERNEL_TYPE_SEDI],
+                       slots=48, hbm_budget=150e9, del_t=args.del_t, mode=mode)
+    sm = serve.run(jobs, srv)
+    del srv
+    out["serving"] = aggregate(dict(sm, unit="pair-tests/s", rate_jobs_per_s=50.0), sm["pair_tests_per_s"] * sm["wall_s"],
+                               sm["wall_s"], ws)
 
     out["e2e"] = aggregate({"unit": "pair-tests/s", "h2d_bytes_per_step": 16,
                             "d2h_bytes_per_step": int(res_d2h / max(args.steps, 1)),

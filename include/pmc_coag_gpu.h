@@ -171,6 +171,13 @@ int pmc_coag_gpu_set_mode(pmc_coag_gpu_ctx *ctx, int mode);
  * loop.  No counterpart in the reference (an execution choice). */
 int pmc_coag_gpu_set_graphs(pmc_coag_gpu_ctx *ctx, int enable);
 
+/* New seed for population `pop`, with its step counter back at zero
+ * (pmc_srand, rand.F90:66-113, for one population): its random streams then
+ * depend only on the seed and the steps taken since, not on when the
+ * population entered a batched context.  A server that reuses a population
+ * slot for a new job calls this when it uploads the job. */
+int pmc_coag_gpu_set_seed(pmc_coag_gpu_ctx *ctx, int pop, uint64_t seed);
+
 /* Replay stream: uniforms in [0, 1) consumed in the reference's order
  * (pmc_random, rand.F90:138-167).  Copied to the device. */
 int pmc_coag_gpu_replay_set(pmc_coag_gpu_ctx *ctx, const double *u, int64_t n);

@@ -53,6 +53,7 @@ SIGNATURES = {
     "pmc_coag_gpu_get_next_id": (_I, [_P, _I, _LP]),
     "pmc_coag_gpu_set_mode": (_I, [_P, _I]),
     "pmc_coag_gpu_set_graphs": (_I, [_P, _I]),
+    "pmc_coag_gpu_set_seed": (_I, [_P, _I, ctypes.c_uint64]),
     "pmc_coag_gpu_replay_set": (_I, [_P, _DP, ctypes.c_int64]),
     "pmc_coag_gpu_replay_open": (_I, [_P, ctypes.c_char_p]),
     "pmc_coag_gpu_replay_used": (_I, [_P, _LP]),

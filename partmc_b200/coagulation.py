@@ -142,6 +142,10 @@ class AeroState:
         check(_lib.lib().pmc_coag_gpu_set_mode(self.ctx, mode), "pmc_coag_gpu_set_mode")
         self.mode = mode
 
+    def set_seed(self, seed, pop=0):
+        """New seed for population ``pop``; its step counter restarts."""
+        check(_lib.lib().pmc_coag_gpu_set_seed(self.ctx, pop, int(seed)), "pmc_coag_gpu_set_seed")
+
     def set_graphs(self, enable):
         """Redraw rounds as one device-driven CUDA graph (default) or from a
         host loop; the particles are the same either way."""

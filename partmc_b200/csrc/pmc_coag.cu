@@ -2588,6 +2588,16 @@ int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx* x, int pop, int64_t* next_id) {
   GUARD_END
 }
 
+int pmc_coag_gpu_set_seed(pmc_coag_gpu_ctx* x, int pop, uint64_t seed) {
+  if (!x || pop < 0 || pop >= x->c.n_pop) return PMC_ERR_INVALID_ARG;
+  PopHost& ph = x->c.pops[pop];
+  ph.seed = seed;
+  ph.h.seed = seed;
+  ph.step = 0;  // the population's streams start again at step 1
+  x->c.dirty = true;
+  return PMC_OK;
+}
+
 int pmc_coag_gpu_set_graphs(pmc_coag_gpu_ctx* x, int enable) {
   if (!x || (enable != 0 && enable != 1)) return PMC_ERR_INVALID_ARG;
   x->c.use_graph = enable == 1;
