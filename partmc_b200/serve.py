@@ -7,7 +7,7 @@ server keeps one batched context per kernel type with a fixed number of
 population slots and, every tick:
 
   1. admits arrived jobs into free slots while the HBM budget allows
-     (upload, weights and a fresh seed for the slot);
+     (upload, weights, and a fresh seed and ID counter for the slot);
   2. advances every context that holds jobs by one step (one batched launch
      sequence per context);
   3. retires jobs whose steps are done (their slot is emptied).
@@ -112,6 +112,7 @@ class Server:
             return False
         st = self.ctx[job.kernel]
         st.set_weight_pop(k, job.pop.awa)
+        st.set_next_id(1, pop=k)  # IDs as in a fresh run of the job (aero_particle.F90:72)
         st.add_particles(job.pop.vol, job.pop.group, pop=k)
         st.set_seed(job.seed, pop=k)
         slots[k] = job
