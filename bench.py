@@ -370,6 +370,7 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     jobs = serve.poisson_jobs(args.serve_jobs, rate=50.0, seed=5 + 1000 * (ws > 1))
     srv = serve.Server([pm.COAG_KERNEL_TYPE_ADDITIVE, pm.COAG_KERNEL_TYPE_BROWN, pm.COAG_KERNEL_TYPE_SEDI],
                        slots=48, hbm_budget=150e9, del_t=args.del_t, mode=mode)
+    serve.warm_up(srv)
     sm = serve.run(jobs, srv)
     del srv
     out["serving"] = aggregate(dict(sm, unit="pair-tests/s", rate_jobs_per_s=50.0), sm["pair_tests_per_s"] * sm["wall_s"],

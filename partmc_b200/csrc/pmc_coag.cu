@@ -576,6 +576,7 @@ struct PopHost {
   // environment and weights
   bool caches_valid = false;
   int key_kt = 0, key_wver = -1;
+  int wver = 0;  // bumped when this population's weights change
   double key_temp = 0, key_press = 0, key_coeff = 0;
 };
 
@@ -601,6 +602,7 @@ struct Ctx {
   cudaGraph_t rg_graph = nullptr;
   cudaGraphExec_t rg_exec = nullptr;
   std::vector<long long> rg_key;
+  std::vector<long long> rg_seen;  // the key of the previous step's redraw rounds
   long long rg_nodes = 0, rg_builds = 0;
   DevBuf<long long> graph_stats;
   size_t sort_smem = 0;  // dynamic shared memory the sort grid was sized for
@@ -1129,7 +1131,7 @@ void run_sort(Ctx& c) {
 
 bool caches_current(const Ctx& c, const PopHost& ph) {
   return ph.caches_valid && ph.key_kt == ph.h.kernel_type && ph.key_temp == ph.h.temp &&
-         ph.key_press == ph.h.pressure && ph.key_coeff == ph.h.coeff && ph.key_wver == c.wver;
+         ph.key_press == ph.h.pressure && ph.key_coeff == ph.h.coeff && ph.key_wver == ph.wver;
 }
 
 // recompute radius, bin and records of every live slot of the marked
@@ -1161,7 +1163,7 @@ void refresh_caches(Ctx& c, const std::vector<uint8_t>& on) {
       ph.key_temp = ph.h.temp;
       ph.key_press = ph.h.pressure;
       ph.key_coeff = ph.h.coeff;
-      ph.key_wver = c.wver;
+      ph.key_wver = ph.wver;
     }
 }
 
@@ -1592,8 +1594,9 @@ void free_redraw_graph(Ctx& c) {
 }
 
 // Run the redraw rounds of this step as the graph (captured again when a
-// bound or an address changed).  losers0: round 0's per-set losers.
-// Returns the rounds run.
+// bound or an address changed and the change held for two steps in a row).
+// losers0: round 0's per-set losers.  Returns the rounds run, or -1 if the
+// caller should run them from the host loop.
 long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pairs, long long losers0,
                            float inflate, long long* redraws, long long* events) {
   RedrawBounds b;
@@ -1629,6 +1632,12 @@ long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pair
   size_sort(c, b.max_cells);
   if (c.dirty) push_pops(c);
   std::vector<long long> key = redraw_key(c, b);
+  if (key != c.rg_key && key != c.rg_seen) {
+    // bounds or addresses new since the last step: capturing pays only when
+    // they hold, so this step's redraw rounds run from the host loop
+    c.rg_seen = key;
+    return -1;
+  }
   if (key != c.rg_key) {
     free_redraw_graph(c);
     CK(cudaGraphCreate(&c.rg_graph, 0));
@@ -1963,11 +1972,13 @@ void step_parallel(Ctx& c, int kt) {
       // the redraw rounds, device-driven
       long long g_redraws = 0, g_events = 0;
       long long n = run_redraw_graph(c, kt, flat, n_gpairs, max_pairs, set_losers, inflate, &g_redraws, &g_events);
-      redraws += g_redraws;
-      c.last_set_losers += g_redraws;
-      c.last_events += g_events;
-      round += (int)n;
-      break;
+      if (n >= 0) {
+        redraws += g_redraws;
+        c.last_set_losers += g_redraws;
+        c.last_events += g_events;
+        round += (int)n;
+        break;
+      }
     }
     if (round >= c.max_rounds) {
       std::vector<PopCtr>& r = read_ctrs(c);
@@ -2532,6 +2543,7 @@ int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx* x, const int* w_type, const double
     }
   c.wver++;
   for (auto& ph : c.pops) {
+    if (!ph.own_w) ph.wver++;  // populations with weights of their own keep them
     set_params(c, ph);
     ph.valid_sort = false;  // aero_state_set_weight clears valid_sort
   }
@@ -2559,7 +2571,7 @@ int pmc_coag_gpu_set_weight_pop(pmc_coag_gpu_ctx* x, int pop, const int* w_type,
     }
   ph.w = w;
   ph.own_w = true;
-  c.wver++;
+  ph.wver++;  // only this population's caches go stale
   set_params(c, ph);
   ph.valid_sort = false;
   c.replay.valid = false;

@@ -147,6 +147,16 @@ class Server:
         return [j for _, _, j in done], lat
 
 
+def warm_up(server, seed=99):
+    """Run a few small jobs of every kernel type through the server, so that
+    first launches (module loading, buffer growth, graph capture) fall
+    outside a timed run."""
+    kernels = tuple(server.ctx)
+    jobs = poisson_jobs(4 * len(kernels), rate=1e4, seed=seed, n_min=2e3, n_max=2e5, steps=(4, 8), kernels=kernels)
+    run(jobs, server)
+    server.n_samp_total = 0
+
+
 def run(jobs, server):
     """Serve a job stream in wall-clock time (arrival times are seconds after
     the start).  Returns the metrics."""
