@@ -157,6 +157,23 @@ int pmc_coag_gpu_set_weight_pop(pmc_coag_gpu_ctx *ctx, int pop,
                                 const int *w_type, const double *w_mag,
                                 const double *w_exp);
 
+/* aero_state_rebalance (aero_state.F90:1797-1852) for population `pop`,
+ * called by run_part after every step (run_part.F90:982).  While a weight
+ * (group, class) holds fewer than n_part_ideal/2 particles, and at least
+ * one, it is doubled (aero_state_double, :1722-1746: every member copied
+ * with a new ID, the weight magnitude halved); while it holds more than
+ * 2*n_part_ideal it is halved (aero_state_halve, :1749-1783: each member
+ * removed with probability 1/2, the magnitude doubled).  n_part_ideal is
+ * n_group x n_class (aero_state%n_part_ideal).  The population then has
+ * weights of its own (read them back with pmc_coag_gpu_get_weight). */
+int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx *ctx, int pop,
+                           const double *n_part_ideal, int allow_doubling,
+                           int allow_halving);
+
+/* The weight magnitudes population `pop` uses now (n_group x n_class),
+ * aero_weight_array_t%weight(:,:)%magnitude (aero_weight_array.F90:35-39). */
+int pmc_coag_gpu_get_weight(pmc_coag_gpu_ctx *ctx, int pop, double *w_mag);
+
 /* The ID counter (next_id, aero_particle.F90:72, new_id :157-165). */
 int pmc_coag_gpu_set_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t next_id);
 int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t *next_id);

@@ -142,6 +142,25 @@ class AeroState:
         check(_lib.lib().pmc_coag_gpu_set_mode(self.ctx, mode), "pmc_coag_gpu_set_mode")
         self.mode = mode
 
+    def rebalance(self, n_part_ideal, allow_doubling=True, allow_halving=True, pop=0):
+        """aero_state_rebalance (aero_state.F90:1797-1852) of population
+        ``pop``; n_part_ideal per (group, class), or one number for all.
+        Returns the population's weight magnitudes afterwards."""
+        ideal = np.asfortranarray(np.broadcast_to(n_part_ideal, self.awa.magnitude.shape), dtype=np.float64)
+        flat = np.ascontiguousarray(ideal.ravel(order="F"))
+        check(_lib.lib().pmc_coag_gpu_rebalance(self.ctx, pop, dp(flat), int(bool(allow_doubling)),
+                                                 int(bool(allow_halving))), "pmc_coag_gpu_rebalance")
+        mag = self.weight_magnitudes(pop)
+        if self.n_pop == 1:
+            self.awa = AeroWeightArray(self.awa.type, mag, self.awa.exponent)
+        return mag
+
+    def weight_magnitudes(self, pop=0):
+        """Weight magnitudes (n_group, n_class) population ``pop`` uses now."""
+        m = np.empty(self.awa.magnitude.size, dtype=np.float64)
+        check(_lib.lib().pmc_coag_gpu_get_weight(self.ctx, pop, dp(m)), "pmc_coag_gpu_get_weight")
+        return m.reshape(self.awa.magnitude.shape, order="F")
+
     def set_seed(self, seed, pop=0):
         """New seed for population ``pop``; its step counter restarts."""
         check(_lib.lib().pmc_coag_gpu_set_seed(self.ctx, pop, int(seed)), "pmc_coag_gpu_set_seed")

@@ -374,6 +374,81 @@ __global__ void k_gather_changed(PopDev P, const long long* off, int n_range, in
   }
 }
 
+// ---------------------------------------------------------------------------
+// aero_state_rebalance (aero_state.F90:1722-1852) on the device
+
+// live particles per (group, class): counts[(g-1) + n_group*(c-1)]
+__global__ void k_count_group_class(PopDev P, int* counts) {
+  int n = P.ctr->n_slots;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!P.alive[i]) continue;
+    int g = P.grp[i], c = P.cls[i];
+    if (g >= 1 && g <= P.n_group && c >= 1 && c <= P.n_class) atomicAdd(&counts[(g - 1) + P.n_group * (c - 1)], 1);
+  }
+}
+
+// members of (g, c) among slots 0..n-1
+__global__ void k_flag_group_class(PopDev P, int n, int g, int c, uint8_t* flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    flag[i] = (P.alive[i] && P.grp[i] == g && P.cls[i] == c) ? 1 : 0;
+}
+
+// aero_state_double: member j (in slot order) is copied to slot n + j with
+// ID id0 + j (aero_particle_new_id); every field is copied, caches included
+__global__ void k_double(PopDev P, int n, const uint8_t* flag, const long long* off, long long id0) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    int d = n + (int)off[i];
+    if (d >= P.cap) {
+      set_status(P.ctr, kErrCapacity);
+      continue;
+    }
+    for (int s = 0; s < P.n_spec; s++) P.vol[vol_at(P, d, s)] = P.vol[vol_at(P, i, s)];
+    P.vtot[d] = P.vtot[i];
+    P.mass[d] = P.mass[i];
+    P.rad[d] = P.rad[i];
+    P.grp[d] = P.grp[i];
+    P.cls[d] = P.cls[i];
+    P.id[d] = id0 + off[i];
+    P.nprim[d] = P.nprim[i];
+    P.ncomp[d] = P.ncomp[i];
+    for (int k = 0; k < P.ncomp[i]; k++) {
+      P.csrc[comp_at(d, k)] = P.csrc[comp_at(i, k)];
+      P.ctime[comp_at(d, k)] = P.ctime[comp_at(i, k)];
+    }
+    P.lct[d] = P.lct[i];
+    P.gct[d] = P.gct[i];
+    P.imf[d] = P.imf[i];
+    P.den_ice[d] = P.den_ice[i];
+    P.phi[d] = P.phi[i];
+    P.hyst[d] = P.hyst[i];
+    P.frozen[d] = P.frozen[i];
+    P.cell[d] = P.cell[i];
+    P.recd[d] = P.recd[i];
+    P.recf[d] = P.recf[i];
+    P.claim[d] = ~0ULL;
+    P.alive[d] = 1;
+    P.changed[d] = 1;
+  }
+}
+
+// aero_state_halve: each member removed with probability 1/2; the draw of
+// slot i is keyed by the population's seed and step, the rebalance call and i
+__global__ void k_halve(PopDev P, int g, int c, uint32_t call) {
+  int n = P.ctr->n_slots;
+  int removed = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!(P.alive[i] && P.grp[i] == g && P.cls[i] == c)) continue;
+    U4 r = philox4x32_10(U4{P.step, (call << 4) | kStreamHalve, (uint32_t)i, 0u}, (uint32_t)P.seed,
+                         (uint32_t)(P.seed >> 32));
+    if (u53(r.x, r.y) < 0.5) {
+      kill_slot(P, i);
+      removed++;
+    }
+  }
+  if (removed) add_ll(&P.ctr->n_live, -(long long)removed);
+}
+
 // move live slots of src into dst compactly (relayout)
 __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_slots,
                            int compact) {
@@ -570,6 +645,7 @@ struct PopHost {
   // after an upload or a compaction, else by the slots written since
   bool mirror_full = true;
   int mirror_slots = 0;
+  uint32_t rebalance_calls = 0;  // halving draws: one stream per call
   Weights w{};
   int chunk_hist_cap = 0;
   // per-slot radius/bin/record caches are valid for this grid, kernel,
@@ -2411,6 +2487,110 @@ static int do_download(Ctx& c, int pop, int max_part, double* vol, int* group, i
     if (comp_time) CK(cudaMemcpyAsync(comp_time, dct, sizeof(double) * nl * kMaxComponent, cudaMemcpyDeviceToHost, c.stream));
   }
   CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+}
+
+// particles of population k per (group, class)
+static std::vector<int> count_group_class(Ctx& c, int k) {
+  PopHost& ph = c.pops[k];
+  int ngc = c.n_group * c.n_class;
+  c.st_i.reserve(ngc);
+  CK(cudaMemsetAsync(c.st_i.p, 0, sizeof(int) * ngc, c.stream));
+  PopCtr r = read_ctr(c, k);
+  if (r.n_slots > 0) {
+    k_count_group_class<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(ph.h, c.st_i.p);
+    note_launch();
+  }
+  std::vector<int> n(ngc);
+  CK(cudaMemcpyAsync(n.data(), c.st_i.p, sizeof(int) * ngc, cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return n;
+}
+
+// scale the weight magnitude of (g, c) of population k (aero_weight_scale);
+// the population takes weights of its own
+static void scale_weight(Ctx& c, int k, int g, int cl, double f) {
+  PopHost& ph = c.pops[k];
+  if (!ph.own_w) {
+    ph.w = c.w;
+    ph.own_w = true;
+  }
+  ph.w.mag[(g - 1) + kMaxGroup * (cl - 1)] *= f;
+  ph.wver++;
+  set_params(c, ph);
+}
+
+int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx* x, int pop, const double* n_part_ideal, int allow_doubling,
+                           int allow_halving) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || !n_part_ideal) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  bool changed = false;
+  if (allow_doubling)
+    for (int g = 1; g <= c.n_group; g++)
+      for (int cl = 1; cl <= c.n_class; cl++) {
+        int idx = (g - 1) + c.n_group * (cl - 1);
+        double ideal = n_part_ideal[idx];
+        for (int it = 0; it < 64; it++) {
+          int cnt = count_group_class(c, pop)[idx];
+          if (!((double)cnt < ideal / 2.0 && cnt > 0)) break;
+          PopCtr r = read_ctr(c, pop);
+          long long need = (long long)r.n_slots + cnt;
+          if (need > ph.h.cap)
+            relayout(c, pop, (int)std::min<long long>(need * 3 / 2 + 1024, (1LL << 31) - 1), false);
+          r = read_ctr(c, pop);
+          size_t n = (size_t)r.n_slots;
+          c.st_l.reserve(n + 1);
+          c.flag.reserve(n + 1);
+          if (c.dirty) push_pops(c);
+          k_flag_group_class<<<grid_for(n, 256), 256, 0, c.stream>>>(ph.h, r.n_slots, g, cl, c.flag.p);
+          note_launch();
+          long long members = scan(c, c.flag.p, (long long)n, c.st_l.p, true);
+          k_double<<<grid_for(n, 256), 256, 0, c.stream>>>(ph.h, r.n_slots, c.flag.p, c.st_l.p, r.next_id);
+          note_launch();
+          r.n_slots += (int)members;
+          r.n_live += (int)members;
+          r.next_id += members;
+          write_ctr(c, pop, r);
+          scale_weight(c, pop, g, cl, 0.5);
+          changed = true;
+        }
+      }
+  if (allow_halving)
+    for (int g = 1; g <= c.n_group; g++)
+      for (int cl = 1; cl <= c.n_class; cl++) {
+        int idx = (g - 1) + c.n_group * (cl - 1);
+        double ideal = n_part_ideal[idx];
+        for (int it = 0; it < 64; it++) {
+          int cnt = count_group_class(c, pop)[idx];
+          if (!((double)cnt > ideal * 2.0)) break;
+          push_pops(c);
+          PopCtr r = read_ctr(c, pop);
+          k_halve<<<grid_for(r.n_slots, 256), 256, 0, c.stream>>>(ph.h, g, cl, ph.rebalance_calls++);
+          note_launch();
+          scale_weight(c, pop, g, cl, 2.0);
+          changed = true;
+        }
+      }
+  if (changed) {
+    ph.valid_sort = false;  // aero_state_double clears valid_sort; halving removed particles
+    c.replay.valid = false;
+    push_pops(c);
+    CK(cudaStreamSynchronize(c.stream));
+    PopCtr r = read_ctr(c, pop);
+    if (r.status) return r.status;
+  }
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_get_weight(pmc_coag_gpu_ctx* x, int pop, double* w_mag) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || !w_mag) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  const Weights& w = c.pops[pop].own_w ? c.pops[pop].w : c.w;
+  for (int cl = 0; cl < c.n_class; cl++)
+    for (int g = 0; g < c.n_group; g++) w_mag[g + c.n_group * cl] = w.mag[g + kMaxGroup * cl];
   return PMC_OK;
 }
 

@@ -41,6 +41,7 @@ enum Stream : uint32_t {
   kStreamTest = 2,
   kStreamMerge = 3,
   kStreamPart = 4,
+  kStreamHalve = 5,  // aero_state_halve draws, keyed by the rebalance call and the slot
 };
 
 __device__ __forceinline__ void set_status(PopCtr* c, int code) { atomicCAS(&c->status, 0, code); }
