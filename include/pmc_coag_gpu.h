@@ -170,6 +170,20 @@ int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx *ctx, int pop,
                            const double *n_part_ideal, int allow_doubling,
                            int allow_halving);
 
+/* Size distributions of population `pop` without a download: the
+ * reference's aero_state diameter histograms (extract_aero_size.F90:132-138,
+ * bin_grid_histogram_1d, bin_grid.F90:225-248) on a log grid of n_bin
+ * diameter bins from d_min to d_max (m).  Each particle counts with its
+ * number concentration, divided by the bin's log width: num_dist[b] in
+ * m^-3 per unit ln(D); mass_dist (may be NULL) [b * n_spec + s] in kg m^-3
+ * per unit ln(D), per species (their sum is the mass distribution).
+ * Particles outside the grid are not counted.  n_bin * (1 + n_spec) <= 12288.
+ * The per-bin sums are accumulated in an order that varies from call to
+ * call (differences at the level of rounding). */
+int pmc_coag_gpu_size_dist(pmc_coag_gpu_ctx *ctx, int pop, int n_bin,
+                           double d_min, double d_max, double *num_dist,
+                           double *mass_dist);
+
 /* The weight magnitudes population `pop` uses now (n_group x n_class),
  * aero_weight_array_t%weight(:,:)%magnitude (aero_weight_array.F90:35-39). */
 int pmc_coag_gpu_get_weight(pmc_coag_gpu_ctx *ctx, int pop, double *w_mag);

@@ -56,6 +56,7 @@ SIGNATURES = {
     "pmc_coag_gpu_set_seed": (_I, [_P, _I, ctypes.c_uint64]),
     "pmc_coag_gpu_rebalance": (_I, [_P, _I, _DP, _I, _I]),
     "pmc_coag_gpu_get_weight": (_I, [_P, _I, _DP]),
+    "pmc_coag_gpu_size_dist": (_I, [_P, _I, _I, _D, _D, _DP, _DP]),
     "pmc_coag_gpu_replay_set": (_I, [_P, _DP, ctypes.c_int64]),
     "pmc_coag_gpu_replay_open": (_I, [_P, ctypes.c_char_p]),
     "pmc_coag_gpu_replay_used": (_I, [_P, _LP]),

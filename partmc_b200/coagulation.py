@@ -155,6 +155,16 @@ class AeroState:
             self.awa = AeroWeightArray(self.awa.type, mag, self.awa.exponent)
         return mag
 
+    def size_dist(self, n_bin, d_min, d_max, pop=0):
+        """Number and per-species mass distributions on a log diameter grid
+        (per unit ln D), computed on the device (pmc_coag_gpu_size_dist).
+        Returns (num (n_bin,), mass (n_bin, n_spec))."""
+        num = np.empty(n_bin)
+        mass = np.empty((n_bin, self.aero_data.n_spec))
+        check(_lib.lib().pmc_coag_gpu_size_dist(self.ctx, pop, int(n_bin), float(d_min), float(d_max), dp(num),
+                                                 dp(mass)), "pmc_coag_gpu_size_dist")
+        return num, mass
+
     def weight_magnitudes(self, pop=0):
         """Weight magnitudes (n_group, n_class) population ``pop`` uses now."""
         m = np.empty(self.awa.magnitude.size, dtype=np.float64)

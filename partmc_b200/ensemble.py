@@ -53,21 +53,25 @@ def reduce_counters(n_samp, n_coag, seconds, device="cpu"):
     return {"n_samp": int(work[0].item()), "n_coag": int(work[1].item()), "seconds": float(t.item())}
 
 
-def binned_totals(vol, num_conc, edges):
-    """Number concentration and per-species volume concentration per
-    diameter bin of one population: vol (n_part, n_spec) m^3, num_conc
-    (n_part,) m^-3 (each particle's weight), edges (n_bin + 1,) diameters.
-    Returns an (n_bin, 1 + n_spec) array."""
+def binned_totals(vol, num_conc, edges, density):
+    """Number and per-species mass distributions of one population per unit
+    ln(D) on the diameter grid `edges` (n_bin + 1, log-spaced), as
+    bin_grid_histogram_1d (bin_grid.F90:225-248) weights them: vol (n_part,
+    n_spec) m^3, num_conc (n_part,) m^-3, density (n_spec,) kg m^-3.
+    Returns an (n_bin, 1 + n_spec) array (number, then species masses).  The
+    GPU shard computes the same on the device (pmc_coag_gpu_size_dist)."""
     vol = np.asarray(vol, dtype=np.float64)
     if vol.ndim == 1:
         vol = vol[:, None]
+    n_bin = len(edges) - 1
+    width = (np.log(edges[-1]) - np.log(edges[0])) / n_bin
     d = 2.0 * np.cbrt(3.0 * vol.sum(1) / (4.0 * np.pi))
-    k = np.searchsorted(edges, d, side="right") - 1
-    ok = (k >= 0) & (k < len(edges) - 1)
-    out = np.zeros((len(edges) - 1, 1 + vol.shape[1]))
-    np.add.at(out[:, 0], k[ok], num_conc[ok])
+    k = np.floor((np.log(d) - np.log(edges[0])) / (np.log(edges[-1]) - np.log(edges[0])) * n_bin).astype(np.int64)
+    ok = (k >= 0) & (k < n_bin)
+    out = np.zeros((n_bin, 1 + vol.shape[1]))
+    np.add.at(out[:, 0], k[ok], num_conc[ok] / width)
     for s in range(vol.shape[1]):
-        np.add.at(out[:, 1 + s], k[ok], num_conc[ok] * vol[ok, s])
+        np.add.at(out[:, 1 + s], k[ok], num_conc[ok] * vol[ok, s] * density[s] / width)
     return out
 
 
@@ -91,7 +95,7 @@ class Ensemble:
     replace it (a callable factory taking the shard's populations, their
     temperatures, pressures and seeds, and returning an object with
     step(kernel_type, del_t, n_steps) -> (n_samp, n_coag) and
-    particles(k) -> (vol, num_conc))."""
+    histogram(k, edges) -> binned_totals of population k)."""
 
     def __init__(self, populations, temps, pressures, seeds, rank=0, world_size=1, mode=None, stepper=None):
         self.index = shard([p.vol.shape[0] for p in populations], world_size)[rank]
@@ -109,12 +113,12 @@ class Ensemble:
         return self.engine.step(kernel_type, del_t, n_steps)
 
     def histogram(self, edges):
-        """Binned totals summed over this rank's populations."""
+        """Size distributions (binned_totals layout) summed over this rank's
+        populations."""
         n_spec = self.pops[0].vol.shape[1] if self.pops else 1
         out = np.zeros((len(edges) - 1, 1 + n_spec))
         for k in range(len(self.pops)):
-            vol, nc = self.engine.particles(k)
-            out += binned_totals(vol, nc, edges)
+            out += self.engine.histogram(k, edges)
         return out
 
 
@@ -135,7 +139,7 @@ class _GpuShard:
     def step(self, kernel_type, del_t, n_steps):
         return self.C.mc_coag_batch(kernel_type, self.temps, self.pressures, 0.0, self.st, del_t, n_steps=n_steps)
 
-    def particles(self, k):
-        out = self.st.particles(pop=k)
-        r = np.cbrt(3.0 * out["vol"].sum(1) / (4.0 * np.pi))
-        return out["vol"], self.pops[k].awa.num_conc_at_radius(1, r)
+    def histogram(self, k, edges):
+        """On the device, without a download (log-spaced edges)."""
+        num, mass = self.st.size_dist(len(edges) - 1, edges[0], edges[-1], pop=k)
+        return np.concatenate([num[:, None], mass], axis=1)

@@ -42,10 +42,11 @@ class OracleShard:
                 c += b
         return s, c
 
-    def particles(self, k):
+    def histogram(self, k, edges):
         vol = self.orcs[k].particles()[0]
         r = np.cbrt(3.0 * vol.sum(1) / (4.0 * np.pi))
-        return vol, self.pops[k].awa.num_conc_at_radius(1, r)
+        p = self.pops[k]
+        return ens.binned_totals(vol, p.awa.num_conc_at_radius(1, r), edges, p.aero_data.density)
 
 
 def problem():
@@ -99,11 +100,13 @@ def test_binned_totals_conserve():
     rng = np.random.default_rng(3)
     vol = rng.uniform(1e-24, 1e-21, size=(500, 3))
     nc = rng.uniform(1e8, 1e9, size=500)
+    rho = np.array([1000.0, 1500.0, 2000.0])
     edges = np.logspace(-9, -5, 30)
-    h = ens.binned_totals(vol, nc, edges)
+    width = np.log(edges[-1] / edges[0]) / 29
+    h = ens.binned_totals(vol, nc, edges, rho) * width  # per unit ln D, times the width
     assert np.isclose(h[:, 0].sum(), nc.sum())
     for s in range(3):
-        assert np.isclose(h[:, 1 + s].sum(), (nc * vol[:, s]).sum())
+        assert np.isclose(h[:, 1 + s].sum(), (nc * vol[:, s] * rho[s]).sum())
 
 
 def test_two_gloo_ranks_match_one_process():
