@@ -50,6 +50,8 @@ extern "C" {
 #define PMC_KERNEL_CONSTANT 3
 #define PMC_KERNEL_BROWN 4
 #define PMC_KERNEL_ZERO 5
+#define PMC_KERNEL_BROWN_FREE 6  /* coag_kernel_brown_free.F90, spherical fractal parameters */
+#define PMC_KERNEL_BROWN_CONT 7  /* coag_kernel_brown_cont.F90, spherical fractal parameters */
 
 /* weight types, aero_weight.F90:24-30 */
 #define PMC_WEIGHT_NONE 1

@@ -14,6 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 KERNEL_SEDI, KERNEL_ADDITIVE, KERNEL_CONSTANT, KERNEL_BROWN, KERNEL_ZERO = 1, 2, 3, 4, 5
+KERNEL_BROWN_FREE, KERNEL_BROWN_CONT = 6, 7
 WEIGHT_NONE, WEIGHT_POWER, WEIGHT_MFA = 1, 2, 3
 MAX_COMPONENT = 20
 

@@ -890,6 +890,37 @@ static double sedi_helper(orc_state *st, double v1, double v2) {
 
 static const double BETA_0 = 0.25 / (60.0 * 2e8); /* coag_kernel_constant.F90:22 */
 
+/* Fractal parameters of spherical particles, fractal_set_spherical
+ * (fractal.F90:68-80): volume fractal dimension 3, primary radius 1e-8 m. */
+static const double FRAC_DIM = 3.0, PRIME_RADIUS = 1e-8;
+static const double AIR_DYN_VISC = 1.78e-5; /* constants.F90:65 */
+
+/* fractal_vol_to_num_of_monomers, fractal.F90:84-100 */
+static double num_of_monomers(double v) {
+  double x = orc_vol2rad(v) / PRIME_RADIUS;
+  return x * x * x;
+}
+
+/* kernel_brown_free_helper, coag_kernel_brown_free.F90 (free molecular
+ * regime) */
+static double brown_free_helper(double v1, double d1, double v2, double d2,
+                                double temp) {
+  double rho = (v1 / (v1 + v2)) * d1 + (v2 / (v1 + v2)) * d2;
+  double ni = num_of_monomers(v1), nj = num_of_monomers(v2);
+  double nif = pow(ni, 1.0 / FRAC_DIM), njf = pow(nj, 1.0 / FRAC_DIM);
+  double s = nif + njf;
+  return sqrt(6.0 * C_BOLTZMANN * temp * PRIME_RADIUS / rho *
+              (1.0 / ni + 1.0 / nj)) * (s * s);
+}
+
+/* kernel_brown_cont_helper, coag_kernel_brown_cont.F90 (continuum regime) */
+static double brown_cont_helper(double v1, double v2, double temp) {
+  double nif = pow(num_of_monomers(v1), 1.0 / FRAC_DIM);
+  double njf = pow(num_of_monomers(v2), 1.0 / FRAC_DIM);
+  return 2.0 * C_BOLTZMANN * temp / 3.0 / AIR_DYN_VISC *
+         (1.0 / nif + 1.0 / njf) * (nif + njf);
+}
+
 double orc_kernel_value(int kt, double v1, double d1, double v2, double d2,
                         double temp, double pressure, double coeff) {
   switch (kt) {
@@ -898,6 +929,8 @@ double orc_kernel_value(int kt, double v1, double d1, double v2, double d2,
     case ORC_KERNEL_CONSTANT: return BETA_0;
     case ORC_KERNEL_BROWN: return brown_helper(v1, d1, v2, d2, temp, pressure);
     case ORC_KERNEL_ZERO: return 0.0;
+    case ORC_KERNEL_BROWN_FREE: return brown_free_helper(v1, d1, v2, d2, temp);
+    case ORC_KERNEL_BROWN_CONT: return brown_cont_helper(v1, v2, temp);
   }
   return NAN;
 }
@@ -915,6 +948,10 @@ static double kernel_particles(orc_state *st, int kt, const double *va,
       return brown_helper(v1, vol_density(st, va), v2, vol_density(st, vb),
                           temp, pressure);
     case ORC_KERNEL_ZERO: return 0.0;
+    case ORC_KERNEL_BROWN_FREE:
+      return brown_free_helper(v1, vol_density(st, va), v2, vol_density(st, vb),
+                               temp);
+    case ORC_KERNEL_BROWN_CONT: return brown_cont_helper(v1, v2, temp);
   }
   orc_fail(st, ORC_ERR_ARG);
   return 0.0;
@@ -938,7 +975,10 @@ void orc_kernel_minmax(orc_state *st, int kt, double v1, double v2,
     case ORC_KERNEL_ZERO:
       *kmin = *kmax = 0.0;
       return;
-    case ORC_KERNEL_BROWN: {
+    case ORC_KERNEL_BROWN:
+    case ORC_KERNEL_BROWN_FREE:
+    case ORC_KERNEL_BROWN_CONT: {
+      /* kernel_brown*_minmax: 3x3 density samples */
       double dmin = st->density[0], dmax = st->density[0];
       for (int k = 1; k < st->n_spec; k++) {
         if (st->density[k] < dmin) dmin = st->density[k];
@@ -949,7 +989,11 @@ void orc_kernel_minmax(orc_state *st, int kt, double v1, double v2,
         for (int j = 1; j <= 3; j++) {
           double d1 = interp_linear_disc(dmin, dmax, 3, i);
           double d2 = interp_linear_disc(dmin, dmax, 3, j);
-          double k = brown_helper(v1, d1, v2, d2, temp, pressure);
+          double k = kt == ORC_KERNEL_BROWN
+                         ? brown_helper(v1, d1, v2, d2, temp, pressure)
+                         : kt == ORC_KERNEL_BROWN_FREE
+                               ? brown_free_helper(v1, d1, v2, d2, temp)
+                               : brown_cont_helper(v1, v2, temp);
           if (first) {
             first = 0;
             *kmin = k;
@@ -1623,7 +1667,7 @@ int orc_mc_coag(orc_state *st, int kt, double temp, double pressure,
   jmp_buf jb;
   *tot_n_samp = 0;
   *tot_n_coag = 0;
-  if (kt < ORC_KERNEL_SEDI || kt > ORC_KERNEL_ZERO) return ORC_ERR_ARG;
+  if (kt < ORC_KERNEL_SEDI || kt > ORC_KERNEL_BROWN_CONT) return ORC_ERR_ARG;
   st->fail = &jb;
   st->fail_code = ORC_OK;
   if (setjmp(jb)) {

@@ -39,7 +39,9 @@ enum {
   ORC_KERNEL_ADDITIVE = 2,
   ORC_KERNEL_CONSTANT = 3,
   ORC_KERNEL_BROWN = 4,
-  ORC_KERNEL_ZERO = 5
+  ORC_KERNEL_ZERO = 5,
+  ORC_KERNEL_BROWN_FREE = 6,
+  ORC_KERNEL_BROWN_CONT = 7
 };
 
 /* weight type codes, src/aero_weight.F90:24-30 */

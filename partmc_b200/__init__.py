@@ -6,5 +6,6 @@ reference's interface for that path.
 """
 from .coagulation import (AeroData, AeroState, AeroWeightArray, EnvState, HostMirror, mc_coag, mc_coag_batch,  # noqa: F401
                           COAG_KERNEL_TYPE_ADDITIVE, COAG_KERNEL_TYPE_BROWN, COAG_KERNEL_TYPE_CONSTANT,
-                          COAG_KERNEL_TYPE_SEDI, COAG_KERNEL_TYPE_ZERO, MODE_FP64, MODE_MIXED, MODE_REPLAY)
+                          COAG_KERNEL_TYPE_SEDI, COAG_KERNEL_TYPE_ZERO, COAG_KERNEL_TYPE_BROWN_FREE,
+                          COAG_KERNEL_TYPE_BROWN_CONT, MODE_FP64, MODE_MIXED, MODE_REPLAY)
 from ._lib import PmcError  # noqa: F401

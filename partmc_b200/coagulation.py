@@ -20,7 +20,9 @@ COAG_KERNEL_TYPE_ADDITIVE = 2
 COAG_KERNEL_TYPE_CONSTANT = 3
 COAG_KERNEL_TYPE_BROWN = 4
 COAG_KERNEL_TYPE_ZERO = 5
-KERNEL_NAMES = {"sedi": 1, "additive": 2, "constant": 3, "brown": 4, "zero": 5}
+COAG_KERNEL_TYPE_BROWN_FREE = 6
+COAG_KERNEL_TYPE_BROWN_CONT = 7
+KERNEL_NAMES = {"sedi": 1, "additive": 2, "constant": 3, "brown": 4, "zero": 5, "brown_free": 6, "brown_cont": 7}
 
 # aero_weight.F90:24-30
 AERO_WEIGHT_TYPE_NONE = 1

@@ -549,6 +549,12 @@ __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, 
       q[k].c = bp.deltasq;
     }
     if (P.kernel_type == kKernelSedi) q[k].a = fall_g(vol2rad(vt[k]));
+    if (P.kernel_type == kKernelBrownFree) {
+      q[k].a = vt[k];
+      q[k].b = ms[k] / vt[k];
+      q[k].c = pow(num_of_monomers(P.benv, vt[k]), 1.0 / P.benv.frac_dim);
+    }
+    if (P.kernel_type == kKernelBrownCont) q[k].a = pow(num_of_monomers(P.benv, vt[k]), 1.0 / P.benv.frac_dim);
   }
   int cc = cij[i] - 1;
   double k;
@@ -560,6 +566,8 @@ __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, 
       case kKernelConstant: k = pair_kernel<kKernelConstant, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
       case kKernelBrown: k = pair_kernel<kKernelBrown, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
       case kKernelSedi: k = pair_kernel<kKernelSedi, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
+      case kKernelBrownFree: k = pair_kernel<kKernelBrownFree, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
+      case kKernelBrownCont: k = pair_kernel<kKernelBrownCont, double, false>(P, a, b, cl[0], cl[1], cc, 0.0, P.coeff); break;
       default: k = 0.0;
     }
   } else {
@@ -576,6 +584,8 @@ __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, 
       case kKernelConstant: kf = pair_kernel<kKernelConstant, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
       case kKernelBrown: kf = pair_kernel<kKernelBrown, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
       case kKernelSedi: kf = pair_kernel<kKernelSedi, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
+      case kKernelBrownFree: kf = pair_kernel<kKernelBrownFree, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
+      case kKernelBrownCont: kf = pair_kernel<kKernelBrownCont, float, false>(P, a, b, cl[0], cl[1], cc, 0.f, (float)P.coeff); break;
       default: kf = 0.f;
     }
     k = kf;
@@ -1394,6 +1404,14 @@ void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaSt
       f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs, W, st)
           : launch_test<kKernelSedi, double>(c, flat, n_gpairs, W, st);
       break;
+    case kKernelBrownFree:
+      f32 ? launch_test<kKernelBrownFree, float>(c, flat, n_gpairs, W, st)
+          : launch_test<kKernelBrownFree, double>(c, flat, n_gpairs, W, st);
+      break;
+    case kKernelBrownCont:
+      f32 ? launch_test<kKernelBrownCont, float>(c, flat, n_gpairs, W, st)
+          : launch_test<kKernelBrownCont, double>(c, flat, n_gpairs, W, st);
+      break;
     default:
       launch_test<kKernelZero, double>(c, flat, n_gpairs, W, st);
   }
@@ -1413,6 +1431,12 @@ void launch_pp(Ctx& c, int kt, long long Q) {
       break;
     case kKernelSedi:
       k_pp_ops<kKernelSedi><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+      break;
+    case kKernelBrownFree:
+      k_pp_ops<kKernelBrownFree><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
+      break;
+    case kKernelBrownCont:
+      k_pp_ops<kKernelBrownCont><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
       break;
     default:
       k_pp_ops<kKernelZero><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
@@ -2396,7 +2420,7 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
 int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* temp,
                             const double* pressure, double additive_coeff, double del_t, int n_steps,
                             int64_t* tot_n_samp, int64_t* tot_n_coag) {
-  if (!x || kernel_type < 1 || kernel_type > 5 || !temp || !pressure || n_steps < 0)
+  if (!x || kernel_type < 1 || kernel_type > 7 || !temp || !pressure || n_steps < 0)
     return PMC_ERR_INVALID_ARG;
   Ctx& c = x->c;
   GUARD_BEGIN

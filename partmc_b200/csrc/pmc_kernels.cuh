@@ -123,6 +123,14 @@ __device__ __forceinline__ RecD make_rec(const PopDev& P, int i) {
       break;
     }
     case kKernelSedi: q.a = fall_g(vol2rad(P.vtot[i])); break;
+    case kKernelBrownFree: {
+      double v = P.vtot[i];
+      q.a = v;
+      q.b = P.mass[i] / v;
+      q.c = pow(num_of_monomers(P.benv, v), 1.0 / P.benv.frac_dim);
+      break;
+    }
+    case kKernelBrownCont: q.a = pow(num_of_monomers(P.benv, P.vtot[i]), 1.0 / P.benv.frac_dim); break;
     default: break;
   }
   return q;
@@ -507,6 +515,16 @@ __device__ __forceinline__ T pair_kernel(const PopDev& P, const T* q1, const T* 
     k = brown_pair<T>(q1[0], q1[3], q1[4], q1[5], q2[0], q2[3], q2[4], q2[5]);
   } else if (KT == kKernelSedi) {
     k = sedi_pair<T>(q1[0], q1[3], q2[0], q2[3]);
+  } else if (KT == kKernelBrownFree) {
+    // q = {r, rv, nc, volume, density, N^(1/d_f)}; 1/N = (R0 / r)^3
+    T v1 = q1[3], v2 = q2[3];
+    T rho = (v1 / (v1 + v2)) * q1[4] + (v2 / (v1 + v2)) * q2[4];
+    T x1 = T(P.benv.prime_radius) / q1[0], x2 = T(P.benv.prime_radius) / q2[0];
+    T s = q1[5] + q2[5];
+    k = sqrt(T(6.0 * kBoltzmann * P.benv.temp * P.benv.prime_radius) / rho * (x1 * x1 * x1 + x2 * x2 * x2)) * (s * s);
+  } else if (KT == kKernelBrownCont) {
+    // q = {r, rv, nc, N^(1/d_f), -, -}
+    k = T(2.0 * kBoltzmann * P.benv.temp / 3.0 / kAirDynVisc) * (T(1) / q1[3] + T(1) / q2[3]) * (q1[3] + q2[3]);
   } else {
     k = T(0);
   }

@@ -31,8 +31,11 @@ enum KernelType : int {
   kKernelAdditive = 2,
   kKernelConstant = 3,
   kKernelBrown = 4,
-  kKernelZero = 5
+  kKernelZero = 5,
+  kKernelBrownFree = 6,  // coag_kernel_brown_free.F90 (free molecular regime)
+  kKernelBrownCont = 7   // coag_kernel_brown_cont.F90 (continuum regime)
 };
+constexpr double kAirDynVisc = 1.78e-5;  // constants.F90:65
 // aero_weight.F90:24-30
 enum WeightType : int { kWeightNone = 1, kWeightPower = 2, kWeightMfa = 3 };
 
@@ -134,6 +137,9 @@ PMC_HD bool weights_flat(const Weights& w) {
 // environment, coag_kernel_brown.F90:143-151.
 struct BrownEnv {
   double temp, viscosd, gasfreepath;
+  // fractal_t (fractal.F90:56-63) for the free and continuum kernels;
+  // brown_env sets the spherical values of fractal_set_spherical
+  double frac_dim, prime_radius;
 };
 
 PMC_HD BrownEnv brown_env(double temp, double pressure) {
@@ -144,6 +150,8 @@ PMC_HD BrownEnv brown_env(double temp, double pressure) {
   double gasspeed = sqrt((8.0 * kBoltzmann * temp * kAvogadro) / (kPi * kAirMolecWeight));
   e.gasfreepath = 2.0 * viscosk / gasspeed;
   e.temp = temp;
+  e.frac_dim = 3.0;
+  e.prime_radius = 1e-8;
   return e;
 }
 
@@ -349,6 +357,29 @@ PMC_HD double sedi_kernel(double v1, double v2) {
   return sedi_pair<double>(r1, fall_g(vol2rad(v1)), r2, fall_g(vol2rad(v2)));
 }
 
+// fractal_vol_to_num_of_monomers (fractal.F90:84-100): N = (r / R0)^3
+PMC_HD double num_of_monomers(const BrownEnv& e, double v) {
+  double x = vol2rad(v) / e.prime_radius;
+  return x * x * x;
+}
+
+// kernel_brown_free_helper (coag_kernel_brown_free.F90): free molecular
+// regime, d1/d2 particle densities
+PMC_HD double brown_free_kernel(const BrownEnv& e, double v1, double d1, double v2, double d2) {
+  double rho = (v1 / (v1 + v2)) * d1 + (v2 / (v1 + v2)) * d2;
+  double ni = num_of_monomers(e, v1), nj = num_of_monomers(e, v2);
+  double nif = pow(ni, 1.0 / e.frac_dim), njf = pow(nj, 1.0 / e.frac_dim);
+  double s = nif + njf;
+  return sqrt(6.0 * kBoltzmann * e.temp * e.prime_radius / rho * (1.0 / ni + 1.0 / nj)) * (s * s);
+}
+
+// kernel_brown_cont_helper (coag_kernel_brown_cont.F90): continuum regime
+PMC_HD double brown_cont_kernel(const BrownEnv& e, double v1, double v2) {
+  double nif = pow(num_of_monomers(e, v1), 1.0 / e.frac_dim);
+  double njf = pow(num_of_monomers(e, v2), 1.0 / e.frac_dim);
+  return 2.0 * kBoltzmann * e.temp / 3.0 / kAirDynVisc * (1.0 / nif + 1.0 / njf) * (nif + njf);
+}
+
 // kernel_minmax, coag_kernel.F90:130-169 (Brownian: 3x3 density samples,
 // coag_kernel_brown.F90:58-101).  Returns false for a sedimentation error.
 PMC_HD bool kernel_minmax(int kt, double v1, double v2, const BrownEnv& be, double coeff,
@@ -362,13 +393,18 @@ PMC_HD bool kernel_minmax(int kt, double v1, double v2, const BrownEnv& be, doub
     case kKernelAdditive: *kmin = *kmax = coeff * (v1 + v2); return true;
     case kKernelConstant: *kmin = *kmax = kBeta0; return true;
     case kKernelZero: *kmin = *kmax = 0.0; return true;
-    case kKernelBrown: {
+    case kKernelBrown:
+    case kKernelBrownFree:
+    case kKernelBrownCont: {
+      // kernel_brown*_minmax: 3x3 density samples
       bool first = true;
       for (int i = 1; i <= 3; i++)
         for (int j = 1; j <= 3; j++) {
           double d1 = interp_linear_disc(dmin, dmax, 3, i);
           double d2 = interp_linear_disc(dmin, dmax, 3, j);
-          double k = brown_kernel(be, v1, d1, v2, d2);
+          double k = kt == kKernelBrown ? brown_kernel(be, v1, d1, v2, d2)
+                     : kt == kKernelBrownFree ? brown_free_kernel(be, v1, d1, v2, d2)
+                                              : brown_cont_kernel(be, v1, v2);
           if (first) {
             first = false;
             *kmin = *kmax = k;

@@ -238,6 +238,14 @@ struct Seq {
         }
         kk = brown_kernel(P->benv, v1, m1 / v1, v2, m2 / v2);
         break;
+      case kKernelBrownFree:
+        for (int s = 0; s < P->n_spec; s++) {
+          m1 = m1 + va[s] * P->density[s];
+          m2 = m2 + vb[s] * P->density[s];
+        }
+        kk = brown_free_kernel(P->benv, v1, m1 / v1, v2, m2 / v2);
+        break;
+      case kKernelBrownCont: kk = brown_cont_kernel(P->benv, v1, v2); break;
       default: kk = 0.0;
     }
     double ri = vol2rad(v1), rj = vol2rad(v2);

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 ENV = pm.EnvState(288.0, 1e5, 1000.0)
 KERNELS = [pm.COAG_KERNEL_TYPE_ADDITIVE, pm.COAG_KERNEL_TYPE_CONSTANT, pm.COAG_KERNEL_TYPE_BROWN,
-           pm.COAG_KERNEL_TYPE_SEDI]
+           pm.COAG_KERNEL_TYPE_SEDI, pm.COAG_KERNEL_TYPE_BROWN_FREE, pm.COAG_KERNEL_TYPE_BROWN_CONT]
 
 
 def populations():

@@ -51,9 +51,13 @@ def test_additive_matches_exact_solution(gpu_lib, mode):
         assert err < 0.05, (t, err)
 
 
-def test_brownian_matches_oracle_ensemble(gpu_lib):
-    """Number and mass distributions of a power-weighted Brownian run agree
-    with the oracle's ensemble within 3 sigma of the Monte Carlo error."""
+@pytest.mark.parametrize("kt", [pm.COAG_KERNEL_TYPE_BROWN, pm.COAG_KERNEL_TYPE_BROWN_FREE,
+                                pm.COAG_KERNEL_TYPE_BROWN_CONT])
+def test_brownian_matches_oracle_ensemble(gpu_lib, kt):
+    """Number and mass distributions of a power-weighted run with each of
+    the Brownian kernels (transition regime, free molecular, continuum)
+    agree with the oracle's ensemble within 3 sigma of the Monte Carlo
+    error."""
     n_part, n_runs, n_steps = 4000, 8, 30
     env = pm.EnvState(288.0, 1e5)
     hist = {"gpu": [], "cpu": []}
@@ -65,8 +69,8 @@ def test_brownian_matches_oracle_ensemble(gpu_lib):
         orc.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
         orc.set_next_id(pop.n_part + 1)
         for _ in range(n_steps):
-            pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, 600.0)
-            orc.mc_coag(O.KERNEL_BROWN, 288.0, 1e5, 0.0, 600.0)
+            pm.mc_coag(kt, env, pop.aero_data, st, 600.0)
+            orc.mc_coag(kt, 288.0, 1e5, 0.0, 600.0)
         for key, vol in (("gpu", st.particles()["vol"]), ("cpu", orc.particles()[0])):
             r = E.vol2rad(vol.sum(1))
             nc = pop.awa.num_conc_at_radius(1, r)
