@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 #include <thread>
+#include <type_traits>
 
 #include "../../include/pmc_coag_gpu.h"
 #include "pmc_kernels.cuh"
@@ -181,27 +182,53 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
 // small helper kernels
 
 
-// accepted samples in sample order: event e gets its sample index, its two
-// slots and its global pair
+// accepted samples of round 0 in sample order: event e gets its key (pair,
+// sample), its two slots, its global pair and its position in the pair's
+// test sequence ((s + 1) / n_samp: the part of the pair done after it)
 __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const long long* n_samples,
-                                long long* outw, const int2* ev, const int* ev_gp, int2* ev_c,
-                                int* gp_c) {
+                                const int2* ev, const int* ev_gp, const int* gpair_local, const long long* work_off,
+                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len) {
   long long n = *n_samples;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     if (flag[i]) {
       long long e = off[i];
-      outw[e] = i;
+      int gp = ev_gp[i];
+      long long s = i - work_off[gp], ns = work_off[gp + 1] - work_off[gp];
+      ev_key[e] = make_key((uint32_t)gpair_local[gp], 0u, (uint32_t)s);
       ev_c[e] = ev[i];
-      gp_c[e] = ev_gp[i];
+      gp_c[e] = gp;
+      ev_pos[e] = (float)((double)(s + 1) / (double)ns);
+      ev_len[e] = 0;
+    }
+}
+
+// the events a later round's items made, in item order
+__global__ void k_compact_items(const uint8_t* it_flag, const long long* off, const long long* n_items,
+                                const unsigned long long* it_key, const int2* it_c, const int* it_gp,
+                                const float* it_pos, const int* it_len, const int* it_head, const uint8_t* it_done,
+                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len,
+                                int* ev_head, uint8_t* ev_done) {
+  long long n = *n_items;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    if (it_flag[i]) {
+      long long e = off[i];
+      ev_key[e] = it_key[i];
+      ev_c[e] = it_c[i];
+      gp_c[e] = it_gp[i];
+      ev_pos[e] = it_pos[i];
+      ev_len[e] = it_len[i];
+      ev_head[e] = it_head[i];
+      ev_done[e] = it_done[i];
     }
 }
 
 // target operations of round 0, in the reference's backwards target order
 // (coagulation.F90:220-237)
 __global__ void k_build_ops(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
-                            const long long* pp_off, const long long* prio_off, int n_gpairs,
-                            int* op_pop, int* op_pair, int* op_slot, int* op_k, unsigned* op_prio) {
+                            const long long* pp_off, int n_gpairs, int* op_pop, int* op_pair, int* op_slot,
+                            int* op_k, unsigned long long* op_key) {
   int gp = blockIdx.x;
   if (gp >= n_gpairs) return;
   long long n = pp_off[gp + 1] - pp_off[gp];
@@ -218,15 +245,16 @@ __global__ void k_build_ops(const PopDev* pops, const int* gpair_pop, const int*
     op_pair[q] = p;
     op_slot[q] = P.list[start + (int)(n - 1 - k)];
     op_k[q] = (int)k;
-    op_prio[q] = (unsigned)(prio_off[gp] + k);
+    op_key[q] = make_key((uint32_t)p, 0u, (uint32_t)k);
   }
 }
 
-// redo list of lost target operations (order of q kept)
+// redo list of lost target operations (order of q kept); a redo keeps its
+// place in the loop order (its key)
 __global__ void k_build_redo(const int* op_pop, const int* op_pair, const int* op_slot,
-                             const int* op_k, const int* lost, const long long* lost_off,
-                             long long Q, int* r_pop, int* r_pair, int* r_slot, int* r_k,
-                             unsigned* r_prio, unsigned prio_base) {
+                             const int* op_k, const unsigned long long* op_key, const int* lost,
+                             const long long* lost_off, long long Q, int* r_pop, int* r_pair, int* r_slot,
+                             int* r_k, unsigned long long* r_key) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
     if (!lost[q]) continue;
@@ -235,8 +263,19 @@ __global__ void k_build_redo(const int* op_pop, const int* op_pair, const int* o
     r_pair[j] = op_pair[q];
     r_slot[j] = op_slot[q];
     r_k[j] = op_k[q] + (1 << 24);  // fresh random stream for the redo
-    r_prio[j] = prio_base + (unsigned)j;
+    r_key[j] = op_key[q];
   }
+}
+
+// first event of population k (events are ordered by population)
+__device__ long long first_event_of(int k, long long E, const int* ev_gp, const int* gpair_pop) {
+  long long lo = 0, hi = E;
+  while (lo < hi) {
+    long long mid = (lo + hi) >> 1;
+    if (gpair_pop[ev_gp[mid]] < k) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
 }
 
 // Per-population bases of the allocations of one round.  Events and target
@@ -247,24 +286,24 @@ __global__ void k_build_redo(const int* op_pop, const int* op_pair, const int* o
 // per_pop by k_count_per_pop.  The slot and ID counters of each population
 // advance here by the round's allocations: the apply kernels read only the
 // bases.  One block; populations in tiles of blockDim.x.
-__global__ void k_alloc_bases(const PopDev* pops, int n_pop, const long long* pop_pair_base,
-                              const long long* work_off, const long long* flag_off, int has_set,
-                              const long long* rank_slot_set, const long long* rank_id_set, int* per_pop,
-                              int* set_slot_base, long long* set_id_base, int* pp_slot_base,
-                              long long* pp_id_base) {
+__global__ void k_alloc_bases(const PopDev* pops, int n_pop, const long long* n_events, const int* ev_gp,
+                              const int* gpair_pop, int has_set, const long long* rank_slot_set,
+                              const long long* rank_id_set, int* per_pop, int* set_slot_base,
+                              long long* set_id_base, int* pp_slot_base, long long* pp_id_base) {
   long long carry[4] = {0, 0, 0, 0};
+  long long E = has_set ? *n_events : 0;
   for (int base = 0; base < n_pop; base += blockDim.x) {
     int k = base + threadIdx.x;
     long long cnt[4] = {0, 0, 0, 0};
     if (k < n_pop) {
-      if (has_set) {
-        long long e_lo = flag_off[work_off[pop_pair_base[k]]];
-        long long e_hi = flag_off[work_off[pop_pair_base[k + 1]]];
+      if (E > 0) {
+        long long e_lo = first_event_of(k, E, ev_gp, gpair_pop);
+        long long e_hi = first_event_of(k + 1, E, ev_gp, gpair_pop);
         cnt[0] = rank_slot_set[e_hi] - rank_slot_set[e_lo];
         cnt[1] = rank_id_set[e_hi] - rank_id_set[e_lo];
-        per_pop[k] = (int)cnt[0];
-        per_pop[n_pop + k] = (int)cnt[1];
       }
+      per_pop[k] = (int)cnt[0];
+      per_pop[n_pop + k] = (int)cnt[1];
       cnt[2] = per_pop[2 * n_pop + k];
       cnt[3] = per_pop[3 * n_pop + k];
     }
@@ -427,6 +466,7 @@ __global__ void k_double(PopDev P, int n, const uint8_t* flag, const long long* 
     P.recd[d] = P.recd[i];
     P.recf[d] = P.recf[i];
     P.claim[d] = ~0ULL;
+    P.touched[d] = ~0u;
     P.alive[d] = 1;
     P.changed[d] = 1;
   }
@@ -507,6 +547,7 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.changed[j] = S.changed[i];
     D.cell[j] = S.cell[i];
     D.claim[j] = S.claim[i];
+    D.touched[j] = S.touched[i];
     D.recd[j] = S.recd[i];
     D.recf[j] = S.recf[i];
   }
@@ -708,15 +749,15 @@ struct Ctx {
   bool dirty = true;            // host PopDev copies changed since the last push
   std::vector<PopCtr> h_ctrs;
   cudaStream_t stream = nullptr;
-  int max_rounds = 32;
+  int max_rounds = 200;  // below 256: the round is 8 bits of the random streams' counters
   int n_sm = 148;        // multiprocessors of the device
-  // redraw rounds as a CUDA graph
+  // later rounds as a CUDA graph
   bool use_graph = true;
   cudaStream_t cap_stream = nullptr;  // capture stream
   cudaGraph_t rg_graph = nullptr;
   cudaGraphExec_t rg_exec = nullptr;
   std::vector<long long> rg_key;
-  std::vector<long long> rg_seen;  // the key of the previous step's redraw rounds
+  std::vector<long long> rg_seen;  // the key of the previous step's later rounds
   long long rg_nodes = 0, rg_builds = 0;
   DevBuf<long long> graph_stats;
   size_t sort_smem = 0;  // dynamic shared memory the sort grid was sized for
@@ -724,19 +765,34 @@ struct Ctx {
   // per-round buffers
   DevBuf<int> gpair_pop, gpair_local;
   DevBuf<long long> pop_pair_base;
-  DevBuf<long long> nwork_set, nwork_pp, nprio, work_off, pp_off, prio_off;
-  DevBuf<int> pair_losers;
+  DevBuf<long long> nwork_set, nwork_pp, work_off, pp_off;
   DevBuf<uint8_t> flag, win_set, win_pp;
   DevBuf<uint32_t> dec_set;  // merge decision of each accepted per-set event
   DevBuf<int> ev_gp, gp_c;   // global pair of each accepted sample / event
   DevBuf<int2> ev_c;         // slots of each event
+  DevBuf<unsigned long long> ev_key;  // key of each event (make_key)
+  DevBuf<float> ev_pos;      // position of each event in its pair's test sequence
+  DevBuf<int> ev_dest;       // slot of the particle each event made (-1: none)
+  DevBuf<int> ev_len, ev_head, ev_app;  // chains: events, first chunk, events applied
+  DevBuf<uint8_t> ev_done;   // chains: the walk ran to the end
   DevBuf<double2> ice_set;   // water volumes of the sources of each event
   DevBuf<int2> ev;
-  DevBuf<long long> flag_off, ev_w;
+  DevBuf<long long> flag_off;
+  // a later round's items (one per event of the round before) and what they made
+  DevBuf<uint8_t> it_flag, it_done;
+  DevBuf<unsigned long long> it_key;
+  DevBuf<int2> it_c;
+  DevBuf<int> it_gp, it_len, it_head;
+  DevBuf<float> it_pos;
+  DevBuf<long long> it_off;
+  // chain events of a round (ChainPool), in chunks
+  DevBuf<int> ch_y, ch_q;
+  DevBuf<float> ch_pos;
+  long long ch_chunks = 0;
   DevBuf<int> need_slot_set, need_id_set, need_slot_pp, need_id_pp, lost_pp;
   DevBuf<long long> rank_slot_set, rank_id_set, rank_slot_pp, rank_id_pp, lost_off;
   DevBuf<int> op_pop, op_pair, op_slot, op_k, r_pop, r_pair, r_slot, r_k;
-  DevBuf<unsigned> op_prio, r_prio;
+  DevBuf<unsigned long long> op_key, r_key;
   DevBuf<PPResult> pp_res;
   DevBuf<double> pp_vol;
   DevBuf<int> per_pop_i;  // 4 x n_pop counters
@@ -758,7 +814,7 @@ struct Ctx {
   long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
   long long last_set_losers = 0, last_pp_lost = 0, last_events = 0, last_ops = 0;
   // optional per-kernel timing with CUDA events on the library's stream:
-  // 0 pair tests, 1 sorts (k_sort_all), 2 redraw-round graph launches,
+  // 0 pair tests, 1 sorts (k_sort_all), 2 later-round graph launches,
   // 3 whole steps
   bool prof = false;
   struct ProfPair {
@@ -771,7 +827,8 @@ struct Ctx {
   // host copy of each population's slot count, kept current after every
   // round so the sort can size itself without reading the device
   std::vector<int> n_slots_host;
-  // device scalars of a round: [0] per-set losers; [1..3] spare
+  // device scalars of a round: [0] events that lost a claim, [1] events,
+  // [2] items (the events of the round before), [3] chain chunks handed out
   DevBuf<long long> round_dev;
   std::vector<long long> base_cached;  // pair-list layout last uploaded
   double prof_ms[4] = {0, 0, 0, 0};
@@ -977,9 +1034,11 @@ void alloc_slots(Ctx& c, PopHost& ph, int cap) {
   h.recd = dalloc<RecD>(o, cap);
   h.recf = dalloc<RecF>(o, cap);
   h.claim = dalloc<unsigned long long>(o, cap);
+  h.touched = dalloc<uint32_t>(o, cap);
   CK(cudaMemsetAsync(h.alive, 0, cap, c.stream));
   CK(cudaMemsetAsync(h.changed, 0, cap, c.stream));
   CK(cudaMemsetAsync(h.claim, 0xff, sizeof(unsigned long long) * cap, c.stream));  // no claim
+  CK(cudaMemsetAsync(h.touched, 0xff, sizeof(uint32_t) * cap, c.stream));        // no generation
   c.dirty = true;
 }
 
@@ -1011,6 +1070,31 @@ void alloc_sort(Ctx& c, PopHost& ph) {
           ph.pair_desc.push_back(d);
         }
   h.n_pairs = (int)ph.pair_desc.size();
+  if (h.n_pairs >= (1 << 20)) throw Fail(PMC_ERR_CAPACITY);  // pair numbers in keys and random streams
+  // the pairs of each cell in loop order, for walks
+  {
+    std::vector<int> off(h.n_cells + 1, 0), list;
+    for (const PairDesc& d : ph.pair_desc) {
+      off[d.b1 + nb * d.c1 + 1]++;
+      if (d.b2 + nb * d.c2 != d.b1 + nb * d.c1) off[d.b2 + nb * d.c2 + 1]++;
+    }
+    for (int k = 0; k < h.n_cells; k++) off[k + 1] += off[k];
+    list.assign(std::max(off[h.n_cells], 1), 0);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int p = 0; p < h.n_pairs; p++) {
+      const PairDesc& d = ph.pair_desc[p];
+      int a = d.b1 + nb * d.c1, b = d.b2 + nb * d.c2;
+      list[fill[a]++] = p;
+      if (b != a) list[fill[b]++] = p;
+    }
+    int* d_off = dalloc<int>(o, off.size());
+    int* d_list = dalloc<int>(o, list.size());
+    CK(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));  // the host vectors go out of scope
+    h.cp_off = d_off;
+    h.cp_list = d_list;
+  }
   PairDesc* pd = dalloc<PairDesc>(o, std::max<size_t>(ph.pair_desc.size(), 1));
   if (!ph.pair_desc.empty())
     CK(cudaMemcpyAsync(pd, ph.pair_desc.data(), sizeof(PairDesc) * ph.pair_desc.size(),
@@ -1370,77 +1454,78 @@ void sort_pops(Ctx& c, bool decide_grid) {
 // ---------------------------------------------------------------------------
 // one step over all populations
 
-template <int KT, class T>
-void launch_test(Ctx& c, bool flat, int n_gpairs, long long W, cudaStream_t st) {
-  // sized from the round's sample count: redraw rounds are small
-  int blocks = (int)std::min<long long>(148 * 8, std::max<long long>(1, (W + 255) / 256));
-  if (flat)
-    k_test<KT, T, true><<<blocks, 256, 0, st>>>(
-        c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
-        c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
-  else
-    k_test<KT, T, false><<<blocks, 256, 0, st>>>(
-        c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, n_gpairs,
-        c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
-  note_launch();
+// call f(std::integral_constant<int, KT>, T{}) with the kernel type kt and the
+// pair-test arithmetic of the mode (FP32 in MIXED, else FP64)
+template <class F>
+void with_kt(const Ctx& c, int kt, F&& f) {
+  bool f32 = c.mode == PMC_MODE_MIXED;
+  auto go = [&](auto ktc) {
+    if (f32) f(ktc, float{});
+    else f(ktc, double{});
+  };
+  switch (kt) {
+    case kKernelAdditive: go(std::integral_constant<int, kKernelAdditive>{}); break;
+    case kKernelConstant: go(std::integral_constant<int, kKernelConstant>{}); break;
+    case kKernelBrown: go(std::integral_constant<int, kKernelBrown>{}); break;
+    case kKernelSedi: go(std::integral_constant<int, kKernelSedi>{}); break;
+    case kKernelBrownFree: go(std::integral_constant<int, kKernelBrownFree>{}); break;
+    case kKernelBrownCont: go(std::integral_constant<int, kKernelBrownCont>{}); break;
+    default: f(std::integral_constant<int, kKernelZero>{}, double{});
+  }
 }
 
 void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaStream_t st) {
-  bool f32 = c.mode == PMC_MODE_MIXED;
-  switch (kt) {
-    case kKernelAdditive:
-      f32 ? launch_test<kKernelAdditive, float>(c, flat, n_gpairs, W, st)
-          : launch_test<kKernelAdditive, double>(c, flat, n_gpairs, W, st);
-      break;
-    case kKernelConstant:
-      f32 ? launch_test<kKernelConstant, float>(c, flat, n_gpairs, W, st)
-          : launch_test<kKernelConstant, double>(c, flat, n_gpairs, W, st);
-      break;
-    case kKernelBrown:
-      f32 ? launch_test<kKernelBrown, float>(c, flat, n_gpairs, W, st)
-          : launch_test<kKernelBrown, double>(c, flat, n_gpairs, W, st);
-      break;
-    case kKernelSedi:
-      f32 ? launch_test<kKernelSedi, float>(c, flat, n_gpairs, W, st)
-          : launch_test<kKernelSedi, double>(c, flat, n_gpairs, W, st);
-      break;
-    case kKernelBrownFree:
-      f32 ? launch_test<kKernelBrownFree, float>(c, flat, n_gpairs, W, st)
-          : launch_test<kKernelBrownFree, double>(c, flat, n_gpairs, W, st);
-      break;
-    case kKernelBrownCont:
-      f32 ? launch_test<kKernelBrownCont, float>(c, flat, n_gpairs, W, st)
-          : launch_test<kKernelBrownCont, double>(c, flat, n_gpairs, W, st);
-      break;
-    default:
-      launch_test<kKernelZero, double>(c, flat, n_gpairs, W, st);
-  }
+  // sized from the round's sample count
+  int blocks = (int)std::min<long long>(148 * 8, std::max<long long>(1, (W + 255) / 256));
+  with_kt(c, kt, [&](auto ktc, auto tt) {
+    constexpr int KT = decltype(ktc)::value;
+    using T = decltype(tt);
+    if (flat)
+      k_test<KT, T, true><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
+                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
+    else
+      k_test<KT, T, false><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
+                                                   c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
+  });
+  note_launch();
+}
+
+ChainPool chain_pool(Ctx& c) {
+  ChainPool pool;
+  pool.y = c.ch_y.p;
+  pool.q = c.ch_q.p;
+  pool.pos = c.ch_pos.p;
+  pool.ctr = c.round_dev.p + 3;
+  pool.n_chunks = c.ch_chunks;
+  return pool;
+}
+
+// a later round's items: the events of the round before, n_items =
+// round_dev[2] on the device, W bounds it
+void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaStream_t st) {
+  int blocks = grid_for(W, 256);
+  const long long* n_items = c.round_dev.p + 2;
+  ChainPool pool = chain_pool(c);
+  with_kt(c, kt, [&](auto ktc, auto tt) {
+    constexpr int KT = decltype(ktc)::value;
+    using T = decltype(tt);
+    auto k = flat ? k_items<KT, T, true> : k_items<KT, T, false>;
+    k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
+                              c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, pool,
+                              c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
+                              c.it_done.p);
+  });
+  note_launch();
 }
 
 void launch_pp(Ctx& c, int kt, long long Q) {
   int blocks = grid_for(Q, 128);
-  switch (kt) {
-    case kKernelAdditive:
-      k_pp_ops<kKernelAdditive><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-      break;
-    case kKernelConstant:
-      k_pp_ops<kKernelConstant><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-      break;
-    case kKernelBrown:
-      k_pp_ops<kKernelBrown><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-      break;
-    case kKernelSedi:
-      k_pp_ops<kKernelSedi><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-      break;
-    case kKernelBrownFree:
-      k_pp_ops<kKernelBrownFree><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-      break;
-    case kKernelBrownCont:
-      k_pp_ops<kKernelBrownCont><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-      break;
-    default:
-      k_pp_ops<kKernelZero><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_prio.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p); note_launch();
-  }
+  with_kt(c, kt, [&](auto ktc, auto) {
+    constexpr int KT = decltype(ktc)::value;
+    k_pp_ops<KT><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
+                                               c.op_key.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p);
+  });
+  note_launch();
 }
 
 void set_n_dev(Ctx& c, long long v) {
@@ -1578,7 +1663,7 @@ int replay_step_host(Ctx& c, long long* s_out, long long* k_out) {
 __global__ void k_step_reset(PopCtr* ctrs, int n_pop) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_pop) return;
-  ctrs[k].tot_samp = ctrs[k].tot_coag = ctrs[k].kmax_warn = ctrs[k].redraws = 0;
+  ctrs[k].tot_samp = ctrs[k].tot_coag = ctrs[k].kmax_warn = ctrs[k].redraws = ctrs[k].walk_tests = 0;
   ctrs[k].status = 0;
   ctrs[k].bad_site = 0;
   ctrs[k].bad_index = 0;
@@ -1591,8 +1676,10 @@ __global__ void k_fill_claims(const PopDev* pops) {
     if (blockIdx.x == 0 && threadIdx.x == 0) bad_index(P.ctr, kBadSlotCount, n);
     n = P.cap;
   }
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     P.claim[i] = ~0ULL;
+    P.touched[i] = ~0u;
+  }
 }
 
 // per-population work of a round: samples and target operations
@@ -1606,111 +1693,151 @@ __global__ void k_pop_work(const long long* pop_pair_base, int n_pop, const long
 }
 
 // ---------------------------------------------------------------------------
-// Redraw rounds as one CUDA graph.  After round 0 the host knows a bound on
-// the samples of every later round (round 0's losers) and every kernel of a
-// round reads its exact counts from the device, so the rounds up to the
-// step's end run as the body of a conditional WHILE node: k_round_begin
-// advances the round and the claim generation and clears the round's
-// scalars; k_round_end accumulates the step's statistics and sets the loop
-// condition (losers left and fewer than max_rounds rounds).  Only per-set
-// rounds run this way; a step with per-particle work keeps the host loop.
+// Later rounds.  After round 0 every kernel of a round reads its counts from
+// the device, and round 0's events bound every later round's items and
+// events (each event yields at most one item of the next round, each item at
+// most one event or chain).  So the later rounds run as the body of a
+// conditional WHILE node of one CUDA graph: k_round_begin advances the round
+// and the claim generation and makes the last round's events this round's
+// items; k_round_end adds up the step's statistics and sets the loop
+// condition: events in this round, fewer than max_rounds rounds, and room
+// in every population for the next round's new slots.  Without room the
+// graph stops and the host loop, which can grow the slot arrays, carries
+// on.  Rounds with per-particle redo operations run from the host loop.
 
 __global__ void k_round_begin(uint32_t* d_round, long long* round_dev, int* per_pop, int n_per_pop) {
   if (blockIdx.x != 0) return;
   if (threadIdx.x == 0) {
     d_round[0] += 1u;
     d_round[1] += 1u;
+    round_dev[2] = round_dev[1];
+    round_dev[0] = 0;
+    round_dev[1] = 0;
+    round_dev[3] = 0;
   }
-  for (int k = threadIdx.x; k < 4; k += blockDim.x) round_dev[k] = 0;
   for (int k = threadIdx.x; k < n_per_pop; k += blockDim.x) per_pop[k] = 0;
 }
 
-// stats: [0] per-set losers (redraws), [1] events, [2] rounds
+// stats: [0] events that lost a claim, [1] events, [2] rounds, [3] 1 if the
+// graph stopped for lack of slots with events left
 __global__ void k_round_end(const long long* round_dev, long long* stats, const uint32_t* d_round, int max_rounds,
-                            PopCtr* ctrs, int n_pop, cudaGraphConditionalHandle cond) {
+                            const PopDev* pops, PopCtr* ctrs, int n_pop, cudaGraphConditionalHandle cond) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  long long losers = round_dev[0];
-  stats[0] += losers;
-  stats[1] += round_dev[1];
+  long long E = round_dev[1];
+  stats[0] += round_dev[0];
+  stats[1] += E;
   stats[2] += 1;
-  bool more = losers > 0 && (int)d_round[0] + 1 < max_rounds;
-  if (losers > 0 && !more)
+  bool room = true;
+  for (int k = 0; k < n_pop; k++)
+    if ((long long)ctrs[k].n_slots + E > (long long)pops[k].cap) room = false;
+  bool more = E > 0 && room && (int)d_round[0] + 1 < max_rounds;
+  if (E > 0 && room && !more)
     for (int k = 0; k < n_pop; k++)
       if (ctrs[k].status == 0) ctrs[k].status = kErrTimeout;
+  if (E > 0 && !room) stats[3] = 1;
   cudaGraphSetConditional(cond, more ? 1u : 0u);
 }
 
-struct RedrawBounds {
-  int kt;
-  bool flat;
-  int n_gpairs, max_pairs;
-  long long W;     // samples per round, at most
-  int max_chunks;  // sort chunks per population, at most
-  int max_cells;
-  float inflate;
-};
-
-// the kernels of one redraw round on stream st (per-set path only)
-void enqueue_redraw_round(Ctx& c, cudaStream_t st, const RedrawBounds& b, cudaGraphConditionalHandle cond) {
-  size_t ng = (size_t)b.n_gpairs + 1;
-  long long W = b.W;
-  k_round_begin<<<1, 128, 0, st>>>(c.d_round, c.round_dev.p, c.per_pop_i.p, 4 * c.n_pop);
-  note_launch();
-  launch_sort(c, st, b.max_chunks, b.max_cells);
-  {
-    dim3 gp((b.max_pairs + 127) / 128, c.n_pop);
-    k_pairs<<<gp, 128, 0, st>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, c.nprio.p,
-                                c.pair_losers.p, 1, b.inflate);
+// Resolve and apply the events of a round (E at round_dev[1], at most W) and,
+// with Q > 0 (host loop only), its Q target operations.
+void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
+  long long* Ed = c.round_dev.p + 1;
+  ChainPool pool = chain_pool(c);
+  if (W > 0) {
+    k_resolve_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+                                                    c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p,
+                                                    c.round_dev.p, c.ev_len.p, c.ev_head.p, c.ev_app.p, pool);
+    note_launch();
+    scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}},
+                    st);
+  }
+  if (Q > 0) {
+    set_n_dev(c, Q);
+    k_pp_resolve<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.op_key.p, c.n_dev.p, c.pp_res.p,
+                                                   c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
+    note_launch();
+    scan_multi<int>(c, {{c.need_slot_pp.p, Q, nullptr, c.rank_slot_pp.p}, {c.need_id_pp.p, Q, nullptr, c.rank_id_pp.p}},
+                    st);
+    k_count_per_pop<<<grid_for(Q, 256), 256, 0, st>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p,
+                                                      c.per_pop_i.p + 2 * c.n_pop);
+    note_launch();
+    k_count_per_pop<<<grid_for(Q, 256), 256, 0, st>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p,
+                                                      c.per_pop_i.p + 3 * c.n_pop);
     note_launch();
   }
-  scan_multi<long long>(c, {{c.nwork_set.p, b.n_gpairs, nullptr, c.work_off.p},
-                            {c.nwork_pp.p, b.n_gpairs, nullptr, c.pp_off.p},
-                            {c.nprio.p, b.n_gpairs, nullptr, c.prio_off.p}}, st);
-  CK(cudaMemsetAsync(c.pair_losers.p, 0, sizeof(int) * ng, st));
-  launch_test_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
-  const long long* Wd = c.work_off.p + b.n_gpairs;
+  k_alloc_bases<<<1, 256, 0, st>>>(c.d_pops, c.n_pop, Ed, c.gp_c.p, c.gpair_pop.p, W > 0 ? 1 : 0, c.rank_slot_set.p,
+                                   c.rank_id_set.p, c.per_pop_i.p, c.slot_base_set.p, c.id_base_set.p,
+                                   c.slot_base_pp.p, c.id_base_pp.p);
+  note_launch();
+  if (W > 0) {
+    // part 1, one warp per event: species and components
+    k_apply_move<<<grid_for(W * 32, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+                                                        c.win_set.p, c.dec_set.p, c.rank_slot_set.p,
+                                                        c.slot_base_set.p, c.ice_set.p);
+    note_launch();
+    // part 2, one thread per event: removals, scalar fields, caches
+    k_apply_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+                                                  c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
+                                                  c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_dest.p);
+    note_launch();
+    // chains, one thread each
+    k_apply_chain<<<grid_for(W, 128), 128, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, Ed, c.ev_key.p,
+                                                    c.win_set.p, c.ev_len.p, c.ev_app.p, c.ev_head.p, c.ev_done.p,
+                                                    pool, c.gp_c.p, c.ev_pos.p, c.ev_dest.p);
+    note_launch();
+  }
+  if (Q > 0) {
+    k_pp_apply<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
+                                                 c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p, c.slot_base_pp.p,
+                                                 c.id_base_pp.p);
+    note_launch();
+    scan_multi<int>(c, {ScanArg<int>{c.lost_pp.p, Q, nullptr, c.lost_off.p}}, st);
+  }
+}
+
+struct RoundBounds {
+  int kt;
+  bool flat;
+  int n_gpairs;
+  long long W;  // items and events of a round, at most
+};
+
+// The kernels of one later round on stream st, after k_round_begin: items,
+// their events in item order, then resolve and apply.  With Q > 0 (host
+// loop only) the round's per-particle redo operations claim alongside.
+void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long Q) {
+  long long W = b.W;
+  launch_items_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
+  if (Q > 0) {
+    set_n_dev(c, Q);
+    launch_pp(c, b.kt, Q);
+  }
+  const long long* Id = c.round_dev.p + 2;
   long long* Ed = c.round_dev.p + 1;
-  scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, Ed}}, st);
-  k_compact_flags<<<grid_for(W, 256), 256, 0, st>>>(c.flag.p, c.flag_off.p, Wd, c.ev_w.p, c.ev.p, c.ev_gp.p,
-                                                    c.ev_c.p, c.gp_c.p);
+  scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.it_flag.p, W, Id, c.it_off.p, Ed}}, st);
+  k_compact_items<<<grid_for(W, 256), 256, 0, st>>>(c.it_flag.p, c.it_off.p, Id, c.it_key.p, c.it_c.p, c.it_gp.p,
+                                                    c.it_pos.p, c.it_len.p, c.it_head.p, c.it_done.p, c.ev_key.p,
+                                                    c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.ev_len.p, c.ev_head.p,
+                                                    c.ev_done.p);
   note_launch();
-  k_resolve_set<<<grid_for(W, 256), 256, 0, st>>>(
-      c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p,
-      c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p, c.round_dev.p);
-  note_launch();
-  scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}},
-                  st);
-  k_alloc_bases<<<1, 256, 0, st>>>(c.d_pops, c.n_pop, c.pop_pair_base.p, c.work_off.p, c.flag_off.p, 1,
-                                   c.rank_slot_set.p, c.rank_id_set.p, c.per_pop_i.p, c.slot_base_set.p,
-                                   c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p);
-  note_launch();
-  k_apply_move<<<grid_for(W * 32, 256), 256, 0, st>>>(
-      c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p, c.win_set.p,
-      c.dec_set.p, c.rank_slot_set.p, c.slot_base_set.p, c.ice_set.p);
-  note_launch();
-  k_apply_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, Ed, c.ev_c.p, c.gp_c.p,
-                                                c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
-                                                c.slot_base_set.p, c.id_base_set.p, c.ice_set.p);
-  note_launch();
-  k_round_end<<<1, 32, 0, st>>>(c.round_dev.p, c.graph_stats.p, c.d_round, c.max_rounds, c.d_ctrs, c.n_pop, cond);
-  note_launch();
+  resolve_apply(c, st, W, Q);
 }
 
 // everything the captured launches depend on: sizes and device addresses
-std::vector<long long> redraw_key(const Ctx& c, const RedrawBounds& b) {
-  return {c.n_pop, b.kt, b.flat, b.n_gpairs, b.max_pairs, b.W, b.max_chunks, b.max_cells,
-          (long long)(b.inflate * 1e9f), c.max_rounds, c.sort_blocks, (long long)c.sort_smem,
+std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
+  return {c.n_pop, b.kt, b.flat, b.n_gpairs, b.W, c.max_rounds, c.mode, c.ch_chunks,
           (long long)c.d_pops, (long long)c.d_round, (long long)c.d_ctrs, (long long)c.round_dev.p,
           (long long)c.per_pop_i.p, (long long)c.pop_pair_base.p, (long long)c.gpair_pop.p,
-          (long long)c.gpair_local.p, (long long)c.nwork_set.p, (long long)c.nwork_pp.p, (long long)c.nprio.p,
-          (long long)c.pair_losers.p, (long long)c.work_off.p, (long long)c.pp_off.p, (long long)c.prio_off.p,
-          (long long)c.flag.p, (long long)c.flag_off.p, (long long)c.ev.p, (long long)c.ev_gp.p,
-          (long long)c.ev_w.p, (long long)c.ev_c.p, (long long)c.gp_c.p, (long long)c.need_slot_set.p,
-          (long long)c.need_id_set.p, (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p,
-          (long long)c.rank_id_set.p, (long long)c.slot_base_set.p, (long long)c.id_base_set.p,
-          (long long)c.slot_base_pp.p, (long long)c.id_base_pp.p, (long long)c.ice_set.p,
-          (long long)c.scan_status.p, (long long)c.scan_ctr.p, (long long)c.scan_err.p,
-          (long long)c.graph_stats.p, c.mode};
+          (long long)c.gpair_local.p, (long long)c.ev_key.p, (long long)c.ev_c.p, (long long)c.gp_c.p,
+          (long long)c.ev_pos.p, (long long)c.ev_dest.p, (long long)c.ev_len.p, (long long)c.ev_head.p,
+          (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.it_flag.p, (long long)c.it_key.p,
+          (long long)c.it_c.p, (long long)c.it_gp.p, (long long)c.it_pos.p, (long long)c.it_len.p,
+          (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_off.p, (long long)c.ch_y.p,
+          (long long)c.ch_q.p, (long long)c.ch_pos.p, (long long)c.need_slot_set.p, (long long)c.need_id_set.p,
+          (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p, (long long)c.rank_id_set.p,
+          (long long)c.slot_base_set.p, (long long)c.id_base_set.p, (long long)c.slot_base_pp.p,
+          (long long)c.id_base_pp.p, (long long)c.ice_set.p, (long long)c.scan_status.p, (long long)c.scan_ctr.p,
+          (long long)c.scan_err.p, (long long)c.graph_stats.p};
 }
 
 void free_redraw_graph(Ctx& c) {
@@ -1721,50 +1848,89 @@ void free_redraw_graph(Ctx& c) {
   c.rg_key.clear();
 }
 
-// Run the redraw rounds of this step as the graph (captured again when a
+// the item and event bound of the later rounds' graph for round-0 events
+// e0: a power of two, at least 4096, so that it holds from step to step
+long long graph_bound(long long e0) {
+  long long w = 4096;
+  while (w < e0) w *= 2;
+  return w;
+}
+
+// Event arrays, sized in round 0 for graph_bound(samples), which bounds the
+// events of every later round.  Some of them (key, slots, pair, position,
+// win, destination) carry a round's events into the next one (k_items reads
+// them), so nothing may reallocate them while a step runs.  The chain pool
+// gets one chunk per possible chain start and 4096 more for long chains.
+void reserve_events(Ctx& c, long long W) {
+  size_t w = (size_t)graph_bound(W);
+  c.ev_key.reserve(w + 1); c.ev_c.reserve(w + 1); c.gp_c.reserve(w + 1); c.ev_pos.reserve(w + 1);
+  c.ev_dest.reserve(w + 1); c.win_set.reserve(w + 1); c.dec_set.reserve(w + 1);
+  c.ev_len.reserve(w + 1); c.ev_head.reserve(w + 1); c.ev_app.reserve(w + 1); c.ev_done.reserve(w + 1);
+  c.need_slot_set.reserve(w + 1); c.need_id_set.reserve(w + 1); c.ice_set.reserve(w + 1);
+  c.rank_slot_set.reserve(w + 2); c.rank_id_set.reserve(w + 2);
+  size_t chunks = w + 4096;
+  c.ch_y.reserve(chunks * kChainChunk);
+  c.ch_q.reserve(chunks * kChainChunk);
+  c.ch_pos.reserve(chunks * kChainChunk);
+  c.ch_chunks = (long long)(std::min(std::min(c.ch_y.n, c.ch_q.n), c.ch_pos.n) / kChainChunk);
+}
+
+bool events_fit(const Ctx& c, long long W) {
+  size_t w = (size_t)W;
+  return c.ev_key.n >= w + 1 && c.ev_c.n >= w + 1 && c.gp_c.n >= w + 1 && c.ev_pos.n >= w + 1 &&
+         c.ev_dest.n >= w + 1 && c.win_set.n >= w + 1 && c.dec_set.n >= w + 1 && c.ev_len.n >= w + 1 &&
+         c.ev_head.n >= w + 1 && c.ev_app.n >= w + 1 && c.ev_done.n >= w + 1 && c.need_slot_set.n >= w + 1 &&
+         c.need_id_set.n >= w + 1 && c.ice_set.n >= w + 1 && c.rank_slot_set.n >= w + 2 &&
+         c.rank_id_set.n >= w + 2;
+}
+
+// the item buffers of a later round, sized for W items (they hold nothing
+// from one round to the next)
+void reserve_round(Ctx& c, long long W) {
+  size_t w = (size_t)std::max<long long>(W, 1);
+  c.it_flag.reserve(w + 1); c.it_key.reserve(w + 1); c.it_c.reserve(w + 1); c.it_gp.reserve(w + 1);
+  c.it_pos.reserve(w + 1); c.it_len.reserve(w + 1); c.it_head.reserve(w + 1); c.it_done.reserve(w + 1);
+  c.it_off.reserve(w + 2);
+}
+
+struct GraphRun {
+  long long rounds = -1;  // -1: the caller runs the rounds from the host loop
+  long long losers = 0, events = 0;
+  bool stopped_for_room = false;
+};
+
+// Run the later rounds of this step as the graph (captured again when a
 // bound or an address changed and the change held for two steps in a row).
-// losers0: round 0's per-set losers.  Returns the rounds run, or -1 if the
-// caller should run them from the host loop.
-long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pairs, long long losers0,
-                           float inflate, long long* redraws, long long* events) {
-  RedrawBounds b;
+// e0: the events of the round before.
+GraphRun run_round_graph(Ctx& c, int kt, bool flat, int n_gpairs, long long e0) {
+  GraphRun out;
+  RoundBounds b;
   b.kt = kt;
   b.flat = flat;
   b.n_gpairs = n_gpairs;
-  b.max_pairs = max_pairs;
-  // bounds rounded up so that the graph survives ordinary step-to-step changes
-  b.W = 4096;
-  while (b.W < losers0) b.W *= 2;
-  long long slots = 0;
-  for (int k = 0; k < c.n_pop; k++) slots = std::max<long long>(slots, c.n_slots_host[k]);
-  b.max_chunks = (int)((slots + b.W + kChunk - 1) / kChunk);
-  b.max_chunks = (b.max_chunks + 15) / 16 * 16;
-  b.max_cells = max_cells_of(c);
-  b.inflate = inflate;
-  // every buffer at its final size before the addresses are taken
-  prepare_chunks(c, (long long)b.max_chunks * kChunk - slots);
-  size_t w = (size_t)b.W;
-  c.flag.reserve(w + 1); c.ev.reserve(w + 1); c.flag_off.reserve(w + 2); c.ev_w.reserve(w + 1);
-  c.need_slot_set.reserve(w + 1); c.need_id_set.reserve(w + 1); c.win_set.reserve(w + 1);
-  c.dec_set.reserve(w + 1); c.ev_gp.reserve(w + 1); c.gp_c.reserve(w + 1); c.ev_c.reserve(w + 1);
-  c.ice_set.reserve(w + 1); c.rank_slot_set.reserve(w + 2); c.rank_id_set.reserve(w + 2);
+  // rounded up so that the graph survives ordinary step-to-step changes
+  b.W = graph_bound(e0);
+  // the event arrays hold the last round's events: they must already be
+  // large enough (reserve_events), never reallocated here
+  if (!events_fit(c, b.W)) return out;
+  // every other buffer at its final size before the addresses are taken
+  reserve_round(c, b.W);
   c.graph_stats.reserve(4);
   {
-    long long nb = std::max<long long>((b.W + kScanTile - 1) / kScanTile, (n_gpairs + kScanTile) / kScanTile);
+    long long nb = (b.W + kScanTile - 1) / kScanTile;
     c.scan_status.reserve((size_t)kScanMaxJobs * nb);
     if (c.scan_status.n > c.scan_status_n) {
       CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, c.stream));
       c.scan_status_n = c.scan_status.n;
     }
   }
-  size_sort(c, b.max_cells);
   if (c.dirty) push_pops(c);
-  std::vector<long long> key = redraw_key(c, b);
+  std::vector<long long> key = round_graph_key(c, b);
   if (key != c.rg_key && key != c.rg_seen) {
     // bounds or addresses new since the last step: capturing pays only when
-    // they hold, so this step's redraw rounds run from the host loop
+    // they hold, so this step's later rounds run from the host loop
     c.rg_seen = key;
-    return -1;
+    return out;
   }
   if (key != c.rg_key) {
     free_redraw_graph(c);
@@ -1784,7 +1950,12 @@ long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pair
     long long n0 = g_launches;
     CK(cudaStreamBeginCaptureToGraph(c.cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     try {
-      enqueue_redraw_round(c, c.cap_stream, b, cond);
+      k_round_begin<<<1, 128, 0, c.cap_stream>>>(c.d_round, c.round_dev.p, c.per_pop_i.p, 4 * c.n_pop);
+      note_launch();
+      enqueue_round_body(c, c.cap_stream, b, 0);
+      k_round_end<<<1, 32, 0, c.cap_stream>>>(c.round_dev.p, c.graph_stats.p, c.d_round, c.max_rounds, c.d_pops,
+                                              c.d_ctrs, c.n_pop, cond);
+      note_launch();
     } catch (...) {
       cudaGraph_t dummy;
       cudaStreamEndCapture(c.cap_stream, &dummy);
@@ -1816,10 +1987,23 @@ long long run_redraw_graph(Ctx& c, int kt, bool flat, int n_gpairs, int max_pair
     throw Fail(PMC_ERR_TIMEOUT);
   }
   g_launches += c.rg_nodes * st[2];
-  *redraws = st[0];
-  *events = st[1];
   c.claim_gen += (uint32_t)st[2];
-  return st[2];
+  out.rounds = st[2];
+  out.losers = st[0];
+  out.events = st[1];
+  out.stopped_for_room = st[3] != 0;
+  return out;
+}
+
+// capacity for a round that may add `slots` new slots to every population
+void ensure_room(Ctx& c, long long slots) {
+  for (int k = 0; k < c.n_pop; k++) {
+    long long need = (long long)c.n_slots_host[k] + slots;
+    if (need > c.pops[k].h.cap) {
+      int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
+      relayout(c, k, nc, false);  // slot numbers kept
+    }
+  }
 }
 
 void step_parallel(Ctx& c, int kt) {
@@ -1850,11 +2034,8 @@ void step_parallel(Ctx& c, int kt) {
   }
   c.nwork_set.reserve(ng);
   c.nwork_pp.reserve(ng);
-  c.nprio.reserve(ng);
   c.work_off.reserve(ng);
   c.pp_off.reserve(ng);
-  c.prio_off.reserve(ng);
-  c.pair_losers.reserve(ng);
   c.per_pop_i.reserve(4 * (size_t)c.n_pop);
   c.slot_base_set.reserve(c.n_pop);
   c.slot_base_pp.reserve(c.n_pop);
@@ -1871,214 +2052,143 @@ void step_parallel(Ctx& c, int kt) {
   bool flat = true;
   for (int k = 0; k < c.n_pop; k++) flat = flat && c.pops[k].h.flat;
   float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
-  long long redraws = 0, Qprev = 0, last_set_losers = 0;
-  bool any_pp = false;
   c.last_set_losers = c.last_pp_lost = c.last_events = c.last_ops = 0;
   std::vector<long long> hw(3 + 2 * (size_t)c.n_pop);
   std::vector<int> per_pop(4 * (size_t)c.n_pop);
-  int round = 0;
-  for (;;) {
-    bool claims_wrapped = false;
-    {
-      // every round gets a new claim generation; when the counter wraps,
-      // the claim words are cleared once
-      c.claim_gen++;
-      if (c.claim_gen >= 0xffffffffu - 4u * (uint32_t)c.max_rounds) {  // room for a graph's rounds
-        c.claim_gen = 0;
-        claims_wrapped = true;
-      }
-      uint32_t rg[2] = {(uint32_t)round, c.claim_gen};  // staged before the call returns
-      CK(cudaMemcpyAsync(c.d_round, rg, sizeof(rg), cudaMemcpyHostToDevice, c.stream));
+
+  // ---- round 0: every pair's samples and target operations
+  {
+    // a new claim generation for every round; they restart (with every
+    // claim and touched word cleared) before a step could run out of them
+    c.claim_gen++;
+    bool wrapped = false;
+    if (c.claim_gen + (uint32_t)c.max_rounds + 2u >= kGenLimit) {
+      c.claim_gen = 1;
+      wrapped = true;
     }
+    uint32_t rg[2] = {0u, c.claim_gen};  // staged before the call returns
+    CK(cudaMemcpyAsync(c.d_round, rg, sizeof(rg), cudaMemcpyHostToDevice, c.stream));
     if (c.dirty) push_pops(c);
-    if (round > 0) sort_pops(c, false);
-    if (round == 0) {
-      bool need_kmax = false, need_setup = false;
-      for (int k = 0; k < c.n_pop; k++) {
-        need_kmax = need_kmax || !c.pops[k].h.kmax_valid;
-        need_setup = need_setup || !c.pops[k].h.pair_setup_valid;
-      }
-      if (need_kmax) {
-        dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
-        k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
-        note_launch();
-      }
-      if (need_setup) {
-        dim3 g((unsigned)(((long long)max_pairs * 32 + 255) / 256), c.n_pop);
-        k_pair_setup<<<g, 256, 0, c.stream>>>(c.d_pops);
-        note_launch();
-      }
-    }
-    {
-      dim3 gp((max_pairs + 127) / 128, c.n_pop);
-      k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, c.nprio.p,
-                                        c.pair_losers.p, 1, inflate);
-      note_launch();
-    }
-    if (round == 0) {
-      // the device copies learn this with the next push
-      for (int k = 0; k < c.n_pop; k++) {
-        c.pops[k].h.kmax_valid = 1;
-        c.pops[k].h.pair_setup_valid = 1;
-      }
-      c.dirty = true;
-    }
-    scan_multi<long long>(c, {{c.nwork_set.p, n_gpairs, nullptr, c.work_off.p},
-                              {c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p},
-                              {c.nprio.p, n_gpairs, nullptr, c.prio_off.p}});
-    long long W, Q;
-    if (round == 0) {
-      long long* popw = c.n_dev.p + 4;
-      if (c.n_pop > 1) {
-        k_pop_work<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.pop_pair_base.p, c.n_pop, c.work_off.p,
-                                                                c.pp_off.p, popw);
-        note_launch();
-      }
-      // one read-back: totals and per-population work
-      CK(cudaMemcpyAsync(&hw[0], c.work_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaMemcpyAsync(&hw[1], c.pp_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaMemcpyAsync(&hw[2], c.prio_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-      if (c.n_pop > 1)
-        CK(cudaMemcpyAsync(&hw[3], popw, sizeof(long long) * 2 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
-      unsigned long long pair_scan_err = 0;
-      CK(cudaMemcpyAsync(&pair_scan_err, c.scan_err.p, sizeof(pair_scan_err), cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaStreamSynchronize(c.stream));
-      if (pair_scan_err) {
-        CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(pair_scan_err), c.stream));
-        throw Fail(PMC_ERR_TIMEOUT);
-      }
-      W = hw[0];
-      Q = hw[1];
-      if (c.n_pop == 1) {
-        hw[3] = W;
-        hw[4] = Q;
-      }
-      if (hw[2] + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
-    } else {
-      // later rounds redraw the losers of the previous round: their count
-      // bounds this round's samples, and every kernel reads the exact count
-      // from the device, so the round needs no read-back before its launches
-      W = last_set_losers;
-      Q = Qprev;
-      for (int k = 0; k < c.n_pop; k++) {
-        hw[3 + 2 * k] = W;
-        hw[3 + 2 * k + 1] = Q;
-      }
-    }
-    // capacity for the worst case of this round: every sample creates a
-    // particle and every target operation makes kMaxCopies - 1 copies
-    for (int k = 0; k < c.n_pop; k++) {
-      long long need = (long long)c.n_slots_host[k] + hw[3 + 2 * k] + (kMaxCopies - 1) * hw[3 + 2 * k + 1];
-      if (need > c.pops[k].h.cap) {
-        int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
-        relayout(c, k, nc, false);  // slot numbers kept
-      }
-    }
-    c.flag.reserve((size_t)W + 1);
-    c.ev.reserve((size_t)W + 1);
-    c.flag_off.reserve((size_t)W + 2);
-    c.ev_w.reserve((size_t)W + 1);
-    c.need_slot_set.reserve(W + 1);
-    c.need_id_set.reserve(W + 1);
-    c.win_set.reserve(W + 1);
-    c.dec_set.reserve(W + 1);
-    c.ev_gp.reserve(W + 1);
-    c.gp_c.reserve(W + 1);
-    c.ev_c.reserve(W + 1);
-    c.ice_set.reserve(W + 1);
-    c.rank_slot_set.reserve(W + 2);
-    c.rank_id_set.reserve(W + 2);
-    c.need_slot_pp.reserve(Q + 1);
-    c.need_id_pp.reserve(Q + 1);
-    c.win_pp.reserve(Q + 1);
-    c.lost_pp.reserve(Q + 1);
-    c.lost_off.reserve(Q + 2);
-    c.rank_slot_pp.reserve(Q + 2);
-    c.rank_id_pp.reserve(Q + 2);
-    if (claims_wrapped) {
+    if (wrapped) {
       dim3 g(grid_for(max_cap, 256), c.n_pop);
       k_fill_claims<<<g, 256, 0, c.stream>>>(c.d_pops);
       note_launch();
     }
-    CK(cudaMemsetAsync(c.pair_losers.p, 0, sizeof(int) * ng, c.stream));
-    CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 4, c.stream));
-    CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
-    if (W > 0) {
-      ProfScope ps(c, 0, W);
-      launch_test_kt(c, kt, flat, n_gpairs, W, c.stream);
-    }
-    if (Q > 0) {
-      if (round == 0) {
-        c.op_pop.reserve(Q); c.op_pair.reserve(Q); c.op_slot.reserve(Q); c.op_k.reserve(Q); c.op_prio.reserve(Q);
-        k_build_ops<<<n_gpairs, 128, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pp_off.p,
-                                                    c.prio_off.p, n_gpairs, c.op_pop.p, c.op_pair.p,
-                                                    c.op_slot.p, c.op_k.p, c.op_prio.p);
-        note_launch();
-      }
-      c.pp_res.reserve(Q);
-      c.pp_vol.reserve((size_t)Q * c.n_spec);
-      set_n_dev(c, Q);
-      launch_pp(c, kt, Q);
-    }
-    // accepted per-set samples in sample order; the sample count is
-    // work_off[n_gpairs] and the event count E goes to round_dev[1], both on
-    // the device
-    const long long* Wd = c.work_off.p + n_gpairs;
-    long long* Ed = c.round_dev.p + 1;
-    if (W > 0) {
-      scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, Ed}});
-      k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, Wd, c.ev_w.p, c.ev.p,
-                                                             c.ev_gp.p, c.ev_c.p, c.gp_c.p);
-      note_launch();
-      k_resolve_set<<<grid_for(W, 256), 256, 0, c.stream>>>(
-          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, c.prio_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p,
-          c.pair_losers.p, c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p, c.round_dev.p);
-      note_launch();
-      scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}});
-    }
-    if (Q > 0) {
-      set_n_dev(c, Q);
-      k_pp_resolve<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_prio.p, c.n_dev.p, c.pp_res.p,
-                                                           c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
-      note_launch();
-      scan_multi<int>(c, {{c.need_slot_pp.p, Q, nullptr, c.rank_slot_pp.p},
-                          {c.need_id_pp.p, Q, nullptr, c.rank_id_pp.p}});
-      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p,
-                                                             c.per_pop_i.p + 2 * c.n_pop);
-      note_launch();
-      k_count_per_pop<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.need_id_pp.p, c.n_dev.p, c.op_pop.p,
-                                                             c.per_pop_i.p + 3 * c.n_pop);
-      note_launch();
-    }
-    k_alloc_bases<<<1, 256, 0, c.stream>>>(c.d_pops, c.n_pop, c.pop_pair_base.p, c.work_off.p, c.flag_off.p,
-                                           W > 0 ? 1 : 0, c.rank_slot_set.p, c.rank_id_set.p, c.per_pop_i.p,
-                                           c.slot_base_set.p, c.id_base_set.p, c.slot_base_pp.p, c.id_base_pp.p);
+  }
+  bool need_kmax = false, need_setup = false;
+  for (int k = 0; k < c.n_pop; k++) {
+    need_kmax = need_kmax || !c.pops[k].h.kmax_valid;
+    need_setup = need_setup || !c.pops[k].h.pair_setup_valid;
+  }
+  if (need_kmax) {
+    dim3 g((nb_max * nb_max + 255) / 256, c.n_pop);
+    k_kmax_table<<<g, 256, 0, c.stream>>>(c.d_pops);
     note_launch();
-    if (W > 0) {
-      // part 1, one warp per event: species and components
-      k_apply_move<<<grid_for(W * 32, 256), 256, 0, c.stream>>>(
-          c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, Ed, c.ev_w.p, c.ev_c.p, c.gp_c.p, c.win_set.p,
-          c.dec_set.p, c.rank_slot_set.p, c.slot_base_set.p, c.ice_set.p);
-      note_launch();
-      // part 2, one thread per event: removals, scalar fields, caches
-      k_apply_set<<<grid_for(W, 256), 256, 0, c.stream>>>(
-          c.d_pops, c.gpair_pop.p, c.gpair_local.p, Ed, c.ev_c.p, c.gp_c.p, c.win_set.p, c.dec_set.p,
-          c.rank_slot_set.p, c.rank_id_set.p, c.slot_base_set.p, c.id_base_set.p, c.ice_set.p);
+  }
+  if (need_setup) {
+    dim3 g((unsigned)(((long long)max_pairs * 32 + 255) / 256), c.n_pop);
+    k_pair_setup<<<g, 256, 0, c.stream>>>(c.d_pops);
+    note_launch();
+  }
+  {
+    dim3 gp((max_pairs + 127) / 128, c.n_pop);
+    k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, 1, inflate);
+    note_launch();
+  }
+  // the device copies learn this with the next push
+  for (int k = 0; k < c.n_pop; k++) {
+    c.pops[k].h.kmax_valid = 1;
+    c.pops[k].h.pair_setup_valid = 1;
+  }
+  c.dirty = true;
+  scan_multi<long long>(c, {{c.nwork_set.p, n_gpairs, nullptr, c.work_off.p},
+                            {c.nwork_pp.p, n_gpairs, nullptr, c.pp_off.p}});
+  long long W, Q;
+  {
+    long long* popw = c.n_dev.p + 4;
+    if (c.n_pop > 1) {
+      k_pop_work<<<(c.n_pop + 127) / 128, 128, 0, c.stream>>>(c.pop_pair_base.p, c.n_pop, c.work_off.p, c.pp_off.p,
+                                                              popw);
       note_launch();
     }
-    if (Q > 0) {
-      k_pp_apply<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
-                                                         c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p,
-                                                         c.slot_base_pp.p, c.id_base_pp.p);
-      note_launch();
-      scan_dev(c, c.lost_pp.p, Q, nullptr, c.lost_off.p);
+    // one read-back: totals and per-population work
+    CK(cudaMemcpyAsync(&hw[0], c.work_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&hw[1], c.pp_off.p + n_gpairs, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    if (c.n_pop > 1)
+      CK(cudaMemcpyAsync(&hw[3], popw, sizeof(long long) * 2 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
+    unsigned long long pair_scan_err = 0;
+    CK(cudaMemcpyAsync(&pair_scan_err, c.scan_err.p, sizeof(pair_scan_err), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (pair_scan_err) {
+      CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(pair_scan_err), c.stream));
+      throw Fail(PMC_ERR_TIMEOUT);
     }
-    // one read-back at the end of the round
-    long long set_losers = 0, pp_lost = 0, E = 0;
-    CK(cudaMemcpyAsync(&set_losers, c.round_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-    if (W > 0) CK(cudaMemcpyAsync(&E, Ed, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-    last_set_losers = set_losers;
-    if (Q > 0) CK(cudaMemcpyAsync(&pp_lost, c.lost_off.p + Q, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    W = hw[0];
+    Q = hw[1];
+    if (c.n_pop == 1) {
+      hw[3] = W;
+      hw[4] = Q;
+    }
+    // sample numbers fit in a key's 31 bits below the walk flag of the merge stream
+    if (W + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
+  }
+  // capacity for the worst case of this round: every sample creates a
+  // particle and every target operation makes kMaxCopies - 1 copies
+  for (int k = 0; k < c.n_pop; k++) {
+    long long need = (long long)c.n_slots_host[k] + hw[3 + 2 * k] + (kMaxCopies - 1) * hw[3 + 2 * k + 1];
+    if (need > c.pops[k].h.cap) {
+      int nc = (int)std::min<long long>(std::max<long long>(need * 3 / 2, 1024), (1LL << 31) - 1);
+      relayout(c, k, nc, false);  // slot numbers kept
+    }
+  }
+  {
+    size_t w = (size_t)W;
+    c.flag.reserve(w + 1); c.ev.reserve(w + 1); c.flag_off.reserve(w + 2); c.ev_gp.reserve(w + 1);
+    reserve_events(c, W);
+    c.need_slot_pp.reserve(Q + 1); c.need_id_pp.reserve(Q + 1); c.win_pp.reserve(Q + 1); c.lost_pp.reserve(Q + 1);
+    c.lost_off.reserve(Q + 2); c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
+  }
+  if (c.dirty) push_pops(c);
+  CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 4, c.stream));
+  CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
+  if (W > 0) {
+    ProfScope ps(c, 0, W);
+    launch_test_kt(c, kt, flat, n_gpairs, W, c.stream);
+  }
+  if (Q > 0) {
+    c.op_pop.reserve(Q); c.op_pair.reserve(Q); c.op_slot.reserve(Q); c.op_k.reserve(Q); c.op_key.reserve(Q);
+    k_build_ops<<<n_gpairs, 128, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pp_off.p, n_gpairs,
+                                                c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.op_key.p);
+    note_launch();
+    c.pp_res.reserve(Q);
+    c.pp_vol.reserve((size_t)Q * c.n_spec);
+    set_n_dev(c, Q);
+    launch_pp(c, kt, Q);
+  }
+  // accepted samples in sample order; the sample count is work_off[n_gpairs]
+  // and the event count E goes to round_dev[1], both on the device
+  if (W > 0) {
+    const long long* Wd = c.work_off.p + n_gpairs;
+    scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, c.round_dev.p + 1}});
+    k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, Wd, c.ev.p, c.ev_gp.p,
+                                                           c.gpair_local.p, c.work_off.p, c.ev_key.p, c.ev_c.p,
+                                                           c.gp_c.p, c.ev_pos.p, c.ev_len.p);
+    note_launch();
+  }
+  resolve_apply(c, c.stream, W, Q);
+
+  // ---- later rounds: retries, walks and per-particle redo operations
+  long long redraws = 0, E = 0, pp_lost = 0;
+  int round = 0;
+  bool graph_tried = false;
+  for (;;) {
+    // one read-back at the end of each host round
+    long long losers = 0;
+    CK(cudaMemcpyAsync(&losers, c.round_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&E, c.round_dev.p + 1, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    long long Qr = round == 0 ? Q : pp_lost;
+    pp_lost = 0;
+    if (Qr > 0) CK(cudaMemcpyAsync(&pp_lost, c.lost_off.p + Qr, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
     unsigned long long scan_err = 0;
     CK(cudaMemcpyAsync(&scan_err, c.scan_err.p, sizeof(scan_err), cudaMemcpyDeviceToHost, c.stream));
@@ -2088,26 +2198,13 @@ void step_parallel(Ctx& c, int kt) {
       throw Fail(PMC_ERR_TIMEOUT);
     }
     for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] += per_pop[0 * c.n_pop + k] + per_pop[2 * c.n_pop + k];
-    redraws += set_losers + pp_lost;
-    c.last_set_losers += set_losers;
+    redraws += losers + pp_lost;
+    c.last_set_losers += losers;
     c.last_pp_lost += pp_lost;
     c.last_events += E;
-    c.last_ops += Q;
-    if (Q > 0) any_pp = true;
+    c.last_ops += Qr;
     round++;
-    if (set_losers + pp_lost == 0) break;
-    if (round == 1 && c.use_graph && !any_pp && pp_lost == 0 && round < c.max_rounds) {
-      // the redraw rounds, device-driven
-      long long g_redraws = 0, g_events = 0;
-      long long n = run_redraw_graph(c, kt, flat, n_gpairs, max_pairs, set_losers, inflate, &g_redraws, &g_events);
-      if (n >= 0) {
-        redraws += g_redraws;
-        c.last_set_losers += g_redraws;
-        c.last_events += g_events;
-        round += (int)n;
-        break;
-      }
-    }
+    if (E == 0 && pp_lost == 0) break;
     if (round >= c.max_rounds) {
       std::vector<PopCtr>& r = read_ctrs(c);
       for (int k = 0; k < c.n_pop; k++)
@@ -2115,17 +2212,59 @@ void step_parallel(Ctx& c, int kt) {
       write_ctrs(c);
       break;
     }
-    if (pp_lost > 0) {
-      c.r_pop.reserve(pp_lost); c.r_pair.reserve(pp_lost); c.r_slot.reserve(pp_lost); c.r_k.reserve(pp_lost);
-      c.r_prio.reserve(pp_lost);
-      k_build_redo<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p, c.lost_pp.p,
-                                                           c.lost_off.p, Q, c.r_pop.p, c.r_pair.p, c.r_slot.p, c.r_k.p,
-                                                           c.r_prio.p, 0x40000000u);
+    // room for this round's new slots: at most one per item, and
+    // kMaxCopies - 1 per target operation
+    ensure_room(c, E + (kMaxCopies - 1) * pp_lost);
+    if (!graph_tried && c.use_graph && pp_lost == 0) {
+      graph_tried = true;
+      GraphRun g = run_round_graph(c, kt, flat, n_gpairs, E);
+      if (g.rounds >= 0) {
+        redraws += g.losers;
+        c.last_set_losers += g.losers;
+        c.last_events += g.events;
+        round += (int)g.rounds;
+        if (!g.stopped_for_room) break;
+        // out of room inside the graph: the host loop grows the slot arrays
+        // and carries on from the device's counts
+        std::vector<PopCtr>& r = read_ctrs(c);
+        for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] = r[k].n_slots;
+        CK(cudaMemcpyAsync(&E, c.round_dev.p + 1, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        if (round >= c.max_rounds) {
+          for (int k = 0; k < c.n_pop; k++)
+            if (r[k].status == 0) r[k].status = PMC_ERR_TIMEOUT;
+          write_ctrs(c);
+          break;
+        }
+        ensure_room(c, E);
+      }
+    }
+    // one host-driven round
+    reserve_round(c, E);
+    long long Qn = pp_lost;
+    if (Qn > 0) {
+      c.r_pop.reserve(Qn); c.r_pair.reserve(Qn); c.r_slot.reserve(Qn); c.r_k.reserve(Qn); c.r_key.reserve(Qn);
+      k_build_redo<<<grid_for(Qr, 256), 256, 0, c.stream>>>(c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
+                                                            c.op_key.p, c.lost_pp.p, c.lost_off.p, Qr, c.r_pop.p,
+                                                            c.r_pair.p, c.r_slot.p, c.r_k.p, c.r_key.p);
       note_launch();
       std::swap(c.op_pop, c.r_pop); std::swap(c.op_pair, c.r_pair); std::swap(c.op_slot, c.r_slot);
-      std::swap(c.op_k, c.r_k); std::swap(c.op_prio, c.r_prio);
+      std::swap(c.op_k, c.r_k); std::swap(c.op_key, c.r_key);
+      c.pp_res.reserve(Qn);
+      c.pp_vol.reserve((size_t)Qn * c.n_spec);
+      c.need_slot_pp.reserve(Qn + 1); c.need_id_pp.reserve(Qn + 1); c.win_pp.reserve(Qn + 1);
+      c.lost_pp.reserve(Qn + 1); c.lost_off.reserve(Qn + 2); c.rank_slot_pp.reserve(Qn + 2);
+      c.rank_id_pp.reserve(Qn + 2);
+      // target operations sample their sources from the current cells
+      sort_pops(c, false);
     }
-    Qprev = pp_lost;
+    if (c.dirty) push_pops(c);
+    RoundBounds b{kt, flat, n_gpairs, E};
+    k_round_begin<<<1, 128, 0, c.stream>>>(c.d_round, c.round_dev.p, c.per_pop_i.p, 4 * c.n_pop);
+    note_launch();
+    c.claim_gen++;  // as k_round_begin on the device
+    enqueue_round_body(c, c.stream, b, Qn);
+    pp_lost = Qn;  // read back as this round's operations at the top of the loop
   }
   c.last_redraws = redraws;
   c.last_rounds = round;
@@ -2251,16 +2390,25 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   cudaFree(c.d_pops);
   cudaFree(c.d_ctrs);
   cudaFree(c.d_round);
-  DevBuf<int>* bi[] = {&c.gpair_pop, &c.gpair_local, &c.pair_losers, &c.need_slot_set, &c.need_id_set,
-                       &c.need_slot_pp, &c.need_id_pp, &c.lost_pp, &c.op_pop, &c.op_pair, &c.op_slot,
-                       &c.op_k, &c.r_pop, &c.r_pair, &c.r_slot, &c.r_k, &c.per_pop_i,
-                       &c.slot_base_set, &c.slot_base_pp};
+  DevBuf<int>* bi[] = {&c.gpair_pop, &c.gpair_local, &c.need_slot_set, &c.need_id_set, &c.need_slot_pp,
+                       &c.need_id_pp, &c.lost_pp, &c.op_pop, &c.op_pair, &c.op_slot, &c.op_k, &c.r_pop,
+                       &c.r_pair, &c.r_slot, &c.r_k, &c.per_pop_i, &c.slot_base_set, &c.slot_base_pp,
+                       &c.ev_dest, &c.ev_len, &c.ev_head, &c.ev_app, &c.it_gp, &c.it_len, &c.it_head,
+                       &c.ch_y, &c.ch_q};
   for (auto* b : bi) b->release();
-  DevBuf<long long>* bl[] = {&c.pop_pair_base, &c.nwork_set, &c.nwork_pp, &c.nprio, &c.work_off, &c.pp_off,
-                             &c.prio_off, &c.flag_off, &c.ev_w, &c.rank_slot_set, &c.rank_id_set,
-                             &c.rank_slot_pp, &c.rank_id_pp, &c.lost_off, &c.id_base_set, &c.id_base_pp,
-                             &c.n_dev};
+  DevBuf<long long>* bl[] = {&c.pop_pair_base, &c.nwork_set, &c.nwork_pp, &c.work_off, &c.pp_off, &c.flag_off,
+                             &c.rank_slot_set, &c.rank_id_set, &c.rank_slot_pp, &c.rank_id_pp, &c.lost_off,
+                             &c.id_base_set, &c.id_base_pp, &c.n_dev, &c.it_off};
   for (auto* b : bl) b->release();
+  DevBuf<unsigned long long>* bk[] = {&c.ev_key, &c.it_key, &c.op_key, &c.r_key};
+  for (auto* b : bk) b->release();
+  c.ev_pos.release();
+  c.it_pos.release();
+  c.ch_pos.release();
+  c.it_flag.release();
+  c.it_done.release();
+  c.ev_done.release();
+  c.it_c.release();
   c.flag.release();
   c.win_set.release();
   c.dec_set.release();
@@ -2273,8 +2421,6 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.scan_err.release();
   c.win_pp.release();
   c.ev.release();
-  c.op_prio.release();
-  c.r_prio.release();
   c.pp_res.release();
   c.pp_vol.release();
   c.replay_u.release();

@@ -16,10 +16,19 @@
 //             an accepted sample claims both particles with atomicMin of its
 //             priority (its position in the reference's loop order);
 //   resolve   an accepted sample that holds both claims is applied
-//             (coagulate / coagulate_weighting, coagulation.F90:810-985);
-//             one that lost a claim is redrawn in the next round.
-// Later rounds re-sort and redraw only the lost samples, so a particle can
-// take part in several coagulations per step, as in the sequential loop.
+//             (coagulate / coagulate_weighting, coagulation.F90:810-985).
+// Later rounds (k_items, one thread per event of the round before) carry on
+// the sequential loop's order:
+//   - an event that lost a claim is retried unchanged if neither of its
+//     particles was consumed, and dropped if one was: in the sequential loop
+//     a test never meets a particle that an earlier event removed, so the
+//     step-start samples that would have are thinned away;
+//   - a particle that an event created or changed walks the pairs after the
+//     event's pair that contain its cell, with Poisson tests against members
+//     of the other cell at rate k_max * del_t per member, as the later pairs'
+//     samples of the sequential loop would test it; its accepted tests are
+//     the next events (a chain of them when each absorbs the partner).
+// The step ends when a round has no events.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -42,6 +51,8 @@ enum Stream : uint32_t {
   kStreamMerge = 3,
   kStreamPart = 4,
   kStreamHalve = 5,  // aero_state_halve draws, keyed by the rebalance call and the slot
+  kStreamWalk = 6,   // a walk's tests, keyed by the round and the walking slot
+  kStreamChain = 7,  // merge of a chain's event i >= 2, keyed by i, the round and the walking slot
 };
 
 __device__ __forceinline__ void set_status(PopCtr* c, int code) { atomicCAS(&c->status, 0, code); }
@@ -104,36 +115,39 @@ __device__ int block_excl_scan(int v, int* total) {
   return pre;
 }
 
-// pair-test record of slot i (see RecD)
-__device__ __forceinline__ RecD make_rec(const PopDev& P, int i) {
+// pair-test record of a particle of radius r, total volume v, mass m and
+// class cls (1-based) (see RecD)
+__device__ __forceinline__ RecD make_rec_v(const PopDev& P, double r, double v, double m, int cls) {
   RecD q;
-  double r = P.rad[i];
   q.r = r;
   q.rv = rad2vol(r);
-  q.nc = num_conc_at_radius<double>(P.w, P.cls[i] - 1, r);
+  q.nc = num_conc_at_radius<double>(P.w, cls - 1, r);
   q.a = q.b = q.c = 0.0;
   switch (P.kernel_type) {
-    case kKernelAdditive: q.a = P.vtot[i]; break;
+    case kKernelAdditive: q.a = v; break;
     case kKernelBrown: {
-      double v = P.vtot[i];
-      BrownPart bp = brown_part(P.benv, v, P.mass[i] / v);
+      BrownPart bp = brown_part(P.benv, v, m / v);
       q.a = bp.diffus;
       q.b = bp.speedsq;
       q.c = bp.deltasq;
       break;
     }
-    case kKernelSedi: q.a = fall_g(vol2rad(P.vtot[i])); break;
+    case kKernelSedi: q.a = fall_g(vol2rad(v)); break;
     case kKernelBrownFree: {
-      double v = P.vtot[i];
       q.a = v;
-      q.b = P.mass[i] / v;
+      q.b = m / v;
       q.c = pow(num_of_monomers(P.benv, v), 1.0 / P.benv.frac_dim);
       break;
     }
-    case kKernelBrownCont: q.a = pow(num_of_monomers(P.benv, P.vtot[i]), 1.0 / P.benv.frac_dim); break;
+    case kKernelBrownCont: q.a = pow(num_of_monomers(P.benv, v), 1.0 / P.benv.frac_dim); break;
     default: break;
   }
   return q;
+}
+
+// pair-test record of slot i
+__device__ __forceinline__ RecD make_rec(const PopDev& P, int i) {
+  return make_rec_v(P, P.rad[i], P.vtot[i], P.mass[i], P.cls[i]);
 }
 
 __device__ __forceinline__ RecF to_f32(const RecD& q) {
@@ -425,10 +439,10 @@ __global__ void k_pair_setup(const PopDev* pops) {
 // pair set-up for round 0: mc_coag_for_bin, try_per_particle_coag's
 // eligibility tests and compute_n_samp (coagulation.F90:101-241, 648-702).
 // nwork_set[gp] = samples of a per-set pair; nwork_pp[gp] = targets of a
-// per-particle pair; nprio[gp] = both (priority space in loop order).
+// per-particle pair.  k_max is set for every pair, empty ones included:
+// walks test particles that arrive in a pair's cells during the step.
 __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long long* nwork_set,
-                        long long* nwork_pp, long long* nprio, const int* pair_losers,
-                        int use_particle_path, float kmax_inflate) {
+                        long long* nwork_pp, int use_particle_path, float kmax_inflate) {
   const PopDev& P = pops[blockIdx.y];
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n_pairs) return;
@@ -448,24 +462,15 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
     S.n1 = S.n2 = n1 = n2 = 0;
   }
   bool same = (b1 == b2) && (c1 == c2);
-  if (*P.round_p > 0) {
-    // redraws of lost samples; a per-particle pair is not redone
-    long long nl = S.path == kPathSet ? pair_losers[gp] : 0;
-    if ((same && n1 < 2) || n1 < 1 || n2 < 1) nl = 0;
-    nwork_set[gp] = nl;
-    nwork_pp[gp] = 0;
-    nprio[gp] = nl;
-    return;
-  }
-  if (n1 == 0 || n2 == 0) {
-    S.path = kPathSkip;
-    nwork_set[gp] = nwork_pp[gp] = nprio[gp] = 0;
-    return;
-  }
   double k_max = P.kmax_tab[b1 + nb * b2] * S.f_max;
   if (kmax_inflate != 0.f) k_max = k_max * (1.0 + (double)kmax_inflate);
   S.k_max = k_max;
   S.inv_k_max = 1.0 / k_max;
+  if (n1 == 0 || n2 == 0) {
+    S.path = kPathSkip;
+    nwork_set[gp] = nwork_pp[gp] = 0;
+    return;
+  }
   // try_per_particle_coag eligibility (coagulation.F90:191-217): the weight
   // conditions were settled by k_pair_setup; the cell-count ones are here
   if (use_particle_path && P.mono_dec && S.pp_ok) {
@@ -478,7 +483,6 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
       int nt = P.cell_count[S.bt + nb * S.ct];
       nwork_set[gp] = 0;
       nwork_pp[gp] = nt;
-      nprio[gp] = nt;
       return;
     }
   }
@@ -496,7 +500,6 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
   if ((same && n1 < 2) || n1 < 1 || n2 < 1) ns = 0;
   nwork_set[gp] = ns;
   nwork_pp[gp] = 0;
-  nprio[gp] = ns;
 }
 
 // ---------------------------------------------------------------------------
@@ -554,9 +557,8 @@ __device__ __forceinline__ int find_pair(const long long* off, int n, long long 
 template <int KT, class T, bool FLAT>
 __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpair_pop,
                                               const int* gpair_local, const long long* work_off,
-                                              const long long* prio_off, int n_gpairs,
-                                              const long long* total, uint8_t* flag, int2* ev,
-                                              int* ev_gp) {
+                                              int n_gpairs, const long long* total, uint8_t* flag,
+                                              int2* ev, int* ev_gp) {
   long long W = *total;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < W;
        w += (long long)gridDim.x * blockDim.x) {
@@ -611,9 +613,9 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
     bool acc = (T)u53(rnd.z, rnd.w) < prob;
     flag[w] = acc ? 1 : 0;
     if (acc) {
-      unsigned prio = (unsigned)(prio_off[gp] + s);
-      atomicMin(&P.claim[s1], claim_key(P, prio));
-      atomicMin(&P.claim[s2], claim_key(P, prio));
+      unsigned long long key = make_key((uint32_t)p, 0u, (uint32_t)s);
+      atomicMin(&P.claim[s1], claim_key(P, key));
+      atomicMin(&P.claim[s2], claim_key(P, key));
       ev[w] = make_int2(s1, s2);
       ev_gp[w] = gp;
     }

@@ -5,14 +5,65 @@
 // coag_target_with_source (coagulation.F90:333-582), one thread per target.
 // Every write to a particle slot is guarded by the slot's claim word: an
 // event or target operation is applied only if it holds the lowest priority
-// on every slot it writes or removes; otherwise it is redone in the next
-// round against the re-sorted state.
+// on every slot it writes or removes; otherwise it is retried (or dropped,
+// k_items) in the next round.
 #pragma once
 
 #include "pmc_kernels.cuh"
 #include "pmc_particle.cuh"
 
 namespace pmc {
+
+// Chains (see the walks below): the events of one walk that absorbs its
+// partners one after another, in chunks of kChainChunk entries; entry
+// kChainChunk - 1 of a chunk's y holds the index of the next chunk (-1: none)
+constexpr int kChainChunk = 32;
+constexpr int kChainMaxLen = 1 << 16;  // events of one chain in one round
+
+struct ChainPool {
+  int* y;          // [n_chunks * kChainChunk] partner slot; the last entry of a chunk links the next chunk
+  int* q;          // pair (local)
+  float* pos;      // position in the pair's test sequence
+  long long* ctr;  // chunks handed out in this round (device)
+  long long n_chunks;
+};
+
+struct ChainWriter {
+  int head = -1, chunk = -1, fill = 0, len = 0;
+  __device__ bool append(const ChainPool& C, int y, int q, float pos) {
+    if (chunk < 0 || fill == kChainChunk - 1) {
+      long long nc = (long long)atomicAdd((unsigned long long*)C.ctr, 1ULL);
+      if (nc >= C.n_chunks) return false;
+      if (chunk >= 0) C.y[(size_t)chunk * kChainChunk + kChainChunk - 1] = (int)nc;
+      else head = (int)nc;
+      chunk = (int)nc;
+      fill = 0;
+      C.y[(size_t)chunk * kChainChunk + kChainChunk - 1] = -1;
+    }
+    size_t i = (size_t)chunk * kChainChunk + fill;
+    C.y[i] = y;
+    C.q[i] = q;
+    C.pos[i] = pos;
+    fill++;
+    len++;
+    return true;
+  }
+};
+
+struct ChainReader {
+  int chunk, k = 0;
+  __device__ explicit ChainReader(int head) : chunk(head) {}
+  // index of the next entry, -1 past the end of the links
+  __device__ long long next(const ChainPool& C) {
+    if (chunk < 0 || (long long)chunk >= C.n_chunks) return -1;
+    size_t i = (size_t)chunk * kChainChunk + k;
+    if (++k == kChainChunk - 1) {
+      chunk = C.y[(size_t)chunk * kChainChunk + kChainChunk - 1];
+      k = 0;
+    }
+    return (long long)i;
+  }
+};
 
 __device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
   P.alive[i] = 0;
@@ -26,10 +77,12 @@ struct MergeDecision {
   int new_group;  // 1-based
 };
 
+// particle 1 (radius r1, total volume vt1) from the pair's first cell,
+// particle 2 from its second
 template <class R>
-__device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int c1, int c2, int cc) {
+__device__ MergeDecision merge_decide_v(const PopDev& P, R& g, double r1, double vt1, double r2, double vt2, int c1,
+                                        int c2, int cc) {
   MergeDecision d;
-  double r1 = P.rad[s1], r2 = P.rad[s2];
   double rc = vol2rad(rad2vol(r1) + rad2vol(r2));
   double nc1 = num_conc_at_radius<double>(P.w, c1, r1);
   double nc2 = num_conc_at_radius<double>(P.w, c2, r2);
@@ -44,7 +97,7 @@ __device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int
   if (d.create) {
     d.lost1 = d.lost2 = false;
     if (d.rm1 && d.rm2) {
-      if (P.vtot[s1] > P.vtot[s2]) d.lost2 = true;
+      if (vt1 > vt2) d.lost2 = true;
       else d.lost1 = true;
     }
   } else {
@@ -52,6 +105,11 @@ __device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int
     d.lost2 = d.rm2;
   }
   return d;
+}
+
+template <class R>
+__device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int c1, int c2, int cc) {
+  return merge_decide_v(P, g, P.rad[s1], P.vtot[s1], P.rad[s2], P.vtot[s2], c1, c2, cc);
 }
 
 // A merge decision and the number of uniforms its stream had used, in one
@@ -73,44 +131,66 @@ __device__ __forceinline__ MergeDecision unpack_decision(uint32_t x, uint32_t* u
   return m;
 }
 
-// Resolve accepted per-set samples: winner test, slot/id needs.  Event e
-// has sample index ev_w[e], slots ev[e] and global pair ev_gp[e] (in sample
-// order, compacted from the pair tests).
-__global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
-                              const long long* work_off, const long long* prio_off,
-                              const long long* n_events, const long long* ev_w, const int2* ev,
-                              const int* ev_gp, int* pair_losers, int* need_slot, int* need_id,
-                              uint8_t* win, uint32_t* dec, long long* n_losers) {
+// random stream of an event's merge: the pair and the sample for the pair's
+// own samples, the pair and the walking slot for a walk's test
+__device__ __forceinline__ Rng merge_rng(const PopDev& P, unsigned long long key) {
+  uint32_t idx = key_idx(key);
+  if (key_kind(key)) idx |= 0x80000000u;
+  return make_rng(P, kStreamMerge, key_pair(key), idx);
+}
+
+// Resolve the events of a round: winner test, slot/id needs.  Event e has
+// key ev_key[e], slots ev[e] and global pair ev_gp[e]; the events are
+// ordered by population.  A winning chain (ev_len[e] > 0) gets win 2 and the
+// number of its events whose claims hold (ev_app[e]).
+__global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const long long* n_events,
+                              const unsigned long long* ev_key, const int2* ev, const int* ev_gp, int* need_slot,
+                              int* need_id, uint8_t* win, uint32_t* dec, long long* n_losers, const int* ev_len,
+                              const int* ev_head, int* ev_app, ChainPool pool) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
-    long long w = ev_w[e];
     int gp = ev_gp[e];
     const PopDev& P = pops[gpair_pop[gp]];
-    int p = gpair_local[gp];
-    long long s = w - work_off[gp];
-    unsigned prio = (unsigned)(prio_off[gp] + s);
+    unsigned long long key = ev_key[e];
+    int p = (int)key_pair(key);
     int2 sl = ev[e];
-    if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
-      bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
-      win[e] = 0;
-      need_slot[e] = 0;
-      need_id[e] = 0;
-      continue;
-    }
-    unsigned long long key = claim_key(P, prio);
-    bool winner = P.claim[sl.x] == key && P.claim[sl.y] == key;
-    win[e] = winner ? 1 : 0;
+    win[e] = 0;
     need_slot[e] = 0;
     need_id[e] = 0;
+    if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap || p >= P.n_pairs) {
+      bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+      continue;
+    }
+    unsigned long long ck = claim_key(P, key);
+    bool winner = P.claim[sl.x] == ck && P.claim[sl.y] == ck;
     if (!winner) {
-      atomicAdd(&pair_losers[gp], 1);
       add_ll(n_losers, 1);
       continue;
     }
+    int len = ev_len[e];
+    if (len > 0) {
+      // a chain: its events apply as far as each partner's claim holds (the
+      // walking particle's is the first event's)
+      ChainReader rd(ev_head[e]);
+      uint32_t x = key_idx(key);
+      int app = 0;
+      for (int i = 0; i < len; i++) {
+        long long ix = rd.next(pool);
+        if (ix < 0) break;
+        int y = pool.y[ix], q = pool.q[ix];
+        if (y < 0 || y >= P.cap || q < 0 || q >= P.n_pairs) break;
+        if (P.claim[y] != claim_key(P, make_key((uint32_t)q, 1u, x))) break;
+        app++;
+      }
+      ev_app[e] = app;
+      win[e] = 2;
+      continue;
+    }
+    win[e] = 1;
     PairDesc d = P.pair_desc[p];
     const PairState& S = P.pair[p];
-    Rng g = make_rng(P, kStreamMerge, (uint32_t)p, (uint32_t)s);
+    Rng g = merge_rng(P, key);
     MergeDecision m = merge_decide(P, g, sl.x, sl.y, d.c1, d.c2, S.cc);
     if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
     dec[e] = pack_decision(m, g.used());
@@ -140,8 +220,7 @@ __device__ __forceinline__ int event_dest(const MergeDecision& m, int s1, int s2
 // volumes of the sources, which part 2 needs after the destination may have
 // been overwritten, go to ice[e].
 __global__ void __launch_bounds__(256) k_apply_move(const PopDev* pops, const int* gpair_pop,
-                                                    const int* gpair_local, const long long* work_off,
-                                                    const long long* n_events, const long long* ev_w,
+                                                    const long long* n_events, const unsigned long long* ev_key,
                                                     const int2* ev, const int* ev_gp, const uint8_t* win,
                                                     const uint32_t* dec, const long long* slot_rank,
                                                     const int* slot_base, double2* ice) {
@@ -151,7 +230,7 @@ __global__ void __launch_bounds__(256) k_apply_move(const PopDev* pops, const in
   long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long e = warp; e < E; e += n_warps) {
-    if (!win[e]) continue;  // the same e for the whole warp
+    if (win[e] != 1) continue;  // the same e for the whole warp; chains apply in k_apply_chain
     uint32_t used;
     MergeDecision m = unpack_decision(dec[e], &used);
     if (!m.create) continue;
@@ -185,7 +264,7 @@ __global__ void __launch_bounds__(256) k_apply_move(const PopDev* pops, const in
     bool from_a = lane < na;
     if (na + nb > kMaxComponent) {
       int np1 = P.nprim[s1], np2 = P.nprim[s2];
-      Rng g = make_rng(P, kStreamMerge, (uint32_t)gpair_local[gp], (uint32_t)(ev_w[e] - work_off[gp]));
+      Rng g = merge_rng(P, ev_key[e]);
       g.seek(used);
       int sa[kMaxComponent], sb[kMaxComponent];
       coag_components(g, na, np1, nb, np2, &n1_new, &n2_new, sa, sb);
@@ -234,24 +313,31 @@ __device__ __forceinline__ void load_scalars(const PopDev& P, int i, PMeta& m) {
 }
 
 // Part 2, one thread per event: removals, the scalar fields of the
-// coagulated particle, its radius, bin and pair-test record.
-__global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
-                            const long long* n_events, const int2* ev, const int* ev_gp, const uint8_t* win,
-                            const uint32_t* dec, const long long* slot_rank, const long long* id_rank,
-                            const int* slot_base, const long long* id_base, const double2* ice) {
+// coagulated particle, its radius, bin and pair-test record.  Every slot an
+// event removes or rewrites is stamped with the round's claim generation,
+// and dest[e] gets the slot of the particle the event made (-1 if none).
+__global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long long* n_events,
+                            const unsigned long long* ev_key, const int2* ev, const int* ev_gp,
+                            const uint8_t* win, const uint32_t* dec, const long long* slot_rank,
+                            const long long* id_rank, const int* slot_base, const long long* id_base,
+                            const double2* ice, int* dest_out) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
-    if (!win[e]) continue;
+    dest_out[e] = -1;
+    if (win[e] != 1) continue;
     int gp = ev_gp[e];
     int pop = gpair_pop[gp];
     const PopDev& P = pops[pop];
-    int p = gpair_local[gp];
+    int p = (int)key_pair(ev_key[e]);
     int2 sl = ev[e];
     int s1 = sl.x, s2 = sl.y;
+    uint32_t gen = *P.gen_p;
     uint32_t used;
     MergeDecision m = unpack_decision(dec[e], &used);
     add_ll(&P.ctr->tot_coag, (long long)(1LL));
+    if (m.rm1) P.touched[s1] = gen;
+    if (m.rm2) P.touched[s2] = gen;
     if (!m.create) {
       if (m.rm1) kill_slot(P, s1);
       if (m.rm2) kill_slot(P, s2);
@@ -290,12 +376,415 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const int*
     P.changed[dest] = 1;
     // the coagulated particle must lie on the grid (aero_state_add_particle
     // with allow_resort=.false., aero_sorted.F90:427-440)
+    P.touched[dest] = gen;
     int nbin = refresh_slot(P, dest);
     if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
+    else dest_out[e] = dest;
     if (m.rm1 && dest != s1) kill_slot(P, s1);
     if (m.rm2 && dest != s2) kill_slot(P, s2);
     int dlive = 1 - (int)m.rm1 - (int)m.rm2;
     if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Walks.  In the sequential loop a particle that an event creates (or
+// changes) at pair p0 takes part in the rest of the step: every later pair
+// that contains its cell draws its samples with the particle among the
+// cell's members, so it is tested against each member of the pair's other
+// cell at rate k_max * del_t (the pair's samples, n1 * n2 * k_max * del_t in
+// mean, fall on each of the n1 * n2 possible pairs alike; for one cell with
+// itself n (n - 1) / 2 pairs and n - 1 partners).  A walk draws those tests
+// as one Poisson process along the pairs that follow p0 in loop order, the
+// rest of p0 itself from position pos0 (the fraction of p0's test sequence
+// already done).
+//
+// Partners come from the cell lists of the last sort: a listed slot that is
+// dead, has left the cell since, is the walking particle itself or was
+// absorbed earlier in its chain is no member now, and a test that falls on
+// it is dropped, which thins the step-start members down to the ones still
+// there.  Particles that arrived in the other cell since the sort are not
+// partners; tests between two particles that both changed in the step are
+// left out.  Pairs on the per-particle path are not walked.
+//
+// Chains.  A walk's accepted test whose merge decision (coagulate_weighting,
+// drawn from the stream the event's apply uses) replaces the walking particle
+// by the coagulated one is an absorb: the walk goes on at once with the
+// coagulated particle's values (volumes summed as the apply sums them,
+// radius, record, cell), as the sequential loop would test it next.  Each
+// absorbed partner is claimed with its own key; the events are recorded in
+// a chain (ChainPool) and applied, as far as their claims hold, by one
+// thread in order (k_apply_chain).  A runaway collector that absorbs
+// thousands of droplets in one step (the sedimentation kernel) takes one
+// round, not one round per droplet.  The chain stops before an accepted
+// test that is not an absorb; the walk resumes there in the next round.
+
+// cell of a particle of radius r and class cls (1-based); -1 off the grid
+__device__ __forceinline__ int cell_of(const PopDev& P, double r, int cls) {
+  const GridDev& G = *P.grid;
+  int b = bin_find(G.n_bin, G.log_lo, G.log_hi, r);
+  if (b < 1 || b > G.n_bin || cls < 1 || cls > P.n_class) return -1;
+  return (b - 1) + G.n_bin * (cls - 1);
+}
+
+// the walk's first accepted test, and its chain
+struct WalkOut {
+  bool found = false;
+  int q = 0, y = 0;  // pair and partner of the first event
+  float pos = 0.f;
+  bool first_cell1 = true;  // the walking particle is in the pair's first cell
+  int chain_len = 0;        // events in the chain (0: the first event alone)
+  int chain_head = -1;
+  bool done = false;        // the walk ran to the end after its last event
+};
+
+// true if this round's claim on slot y is the chain of walker x
+__device__ __forceinline__ bool claimed_by_walk(const PopDev& P, int y, int x) {
+  unsigned long long w = P.claim[y];
+  return (w >> 53) == (unsigned long long)(~*P.gen_p & kGenLimit) && ((w >> 32) & 1ULL) &&
+         (uint32_t)w == (uint32_t)x;
+}
+
+template <int KT, class T, bool FLAT>
+__device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, float pos0, WalkOut* out) {
+  if (x < 0 || x >= P.cap || !P.alive[x]) return;
+  int C = P.cell[x];
+  if (C < 0 || C >= P.n_cells) return;
+  const int nb = P.grid->n_bin;
+  // the walking particle: its record, and in a chain its summed volumes
+  double r = P.rad[x], vt = P.vtot[x];
+  RecD rec = P.recd[x];
+  RecF recf = P.recf[x];
+  double vcur[kMaxSpec];
+  ChainWriter cw;
+  Rng g = make_rng(P, kStreamWalk, 0u, (uint32_t)x);
+  long long n_tests = 0, n_iter = 0;
+  double t = -log(g.next());  // distance to the next test, in expected tests
+  bool stop = false;
+  while (!stop) {
+    // pairs of cell C from (p0, pos0) on
+    int lo = P.cp_off[C], end = P.cp_off[C + 1];
+    {
+      int hi = end;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (P.cp_list[mid] < p0) lo = mid + 1;
+        else hi = mid;
+      }
+    }
+    bool moved = false;
+    for (int j = lo; j < end && !stop && !moved; j++) {
+      int q = P.cp_list[j];
+      const PairState& S = P.pair[q];
+      if (S.path == kPathParticle) continue;
+      PairDesc d = P.pair_desc[q];
+      int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
+      int O = cell1 == C ? cell2 : cell1;
+      int n_o = P.cell_count[O];
+      int o_start = P.cell_start[O];
+      if (n_o < 1) continue;
+      if (o_start < 0 || (long long)o_start + n_o > P.cap) {
+        bad_index(P.ctr, kBadPairCells, q);
+        stop = true;
+        break;
+      }
+      double lam = S.k_max * P.del_t * (double)n_o;  // expected tests over the whole pair
+      if (!(lam > 0.0)) continue;
+      double pos = q == p0 ? (double)pos0 : 0.0;
+      for (;;) {
+        double adv = t / lam;
+        if (pos + adv >= 1.0) {
+          t -= lam * (1.0 - pos);
+          break;
+        }
+        pos += adv;
+        t = -log(g.next());
+        if (++n_iter > (1LL << 26)) {  // far past any mean the step can ask for
+          set_status(P.ctr, kErrTimeout);
+          stop = true;
+          break;
+        }
+        int i = (int)(g.next() * (double)n_o);
+        if (i >= n_o) i = n_o - 1;
+        int y = P.list[o_start + i];
+        if (y < 0 || y >= P.cap) {
+          bad_index(P.ctr, kBadTestSlot, y);
+          continue;
+        }
+        if (y == x || !P.alive[y] || P.cell[y] != O) continue;
+        if (cw.len > 0 && claimed_by_walk(P, y, x)) continue;  // absorbed earlier in this chain
+        n_tests++;
+        bool first = cell1 == C;
+        T k;
+        if constexpr (sizeof(T) == 8) {
+          const double* qw = (const double*)&rec;
+          const double* qy = (const double*)&P.recd[y];
+          k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat,
+                                               P.coeff);
+        } else {
+          const float* qw = (const float*)&recf;
+          const float* qy = (const float*)&P.recf[y];
+          k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc,
+                                              (float)S.fflat, (float)P.coeff);
+        }
+        T prob = k * (T)S.inv_k_max;
+        if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
+        if (!((T)g.next() < prob)) continue;
+        // an accepted test: would its merge replace the walking particle?
+        unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
+        Rng gm = cw.len == 0 ? merge_rng(P, key) : make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
+        double ry = P.rad[y], vty = P.vtot[y];
+        MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
+                                : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
+        bool absorb = m.create && (first ? m.rm1 : m.rm2) && m.new_group != 0;
+        if (!out->found) {
+          // the first event: claimed whatever follows
+          out->found = true;
+          out->q = q;
+          out->y = y;
+          out->pos = (float)pos;
+          out->first_cell1 = first;
+          atomicMin(&P.claim[x], claim_key(P, key));
+          atomicMin(&P.claim[y], claim_key(P, key));
+          if (!absorb || !cw.append(pool, y, q, (float)pos)) {  // the first event alone
+            stop = true;
+            break;
+          }
+          for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
+        } else {
+          // the chain ends before an event that is no absorb, or when the
+          // pool is full; the walk resumes there in the next round
+          if (!absorb || !cw.append(pool, y, q, (float)pos)) {
+            stop = true;
+            break;
+          }
+          atomicMin(&P.claim[y], claim_key(P, key));
+        }
+        // absorb y: the coagulated particle's volumes, radius, class, record
+        double s_v = 0.0, s_m = 0.0;
+        for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
+        for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
+        for (int s = 0; s < P.n_spec; s++) s_m = s_m + vcur[s] * P.density[s];
+        vt = s_v;
+        r = vol2rad(vt);
+        int cls = S.cc + 1;
+        rec = make_rec_v(P, r, vt, s_m, cls);
+        recf = to_f32(rec);
+        int C2 = cell_of(P, r, cls);
+        if (C2 < 0 || cw.len >= kChainMaxLen) {  // off the grid (reported by the apply) or long enough
+          stop = true;
+          break;
+        }
+        if (C2 != C) {
+          C = C2;
+          p0 = q;
+          pos0 = (float)pos;
+          moved = true;
+          break;
+        }
+      }
+    }
+    if (!moved && !stop) {
+      out->done = true;  // every later pair of the cell was walked
+      break;
+    }
+  }
+  out->chain_len = cw.len;
+  out->chain_head = cw.head;
+  if (n_tests) {
+    add_ll(&P.ctr->tot_samp, n_tests);
+    add_ll(&P.ctr->walk_tests, n_tests);
+  }
+}
+
+// The work of a later round, one thread per event e of the round before:
+//   - a winner that created or changed a particle (dest[e] >= 0): that
+//     particle walks from the event's pair and position (for a chain, its
+//     last applied event's);
+//   - a loser: consumed = removed or rewritten in the round before
+//     (touched), or dead.  A sample (kind 0) is retried with its key if
+//     neither particle was consumed, else dropped.  A walk's test (kind 1,
+//     a chain's first event): dropped if the walking particle was consumed,
+//     the walk resumed after the test if only the partner was, else retried
+//     alone.
+// Output per e: flag, and key, slots, global pair and position of the new
+// event (for a chain its first event) with the chain's length and head; the
+// new event holds claims on its slots.
+template <int KT, class T, bool FLAT>
+__global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
+                                               const long long* pop_pair_base, int n_gpairs, const long long* n_items,
+                                               const uint8_t* win, const int* dest,
+                                               const unsigned long long* ev_key, const int2* ev_c,
+                                               const int* gp_c, const float* ev_pos, ChainPool pool,
+                                               uint8_t* it_flag, unsigned long long* it_key, int2* it_c, int* it_gp,
+                                               float* it_pos, int* it_len, int* it_head, uint8_t* it_done) {
+  long long n = *n_items;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    it_flag[e] = 0;
+    int gp = gp_c[e];
+    if (gp < 0 || gp >= n_gpairs) {
+      bad_index(pops[0].ctr, kBadEventSlot, gp);
+      continue;
+    }
+    int pop = gpair_pop[gp];
+    const PopDev& P = pops[pop];
+    int walker = -1, p0 = 0;
+    float pos0 = ev_pos[e];
+    unsigned long long key = ev_key[e];
+    int2 sl = ev_c[e];
+    if (win[e]) {
+      walker = dest[e];
+      p0 = gpair_local[gp];
+      if (walker < 0) continue;
+    } else {
+      if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
+        bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+        continue;
+      }
+      uint32_t gen_prev = *P.gen_p - 1u;
+      bool c1 = P.touched[sl.x] == gen_prev || !P.alive[sl.x];
+      bool c2 = P.touched[sl.y] == gen_prev || !P.alive[sl.y];
+      if (key_kind(key) == 0u) {
+        if (c1 || c2) continue;
+      } else {
+        int x = (int)key_idx(key);
+        bool cx = x == sl.x ? c1 : c2, cy = x == sl.x ? c2 : c1;
+        if (cx) continue;
+        if (cy) {
+          walker = x;
+          p0 = (int)key_pair(key);
+        }
+      }
+    }
+    int len = 0, head = -1;
+    bool done = false;
+    if (walker >= 0) {
+      WalkOut w;
+      walk<KT, T, FLAT>(P, pool, walker, p0, pos0, &w);
+      if (!w.found) continue;
+      key = make_key((uint32_t)w.q, 1u, (uint32_t)walker);
+      sl = w.first_cell1 ? make_int2(walker, w.y) : make_int2(w.y, walker);
+      gp = (int)(pop_pair_base[pop] + w.q);
+      pos0 = w.pos;
+      len = w.chain_len;
+      head = w.chain_head;
+      done = w.done;
+    } else {
+      atomicMin(&P.claim[sl.x], claim_key(P, key));
+      atomicMin(&P.claim[sl.y], claim_key(P, key));
+    }
+    it_flag[e] = 1;
+    it_key[e] = key;
+    it_c[e] = sl;
+    it_gp[e] = gp;
+    it_pos[e] = pos0;
+    it_len[e] = len;
+    it_head[e] = head;
+    it_done[e] = done ? 1 : 0;
+  }
+}
+
+// Apply the winning chains (win[e] == 2), one thread per chain: the first
+// ev_app[e] events in order, each a coagulate (coagulation.F90:928-985) of
+// the walking particle with the next partner, with the merge decision
+// recomputed from the values and the stream the walk used.  The coagulated
+// particle stays in the walking particle's slot; absorbed partners that the
+// decision removes are killed.  dest[e], gp_c[e] and ev_pos[e] are set to
+// where the particle walks on (dest -1 if its walk ran to the end).
+__global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const long long* pop_pair_base,
+                              const long long* n_events, const unsigned long long* ev_key, const uint8_t* win,
+                              const int* ev_len, const int* ev_app, const int* ev_head, const uint8_t* ev_done,
+                              ChainPool pool, int* gp_c, float* ev_pos, int* dest_out) {
+  long long E = *n_events;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (win[e] != 2) continue;
+    int pop = gpair_pop[gp_c[e]];
+    const PopDev& P = pops[pop];
+    unsigned long long key1 = ev_key[e];
+    int x = (int)key_idx(key1);
+    int app = ev_app[e];
+    if (x < 0 || x >= P.cap) {
+      bad_index(P.ctr, kBadEventSlot, x);
+      continue;
+    }
+    const int nb = P.grid->n_bin;
+    uint32_t gen = *P.gen_p;
+    double vcur[kMaxSpec];
+    for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
+    PMeta cur, ym, nm;
+    load_meta(P, x, cur);
+    double r = P.rad[x], vt = P.vtot[x];
+    int C = P.cell[x];
+    ChainReader rd(ev_head[e]);
+    int done_ev = 0, last_q = -1, dlive = 0;
+    float last_pos = 0.f;
+    for (int i = 0; i < app; i++) {
+      long long ix = rd.next(pool);
+      if (ix < 0) {
+        bad_index(P.ctr, kBadEventSlot, -1);
+        break;
+      }
+      int y = pool.y[ix], q = pool.q[ix];
+      if (y < 0 || y >= P.cap || q < 0 || q >= P.n_pairs) {
+        bad_index(P.ctr, kBadEventSlot, y);
+        break;
+      }
+      PairDesc d = P.pair_desc[q];
+      const PairState& S = P.pair[q];
+      bool first = C == d.b1 + nb * d.c1;
+      Rng g = i == 0 ? merge_rng(P, key1) : make_rng(P, kStreamChain, (uint32_t)(i + 1), (uint32_t)x);
+      double ry = P.rad[y], vty = P.vtot[y];
+      MergeDecision m = first ? merge_decide_v(P, g, r, vt, ry, vty, d.c1, d.c2, S.cc)
+                              : merge_decide_v(P, g, ry, vty, r, vt, d.c1, d.c2, S.cc);
+      bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
+      bool lost_x = first ? m.lost1 : m.lost2, lost_y = first ? m.lost2 : m.lost1;
+      if (!(m.create && rm_x && m.new_group != 0)) {  // the walk decided an absorb here
+        set_status(P.ctr, kErrAssert);
+        break;
+      }
+      load_meta(P, y, ym);
+      double ice_x = P.i_water > 0 ? vcur[P.i_water - 1] : 0.0;
+      double ice_y = P.i_water > 0 ? P.vol[vol_at(P, y, P.i_water - 1)] : 0.0;
+      if (first) coag_meta(g, cur, ice_x, ym, ice_y, nm);
+      else coag_meta(g, ym, ice_y, cur, ice_x, nm);
+      if (!lost_x) nm.id = cur.id;
+      else if (rm_y && !lost_y) nm.id = ym.id;
+      else {
+        set_status(P.ctr, kErrAssert);
+        break;
+      }
+      nm.grp = m.new_group;
+      nm.cls = S.cc + 1;
+      double s_v = 0.0;
+      for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
+      for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
+      vt = s_v;
+      r = vol2rad(vt);
+      C = cell_of(P, r, nm.cls);
+      if (rm_y) {
+        kill_slot(P, y);
+        P.touched[y] = gen;
+        dlive--;
+      }
+      cur = nm;
+      done_ev++;
+      last_q = q;
+      last_pos = pool.pos[ix];
+    }
+    if (done_ev == 0) continue;
+    store_particle(P, x, vcur, cur);
+    P.touched[x] = gen;
+    int nbin = refresh_slot(P, x);
+    bool on_grid = nbin >= 1 && nbin <= nb;
+    if (!on_grid) set_status(P.ctr, kErrOutOfGrid);
+    add_ll(&P.ctr->tot_coag, (long long)done_ev);
+    if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
+    bool walk_done = ev_done[e] && done_ev == ev_len[e];
+    dest_out[e] = (walk_done || !on_grid) ? -1 : x;
+    gp_c[e] = (int)(pop_pair_base[pop] + last_q);
+    ev_pos[e] = last_pos;
   }
 }
 
@@ -326,14 +815,14 @@ __device__ double pp_kernel(const PopDev& P, const RecD& qs, const RecD& qt, int
 
 template <int KT>
 __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pair,
-                         const int* op_slot, const int* op_k, const unsigned* op_prio,
+                         const int* op_slot, const int* op_k, const unsigned long long* op_key,
                          const long long* n_ops, PPResult* res, double* res_vol) {
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
     const PopDev& P = pops[op_pop[q]];
     int p = op_pair[q], t = op_slot[q];
-    unsigned prio = op_prio[q];
+    unsigned long long prio = op_key[q];
     PPResult& R = res[q];
     R.target = t;
     R.p = p;
@@ -520,7 +1009,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
 }
 
 // phase 2a: winners and allocation needs of the target operations
-__global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsigned* op_prio,
+__global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsigned long long* op_key,
                              const long long* n_ops, const PPResult* res, uint8_t* win,
                              int* need_slot, int* need_id, int* lost) {
   long long Q = *n_ops;
@@ -528,7 +1017,7 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
        q += (long long)gridDim.x * blockDim.x) {
     const PopDev& P = pops[op_pop[q]];
     const PPResult& R = res[q];
-    unsigned prio = op_prio[q];
+    unsigned long long prio = op_key[q];
     bool ok = true;
     if (R.merged) ok = ok && P.claim[R.target] == claim_key(P, prio);
     for (int z = 0; z < R.n_rm; z++) ok = ok && P.claim[R.rm[z]] == claim_key(P, prio);
@@ -556,14 +1045,17 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
     // operations count their samples and coagulations
     if (R.n_samp) add_ll(&P.ctr->tot_samp, (long long)R.n_samp);
     if (R.n_coag) add_ll(&P.ctr->tot_coag, (long long)R.n_coag);
+    uint32_t gen = *P.gen_p;
     int dlive = 0;
     for (int z = 0; z < R.n_rm; z++) {
       kill_slot(P, R.rm[z]);
+      P.touched[R.rm[z]] = gen;
       dlive--;
     }
     if (R.merged) {
       const double* v = res_vol + (size_t)q * P.n_spec;
       int t = R.target;
+      P.touched[t] = gen;
       if (R.n_copies == 0) {
         kill_slot(P, t);
         dlive--;
@@ -581,6 +1073,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
           cm.id = id_base[pop] + id_rank[q] + (z - 1);
           store_particle(P, dest, v, cm);
           refresh_slot(P, dest);
+          P.touched[dest] = gen;
           dlive++;
         }
       }

@@ -104,6 +104,7 @@ struct PopCtr {
   long long rng_used;      // replay: uniforms consumed
   int bad_site;            // first failed bounds check (kBad*), 0 if none
   long long bad_index;     // the index that failed it
+  long long walk_tests;    // pair tests made by walks in the current step
 };
 
 // sites of the device bounds checks (PopCtr::bad_site)
@@ -181,11 +182,19 @@ struct PopDev {
 
   const PairDesc* pair_desc;  // [n_pairs]
   PairState* pair;            // [n_pairs]
+  // pairs that contain each cell, in loop order (CSR): the pairs of cell c
+  // are cp_list[cp_off[c] .. cp_off[c + 1])
+  const int* cp_off;   // [n_cells + 1]
+  const int* cp_list;  // [cp_off[n_cells]]
 
-  // [cap] lowest claim key of the current round: (~generation << 32) |
-  // priority, so a key from any earlier round is larger and is replaced by
-  // the first claim of this round; no per-round reset is needed
+  // [cap] lowest claim key of the current round (claim_key), so a key from
+  // any earlier round is larger and is replaced by the first claim of this
+  // round; no per-round reset is needed
   unsigned long long* claim;
+  // [cap] claim generation of the round that last removed or rewrote the
+  // slot: an event that lost a claim in round r is retried in round r + 1
+  // only if neither of its particles was consumed in round r
+  uint32_t* touched;
 
   PopCtr* ctr;
 };
@@ -194,10 +203,27 @@ __host__ __device__ __forceinline__ size_t vol_at(const PopDev& P, long long i, 
   return PMC_VOL_AT(P.n_spec, i, s);
 }
 
+// Event priorities follow the reference's order of tests within one step:
+// the pair p in loop order first, then the test.  kind 0 is test idx of the
+// pair's own samples (round 0; a per-particle pair's target operation idx);
+// kind 1 is a walk's test in pair p made by the particle in slot idx, placed
+// after the pair's own samples.  p < 2^20, idx < 2^32: 53 bits.
+__host__ __device__ __forceinline__ unsigned long long make_key(uint32_t p, uint32_t kind, uint32_t idx) {
+  return ((unsigned long long)p << 33) | ((unsigned long long)kind << 32) | (unsigned long long)idx;
+}
+__host__ __device__ __forceinline__ uint32_t key_pair(unsigned long long k) { return (uint32_t)(k >> 33); }
+__host__ __device__ __forceinline__ uint32_t key_kind(unsigned long long k) { return (uint32_t)(k >> 32) & 1u; }
+__host__ __device__ __forceinline__ uint32_t key_idx(unsigned long long k) { return (uint32_t)k; }
+
+// claim generations live in the top 11 bits of a claim word; the host
+// restarts them (clearing every claim and touched word) before they run out
+constexpr uint32_t kGenLimit = 2047;
+
 #ifdef __CUDACC__
-// claim key of priority prio in the current round
-__device__ __forceinline__ unsigned long long claim_key(const PopDev& P, unsigned prio) {
-  return ((unsigned long long)(~*P.gen_p) << 32) | (unsigned long long)prio;
+// claim word of an event key in the current round: a later generation gives
+// a smaller word, so the first claim of a round replaces any older one
+__device__ __forceinline__ unsigned long long claim_key(const PopDev& P, unsigned long long key) {
+  return ((unsigned long long)(~*P.gen_p & kGenLimit) << 53) | key;
 }
 #endif
 
