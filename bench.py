@@ -364,12 +364,13 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     del mirror, str_
 
     # serving (cfg 5): Poisson arrivals at 50 jobs/s, 1e3..1e6 particles,
-    # additive / Brownian / sedimentation, 10..200 steps of del_t, continuous
-    # batching within a 150 GB HBM budget
+    # additive / Brownian / sedimentation, 10..200 steps each of the step
+    # length of the reference's test for the kernel (serve.DEL_T: 1 s, 600 s,
+    # 5 s), continuous batching within a 150 GB HBM budget
     from partmc_b200 import serve
     jobs = serve.poisson_jobs(args.serve_jobs, rate=50.0, seed=5 + 1000 * (ws > 1))
     srv = serve.Server([pm.COAG_KERNEL_TYPE_ADDITIVE, pm.COAG_KERNEL_TYPE_BROWN, pm.COAG_KERNEL_TYPE_SEDI],
-                       slots=48, hbm_budget=150e9, del_t=args.del_t, mode=mode)
+                       slots=48, hbm_budget=150e9, mode=mode)
     serve.warm_up(srv)
     sm = serve.run(jobs, srv)
     del srv

@@ -1699,11 +1699,13 @@ __global__ void k_pop_work(const long long* pop_pair_base, int n_pop, const long
 // most one event or chain).  So the later rounds run as the body of a
 // conditional WHILE node of one CUDA graph: k_round_begin advances the round
 // and the claim generation and makes the last round's events this round's
-// items; k_round_end adds up the step's statistics and sets the loop
-// condition: events in this round, fewer than max_rounds rounds, and room
-// in every population for the next round's new slots.  Without room the
-// graph stops and the host loop, which can grow the slot arrays, carries
-// on.  Rounds with per-particle redo operations run from the host loop.
+// items; the sort brings the cell lists to the round's start, so walks meet
+// the particles earlier rounds made; k_round_end adds up the step's
+// statistics and sets the loop condition: events in this round, fewer than
+// max_rounds rounds, and room in every population for the next round's new
+// slots, in the slot arrays and in the sort's chunks.  Without room the
+// graph stops and the host loop, which can grow both, carries on.  Rounds
+// with per-particle redo operations run from the host loop.
 
 __global__ void k_round_begin(uint32_t* d_round, long long* round_dev, int* per_pop, int n_per_pop) {
   if (blockIdx.x != 0) return;
@@ -1721,15 +1723,18 @@ __global__ void k_round_begin(uint32_t* d_round, long long* round_dev, int* per_
 // stats: [0] events that lost a claim, [1] events, [2] rounds, [3] 1 if the
 // graph stopped for lack of slots with events left
 __global__ void k_round_end(const long long* round_dev, long long* stats, const uint32_t* d_round, int max_rounds,
-                            const PopDev* pops, PopCtr* ctrs, int n_pop, cudaGraphConditionalHandle cond) {
+                            const PopDev* pops, PopCtr* ctrs, int n_pop, long long sort_slots,
+                            cudaGraphConditionalHandle cond) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   long long E = round_dev[1];
   stats[0] += round_dev[0];
   stats[1] += E;
   stats[2] += 1;
   bool room = true;
-  for (int k = 0; k < n_pop; k++)
-    if ((long long)ctrs[k].n_slots + E > (long long)pops[k].cap) room = false;
+  for (int k = 0; k < n_pop; k++) {
+    long long need = (long long)ctrs[k].n_slots + E;
+    if (need > (long long)pops[k].cap || need > sort_slots) room = false;
+  }
   bool more = E > 0 && room && (int)d_round[0] + 1 < max_rounds;
   if (E > 0 && room && !more)
     for (int k = 0; k < n_pop; k++)
@@ -1799,14 +1804,18 @@ struct RoundBounds {
   int kt;
   bool flat;
   int n_gpairs;
-  long long W;  // items and events of a round, at most
+  long long W;     // items and events of a round, at most
+  int max_chunks;  // sort chunks per population, at most
+  int max_cells;
 };
 
-// The kernels of one later round on stream st, after k_round_begin: items,
-// their events in item order, then resolve and apply.  With Q > 0 (host
-// loop only) the round's per-particle redo operations claim alongside.
+// The kernels of one later round on stream st, after k_round_begin: the
+// sort, items, their events in item order, then resolve and apply.  With
+// Q > 0 (host loop only) the round's per-particle redo operations claim
+// alongside.
 void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long Q) {
   long long W = b.W;
+  launch_sort(c, st, b.max_chunks, b.max_cells);
   launch_items_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
   if (Q > 0) {
     set_n_dev(c, Q);
@@ -1825,7 +1834,8 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
 
 // everything the captured launches depend on: sizes and device addresses
 std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
-  return {c.n_pop, b.kt, b.flat, b.n_gpairs, b.W, c.max_rounds, c.mode, c.ch_chunks,
+  return {c.n_pop, b.kt, b.flat, b.n_gpairs, b.W, b.max_chunks, b.max_cells, c.sort_blocks, (long long)c.sort_smem,
+          c.max_rounds, c.mode, c.ch_chunks,
           (long long)c.d_pops, (long long)c.d_round, (long long)c.d_ctrs, (long long)c.round_dev.p,
           (long long)c.per_pop_i.p, (long long)c.pop_pair_base.p, (long long)c.gpair_pop.p,
           (long long)c.gpair_local.p, (long long)c.ev_key.p, (long long)c.ev_c.p, (long long)c.gp_c.p,
@@ -1913,6 +1923,18 @@ GraphRun run_round_graph(Ctx& c, int kt, bool flat, int n_gpairs, long long e0) 
   // the event arrays hold the last round's events: they must already be
   // large enough (reserve_events), never reallocated here
   if (!events_fit(c, b.W)) return out;
+  // the sort's chunks cover the slots of several rounds' growth; the graph
+  // stops before they would not
+  long long slots = 0, min_slots = -1;
+  for (int k = 0; k < c.n_pop; k++) {
+    slots = std::max<long long>(slots, c.n_slots_host[k]);
+    min_slots = min_slots < 0 ? c.n_slots_host[k] : std::min<long long>(min_slots, c.n_slots_host[k]);
+  }
+  b.max_chunks = (int)((slots + 4 * b.W + kChunk - 1) / kChunk);
+  b.max_chunks = (b.max_chunks + 15) / 16 * 16;
+  b.max_cells = max_cells_of(c);
+  prepare_chunks(c, (long long)b.max_chunks * kChunk - min_slots);
+  size_sort(c, b.max_cells);
   // every other buffer at its final size before the addresses are taken
   reserve_round(c, b.W);
   c.graph_stats.reserve(4);
@@ -1954,7 +1976,7 @@ GraphRun run_round_graph(Ctx& c, int kt, bool flat, int n_gpairs, long long e0) 
       note_launch();
       enqueue_round_body(c, c.cap_stream, b, 0);
       k_round_end<<<1, 32, 0, c.cap_stream>>>(c.round_dev.p, c.graph_stats.p, c.d_round, c.max_rounds, c.d_pops,
-                                              c.d_ctrs, c.n_pop, cond);
+                                              c.d_ctrs, c.n_pop, (long long)b.max_chunks * kChunk, cond);
       note_launch();
     } catch (...) {
       cudaGraph_t dummy;
@@ -2255,11 +2277,13 @@ void step_parallel(Ctx& c, int kt) {
       c.need_slot_pp.reserve(Qn + 1); c.need_id_pp.reserve(Qn + 1); c.win_pp.reserve(Qn + 1);
       c.lost_pp.reserve(Qn + 1); c.lost_off.reserve(Qn + 2); c.rank_slot_pp.reserve(Qn + 2);
       c.rank_id_pp.reserve(Qn + 2);
-      // target operations sample their sources from the current cells
-      sort_pops(c, false);
     }
+    // the round's sort covers the current slots exactly
+    prepare_chunks(c);
+    int mc = 1;
+    for (int k = 0; k < c.n_pop; k++) mc = std::max(mc, c.pops[k].h.n_chunks);
     if (c.dirty) push_pops(c);
-    RoundBounds b{kt, flat, n_gpairs, E};
+    RoundBounds b{kt, flat, n_gpairs, E, mc, max_cells_of(c)};
     k_round_begin<<<1, 128, 0, c.stream>>>(c.d_round, c.round_dev.p, c.per_pop_i.p, 4 * c.n_pop);
     note_launch();
     c.claim_gen++;  // as k_round_begin on the device

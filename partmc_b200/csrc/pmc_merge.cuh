@@ -399,13 +399,13 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
 // rest of p0 itself from position pos0 (the fraction of p0's test sequence
 // already done).
 //
-// Partners come from the cell lists of the last sort: a listed slot that is
-// dead, has left the cell since, is the walking particle itself or was
-// absorbed earlier in its chain is no member now, and a test that falls on
-// it is dropped, which thins the step-start members down to the ones still
-// there.  Particles that arrived in the other cell since the sort are not
-// partners; tests between two particles that both changed in the step are
-// left out.  Pairs on the per-particle path are not walked.
+// Partners come from the cell lists of the sort at the round's start, so a
+// walk meets every particle that earlier rounds of the step made.  A listed
+// slot that is dead, has left the cell since, is the walking particle itself
+// or was absorbed earlier in its chain is no member now, and a test that
+// falls on it is dropped.  Particles that other walks of the same round
+// change are met with the values they had at the round's start.  Pairs on
+// the per-particle path are not walked.
 //
 // Chains.  A walk's accepted test whose merge decision (coagulate_weighting,
 // drawn from the stream the event's apply uses) replaces the walking particle

@@ -1,8 +1,9 @@
 """Serving many coagulation jobs on one GPU with continuous batching.
 
-A job is one particle population advanced by a number of mc_coag steps of
-length del_t with one coagulation kernel (the reference's run_part loop with
-only coagulation on, run_part.F90:917-931).  Jobs arrive over time; the
+A job is one particle population advanced by a number of mc_coag steps
+with one coagulation kernel (the reference's run_part loop with only
+coagulation on, run_part.F90:917-931).  The step length of each kernel type
+is the one of the reference's own test for it (DEL_T).  Jobs arrive over time; the
 server keeps one batched context per kernel type with a fixed number of
 population slots and, every tick:
 
@@ -32,6 +33,10 @@ from . import coagulation as C
 # (about 80 B), components (20 x 12 B), sort and claim words (20 B), at the
 # library's 1.5x capacity
 BYTES_PER_PARTICLE = int(1.5 * (32 + 80 + 80 + 240 + 20))
+
+# step length per kernel type: del_t of test/additive, test/sedi and
+# test/brownian (run_part.spec of each)
+DEL_T = {C.COAG_KERNEL_TYPE_ADDITIVE: 1.0, C.COAG_KERNEL_TYPE_SEDI: 5.0, C.COAG_KERNEL_TYPE_BROWN: 600.0}
 
 
 class Job:
@@ -85,8 +90,10 @@ class Server:
     """Batched contexts per kernel type, `slots` populations each.  All jobs
     of one kernel type share its species (species_of)."""
 
-    def __init__(self, kernels, slots=32, hbm_budget=150e9, del_t=60.0, mode=C.MODE_MIXED, keep_results=False):
-        self.del_t, self.budget, self.used = float(del_t), float(hbm_budget), 0.0
+    def __init__(self, kernels, slots=32, hbm_budget=150e9, del_t=None, mode=C.MODE_MIXED, keep_results=False):
+        # del_t: one step length for every kernel, or None for DEL_T
+        self.del_t = {k: float(del_t) if del_t is not None else DEL_T.get(k, 60.0) for k in kernels}
+        self.budget, self.used = float(hbm_budget), 0.0
         self.keep_results = keep_results
         self.n_samp_total = 0
         self.ctx, self.jobs = {}, {}
@@ -130,7 +137,7 @@ class Server:
             temps = np.array([j.temp if j else 288.0 for j in slots])
             press = np.array([j.pressure if j else 1e5 for j in slots])
             t0 = time.perf_counter()
-            s, c = C.mc_coag_batch(kern, temps, press, 1000.0, st, self.del_t)
+            s, c = C.mc_coag_batch(kern, temps, press, 1000.0, st, self.del_t[kern])
             lat.append(time.perf_counter() - t0)
             for k, j in enumerate(slots):
                 if j is None:
@@ -187,7 +194,7 @@ def run(jobs, server):
     turn = np.array([j.finish - j.arrival for j in finished])
     wait = np.array([j.start - j.arrival for j in finished])
     lat = np.array(tick_lat) * 1e3
-    sim_s = sum(j.n_steps for j in finished) * server.del_t
+    sim_s = sum(j.n_steps * server.del_t[j.kernel] for j in finished)
     return {"jobs": len(finished), "wall_s": wall, "sim_s_per_s": sim_s / wall,
             "pair_tests_per_s": server.n_samp_total / wall,
             "particle_steps_per_s": sum(j.n_part * j.n_steps for j in finished) / wall,

@@ -21,7 +21,7 @@ def test_job_same_served_and_alone(gpu_lib):
         alone = pm.AeroState(serve.species_of(j.kernel), j.pop.awa, seed=j.seed, mode=pm.MODE_MIXED)
         alone.add_particles(j.pop.vol, j.pop.group)
         for _ in range(j.n_steps):
-            pm.mc_coag(j.kernel, pm.EnvState(j.temp, j.pressure, 1000.0), alone.aero_data, alone, server.del_t)
+            pm.mc_coag(j.kernel, pm.EnvState(j.temp, j.pressure, 1000.0), alone.aero_data, alone, server.del_t[j.kernel])
         a = alone.particles()
         for key in a:
             assert np.array_equal(a[key], j.result[key]), (j.jid, key)
