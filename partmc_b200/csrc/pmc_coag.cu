@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
 // test sequence ((s + 1) / n_samp: the part of the pair done after it)
 __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const long long* n_samples,
                                 const int2* ev, const int* ev_gp, const int* gpair_local, const long long* work_off,
-                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len) {
+                                const uint32_t* sdec, unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos,
+                                int* ev_len, uint32_t* dec) {
   long long n = *n_samples;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -200,6 +201,7 @@ __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const
       gp_c[e] = gp;
       ev_pos[e] = (float)((double)(s + 1) / (double)ns);
       ev_len[e] = 0;
+      dec[e] = sdec[i];
     }
 }
 
@@ -207,8 +209,8 @@ __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const
 __global__ void k_compact_items(const uint8_t* it_flag, const long long* off, const long long* n_items,
                                 const unsigned long long* it_key, const int2* it_c, const int* it_gp,
                                 const float* it_pos, const int* it_len, const int* it_head, const uint8_t* it_done,
-                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len,
-                                int* ev_head, uint8_t* ev_done) {
+                                const uint32_t* it_dec, unsigned long long* ev_key, int2* ev_c, int* gp_c,
+                                float* ev_pos, int* ev_len, int* ev_head, uint8_t* ev_done, uint32_t* dec) {
   long long n = *n_items;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -221,6 +223,7 @@ __global__ void k_compact_items(const uint8_t* it_flag, const long long* off, co
       ev_len[e] = it_len[i];
       ev_head[e] = it_head[i];
       ev_done[e] = it_done[i];
+      dec[e] = it_dec[i];
     }
 }
 
@@ -297,8 +300,8 @@ __global__ void k_alloc_bases(const PopDev* pops, int n_pop, const long long* n_
     long long cnt[4] = {0, 0, 0, 0};
     if (k < n_pop) {
       if (E > 0) {
-        long long e_lo = first_event_of(k, E, ev_gp, gpair_pop);
-        long long e_hi = first_event_of(k + 1, E, ev_gp, gpair_pop);
+        long long e_lo = n_pop == 1 ? 0 : first_event_of(k, E, ev_gp, gpair_pop);
+        long long e_hi = n_pop == 1 ? E : first_event_of(k + 1, E, ev_gp, gpair_pop);
         cnt[0] = rank_slot_set[e_hi] - rank_slot_set[e_lo];
         cnt[1] = rank_id_set[e_hi] - rank_id_set[e_lo];
       }
@@ -466,6 +469,7 @@ __global__ void k_double(PopDev P, int n, const uint8_t* flag, const long long* 
     P.recd[d] = P.recd[i];
     P.recf[d] = P.recf[i];
     P.claim[d] = ~0ULL;
+    P.rclaim[d] = ~0ULL;
     P.touched[d] = ~0u;
     P.alive[d] = 1;
     P.changed[d] = 1;
@@ -547,6 +551,7 @@ __global__ void k_relayout(PopDev S, PopDev D, const long long* live_off, int n_
     D.changed[j] = S.changed[i];
     D.cell[j] = S.cell[i];
     D.claim[j] = S.claim[i];
+    D.rclaim[j] = S.rclaim[i];
     D.touched[j] = S.touched[i];
     D.recd[j] = S.recd[i];
     D.recf[j] = S.recf[i];
@@ -767,7 +772,8 @@ struct Ctx {
   DevBuf<long long> pop_pair_base;
   DevBuf<long long> nwork_set, nwork_pp, work_off, pp_off;
   DevBuf<uint8_t> flag, win_set, win_pp;
-  DevBuf<uint32_t> dec_set;  // merge decision of each accepted per-set event
+  DevBuf<uint32_t> dec_set;  // merge decision of each event (drawn when the event is formed)
+  DevBuf<uint32_t> sdec;     // merge decision of each accepted round-0 sample
   DevBuf<int> ev_gp, gp_c;   // global pair of each accepted sample / event
   DevBuf<int2> ev_c;         // slots of each event
   DevBuf<unsigned long long> ev_key;  // key of each event (make_key)
@@ -784,6 +790,7 @@ struct Ctx {
   DevBuf<int2> it_c;
   DevBuf<int> it_gp, it_len, it_head;
   DevBuf<float> it_pos;
+  DevBuf<uint32_t> it_dec;
   DevBuf<long long> it_off;
   // chain events of a round (ChainPool), in chunks
   DevBuf<int> ch_y, ch_q;
@@ -1034,10 +1041,12 @@ void alloc_slots(Ctx& c, PopHost& ph, int cap) {
   h.recd = dalloc<RecD>(o, cap);
   h.recf = dalloc<RecF>(o, cap);
   h.claim = dalloc<unsigned long long>(o, cap);
+  h.rclaim = dalloc<unsigned long long>(o, cap);
   h.touched = dalloc<uint32_t>(o, cap);
   CK(cudaMemsetAsync(h.alive, 0, cap, c.stream));
   CK(cudaMemsetAsync(h.changed, 0, cap, c.stream));
   CK(cudaMemsetAsync(h.claim, 0xff, sizeof(unsigned long long) * cap, c.stream));  // no claim
+  CK(cudaMemsetAsync(h.rclaim, 0xff, sizeof(unsigned long long) * cap, c.stream));
   CK(cudaMemsetAsync(h.touched, 0xff, sizeof(uint32_t) * cap, c.stream));        // no generation
   c.dirty = true;
 }
@@ -1089,6 +1098,7 @@ void alloc_sort(Ctx& c, PopHost& ph) {
     }
     int* d_off = dalloc<int>(o, off.size());
     int* d_list = dalloc<int>(o, list.size());
+    h.cp_cum = dalloc<double>(o, (size_t)off[h.n_cells] + h.n_cells);
     CK(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaStreamSynchronize(c.stream));  // the host vectors go out of scope
@@ -1482,10 +1492,10 @@ void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaSt
     using T = decltype(tt);
     if (flat)
       k_test<KT, T, true><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
-                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
+                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p, c.sdec.p);
     else
       k_test<KT, T, false><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
-                                                   c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
+                                                   c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p, c.sdec.p);
   });
   note_launch();
 }
@@ -1511,9 +1521,9 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
     using T = decltype(tt);
     auto k = flat ? k_items<KT, T, true> : k_items<KT, T, false>;
     k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
-                              c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, pool,
+                              c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p, pool,
                               c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
-                              c.it_done.p);
+                              c.it_done.p, c.it_dec.p);
   });
   note_launch();
 }
@@ -1678,6 +1688,7 @@ __global__ void k_fill_claims(const PopDev* pops) {
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     P.claim[i] = ~0ULL;
+    P.rclaim[i] = ~0ULL;
     P.touched[i] = ~0u;
   }
 }
@@ -1816,6 +1827,11 @@ struct RoundBounds {
 void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long Q) {
   long long W = b.W;
   launch_sort(c, st, b.max_chunks, b.max_cells);
+  {
+    dim3 g((b.max_cells + 127) / 128, c.n_pop);
+    k_walk_rates<<<g, 128, 0, st>>>(c.d_pops);
+    note_launch();
+  }
   launch_items_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
   if (Q > 0) {
     set_n_dev(c, Q);
@@ -1825,9 +1841,9 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
   long long* Ed = c.round_dev.p + 1;
   scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.it_flag.p, W, Id, c.it_off.p, Ed}}, st);
   k_compact_items<<<grid_for(W, 256), 256, 0, st>>>(c.it_flag.p, c.it_off.p, Id, c.it_key.p, c.it_c.p, c.it_gp.p,
-                                                    c.it_pos.p, c.it_len.p, c.it_head.p, c.it_done.p, c.ev_key.p,
-                                                    c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.ev_len.p, c.ev_head.p,
-                                                    c.ev_done.p);
+                                                    c.it_pos.p, c.it_len.p, c.it_head.p, c.it_done.p, c.it_dec.p,
+                                                    c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.ev_len.p,
+                                                    c.ev_head.p, c.ev_done.p, c.dec_set.p);
   note_launch();
   resolve_apply(c, st, W, Q);
 }
@@ -1842,7 +1858,8 @@ std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
           (long long)c.ev_pos.p, (long long)c.ev_dest.p, (long long)c.ev_len.p, (long long)c.ev_head.p,
           (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.it_flag.p, (long long)c.it_key.p,
           (long long)c.it_c.p, (long long)c.it_gp.p, (long long)c.it_pos.p, (long long)c.it_len.p,
-          (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_off.p, (long long)c.ch_y.p,
+          (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_dec.p, (long long)c.it_off.p,
+          (long long)c.ch_y.p,
           (long long)c.ch_q.p, (long long)c.ch_pos.p, (long long)c.need_slot_set.p, (long long)c.need_id_set.p,
           (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p, (long long)c.rank_id_set.p,
           (long long)c.slot_base_set.p, (long long)c.id_base_set.p, (long long)c.slot_base_pp.p,
@@ -1900,6 +1917,7 @@ void reserve_round(Ctx& c, long long W) {
   size_t w = (size_t)std::max<long long>(W, 1);
   c.it_flag.reserve(w + 1); c.it_key.reserve(w + 1); c.it_c.reserve(w + 1); c.it_gp.reserve(w + 1);
   c.it_pos.reserve(w + 1); c.it_len.reserve(w + 1); c.it_head.reserve(w + 1); c.it_done.reserve(w + 1);
+  c.it_dec.reserve(w + 1);
   c.it_off.reserve(w + 2);
 }
 
@@ -2166,6 +2184,7 @@ void step_parallel(Ctx& c, int kt) {
   {
     size_t w = (size_t)W;
     c.flag.reserve(w + 1); c.ev.reserve(w + 1); c.flag_off.reserve(w + 2); c.ev_gp.reserve(w + 1);
+    c.sdec.reserve(w + 1);
     reserve_events(c, W);
     c.need_slot_pp.reserve(Q + 1); c.need_id_pp.reserve(Q + 1); c.win_pp.reserve(Q + 1); c.lost_pp.reserve(Q + 1);
     c.lost_off.reserve(Q + 2); c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
@@ -2193,8 +2212,8 @@ void step_parallel(Ctx& c, int kt) {
     const long long* Wd = c.work_off.p + n_gpairs;
     scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, c.round_dev.p + 1}});
     k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, Wd, c.ev.p, c.ev_gp.p,
-                                                           c.gpair_local.p, c.work_off.p, c.ev_key.p, c.ev_c.p,
-                                                           c.gp_c.p, c.ev_pos.p, c.ev_len.p);
+                                                           c.gpair_local.p, c.work_off.p, c.sdec.p, c.ev_key.p,
+                                                           c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.ev_len.p, c.dec_set.p);
     note_launch();
   }
   resolve_apply(c, c.stream, W, Q);
@@ -2428,6 +2447,8 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   for (auto* b : bk) b->release();
   c.ev_pos.release();
   c.it_pos.release();
+  c.sdec.release();
+  c.it_dec.release();
   c.ch_pos.release();
   c.it_flag.release();
   c.it_done.release();

@@ -552,13 +552,84 @@ __device__ __forceinline__ int find_pair(const long long* off, int n, long long 
   return lo;
 }
 
+// Decisions of coagulate_weighting (coagulation.F90:855-892).
+struct MergeDecision {
+  bool rm1, rm2, create, lost1, lost2;
+  int new_group;  // 1-based
+};
+
+// particle 1 (radius r1, total volume vt1) from the pair's first cell,
+// particle 2 from its second
+template <class R>
+__device__ MergeDecision merge_decide_v(const PopDev& P, R& g, double r1, double vt1, double r2, double vt2, int c1,
+                                        int c2, int cc) {
+  MergeDecision d;
+  double rc = vol2rad(rad2vol(r1) + rad2vol(r2));
+  double nc1 = num_conc_at_radius<double>(P.w, c1, r1);
+  double nc2 = num_conc_at_radius<double>(P.w, c2, r2);
+  double ncc = num_conc_at_radius<double>(P.w, cc, rc);
+  d.new_group = rand_group(g, P.w, cc, rc);
+  double mn = nc1;
+  if (nc2 < mn) mn = nc2;
+  if (ncc < mn) mn = ncc;
+  d.rm1 = g.next() < mn / nc1;
+  d.rm2 = g.next() < mn / nc2;
+  d.create = g.next() < mn / ncc;
+  if (d.create) {
+    d.lost1 = d.lost2 = false;
+    if (d.rm1 && d.rm2) {
+      if (vt1 > vt2) d.lost2 = true;
+      else d.lost1 = true;
+    }
+  } else {
+    d.lost1 = d.rm1;
+    d.lost2 = d.rm2;
+  }
+  return d;
+}
+
+template <class R>
+__device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int c1, int c2, int cc) {
+  return merge_decide_v(P, g, P.rad[s1], P.vtot[s1], P.rad[s2], P.vtot[s2], c1, c2, cc);
+}
+
+// A merge decision and the number of uniforms its stream had used, in one
+// word: bits 0-4 rm1, rm2, create, lost1, lost2; bits 5-7 the new weight
+// group; bits 8-31 the uniforms used.
+__device__ __forceinline__ uint32_t pack_decision(const MergeDecision& m, uint32_t used) {
+  return (m.rm1 ? 1u : 0u) | (m.rm2 ? 2u : 0u) | (m.create ? 4u : 0u) | (m.lost1 ? 8u : 0u) |
+         (m.lost2 ? 16u : 0u) | ((uint32_t)(m.new_group & 7) << 5) | (used << 8);
+}
+__device__ __forceinline__ MergeDecision unpack_decision(uint32_t x, uint32_t* used) {
+  MergeDecision m;
+  m.rm1 = x & 1u;
+  m.rm2 = x & 2u;
+  m.create = x & 4u;
+  m.lost1 = x & 8u;
+  m.lost2 = x & 16u;
+  m.new_group = (int)((x >> 5) & 7u);
+  *used = x >> 8;
+  return m;
+}
+
+// random stream of an event's merge: the pair and the sample for the pair's
+// own samples, the pair and the walking slot for a walk's test
+__device__ __forceinline__ Rng merge_rng(const PopDev& P, unsigned long long key) {
+  uint32_t idx = key_idx(key);
+  if (key_kind(key)) idx |= 0x80000000u;
+  return make_rng(P, kStreamMerge, key_pair(key), idx);
+}
+
 // Per-set pair tests (maybe_coag_pair, coagulation.F90:712-759).  One thread
-// per sample w of the flattened (population, pair, sample) space.
+// per sample w of the flattened (population, pair, sample) space.  An
+// accepted sample draws its merge decision (coagulate_weighting) at once,
+// stores it in dec[w] and claims its two slots by it: a write claim on a slot
+// the merge removes or rewrites, a read claim on one it keeps.
 template <int KT, class T, bool FLAT>
 __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpair_pop,
                                               const int* gpair_local, const long long* work_off,
                                               int n_gpairs, const long long* total, uint8_t* flag,
-                                              int2* ev, int* ev_gp) {
+                                              int2* ev, int* ev_gp, uint32_t* dec) {
   long long W = *total;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < W;
        w += (long long)gridDim.x * blockDim.x) {
@@ -614,8 +685,13 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
     flag[w] = acc ? 1 : 0;
     if (acc) {
       unsigned long long key = make_key((uint32_t)p, 0u, (uint32_t)s);
-      atomicMin(&P.claim[s1], claim_key(P, key));
-      atomicMin(&P.claim[s2], claim_key(P, key));
+      unsigned long long ck = claim_key(P, key);
+      Rng gm = merge_rng(P, key);
+      MergeDecision m = merge_decide(P, gm, s1, s2, d.c1, d.c2, S.cc);
+      if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+      dec[w] = pack_decision(m, gm.used());
+      claim_slot(P, s1, ck, m.rm1);
+      claim_slot(P, s2, ck, m.rm2);
       ev[w] = make_int2(s1, s2);
       ev_gp[w] = gp;
     }

@@ -19,10 +19,13 @@ namespace pmc {
 // kChainChunk - 1 of a chunk's y holds the index of the next chunk (-1: none)
 constexpr int kChainChunk = 32;
 constexpr int kChainMaxLen = 1 << 16;  // events of one chain in one round
+// q of an entry: the pair, and kChainRemoves if the merge removes the partner
+constexpr int kChainPairMask = (1 << 20) - 1;
+constexpr int kChainRemoves = 1 << 30;
 
 struct ChainPool {
   int* y;          // [n_chunks * kChainChunk] partner slot; the last entry of a chunk links the next chunk
-  int* q;          // pair (local)
+  int* q;          // pair (local), with kChainRemoves if the merge removes the partner
   float* pos;      // position in the pair's test sequence
   long long* ctr;  // chunks handed out in this round (device)
   long long n_chunks;
@@ -71,81 +74,14 @@ __device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
   P.cell[i] = -1;
 }
 
-// Decisions of coagulate_weighting (coagulation.F90:855-892).
-struct MergeDecision {
-  bool rm1, rm2, create, lost1, lost2;
-  int new_group;  // 1-based
-};
-
-// particle 1 (radius r1, total volume vt1) from the pair's first cell,
-// particle 2 from its second
-template <class R>
-__device__ MergeDecision merge_decide_v(const PopDev& P, R& g, double r1, double vt1, double r2, double vt2, int c1,
-                                        int c2, int cc) {
-  MergeDecision d;
-  double rc = vol2rad(rad2vol(r1) + rad2vol(r2));
-  double nc1 = num_conc_at_radius<double>(P.w, c1, r1);
-  double nc2 = num_conc_at_radius<double>(P.w, c2, r2);
-  double ncc = num_conc_at_radius<double>(P.w, cc, rc);
-  d.new_group = rand_group(g, P.w, cc, rc);
-  double mn = nc1;
-  if (nc2 < mn) mn = nc2;
-  if (ncc < mn) mn = ncc;
-  d.rm1 = g.next() < mn / nc1;
-  d.rm2 = g.next() < mn / nc2;
-  d.create = g.next() < mn / ncc;
-  if (d.create) {
-    d.lost1 = d.lost2 = false;
-    if (d.rm1 && d.rm2) {
-      if (vt1 > vt2) d.lost2 = true;
-      else d.lost1 = true;
-    }
-  } else {
-    d.lost1 = d.rm1;
-    d.lost2 = d.rm2;
-  }
-  return d;
-}
-
-template <class R>
-__device__ MergeDecision merge_decide(const PopDev& P, R& g, int s1, int s2, int c1, int c2, int cc) {
-  return merge_decide_v(P, g, P.rad[s1], P.vtot[s1], P.rad[s2], P.vtot[s2], c1, c2, cc);
-}
-
-// A merge decision and the number of uniforms its stream had used, in one
-// word: bits 0-4 rm1, rm2, create, lost1, lost2; bits 5-7 the new weight
-// group; bits 8-31 the uniforms used.
-__device__ __forceinline__ uint32_t pack_decision(const MergeDecision& m, uint32_t used) {
-  return (m.rm1 ? 1u : 0u) | (m.rm2 ? 2u : 0u) | (m.create ? 4u : 0u) | (m.lost1 ? 8u : 0u) |
-         (m.lost2 ? 16u : 0u) | ((uint32_t)(m.new_group & 7) << 5) | (used << 8);
-}
-__device__ __forceinline__ MergeDecision unpack_decision(uint32_t x, uint32_t* used) {
-  MergeDecision m;
-  m.rm1 = x & 1u;
-  m.rm2 = x & 2u;
-  m.create = x & 4u;
-  m.lost1 = x & 8u;
-  m.lost2 = x & 16u;
-  m.new_group = (int)((x >> 5) & 7u);
-  *used = x >> 8;
-  return m;
-}
-
-// random stream of an event's merge: the pair and the sample for the pair's
-// own samples, the pair and the walking slot for a walk's test
-__device__ __forceinline__ Rng merge_rng(const PopDev& P, unsigned long long key) {
-  uint32_t idx = key_idx(key);
-  if (key_kind(key)) idx |= 0x80000000u;
-  return make_rng(P, kStreamMerge, key_pair(key), idx);
-}
-
 // Resolve the events of a round: winner test, slot/id needs.  Event e has
-// key ev_key[e], slots ev[e] and global pair ev_gp[e]; the events are
-// ordered by population.  A winning chain (ev_len[e] > 0) gets win 2 and the
-// number of its events whose claims hold (ev_app[e]).
+// key ev_key[e], slots ev[e], global pair ev_gp[e] and merge decision dec[e]
+// (drawn when the event was formed); the events are ordered by population.
+// A winning chain (ev_len[e] > 0) gets win 2 and the number of its events
+// whose claims hold (ev_app[e]).
 __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const long long* n_events,
                               const unsigned long long* ev_key, const int2* ev, const int* ev_gp, int* need_slot,
-                              int* need_id, uint8_t* win, uint32_t* dec, long long* n_losers, const int* ev_len,
+                              int* need_id, uint8_t* win, const uint32_t* dec, long long* n_losers, const int* ev_len,
                               const int* ev_head, int* ev_app, ChainPool pool) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
@@ -162,8 +98,10 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const lo
       bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
       continue;
     }
+    uint32_t used;
+    MergeDecision m = unpack_decision(dec[e], &used);
     unsigned long long ck = claim_key(P, key);
-    bool winner = P.claim[sl.x] == ck && P.claim[sl.y] == ck;
+    bool winner = holds_slot(P, sl.x, ck, m.rm1) && holds_slot(P, sl.y, ck, m.rm2);
     if (!winner) {
       add_ll(n_losers, 1);
       continue;
@@ -178,9 +116,10 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const lo
       for (int i = 0; i < len; i++) {
         long long ix = rd.next(pool);
         if (ix < 0) break;
-        int y = pool.y[ix], q = pool.q[ix];
+        int y = pool.y[ix], qw = pool.q[ix];
+        int q = qw & kChainPairMask;
         if (y < 0 || y >= P.cap || q < 0 || q >= P.n_pairs) break;
-        if (P.claim[y] != claim_key(P, make_key((uint32_t)q, 1u, x))) break;
+        if (!holds_slot(P, y, claim_key(P, make_key((uint32_t)q, 1u, x)), (qw & kChainRemoves) != 0)) break;
         app++;
       }
       ev_app[e] = app;
@@ -188,12 +127,6 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const lo
       continue;
     }
     win[e] = 1;
-    PairDesc d = P.pair_desc[p];
-    const PairState& S = P.pair[p];
-    Rng g = merge_rng(P, key);
-    MergeDecision m = merge_decide(P, g, sl.x, sl.y, d.c1, d.c2, S.cc);
-    if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
-    dec[e] = pack_decision(m, g.used());
     if (m.create) {
       need_slot[e] = (!m.rm1 && !m.rm2) ? 1 : 0;
       bool keep1 = m.rm1 && !m.lost1, keep2 = m.rm2 && !m.lost2;
@@ -436,6 +369,7 @@ struct WalkOut {
   int chain_len = 0;        // events in the chain (0: the first event alone)
   int chain_head = -1;
   bool done = false;        // the walk ran to the end after its last event
+  uint32_t dec = 0;         // merge decision of the first event
 };
 
 // true if this round's claim on slot y is the chain of walker x
@@ -459,11 +393,12 @@ __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, floa
   ChainWriter cw;
   Rng g = make_rng(P, kStreamWalk, 0u, (uint32_t)x);
   long long n_tests = 0, n_iter = 0;
-  double t = -log(g.next());  // distance to the next test, in expected tests
   bool stop = false;
   while (!stop) {
-    // pairs of cell C from (p0, pos0) on
+    // the pairs of cell C from (p0, pos0) on, as one stretch of expected
+    // tests: cum[j] over the cell's pairs (cp_cum)
     int lo = P.cp_off[C], end = P.cp_off[C + 1];
+    const double* cum = P.cp_cum + (P.cp_off[C] + C) - lo;  // cum[j], j = lo..end
     {
       int hi = end;
       while (lo < hi) {
@@ -472,11 +407,34 @@ __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, floa
         else hi = mid;
       }
     }
+    double at = cum[lo];
+    if (lo < end && P.cp_list[lo] == p0) at += (cum[lo + 1] - cum[lo]) * (double)pos0;
+    const double at_end = cum[end];
+    int j = lo;
     bool moved = false;
-    for (int j = lo; j < end && !stop && !moved; j++) {
+    for (;;) {
+      at += -log(g.next());
+      if (!(at < at_end)) break;  // no test left in the cell's later pairs
+      if (++n_iter > (1LL << 26)) {  // far past any mean the step can ask for
+        set_status(P.ctr, kErrTimeout);
+        stop = true;
+        break;
+      }
+      {
+        // the pair whose stretch holds at: cum[j] <= at < cum[j + 1]
+        int a = j, b = end - 1;
+        while (a < b) {
+          int mid = (a + b + 1) >> 1;
+          if (cum[mid] <= at) a = mid;
+          else b = mid - 1;
+        }
+        j = a;
+      }
       int q = P.cp_list[j];
+      double lam = cum[j + 1] - cum[j];
+      if (!(lam > 0.0)) continue;
+      double pos = (at - cum[j]) / lam;
       const PairState& S = P.pair[q];
-      if (S.path == kPathParticle) continue;
       PairDesc d = P.pair_desc[q];
       int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
       int O = cell1 == C ? cell2 : cell1;
@@ -488,100 +446,89 @@ __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, floa
         stop = true;
         break;
       }
-      double lam = S.k_max * P.del_t * (double)n_o;  // expected tests over the whole pair
-      if (!(lam > 0.0)) continue;
-      double pos = q == p0 ? (double)pos0 : 0.0;
-      for (;;) {
-        double adv = t / lam;
-        if (pos + adv >= 1.0) {
-          t -= lam * (1.0 - pos);
-          break;
-        }
-        pos += adv;
-        t = -log(g.next());
-        if (++n_iter > (1LL << 26)) {  // far past any mean the step can ask for
-          set_status(P.ctr, kErrTimeout);
+      int i = (int)(g.next() * (double)n_o);
+      if (i >= n_o) i = n_o - 1;
+      int y = P.list[o_start + i];
+      if (y < 0 || y >= P.cap) {
+        bad_index(P.ctr, kBadTestSlot, y);
+        continue;
+      }
+      if (y == x || !P.alive[y] || P.cell[y] != O) continue;
+      if (cw.len > 0 && claimed_by_walk(P, y, x)) continue;  // absorbed earlier in this chain
+      n_tests++;
+      bool first = cell1 == C;
+      T k;
+      if constexpr (sizeof(T) == 8) {
+        const double* qw = (const double*)&rec;
+        const double* qy = (const double*)&P.recd[y];
+        k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat,
+                                             P.coeff);
+      } else {
+        const float* qw = (const float*)&recf;
+        const float* qy = (const float*)&P.recf[y];
+        k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc,
+                                            (float)S.fflat, (float)P.coeff);
+      }
+      T prob = k * (T)S.inv_k_max;
+      if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
+      if (!((T)g.next() < prob)) continue;
+      // an accepted test: its merge decision; an absorb replaces the walking
+      // particle by the coagulated one
+      unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
+      unsigned long long ck = claim_key(P, key);
+      Rng gm = cw.len == 0 ? merge_rng(P, key) : make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
+      double ry = P.rad[y], vty = P.vtot[y];
+      MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
+                              : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
+      bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
+      bool absorb = m.create && rm_x && m.new_group != 0;
+      int qw = q | (rm_y ? kChainRemoves : 0);
+      if (!out->found) {
+        // the first event: claimed whatever follows
+        out->found = true;
+        out->q = q;
+        out->y = y;
+        out->pos = (float)pos;
+        out->first_cell1 = first;
+        out->dec = pack_decision(m, gm.used());
+        if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+        claim_slot(P, x, ck, rm_x);
+        claim_slot(P, y, ck, rm_y);
+        if (!absorb || !cw.append(pool, y, qw, (float)pos)) {  // the first event alone
           stop = true;
           break;
         }
-        int i = (int)(g.next() * (double)n_o);
-        if (i >= n_o) i = n_o - 1;
-        int y = P.list[o_start + i];
-        if (y < 0 || y >= P.cap) {
-          bad_index(P.ctr, kBadTestSlot, y);
-          continue;
-        }
-        if (y == x || !P.alive[y] || P.cell[y] != O) continue;
-        if (cw.len > 0 && claimed_by_walk(P, y, x)) continue;  // absorbed earlier in this chain
-        n_tests++;
-        bool first = cell1 == C;
-        T k;
-        if constexpr (sizeof(T) == 8) {
-          const double* qw = (const double*)&rec;
-          const double* qy = (const double*)&P.recd[y];
-          k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat,
-                                               P.coeff);
-        } else {
-          const float* qw = (const float*)&recf;
-          const float* qy = (const float*)&P.recf[y];
-          k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc,
-                                              (float)S.fflat, (float)P.coeff);
-        }
-        T prob = k * (T)S.inv_k_max;
-        if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
-        if (!((T)g.next() < prob)) continue;
-        // an accepted test: would its merge replace the walking particle?
-        unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
-        Rng gm = cw.len == 0 ? merge_rng(P, key) : make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
-        double ry = P.rad[y], vty = P.vtot[y];
-        MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
-                                : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
-        bool absorb = m.create && (first ? m.rm1 : m.rm2) && m.new_group != 0;
-        if (!out->found) {
-          // the first event: claimed whatever follows
-          out->found = true;
-          out->q = q;
-          out->y = y;
-          out->pos = (float)pos;
-          out->first_cell1 = first;
-          atomicMin(&P.claim[x], claim_key(P, key));
-          atomicMin(&P.claim[y], claim_key(P, key));
-          if (!absorb || !cw.append(pool, y, q, (float)pos)) {  // the first event alone
-            stop = true;
-            break;
-          }
-          for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
-        } else {
-          // the chain ends before an event that is no absorb, or when the
-          // pool is full; the walk resumes there in the next round
-          if (!absorb || !cw.append(pool, y, q, (float)pos)) {
-            stop = true;
-            break;
-          }
-          atomicMin(&P.claim[y], claim_key(P, key));
-        }
-        // absorb y: the coagulated particle's volumes, radius, class, record
-        double s_v = 0.0, s_m = 0.0;
-        for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
-        for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
-        for (int s = 0; s < P.n_spec; s++) s_m = s_m + vcur[s] * P.density[s];
-        vt = s_v;
-        r = vol2rad(vt);
-        int cls = S.cc + 1;
-        rec = make_rec_v(P, r, vt, s_m, cls);
-        recf = to_f32(rec);
-        int C2 = cell_of(P, r, cls);
-        if (C2 < 0 || cw.len >= kChainMaxLen) {  // off the grid (reported by the apply) or long enough
+        for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
+      } else {
+        // the chain ends before an event that is no absorb, or when the
+        // pool is full; the walk resumes there in the next round
+        if (!absorb || !cw.append(pool, y, qw, (float)pos)) {
           stop = true;
           break;
         }
-        if (C2 != C) {
-          C = C2;
-          p0 = q;
-          pos0 = (float)pos;
-          moved = true;
-          break;
-        }
+        claim_slot(P, y, ck, rm_y);
+      }
+      // absorb y: the coagulated particle's volumes, radius, class, record
+      double s_v = 0.0, s_m = 0.0;
+      for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
+      for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
+      for (int s = 0; s < P.n_spec; s++) s_m = s_m + vcur[s] * P.density[s];
+      vt = s_v;
+      r = vol2rad(vt);
+      int cls = S.cc + 1;
+      rec = make_rec_v(P, r, vt, s_m, cls);
+      recf = to_f32(rec);
+      int C2 = cell_of(P, r, cls);
+      if (C2 < 0 || cw.len >= kChainMaxLen) {  // off the grid (reported by the apply) or long enough
+        stop = true;
+        break;
+      }
+      if (C2 != C) {
+        C = C2;
+        p0 = q;
+        pos0 = (float)pos;
+        moved = true;
+        break;
       }
     }
     if (!moved && !stop) {
@@ -615,9 +562,10 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
                                                const long long* pop_pair_base, int n_gpairs, const long long* n_items,
                                                const uint8_t* win, const int* dest,
                                                const unsigned long long* ev_key, const int2* ev_c,
-                                               const int* gp_c, const float* ev_pos, ChainPool pool,
-                                               uint8_t* it_flag, unsigned long long* it_key, int2* it_c, int* it_gp,
-                                               float* it_pos, int* it_len, int* it_head, uint8_t* it_done) {
+                                               const int* gp_c, const float* ev_pos, const uint32_t* dec,
+                                               ChainPool pool, uint8_t* it_flag, unsigned long long* it_key,
+                                               int2* it_c, int* it_gp, float* it_pos, int* it_len, int* it_head,
+                                               uint8_t* it_done, uint32_t* it_dec) {
   long long n = *n_items;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
@@ -659,6 +607,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     }
     int len = 0, head = -1;
     bool done = false;
+    uint32_t dc = dec[e];
     if (walker >= 0) {
       WalkOut w;
       walk<KT, T, FLAT>(P, pool, walker, p0, pos0, &w);
@@ -670,9 +619,14 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
       len = w.chain_len;
       head = w.chain_head;
       done = w.done;
+      dc = w.dec;
     } else {
-      atomicMin(&P.claim[sl.x], claim_key(P, key));
-      atomicMin(&P.claim[sl.y], claim_key(P, key));
+      // a retry keeps its merge decision and claims by it
+      uint32_t used;
+      MergeDecision m = unpack_decision(dc, &used);
+      unsigned long long ck = claim_key(P, key);
+      claim_slot(P, sl.x, ck, m.rm1);
+      claim_slot(P, sl.y, ck, m.rm2);
     }
     it_flag[e] = 1;
     it_key[e] = key;
@@ -682,6 +636,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     it_len[e] = len;
     it_head[e] = head;
     it_done[e] = done ? 1 : 0;
+    it_dec[e] = dc;
   }
 }
 
@@ -726,8 +681,8 @@ __global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const lo
         bad_index(P.ctr, kBadEventSlot, -1);
         break;
       }
-      int y = pool.y[ix], q = pool.q[ix];
-      if (y < 0 || y >= P.cap || q < 0 || q >= P.n_pairs) {
+      int y = pool.y[ix], q = pool.q[ix] & kChainPairMask;
+      if (y < 0 || y >= P.cap || q >= P.n_pairs) {
         bad_index(P.ctr, kBadEventSlot, y);
         break;
       }
@@ -786,6 +741,31 @@ __global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const lo
     gp_c[e] = (int)(pop_pair_base[pop] + last_q);
     ev_pos[e] = last_pos;
   }
+}
+
+// Walk rates after a round's sort: for every cell, the running sum over its
+// pairs (loop order) of k_max * del_t * members of the pair's other cell;
+// pairs on the per-particle path add nothing.  One thread per cell.
+__global__ void k_walk_rates(const PopDev* pops) {
+  const PopDev& P = pops[blockIdx.y];
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= P.n_cells || P.n_pairs == 0) return;
+  const int nb = P.grid->n_bin;
+  int lo = P.cp_off[c], hi = P.cp_off[c + 1];
+  double* cum = P.cp_cum + lo + c;
+  double acc = 0.0;
+  for (int j = lo; j < hi; j++) {
+    cum[j - lo] = acc;
+    int q = P.cp_list[j];
+    const PairState& S = P.pair[q];
+    if (S.path == kPathParticle) continue;
+    PairDesc d = P.pair_desc[q];
+    int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
+    int O = cell1 == c ? cell2 : cell1;
+    double lam = S.k_max * P.del_t * (double)P.cell_count[O];
+    if (lam > 0.0) acc += lam;
+  }
+  cum[hi - lo] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1019,8 +999,8 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
     const PPResult& R = res[q];
     unsigned long long prio = op_key[q];
     bool ok = true;
-    if (R.merged) ok = ok && P.claim[R.target] == claim_key(P, prio);
-    for (int z = 0; z < R.n_rm; z++) ok = ok && P.claim[R.rm[z]] == claim_key(P, prio);
+    if (R.merged) ok = ok && holds_slot(P, R.target, claim_key(P, prio), true);
+    for (int z = 0; z < R.n_rm; z++) ok = ok && holds_slot(P, R.rm[z], claim_key(P, prio), true);
     win[q] = ok ? 1 : 0;
     lost[q] = ok ? 0 : 1;
     int extra = (ok && R.merged && R.n_copies > 1) ? R.n_copies - 1 : 0;

@@ -186,11 +186,20 @@ struct PopDev {
   // are cp_list[cp_off[c] .. cp_off[c + 1])
   const int* cp_off;   // [n_cells + 1]
   const int* cp_list;  // [cp_off[n_cells]]
+  // walk rates, brought up to date after each later round's sort: the
+  // segment of cell c, cp_cum[cp_off[c] + c + j] for j = 0..len, holds the
+  // expected walk tests (k_max * del_t * members of the other cell) of the
+  // cell's first j pairs
+  double* cp_cum;      // [cp_off[n_cells] + n_cells]
 
-  // [cap] lowest claim key of the current round (claim_key), so a key from
+  // [cap] lowest claim key (claim_key) of the current round's events that
+  // remove or rewrite the slot, and of those that only read it; a key from
   // any earlier round is larger and is replaced by the first claim of this
-  // round; no per-round reset is needed
+  // round, so no per-round reset is needed.  An event that writes a slot
+  // wins it if it holds the write claim and no earlier event reads it; an
+  // event that reads a slot wins it if no earlier event writes it.
   unsigned long long* claim;
+  unsigned long long* rclaim;
   // [cap] claim generation of the round that last removed or rewrote the
   // slot: an event that lost a claim in round r is retried in round r + 1
   // only if neither of its particles was consumed in round r
@@ -224,6 +233,15 @@ constexpr uint32_t kGenLimit = 2047;
 // a smaller word, so the first claim of a round replaces any older one
 __device__ __forceinline__ unsigned long long claim_key(const PopDev& P, unsigned long long key) {
   return ((unsigned long long)(~*P.gen_p & kGenLimit) << 53) | key;
+}
+
+// an event's claim on slot s: a write claim if it removes or rewrites s,
+// else a read claim; and whether it holds s after every claim of the round
+__device__ __forceinline__ void claim_slot(const PopDev& P, int s, unsigned long long ck, bool write) {
+  atomicMin(write ? &P.claim[s] : &P.rclaim[s], ck);
+}
+__device__ __forceinline__ bool holds_slot(const PopDev& P, int s, unsigned long long ck, bool write) {
+  return write ? (P.claim[s] == ck && P.rclaim[s] > ck) : P.claim[s] > ck;
 }
 #endif
 
