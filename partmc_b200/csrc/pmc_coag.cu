@@ -790,7 +790,7 @@ struct Ctx {
   DevBuf<int2> it_c;
   DevBuf<int> it_gp, it_len, it_head;
   DevBuf<float> it_pos;
-  DevBuf<uint32_t> it_dec;
+  DevBuf<uint32_t> it_dec, it_gused;
   DevBuf<long long> it_off;
   // chain events of a round (ChainPool), in chunks
   DevBuf<int> ch_y, ch_q;
@@ -1523,8 +1523,13 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
     k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
                               c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p, pool,
                               c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
-                              c.it_done.p, c.it_dec.p);
+                              c.it_done.p, c.it_dec.p, c.it_gused.p);
+    auto kc = flat ? k_chain<KT, T, true> : k_chain<KT, T, false>;
+    kc<<<grid_for(W, 128), 128, 0, st>>>(c.d_pops, c.gpair_pop.p, n_items, c.it_flag.p, c.it_key.p, c.it_c.p,
+                                         c.it_gp.p, c.it_pos.p, c.it_dec.p, c.it_gused.p, pool, c.it_len.p,
+                                         c.it_head.p, c.it_done.p);
   });
+  note_launch();
   note_launch();
 }
 
@@ -1797,7 +1802,7 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
                                                   c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_dest.p);
     note_launch();
     // chains, one thread each
-    k_apply_chain<<<grid_for(W, 128), 128, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, Ed, c.ev_key.p,
+    k_apply_chain<<<grid_for(W * 32, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, Ed, c.ev_key.p,
                                                     c.win_set.p, c.ev_len.p, c.ev_app.p, c.ev_head.p, c.ev_done.p,
                                                     pool, c.gp_c.p, c.ev_pos.p, c.ev_dest.p);
     note_launch();
@@ -1828,7 +1833,7 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
   long long W = b.W;
   launch_sort(c, st, b.max_chunks, b.max_cells);
   {
-    dim3 g((b.max_cells + 127) / 128, c.n_pop);
+    dim3 g(b.max_cells, c.n_pop);
     k_walk_rates<<<g, 128, 0, st>>>(c.d_pops);
     note_launch();
   }
@@ -1858,7 +1863,7 @@ std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
           (long long)c.ev_pos.p, (long long)c.ev_dest.p, (long long)c.ev_len.p, (long long)c.ev_head.p,
           (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.it_flag.p, (long long)c.it_key.p,
           (long long)c.it_c.p, (long long)c.it_gp.p, (long long)c.it_pos.p, (long long)c.it_len.p,
-          (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_dec.p, (long long)c.it_off.p,
+          (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_dec.p, (long long)c.it_gused.p, (long long)c.it_off.p,
           (long long)c.ch_y.p,
           (long long)c.ch_q.p, (long long)c.ch_pos.p, (long long)c.need_slot_set.p, (long long)c.need_id_set.p,
           (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p, (long long)c.rank_id_set.p,
@@ -1917,7 +1922,7 @@ void reserve_round(Ctx& c, long long W) {
   size_t w = (size_t)std::max<long long>(W, 1);
   c.it_flag.reserve(w + 1); c.it_key.reserve(w + 1); c.it_c.reserve(w + 1); c.it_gp.reserve(w + 1);
   c.it_pos.reserve(w + 1); c.it_len.reserve(w + 1); c.it_head.reserve(w + 1); c.it_done.reserve(w + 1);
-  c.it_dec.reserve(w + 1);
+  c.it_dec.reserve(w + 1); c.it_gused.reserve(w + 1);
   c.it_off.reserve(w + 2);
 }
 
@@ -2449,6 +2454,7 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.it_pos.release();
   c.sdec.release();
   c.it_dec.release();
+  c.it_gused.release();
   c.ch_pos.release();
   c.it_flag.release();
   c.it_done.release();

@@ -370,6 +370,8 @@ struct WalkOut {
   int chain_head = -1;
   bool done = false;        // the walk ran to the end after its last event
   uint32_t dec = 0;         // merge decision of the first event
+  bool cont = false;        // the first event is an absorb: k_chain carries the walk on
+  uint32_t g_used = 0;      // uniforms the walk's stream had used at the first event
 };
 
 // true if this round's claim on slot y is the chain of walker x
@@ -379,165 +381,250 @@ __device__ __forceinline__ bool claimed_by_walk(const PopDev& P, int y, int x) {
          (uint32_t)w == (uint32_t)x;
 }
 
+// The rest of a chain after its first absorb (kept out of line: the chain's
+// state, the coagulated particle's volumes and record, stays out of the
+// walk's registers).  Continues the Poisson process of g along the pairs of
+// the coagulated particle's cell from (q, pos); returns the walk's end state.
+template <int KT, class T, bool FLAT>
+__device__ void walk_chain(const PopDev& P, const ChainPool& pool, int x, int y1, int q, double pos,
+                                        int cls, Rng& g, ChainWriter& cw, WalkOut* out, long long* n_tests_io) {
+  const int nb = P.grid->n_bin;
+  double vcur[kMaxSpec];
+  double vt, r;
+  RecD rec;
+  RecF recf;
+  long long n_tests = *n_tests_io, n_iter = 0;
+  int y = y1;
+  int C = -1, p0 = q;
+  float pos0 = (float)pos;
+  for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
+  bool stop = false;
+  for (;;) {
+    // absorb y: the coagulated particle's volumes, radius, class, record
+    double s_v = 0.0, s_m = 0.0;
+    for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
+    for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
+    for (int s = 0; s < P.n_spec; s++) s_m = s_m + vcur[s] * P.density[s];
+    vt = s_v;
+    r = vol2rad(vt);
+    rec = make_rec_v(P, r, vt, s_m, cls);
+    recf = to_f32(rec);
+    C = cell_of(P, r, cls);
+    if (C < 0 || cw.len >= kChainMaxLen) break;  // off the grid (reported by the apply) or long enough
+    // the next accepted test of the coagulated particle
+    bool found = false, moved = true;
+    while (moved && !stop && !found) {
+      moved = false;
+      int lo = P.cp_off[C], end = P.cp_off[C + 1];
+      const double* cum = P.cp_cum + (P.cp_off[C] + C) - lo;
+      {
+        int hi = end;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (P.cp_list[mid] < p0) lo = mid + 1;
+          else hi = mid;
+        }
+      }
+      double at = cum[lo];
+      if (lo < end && P.cp_list[lo] == p0) at += (cum[lo + 1] - cum[lo]) * (double)pos0;
+      const double at_end = cum[end];
+      int j = lo;
+      for (;;) {
+        at += -log(g.next());
+        if (!(at < at_end)) {
+          out->done = true;  // every later pair of the cell was walked
+          stop = true;
+          break;
+        }
+        if (++n_iter > (1LL << 26)) {
+          set_status(P.ctr, kErrTimeout);
+          stop = true;
+          break;
+        }
+        {
+          int a = j, b = end - 1;
+          while (a < b) {
+            int mid = (a + b + 1) >> 1;
+            if (cum[mid] <= at) a = mid;
+            else b = mid - 1;
+          }
+          j = a;
+        }
+        int qq = P.cp_list[j];
+        double lam = cum[j + 1] - cum[j];
+        if (!(lam > 0.0)) continue;
+        double pp = (at - cum[j]) / lam;
+        const PairState& S = P.pair[qq];
+        PairDesc d = P.pair_desc[qq];
+        int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
+        int O = cell1 == C ? cell2 : cell1;
+        int n_o = P.cell_count[O];
+        int o_start = P.cell_start[O];
+        if (n_o < 1) continue;
+        if (o_start < 0 || (long long)o_start + n_o > P.cap) {
+          bad_index(P.ctr, kBadPairCells, qq);
+          stop = true;
+          break;
+        }
+        int i = (int)(g.next() * (double)n_o);
+        if (i >= n_o) i = n_o - 1;
+        int yy = P.list[o_start + i];
+        if (yy < 0 || yy >= P.cap) {
+          bad_index(P.ctr, kBadTestSlot, yy);
+          continue;
+        }
+        if (yy == x || !P.alive[yy] || P.cell[yy] != O) continue;
+        if (claimed_by_walk(P, yy, x)) continue;  // absorbed earlier in this chain
+        n_tests++;
+        bool first = cell1 == C;
+        T k;
+        if constexpr (sizeof(T) == 8) {
+          const double* qw = (const double*)&rec;
+          const double* qy = (const double*)&P.recd[yy];
+          k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat,
+                                               P.coeff);
+        } else {
+          const float* qw = (const float*)&recf;
+          const float* qy = (const float*)&P.recf[yy];
+          k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc,
+                                              (float)S.fflat, (float)P.coeff);
+        }
+        T prob = k * (T)S.inv_k_max;
+        if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
+        if (!((T)g.next() < prob)) continue;
+        // the chain ends before an event that is no absorb, or when the pool
+        // is full; the walk resumes there in the next round
+        unsigned long long key = make_key((uint32_t)qq, 1u, (uint32_t)x);
+        Rng gm = make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
+        double ry = P.rad[yy], vty = P.vtot[yy];
+        MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
+                                : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
+        bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
+        if (!(m.create && rm_x && m.new_group != 0) ||
+            !cw.append(pool, yy, qq | (rm_y ? kChainRemoves : 0), (float)pp)) {
+          stop = true;
+          break;
+        }
+        claim_slot(P, yy, claim_key(P, key), rm_y);
+        y = yy;
+        cls = S.cc + 1;
+        p0 = qq;
+        pos0 = (float)pp;
+        found = true;
+        break;
+      }
+    }
+    if (stop || !found) break;
+  }
+  *n_tests_io = n_tests;
+}
+
 template <int KT, class T, bool FLAT>
 __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, float pos0, WalkOut* out) {
   if (x < 0 || x >= P.cap || !P.alive[x]) return;
-  int C = P.cell[x];
+  const int C = P.cell[x];
   if (C < 0 || C >= P.n_cells) return;
   const int nb = P.grid->n_bin;
-  // the walking particle: its record, and in a chain its summed volumes
-  double r = P.rad[x], vt = P.vtot[x];
-  RecD rec = P.recd[x];
-  RecF recf = P.recf[x];
-  double vcur[kMaxSpec];
-  ChainWriter cw;
   Rng g = make_rng(P, kStreamWalk, 0u, (uint32_t)x);
   long long n_tests = 0, n_iter = 0;
-  bool stop = false;
-  while (!stop) {
-    // the pairs of cell C from (p0, pos0) on, as one stretch of expected
-    // tests: cum[j] over the cell's pairs (cp_cum)
-    int lo = P.cp_off[C], end = P.cp_off[C + 1];
-    const double* cum = P.cp_cum + (P.cp_off[C] + C) - lo;  // cum[j], j = lo..end
-    {
-      int hi = end;
-      while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (P.cp_list[mid] < p0) lo = mid + 1;
-        else hi = mid;
-      }
-    }
-    double at = cum[lo];
-    if (lo < end && P.cp_list[lo] == p0) at += (cum[lo + 1] - cum[lo]) * (double)pos0;
-    const double at_end = cum[end];
-    int j = lo;
-    bool moved = false;
-    for (;;) {
-      at += -log(g.next());
-      if (!(at < at_end)) break;  // no test left in the cell's later pairs
-      if (++n_iter > (1LL << 26)) {  // far past any mean the step can ask for
-        set_status(P.ctr, kErrTimeout);
-        stop = true;
-        break;
-      }
-      {
-        // the pair whose stretch holds at: cum[j] <= at < cum[j + 1]
-        int a = j, b = end - 1;
-        while (a < b) {
-          int mid = (a + b + 1) >> 1;
-          if (cum[mid] <= at) a = mid;
-          else b = mid - 1;
-        }
-        j = a;
-      }
-      int q = P.cp_list[j];
-      double lam = cum[j + 1] - cum[j];
-      if (!(lam > 0.0)) continue;
-      double pos = (at - cum[j]) / lam;
-      const PairState& S = P.pair[q];
-      PairDesc d = P.pair_desc[q];
-      int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
-      int O = cell1 == C ? cell2 : cell1;
-      int n_o = P.cell_count[O];
-      int o_start = P.cell_start[O];
-      if (n_o < 1) continue;
-      if (o_start < 0 || (long long)o_start + n_o > P.cap) {
-        bad_index(P.ctr, kBadPairCells, q);
-        stop = true;
-        break;
-      }
-      int i = (int)(g.next() * (double)n_o);
-      if (i >= n_o) i = n_o - 1;
-      int y = P.list[o_start + i];
-      if (y < 0 || y >= P.cap) {
-        bad_index(P.ctr, kBadTestSlot, y);
-        continue;
-      }
-      if (y == x || !P.alive[y] || P.cell[y] != O) continue;
-      if (cw.len > 0 && claimed_by_walk(P, y, x)) continue;  // absorbed earlier in this chain
-      n_tests++;
-      bool first = cell1 == C;
-      T k;
-      if constexpr (sizeof(T) == 8) {
-        const double* qw = (const double*)&rec;
-        const double* qy = (const double*)&P.recd[y];
-        k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat,
-                                             P.coeff);
-      } else {
-        const float* qw = (const float*)&recf;
-        const float* qy = (const float*)&P.recf[y];
-        k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc,
-                                            (float)S.fflat, (float)P.coeff);
-      }
-      T prob = k * (T)S.inv_k_max;
-      if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
-      if (!((T)g.next() < prob)) continue;
-      // an accepted test: its merge decision; an absorb replaces the walking
-      // particle by the coagulated one
-      unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
-      unsigned long long ck = claim_key(P, key);
-      Rng gm = cw.len == 0 ? merge_rng(P, key) : make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
-      double ry = P.rad[y], vty = P.vtot[y];
-      MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
-                              : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
-      bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
-      bool absorb = m.create && rm_x && m.new_group != 0;
-      int qw = q | (rm_y ? kChainRemoves : 0);
-      if (!out->found) {
-        // the first event: claimed whatever follows
-        out->found = true;
-        out->q = q;
-        out->y = y;
-        out->pos = (float)pos;
-        out->first_cell1 = first;
-        out->dec = pack_decision(m, gm.used());
-        if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
-        claim_slot(P, x, ck, rm_x);
-        claim_slot(P, y, ck, rm_y);
-        if (!absorb || !cw.append(pool, y, qw, (float)pos)) {  // the first event alone
-          stop = true;
-          break;
-        }
-        for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
-      } else {
-        // the chain ends before an event that is no absorb, or when the
-        // pool is full; the walk resumes there in the next round
-        if (!absorb || !cw.append(pool, y, qw, (float)pos)) {
-          stop = true;
-          break;
-        }
-        claim_slot(P, y, ck, rm_y);
-      }
-      // absorb y: the coagulated particle's volumes, radius, class, record
-      double s_v = 0.0, s_m = 0.0;
-      for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
-      for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
-      for (int s = 0; s < P.n_spec; s++) s_m = s_m + vcur[s] * P.density[s];
-      vt = s_v;
-      r = vol2rad(vt);
-      int cls = S.cc + 1;
-      rec = make_rec_v(P, r, vt, s_m, cls);
-      recf = to_f32(rec);
-      int C2 = cell_of(P, r, cls);
-      if (C2 < 0 || cw.len >= kChainMaxLen) {  // off the grid (reported by the apply) or long enough
-        stop = true;
-        break;
-      }
-      if (C2 != C) {
-        C = C2;
-        p0 = q;
-        pos0 = (float)pos;
-        moved = true;
-        break;
-      }
-    }
-    if (!moved && !stop) {
-      out->done = true;  // every later pair of the cell was walked
-      break;
+  // the pairs of cell C from (p0, pos0) on, as one stretch of expected
+  // tests: cum[j] over the cell's pairs (cp_cum)
+  int lo = P.cp_off[C], end = P.cp_off[C + 1];
+  const double* cum = P.cp_cum + (P.cp_off[C] + C) - lo;  // cum[j], j = lo..end
+  {
+    int hi = end;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (P.cp_list[mid] < p0) lo = mid + 1;
+      else hi = mid;
     }
   }
-  out->chain_len = cw.len;
-  out->chain_head = cw.head;
+  double at = cum[lo];
+  if (lo < end && P.cp_list[lo] == p0) at += (cum[lo + 1] - cum[lo]) * (double)pos0;
+  const double at_end = cum[end];
+  int j = lo;
+  for (;;) {
+    at += -log(g.next());
+    if (!(at < at_end)) {
+      out->done = true;  // no test left in the cell's later pairs
+      break;
+    }
+    if (++n_iter > (1LL << 26)) {  // far past any mean the step can ask for
+      set_status(P.ctr, kErrTimeout);
+      break;
+    }
+    {
+      // the pair whose stretch holds at: cum[j] <= at < cum[j + 1]
+      int a = j, b = end - 1;
+      while (a < b) {
+        int mid = (a + b + 1) >> 1;
+        if (cum[mid] <= at) a = mid;
+        else b = mid - 1;
+      }
+      j = a;
+    }
+    int q = P.cp_list[j];
+    double lam = cum[j + 1] - cum[j];
+    if (!(lam > 0.0)) continue;
+    double pos = (at - cum[j]) / lam;
+    const PairState& S = P.pair[q];
+    PairDesc d = P.pair_desc[q];
+    int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
+    int O = cell1 == C ? cell2 : cell1;
+    int n_o = P.cell_count[O];
+    int o_start = P.cell_start[O];
+    if (n_o < 1) continue;
+    if (o_start < 0 || (long long)o_start + n_o > P.cap) {
+      bad_index(P.ctr, kBadPairCells, q);
+      break;
+    }
+    int i = (int)(g.next() * (double)n_o);
+    if (i >= n_o) i = n_o - 1;
+    int y = P.list[o_start + i];
+    if (y < 0 || y >= P.cap) {
+      bad_index(P.ctr, kBadTestSlot, y);
+      continue;
+    }
+    if (y == x || !P.alive[y] || P.cell[y] != O) continue;
+    n_tests++;
+    bool first = cell1 == C;
+    T k;
+    if constexpr (sizeof(T) == 8) {
+      const double* qw = (const double*)&P.recd[x];
+      const double* qy = (const double*)&P.recd[y];
+      k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat, P.coeff);
+    } else {
+      const float* qw = (const float*)&P.recf[x];
+      const float* qy = (const float*)&P.recf[y];
+      k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, (float)S.fflat,
+                                          (float)P.coeff);
+    }
+    T prob = k * (T)S.inv_k_max;
+    if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
+    if (!((T)g.next() < prob)) continue;
+    // the first accepted test: an event of the next step of the round,
+    // claimed by its merge decision; an absorb (the walking particle is
+    // replaced by the coagulated one) continues as a chain
+    unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
+    unsigned long long ck = claim_key(P, key);
+    Rng gm = merge_rng(P, key);
+    double rx = P.rad[x], vtx = P.vtot[x], ry = P.rad[y], vty = P.vtot[y];
+    MergeDecision m = first ? merge_decide_v(P, gm, rx, vtx, ry, vty, d.c1, d.c2, S.cc)
+                            : merge_decide_v(P, gm, ry, vty, rx, vtx, d.c1, d.c2, S.cc);
+    bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
+    out->found = true;
+    out->q = q;
+    out->y = y;
+    out->pos = (float)pos;
+    out->first_cell1 = first;
+    out->dec = pack_decision(m, gm.used());
+    if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+    claim_slot(P, x, ck, rm_x);
+    claim_slot(P, y, ck, rm_y);
+    out->cont = m.create && rm_x && m.new_group != 0;
+    out->g_used = g.used();
+    break;
+  }
   if (n_tests) {
     add_ll(&P.ctr->tot_samp, n_tests);
     add_ll(&P.ctr->walk_tests, n_tests);
@@ -565,7 +652,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
                                                const int* gp_c, const float* ev_pos, const uint32_t* dec,
                                                ChainPool pool, uint8_t* it_flag, unsigned long long* it_key,
                                                int2* it_c, int* it_gp, float* it_pos, int* it_len, int* it_head,
-                                               uint8_t* it_done, uint32_t* it_dec) {
+                                               uint8_t* it_done, uint32_t* it_dec, uint32_t* it_gused) {
   long long n = *n_items;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
@@ -616,10 +703,10 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
       sl = w.first_cell1 ? make_int2(walker, w.y) : make_int2(w.y, walker);
       gp = (int)(pop_pair_base[pop] + w.q);
       pos0 = w.pos;
-      len = w.chain_len;
-      head = w.chain_head;
+      len = w.cont ? -1 : 0;  // -1: k_chain carries the walk on
       done = w.done;
       dc = w.dec;
+      it_gused[e] = w.g_used;
     } else {
       // a retry keeps its merge decision and claims by it
       uint32_t used;
@@ -640,36 +727,95 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
   }
 }
 
-// Apply the winning chains (win[e] == 2), one thread per chain: the first
+// Chains, after k_items: an item whose first event is an absorb (it_len -1)
+// carries its walk on from that event with the coagulated particle
+// (walk_chain), from the stream position the walk had reached.  The chain's
+// events go to the pool, the first one included; the item gets the chain's
+// length and head, or length 0 (the first event alone) if the pool is full.
+template <int KT, class T, bool FLAT>
+__global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gpair_pop, const long long* n_items,
+                                               const uint8_t* it_flag, const unsigned long long* it_key,
+                                               const int2* it_c, const int* it_gp, const float* it_pos,
+                                               const uint32_t* it_dec, const uint32_t* it_gused, ChainPool pool,
+                                               int* it_len, int* it_head, uint8_t* it_done) {
+  long long n = *n_items;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (!it_flag[e] || it_len[e] != -1) continue;
+    const PopDev& P = pops[gpair_pop[it_gp[e]]];
+    unsigned long long key = it_key[e];
+    int x = (int)key_idx(key), q = (int)key_pair(key);
+    int2 sl = it_c[e];
+    bool first = sl.x == x;
+    int y = first ? sl.y : sl.x;
+    uint32_t used;
+    MergeDecision m = unpack_decision(it_dec[e], &used);
+    bool rm_y = first ? m.rm2 : m.rm1;
+    it_len[e] = 0;
+    if (x < 0 || x >= P.cap || y < 0 || y >= P.cap || q >= P.n_pairs) continue;
+    ChainWriter cw;
+    if (!cw.append(pool, y, q | (rm_y ? kChainRemoves : 0), it_pos[e])) continue;
+    Rng g = make_rng(P, kStreamWalk, 0u, (uint32_t)x);
+    g.seek(it_gused[e]);
+    WalkOut out;
+    long long n_tests = 0;
+    walk_chain<KT, T, FLAT>(P, pool, x, y, q, (double)it_pos[e], P.pair[q].cc + 1, g, cw, &out, &n_tests);
+    it_len[e] = cw.len;
+    it_head[e] = cw.head;
+    it_done[e] = out.done ? 1 : 0;
+    if (n_tests) {
+      add_ll(&P.ctr->tot_samp, n_tests);
+      add_ll(&P.ctr->walk_tests, n_tests);
+    }
+  }
+}
+
+// Apply the winning chains (win[e] == 2), one warp per chain: the first
 // ev_app[e] events in order, each a coagulate (coagulation.F90:928-985) of
 // the walking particle with the next partner, with the merge decision
-// recomputed from the values and the stream the walk used.  The coagulated
-// particle stays in the walking particle's slot; absorbed partners that the
-// decision removes are killed.  dest[e], gp_c[e] and ev_pos[e] are set to
-// where the particle walks on (dest -1 if its walk ran to the end).
-__global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const long long* pop_pair_base,
-                              const long long* n_events, const unsigned long long* ev_key, const uint8_t* win,
-                              const int* ev_len, const int* ev_app, const int* ev_head, const uint8_t* ev_done,
-                              ChainPool pool, int* gp_c, float* ev_pos, int* dest_out) {
+// recomputed from the values and the stream the walk used.  Lanes hold the
+// particle's species (lane, lane + 32) and components (lane); every lane
+// draws the same merge decision and component selection; sums run in the
+// walk's order (per species over the events, then over the species), so the
+// decisions are the walk's.  The coagulated particle stays in the walking
+// particle's slot; partners that a decision removes are killed.  dest[e],
+// gp_c[e] and ev_pos[e] are set to where the particle walks on (dest -1 if
+// its walk ran to the end).
+__global__ void __launch_bounds__(256) k_apply_chain(const PopDev* pops, const int* gpair_pop,
+                                                     const long long* pop_pair_base, const long long* n_events,
+                                                     const unsigned long long* ev_key, const uint8_t* win,
+                                                     const int* ev_len, const int* ev_app, const int* ev_head,
+                                                     const uint8_t* ev_done, ChainPool pool, int* gp_c, float* ev_pos,
+                                                     int* dest_out) {
+  constexpr unsigned kFull = 0xffffffffu;
   long long E = *n_events;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
-       e += (long long)gridDim.x * blockDim.x) {
-    if (win[e] != 2) continue;
+  const int lane = threadIdx.x & 31;
+  long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long e = warp; e < E; e += n_warps) {
+    if (win[e] != 2) continue;  // the same e for the whole warp
     int pop = gpair_pop[gp_c[e]];
     const PopDev& P = pops[pop];
     unsigned long long key1 = ev_key[e];
     int x = (int)key_idx(key1);
     int app = ev_app[e];
     if (x < 0 || x >= P.cap) {
-      bad_index(P.ctr, kBadEventSlot, x);
+      if (lane == 0) bad_index(P.ctr, kBadEventSlot, x);
       continue;
     }
-    const int nb = P.grid->n_bin;
+    const int nb = P.grid->n_bin, ns = P.n_spec;
     uint32_t gen = *P.gen_p;
-    double vcur[kMaxSpec];
-    for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
-    PMeta cur, ym, nm;
-    load_meta(P, x, cur);
+    // the walking particle, spread over the lanes
+    double v_lo = lane < ns ? P.vol[vol_at(P, x, lane)] : 0.0;
+    double v_hi = lane + 32 < ns ? P.vol[vol_at(P, x, lane + 32)] : 0.0;
+    PScal cur;
+    load_scal(P, x, cur);
+    int cc_ = 0;
+    double ct_ = 0.0;
+    if (lane < cur.ncomp && lane < kMaxComponent) {
+      cc_ = P.csrc[comp_at(x, lane)];
+      ct_ = P.ctime[comp_at(x, lane)];
+    }
     double r = P.rad[x], vt = P.vtot[x];
     int C = P.cell[x];
     ChainReader rd(ev_head[e]);
@@ -677,13 +823,10 @@ __global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const lo
     float last_pos = 0.f;
     for (int i = 0; i < app; i++) {
       long long ix = rd.next(pool);
-      if (ix < 0) {
-        bad_index(P.ctr, kBadEventSlot, -1);
-        break;
-      }
-      int y = pool.y[ix], q = pool.q[ix] & kChainPairMask;
-      if (y < 0 || y >= P.cap || q >= P.n_pairs) {
-        bad_index(P.ctr, kBadEventSlot, y);
+      int y = ix < 0 ? -1 : pool.y[ix];
+      int q = ix < 0 ? -1 : (pool.q[ix] & kChainPairMask);
+      if (ix < 0 || y < 0 || y >= P.cap || q >= P.n_pairs) {
+        if (lane == 0) bad_index(P.ctr, kBadEventSlot, y);
         break;
       }
       PairDesc d = P.pair_desc[q];
@@ -695,32 +838,69 @@ __global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const lo
                               : merge_decide_v(P, g, ry, vty, r, vt, d.c1, d.c2, S.cc);
       bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
       bool lost_x = first ? m.lost1 : m.lost2, lost_y = first ? m.lost2 : m.lost1;
-      if (!(m.create && rm_x && m.new_group != 0)) {  // the walk decided an absorb here
-        set_status(P.ctr, kErrAssert);
+      if (!(m.create && rm_x && m.new_group != 0) || (lost_x && !(rm_y && !lost_y))) {
+        if (lane == 0) set_status(P.ctr, kErrAssert);  // the walk decided an absorb here
         break;
       }
-      load_meta(P, y, ym);
-      double ice_x = P.i_water > 0 ? vcur[P.i_water - 1] : 0.0;
-      double ice_y = P.i_water > 0 ? P.vol[vol_at(P, y, P.i_water - 1)] : 0.0;
-      if (first) coag_meta(g, cur, ice_x, ym, ice_y, nm);
-      else coag_meta(g, ym, ice_y, cur, ice_x, nm);
-      if (!lost_x) nm.id = cur.id;
-      else if (rm_y && !lost_y) nm.id = ym.id;
-      else {
-        set_status(P.ctr, kErrAssert);
-        break;
+      // the partner
+      PScal ys;
+      load_scal(P, y, ys);
+      double y_lo = lane < ns ? P.vol[vol_at(P, y, lane)] : 0.0;
+      double y_hi = lane + 32 < ns ? P.vol[vol_at(P, y, lane + 32)] : 0.0;
+      int yc = 0;
+      double yt = 0.0;
+      if (lane < ys.ncomp && lane < kMaxComponent) {
+        yc = P.csrc[comp_at(y, lane)];
+        yt = P.ctime[comp_at(y, lane)];
       }
+      double ice_x = 0.0, ice_y = 0.0;
+      if (P.i_water > 0) {
+        int w = P.i_water - 1;
+        ice_x = __shfl_sync(kFull, w < 32 ? v_lo : v_hi, w & 31);
+        ice_y = __shfl_sync(kFull, w < 32 ? y_lo : y_hi, w & 31);
+      }
+      // components of aero_particle_coagulate with a = particle 1, b = particle 2
+      const PScal& A = first ? cur : ys;
+      const PScal& B = first ? ys : cur;
+      int ca = first ? cc_ : yc, cb = first ? yc : cc_;
+      double ta = first ? ct_ : yt, tb = first ? yt : ct_;
+      int na = A.ncomp, nbc = B.ncomp;
+      int n1_new = na, n2_new = nbc;
+      bool from_a = lane < na;
+      int k_src = from_a ? lane : lane - na;
+      if (na + nbc > kMaxComponent) {
+        int sa[kMaxComponent], sb[kMaxComponent];
+        coag_components(g, na, A.nprim, nbc, B.nprim, &n1_new, &n2_new, sa, sb);
+        from_a = lane < n1_new;
+        k_src = 0;
+        if (from_a) k_src = sa[lane] - 1;
+        else if (lane - n1_new < n2_new) k_src = sb[lane - n1_new] - 1;
+      }
+      k_src &= 31;
+      int xa = __shfl_sync(kFull, ca, k_src), xb = __shfl_sync(kFull, cb, k_src);
+      double za = __shfl_sync(kFull, ta, k_src), zb = __shfl_sync(kFull, tb, k_src);
+      int n_out = n1_new + n2_new;
+      PScal nm;
+      coag_scalars(A, first ? ice_x : ice_y, B, first ? ice_y : ice_x, nm);
+      nm.ncomp = n_out;
+      nm.id = !lost_x ? cur.id : ys.id;
       nm.grp = m.new_group;
       nm.cls = S.cc + 1;
+      cc_ = lane < n_out ? (from_a ? xa : xb) : 0;
+      ct_ = lane < n_out ? (from_a ? za : zb) : 0.0;
+      // volumes: per species over the events, then the total over the species
+      v_lo = v_lo + y_lo;
+      v_hi = v_hi + y_hi;
       double s_v = 0.0;
-      for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
-      for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
+      for (int s = 0; s < ns; s++) s_v = s_v + __shfl_sync(kFull, s < 32 ? v_lo : v_hi, s & 31);
       vt = s_v;
       r = vol2rad(vt);
       C = cell_of(P, r, nm.cls);
       if (rm_y) {
-        kill_slot(P, y);
-        P.touched[y] = gen;
+        if (lane == 0) {
+          kill_slot(P, y);
+          P.touched[y] = gen;
+        }
         dlive--;
       }
       cur = nm;
@@ -729,43 +909,93 @@ __global__ void k_apply_chain(const PopDev* pops, const int* gpair_pop, const lo
       last_pos = pool.pos[ix];
     }
     if (done_ev == 0) continue;
-    store_particle(P, x, vcur, cur);
-    P.touched[x] = gen;
-    int nbin = refresh_slot(P, x);
-    bool on_grid = nbin >= 1 && nbin <= nb;
-    if (!on_grid) set_status(P.ctr, kErrOutOfGrid);
-    add_ll(&P.ctr->tot_coag, (long long)done_ev);
-    if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
-    bool walk_done = ev_done[e] && done_ev == ev_len[e];
-    dest_out[e] = (walk_done || !on_grid) ? -1 : x;
-    gp_c[e] = (int)(pop_pair_base[pop] + last_q);
-    ev_pos[e] = last_pos;
+    // the coagulated particle in the walking particle's slot
+    __syncwarp();
+    if (lane < ns) P.vol[vol_at(P, x, lane)] = v_lo;
+    if (lane + 32 < ns) P.vol[vol_at(P, x, lane + 32)] = v_hi;
+    if (lane < cur.ncomp && lane < kMaxComponent) {
+      P.csrc[comp_at(x, lane)] = cc_;
+      P.ctime[comp_at(x, lane)] = ct_;
+    }
+    double ms = 0.0;
+    for (int s = 0; s < ns; s++)
+      ms = ms + __shfl_sync(kFull, s < 32 ? v_lo : v_hi, s & 31) * P.density[s];
+    if (lane == 0) {
+      P.vtot[x] = vt;
+      P.mass[x] = ms;
+      P.grp[x] = cur.grp;
+      P.cls[x] = cur.cls;
+      P.id[x] = cur.id;
+      P.nprim[x] = cur.nprim;
+      P.ncomp[x] = cur.ncomp;
+      P.lct[x] = cur.lct;
+      P.gct[x] = cur.gct;
+      P.imf[x] = cur.imf;
+      P.den_ice[x] = cur.den_ice;
+      P.phi[x] = cur.phi;
+      P.hyst[x] = cur.hyst;
+      P.frozen[x] = cur.frozen;
+      P.alive[x] = 1;
+      P.changed[x] = 1;
+      P.touched[x] = gen;
+      int nbin = refresh_slot(P, x);
+      bool on_grid = nbin >= 1 && nbin <= nb;
+      if (!on_grid) set_status(P.ctr, kErrOutOfGrid);
+      add_ll(&P.ctr->tot_coag, (long long)done_ev);
+      if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
+      bool walk_done = ev_done[e] && done_ev == ev_len[e];
+      dest_out[e] = (walk_done || !on_grid) ? -1 : x;
+      gp_c[e] = (int)(pop_pair_base[pop] + last_q);
+      ev_pos[e] = last_pos;
+    }
   }
 }
 
 // Walk rates after a round's sort: for every cell, the running sum over its
 // pairs (loop order) of k_max * del_t * members of the pair's other cell;
-// pairs on the per-particle path add nothing.  One thread per cell.
-__global__ void k_walk_rates(const PopDev* pops) {
+// pairs on the per-particle path add nothing.  One block per cell, its
+// threads over the cell's pairs, a block-wide scan in a fixed order.
+__global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = blockIdx.x;
   if (c >= P.n_cells || P.n_pairs == 0) return;
   const int nb = P.grid->n_bin;
-  int lo = P.cp_off[c], hi = P.cp_off[c + 1];
+  const int lo = P.cp_off[c], hi = P.cp_off[c + 1];
   double* cum = P.cp_cum + lo + c;
-  double acc = 0.0;
-  for (int j = lo; j < hi; j++) {
-    cum[j - lo] = acc;
-    int q = P.cp_list[j];
-    const PairState& S = P.pair[q];
-    if (S.path == kPathParticle) continue;
-    PairDesc d = P.pair_desc[q];
-    int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
-    int O = cell1 == c ? cell2 : cell1;
-    double lam = S.k_max * P.del_t * (double)P.cell_count[O];
-    if (lam > 0.0) acc += lam;
+  __shared__ double wsum[4];
+  __shared__ double carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0.0;
+  __syncthreads();
+  for (int base = lo; base < hi; base += blockDim.x) {
+    int j = base + threadIdx.x;
+    double lam = 0.0;
+    if (j < hi) {
+      int q = P.cp_list[j];
+      const PairState& S = P.pair[q];
+      if (S.path != kPathParticle) {
+        PairDesc d = P.pair_desc[q];
+        int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
+        int O = cell1 == c ? cell2 : cell1;
+        double l = S.k_max * P.del_t * (double)P.cell_count[O];
+        if (l > 0.0) lam = l;
+      }
+    }
+    double x = lam;  // inclusive scan within the warp
+    for (int o = 1; o < 32; o <<= 1) {
+      double y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    double before = carry;
+    for (int w = 0; w < wid; w++) before += wsum[w];
+    if (j < hi) cum[j - lo] = before + x - lam;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += wsum[0] + wsum[1] + wsum[2] + wsum[3];
+    __syncthreads();
   }
-  cum[hi - lo] = acc;
+  if (threadIdx.x == 0) cum[hi - lo] = carry;
 }
 
 // ---------------------------------------------------------------------------

@@ -78,10 +78,34 @@ __device__ __forceinline__ void zero_meta(PMeta& m) {
   m.hyst = m.frozen = 0;
 }
 
+// The scalar fields of a particle (PMeta without the component lists).
+struct PScal {
+  int grp, cls;
+  long long id;
+  int nprim, ncomp;
+  double lct, gct, imf, den_ice, phi;
+  int hyst, frozen;
+};
+
+__device__ __forceinline__ void load_scal(const PopDev& P, int i, PScal& m) {
+  m.grp = P.grp[i];
+  m.cls = P.cls[i];
+  m.id = P.id[i];
+  m.nprim = P.nprim[i];
+  m.ncomp = P.ncomp[i];
+  m.lct = P.lct[i];
+  m.gct = P.gct[i];
+  m.imf = P.imf[i];
+  m.den_ice = P.den_ice[i];
+  m.phi = P.phi[i];
+  m.hyst = P.hyst[i];
+  m.frozen = P.frozen[i];
+}
+
 // The non-component fields of aero_particle_coagulate (aero_particle.F90:
 // 917-1033): the caller sets id, weight group and class.  r may alias a.
-__device__ __forceinline__ void coag_scalars(const PMeta& a, double ice_a, const PMeta& b, double ice_b,
-                                             PMeta& r) {
+template <class M>
+__device__ __forceinline__ void coag_scalars(const M& a, double ice_a, const M& b, double ice_b, M& r) {
   int hyst = (a.hyst == 1 && b.hyst == 1) ? 1 : 0;
   double lct = a.lct < b.lct ? a.lct : b.lct;
   double gct = a.gct > b.gct ? a.gct : b.gct;
