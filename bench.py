@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--batch-same", type=int, default=8)
     ap.add_argument("--serve-jobs", type=int, default=200)
     ap.add_argument("--no-graphs", action="store_true",
-                    help="redraw rounds from the host loop instead of the CUDA graph (for launch lists)")
+                    help="later rounds from the host loop instead of the CUDA graph (for launch lists)")
     ap.add_argument("--headline-only", action="store_true",
                     help="measure the headline step only (no FP64, batched or end-to-end lines)")
     return ap.parse_args()

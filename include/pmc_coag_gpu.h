@@ -197,11 +197,12 @@ int pmc_coag_gpu_get_next_id(pmc_coag_gpu_ctx *ctx, int pop, int64_t *next_id);
 /* PMC_MODE_FP64 (default), PMC_MODE_MIXED or PMC_MODE_REPLAY. */
 int pmc_coag_gpu_set_mode(pmc_coag_gpu_ctx *ctx, int mode);
 
-/* Run the redraw rounds of a step (every round after the first) as one CUDA
- * graph whose loop condition is set on the device (enable = 1, the default),
- * or from a host loop (enable = 0).  Both give the same particles, bit for
- * bit.  A step with per-particle (accelerated) work always uses the host
- * loop.  No counterpart in the reference (an execution choice). */
+/* Run the later rounds of a step (every round after the first: retried
+ * events, walks of the particles the step made, chains) as one CUDA graph
+ * whose loop condition is set on the device (enable = 1, the default), or
+ * from a host loop (enable = 0).  Both give the same particles, bit for bit.
+ * Rounds with per-particle (accelerated) redo operations use the host loop.
+ * No counterpart in the reference (an execution choice). */
 int pmc_coag_gpu_set_graphs(pmc_coag_gpu_ctx *ctx, int enable);
 
 /* New seed for population `pop`, with its step counter back at zero
@@ -220,14 +221,16 @@ int pmc_coag_gpu_replay_open(pmc_coag_gpu_ctx *ctx, const char *path);
 int pmc_coag_gpu_replay_used(pmc_coag_gpu_ctx *ctx, int64_t *n_used);
 
 /* Counters of the last step: kernel-bound violations (warn_assert_msg
- * 532446093, coagulation.F90:749-751), conflict redraws, sub-rounds. */
+ * 532446093, coagulation.F90:749-751), events that lost a claim (each is
+ * retried or dropped in the next round), rounds. */
 int pmc_coag_gpu_stats(pmc_coag_gpu_ctx *ctx, int64_t *kmax_violations,
                        int64_t *redraws, int64_t *rounds);
 
 /* Conflicts of the last step, summed over its rounds: accepted per-set
  * events and how many lost a claim, per-particle target operations and how
- * many lost a claim (each loser is redone in a later round).  No counterpart
- * in the reference, which applies events one at a time. */
+ * many lost a claim (each loser is retried, dropped or redone in a later
+ * round).  No counterpart in the reference, which applies events one at a
+ * time. */
 int pmc_coag_gpu_conflicts(pmc_coag_gpu_ctx *ctx, int64_t *events,
                            int64_t *event_losers, int64_t *target_ops,
                            int64_t *target_op_losers);

@@ -178,8 +178,9 @@ class AeroState:
         check(_lib.lib().pmc_coag_gpu_set_seed(self.ctx, pop, int(seed)), "pmc_coag_gpu_set_seed")
 
     def set_graphs(self, enable):
-        """Redraw rounds as one device-driven CUDA graph (default) or from a
-        host loop; the particles are the same either way."""
+        """The later rounds of a step (retries, walks, chains) as one
+        device-driven CUDA graph (default) or from a host loop; the particles
+        are the same either way."""
         check(_lib.lib().pmc_coag_gpu_set_graphs(self.ctx, 1 if enable else 0), "pmc_coag_gpu_set_graphs")
 
     def set_weight(self, aero_weight_array):
@@ -271,6 +272,8 @@ class AeroState:
         return v.value
 
     def stats(self):
+        """Last step: k_max violations, events that lost a claim ("redraws":
+        each was retried or dropped in the next round), rounds."""
         a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         check(_lib.lib().pmc_coag_gpu_stats(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
               "pmc_coag_gpu_stats")
