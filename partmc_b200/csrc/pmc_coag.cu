@@ -781,6 +781,7 @@ struct Ctx {
   DevBuf<int> ev_dest;       // slot of the particle each event made (-1: none)
   DevBuf<int> ev_len, ev_head, ev_app;  // chains: events, first chunk, events applied
   DevBuf<uint8_t> ev_done;   // chains: the walk ran to the end
+  DevBuf<int> chain_list;    // the round's winning chains (round_dev[4] of them)
   DevBuf<double2> ice_set;   // water volumes of the sources of each event
   DevBuf<int2> ev;
   DevBuf<long long> flag_off;
@@ -835,7 +836,8 @@ struct Ctx {
   // round so the sort can size itself without reading the device
   std::vector<int> n_slots_host;
   // device scalars of a round: [0] events that lost a claim, [1] events,
-  // [2] items (the events of the round before), [3] chain chunks handed out
+  // [2] items (the events of the round before), [3] chain chunks handed out,
+  // [4] winning chains of the round
   DevBuf<long long> round_dev;
   std::vector<long long> base_cached;  // pair-list layout last uploaded
   double prof_ms[4] = {0, 0, 0, 0};
@@ -1099,6 +1101,8 @@ void alloc_sort(Ctx& c, PopHost& ph) {
     int* d_off = dalloc<int>(o, off.size());
     int* d_list = dalloc<int>(o, list.size());
     h.cp_cum = dalloc<double>(o, (size_t)off[h.n_cells] + h.n_cells);
+    h.cp_ent = dalloc<int4>(o, std::max(off[h.n_cells], 1));
+    h.cp_tab = dalloc<int>(o, (size_t)h.n_cells * kWalkTab);
     CK(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaStreamSynchronize(c.stream));  // the host vectors go out of scope
@@ -1732,6 +1736,7 @@ __global__ void k_round_begin(uint32_t* d_round, long long* round_dev, int* per_
     round_dev[0] = 0;
     round_dev[1] = 0;
     round_dev[3] = 0;
+    round_dev[4] = 0;
   }
   for (int k = threadIdx.x; k < n_per_pop; k += blockDim.x) per_pop[k] = 0;
 }
@@ -1767,7 +1772,8 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   if (W > 0) {
     k_resolve_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
                                                     c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p,
-                                                    c.round_dev.p, c.ev_len.p, c.ev_head.p, c.ev_app.p, pool);
+                                                    c.round_dev.p, c.ev_len.p, c.ev_head.p, c.ev_app.p, pool,
+                                                    c.chain_list.p, c.round_dev.p + 4);
     note_launch();
     scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}},
                     st);
@@ -1799,12 +1805,14 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
     // part 2, one thread per event: removals, scalar fields, caches
     k_apply_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
                                                   c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
-                                                  c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_dest.p);
+                                                  c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_done.p,
+                                                  c.ev_dest.p);
     note_launch();
-    // chains, one thread each
-    k_apply_chain<<<grid_for(W * 32, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, Ed, c.ev_key.p,
-                                                    c.win_set.p, c.ev_len.p, c.ev_app.p, c.ev_head.p, c.ev_done.p,
-                                                    pool, c.gp_c.p, c.ev_pos.p, c.ev_dest.p);
+    // chains, one warp each
+    k_apply_chain<<<grid_for(W, 32), 32, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, c.chain_list.p,
+                                                    c.round_dev.p + 4, c.ev_key.p, c.ev_len.p, c.ev_app.p,
+                                                    c.ev_head.p, c.ev_done.p, pool, c.gp_c.p, c.ev_pos.p,
+                                                    c.ev_dest.p);
     note_launch();
   }
   if (Q > 0) {
@@ -1861,7 +1869,7 @@ std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
           (long long)c.per_pop_i.p, (long long)c.pop_pair_base.p, (long long)c.gpair_pop.p,
           (long long)c.gpair_local.p, (long long)c.ev_key.p, (long long)c.ev_c.p, (long long)c.gp_c.p,
           (long long)c.ev_pos.p, (long long)c.ev_dest.p, (long long)c.ev_len.p, (long long)c.ev_head.p,
-          (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.it_flag.p, (long long)c.it_key.p,
+          (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.chain_list.p, (long long)c.it_flag.p, (long long)c.it_key.p,
           (long long)c.it_c.p, (long long)c.it_gp.p, (long long)c.it_pos.p, (long long)c.it_len.p,
           (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_dec.p, (long long)c.it_gused.p, (long long)c.it_off.p,
           (long long)c.ch_y.p,
@@ -1898,6 +1906,7 @@ void reserve_events(Ctx& c, long long W) {
   c.ev_key.reserve(w + 1); c.ev_c.reserve(w + 1); c.gp_c.reserve(w + 1); c.ev_pos.reserve(w + 1);
   c.ev_dest.reserve(w + 1); c.win_set.reserve(w + 1); c.dec_set.reserve(w + 1);
   c.ev_len.reserve(w + 1); c.ev_head.reserve(w + 1); c.ev_app.reserve(w + 1); c.ev_done.reserve(w + 1);
+  c.chain_list.reserve(w + 1);
   c.need_slot_set.reserve(w + 1); c.need_id_set.reserve(w + 1); c.ice_set.reserve(w + 1);
   c.rank_slot_set.reserve(w + 2); c.rank_id_set.reserve(w + 2);
   size_t chunks = w + 4096;
@@ -1911,7 +1920,8 @@ bool events_fit(const Ctx& c, long long W) {
   size_t w = (size_t)W;
   return c.ev_key.n >= w + 1 && c.ev_c.n >= w + 1 && c.gp_c.n >= w + 1 && c.ev_pos.n >= w + 1 &&
          c.ev_dest.n >= w + 1 && c.win_set.n >= w + 1 && c.dec_set.n >= w + 1 && c.ev_len.n >= w + 1 &&
-         c.ev_head.n >= w + 1 && c.ev_app.n >= w + 1 && c.ev_done.n >= w + 1 && c.need_slot_set.n >= w + 1 &&
+         c.ev_head.n >= w + 1 && c.ev_app.n >= w + 1 && c.ev_done.n >= w + 1 && c.chain_list.n >= w + 1 &&
+         c.need_slot_set.n >= w + 1 &&
          c.need_id_set.n >= w + 1 && c.ice_set.n >= w + 1 && c.rank_slot_set.n >= w + 2 &&
          c.rank_id_set.n >= w + 2;
 }
@@ -2087,7 +2097,7 @@ void step_parallel(Ctx& c, int kt) {
   c.id_base_set.reserve(c.n_pop);
   c.id_base_pp.reserve(c.n_pop);
   c.n_dev.reserve(4 + 2 * (size_t)c.n_pop);
-  c.round_dev.reserve(4);
+  c.round_dev.reserve(5);
   int max_pairs = 1, nb_max = 1, max_cap = 1;
   for (int k = 0; k < c.n_pop; k++) {
     max_pairs = std::max(max_pairs, c.pops[k].h.n_pairs);
@@ -2195,7 +2205,7 @@ void step_parallel(Ctx& c, int kt) {
     c.lost_off.reserve(Q + 2); c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
   }
   if (c.dirty) push_pops(c);
-  CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 4, c.stream));
+  CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 5, c.stream));
   CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
   if (W > 0) {
     ProfScope ps(c, 0, W);
@@ -2459,6 +2469,7 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.it_flag.release();
   c.it_done.release();
   c.ev_done.release();
+  c.chain_list.release();
   c.it_c.release();
   c.flag.release();
   c.win_set.release();

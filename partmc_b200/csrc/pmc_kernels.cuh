@@ -75,6 +75,31 @@ __device__ __forceinline__ void add_ll(long long* p, long long v) {
 }
 __device__ __forceinline__ void add_ll(int* p, long long v) { atomicAdd(p, (int)v); }
 
+// add_ll for counters that many threads of a launch bump: the converged
+// lanes that add to the same counter sum their values (|v| small) and one of
+// them adds the sum, so a warp makes one atomic per counter instead of 32
+__device__ __forceinline__ void add_ll_warp(long long* p, int v) {
+  const unsigned peers = __match_any_sync(__activemask(), (unsigned long long)p);
+  const int sum = (int)__reduce_add_sync(peers, (unsigned)v);
+  if ((int)(threadIdx.x & 31) == __ffs(peers) - 1 && sum != 0)
+    atomicAdd((unsigned long long*)p, (unsigned long long)(long long)sum);
+}
+// atomicAdd(p, 1) with the old value, one atomic for the converged lanes
+// that bump the same counter: each gets the old value plus its rank
+__device__ __forceinline__ unsigned long long inc_warp(unsigned long long* p) {
+  const unsigned peers = __match_any_sync(__activemask(), (unsigned long long)p);
+  const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(p, (unsigned long long)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + (unsigned long long)__popc(peers & ((1u << lane) - 1u));
+}
+__device__ __forceinline__ void add_ll_warp(int* p, int v) {
+  const unsigned peers = __match_any_sync(__activemask(), (unsigned long long)p);
+  const int sum = (int)__reduce_add_sync(peers, (unsigned)v);
+  if ((int)(threadIdx.x & 31) == __ffs(peers) - 1 && sum != 0) atomicAdd(p, sum);
+}
+
 // sort chunks covering the population's slots (the slot count lives on the
 // device and grows inside a step)
 __device__ __forceinline__ int n_chunks_of(const PopDev& P) {

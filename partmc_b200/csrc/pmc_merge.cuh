@@ -35,7 +35,7 @@ struct ChainWriter {
   int head = -1, chunk = -1, fill = 0, len = 0;
   __device__ bool append(const ChainPool& C, int y, int q, float pos) {
     if (chunk < 0 || fill == kChainChunk - 1) {
-      long long nc = (long long)atomicAdd((unsigned long long*)C.ctr, 1ULL);
+      long long nc = (long long)inc_warp((unsigned long long*)C.ctr);
       if (nc >= C.n_chunks) return false;
       if (chunk >= 0) C.y[(size_t)chunk * kChainChunk + kChainChunk - 1] = (int)nc;
       else head = (int)nc;
@@ -82,7 +82,7 @@ __device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
 __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const long long* n_events,
                               const unsigned long long* ev_key, const int2* ev, const int* ev_gp, int* need_slot,
                               int* need_id, uint8_t* win, const uint32_t* dec, long long* n_losers, const int* ev_len,
-                              const int* ev_head, int* ev_app, ChainPool pool) {
+                              const int* ev_head, int* ev_app, ChainPool pool, int* chain_list, long long* n_chain) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
@@ -103,7 +103,7 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const lo
     unsigned long long ck = claim_key(P, key);
     bool winner = holds_slot(P, sl.x, ck, m.rm1) && holds_slot(P, sl.y, ck, m.rm2);
     if (!winner) {
-      add_ll(n_losers, 1);
+      add_ll_warp(n_losers, 1);
       continue;
     }
     int len = ev_len[e];
@@ -124,6 +124,7 @@ __global__ void k_resolve_set(const PopDev* pops, const int* gpair_pop, const lo
       }
       ev_app[e] = app;
       win[e] = 2;
+      chain_list[inc_warp((unsigned long long*)n_chain)] = (int)e;
       continue;
     }
     win[e] = 1;
@@ -253,7 +254,7 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
                             const unsigned long long* ev_key, const int2* ev, const int* ev_gp,
                             const uint8_t* win, const uint32_t* dec, const long long* slot_rank,
                             const long long* id_rank, const int* slot_base, const long long* id_base,
-                            const double2* ice, int* dest_out) {
+                            const double2* ice, const uint8_t* ev_done, int* dest_out) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
@@ -268,14 +269,14 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
     uint32_t gen = *P.gen_p;
     uint32_t used;
     MergeDecision m = unpack_decision(dec[e], &used);
-    add_ll(&P.ctr->tot_coag, (long long)(1LL));
+    add_ll_warp(&P.ctr->tot_coag, 1);
     if (m.rm1) P.touched[s1] = gen;
     if (m.rm2) P.touched[s2] = gen;
     if (!m.create) {
       if (m.rm1) kill_slot(P, s1);
       if (m.rm2) kill_slot(P, s2);
       int dlive = -(int)m.rm1 - (int)m.rm2;
-      if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
+      if (dlive) add_ll_warp(&P.ctr->n_live, dlive);
       continue;
     }
     int dest = event_dest(m, s1, s2, slot_base[pop], m.rm1 || m.rm2 ? 0 : slot_rank[e]);
@@ -312,11 +313,11 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
     P.touched[dest] = gen;
     int nbin = refresh_slot(P, dest);
     if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
-    else dest_out[e] = dest;
+    else if (!(key_kind(ev_key[e]) == 1u && ev_done[e])) dest_out[e] = dest;  // a walk that ran to its end stops
     if (m.rm1 && dest != s1) kill_slot(P, s1);
     if (m.rm2 && dest != s2) kill_slot(P, s2);
     int dlive = 1 - (int)m.rm1 - (int)m.rm2;
-    if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
+    if (dlive) add_ll_warp(&P.ctr->n_live, dlive);
   }
 }
 
@@ -371,7 +372,7 @@ struct WalkOut {
   bool done = false;        // the walk ran to the end after its last event
   uint32_t dec = 0;         // merge decision of the first event
   bool cont = false;        // the first event is an absorb: k_chain carries the walk on
-  uint32_t g_used = 0;      // uniforms the walk's stream had used at the first event
+  uint32_t g_used = 0;      // index of the walk's next test after the first event
 };
 
 // true if this round's claim on slot y is the chain of walker x
@@ -381,230 +382,190 @@ __device__ __forceinline__ bool claimed_by_walk(const PopDev& P, int y, int x) {
          (uint32_t)w == (uint32_t)x;
 }
 
-// The rest of a chain after its first absorb (kept out of line: the chain's
-// state, the coagulated particle's volumes and record, stays out of the
-// walk's registers).  Continues the Poisson process of g along the pairs of
-// the coagulated particle's cell from (q, pos); returns the walk's end state.
-template <int KT, class T, bool FLAT>
-__device__ void walk_chain(const PopDev& P, const ChainPool& pool, int x, int y1, int q, double pos,
-                                        int cls, Rng& g, ChainWriter& cw, WalkOut* out, long long* n_tests_io) {
-  const int nb = P.grid->n_bin;
-  double vcur[kMaxSpec];
-  double vt, r;
-  RecD rec;
-  RecF recf;
-  long long n_tests = *n_tests_io, n_iter = 0;
-  int y = y1;
-  int C = -1, p0 = q;
-  float pos0 = (float)pos;
-  for (int s = 0; s < P.n_spec; s++) vcur[s] = P.vol[vol_at(P, x, s)];
-  bool stop = false;
-  for (;;) {
-    // absorb y: the coagulated particle's volumes, radius, class, record
-    double s_v = 0.0, s_m = 0.0;
-    for (int s = 0; s < P.n_spec; s++) vcur[s] = vcur[s] + P.vol[vol_at(P, y, s)];
-    for (int s = 0; s < P.n_spec; s++) s_v = s_v + vcur[s];
-    for (int s = 0; s < P.n_spec; s++) s_m = s_m + vcur[s] * P.density[s];
-    vt = s_v;
-    r = vol2rad(vt);
-    rec = make_rec_v(P, r, vt, s_m, cls);
-    recf = to_f32(rec);
-    C = cell_of(P, r, cls);
-    if (C < 0 || cw.len >= kChainMaxLen) break;  // off the grid (reported by the apply) or long enough
-    // the next accepted test of the coagulated particle
-    bool found = false, moved = true;
-    while (moved && !stop && !found) {
-      moved = false;
-      int lo = P.cp_off[C], end = P.cp_off[C + 1];
-      const double* cum = P.cp_cum + (P.cp_off[C] + C) - lo;
-      {
-        int hi = end;
-        while (lo < hi) {
-          int mid = (lo + hi) >> 1;
-          if (P.cp_list[mid] < p0) lo = mid + 1;
-          else hi = mid;
-        }
-      }
-      double at = cum[lo];
-      if (lo < end && P.cp_list[lo] == p0) at += (cum[lo + 1] - cum[lo]) * (double)pos0;
-      const double at_end = cum[end];
-      int j = lo;
-      for (;;) {
-        at += -log(g.next());
-        if (!(at < at_end)) {
-          out->done = true;  // every later pair of the cell was walked
-          stop = true;
-          break;
-        }
-        if (++n_iter > (1LL << 26)) {
-          set_status(P.ctr, kErrTimeout);
-          stop = true;
-          break;
-        }
-        {
-          int a = j, b = end - 1;
-          while (a < b) {
-            int mid = (a + b + 1) >> 1;
-            if (cum[mid] <= at) a = mid;
-            else b = mid - 1;
-          }
-          j = a;
-        }
-        int qq = P.cp_list[j];
-        double lam = cum[j + 1] - cum[j];
-        if (!(lam > 0.0)) continue;
-        double pp = (at - cum[j]) / lam;
-        const PairState& S = P.pair[qq];
-        PairDesc d = P.pair_desc[qq];
-        int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
-        int O = cell1 == C ? cell2 : cell1;
-        int n_o = P.cell_count[O];
-        int o_start = P.cell_start[O];
-        if (n_o < 1) continue;
-        if (o_start < 0 || (long long)o_start + n_o > P.cap) {
-          bad_index(P.ctr, kBadPairCells, qq);
-          stop = true;
-          break;
-        }
-        int i = (int)(g.next() * (double)n_o);
-        if (i >= n_o) i = n_o - 1;
-        int yy = P.list[o_start + i];
-        if (yy < 0 || yy >= P.cap) {
-          bad_index(P.ctr, kBadTestSlot, yy);
-          continue;
-        }
-        if (yy == x || !P.alive[yy] || P.cell[yy] != O) continue;
-        if (claimed_by_walk(P, yy, x)) continue;  // absorbed earlier in this chain
-        n_tests++;
-        bool first = cell1 == C;
-        T k;
-        if constexpr (sizeof(T) == 8) {
-          const double* qw = (const double*)&rec;
-          const double* qy = (const double*)&P.recd[yy];
-          k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat,
-                                               P.coeff);
-        } else {
-          const float* qw = (const float*)&recf;
-          const float* qy = (const float*)&P.recf[yy];
-          k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc,
-                                              (float)S.fflat, (float)P.coeff);
-        }
-        T prob = k * (T)S.inv_k_max;
-        if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
-        if (!((T)g.next() < prob)) continue;
-        // the chain ends before an event that is no absorb, or when the pool
-        // is full; the walk resumes there in the next round
-        unsigned long long key = make_key((uint32_t)qq, 1u, (uint32_t)x);
-        Rng gm = make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
-        double ry = P.rad[yy], vty = P.vtot[yy];
-        MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
-                                : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
-        bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
-        if (!(m.create && rm_x && m.new_group != 0) ||
-            !cw.append(pool, yy, qq | (rm_y ? kChainRemoves : 0), (float)pp)) {
-          stop = true;
-          break;
-        }
-        claim_slot(P, yy, claim_key(P, key), rm_y);
-        y = yy;
-        cls = S.cc + 1;
-        p0 = qq;
-        pos0 = (float)pp;
-        found = true;
-        break;
-      }
-    }
-    if (stop || !found) break;
-  }
-  *n_tests_io = n_tests;
+// The uniforms of a walk's test t: one Philox block keyed by the population,
+// counted by (step, round, walk stream, walking slot, t).  x, y: the gap to
+// the test (u53 -> exponential); z: the partner; w: the accept draw.  Every
+// test takes one block whether or not its partner is a member, so a test's
+// draws depend on its index alone.
+__device__ __forceinline__ U4 walk_draws(const PopDev& P, int x, uint32_t t) {
+  return philox4x32_10(U4{P.step, ((*P.round_p & 0xffu) << 4) | kStreamWalk, (uint32_t)x, t}, (uint32_t)P.seed,
+                       (uint32_t)(P.seed >> 32));
 }
 
+// A walk's place in the stretch of its cell C: the entries lo..end of the
+// cell's pair list, cum[j] (indexable by list entry j) the expected tests
+// before entry j, at the running position, j the entry that holds it.
+struct Stretch {
+  const double* cum;
+  const int* tab;
+  int C, end, j;
+  double at, total;
+};
+
+// the stretch of cell C from (pair p0, position pos0 in it) on: a binary
+// search of the cell's pair list for the first entry whose pair is p0 or later
+__device__ __forceinline__ void walk_stretch(const PopDev& P, int C, int p0, float pos0, Stretch* s) {
+  int lo = P.cp_off[C], end = P.cp_off[C + 1];
+  const double* cum = P.cp_cum + (lo + C) - lo;
+  int a = lo, hi = end;
+  while (a < hi) {
+    int mid = (a + hi) >> 1;
+    if (P.cp_list[mid] < p0) a = mid + 1;
+    else hi = mid;
+  }
+  double at = cum[a];
+  if (a < end && P.cp_list[a] == p0) at += (cum[a + 1] - cum[a]) * (double)pos0;
+  s->cum = cum;
+  s->tab = P.cp_tab + (size_t)C * kWalkTab;
+  s->C = C;
+  s->end = end;
+  s->j = a < end ? a : end - 1;
+  s->at = at;
+  s->total = cum[end];
+}
+
+// the entry j >= s.j with cum[j] <= at < cum[j + 1] (at < total): the
+// cell's bucket table gives a start at or before it, a short scan forward
+// usually ends there, a binary search covers the rest
+__device__ __forceinline__ int walk_pair(const Stretch& s, double at) {
+  const double* cum = s.cum;
+  int b = (int)(at / s.total * (double)kWalkTab);
+  b = b < 0 ? 0 : (b >= kWalkTab ? kWalkTab - 1 : b);
+  int hi = s.end - 1;
+  int j = s.tab[b];
+  j = j < s.j ? s.j : (j > hi ? hi : j);
+  int a, z;
+  if (cum[j] > at) {  // rounding put the bucket past at
+    a = s.j;
+    z = j - 1 < s.j ? s.j : j - 1;
+  } else {
+    for (int k = 0; k < 4 && j < hi; k++) {
+      if (cum[j + 1] > at) return j;
+      j++;
+    }
+    a = j;
+    z = hi;
+  }
+  while (a < z) {
+    int mid = (a + z + 1) >> 1;
+    if (cum[mid] <= at) a = mid;
+    else z = mid - 1;
+  }
+  return a;
+}
+
+// One walk test of particle x (records qxd/qxf) at running position at of
+// its stretch, in entry j: the partner drawn from the other cell's members
+// and the accept test.  The pair's fields and the partner slot are loaded
+// together, then the partner's state.  Returns 0 for no test (no member,
+// itself, a dead or moved member, or one this chain absorbed), 1 for a
+// rejected test, 2 for an accepted one, -1 for a failed bounds check.
+template <int KT, class T, bool FLAT>
+__device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& s, int j, double at, uint32_t pick,
+                                         uint32_t accu, const RecD& qxd, const RecF& qxf, bool chain, int* y_out,
+                                         float* pos_out, int* q_out, bool* first_out) {
+  const double c0 = s.cum[j], c1 = s.cum[j + 1];
+  const int4 ent = P.cp_ent[j];
+  double lam = c1 - c0;
+  int n_o = ent.w, o_start = ent.z;
+  if (!(lam > 0.0) || n_o < 1) return 0;
+  if (o_start < 0 || (long long)o_start + n_o > P.cap || ent.x < 0 || ent.x >= P.n_pairs) {
+    bad_index(P.ctr, kBadPairCells, ent.x);
+    return -1;
+  }
+  const int q = ent.x, O = ent.y & ((1 << 30) - 1);
+  const bool first = (ent.y >> 30) & 1;
+  int i = (int)(u32d(pick) * (double)n_o);
+  if (i >= n_o) i = n_o - 1;
+  const int y = P.list[o_start + i];
+  const PairDesc d = P.pair_desc[q];
+  const PairState& S = P.pair[q];
+  const double inv_k_max = S.inv_k_max, fflat = S.fflat;
+  const int cc = S.cc;
+  if (y < 0 || y >= P.cap) {
+    bad_index(P.ctr, kBadTestSlot, y);
+    return -1;
+  }
+  const uint8_t alive = P.alive[y];
+  const int cell_y = P.cell[y];
+  if (y == x || !alive || cell_y != O) return 0;
+  if (chain && claimed_by_walk(P, y, x)) return 0;  // absorbed earlier in this chain
+  T k;
+  if constexpr (sizeof(T) == 8) {
+    const RecD qy = P.recd[y];
+    const double* qw = (const double*)&qxd;
+    const double* py = (const double*)&qy;
+    k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : py, first ? py : qw, d.c1, d.c2, cc, fflat, P.coeff);
+  } else {
+    const RecF qy = P.recf[y];
+    const float* qw = (const float*)&qxf;
+    const float* py = (const float*)&qy;
+    k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : py, first ? py : qw, d.c1, d.c2, cc, (float)fflat,
+                                        (float)P.coeff);
+  }
+  T prob = k * (T)inv_k_max;
+  if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
+  *y_out = y;
+  *pos_out = (float)((at - c0) / lam);
+  *q_out = q;
+  *first_out = first;
+  return (T)u32d(accu) < prob ? 2 : 1;
+}
+
+// The next accepted test of walker x from s on, drawing tests t_next,
+// t_next + 1, ...: returns 1 with the test's entry in s.j and position in
+// s.at, 0 if the walk ran to the end of the stretch, -1 on a failed check or
+// the test limit.  n_tests counts the tests with a partner.
+template <int KT, class T, bool FLAT>
+__device__ __forceinline__ int walk_next(const PopDev& P, int x, Stretch& s, uint32_t& t_next, const RecD& qxd,
+                                         const RecF& qxf, bool chain, long long* n_tests, int* y, float* pos,
+                                         int* q, bool* first) {
+  for (;;) {
+    const uint32_t t = t_next++;
+    U4 u = walk_draws(P, x, t);
+    double at = s.at - log(u53(u.x, u.y));
+    if (!(at < s.total)) {
+      s.at = at;
+      return 0;  // no test left in the cell's later pairs
+    }
+    if (t >= (1u << 26)) {  // far past any mean the step can ask for
+      set_status(P.ctr, kErrTimeout);
+      return -1;
+    }
+    int j = walk_pair(s, at);
+    s.j = j;
+    s.at = at;
+    int r = walk_test<KT, T, FLAT>(P, x, s, j, at, u.z, u.w, qxd, qxf, chain, y, pos, q, first);
+    if (r < 0) return -1;
+    if (r == 0) continue;
+    (*n_tests)++;
+    if (r == 2) return 1;
+  }
+}
+
+// The first event of walker x from (p0, pos0): the first accepted test,
+// claimed by its merge decision; an absorb (the walking particle is replaced
+// by the coagulated one) is carried on as a chain by k_chain from the next
+// test on.
 template <int KT, class T, bool FLAT>
 __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, float pos0, WalkOut* out) {
   if (x < 0 || x >= P.cap || !P.alive[x]) return;
   const int C = P.cell[x];
   if (C < 0 || C >= P.n_cells) return;
-  const int nb = P.grid->n_bin;
-  Rng g = make_rng(P, kStreamWalk, 0u, (uint32_t)x);
-  long long n_tests = 0, n_iter = 0;
-  // the pairs of cell C from (p0, pos0) on, as one stretch of expected
-  // tests: cum[j] over the cell's pairs (cp_cum)
-  int lo = P.cp_off[C], end = P.cp_off[C + 1];
-  const double* cum = P.cp_cum + (P.cp_off[C] + C) - lo;  // cum[j], j = lo..end
-  {
-    int hi = end;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (P.cp_list[mid] < p0) lo = mid + 1;
-      else hi = mid;
-    }
-  }
-  double at = cum[lo];
-  if (lo < end && P.cp_list[lo] == p0) at += (cum[lo + 1] - cum[lo]) * (double)pos0;
-  const double at_end = cum[end];
-  int j = lo;
-  for (;;) {
-    at += -log(g.next());
-    if (!(at < at_end)) {
-      out->done = true;  // no test left in the cell's later pairs
-      break;
-    }
-    if (++n_iter > (1LL << 26)) {  // far past any mean the step can ask for
-      set_status(P.ctr, kErrTimeout);
-      break;
-    }
-    {
-      // the pair whose stretch holds at: cum[j] <= at < cum[j + 1]
-      int a = j, b = end - 1;
-      while (a < b) {
-        int mid = (a + b + 1) >> 1;
-        if (cum[mid] <= at) a = mid;
-        else b = mid - 1;
-      }
-      j = a;
-    }
-    int q = P.cp_list[j];
-    double lam = cum[j + 1] - cum[j];
-    if (!(lam > 0.0)) continue;
-    double pos = (at - cum[j]) / lam;
+  Stretch s;
+  walk_stretch(P, C, p0, pos0, &s);
+  const RecD qxd = P.recd[x];
+  const RecF qxf = P.recf[x];
+  long long n_tests = 0;
+  uint32_t t_next = 0;
+  int y, q;
+  float pos;
+  bool first;
+  int r = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, false, &n_tests, &y, &pos, &q, &first);
+  if (r == 0) out->done = true;
+  if (r == 1) {
+    const PairDesc d = P.pair_desc[q];
     const PairState& S = P.pair[q];
-    PairDesc d = P.pair_desc[q];
-    int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
-    int O = cell1 == C ? cell2 : cell1;
-    int n_o = P.cell_count[O];
-    int o_start = P.cell_start[O];
-    if (n_o < 1) continue;
-    if (o_start < 0 || (long long)o_start + n_o > P.cap) {
-      bad_index(P.ctr, kBadPairCells, q);
-      break;
-    }
-    int i = (int)(g.next() * (double)n_o);
-    if (i >= n_o) i = n_o - 1;
-    int y = P.list[o_start + i];
-    if (y < 0 || y >= P.cap) {
-      bad_index(P.ctr, kBadTestSlot, y);
-      continue;
-    }
-    if (y == x || !P.alive[y] || P.cell[y] != O) continue;
-    n_tests++;
-    bool first = cell1 == C;
-    T k;
-    if constexpr (sizeof(T) == 8) {
-      const double* qw = (const double*)&P.recd[x];
-      const double* qy = (const double*)&P.recd[y];
-      k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, S.fflat, P.coeff);
-    } else {
-      const float* qw = (const float*)&P.recf[x];
-      const float* qy = (const float*)&P.recf[y];
-      k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : qy, first ? qy : qw, d.c1, d.c2, S.cc, (float)S.fflat,
-                                          (float)P.coeff);
-    }
-    T prob = k * (T)S.inv_k_max;
-    if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
-    if (!((T)g.next() < prob)) continue;
-    // the first accepted test: an event of the next step of the round,
-    // claimed by its merge decision; an absorb (the walking particle is
-    // replaced by the coagulated one) continues as a chain
     unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
     unsigned long long ck = claim_key(P, key);
     Rng gm = merge_rng(P, key);
@@ -615,19 +576,18 @@ __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, floa
     out->found = true;
     out->q = q;
     out->y = y;
-    out->pos = (float)pos;
+    out->pos = pos;
     out->first_cell1 = first;
     out->dec = pack_decision(m, gm.used());
     if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
     claim_slot(P, x, ck, rm_x);
     claim_slot(P, y, ck, rm_y);
     out->cont = m.create && rm_x && m.new_group != 0;
-    out->g_used = g.used();
-    break;
+    out->g_used = t_next;
   }
   if (n_tests) {
-    add_ll(&P.ctr->tot_samp, n_tests);
-    add_ll(&P.ctr->walk_tests, n_tests);
+    add_ll_warp(&P.ctr->tot_samp, (int)n_tests);
+    add_ll_warp(&P.ctr->walk_tests, (int)n_tests);
   }
 }
 
@@ -728,10 +688,17 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
 }
 
 // Chains, after k_items: an item whose first event is an absorb (it_len -1)
-// carries its walk on from that event with the coagulated particle
-// (walk_chain), from the stream position the walk had reached.  The chain's
-// events go to the pool, the first one included; the item gets the chain's
-// length and head, or length 0 (the first event alone) if the pool is full.
+// carries its walk on from that event with the coagulated particle, one
+// thread per chain, drawing the walk's tests on from where k_items stopped.
+// The coagulated particle's volumes are summed per species over the events,
+// then over the species, as k_apply_chain sums them, so its decisions are
+// the apply's.  While the particle stays in the cell it walked, the walk goes
+// on in place; a new cell's stretch starts at the event's pair and position.
+// The next accepted test is the next event: an absorb extends the chain, any
+// other decision ends the chain before it (the walk resumes there in the
+// next round).  The chain's events go to the pool, the first one included;
+// the item gets the chain's length and head, or length 0 (the first event
+// alone) if the pool is full.
 template <int KT, class T, bool FLAT>
 __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gpair_pop, const long long* n_items,
                                                const uint8_t* it_flag, const unsigned long long* it_key,
@@ -744,28 +711,68 @@ __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gp
     if (!it_flag[e] || it_len[e] != -1) continue;
     const PopDev& P = pops[gpair_pop[it_gp[e]]];
     unsigned long long key = it_key[e];
-    int x = (int)key_idx(key), q = (int)key_pair(key);
+    const int x = (int)key_idx(key);
+    int q = (int)key_pair(key);
     int2 sl = it_c[e];
-    bool first = sl.x == x;
-    int y = first ? sl.y : sl.x;
+    int y = sl.x == x ? sl.y : sl.x;
     uint32_t used;
-    MergeDecision m = unpack_decision(it_dec[e], &used);
-    bool rm_y = first ? m.rm2 : m.rm1;
+    MergeDecision m1 = unpack_decision(it_dec[e], &used);
+    bool rm_y1 = sl.x == x ? m1.rm2 : m1.rm1;
     it_len[e] = 0;
     if (x < 0 || x >= P.cap || y < 0 || y >= P.cap || q >= P.n_pairs) continue;
     ChainWriter cw;
-    if (!cw.append(pool, y, q | (rm_y ? kChainRemoves : 0), it_pos[e])) continue;
-    Rng g = make_rng(P, kStreamWalk, 0u, (uint32_t)x);
-    g.seek(it_gused[e]);
-    WalkOut out;
+    float pos = it_pos[e];
+    if (!cw.append(pool, y, q | (rm_y1 ? kChainRemoves : 0), pos)) continue;
+    uint32_t t_next = it_gused[e];
     long long n_tests = 0;
-    walk_chain<KT, T, FLAT>(P, pool, x, y, q, (double)it_pos[e], P.pair[q].cc + 1, g, cw, &out, &n_tests);
-    it_len[e] = cw.len;
+    bool done = false;
+    const int ns = P.n_spec;
+    double vcur[kMaxSpec];
+    for (int sp = 0; sp < ns; sp++) vcur[sp] = P.vol[vol_at(P, x, sp)];
+    int cls = P.pair[q].cc + 1;
+    Stretch s;
+    s.C = -1;
+    for (;;) {
+      // absorb y: the coagulated particle's volumes, radius, class, record
+      for (int sp = 0; sp < ns; sp++) vcur[sp] = vcur[sp] + P.vol[vol_at(P, y, sp)];
+      double s_v = 0.0, s_m = 0.0;
+      for (int sp = 0; sp < ns; sp++) s_v = s_v + vcur[sp];
+      for (int sp = 0; sp < ns; sp++) s_m = s_m + vcur[sp] * P.density[sp];
+      const double vt = s_v, r = vol2rad(vt);
+      const RecD qxd = make_rec_v(P, r, vt, s_m, cls);
+      const RecF qxf = to_f32(qxd);
+      const int C = cell_of(P, r, cls);
+      if (C < 0 || cw.len >= kChainMaxLen) break;  // off the grid (reported by the apply) or long enough
+      if (C != s.C) walk_stretch(P, C, q, pos, &s);
+      int yy, qq;
+      bool first;
+      int rw = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, true, &n_tests, &yy, &pos, &qq, &first);
+      if (rw == 0) done = true;  // every later pair of the cell was walked
+      if (rw != 1) break;
+      const PairDesc d = P.pair_desc[qq];
+      const PairState& S = P.pair[qq];
+      unsigned long long k2 = make_key((uint32_t)qq, 1u, (uint32_t)x);
+      Rng gm = make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
+      double ry = P.rad[yy], vty = P.vtot[yy];
+      MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
+                              : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
+      bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
+      // the chain ends before an event that is no absorb, or when the pool
+      // is full; the walk resumes there in the next round
+      if (!(m.create && rm_x && m.new_group != 0) || !cw.append(pool, yy, qq | (rm_y ? kChainRemoves : 0), pos))
+        break;
+      claim_slot(P, yy, claim_key(P, k2), rm_y);
+      y = yy;
+      q = qq;
+      cls = S.cc + 1;
+    }
+    // a chain that ended at its first event is that event alone
+    it_len[e] = cw.len > 1 ? cw.len : 0;
     it_head[e] = cw.head;
-    it_done[e] = out.done ? 1 : 0;
+    it_done[e] = done ? 1 : 0;
     if (n_tests) {
-      add_ll(&P.ctr->tot_samp, n_tests);
-      add_ll(&P.ctr->walk_tests, n_tests);
+      add_ll_warp(&P.ctr->tot_samp, (int)n_tests);
+      add_ll_warp(&P.ctr->walk_tests, (int)n_tests);
     }
   }
 }
@@ -773,142 +780,251 @@ __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gp
 // Apply the winning chains (win[e] == 2), one warp per chain: the first
 // ev_app[e] events in order, each a coagulate (coagulation.F90:928-985) of
 // the walking particle with the next partner, with the merge decision
-// recomputed from the values and the stream the walk used.  Lanes hold the
-// particle's species (lane, lane + 32) and components (lane); every lane
-// draws the same merge decision and component selection; sums run in the
-// walk's order (per species over the events, then over the species), so the
-// decisions are the walk's.  The coagulated particle stays in the walking
-// particle's slot; partners that a decision removes are killed.  dest[e],
+// recomputed from the values and the stream the walk used.  One warp per
+// chain of the round's list (chain_list, filled by k_resolve_set); a chain's entries
+// are taken a pool chunk at a time (kBatch events):
+//   1. lane k loads event k's partner (slot, pair, radius, scalar fields,
+//      species volumes) into shared memory;
+//   2. lane s runs species s's sum over the events (the walking particle's
+//      volume plus the partners' in order), keeping the sum after each event;
+//   3. lane k totals event k's sums over the species (the walk's order, so
+//      the values and decisions are the walk's), takes the radius and cell,
+//      and draws event k's merge decision from the particle before event k;
+//   4. the events' scalar fields and components are merged in order (lanes
+//      hold components), and removed partners are killed.
+// The coagulated particle stays in the walking particle's slot.  dest[e],
 // gp_c[e] and ev_pos[e] are set to where the particle walks on (dest -1 if
 // its walk ran to the end).
-__global__ void __launch_bounds__(256) k_apply_chain(const PopDev* pops, const int* gpair_pop,
-                                                     const long long* pop_pair_base, const long long* n_events,
-                                                     const unsigned long long* ev_key, const uint8_t* win,
-                                                     const int* ev_len, const int* ev_app, const int* ev_head,
-                                                     const uint8_t* ev_done, ChainPool pool, int* gp_c, float* ev_pos,
-                                                     int* dest_out) {
+struct ChainStage {
+  int y, q, cell1, cc;
+  int c1, c2;
+  float pos;
+  int pad;
+  double ry, vty, ice_y;
+  PScal s;
+};
+constexpr int kApplyBatch = kChainChunk - 1;
+
+__global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const int* gpair_pop,
+                                                    const long long* pop_pair_base, const int* chain_list,
+                                                    const long long* n_chain, const unsigned long long* ev_key,
+                                                    const int* ev_len, const int* ev_app, const int* ev_head,
+                                                    const uint8_t* ev_done, ChainPool pool, int* gp_c, float* ev_pos,
+                                                    int* dest_out) {
   constexpr unsigned kFull = 0xffffffffu;
-  long long E = *n_events;
-  const int lane = threadIdx.x & 31;
-  long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long e = warp; e < E; e += n_warps) {
-    if (win[e] != 2) continue;  // the same e for the whole warp
-    int pop = gpair_pop[gp_c[e]];
-    const PopDev& P = pops[pop];
-    unsigned long long key1 = ev_key[e];
-    int x = (int)key_idx(key1);
-    int app = ev_app[e];
-    if (x < 0 || x >= P.cap) {
-      if (lane == 0) bad_index(P.ctr, kBadEventSlot, x);
-      continue;
-    }
-    const int nb = P.grid->n_bin, ns = P.n_spec;
-    uint32_t gen = *P.gen_p;
-    // the walking particle, spread over the lanes
-    double v_lo = lane < ns ? P.vol[vol_at(P, x, lane)] : 0.0;
-    double v_hi = lane + 32 < ns ? P.vol[vol_at(P, x, lane + 32)] : 0.0;
-    PScal cur;
-    load_scal(P, x, cur);
-    int cc_ = 0;
-    double ct_ = 0.0;
-    if (lane < cur.ncomp && lane < kMaxComponent) {
-      cc_ = P.csrc[comp_at(x, lane)];
-      ct_ = P.ctime[comp_at(x, lane)];
-    }
-    double r = P.rad[x], vt = P.vtot[x];
-    int C = P.cell[x];
-    ChainReader rd(ev_head[e]);
-    int done_ev = 0, last_q = -1, dlive = 0;
-    float last_pos = 0.f;
-    for (int i = 0; i < app; i++) {
-      long long ix = rd.next(pool);
-      int y = ix < 0 ? -1 : pool.y[ix];
-      int q = ix < 0 ? -1 : (pool.q[ix] & kChainPairMask);
-      if (ix < 0 || y < 0 || y >= P.cap || q >= P.n_pairs) {
-        if (lane == 0) bad_index(P.ctr, kBadEventSlot, y);
-        break;
+  constexpr int kBatch = kApplyBatch;
+  __shared__ ChainStage stage[kBatch];
+  __shared__ double pre[kBatch * kMaxSpec];  // [event][species]
+  const long long n_ch = *n_chain;
+  const int lane = threadIdx.x;
+  for (long long ci = blockIdx.x; ci < n_ch; ci += gridDim.x) {
+    {
+      const long long e = chain_list[ci];
+      int pop = gpair_pop[gp_c[e]];
+      const PopDev& P = pops[pop];
+      unsigned long long key1 = ev_key[e];
+      int x = (int)key_idx(key1);
+      int app = ev_app[e];
+      if (x < 0 || x >= P.cap) {
+        if (lane == 0) bad_index(P.ctr, kBadEventSlot, x);
+        continue;
       }
-      PairDesc d = P.pair_desc[q];
-      const PairState& S = P.pair[q];
-      bool first = C == d.b1 + nb * d.c1;
-      Rng g = i == 0 ? merge_rng(P, key1) : make_rng(P, kStreamChain, (uint32_t)(i + 1), (uint32_t)x);
-      double ry = P.rad[y], vty = P.vtot[y];
-      MergeDecision m = first ? merge_decide_v(P, g, r, vt, ry, vty, d.c1, d.c2, S.cc)
-                              : merge_decide_v(P, g, ry, vty, r, vt, d.c1, d.c2, S.cc);
-      bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
-      bool lost_x = first ? m.lost1 : m.lost2, lost_y = first ? m.lost2 : m.lost1;
-      if (!(m.create && rm_x && m.new_group != 0) || (lost_x && !(rm_y && !lost_y))) {
-        if (lane == 0) set_status(P.ctr, kErrAssert);  // the walk decided an absorb here
-        break;
+      const int nb = P.grid->n_bin, ns = P.n_spec;
+      const int w_ice = P.i_water - 1;  // -1: no water species
+      uint32_t gen = *P.gen_p;
+      // the walking particle: species (lane, lane + 32), scalars, components (lane)
+      double v_lo = lane < ns ? P.vol[vol_at(P, x, lane)] : 0.0;
+      double v_hi = lane + 32 < ns ? P.vol[vol_at(P, x, lane + 32)] : 0.0;
+      double ice_cur = w_ice >= 0 ? P.vol[vol_at(P, x, w_ice)] : 0.0;
+      PScal cur;
+      load_scal(P, x, cur);
+      int cc_ = 0;
+      double ct_ = 0.0;
+      if (lane < cur.ncomp && lane < kMaxComponent) {
+        cc_ = P.csrc[comp_at(x, lane)];
+        ct_ = P.ctime[comp_at(x, lane)];
       }
-      // the partner
-      PScal ys;
-      load_scal(P, y, ys);
-      double y_lo = lane < ns ? P.vol[vol_at(P, y, lane)] : 0.0;
-      double y_hi = lane + 32 < ns ? P.vol[vol_at(P, y, lane + 32)] : 0.0;
-      int yc = 0;
-      double yt = 0.0;
-      if (lane < ys.ncomp && lane < kMaxComponent) {
-        yc = P.csrc[comp_at(y, lane)];
-        yt = P.ctime[comp_at(y, lane)];
-      }
-      double ice_x = 0.0, ice_y = 0.0;
-      if (P.i_water > 0) {
-        int w = P.i_water - 1;
-        ice_x = __shfl_sync(kFull, w < 32 ? v_lo : v_hi, w & 31);
-        ice_y = __shfl_sync(kFull, w < 32 ? y_lo : y_hi, w & 31);
-      }
-      // components of aero_particle_coagulate with a = particle 1, b = particle 2
-      const PScal& A = first ? cur : ys;
-      const PScal& B = first ? ys : cur;
-      int ca = first ? cc_ : yc, cb = first ? yc : cc_;
-      double ta = first ? ct_ : yt, tb = first ? yt : ct_;
-      int na = A.ncomp, nbc = B.ncomp;
-      int n1_new = na, n2_new = nbc;
-      bool from_a = lane < na;
-      int k_src = from_a ? lane : lane - na;
-      if (na + nbc > kMaxComponent) {
-        int sa[kMaxComponent], sb[kMaxComponent];
-        coag_components(g, na, A.nprim, nbc, B.nprim, &n1_new, &n2_new, sa, sb);
-        from_a = lane < n1_new;
-        k_src = 0;
-        if (from_a) k_src = sa[lane] - 1;
-        else if (lane - n1_new < n2_new) k_src = sb[lane - n1_new] - 1;
-      }
-      k_src &= 31;
-      int xa = __shfl_sync(kFull, ca, k_src), xb = __shfl_sync(kFull, cb, k_src);
-      double za = __shfl_sync(kFull, ta, k_src), zb = __shfl_sync(kFull, tb, k_src);
-      int n_out = n1_new + n2_new;
-      PScal nm;
-      coag_scalars(A, first ? ice_x : ice_y, B, first ? ice_y : ice_x, nm);
-      nm.ncomp = n_out;
-      nm.id = !lost_x ? cur.id : ys.id;
-      nm.grp = m.new_group;
-      nm.cls = S.cc + 1;
-      cc_ = lane < n_out ? (from_a ? xa : xb) : 0;
-      ct_ = lane < n_out ? (from_a ? za : zb) : 0.0;
-      // volumes: per species over the events, then the total over the species
-      v_lo = v_lo + y_lo;
-      v_hi = v_hi + y_hi;
-      double s_v = 0.0;
-      for (int s = 0; s < ns; s++) s_v = s_v + __shfl_sync(kFull, s < 32 ? v_lo : v_hi, s & 31);
-      vt = s_v;
-      r = vol2rad(vt);
-      C = cell_of(P, r, nm.cls);
-      if (rm_y) {
-        if (lane == 0) {
-          kill_slot(P, y);
-          P.touched[y] = gen;
+      double r = P.rad[x], vt = P.vtot[x];
+      int C = P.cell[x];
+      int chunk = ev_head[e];
+      int done_ev = 0, last_q = -1, dlive = 0;
+      float last_pos = 0.f;
+      bool stop = false;
+      for (int base = 0; base < app && !stop; base += kBatch) {
+        const int nbatch = app - base < kBatch ? app - base : kBatch;
+        // 1. the chunk's partners, one lane each
+        const bool chunk_ok = chunk >= 0 && (long long)chunk < pool.n_chunks;  // the same on every lane
+        bool bad = !chunk_ok;
+        if (chunk_ok && lane < nbatch) {
+          size_t ix = (size_t)chunk * kChainChunk + lane;
+          int y = pool.y[ix];
+          int q = pool.q[ix] & kChainPairMask;
+          bad = y < 0 || y >= P.cap || q >= P.n_pairs;
+          if (!bad) {
+            ChainStage& st = stage[lane];
+            const PairDesc d = P.pair_desc[q];
+            st.y = y;
+            st.q = q;
+            st.cell1 = d.b1 + nb * d.c1;
+            st.c1 = d.c1;
+            st.c2 = d.c2;
+            st.cc = P.pair[q].cc;
+            st.pos = pool.pos[ix];
+            st.ry = P.rad[y];
+            st.vty = P.vtot[y];
+            st.ice_y = w_ice >= 0 ? P.vol[vol_at(P, y, w_ice)] : 0.0;
+            load_scal(P, y, st.s);
+            for (int sp = 0; sp < ns; sp++) pre[lane * kMaxSpec + sp] = P.vol[vol_at(P, y, sp)];
+          }
         }
-        dlive--;
+        // entries past the first bad one are not applied
+        const unsigned bad_mask = __ballot_sync(kFull, bad && lane < nbatch);
+        const int n_ok = bad_mask ? __ffs(bad_mask) - 1 : nbatch;
+        if (chunk_ok) chunk = pool.y[(size_t)chunk * kChainChunk + kChainChunk - 1];
+        __syncwarp();
+        // 2. per species, the sums after each event
+        const double v_lo0 = v_lo, v_hi0 = v_hi;
+        for (int k = 0; k < n_ok; k++) {
+          if (lane < ns) {
+            v_lo = v_lo + pre[k * kMaxSpec + lane];
+            pre[k * kMaxSpec + lane] = v_lo;
+          }
+          if (lane + 32 < ns) {
+            v_hi = v_hi + pre[k * kMaxSpec + lane + 32];
+            pre[k * kMaxSpec + lane + 32] = v_hi;
+          }
+        }
+        __syncwarp();
+        // 3. per event: total, radius, cell, merge decision
+        double vt_k = 0.0, r_k = 0.0;
+        int C_k = -1;
+        if (lane < n_ok) {
+          double s_v = 0.0;
+          for (int sp = 0; sp < ns; sp++) s_v = s_v + pre[lane * kMaxSpec + sp];
+          vt_k = s_v;
+          r_k = vol2rad(vt_k);
+          C_k = cell_of(P, r_k, stage[lane].cc + 1);
+        }
+        double r_b = __shfl_up_sync(kFull, r_k, 1), vt_b = __shfl_up_sync(kFull, vt_k, 1);
+        int C_b = __shfl_up_sync(kFull, C_k, 1);
+        if (lane == 0) {
+          r_b = r;
+          vt_b = vt;
+          C_b = C;
+        }
+        bool ok = true, first_k = false, rm_y_k = false, lost_x_k = false;
+        int group_k = 0;
+        uint32_t used_k = 0;
+        if (lane < n_ok) {
+          const ChainStage& st = stage[lane];
+          first_k = C_b == st.cell1;
+          const int i = base + lane;
+          Rng g = i == 0 ? merge_rng(P, key1) : make_rng(P, kStreamChain, (uint32_t)(i + 1), (uint32_t)x);
+          MergeDecision m = first_k ? merge_decide_v(P, g, r_b, vt_b, st.ry, st.vty, st.c1, st.c2, st.cc)
+                                    : merge_decide_v(P, g, st.ry, st.vty, r_b, vt_b, st.c1, st.c2, st.cc);
+          bool rm_x = first_k ? m.rm1 : m.rm2;
+          rm_y_k = first_k ? m.rm2 : m.rm1;
+          lost_x_k = first_k ? m.lost1 : m.lost2;
+          bool lost_y = first_k ? m.lost2 : m.lost1;
+          ok = m.create && rm_x && m.new_group != 0 && !(lost_x_k && !(rm_y_k && !lost_y));
+          group_k = m.new_group;
+          used_k = g.used();
+        }
+        const unsigned bad_dec = __ballot_sync(kFull, lane < n_ok && !ok);
+        const int n_app = bad_dec ? __ffs(bad_dec) - 1 : n_ok;
+        if (bad_dec) {
+          if (lane == 0) set_status(P.ctr, kErrAssert);  // the walk decided an absorb here
+          stop = true;
+        }
+        // 4. scalar fields and components, in order
+        int yc = 0;
+        double yt = 0.0;
+        if (n_app > 0 && lane < stage[0].s.ncomp && lane < kMaxComponent) {
+          yc = P.csrc[comp_at(stage[0].y, lane)];
+          yt = P.ctime[comp_at(stage[0].y, lane)];
+        }
+        for (int k = 0; k < n_app; k++) {
+          const ChainStage& st = stage[k];
+          // the next partner's components, loaded ahead
+          int yc_n = 0;
+          double yt_n = 0.0;
+          if (k + 1 < n_app && lane < stage[k + 1].s.ncomp && lane < kMaxComponent) {
+            yc_n = P.csrc[comp_at(stage[k + 1].y, lane)];
+            yt_n = P.ctime[comp_at(stage[k + 1].y, lane)];
+          }
+          const bool first = __shfl_sync(kFull, first_k ? 1 : 0, k) != 0;
+          const bool rm_y = __shfl_sync(kFull, rm_y_k ? 1 : 0, k) != 0;
+          const bool lost_x = __shfl_sync(kFull, lost_x_k ? 1 : 0, k) != 0;
+          const int new_group = __shfl_sync(kFull, group_k, k);
+          const uint32_t used = __shfl_sync(kFull, used_k, k);
+          const PScal ys = st.s;
+          const double ice_x = k == 0 ? ice_cur : (w_ice >= 0 ? pre[(k - 1) * kMaxSpec + w_ice] : 0.0);
+          const double ice_y = st.ice_y;
+          // components of aero_particle_coagulate with a = particle 1, b = particle 2
+          const PScal& A = first ? cur : ys;
+          const PScal& B = first ? ys : cur;
+          int ca = first ? cc_ : yc, cb = first ? yc : cc_;
+          double ta = first ? ct_ : yt, tb = first ? yt : ct_;
+          int na = A.ncomp, nbc = B.ncomp;
+          int n1_new = na, n2_new = nbc;
+          bool from_a = lane < na;
+          int k_src = from_a ? lane : lane - na;
+          if (na + nbc > kMaxComponent) {
+            const int i = base + k;
+            Rng g = i == 0 ? merge_rng(P, key1) : make_rng(P, kStreamChain, (uint32_t)(i + 1), (uint32_t)x);
+            g.seek(used);
+            int sa[kMaxComponent], sb[kMaxComponent];
+            coag_components(g, na, A.nprim, nbc, B.nprim, &n1_new, &n2_new, sa, sb);
+            from_a = lane < n1_new;
+            k_src = 0;
+            if (from_a) k_src = sa[lane] - 1;
+            else if (lane - n1_new < n2_new) k_src = sb[lane - n1_new] - 1;
+          }
+          k_src &= 31;
+          int xa = __shfl_sync(kFull, ca, k_src), xb = __shfl_sync(kFull, cb, k_src);
+          double za = __shfl_sync(kFull, ta, k_src), zb = __shfl_sync(kFull, tb, k_src);
+          int n_out = n1_new + n2_new;
+          PScal nm;
+          coag_scalars(A, first ? ice_x : ice_y, B, first ? ice_y : ice_x, nm);
+          nm.ncomp = n_out;
+          nm.id = !lost_x ? cur.id : ys.id;
+          nm.grp = new_group;
+          nm.cls = st.cc + 1;
+          cc_ = lane < n_out ? (from_a ? xa : xb) : 0;
+          ct_ = lane < n_out ? (from_a ? za : zb) : 0.0;
+          if (rm_y) {
+            if (lane == 0) {
+              kill_slot(P, st.y);
+              P.touched[st.y] = gen;
+            }
+            dlive--;
+          }
+          cur = nm;
+          done_ev++;
+          last_q = st.q;
+          last_pos = st.pos;
+          yc = yc_n;
+          yt = yt_n;
+        }
+        // the particle after the batch's last applied event
+        if (n_app > 0) {
+          r = __shfl_sync(kFull, r_k, n_app - 1);
+          vt = __shfl_sync(kFull, vt_k, n_app - 1);
+          C = __shfl_sync(kFull, C_k, n_app - 1);
+          v_lo = lane < ns ? pre[(n_app - 1) * kMaxSpec + lane] : 0.0;
+          v_hi = lane + 32 < ns ? pre[(n_app - 1) * kMaxSpec + lane + 32] : 0.0;
+          if (w_ice >= 0) ice_cur = pre[(n_app - 1) * kMaxSpec + w_ice];
+        } else {
+          v_lo = v_lo0;
+          v_hi = v_hi0;
+        }
+        if (n_ok < nbatch && !stop) {
+          if (lane == 0) bad_index(P.ctr, kBadEventSlot, -1);
+          stop = true;
+        }
+        __syncwarp();  // the stage is read before the next chunk overwrites it
       }
-      cur = nm;
-      done_ev++;
-      last_q = q;
-      last_pos = pool.pos[ix];
-    }
-    if (done_ev == 0) continue;
+      if (done_ev == 0) continue;
     // the coagulated particle in the walking particle's slot
     __syncwarp();
     if (lane < ns) P.vol[vol_at(P, x, lane)] = v_lo;
@@ -948,6 +1064,7 @@ __global__ void __launch_bounds__(256) k_apply_chain(const PopDev* pops, const i
       gp_c[e] = (int)(pop_pair_base[pop] + last_q);
       ev_pos[e] = last_pos;
     }
+    }
   }
 }
 
@@ -973,11 +1090,13 @@ __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
     if (j < hi) {
       int q = P.cp_list[j];
       const PairState& S = P.pair[q];
+      PairDesc d = P.pair_desc[q];
+      int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
+      int O = cell1 == c ? cell2 : cell1;
+      int n_o = P.cell_count[O];
+      P.cp_ent[j] = make_int4(q, O | (cell1 == c ? (1 << 30) : 0), P.cell_start[O], n_o);
       if (S.path != kPathParticle) {
-        PairDesc d = P.pair_desc[q];
-        int cell1 = d.b1 + nb * d.c1, cell2 = d.b2 + nb * d.c2;
-        int O = cell1 == c ? cell2 : cell1;
-        double l = S.k_max * P.del_t * (double)P.cell_count[O];
+        double l = S.k_max * P.del_t * (double)n_o;
         if (l > 0.0) lam = l;
       }
     }
@@ -995,7 +1114,20 @@ __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
     if (threadIdx.x == 0) carry += wsum[0] + wsum[1] + wsum[2] + wsum[3];
     __syncthreads();
   }
-  if (threadIdx.x == 0) cum[hi - lo] = carry;
+  const double total = carry;
+  if (threadIdx.x == 0) cum[hi - lo] = total;
+  // the bucket table: the last entry whose stretch starts at or before each
+  // bucket's start (cum is visible to the block after the barrier above)
+  if (threadIdx.x < kWalkTab) {
+    double target = total * (double)threadIdx.x / (double)kWalkTab;
+    int a = 0, b = hi - lo - 1;
+    while (a < b) {
+      int mid = (a + b + 1) >> 1;
+      if (cum[mid] <= target) a = mid;
+      else b = mid - 1;
+    }
+    P.cp_tab[c * kWalkTab + threadIdx.x] = lo + a;
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -191,6 +191,12 @@ struct PopDev {
   // expected walk tests (k_max * del_t * members of the other cell) of the
   // cell's first j pairs
   double* cp_cum;      // [cp_off[n_cells] + n_cells]
+  // with the rates, per entry j of the lists: {pair, other cell (bit 30 set
+  // if this cell is the pair's first), the other cell's start and members}
+  int4* cp_ent;        // [cp_off[n_cells]]
+  // per cell, kWalkTab buckets of its stretch of tests: entry b is the last
+  // j of the cell with cp_cum[j] <= b / kWalkTab of the cell's total
+  int* cp_tab;         // [n_cells * kWalkTab]
 
   // [cap] lowest claim key (claim_key) of the current round's events that
   // remove or rewrite the slot, and of those that only read it; a key from
@@ -227,6 +233,7 @@ __host__ __device__ __forceinline__ uint32_t key_idx(unsigned long long k) { ret
 // claim generations live in the top 11 bits of a claim word; the host
 // restarts them (clearing every claim and touched word) before they run out
 constexpr uint32_t kGenLimit = 2047;
+constexpr int kWalkTab = 64;  // buckets of a cell's walk stretch (cp_tab)
 
 #ifdef __CUDACC__
 // claim word of an event key in the current round: a later generation gives
