@@ -28,6 +28,12 @@ sys.path.insert(0, HERE)
 
 B_TEST = 56  # algorithmic bytes per pair test: two cell-list entries and two 24-byte records
 B_SORT = 8  # per slot: its cell key read, its cell-list entry written
+# DRAM traffic per unit (dram__bytes_read.sum + dram__bytes_write.sum) from
+# ncu captures of one launch at this workload: k_test read 46.91 MB and wrote
+# 1.12 MB for about 209,000 tests; k_sort_all read 4.04 MB and wrote none for
+# 1e6 slots.  The roofline's traffic scales these by the units of a launch.
+DRAM_TEST = (46.91e6 + 1.12e6) / 209000
+DRAM_SORT = 4.04e6 / 1e6
 
 
 def parse():
@@ -481,9 +487,9 @@ def main():
         tsc, nsc, usc = prof["sort"]
         # dominant kernel by measured time
         if tsc >= ttest:
-            dom, t_tot, n_l, units, bpu = "k_sort_all (cell counting sort)", tsc, nsc, usc, B_SORT
+            dom, t_tot, n_l, units, bpu, dpu = "k_sort_all (cell counting sort)", tsc, nsc, usc, B_SORT, DRAM_SORT
         else:
-            dom, t_tot, n_l, units, bpu = "k_test (pair tests)", ttest, ntest, utest, B_TEST
+            dom, t_tot, n_l, units, bpu, dpu = "k_test (pair tests)", ttest, ntest, utest, B_TEST, DRAM_TEST
         avg_ms = t_tot / max(n_l, 1)
         bytes_per_launch = units / max(n_l, 1) * bpu
         achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
@@ -511,7 +517,8 @@ def main():
             "sim_s_per_s": args.steps * args.del_t * ws / t_max,
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": units / max(n_l, 1) * dpu, "traffic_unit": "bytes per launch (ncu, scaled)",
                          "avg_launch_ms": avg_ms, "launches": n_l,
                          "bytes_per_unit": bpu, "units_per_launch": units / max(n_l, 1)},
             "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "units": v[2]} for k, v in prof.items()

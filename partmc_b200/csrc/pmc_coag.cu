@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1098,6 +1099,16 @@ void alloc_sort(Ctx& c, PopHost& ph) {
       list[fill[a]++] = p;
       if (b != a) list[fill[b]++] = p;
     }
+    int max_len = 1;
+    for (int k = 0; k < h.n_cells; k++) max_len = std::max(max_len, off[k + 1] - off[k]);
+    const int n_coarse = ((max_len + 15) / 16 + 3) / 4 * 4;
+    std::vector<int> coarse((size_t)h.n_cells * n_coarse, INT_MAX);
+    for (int k = 0; k < h.n_cells; k++)
+      for (int j = off[k], i = 0; j < off[k + 1]; j += 16, i++) coarse[(size_t)k * n_coarse + i] = list[j];
+    int* d_coarse = dalloc<int>(o, coarse.size());
+    CK(cudaMemcpyAsync(d_coarse, coarse.data(), sizeof(int) * coarse.size(), cudaMemcpyHostToDevice, c.stream));
+    h.cp_coarse = d_coarse;
+    h.n_coarse = n_coarse;
     int* d_off = dalloc<int>(o, off.size());
     int* d_list = dalloc<int>(o, list.size());
     h.cp_cum = dalloc<double>(o, (size_t)off[h.n_cells] + h.n_cells);
@@ -1797,8 +1808,8 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
                                    c.slot_base_pp.p, c.id_base_pp.p);
   note_launch();
   if (W > 0) {
-    // part 1, one warp per event: species and components
-    k_apply_move<<<grid_for(W * 32, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+    // part 1, one thread per event: species and components
+    k_apply_move<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
                                                         c.win_set.p, c.dec_set.p, c.rank_slot_set.p,
                                                         c.slot_base_set.p, c.ice_set.p);
     note_launch();

@@ -146,25 +146,27 @@ __device__ __forceinline__ int event_dest(const MergeDecision& m, int s1, int s2
 }
 
 // Apply winning per-set events (coagulate, coagulation.F90:928-985), part 1:
-// the per-particle vectors.  One warp per event: lane q adds species q of the
-// two sources (particle-major, so each source is a few cache lines) and lane
-// k places component k; the random component selection is computed by every
-// lane alike from the stream position k_resolve_set stored.  The summed
-// volume and mass go to the destination's caches for part 2; the water
-// volumes of the sources, which part 2 needs after the destination may have
-// been overwritten, go to ice[e].
+// the per-particle vectors, one thread per event.  The species of the two
+// sources (particle-major, each source a few cache lines) are added in blocks
+// of kMoveBlock: a block's loads are all issued before its sums are stored,
+// and the destination (which may be a source) is written species by species
+// after that species was read.  The components are gathered into local
+// arrays before any is written, in the order of the random selection
+// (computed from the stream position the test stored).  The summed volume and
+// mass go to the destination's caches for part 2; the water volumes of the
+// sources, which part 2 needs after the destination may have been
+// overwritten, go to ice[e].
+constexpr int kMoveBlock = 8;
+
 __global__ void __launch_bounds__(256) k_apply_move(const PopDev* pops, const int* gpair_pop,
                                                     const long long* n_events, const unsigned long long* ev_key,
                                                     const int2* ev, const int* ev_gp, const uint8_t* win,
                                                     const uint32_t* dec, const long long* slot_rank,
                                                     const int* slot_base, double2* ice) {
-  constexpr unsigned kFull = 0xffffffffu;
   long long E = *n_events;
-  int lane = threadIdx.x & 31;
-  long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long e = warp; e < E; e += n_warps) {
-    if (win[e] != 1) continue;  // the same e for the whole warp; chains apply in k_apply_chain
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (win[e] != 1) continue;  // chains apply in k_apply_chain
     uint32_t used;
     MergeDecision m = unpack_decision(dec[e], &used);
     if (!m.create) continue;
@@ -175,61 +177,71 @@ __global__ void __launch_bounds__(256) k_apply_move(const PopDev* pops, const in
     int s1 = sl.x, s2 = sl.y;
     int dest = event_dest(m, s1, s2, slot_base[pop], m.rm1 || m.rm2 ? 0 : slot_rank[e]);
     if (dest < 0 || dest >= P.cap) continue;  // reported by part 2
-    // every read of the two sources comes before the first write to dest
-    int na = P.ncomp[s1], nb = P.ncomp[s2];
-    if (P.i_water > 0 && lane == 0)
-      ice[e] = make_double2(P.vol[vol_at(P, s1, P.i_water - 1)], P.vol[vol_at(P, s2, P.i_water - 1)]);
-    int ca = 0, cb = 0;
-    double ta = 0.0, tb = 0.0;
-    if (lane < na && lane < kMaxComponent) {
-      ca = P.csrc[comp_at(s1, lane)];
-      ta = P.ctime[comp_at(s1, lane)];
-    }
-    if (lane < nb && lane < kMaxComponent) {
-      cb = P.csrc[comp_at(s2, lane)];
-      tb = P.ctime[comp_at(s2, lane)];
-    }
     const int ns = P.n_spec;
-    double v_lo = 0.0, v_hi = 0.0;  // species lane and lane + 32
-    if (lane < ns) v_lo = P.vol[vol_at(P, s1, lane)] + P.vol[vol_at(P, s2, lane)];
-    if (lane + 32 < ns) v_hi = P.vol[vol_at(P, s1, lane + 32)] + P.vol[vol_at(P, s2, lane + 32)];
-    int n1_new = na, n2_new = nb;
-    int k_src = lane < na ? lane : lane - na;
-    bool from_a = lane < na;
-    if (na + nb > kMaxComponent) {
-      int np1 = P.nprim[s1], np2 = P.nprim[s2];
-      Rng g = merge_rng(P, ev_key[e]);
-      g.seek(used);
-      int sa[kMaxComponent], sb[kMaxComponent];
-      coag_components(g, na, np1, nb, np2, &n1_new, &n2_new, sa, sb);
-      from_a = lane < n1_new;
-      k_src = 0;
-      if (from_a) k_src = sa[lane] - 1;
-      else if (lane - n1_new < n2_new) k_src = sb[lane - n1_new] - 1;
+    const double* v1 = P.vol + vol_at(P, s1, 0);
+    const double* v2 = P.vol + vol_at(P, s2, 0);
+    double* vd = P.vol + vol_at(P, dest, 0);
+    if (P.i_water > 0) ice[e] = make_double2(v1[P.i_water - 1], v2[P.i_water - 1]);
+    // components: every source entry is read before the first write
+    int na = P.ncomp[s1], nb = P.ncomp[s2];
+    na = na < kMaxComponent ? na : kMaxComponent;
+    nb = nb < kMaxComponent ? nb : kMaxComponent;
+    int ca[kMaxComponent], cb[kMaxComponent];
+    double ta[kMaxComponent], tb[kMaxComponent];
+    for (int k = 0; k < na; k++) {
+      ca[k] = P.csrc[comp_at(s1, k)];
+      ta[k] = P.ctime[comp_at(s1, k)];
     }
-    k_src &= 31;
-    int xa = __shfl_sync(kFull, ca, k_src), xb = __shfl_sync(kFull, cb, k_src);
-    double ya = __shfl_sync(kFull, ta, k_src), yb = __shfl_sync(kFull, tb, k_src);
+    for (int k = 0; k < nb; k++) {
+      cb[k] = P.csrc[comp_at(s2, k)];
+      tb[k] = P.ctime[comp_at(s2, k)];
+    }
     // totals in the reference's order (species 1..n)
     double vt = 0.0, ms = 0.0;
-    for (int q = 0; q < ns && q < 64; q++) {
-      double v = __shfl_sync(kFull, q < 32 ? v_lo : v_hi, q & 31);
-      vt = vt + v;
-      ms = ms + v * P.density[q];
+    for (int s0 = 0; s0 < ns; s0 += kMoveBlock) {
+      double x1[kMoveBlock], x2[kMoveBlock];
+#pragma unroll
+      for (int j = 0; j < kMoveBlock; j++) {
+        x1[j] = s0 + j < ns ? v1[s0 + j] : 0.0;
+        x2[j] = s0 + j < ns ? v2[s0 + j] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < kMoveBlock; j++) {
+        if (s0 + j < ns) {
+          double v = x1[j] + x2[j];
+          vt = vt + v;
+          ms = ms + v * P.density[s0 + j];
+          vd[s0 + j] = v;
+        }
+      }
     }
-    __syncwarp();
-    if (lane < ns) P.vol[vol_at(P, dest, lane)] = v_lo;
-    if (lane + 32 < ns) P.vol[vol_at(P, dest, lane + 32)] = v_hi;
-    int n_out = n1_new + n2_new;
-    if (lane < n_out) {
-      P.csrc[comp_at(dest, lane)] = from_a ? xa : xb;
-      P.ctime[comp_at(dest, lane)] = from_a ? ya : yb;
+    int n1_new = na, n2_new = nb;
+    if (na + nb > kMaxComponent) {
+      int sa[kMaxComponent], sb[kMaxComponent];
+      Rng g = merge_rng(P, ev_key[e]);
+      g.seek(used);
+      coag_components(g, na, P.nprim[s1], nb, P.nprim[s2], &n1_new, &n2_new, sa, sb);
+      for (int k = 0; k < n1_new; k++) {
+        P.csrc[comp_at(dest, k)] = ca[sa[k] - 1];
+        P.ctime[comp_at(dest, k)] = ta[sa[k] - 1];
+      }
+      for (int k = 0; k < n2_new; k++) {
+        P.csrc[comp_at(dest, n1_new + k)] = cb[sb[k] - 1];
+        P.ctime[comp_at(dest, n1_new + k)] = tb[sb[k] - 1];
+      }
+    } else {
+      for (int k = 0; k < na; k++) {
+        P.csrc[comp_at(dest, k)] = ca[k];
+        P.ctime[comp_at(dest, k)] = ta[k];
+      }
+      for (int k = 0; k < nb; k++) {
+        P.csrc[comp_at(dest, na + k)] = cb[k];
+        P.ctime[comp_at(dest, na + k)] = tb[k];
+      }
     }
-    if (lane == 0) {
-      P.vtot[dest] = vt;
-      P.mass[dest] = ms;
-      P.ncomp[dest] = n_out;
-    }
+    P.vtot[dest] = vt;
+    P.mass[dest] = ms;
+    P.ncomp[dest] = n1_new + n2_new;
   }
 }
 
@@ -402,17 +414,27 @@ struct Stretch {
   double at, total;
 };
 
-// the stretch of cell C from (pair p0, position pos0 in it) on: a binary
-// search of the cell's pair list for the first entry whose pair is p0 or later
+// the stretch of cell C from (pair p0, position pos0 in it) on.  The first
+// entry of the cell's pair list whose pair is p0 or later: the cell's coarse
+// row (every 16th entry, read as int4) counts the coarse entries before p0,
+// then the at most 15 entries after the last of them are counted.
 __device__ __forceinline__ void walk_stretch(const PopDev& P, int C, int p0, float pos0, Stretch* s) {
   int lo = P.cp_off[C], end = P.cp_off[C + 1];
   const double* cum = P.cp_cum + (lo + C) - lo;
-  int a = lo, hi = end;
-  while (a < hi) {
-    int mid = (a + hi) >> 1;
-    if (P.cp_list[mid] < p0) a = mid + 1;
-    else hi = mid;
+  const int4* cz = reinterpret_cast<const int4*>(P.cp_coarse + (size_t)C * P.n_coarse);
+  int k = 0;
+#pragma unroll 4
+  for (int b = 0; b < P.n_coarse / 4; b++) {
+    const int4 v = cz[b];
+    k += (v.x < p0) + (v.y < p0) + (v.z < p0) + (v.w < p0);
   }
+  int a = k == 0 ? lo : lo + 16 * (k - 1) + 1;
+  const int hi = min(lo + 16 * k, end);
+  int cnt = 0;
+#pragma unroll
+  for (int t = 0; t < 15; t++)
+    if (a + t < hi) cnt += P.cp_list[a + t] < p0;
+  a += cnt;
   double at = cum[a];
   if (a < end && P.cp_list[a] == p0) at += (cum[a + 1] - cum[a]) * (double)pos0;
   s->cum = cum;
@@ -463,7 +485,8 @@ __device__ __forceinline__ int walk_pair(const Stretch& s, double at) {
 template <int KT, class T, bool FLAT>
 __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& s, int j, double at, uint32_t pick,
                                          uint32_t accu, const RecD& qxd, const RecF& qxf, bool chain, int* y_out,
-                                         float* pos_out, int* q_out, bool* first_out) {
+                                         float* pos_out, int* q_out, bool* first_out, double* ry_out,
+                                         double* vty_out) {
   const double c0 = s.cum[j], c1 = s.cum[j + 1];
   const int4 ent = P.cp_ent[j];
   double lam = c1 - c0;
@@ -488,6 +511,7 @@ __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& 
   }
   const uint8_t alive = P.alive[y];
   const int cell_y = P.cell[y];
+  const double ry = P.rad[y], vty = P.vtot[y];  // for the merge decision if the test accepts
   if (y == x || !alive || cell_y != O) return 0;
   if (chain && claimed_by_walk(P, y, x)) return 0;  // absorbed earlier in this chain
   T k;
@@ -509,6 +533,8 @@ __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& 
   *pos_out = (float)((at - c0) / lam);
   *q_out = q;
   *first_out = first;
+  *ry_out = ry;
+  *vty_out = vty;
   return (T)u32d(accu) < prob ? 2 : 1;
 }
 
@@ -519,7 +545,7 @@ __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& 
 template <int KT, class T, bool FLAT>
 __device__ __forceinline__ int walk_next(const PopDev& P, int x, Stretch& s, uint32_t& t_next, const RecD& qxd,
                                          const RecF& qxf, bool chain, long long* n_tests, int* y, float* pos,
-                                         int* q, bool* first) {
+                                         int* q, bool* first, double* ry, double* vty) {
   for (;;) {
     const uint32_t t = t_next++;
     U4 u = walk_draws(P, x, t);
@@ -535,7 +561,7 @@ __device__ __forceinline__ int walk_next(const PopDev& P, int x, Stretch& s, uin
     int j = walk_pair(s, at);
     s.j = j;
     s.at = at;
-    int r = walk_test<KT, T, FLAT>(P, x, s, j, at, u.z, u.w, qxd, qxf, chain, y, pos, q, first);
+    int r = walk_test<KT, T, FLAT>(P, x, s, j, at, u.z, u.w, qxd, qxf, chain, y, pos, q, first, ry, vty);
     if (r < 0) return -1;
     if (r == 0) continue;
     (*n_tests)++;
@@ -561,7 +587,8 @@ __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, floa
   int y, q;
   float pos;
   bool first;
-  int r = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, false, &n_tests, &y, &pos, &q, &first);
+  double ry, vty;
+  int r = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, false, &n_tests, &y, &pos, &q, &first, &ry, &vty);
   if (r == 0) out->done = true;
   if (r == 1) {
     const PairDesc d = P.pair_desc[q];
@@ -569,7 +596,7 @@ __device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, floa
     unsigned long long key = make_key((uint32_t)q, 1u, (uint32_t)x);
     unsigned long long ck = claim_key(P, key);
     Rng gm = merge_rng(P, key);
-    double rx = P.rad[x], vtx = P.vtot[x], ry = P.rad[y], vty = P.vtot[y];
+    double rx = P.rad[x], vtx = P.vtot[x];
     MergeDecision m = first ? merge_decide_v(P, gm, rx, vtx, ry, vty, d.c1, d.c2, S.cc)
                             : merge_decide_v(P, gm, ry, vty, rx, vtx, d.c1, d.c2, S.cc);
     bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
@@ -746,14 +773,15 @@ __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gp
       if (C != s.C) walk_stretch(P, C, q, pos, &s);
       int yy, qq;
       bool first;
-      int rw = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, true, &n_tests, &yy, &pos, &qq, &first);
+      double ry, vty;
+      int rw = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, true, &n_tests, &yy, &pos, &qq, &first, &ry,
+                                      &vty);
       if (rw == 0) done = true;  // every later pair of the cell was walked
       if (rw != 1) break;
       const PairDesc d = P.pair_desc[qq];
       const PairState& S = P.pair[qq];
       unsigned long long k2 = make_key((uint32_t)qq, 1u, (uint32_t)x);
       Rng gm = make_rng(P, kStreamChain, (uint32_t)(cw.len + 1), (uint32_t)x);
-      double ry = P.rad[yy], vty = P.vtot[yy];
       MergeDecision m = first ? merge_decide_v(P, gm, r, vt, ry, vty, d.c1, d.c2, S.cc)
                               : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
       bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;

@@ -197,6 +197,10 @@ struct PopDev {
   // per cell, kWalkTab buckets of its stretch of tests: entry b is the last
   // j of the cell with cp_cum[j] <= b / kWalkTab of the cell's total
   int* cp_tab;         // [n_cells * kWalkTab]
+  // every 16th pair of each cell's list, padded with INT_MAX to n_coarse (a
+  // multiple of 4) per cell: the first level of the search for a pair
+  const int* cp_coarse;  // [n_cells * n_coarse]
+  int n_coarse;
 
   // [cap] lowest claim key (claim_key) of the current round's events that
   // remove or rewrite the slot, and of those that only read it; a key from
