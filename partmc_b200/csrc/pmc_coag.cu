@@ -1361,14 +1361,12 @@ bool caches_current(const Ctx& c, const PopHost& ph) {
 // populations (after a grid, environment, kernel or weight change)
 void refresh_caches(Ctx& c, const std::vector<uint8_t>& on) {
   bool any = false;
+  for (int k = 0; k < c.n_pop; k++) any = any || on[k];
+  if (!any) return;  // no read-back (a stream sync) in the common case
   int max_slots = 1;
   std::vector<PopCtr>& r = read_ctrs(c);
   for (int k = 0; k < c.n_pop; k++)
-    if (on[k]) {
-      any = true;
-      max_slots = std::max(max_slots, r[k].n_slots);
-    }
-  if (!any) return;
+    if (on[k]) max_slots = std::max(max_slots, r[k].n_slots);
   push_pops(c);
   DevBuf<uint8_t> don;
   don.reserve(c.n_pop);
