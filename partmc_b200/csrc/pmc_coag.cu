@@ -2608,8 +2608,11 @@ int pmc_coag_gpu_upload_components(pmc_coag_gpu_ctx* x, int pop, int n_part, con
 static int finish_step(Ctx& c, long long* samp, long long* coag) {
   long long s = 0, k = 0, warn = 0;
   int status = 0;
+  // one read-back (a stream sync) for every population; a compaction below
+  // changes only its own population's counters
+  const std::vector<PopCtr> all = read_ctrs(c);
   for (int p = 0; p < c.n_pop; p++) {
-    PopCtr r = read_ctr(c, p);
+    const PopCtr& r = all[p];
     s += r.tot_samp;
     k += r.tot_coag;
     warn += r.kmax_warn;
