@@ -1,0 +1,130 @@
+"""The oracle's restatement of the reference's initial-condition sampler
+(oracle/ic_sampler.py: aero_state.F90:758-831, aero_mode.F90:495-665,
+rand.F90:410-487 and 550-576), pinned by answers that follow from the
+mathematics: quadrature of the weighted mode densities, the moments of the
+sampled radii, the truncation rule of the normal sampler, and the volume
+constraints.  CPU only."""
+import math
+
+import numpy as np
+import pytest
+from scipy import integrate
+
+from oracle import ic_sampler as S
+
+LOG10 = math.log(10.0)
+
+
+def lognormal_density_log10(x, num_conc, mu, sigma):
+    """number concentration per unit log10 r of a log-normal mode"""
+    return num_conc / (sigma * math.sqrt(2.0 * math.pi)) * math.exp(-(x - mu) ** 2 / (2.0 * sigma ** 2))
+
+
+@pytest.mark.parametrize("kind,alpha", [(S.WEIGHT_NONE, 0.0), (S.WEIGHT_POWER, -1.0), (S.WEIGHT_POWER, -3.0),
+                                        (S.WEIGHT_POWER, 0.5), (S.WEIGHT_MFA, -3.0)])
+def test_mode_number_matches_quadrature(kind, alpha):
+    """aero_mode_number of a log-normal mode is the integral of its density
+    divided by the weight at each radius."""
+    mode = S.Mode(S.MODE_LOG_NORMAL, char_radius=5e-8, log10_std=math.log10(1.7), num_conc=3.2e9)
+    w = S.Weight(kind, magnitude=1e7 if kind == S.WEIGHT_NONE else 2.5, exponent=alpha)
+    mu, sigma = math.log10(mode.char_radius), mode.log10_std
+
+    def f(x):
+        return lognormal_density_log10(x, mode.num_conc, mu, sigma) / float(w.num_conc_at_radius(10.0 ** x))
+
+    ref, _ = integrate.quad(f, mu - 12 * sigma, mu + 12 * sigma, epsabs=0.0, epsrel=1e-12, limit=200)
+    assert S.mode_number(mode, w) == pytest.approx(ref, rel=1e-9)
+
+
+@pytest.mark.parametrize("alpha", [0.0, -1.0, -3.0])
+def test_sampled_mode_number_matches_quadrature(alpha):
+    """A sampled mode spreads each interval's concentration uniformly in
+    ln r; its weighted number is the integral of that over the weight."""
+    edges = np.array([1e-8, 3e-8, 1e-7, 4e-7])
+    nc = np.array([1e9, 4e9, 2e8])
+    mode = S.Mode(S.MODE_SAMPLED, sample_radius=edges, sample_num_conc=nc)
+    w = S.Weight(S.WEIGHT_POWER, magnitude=3.0, exponent=alpha)
+    ref = 0.0
+    for i in range(len(nc)):
+        x0, x1 = math.log(edges[i]), math.log(edges[i + 1])
+        val, _ = integrate.quad(lambda x: nc[i] / (x1 - x0) / float(w.num_conc_at_radius(math.exp(x))), x0, x1,
+                                epsabs=0.0, epsrel=1e-12)
+        ref += val
+    assert S.mode_number(mode, w) == pytest.approx(ref, rel=1e-9)
+
+
+@pytest.mark.parametrize("alpha", [0.0, -1.0, -3.0])
+def test_lognormal_radii_follow_the_weighted_density(alpha):
+    """Under a power weight the computational particles' log10 radius is
+    normal with mean log10 r_c - alpha sigma^2 ln 10 and the mode's sigma."""
+    rng = np.random.default_rng(11)
+    mode = S.Mode(S.MODE_LOG_NORMAL, char_radius=1e-7, log10_std=0.25, num_conc=1e9)
+    w = S.Weight(S.WEIGHT_POWER, magnitude=1.0, exponent=alpha)
+    n = 40000
+    x = np.log10([S.sample_radius(rng, mode, w, 0.0) for _ in range(n)])
+    mean = math.log10(mode.char_radius) - alpha * mode.log10_std ** 2 * LOG10
+    assert abs(x.mean() - mean) < 4 * mode.log10_std / math.sqrt(n)
+    assert abs(x.std() / mode.log10_std - 1.0) < 4 / math.sqrt(2 * n)
+
+
+def test_normal_truncation_rule():
+    """rand_normal with a probability threshold keeps only draws with
+    1 - |erf(z / sqrt 2)| >= threshold, which for 0.32 is |z| <= 0.994."""
+    rng = np.random.default_rng(5)
+    z = np.array([S.rand_normal(rng, 0.0, 1.0, 0.32) for _ in range(20000)])
+    assert np.all([1.0 - abs(math.erf(v / math.sqrt(2.0))) >= 0.32 for v in z])
+    assert np.abs(z).max() < 0.9945 and np.abs(z).max() > 0.98
+
+
+def test_sampled_mode_radii_fall_in_intervals_by_weighted_number():
+    """sample_cts_pdf picks an interval with probability proportional to its
+    weighted number, and under a power weight r^-alpha is uniform inside it."""
+    rng = np.random.default_rng(7)
+    edges = np.array([1e-8, 3e-8, 1e-7, 4e-7])
+    mode = S.Mode(S.MODE_SAMPLED, sample_radius=edges, sample_num_conc=np.array([1e9, 4e9, 2e8]))
+    w = S.Weight(S.WEIGHT_POWER, magnitude=1.0, exponent=-1.0)
+    n = 30000
+    r = np.array([S.sample_radius(rng, mode, w, 0.0) for _ in range(n)])
+    idx = np.searchsorted(edges, r) - 1
+    assert idx.min() >= 0 and idx.max() < 3
+    p = S.weighted_sampled_num_conc(mode, w)
+    p = p / p.sum()
+    frac = np.bincount(idx, minlength=3) / n
+    assert np.all(np.abs(frac - p) < 4 * np.sqrt(p * (1 - p) / n))
+    inside = idx == 1
+    u = (r[inside] - edges[1]) / (edges[2] - edges[1])  # r^-alpha = r is uniform on the interval
+    assert abs(u.mean() - 0.5) < 4 * math.sqrt(1 / 12 / inside.sum())
+
+
+def test_volumes_sum_to_the_particle_and_stay_non_negative():
+    """aero_mode_sample_vols: perturbed fractions projected onto sum 1,
+    redrawn while any is negative; their mean stays at vol_frac."""
+    rng = np.random.default_rng(3)
+    mode = S.Mode(S.MODE_LOG_NORMAL, vol_frac=[0.6, 0.3, 0.1], vol_frac_std=[0.2, 0.1, 0.05])
+    v = np.array([S.sample_vols(rng, mode, 2.0) for _ in range(20000)])
+    assert np.allclose(v.sum(1), 2.0, rtol=1e-12, atol=0.0)
+    assert v.min() >= 0.0
+    assert np.allclose(v.mean(0) / 2.0, mode.vol_frac, atol=0.01)
+
+
+def test_dist_sample_counts_and_groups():
+    """aero_state_add_aero_dist_sample: per group and mode a Poisson count
+    with mean sample_prop * aero_mode_number."""
+    modes = [S.Mode(S.MODE_LOG_NORMAL, char_radius=2.5e-8, log10_std=0.2, num_conc=3.2e9),
+             S.Mode(S.MODE_MONO, char_radius=1e-7, num_conc=1e8)]
+    weights = [S.Weight(S.WEIGHT_POWER, magnitude=1e4, exponent=-1.0),
+               S.Weight(S.WEIGHT_POWER, magnitude=3e3, exponent=-1.0)]
+    prop = 1e-3
+    means = np.array([[prop * S.mode_number(m, w) for m in modes] for w in weights])
+    rng = np.random.default_rng(2)
+    reps = 40
+    counts = np.zeros((2, 2))
+    for _ in range(reps):
+        vols, grp, mode_of = S.add_dist_sample(rng, modes, weights, prop)
+        assert vols.shape == (len(grp), 1)
+        for g in range(2):
+            for m in range(2):
+                counts[g, m] += np.sum((grp == g) & (mode_of == m))
+    assert np.all(np.abs(counts / reps - means) < 4 * np.sqrt(means / reps))
+    mono = vols[mode_of == 1, 0]
+    assert np.allclose(mono, S.rad2vol(1e-7), rtol=1e-12)
