@@ -188,8 +188,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
 // test sequence ((s + 1) / n_samp: the part of the pair done after it)
 __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const long long* n_samples,
                                 const int2* ev, const int* ev_gp, const int* gpair_local, const long long* work_off,
-                                const uint32_t* sdec, unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos,
-                                int* ev_len, uint32_t* dec) {
+                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len) {
   long long n = *n_samples;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -202,7 +201,6 @@ __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const
       gp_c[e] = gp;
       ev_pos[e] = (float)((double)(s + 1) / (double)ns);
       ev_len[e] = 0;
-      dec[e] = sdec[i];
     }
 }
 
@@ -774,7 +772,6 @@ struct Ctx {
   DevBuf<long long> nwork_set, nwork_pp, work_off, pp_off;
   DevBuf<uint8_t> flag, win_set, win_pp;
   DevBuf<uint32_t> dec_set;  // merge decision of each event (drawn when the event is formed)
-  DevBuf<uint32_t> sdec;     // merge decision of each accepted round-0 sample
   DevBuf<int> ev_gp, gp_c;   // global pair of each accepted sample / event
   DevBuf<int2> ev_c;         // slots of each event
   DevBuf<unsigned long long> ev_key;  // key of each event (make_key)
@@ -1505,10 +1502,10 @@ void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaSt
     using T = decltype(tt);
     if (flat)
       k_test<KT, T, true><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
-                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p, c.sdec.p);
+                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
     else
       k_test<KT, T, false><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
-                                                   c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p, c.sdec.p);
+                                                   c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
   });
   note_launch();
 }
@@ -2208,7 +2205,6 @@ void step_parallel(Ctx& c, int kt) {
   {
     size_t w = (size_t)W;
     c.flag.reserve(w + 1); c.ev.reserve(w + 1); c.flag_off.reserve(w + 2); c.ev_gp.reserve(w + 1);
-    c.sdec.reserve(w + 1);
     reserve_events(c, W);
     c.need_slot_pp.reserve(Q + 1); c.need_id_pp.reserve(Q + 1); c.win_pp.reserve(Q + 1); c.lost_pp.reserve(Q + 1);
     c.lost_off.reserve(Q + 2); c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
@@ -2236,8 +2232,11 @@ void step_parallel(Ctx& c, int kt) {
     const long long* Wd = c.work_off.p + n_gpairs;
     scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, c.round_dev.p + 1}});
     k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, Wd, c.ev.p, c.ev_gp.p,
-                                                           c.gpair_local.p, c.work_off.p, c.sdec.p, c.ev_key.p,
-                                                           c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.ev_len.p, c.dec_set.p);
+                                                           c.gpair_local.p, c.work_off.p, c.ev_key.p, c.ev_c.p,
+                                                           c.gp_c.p, c.ev_pos.p, c.ev_len.p);
+    note_launch();
+    k_decide<<<grid_for(W, 256), 256, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.round_dev.p + 1, c.ev_key.p,
+                                                    c.ev_c.p, c.gp_c.p, c.dec_set.p);
     note_launch();
   }
   resolve_apply(c, c.stream, W, Q);
@@ -2471,7 +2470,6 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   for (auto* b : bk) b->release();
   c.ev_pos.release();
   c.it_pos.release();
-  c.sdec.release();
   c.it_dec.release();
   c.it_gused.release();
   c.ch_pos.release();

@@ -646,15 +646,15 @@ __device__ __forceinline__ Rng merge_rng(const PopDev& P, unsigned long long key
 }
 
 // Per-set pair tests (maybe_coag_pair, coagulation.F90:712-759).  One thread
-// per sample w of the flattened (population, pair, sample) space.  An
-// accepted sample draws its merge decision (coagulate_weighting) at once,
-// stores it in dec[w] and claims its two slots by it: a write claim on a slot
-// the merge removes or rewrites, a read claim on one it keeps.
+// per sample w of the flattened (population, pair, sample) space; an
+// accepted sample records its slots and global pair.  Its merge decision is
+// drawn after the compaction (k_decide), so the FP64 decisions run in full
+// warps instead of in the few accepting lanes of each warp of tests.
 template <int KT, class T, bool FLAT>
 __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpair_pop,
                                               const int* gpair_local, const long long* work_off,
                                               int n_gpairs, const long long* total, uint8_t* flag,
-                                              int2* ev, int* ev_gp, uint32_t* dec) {
+                                              int2* ev, int* ev_gp) {
   long long W = *total;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < W;
        w += (long long)gridDim.x * blockDim.x) {
@@ -709,17 +709,37 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
     bool acc = (T)u53(rnd.z, rnd.w) < prob;
     flag[w] = acc ? 1 : 0;
     if (acc) {
-      unsigned long long key = make_key((uint32_t)p, 0u, (uint32_t)s);
-      unsigned long long ck = claim_key(P, key);
-      Rng gm = merge_rng(P, key);
-      MergeDecision m = merge_decide(P, gm, s1, s2, d.c1, d.c2, S.cc);
-      if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
-      dec[w] = pack_decision(m, gm.used());
-      claim_slot(P, s1, ck, m.rm1);
-      claim_slot(P, s2, ck, m.rm2);
       ev[w] = make_int2(s1, s2);
       ev_gp[w] = gp;
     }
+  }
+}
+
+// Round 0's merge decisions, one thread per accepted sample in sample order
+// (after the compaction): the decision (coagulate_weighting,
+// coagulation.F90:810-922) from the sample's own stream (merge_rng of its
+// key), stored in dec[e], and the claims on its two slots by it: a write
+// claim on a slot the merge removes or rewrites, a read claim on one it
+// keeps.
+__global__ void __launch_bounds__(256) k_decide(const PopDev* pops, const int* gpair_pop,
+                                                const long long* n_events, const unsigned long long* ev_key,
+                                                const int2* ev_c, const int* gp_c, uint32_t* dec) {
+  long long E = *n_events;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
+       e += (long long)gridDim.x * blockDim.x) {
+    const PopDev& P = pops[gpair_pop[gp_c[e]]];
+    const unsigned long long key = ev_key[e];
+    const int p = (int)key_pair(key);
+    const int2 sl = ev_c[e];
+    const PairState& S = P.pair[p];
+    const PairDesc d = P.pair_desc[p];
+    const unsigned long long ck = claim_key(P, key);
+    Rng gm = merge_rng(P, key);
+    MergeDecision m = merge_decide(P, gm, sl.x, sl.y, d.c1, d.c2, S.cc);
+    if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+    dec[e] = pack_decision(m, gm.used());
+    claim_slot(P, sl.x, ck, m.rm1);
+    claim_slot(P, sl.y, ck, m.rm2);
   }
 }
 
