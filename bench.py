@@ -32,6 +32,9 @@ B_SORT = 8  # per slot: its cell key read, its cell-list entry written
 # ncu captures of one launch at this workload: k_test read 46.91 MB and wrote
 # 1.12 MB for about 209,000 tests; k_sort_all read 4.04 MB and wrote none for
 # 1e6 slots.  The roofline's traffic scales these by the units of a launch.
+# The k_test capture predates the pass that now draws the accepted samples'
+# merge decisions (k_decide): it includes their reads, so for the current
+# kernel it is an upper bound.
 DRAM_TEST = (46.91e6 + 1.12e6) / 209000
 DRAM_SORT = 4.04e6 / 1e6
 
