@@ -1531,7 +1531,7 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
     using T = decltype(tt);
     auto k = flat ? k_items<KT, T, true> : k_items<KT, T, false>;
     k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
-                              c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p, pool,
+                              c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
                               c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
                               c.it_done.p, c.it_dec.p, c.it_gused.p);
     auto kc = flat ? k_chain<KT, T, true> : k_chain<KT, T, false>;

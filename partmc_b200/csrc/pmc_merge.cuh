@@ -379,8 +379,6 @@ struct WalkOut {
   int q = 0, y = 0;  // pair and partner of the first event
   float pos = 0.f;
   bool first_cell1 = true;  // the walking particle is in the pair's first cell
-  int chain_len = 0;        // events in the chain (0: the first event alone)
-  int chain_head = -1;
   bool done = false;        // the walk ran to the end after its last event
   uint32_t dec = 0;         // merge decision of the first event
   bool cont = false;        // the first event is an absorb: k_chain carries the walk on
@@ -574,7 +572,7 @@ __device__ __forceinline__ int walk_next(const PopDev& P, int x, Stretch& s, uin
 // by the coagulated one) is carried on as a chain by k_chain from the next
 // test on.
 template <int KT, class T, bool FLAT>
-__device__ void walk(const PopDev& P, const ChainPool& pool, int x, int p0, float pos0, WalkOut* out) {
+__device__ void walk(const PopDev& P, int x, int p0, float pos0, WalkOut* out) {
   if (x < 0 || x >= P.cap || !P.alive[x]) return;
   const int C = P.cell[x];
   if (C < 0 || C >= P.n_cells) return;
@@ -637,7 +635,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
                                                const uint8_t* win, const int* dest,
                                                const unsigned long long* ev_key, const int2* ev_c,
                                                const int* gp_c, const float* ev_pos, const uint32_t* dec,
-                                               ChainPool pool, uint8_t* it_flag, unsigned long long* it_key,
+                                               uint8_t* it_flag, unsigned long long* it_key,
                                                int2* it_c, int* it_gp, float* it_pos, int* it_len, int* it_head,
                                                uint8_t* it_done, uint32_t* it_dec, uint32_t* it_gused) {
   long long n = *n_items;
@@ -684,7 +682,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     uint32_t dc = dec[e];
     if (walker >= 0) {
       WalkOut w;
-      walk<KT, T, FLAT>(P, pool, walker, p0, pos0, &w);
+      walk<KT, T, FLAT>(P, walker, p0, pos0, &w);
       if (!w.found) continue;
       key = make_key((uint32_t)w.q, 1u, (uint32_t)walker);
       sl = w.first_cell1 ? make_int2(walker, w.y) : make_int2(w.y, walker);
