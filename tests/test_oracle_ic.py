@@ -128,3 +128,28 @@ def test_dist_sample_counts_and_groups():
     assert np.all(np.abs(counts / reps - means) < 4 * np.sqrt(means / reps))
     mono = vols[mode_of == 1, 0]
     assert np.allclose(mono, S.rad2vol(1e-7), rtol=1e-12)
+
+
+@pytest.mark.parametrize("alpha", [0.0, -1.0, -3.0])
+def test_sampled_distribution_matches_the_mode_under_any_weighting(alpha):
+    """The starting point of the reference's test/weighting: test/weighting's
+    initial mode (log-normal, 3.2e9 m^-3, geometric mean diameter 20 nm,
+    log10 of the geometric standard deviation 0.161), sampled with about
+    10,000 computational particles under a flat or power weighting, gives
+    the mode's number distribution on the test's grid (160 log bins of
+    diameter from 1e-8 to 1e-3 m, extract_aero_size --num) within the test's
+    relative 2-norm tolerance of 0.1 (numeric_diff --by col --rel-tol 0.1),
+    each particle counted at the weight at its radius."""
+    from oracle import exact as E
+    mode = S.Mode(S.MODE_LOG_NORMAL, char_radius=1e-8, log10_std=0.161, num_conc=3.2e9)
+    unit = S.Weight(S.WEIGHT_POWER, magnitude=1.0, exponent=alpha)
+    w = S.Weight(S.WEIGHT_POWER, magnitude=S.mode_number(mode, unit) / 10000.0, exponent=alpha)
+    rng = np.random.default_rng(17)
+    vols, grp, _ = S.add_dist_sample(rng, [mode], [w], 1.0)
+    r = S.vol2rad(vols[:, 0])
+    h, centers = E.size_histogram(2.0 * r, w.num_conc_at_radius(r))
+    ln_sigma = mode.log10_std * LOG10
+    exact = mode.num_conc / (math.sqrt(2.0 * math.pi) * ln_sigma) * np.exp(
+        -(np.log(centers) - math.log(2.0 * mode.char_radius)) ** 2 / (2.0 * ln_sigma ** 2))
+    assert abs(len(r) - 10000) < 5 * math.sqrt(10000)
+    assert E.rel_err_by_col(exact, h)[0] < 0.1
