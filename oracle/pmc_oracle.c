@@ -2019,3 +2019,40 @@ int orc_get_weight(const orc_state *st, double *w_mag) {
   memcpy(w_mag, st->w_mag, sizeof(double) * st->n_group * st->n_class);
   return ORC_OK;
 }
+
+/* coad, run_sect.F90:283-359: the loss and gain of one time step over every
+ * bin pair (i <= j) inside the occupied range, in the reference's order. */
+void orc_sect_coad(int n_bin, const double *c, const int *ima, double *g, const double *e, const double *ck) {
+  const double gmin = 1e-60;
+  int i0, i1;
+  /* the Fortran loops leave i0 = n_bin and i1 = 0 when nothing is found */
+  for (i0 = 0; i0 < n_bin - 1; i0++)
+    if (g[i0] > gmin) break;
+  for (i1 = n_bin - 2; i1 >= 0; i1--)
+    if (g[i1] > gmin) break;
+  for (int i = i0; i <= i1; i++)
+    for (int j = i; j <= i1; j++) {
+      int k = ima[i * n_bin + j];
+      double x0 = ck[i * n_bin + j] * g[i] * g[j];
+      double t = g[i] * e[j];
+      x0 = x0 < t ? x0 : t;
+      if (j != k) {
+        t = g[j] * e[i];
+        x0 = x0 < t ? x0 : t;
+      }
+      double gsi = x0 / e[j], gsj = x0 / e[i], gsk = gsi + gsj;
+      g[i] = g[i] - gsi;
+      g[j] = g[j] - gsj;
+      if (k >= 0) {
+        int kp = k + 1;
+        double gk = g[k] + gsk;
+        if (gk > gmin) {
+          double x1 = log(g[kp] / gk + 1e-60);
+          double flux = gsk / x1 * (exp(0.5 * x1) - exp(x1 * (0.5 - c[i * n_bin + j])));
+          flux = flux < gk ? flux : gk;
+          g[k] = gk - flux;
+          g[kp] = g[kp] + flux;
+        }
+      }
+    }
+}

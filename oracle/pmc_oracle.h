@@ -171,6 +171,13 @@ int orc_rebalance(orc_state *st, const double *n_part_ideal, int allow_doubling,
                   int allow_halving);
 int orc_get_weight(const orc_state *st, double *w_mag);
 
+/* One step of the reference's sectional coagulation solver (coad,
+ * run_sect.F90:283-359, Bott's exponential flux method), 0-based: g[n_bin]
+ * mass distribution (updated in place), e[n_bin] bin masses (mg),
+ * c[i*n_bin+j] Courant numbers, ima[i*n_bin+j] the bin that i + j goes to
+ * (-1: none), ck[i*n_bin+j] the smoothed kernel times del_t and bin width. */
+void orc_sect_coad(int n_bin, const double *c, const int *ima, double *g, const double *e, const double *ck);
+
 /* histograms of n draws (k = 0..k_max) */
 void orc_poisson_hist(orc_state *st, double mean, int64_t n, int k_max,
                       int64_t *counts);
