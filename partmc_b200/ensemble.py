@@ -86,6 +86,15 @@ def reduce_histograms(hist, device="cpu"):
     return t.cpu().numpy()
 
 
+def _n_spec(populations):
+    """Species count shared by every population of an ensemble (taken from
+    aero_data, which all members share)."""
+    counts = {int(len(p.aero_data.density)) for p in populations}
+    if len(counts) != 1:
+        raise ValueError("ensemble members must share one aero_data (species count)")
+    return counts.pop()
+
+
 class Ensemble:
     """This rank's shard of independent populations, stepped together.
 
@@ -100,6 +109,10 @@ class Ensemble:
     def __init__(self, populations, temps, pressures, seeds, rank=0, world_size=1, mode=None, stepper=None):
         self.index = shard([p.vol.shape[0] for p in populations], world_size)[rank]
         self.pops = [populations[i] for i in self.index]
+        # species count from the whole ensemble, not this rank's shard: a rank
+        # with no populations still returns histograms of the shared shape,
+        # so every rank's all_reduce in reduce_histograms matches
+        self.n_spec = _n_spec(populations)
         t = np.asarray(temps, dtype=np.float64)[self.index]
         p = np.asarray(pressures, dtype=np.float64)[self.index]
         s = np.asarray(seeds, dtype=np.uint64)[self.index]
@@ -115,8 +128,7 @@ class Ensemble:
     def histogram(self, edges):
         """Size distributions (binned_totals layout) summed over this rank's
         populations."""
-        n_spec = self.pops[0].vol.shape[1] if self.pops else 1
-        out = np.zeros((len(edges) - 1, 1 + n_spec))
+        out = np.zeros((len(edges) - 1, 1 + self.n_spec))
         for k in range(len(self.pops)):
             out += self.engine.histogram(k, edges)
         return out

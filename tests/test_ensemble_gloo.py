@@ -57,8 +57,17 @@ def problem():
     return pops, temps, press, seeds
 
 
-def run_ensemble(rank, world):
-    pops, temps, press, seeds = problem()
+def problem_20spec(n_pop):
+    """n_pop populations of 20 species (nummass weights), small."""
+    pops = [aero_dist.brown_20spec(n, seed=60 + k) for k, n in enumerate((700, 900, 500)[:n_pop])]
+    return pops, np.full(n_pop, 288.0), np.full(n_pop, 1e5), np.arange(21, 21 + n_pop, dtype=np.uint64)
+
+
+def run_ensemble(rank, world, n_pop=N_POP):
+    if n_pop == N_POP:
+        pops, temps, press, seeds = problem()
+    else:
+        pops, temps, press, seeds = problem_20spec(n_pop)
     e = ens.Ensemble(pops, temps, press, seeds, rank=rank, world_size=world, stepper=OracleShard)
     s, c = e.step(O.KERNEL_BROWN, DEL_T, N_STEPS)
     tot = ens.reduce_counters(s, c, seconds=1.0 + rank)
@@ -66,13 +75,13 @@ def run_ensemble(rank, world):
     return tot, hist, e.index
 
 
-def _worker(rank, world, port, out_dir):
+def _worker(rank, world, port, out_dir, n_pop=N_POP):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        tot, hist, idx = run_ensemble(rank, world)
+        tot, hist, idx = run_ensemble(rank, world, n_pop)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), hist=hist, idx=np.array(idx),
                  tot=np.array([tot["n_samp"], tot["n_coag"], tot["seconds"]]))
     finally:
@@ -121,4 +130,22 @@ def test_two_gloo_ranks_match_one_process():
     for x in r:  # the reduced values are the same on every rank
         assert x["tot"][0] == tot1["n_samp"] and x["tot"][1] == tot1["n_coag"]
         assert x["tot"][2] == 2.0  # max over ranks of 1.0 + rank
+        assert np.allclose(x["hist"], hist1, rtol=1e-12, atol=0.0)
+
+
+def test_more_ranks_than_populations():
+    """Three ranks, two populations of 20 species: the rank without a
+    population still takes part in both reductions with histograms of the
+    shared shape (number plus 20 species), and the sums equal one
+    process's."""
+    world, n_pop = 3, 2
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_worker, args=(world, free_port(), d, n_pop), nprocs=world, join=True,
+                           start_method="spawn")
+        r = [np.load(os.path.join(d, f"rank{k}.npz")) for k in range(world)]
+    assert sorted(len(x["idx"]) for x in r) == [0, 1, 1]
+    tot1, hist1, _ = run_ensemble(0, 1, n_pop)
+    for x in r:
+        assert x["hist"].shape == hist1.shape == (len(EDGES) - 1, 21)
+        assert x["tot"][0] == tot1["n_samp"] and x["tot"][1] == tot1["n_coag"]
         assert np.allclose(x["hist"], hist1, rtol=1e-12, atol=0.0)
