@@ -277,9 +277,8 @@ int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx *ctx, int kernel_type,
 
 /* Size-bin sort that allocates nothing.  No counterpart in the reference:
  * it exists for callers that cannot allocate device memory on the call path,
- * such as code being captured into a CUDA graph (where cudaMalloc is not
- * allowed) or a host model whose device memory is all handed out up front by
- * its own allocator.
+ * such as a host model whose device memory is all handed out up front by its
+ * own allocator.
  *
  * Same result as the sort inside a context (aero_sorted_sort_particles on a
  * log grid of n_bin bins from edge_min to edge_max, bin_grid.F90:143-167):
@@ -287,7 +286,11 @@ int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx *ctx, int kernel_type,
  *   cell_count_dev    n_bin x n_class entries, bin fastest
  *   cell_start_dev    n_bin*n_class + 1 exclusive offsets into list_dev
  *   list_dev          0-based particle numbers grouped by (bin, class), in
- *                     increasing particle order inside each group
+ *                     increasing particle order inside each group; only the
+ *                     first cell_start_dev[n_bin*n_class] entries are
+ *                     written, since particles off the grid (bin 0 or
+ *                     n_bin+1) or with a class outside 1..n_class are in no
+ *                     group
  * from vtot_dev[i] (total particle volume, m^3) and 1-based cls_dev[i].
  * All pointers are caller-owned device buffers; work is queued on `stream`
  * (a cudaStream_t, NULL for the legacy default stream) and the call returns
