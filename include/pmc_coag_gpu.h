@@ -226,6 +226,15 @@ int pmc_coag_gpu_replay_used(pmc_coag_gpu_ctx *ctx, int64_t *n_used);
 int pmc_coag_gpu_stats(pmc_coag_gpu_ctx *ctx, int64_t *kmax_violations,
                        int64_t *redraws, int64_t *rounds);
 
+/* Pair tests that MIXED mode decided in FP64, summed over the populations
+ * since they were uploaded.  A test's FP32 acceptance probability is used
+ * only where the uniform lies farther from it than a margin (2^-12) that
+ * bounds the FP32 rounding error; the other tests (near the uniform, or near
+ * or above k_max) are decided from the FP64 records, so every decision, and
+ * the count of k > k_max warnings, is the FP64 mode's.  No counterpart in the
+ * reference, which evaluates in FP64 only. */
+int pmc_coag_gpu_exact_tests(pmc_coag_gpu_ctx *ctx, int64_t *n);
+
 /* Conflicts of the last step, summed over its rounds: accepted per-set
  * events and how many lost a claim, per-particle target operations and how
  * many lost a claim (each loser is retried, dropped or redone in a later

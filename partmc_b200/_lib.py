@@ -69,6 +69,7 @@ SIGNATURES = {
     "pmc_coag_gpu_profile_read": (_I, [_P, _I, _DP, _LP, _LP]),
     "pmc_coag_gpu_launch_count": (_I, [_LP]),
     "pmc_coag_gpu_conflicts": (_I, [_P, _LP, _LP, _LP, _LP]),
+    "pmc_coag_gpu_exact_tests": (_I, [_P, _LP]),
     "pmc_coag_gpu_bin_sort_noalloc": (_I, [_I, _P, _P, _I, _I, _D, _D, _P, _P, _P, _P, _P]),
 }
 

@@ -279,6 +279,13 @@ class AeroState:
               "pmc_coag_gpu_stats")
         return {"kmax_violations": a.value, "redraws": b.value, "rounds": c.value}
 
+    def exact_tests(self):
+        """Pair tests that MIXED mode decided in FP64 (near the uniform or
+        near k_max), summed over the populations since their upload."""
+        n = ctypes.c_int64()
+        check(_lib.lib().pmc_coag_gpu_exact_tests(self.ctx, ctypes.byref(n)), "pmc_coag_gpu_exact_tests")
+        return n.value
+
     def conflicts(self):
         v = [ctypes.c_int64() for _ in range(4)]
         check(_lib.lib().pmc_coag_gpu_conflicts(self.ctx, *[ctypes.byref(x) for x in v]), "pmc_coag_gpu_conflicts")

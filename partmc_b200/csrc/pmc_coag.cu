@@ -817,7 +817,7 @@ struct Ctx {
   PinnedBuf pin;  // host staging of the changed slots
   long long h_total = 0;
   // stats of the last step
-  long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0;
+  long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0, exact_tests = 0;
   long long last_set_losers = 0, last_pp_lost = 0, last_events = 0, last_ops = 0;
   // optional per-kernel timing with CUDA events on the library's stream:
   // 0 pair tests, 1 sorts (k_sort_all), 2 later-round graph launches,
@@ -2112,7 +2112,6 @@ void step_parallel(Ctx& c, int kt) {
   }
   bool flat = true;
   for (int k = 0; k < c.n_pop; k++) flat = flat && c.pops[k].h.flat;
-  float inflate = c.mode == PMC_MODE_MIXED ? (float)ldexp(1.0, -16) : 0.f;
   c.last_set_losers = c.last_pp_lost = c.last_events = c.last_ops = 0;
   std::vector<long long> hw(3 + 2 * (size_t)c.n_pop);
   std::vector<int> per_pop(4 * (size_t)c.n_pop);
@@ -2153,7 +2152,7 @@ void step_parallel(Ctx& c, int kt) {
   }
   {
     dim3 gp((max_pairs + 127) / 128, c.n_pop);
-    k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, 1, inflate);
+    k_pairs<<<gp, 128, 0, c.stream>>>(c.d_pops, c.pop_pair_base.p, c.nwork_set.p, c.nwork_pp.p, 1);
     note_launch();
   }
   // the device copies learn this with the next push
@@ -2604,7 +2603,7 @@ int pmc_coag_gpu_upload_components(pmc_coag_gpu_ctx* x, int pop, int n_part, con
 }
 
 static int finish_step(Ctx& c, long long* samp, long long* coag) {
-  long long s = 0, k = 0, warn = 0;
+  long long s = 0, k = 0, warn = 0, exact = 0;
   int status = 0;
   // one read-back (a stream sync) for every population; a compaction below
   // changes only its own population's counters
@@ -2614,6 +2613,7 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
     s += r.tot_samp;
     k += r.tot_coag;
     warn += r.kmax_warn;
+    exact += r.exact_tests;
     if (r.status && !status) status = r.status;
     if (r.bad_site) {
       static const char* site[] = {"", "pair test: list position", "pair test: slot", "event: slot",
@@ -2630,6 +2630,7 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
     if (r.n_slots > 4096 && r.n_live < r.n_slots / 2) relayout(c, p, c.pops[p].h.cap, true);
   }
   c.last_kmax_warn = warn;
+  c.exact_tests = exact;
   *samp = s;
   *coag = k;
   return status;
@@ -3137,6 +3138,12 @@ int pmc_coag_gpu_stats(pmc_coag_gpu_ctx* x, int64_t* kmax_violations, int64_t* r
   if (kmax_violations) *kmax_violations = x->c.last_kmax_warn;
   if (redraws) *redraws = x->c.last_redraws;
   if (rounds) *rounds = x->c.last_rounds;
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_exact_tests(pmc_coag_gpu_ctx* x, int64_t* n) {
+  if (!x || !n) return PMC_ERR_INVALID_ARG;
+  *n = x->c.exact_tests;
   return PMC_OK;
 }
 

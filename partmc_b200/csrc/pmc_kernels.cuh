@@ -467,7 +467,7 @@ __global__ void k_pair_setup(const PopDev* pops) {
 // per-particle pair.  k_max is set for every pair, empty ones included:
 // walks test particles that arrive in a pair's cells during the step.
 __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long long* nwork_set,
-                        long long* nwork_pp, int use_particle_path, float kmax_inflate) {
+                        long long* nwork_pp, int use_particle_path) {
   const PopDev& P = pops[blockIdx.y];
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n_pairs) return;
@@ -488,7 +488,6 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
   }
   bool same = (b1 == b2) && (c1 == c2);
   double k_max = P.kmax_tab[b1 + nb * b2] * S.f_max;
-  if (kmax_inflate != 0.f) k_max = k_max * (1.0 + (double)kmax_inflate);
   S.k_max = k_max;
   S.inv_k_max = 1.0 / k_max;
   if (n1 == 0 || n2 == 0) {
@@ -549,7 +548,16 @@ __device__ __forceinline__ T pair_kernel(const PopDev& P, const T* q1, const T* 
     T rho = (v1 / (v1 + v2)) * q1[4] + (v2 / (v1 + v2)) * q2[4];
     T x1 = T(P.benv.prime_radius) / q1[0], x2 = T(P.benv.prime_radius) / q2[0];
     T s = q1[5] + q2[5];
-    k = sqrt(T(6.0 * kBoltzmann * P.benv.temp * P.benv.prime_radius) / rho * (x1 * x1 * x1 + x2 * x2 * x2)) * (s * s);
+    if constexpr (sizeof(T) == 8) {
+      k = sqrt(T(6.0 * kBoltzmann * P.benv.temp * P.benv.prime_radius) / rho * (x1 * x1 * x1 + x2 * x2 * x2)) *
+          (s * s);
+    } else {
+      // the same product with the constant's square root taken apart: 6 k T R0
+      // is about 1e-28, and divided by rho and multiplied by 1/N of a large
+      // cluster it would fall below FP32's normal range
+      k = T(sqrt(6.0 * kBoltzmann * P.benv.temp * P.benv.prime_radius)) *
+          sqrt((x1 * x1 * x1 + x2 * x2 * x2) / rho) * (s * s);
+    }
   } else if (KT == kKernelBrownCont) {
     // q = {r, rv, nc, N^(1/d_f), -, -}
     k = T(2.0 * kBoltzmann * P.benv.temp / 3.0 / kAirDynVisc) * (T(1) / q1[3] + T(1) / q2[3]) * (q1[3] + q2[3]);
@@ -564,6 +572,38 @@ __device__ __forceinline__ T pair_kernel(const PopDev& P, const T* q1, const T* 
   if (ncj < mn) mn = ncj;
   if (ncij < mn) mn = ncij;
   return k * (nci * ncj / mn);
+}
+
+// FP32 acceptance with an exact FP64 fallback.  The FP32 probability pf =
+// k32 / k_max of a pair test differs from the FP64 one by less than
+// kAcceptMargin (the rounding-error bound of the FP32 kernel and weight
+// evaluation is below 2^-17 of k_max for every kernel; the margin leaves a
+// factor 32).  So when the uniform u lies farther than the margin from pf,
+// and pf is below 1 - margin, u < pf is the FP64 decision u < p64; otherwise
+// (about 2 * 2^-12 of the tests, and every test near or above k_max) the
+// test is decided in FP64 from the FP64 records.  The decisions, and the
+// k > k_max warnings, are those of the FP64 mode for the same draws.
+constexpr float kAcceptMargin = 1.0f / 4096.0f;
+__device__ __forceinline__ bool f32_decides(float pf, double u) {
+  return pf < 1.0f - kAcceptMargin && fabs((double)pf - u) > (double)kAcceptMargin;
+}
+
+// u < k / k_max in FP64 from the slots' FP64 records, for the pair p's
+// orientation (first cell's particle first); counts k > k_max as the
+// reference's warn_assert_msg does (coagulation.F90:749-751)
+template <int KT, bool FLAT>
+__device__ __forceinline__ bool accept_f64_rec(const PopDev& P, const RecD& a, const RecD& b, const PairDesc& d,
+                                               int cc, double fflat, double inv_k_max, double u) {
+  const double k = pair_kernel<KT, double, FLAT>(P, (const double*)&a, (const double*)&b, d.c1, d.c2, cc, fflat,
+                                                 P.coeff);
+  const double prob = k * inv_k_max;
+  if (!(prob <= 1.0)) add_ll(&P.ctr->kmax_warn, 1LL);
+  return u < prob;
+}
+template <int KT, bool FLAT>
+__device__ __forceinline__ bool accept_f64(const PopDev& P, int s1, int s2, const PairDesc& d, const PairState& S,
+                                           double u) {
+  return accept_f64_rec<KT, FLAT>(P, P.recd[s1], P.recd[s2], d, S.cc, S.fflat, S.inv_k_max, u);
 }
 
 __device__ __forceinline__ int find_pair(const long long* off, int n, long long w) {
@@ -693,20 +733,22 @@ __global__ void __launch_bounds__(256) k_test(const PopDev* pops, const int* gpa
       flag[w] = 0;
       continue;
     }
-    T k;
+    const double u = u53(rnd.z, rnd.w);
+    bool acc;
     if constexpr (sizeof(T) == 8) {
-      const double* q1 = (const double*)&P.recd[s1];
-      const double* q2 = (const double*)&P.recd[s2];
-      k = (T)pair_kernel<KT, double, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, S.fflat, P.coeff);
+      acc = accept_f64<KT, FLAT>(P, s1, s2, d, S, u);
     } else {
       const float* q1 = (const float*)&P.recf[s1];
       const float* q2 = (const float*)&P.recf[s2];
-      k = (T)pair_kernel<KT, float, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, (float)S.fflat,
-                                          (float)P.coeff);
+      const float pf = pair_kernel<KT, float, FLAT>(P, q1, q2, d.c1, d.c2, S.cc, (float)S.fflat, (float)P.coeff) *
+                       (float)S.inv_k_max;
+      if (f32_decides(pf, u)) {
+        acc = u < (double)pf;
+      } else {
+        acc = accept_f64<KT, FLAT>(P, s1, s2, d, S, u);
+        add_ll(&P.ctr->exact_tests, 1LL);
+      }
     }
-    T prob = k * (T)S.inv_k_max;
-    if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, (long long)(1LL));
-    bool acc = (T)u53(rnd.z, rnd.w) < prob;
     flag[w] = acc ? 1 : 0;
     if (acc) {
       ev[w] = make_int2(s1, s2);

@@ -512,28 +512,33 @@ __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& 
   const double ry = P.rad[y], vty = P.vtot[y];  // for the merge decision if the test accepts
   if (y == x || !alive || cell_y != O) return 0;
   if (chain && claimed_by_walk(P, y, x)) return 0;  // absorbed earlier in this chain
-  T k;
+  const double u = u32d(accu);
+  bool acc;
   if constexpr (sizeof(T) == 8) {
     const RecD qy = P.recd[y];
-    const double* qw = (const double*)&qxd;
-    const double* py = (const double*)&qy;
-    k = (T)pair_kernel<KT, double, FLAT>(P, first ? qw : py, first ? py : qw, d.c1, d.c2, cc, fflat, P.coeff);
+    acc = accept_f64_rec<KT, FLAT>(P, first ? qxd : qy, first ? qy : qxd, d, cc, fflat, inv_k_max, u);
   } else {
     const RecF qy = P.recf[y];
     const float* qw = (const float*)&qxf;
     const float* py = (const float*)&qy;
-    k = (T)pair_kernel<KT, float, FLAT>(P, first ? qw : py, first ? py : qw, d.c1, d.c2, cc, (float)fflat,
-                                        (float)P.coeff);
+    const float pf = pair_kernel<KT, float, FLAT>(P, first ? qw : py, first ? py : qw, d.c1, d.c2, cc,
+                                                  (float)fflat, (float)P.coeff) *
+                     (float)inv_k_max;
+    if (f32_decides(pf, u)) {
+      acc = u < (double)pf;
+    } else {  // decided in FP64 (see f32_decides)
+      const RecD qy = P.recd[y];
+      acc = accept_f64_rec<KT, FLAT>(P, first ? qxd : qy, first ? qy : qxd, d, cc, fflat, inv_k_max, u);
+      add_ll(&P.ctr->exact_tests, 1LL);
+    }
   }
-  T prob = k * (T)inv_k_max;
-  if (!(prob <= T(1))) add_ll(&P.ctr->kmax_warn, 1LL);
   *y_out = y;
   *pos_out = (float)((at - c0) / lam);
   *q_out = q;
   *first_out = first;
   *ry_out = ry;
   *vty_out = vty;
-  return (T)u32d(accu) < prob ? 2 : 1;
+  return acc ? 2 : 1;
 }
 
 // The next accepted test of walker x from s on, drawing tests t_next,

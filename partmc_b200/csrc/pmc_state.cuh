@@ -105,6 +105,7 @@ struct PopCtr {
   int bad_site;            // first failed bounds check (kBad*), 0 if none
   long long bad_index;     // the index that failed it
   long long walk_tests;    // pair tests made by walks in the current step
+  long long exact_tests;   // FP32 pair tests decided in FP64 (f32_decides), since the context was made
 };
 
 // sites of the device bounds checks (PopCtr::bad_site)
