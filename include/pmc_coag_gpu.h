@@ -147,6 +147,20 @@ int pmc_coag_gpu_sync_host(pmc_coag_gpu_ctx *ctx, int pop, int cap,
                            int *n_primary, uint8_t *alive, int *n_slots,
                            int *n_changed, int *full);
 
+/* Particle shape of aero_data (fractal_t, fractal.F90:59-66), as
+ * spec_file_read_fractal sets it from the spec file's do_fractal, frac_dim,
+ * prime_radius and vol_fill_factor (fractal.F90:550-593).  Every radius
+ * then follows fractal_vol2rad / fractal_rad2vol (bins, weights, k_max
+ * bounds), the Brownian and sedimentation kernels use the mobility radius
+ * of fractal_vol_to_mobility_rad (fractal.F90:315-362), and the free
+ * molecular and continuum kernels the number of monomers.  d_f = 3 and f = 1
+ * are spherical particles (the default, fractal_set_spherical).  Returns
+ * PMC_ERR_INVALID_ARG for d_f outside (0, 3] (the reference stops for
+ * d_f > 3) or a non-positive R0 or f.  The next step re-sorts every
+ * population and recomputes its k_max bounds. */
+int pmc_coag_gpu_set_fractal(pmc_coag_gpu_ctx *ctx, double frac_dim,
+                             double prime_radius, double vol_fill_factor);
+
 /* New weight magnitudes/exponents, e.g. after aero_state_rebalance doubles or
  * halves a group (aero_state.F90:1722-1852).  Invalidates the sort. */
 int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx *ctx, const int *w_type,

@@ -122,6 +122,11 @@ def lib():
                                         ctypes.POINTER(ctypes.c_int64)]
         L.orc_binomial_hist.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int64)]
+        L.orc_set_fractal.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_fractal_radius.restype = ctypes.c_double
+        L.orc_fractal_radius.argtypes = [ctypes.c_double] * 6 + [dp]
+        L.orc_kernel_value_fractal.restype = ctypes.c_double
+        L.orc_kernel_value_fractal.argtypes = [ctypes.c_int] + [ctypes.c_double] * 10
         L.orc_rebalance.argtypes = [P, dp, ctypes.c_int, ctypes.c_int]
         L.orc_get_weight.argtypes = [P, dp]
         _lib = L
@@ -187,6 +192,12 @@ class Oracle:
         w_exp = np.asfortranarray(np.atleast_2d(w_exp), dtype=np.float64).ravel(order="F")
         self._keep_w = [w_type, w_mag, w_exp]
         lib().orc_set_weight(self.ptr, _ip(w_type), _dp(w_mag), _dp(w_exp))
+
+    def set_fractal(self, frac_dim, prime_radius, vol_fill_factor=1.0):
+        """Particle shape (fractal_t); d_f = 3, f = 1 are spheres."""
+        rc = lib().orc_set_fractal(self.ptr, frac_dim, prime_radius, vol_fill_factor)
+        if rc:
+            raise ValueError(f"orc_set_fractal failed: {rc}")
 
     def seed(self, s):
         lib().orc_set_seed(self.ptr, s)
@@ -340,6 +351,19 @@ def vol2rad(v):
 
 def rad2vol(r):
     return lib().orc_rad2vol(r)
+
+
+def fractal_radius(v, frac_dim, prime_radius, vol_fill_factor=1.0, temp=288.0, pressure=1e5):
+    """(fractal_vol2rad, fractal_vol_to_mobility_rad) of volume v."""
+    m = ctypes.c_double()
+    r = lib().orc_fractal_radius(v, frac_dim, prime_radius, vol_fill_factor, temp, pressure, ctypes.byref(m))
+    return r, m.value
+
+
+def kernel_value_fractal(kernel_type, v1, d1, v2, d2, frac_dim, prime_radius, vol_fill_factor=1.0, temp=288.0,
+                         pressure=1e5, coeff=1000.0):
+    return lib().orc_kernel_value_fractal(kernel_type, v1, d1, v2, d2, temp, pressure, coeff, frac_dim,
+                                          prime_radius, vol_fill_factor)
 
 
 def bin_find(n_bin, emin, emax, r):

@@ -52,7 +52,15 @@ typedef struct {
   ivec *inv;
 } rmap2;
 
+/* fractal_t, fractal.F90:59-66: volume fractal dimension, primary radius
+ * (m), volume filling factor; sph: fractal_is_spherical (d_f = 3, f = 1) */
+typedef struct {
+  double frac_dim, prime_radius, vol_fill_factor;
+  int sph;
+} orc_fractal;
+
 struct orc_state {
+  orc_fractal frac; /* particle shape of aero_data (spherical by default) */
   int n_spec;
   double *density;
   int i_water; /* 1-based, 0 if none */
@@ -416,6 +424,76 @@ double orc_vol2rad(double v) { return pow(3.0 * v / 4.0 / C_PI, 1.0 / 3.0); }
 /* sphere_rad2vol, util.F90:264-271 */
 double orc_rad2vol(double r) { return 4.0 * C_PI * (r * r * r) / 3.0; }
 
+/* fractal_set_spherical, fractal.F90:73-82 */
+static const orc_fractal SPHERE = {3.0, 1e-8, 1.0, 1};
+
+/* fractal_vol_to_num_of_monomers, fractal.F90:90-100 */
+static double num_of_monomers(const orc_fractal *fr, double v) {
+  double x = orc_vol2rad(v) / fr->prime_radius;
+  return x * x * x;
+}
+
+/* fractal_vol2rad, fractal.F90:106-121 */
+static double frac_vol2rad(const orc_fractal *fr, double v) {
+  if (fr->sph) return orc_vol2rad(v);
+  return fr->prime_radius *
+         pow(num_of_monomers(fr, v) * fr->vol_fill_factor, 1.0 / fr->frac_dim);
+}
+
+/* fractal_rad2vol, fractal.F90:142-157 */
+static double frac_rad2vol(const orc_fractal *fr, double r) {
+  if (fr->sph) return orc_rad2vol(r);
+  return orc_rad2vol(fr->prime_radius) * pow(r / fr->prime_radius, fr->frac_dim) /
+         fr->vol_fill_factor;
+}
+
+/* air_mean_free_path, util.F90:289-312 */
+static double air_mean_free_path(double temp, double pressure) {
+  double rhoair = (pressure * C_AIR_MOLEC_WEIGHT) / (C_UNIV_GAS * temp);
+  double viscosd =
+      (1.8325e-5 * (296.16 + 120.0) / (temp + 120.0)) * pow(temp / 296.16, 1.5);
+  double viscosk = viscosd / rhoair;
+  double gasspeed =
+      sqrt(8.0 * C_BOLTZMANN * temp * C_AVOGADRO / (C_PI * C_AIR_MOLEC_WEIGHT));
+  return 2.0 * viscosk / gasspeed;
+}
+
+/* fractal_vol_to_mobility_rad, fractal.F90:315-362, with its helpers:
+ * surface fractal dimension (:177-191), accessible surface (:199-216),
+ * Kirkwood-Riseman ratio (:223-231), continuum mobility radius (:239-249),
+ * effective radius (:257-268) and slip correction (:276-291); constants
+ * fractal.F90:43-53.  Newton's method from the continuum mobility radius,
+ * relative step 1e-14, at most 10 steps; *ok is cleared where the reference
+ * asserts (728724732). */
+static double mobility_rad(const orc_fractal *fr, double v, double temp,
+                           double pressure, int *ok) {
+  if (fr->sph) return frac_vol2rad(fr, v);
+  const double A = 1.142, Q = 0.588, B = 0.999, SF = 1.0, SE = 0.86;
+  double df = fr->frac_dim;
+  double ds = df <= 2.0 ? 3.0 : 6.0 / df;
+  double n = num_of_monomers(fr, v);
+  double s_acc = 4.0 * C_PI * (fr->prime_radius * fr->prime_radius) *
+                 pow(n, ds / 3.0) *
+                 ((ds - 2.0) * pow(SF / n, 1.0 - SE) - ds + 3.0);
+  double kr = -0.06483 * (df * df) + 0.6353 * df - 0.4898;
+  double rmec = kr * frac_vol2rad(fr, v);
+  double reff = s_acc / 4.0 / C_PI / rmec;
+  double fp = air_mean_free_path(temp, pressure);
+  double c_reff = 1.0 + A * fp / reff + Q * fp / reff * exp(-B * reff / fp);
+  double a1 = c_reff, a2 = -rmec, a3 = -rmec * Q * fp, a4 = -B / fp;
+  double a5 = -rmec * A * fp;
+  double x = rmec;
+  int step;
+  for (step = 1; step <= 10; step++) {
+    double f = a1 * (x * x) + a2 * x + a3 * exp(a4 * x) + a5;
+    double dfx = 2.0 * a1 * x + a2 + a3 * a4 * exp(a4 * x);
+    x = x - f / dfx;
+    if (fabs(f / dfx) / (fabs(x + f / dfx) + fabs(x)) < 1e-14) break;
+  }
+  if (!(step < 10)) *ok = 0;
+  return x;
+}
+
 /* interp_linear_disc, util.F90:663-683 */
 static double interp_linear_disc(double x1, double xn, int n, int i) {
   if (x1 == xn) return x1;
@@ -565,7 +643,7 @@ static double part_volume(orc_state *st, int i) {
 }
 
 static double part_radius(orc_state *st, int i) {
-  return orc_vol2rad(part_volume(st, i));
+  return frac_vol2rad(&st->frac, part_volume(st, i));
 }
 
 /* aero_particle_density = mass / volume, aero_particle.F90:491-501 */
@@ -696,10 +774,12 @@ static void particle_coagulate(orc_state *st, const double *va,
 /* ---------------------------------------------------------------------- */
 /* coagulation kernels                                                     */
 
-/* kernel_brown_helper, coag_kernel_brown.F90:111-197 (spherical particles:
- * the mobility radius is the geometric radius, fractal.F90:315-326) */
-static double brown_helper(double vol_i, double den_i, double vol_j,
-                           double den_j, double temp, double pressure) {
+/* kernel_brown_helper, coag_kernel_brown.F90:111-197: geometric radii in
+ * the sum, mobility radii (fractal_vol_to_mobility_rad) in the diffusion
+ * terms */
+static double brown_helper(const orc_fractal *fr, double vol_i, double den_i,
+                           double vol_j, double den_j, double temp,
+                           double pressure, int *ok) {
   double rhoair = (pressure * C_AIR_MOLEC_WEIGHT) / (C_UNIV_GAS * temp);
   double viscosd =
       1.8325e-05 * (416.16 / (temp + 120.0)) * pow(temp / 296.16, 1.5);
@@ -708,8 +788,8 @@ static double brown_helper(double vol_i, double den_i, double vol_j,
                          (C_PI * C_AIR_MOLEC_WEIGHT));
   double gasfreepath = 2.0 * viscosk / gasspeed;
 
-  double rad_i = orc_vol2rad(vol_i);
-  double rme_i = orc_vol2rad(vol_i);
+  double rad_i = frac_vol2rad(fr, vol_i);
+  double rme_i = mobility_rad(fr, vol_i, temp, pressure, ok);
   double knud = gasfreepath / rme_i;
   double cunning = 1.0 + knud * (1.249 + 0.42 * exp(-0.87 / knud));
   double diffus_i =
@@ -722,8 +802,8 @@ static double brown_helper(double vol_i, double den_i, double vol_j,
   double d = (tmp1 - tmp2) / (6.0 * rme_i * freepath) - 2.0 * rme_i;
   double deltasq_i = d * d;
 
-  double rad_j = orc_vol2rad(vol_j);
-  double rme_j = orc_vol2rad(vol_j);
+  double rad_j = frac_vol2rad(fr, vol_j);
+  double rme_j = mobility_rad(fr, vol_j, temp, pressure, ok);
   knud = gasfreepath / rme_j;
   cunning = 1.0 + knud * (1.249 + 0.42 * exp(-0.87 / knud));
   double diffus_j =
@@ -874,13 +954,15 @@ static double effic(double r1, double r2) {
 }
 
 /* kernel_sedi_helper, coag_kernel_sedi.F90:79-105 */
-static double sedi_helper(orc_state *st, double v1, double v2) {
-  double r1 = orc_vol2rad(v1);
-  double r2 = orc_vol2rad(v2);
-  double w1 = fall_g(orc_vol2rad(v1));
-  double w2 = fall_g(orc_vol2rad(v2));
+static double sedi_helper(orc_state *st, const orc_fractal *fr, double v1,
+                          double v2, double temp, double pressure) {
+  int ok = 1;
+  double r1 = frac_vol2rad(fr, v1);
+  double r2 = frac_vol2rad(fr, v2);
+  double w1 = fall_g(mobility_rad(fr, v1, temp, pressure, &ok));
+  double w2 = fall_g(mobility_rad(fr, v2, temp, pressure, &ok));
   double ec = effic(r1, r2);
-  if (ec < 0.0) {
+  if (ec < 0.0 || !ok) {
     if (st) orc_fail(st, ORC_ERR_ASSERT);
     return NAN;
   }
@@ -890,49 +972,86 @@ static double sedi_helper(orc_state *st, double v1, double v2) {
 
 static const double BETA_0 = 0.25 / (60.0 * 2e8); /* coag_kernel_constant.F90:22 */
 
-/* Fractal parameters of spherical particles, fractal_set_spherical
- * (fractal.F90:68-80): volume fractal dimension 3, primary radius 1e-8 m. */
-static const double FRAC_DIM = 3.0, PRIME_RADIUS = 1e-8;
 static const double AIR_DYN_VISC = 1.78e-5; /* constants.F90:65 */
 
-/* fractal_vol_to_num_of_monomers, fractal.F90:84-100 */
-static double num_of_monomers(double v) {
-  double x = orc_vol2rad(v) / PRIME_RADIUS;
-  return x * x * x;
-}
-
-/* kernel_brown_free_helper, coag_kernel_brown_free.F90 (free molecular
- * regime) */
-static double brown_free_helper(double v1, double d1, double v2, double d2,
-                                double temp) {
+/* kernel_brown_free_helper, coag_kernel_brown_free.F90:118-147 (free
+ * molecular regime) */
+static double brown_free_helper(const orc_fractal *fr, double v1, double d1,
+                                double v2, double d2, double temp) {
   double rho = (v1 / (v1 + v2)) * d1 + (v2 / (v1 + v2)) * d2;
-  double ni = num_of_monomers(v1), nj = num_of_monomers(v2);
-  double nif = pow(ni, 1.0 / FRAC_DIM), njf = pow(nj, 1.0 / FRAC_DIM);
+  double ni = num_of_monomers(fr, v1), nj = num_of_monomers(fr, v2);
+  double nif = pow(ni, 1.0 / fr->frac_dim), njf = pow(nj, 1.0 / fr->frac_dim);
   double s = nif + njf;
-  return sqrt(6.0 * C_BOLTZMANN * temp * PRIME_RADIUS / rho *
+  return sqrt(6.0 * C_BOLTZMANN * temp * fr->prime_radius / rho *
               (1.0 / ni + 1.0 / nj)) * (s * s);
 }
 
-/* kernel_brown_cont_helper, coag_kernel_brown_cont.F90 (continuum regime) */
-static double brown_cont_helper(double v1, double v2, double temp) {
-  double nif = pow(num_of_monomers(v1), 1.0 / FRAC_DIM);
-  double njf = pow(num_of_monomers(v2), 1.0 / FRAC_DIM);
+/* kernel_brown_cont_helper, coag_kernel_brown_cont.F90:115-144 (continuum
+ * regime) */
+static double brown_cont_helper(const orc_fractal *fr, double v1, double v2,
+                                double temp) {
+  double nif = pow(num_of_monomers(fr, v1), 1.0 / fr->frac_dim);
+  double njf = pow(num_of_monomers(fr, v2), 1.0 / fr->frac_dim);
   return 2.0 * C_BOLTZMANN * temp / 3.0 / AIR_DYN_VISC *
          (1.0 / nif + 1.0 / njf) * (nif + njf);
 }
 
-double orc_kernel_value(int kt, double v1, double d1, double v2, double d2,
-                        double temp, double pressure, double coeff) {
+static double kernel_value_fr(const orc_fractal *fr, int kt, double v1,
+                              double d1, double v2, double d2, double temp,
+                              double pressure, double coeff) {
+  int ok = 1;
+  double k = NAN;
   switch (kt) {
-    case ORC_KERNEL_SEDI: return sedi_helper(NULL, v1, v2);
+    case ORC_KERNEL_SEDI: return sedi_helper(NULL, fr, v1, v2, temp, pressure);
     case ORC_KERNEL_ADDITIVE: return coeff * (v1 + v2);
     case ORC_KERNEL_CONSTANT: return BETA_0;
-    case ORC_KERNEL_BROWN: return brown_helper(v1, d1, v2, d2, temp, pressure);
+    case ORC_KERNEL_BROWN:
+      k = brown_helper(fr, v1, d1, v2, d2, temp, pressure, &ok);
+      return ok ? k : NAN;
     case ORC_KERNEL_ZERO: return 0.0;
-    case ORC_KERNEL_BROWN_FREE: return brown_free_helper(v1, d1, v2, d2, temp);
-    case ORC_KERNEL_BROWN_CONT: return brown_cont_helper(v1, v2, temp);
+    case ORC_KERNEL_BROWN_FREE: return brown_free_helper(fr, v1, d1, v2, d2, temp);
+    case ORC_KERNEL_BROWN_CONT: return brown_cont_helper(fr, v1, v2, temp);
   }
-  return NAN;
+  return k;
+}
+
+double orc_kernel_value(int kt, double v1, double d1, double v2, double d2,
+                        double temp, double pressure, double coeff) {
+  return kernel_value_fr(&SPHERE, kt, v1, d1, v2, d2, temp, pressure, coeff);
+}
+
+double orc_kernel_value_fractal(int kt, double v1, double d1, double v2,
+                                double d2, double temp, double pressure,
+                                double coeff, double frac_dim,
+                                double prime_radius, double vol_fill_factor) {
+  orc_fractal fr = {frac_dim, prime_radius, vol_fill_factor,
+                    frac_dim == 3.0 && vol_fill_factor == 1.0};
+  return kernel_value_fr(&fr, kt, v1, d1, v2, d2, temp, pressure, coeff);
+}
+
+double orc_fractal_radius(double v, double frac_dim, double prime_radius,
+                          double vol_fill_factor, double temp, double pressure,
+                          double *mobility) {
+  orc_fractal fr = {frac_dim, prime_radius, vol_fill_factor,
+                    frac_dim == 3.0 && vol_fill_factor == 1.0};
+  int ok = 1;
+  if (mobility) *mobility = mobility_rad(&fr, v, temp, pressure, &ok);
+  if (!ok && mobility) *mobility = NAN;
+  return frac_vol2rad(&fr, v);
+}
+
+int orc_set_fractal(orc_state *st, double frac_dim, double prime_radius,
+                    double vol_fill_factor) {
+  if (!(frac_dim > 0.0 && frac_dim <= 3.0) || !(prime_radius > 0.0) ||
+      !(vol_fill_factor > 0.0))
+    return ORC_ERR_ARG;
+  st->frac.frac_dim = frac_dim;
+  st->frac.prime_radius = prime_radius;
+  st->frac.vol_fill_factor = vol_fill_factor;
+  st->frac.sph = frac_dim == 3.0 && vol_fill_factor == 1.0;
+  st->valid_sort = 0; /* radii, bins and bounds all change */
+  st->kbounds_valid = 0;
+  return ORC_OK;
 }
 
 /* kernel dispatch on two particles, coag_kernel.F90:83-125 */
@@ -940,18 +1059,23 @@ static double kernel_particles(orc_state *st, int kt, const double *va,
                                const double *vb, double temp, double pressure,
                                double coeff) {
   double v1 = vol_sum(va, st->n_spec), v2 = vol_sum(vb, st->n_spec);
+  const orc_fractal *fr = &st->frac;
+  int ok = 1;
+  double k;
   switch (kt) {
-    case ORC_KERNEL_SEDI: return sedi_helper(st, v1, v2);
+    case ORC_KERNEL_SEDI: return sedi_helper(st, fr, v1, v2, temp, pressure);
     case ORC_KERNEL_ADDITIVE: return coeff * (v1 + v2);
     case ORC_KERNEL_CONSTANT: return BETA_0;
     case ORC_KERNEL_BROWN:
-      return brown_helper(v1, vol_density(st, va), v2, vol_density(st, vb),
-                          temp, pressure);
+      k = brown_helper(fr, v1, vol_density(st, va), v2, vol_density(st, vb),
+                       temp, pressure, &ok);
+      if (!ok) orc_fail(st, ORC_ERR_ASSERT);
+      return k;
     case ORC_KERNEL_ZERO: return 0.0;
     case ORC_KERNEL_BROWN_FREE:
-      return brown_free_helper(v1, vol_density(st, va), v2, vol_density(st, vb),
-                               temp);
-    case ORC_KERNEL_BROWN_CONT: return brown_cont_helper(v1, v2, temp);
+      return brown_free_helper(fr, v1, vol_density(st, va), v2,
+                               vol_density(st, vb), temp);
+    case ORC_KERNEL_BROWN_CONT: return brown_cont_helper(fr, v1, v2, temp);
   }
   orc_fail(st, ORC_ERR_ARG);
   return 0.0;
@@ -964,7 +1088,7 @@ void orc_kernel_minmax(orc_state *st, int kt, double v1, double v2,
                        double *kmin, double *kmax) {
   switch (kt) {
     case ORC_KERNEL_SEDI:
-      *kmin = *kmax = sedi_helper(st, v1, v2);
+      *kmin = *kmax = sedi_helper(st, &st->frac, v1, v2, temp, pressure);
       return;
     case ORC_KERNEL_ADDITIVE:
       *kmin = *kmax = coeff * (v1 + v2);
@@ -984,16 +1108,18 @@ void orc_kernel_minmax(orc_state *st, int kt, double v1, double v2,
         if (st->density[k] < dmin) dmin = st->density[k];
         if (st->density[k] > dmax) dmax = st->density[k];
       }
-      int first = 1;
+      int first = 1, ok = 1;
+      const orc_fractal *fr = &st->frac;
       for (int i = 1; i <= 3; i++)
         for (int j = 1; j <= 3; j++) {
           double d1 = interp_linear_disc(dmin, dmax, 3, i);
           double d2 = interp_linear_disc(dmin, dmax, 3, j);
           double k = kt == ORC_KERNEL_BROWN
-                         ? brown_helper(v1, d1, v2, d2, temp, pressure)
+                         ? brown_helper(fr, v1, d1, v2, d2, temp, pressure, &ok)
                          : kt == ORC_KERNEL_BROWN_FREE
-                               ? brown_free_helper(v1, d1, v2, d2, temp)
-                               : brown_cont_helper(v1, v2, temp);
+                               ? brown_free_helper(fr, v1, d1, v2, d2, temp)
+                               : brown_cont_helper(fr, v1, v2, temp);
+          if (!ok) orc_fail(st, ORC_ERR_ASSERT);
           if (first) {
             first = 0;
             *kmin = k;
@@ -1012,7 +1138,8 @@ void orc_kernel_minmax(orc_state *st, int kt, double v1, double v2,
 /* coag_num_conc_factor, coag_kernel.F90:346-377 */
 static double num_conc_factor(const orc_state *st, double ri, double rj,
                               int ci, int cj, int cij) {
-  double rij = orc_vol2rad(orc_rad2vol(ri) + orc_rad2vol(rj));
+  const orc_fractal *fr = &st->frac;
+  double rij = frac_vol2rad(fr, frac_rad2vol(fr, ri) + frac_rad2vol(fr, rj));
   double nci = orc_num_conc_at_radius(st, ci, ri);
   double ncj = orc_num_conc_at_radius(st, cj, rj);
   double ncij = orc_num_conc_at_radius(st, cij, rij);
@@ -1027,8 +1154,8 @@ static double weighted_kernel(orc_state *st, int kt, const double *va,
                               const double *vb, int ci, int cj, int cij,
                               double temp, double pressure, double coeff) {
   double k = kernel_particles(st, kt, va, vb, temp, pressure, coeff);
-  double ri = orc_vol2rad(vol_sum(va, st->n_spec));
-  double rj = orc_vol2rad(vol_sum(vb, st->n_spec));
+  double ri = frac_vol2rad(&st->frac, vol_sum(va, st->n_spec));
+  double rj = frac_vol2rad(&st->frac, vol_sum(vb, st->n_spec));
   return k * num_conc_factor(st, ri, rj, ci, cj, cij);
 }
 
@@ -1048,7 +1175,8 @@ int orc_coag_dest_class(const orc_state *st, const double *edges,
   (void)b2;
   double ri = centers[b1 - 1];
   double rj = centers[b1 - 1];
-  double rij = orc_vol2rad(orc_rad2vol(ri) + orc_rad2vol(rj));
+  const orc_fractal *fr = &st->frac;
+  double rij = frac_vol2rad(fr, frac_rad2vol(fr, ri) + frac_rad2vol(fr, rj));
   double nci = orc_num_conc_at_radius(st, c1, rij);
   double ncj = orc_num_conc_at_radius(st, c2, rij);
   return nci < ncj ? c1 : c2;
@@ -1074,10 +1202,10 @@ double orc_max_num_conc_factor(const orc_state *st, const double *edges,
 static void kminmax_for_bin(orc_state *st, int kt, const double *edges,
                             int b1, int b2, double temp, double pressure,
                             double coeff, double *kmin, double *kmax) {
-  double v1lo = orc_rad2vol(edges[b1 - 1]);
-  double v1hi = orc_rad2vol(edges[b1]);
-  double v2lo = orc_rad2vol(edges[b2 - 1]);
-  double v2hi = orc_rad2vol(edges[b2]);
+  double v1lo = frac_rad2vol(&st->frac, edges[b1 - 1]);
+  double v1hi = frac_rad2vol(&st->frac, edges[b1]);
+  double v2lo = frac_rad2vol(&st->frac, edges[b2 - 1]);
+  double v2hi = frac_rad2vol(&st->frac, edges[b2]);
   for (int i = 1; i <= 3; i++)
     for (int j = 1; j <= 3; j++) {
       double v1 = interp_linear_disc(v1lo, v1hi, 3, i);
@@ -1250,7 +1378,7 @@ static void state_add(orc_state *st, const double *v,
   int b = -1;
   if (st->n_bin > 0)
     b = orc_bin_find(st->n_bin, st->edges[0], st->edges[st->n_bin],
-                     orc_vol2rad(vol_sum(v, st->n_spec)));
+                     frac_vol2rad(&st->frac, vol_sum(v, st->n_spec)));
   if (m->weight_group < 1 || m->weight_group > st->n_group ||
       m->weight_class < 1 || m->weight_class > st->n_class)
     orc_fail(st, ORC_ERR_ASSERT);
@@ -1314,7 +1442,8 @@ static void coagulate_weighting(orc_state *st, int p1, int p2, int c1, int c2,
   if (m1->id == m2->id) orc_fail(st, ORC_ERR_ASSERT);
   double r1 = part_radius(st, p1);
   double r2 = part_radius(st, p2);
-  double rc = orc_vol2rad(orc_rad2vol(r1) + orc_rad2vol(r2));
+  double rc = frac_vol2rad(&st->frac, frac_rad2vol(&st->frac, r1) +
+                                         frac_rad2vol(&st->frac, r2));
   double nc1 = orc_num_conc_at_radius(st, c1, r1);
   double nc2 = orc_num_conc_at_radius(st, c2, r2);
   double ncc = orc_num_conc_at_radius(st, cc, rc);
@@ -1476,7 +1605,7 @@ static void sample_source_particle(orc_state *st, const coag_env *env, int bs,
   *n_coag_out = 0;
   if (cell_n(st, bs, cs) == 0) return;
   double nc_target = orc_num_conc_at_radius(
-      st, target->m.weight_class, orc_vol2rad(vol_sum(target->vol, ns)));
+      st, target->m.weight_class, frac_vol2rad(&st->frac, vol_sum(target->vol, ns)));
   int ct = target->m.weight_class;
   double nc_src_min = orc_num_conc_at_radius(st, cs, st->edges[bs - 1]);
   double prm_max = nc_target / nc_src_min;
@@ -1622,8 +1751,8 @@ static int try_per_particle_coag(orc_state *st, const coag_env *env,
   double nspt = k_max * env->del_t * (double)cell_n(st, bs, cs);
   double af = 1.0 / k_max;
   if (nspt < COAG_ACCEL_N_EVENT) return 0;
-  double min_tv = orc_rad2vol(st->edges[bt - 1]);
-  double max_sv = orc_rad2vol(st->edges[bs]);
+  double min_tv = frac_rad2vol(&st->frac, st->edges[bt - 1]);
+  double max_sv = frac_rad2vol(&st->frac, st->edges[bs]);
   double max_new = min_tv + max_sv * nspt;
   if (max_new / min_tv > MAX_ALLOWABLE_GROWTH_FACTOR) return 0;
   for (int e = cell_n(st, bt, ct); e >= 1; e--) {
@@ -1707,6 +1836,7 @@ orc_state *orc_create(int n_spec, const double *density, int i_water,
     return NULL;
   orc_state *st = (orc_state *)calloc(1, sizeof(orc_state));
   if (!st) return NULL;
+  st->frac = SPHERE;
   st->n_spec = n_spec;
   st->density = (double *)malloc(sizeof(double) * n_spec);
   memcpy(st->density, density, sizeof(double) * n_spec);
@@ -1833,8 +1963,9 @@ int orc_check(const orc_state *st) {
   }
   for (int i = 1; i <= st->n_part; i++) {
     int b = orc_bin_find(st->n_bin, st->edges[0], st->edges[st->n_bin],
-                         orc_vol2rad(vol_sum(st->vol + (size_t)(i - 1) * st->n_spec,
-                                             st->n_spec)));
+                         frac_vol2rad(&st->frac,
+                                      vol_sum(st->vol + (size_t)(i - 1) * st->n_spec,
+                                              st->n_spec)));
     if (b != st->size_class.fwd1.e[i - 1]) return 50;
     if (st->meta[i - 1].weight_group != st->group_class.fwd1.e[i - 1] ||
         st->meta[i - 1].weight_class != st->group_class.fwd2.e[i - 1])

@@ -132,7 +132,25 @@ int orc_kmax_table(orc_state *st, int kernel_type, double temp,
                    double pressure, double additive_coeff, double *kmin,
                    double *kmax);
 
+/* Particle shape of aero_data (fractal_t, fractal.F90:59-66); d_f = 3 and
+ * f = 1 are spherical particles, the default.  Invalidates the sort and the
+ * k_max bounds.  ORC_ERR_ARG for d_f outside (0, 3] or R0, f <= 0. */
+int orc_set_fractal(orc_state *st, double frac_dim, double prime_radius,
+                    double vol_fill_factor);
+
 /* ----- pure functions, for unit tests ----- */
+/* fractal_vol2rad of volume v; *mobility (if not NULL) gets
+ * fractal_vol_to_mobility_rad at temp, pressure (NAN if the Newton loop
+ * does not converge) */
+double orc_fractal_radius(double v, double frac_dim, double prime_radius,
+                          double vol_fill_factor, double temp, double pressure,
+                          double *mobility);
+/* orc_kernel_value for particles of the given fractal shape */
+double orc_kernel_value_fractal(int kernel_type, double v1, double d1,
+                                double v2, double d2, double temp,
+                                double pressure, double additive_coeff,
+                                double frac_dim, double prime_radius,
+                                double vol_fill_factor);
 double orc_vol2rad(double v);
 double orc_rad2vol(double r);
 /* unweighted kernel between particles of total volume v and density d */

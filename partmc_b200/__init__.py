@@ -4,7 +4,8 @@ The hot path is CUDA in libpmc_coag_gpu.so behind the C ABI of
 include/pmc_coag_gpu.h; this package is the host-side mirror of the
 reference's interface for that path.
 """
-from .coagulation import (AeroData, AeroState, AeroWeightArray, EnvState, HostMirror, mc_coag, mc_coag_batch,  # noqa: F401
+from .coagulation import (AeroData, AeroState, AeroWeightArray, EnvState, Fractal, HostMirror, mc_coag,  # noqa: F401
+                          mc_coag_batch,
                           COAG_KERNEL_TYPE_ADDITIVE, COAG_KERNEL_TYPE_BROWN, COAG_KERNEL_TYPE_CONSTANT,
                           COAG_KERNEL_TYPE_SEDI, COAG_KERNEL_TYPE_ZERO, COAG_KERNEL_TYPE_BROWN_FREE,
                           COAG_KERNEL_TYPE_BROWN_CONT, MODE_FP64, MODE_MIXED, MODE_REPLAY)

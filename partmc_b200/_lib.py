@@ -70,6 +70,7 @@ SIGNATURES = {
     "pmc_coag_gpu_launch_count": (_I, [_LP]),
     "pmc_coag_gpu_conflicts": (_I, [_P, _LP, _LP, _LP, _LP]),
     "pmc_coag_gpu_exact_tests": (_I, [_P, _LP]),
+    "pmc_coag_gpu_set_fractal": (_I, [_P, _D, _D, _D]),
     "pmc_coag_gpu_bin_sort_noalloc": (_I, [_I, _P, _P, _I, _I, _D, _D, _P, _P, _P, _P, _P]),
 }
 

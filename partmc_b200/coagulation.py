@@ -32,13 +32,30 @@ AERO_WEIGHT_TYPE_MFA = 3
 MAX_AERO_COMPONENT_SIZE = 20
 
 
-class AeroData:
-    """Species densities (kg/m^3) and the water species index (1-based, 0 = none)."""
+class Fractal:
+    """Particle shape (fractal_t, fractal.F90:59-66): volume fractal dimension,
+    primary-particle radius (m) and volume filling factor.  The defaults are
+    spherical particles (fractal_set_spherical, fractal.F90:73-82)."""
 
-    def __init__(self, density, i_water=0, names=None):
+    def __init__(self, frac_dim=3.0, prime_radius=1e-8, vol_fill_factor=1.0):
+        self.frac_dim = float(frac_dim)
+        self.prime_radius = float(prime_radius)
+        self.vol_fill_factor = float(vol_fill_factor)
+
+    @property
+    def spherical(self):
+        return self.frac_dim == 3.0 and self.vol_fill_factor == 1.0
+
+
+class AeroData:
+    """Species densities (kg/m^3), the water species index (1-based, 0 = none)
+    and the particle shape (aero_data%fractal)."""
+
+    def __init__(self, density, i_water=0, names=None, fractal=None):
         self.density = np.ascontiguousarray(np.atleast_1d(density), dtype=np.float64)
         self.i_water = int(i_water)
         self.names = names
+        self.fractal = Fractal() if fractal is None else fractal
 
     @property
     def n_spec(self):
@@ -131,6 +148,13 @@ class AeroState:
         check(rc, "pmc_coag_gpu_init")
         self.ctx = ctx
         self.set_mode(mode)
+        if not aero_data.fractal.spherical:
+            self.set_fractal(aero_data.fractal)
+
+    def set_fractal(self, fractal):
+        """Particle shape of every population (pmc_coag_gpu_set_fractal)."""
+        check(_lib.lib().pmc_coag_gpu_set_fractal(self.ctx, fractal.frac_dim, fractal.prime_radius,
+                                                  fractal.vol_fill_factor), "pmc_coag_gpu_set_fractal")
 
     def __del__(self):
         if getattr(self, "ctx", None):

@@ -507,7 +507,7 @@ __global__ void k_size_dist(PopDev P, int n_bin, double log_lo, double log_hi, d
   int n = P.ctr->n_slots;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (!P.alive[i]) continue;
-    double r = vol2rad(P.vtot[i]);
+    double r = vol2rad(P.benv.frac, P.vtot[i]);  // aero_particle_radius (fractal_vol2rad)
     int b = bin_find(n_bin, log_lo, log_hi, 2.0 * r);
     if (b < 1 || b > n_bin) continue;
     double nc = num_conc_at_radius<double>(P.w, P.cls[i] - 1, r) * inv_width;
@@ -580,27 +580,7 @@ __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, 
   RecD q[2];
   double vt[2] = {vt1, vt2}, ms[2] = {m1, m2};
   int cl[2] = {c1[i] - 1, c2[i] - 1};
-  for (int k = 0; k < 2; k++) {
-    double r = vol2rad(vt[k]);
-    q[k].r = r;
-    q[k].rv = rad2vol(r);
-    q[k].nc = num_conc_at_radius<double>(P.w, cl[k], r);
-    q[k].a = q[k].b = q[k].c = 0.0;
-    if (P.kernel_type == kKernelAdditive) q[k].a = vt[k];
-    if (P.kernel_type == kKernelBrown) {
-      BrownPart bp = brown_part(P.benv, vt[k], ms[k] / vt[k]);
-      q[k].a = bp.diffus;
-      q[k].b = bp.speedsq;
-      q[k].c = bp.deltasq;
-    }
-    if (P.kernel_type == kKernelSedi) q[k].a = fall_g(vol2rad(vt[k]));
-    if (P.kernel_type == kKernelBrownFree) {
-      q[k].a = vt[k];
-      q[k].b = ms[k] / vt[k];
-      q[k].c = pow(num_of_monomers(P.benv, vt[k]), 1.0 / P.benv.frac_dim);
-    }
-    if (P.kernel_type == kKernelBrownCont) q[k].a = pow(num_of_monomers(P.benv, vt[k]), 1.0 / P.benv.frac_dim);
-  }
+  for (int k = 0; k < 2; k++) q[k] = make_rec_v(P, vol2rad(P.benv.frac, vt[k]), vt[k], ms[k], cl[k] + 1);
   int cc = cij[i] - 1;
   double k;
   if (precision == 0) {
@@ -844,6 +824,8 @@ struct Ctx {
   DevBuf<double> replay_u;
   long long replay_n = 0, replay_used = 0;
   ReplayBuffers replay;
+  // particle shape of aero_data (fractal_t); spherical unless set
+  Fractal frac = fractal_spherical();
 };
 
 void free_list(std::vector<void*>& v) {
@@ -1247,7 +1229,7 @@ __global__ void k_radius_minmax_masked(const PopDev* pops, const uint8_t* on) {
   unsigned long long lo = ~0ULL, hi = 0ULL;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (!P.alive[i]) continue;
-    unsigned long long b = (unsigned long long)__double_as_longlong(vol2rad(P.vtot[i]));
+    unsigned long long b = (unsigned long long)__double_as_longlong(vol2rad(P.benv.frac, P.vtot[i]));
     lo = b < lo ? b : lo;
     hi = b > hi ? b : hi;
   }
@@ -2652,7 +2634,7 @@ int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* 
       ph.h.pressure = pressure[k];
       ph.h.coeff = additive_coeff;
       ph.h.del_t = del_t;
-      ph.h.benv = brown_env(temp[k], pressure[k]);
+      ph.h.benv = brown_env(temp[k], pressure[k], c.frac);
       ph.h.step = ++ph.step;
       // the reference keeps its bounds until the grid changes
       // (coag_kernel_bounds_valid, aero_sorted.F90:55); a new kernel type
@@ -3034,6 +3016,30 @@ int pmc_coag_gpu_set_weight(pmc_coag_gpu_ctx* x, const int* w_type, const double
   GUARD_END
 }
 
+int pmc_coag_gpu_set_fractal(pmc_coag_gpu_ctx* x, double frac_dim, double prime_radius, double vol_fill_factor) {
+  // spec_file_read_fractal stops for d_f > 3 (fractal.F90:587); d_f, R0 and
+  // f also divide or take roots, so each must be positive
+  if (!x || !(frac_dim > 0.0 && frac_dim <= 3.0) || !(prime_radius > 0.0) || !(vol_fill_factor > 0.0))
+    return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  c.frac = make_fractal(frac_dim, prime_radius, vol_fill_factor);
+  // radii, records, grid and k_max bounds all follow the particle shape
+  for (auto& ph : c.pops) {
+    ph.h.benv = brown_env(ph.h.temp > 0.0 ? ph.h.temp : 288.0, ph.h.pressure > 0.0 ? ph.h.pressure : 1e5, c.frac);
+    ph.wver++;
+    ph.valid_sort = false;
+    ph.h.kmax_valid = 0;
+    ph.h.pair_setup_valid = 0;
+  }
+  c.replay.valid = false;
+  c.dirty = true;
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
 int pmc_coag_gpu_set_weight_pop(pmc_coag_gpu_ctx* x, int pop, const int* w_type, const double* w_mag,
                                 const double* w_exp) {
   if (!x || pop < 0 || pop >= x->c.n_pop || !w_type || !w_mag || !w_exp) return PMC_ERR_INVALID_ARG;
@@ -3227,7 +3233,7 @@ int pmc_coag_gpu_kmax_table(pmc_coag_gpu_ctx* x, int kernel_type, double temp, d
   ph.h.temp = temp;
   ph.h.pressure = pressure;
   ph.h.coeff = additive_coeff;
-  ph.h.benv = brown_env(temp, pressure);
+  ph.h.benv = brown_env(temp, pressure, c.frac);
   ph.h.kmax_valid = 0;
   push_pops(c);
   int nb = std::max(ph.n_bin, 1);
@@ -3255,7 +3261,7 @@ int pmc_coag_gpu_eval_kernel(pmc_coag_gpu_ctx* x, int kernel_type, double temp, 
   P.temp = temp;
   P.pressure = pressure;
   P.coeff = additive_coeff;
-  P.benv = brown_env(temp, pressure);
+  P.benv = brown_env(temp, pressure, c.frac);
   std::vector<void*> tmp;
   size_t nv = (size_t)n_pairs * c.n_spec;
   double* d1 = dalloc<double>(tmp, nv);

@@ -144,29 +144,32 @@ __device__ int block_excl_scan(int v, int* total) {
 // class cls (1-based) (see RecD)
 __device__ __forceinline__ RecD make_rec_v(const PopDev& P, double r, double v, double m, int cls) {
   RecD q;
+  const Fractal& F = P.benv.frac;
+  bool ok = true;
   q.r = r;
-  q.rv = rad2vol(r);
+  q.rv = rad2vol(F, r);
   q.nc = num_conc_at_radius<double>(P.w, cls - 1, r);
   q.a = q.b = q.c = 0.0;
   switch (P.kernel_type) {
     case kKernelAdditive: q.a = v; break;
     case kKernelBrown: {
-      BrownPart bp = brown_part(P.benv, v, m / v);
+      BrownPart bp = brown_part(P.benv, v, m / v, &ok);
       q.a = bp.diffus;
       q.b = bp.speedsq;
       q.c = bp.deltasq;
       break;
     }
-    case kKernelSedi: q.a = fall_g(vol2rad(v)); break;
+    case kKernelSedi: q.a = fall_g(mobility_rad(F, v, P.benv.fp, &ok)); break;
     case kKernelBrownFree: {
       q.a = v;
       q.b = m / v;
-      q.c = pow(num_of_monomers(P.benv, v), 1.0 / P.benv.frac_dim);
+      q.c = pow(num_of_monomers(F, v), 1.0 / F.frac_dim);
       break;
     }
-    case kKernelBrownCont: q.a = pow(num_of_monomers(P.benv, v), 1.0 / P.benv.frac_dim); break;
+    case kKernelBrownCont: q.a = pow(num_of_monomers(F, v), 1.0 / F.frac_dim); break;
     default: break;
   }
+  if (!ok) set_status(P.ctr, kErrAssert);  // the fractal Newton loop did not converge
   return q;
 }
 
@@ -192,7 +195,7 @@ __device__ __forceinline__ RecF to_f32(const RecD& q) {
 // off the grid, which leaves the slot unsorted)
 __device__ __forceinline__ int refresh_slot(const PopDev& P, int i) {
   const GridDev& G = *P.grid;
-  double r = vol2rad(P.vtot[i]);
+  double r = vol2rad(P.benv.frac, P.vtot[i]);
   P.rad[i] = r;
   int b = bin_find(G.n_bin, G.log_lo, G.log_hi, r);
   int cl = P.cls[i] - 1;
@@ -416,12 +419,13 @@ __global__ void k_pair_setup(const PopDev* pops) {
   PairDesc d = P.pair_desc[p];
   int b1 = d.b1, b2 = d.b2, c1 = d.c1, c2 = d.c2;
   const GridDev& G = *P.grid;
-  int cc = coag_dest_class(P.w, G.centers, b1, b2, c1, c2);
+  const Fractal& F = P.benv.frac;
+  int cc = coag_dest_class(P.w, F, G.centers, b1, b2, c1, c2);
   double f = 0.0;
   if (lane < 25) {
     double ri = interp_linear_disc(G.edges[b1], G.edges[b1 + 1], 5, lane / 5 + 1);
     double rj = interp_linear_disc(G.edges[b2], G.edges[b2 + 1], 5, lane % 5 + 1);
-    f = num_conc_factor(P.w, ri, rj, c1, c2, cc);
+    f = num_conc_factor(P.w, F, ri, rj, c1, c2, cc);
   }
   // the factors are positive: the maximum does not depend on the order
   for (int o = 16; o > 0; o >>= 1) {
@@ -432,7 +436,7 @@ __global__ void k_pair_setup(const PopDev* pops) {
   PairState& S = P.pair[p];
   S.cc = cc;
   S.f_max = f;
-  S.fflat = P.flat ? num_conc_factor(P.w, G.centers[b1], G.centers[b2], c1, c2, cc) : 1.0;
+  S.fflat = P.flat ? num_conc_factor(P.w, F, G.centers[b1], G.centers[b2], c1, c2, cc) : 1.0;
   S.pp_ok = 0;
   if (P.mono_dec) {
     double n1min, n1max, n2min, n2max;
@@ -455,8 +459,8 @@ __global__ void k_pair_setup(const PopDev* pops) {
     }
     S.pp_ok = ok;
     S.bt = bt; S.bs = bs; S.ct = ct; S.cs = cs;
-    S.pp_min_tv = rad2vol(G.edges[bt]);
-    S.pp_max_sv = rad2vol(G.edges[bs + 1]);
+    S.pp_min_tv = rad2vol(F, G.edges[bt]);
+    S.pp_max_sv = rad2vol(F, G.edges[bs + 1]);
   }
 }
 
@@ -543,20 +547,19 @@ __device__ __forceinline__ T pair_kernel(const PopDev& P, const T* q1, const T* 
   } else if (KT == kKernelSedi) {
     k = sedi_pair<T>(q1[0], q1[3], q2[0], q2[3]);
   } else if (KT == kKernelBrownFree) {
-    // q = {r, rv, nc, volume, density, N^(1/d_f)}; 1/N = (R0 / r)^3
+    // q = {r, rv, nc, volume, density, N^(1/d_f)}; 1/N = V(R0) / volume
     T v1 = q1[3], v2 = q2[3];
     T rho = (v1 / (v1 + v2)) * q1[4] + (v2 / (v1 + v2)) * q2[4];
-    T x1 = T(P.benv.prime_radius) / q1[0], x2 = T(P.benv.prime_radius) / q2[0];
+    const T v0 = T(rad2vol(P.benv.frac.prime_radius));
     T s = q1[5] + q2[5];
     if constexpr (sizeof(T) == 8) {
-      k = sqrt(T(6.0 * kBoltzmann * P.benv.temp * P.benv.prime_radius) / rho * (x1 * x1 * x1 + x2 * x2 * x2)) *
-          (s * s);
+      k = sqrt(T(6.0 * kBoltzmann * P.benv.temp * P.benv.frac.prime_radius) / rho * (v0 / v1 + v0 / v2)) * (s * s);
     } else {
       // the same product with the constant's square root taken apart: 6 k T R0
       // is about 1e-28, and divided by rho and multiplied by 1/N of a large
       // cluster it would fall below FP32's normal range
-      k = T(sqrt(6.0 * kBoltzmann * P.benv.temp * P.benv.prime_radius)) *
-          sqrt((x1 * x1 * x1 + x2 * x2 * x2) / rho) * (s * s);
+      k = T(sqrt(6.0 * kBoltzmann * P.benv.temp * P.benv.frac.prime_radius)) * sqrt((v0 / v1 + v0 / v2) / rho) *
+          (s * s);
     }
   } else if (KT == kKernelBrownCont) {
     // q = {r, rv, nc, N^(1/d_f), -, -}
@@ -565,7 +568,7 @@ __device__ __forceinline__ T pair_kernel(const PopDev& P, const T* q1, const T* 
     k = T(0);
   }
   if (FLAT) return k * fflat;
-  T rij = vol2rad(q1[1] + q2[1]);
+  T rij = vol2rad(P.benv.frac, q1[1] + q2[1]);
   T ncij = num_conc_at_radius<T>(P.w, cc, rij);
   T nci = q1[2], ncj = q2[2];
   T mn = nci;
@@ -629,7 +632,8 @@ template <class R>
 __device__ MergeDecision merge_decide_v(const PopDev& P, R& g, double r1, double vt1, double r2, double vt2, int c1,
                                         int c2, int cc) {
   MergeDecision d;
-  double rc = vol2rad(rad2vol(r1) + rad2vol(r2));
+  const Fractal& F = P.benv.frac;
+  double rc = vol2rad(F, rad2vol(F, r1) + rad2vol(F, r2));
   double nc1 = num_conc_at_radius<double>(P.w, c1, r1);
   double nc2 = num_conc_at_radius<double>(P.w, c2, r2);
   double ncc = num_conc_at_radius<double>(P.w, cc, rc);

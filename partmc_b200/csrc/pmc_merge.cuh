@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gp
       double s_v = 0.0, s_m = 0.0;
       for (int sp = 0; sp < ns; sp++) s_v = s_v + vcur[sp];
       for (int sp = 0; sp < ns; sp++) s_m = s_m + vcur[sp] * P.density[sp];
-      const double vt = s_v, r = vol2rad(vt);
+      const double vt = s_v, r = vol2rad(P.benv.frac, vt);
       const RecD qxd = make_rec_v(P, r, vt, s_m, cls);
       const RecF qxf = to_f32(qxd);
       const int C = cell_of(P, r, cls);
@@ -933,7 +933,7 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
           double s_v = 0.0;
           for (int sp = 0; sp < ns; sp++) s_v = s_v + pre[lane * kMaxSpec + sp];
           vt_k = s_v;
-          r_k = vol2rad(vt_k);
+          r_k = vol2rad(P.benv.frac, vt_k);
           C_k = cell_of(P, r_k, stage[lane].cc + 1);
         }
         double r_b = __shfl_up_sync(kFull, r_k, 1), vt_b = __shfl_up_sync(kFull, vt_k, 1);
@@ -1361,7 +1361,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
       acc[k] = P.vol[vol_at(P, t, k)] + acc[k];  // now the new target volumes
       vt = vt + acc[k];
     }
-    double rnew = vol2rad(vt);
+    double rnew = vol2rad(P.benv.frac, vt);
     int cc = S.cc;
     nm.grp = rand_group(g, P.w, cc, rnew);
     nm.cls = cc + 1;

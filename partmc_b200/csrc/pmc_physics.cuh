@@ -53,6 +53,107 @@ PMC_HD double rad2vol(double r) { return 4.0 * kPi * (r * r * r) / 3.0; }
 PMC_HD float vol2rad(float v) { return cbrtf(v * (float)(3.0 / (4.0 * kPi))); }
 PMC_HD float rad2vol(float r) { return (float)(4.0 * kPi / 3.0) * (r * r * r); }
 
+// fractal_t (fractal.F90:59-66, after Naumann 2003): volume fractal
+// dimension, primary-particle radius (m) and volume filling factor.  With
+// d_f = 3 and f = 1 (fractal_is_spherical) every conversion is the sphere's.
+struct Fractal {
+  double frac_dim, prime_radius, vol_fill_factor;
+  int spherical;
+};
+// fractal_set_spherical, fractal.F90:73-82
+PMC_HD Fractal fractal_spherical() { return Fractal{3.0, 1e-8, 1.0, 1}; }
+PMC_HD Fractal make_fractal(double frac_dim, double prime_radius, double vol_fill_factor) {
+  return Fractal{frac_dim, prime_radius, vol_fill_factor, (frac_dim == 3.0 && vol_fill_factor == 1.0) ? 1 : 0};
+}
+
+// fractal_vol_to_num_of_monomers, fractal.F90:90-100: (r_sphere(v) / R0)^3
+PMC_HD double num_of_monomers(const Fractal& F, double v) {
+  double x = vol2rad(v) / F.prime_radius;
+  return x * x * x;
+}
+// fractal_vol2rad, fractal.F90:106-121: R0 (N f)^(1/d_f)
+PMC_HD double vol2rad(const Fractal& F, double v) {
+  if (F.spherical) return vol2rad(v);
+  return F.prime_radius * pow(num_of_monomers(F, v) * F.vol_fill_factor, 1.0 / F.frac_dim);
+}
+PMC_HD float vol2rad(const Fractal& F, float v) {
+  if (F.spherical) return vol2rad(v);
+  float x = vol2rad(v) / (float)F.prime_radius;
+  return (float)F.prime_radius * powf(x * x * x * (float)F.vol_fill_factor, (float)(1.0 / F.frac_dim));
+}
+// fractal_rad2vol, fractal.F90:142-157: V(R0) (r / R0)^d_f / f
+PMC_HD double rad2vol(const Fractal& F, double r) {
+  if (F.spherical) return rad2vol(r);
+  return rad2vol(F.prime_radius) * pow(r / F.prime_radius, F.frac_dim) / F.vol_fill_factor;
+}
+PMC_HD float rad2vol(const Fractal& F, float r) {
+  if (F.spherical) return rad2vol(r);
+  return (float)(rad2vol(F.prime_radius) / F.vol_fill_factor) * powf(r / (float)F.prime_radius, (float)F.frac_dim);
+}
+
+// air_mean_free_path, util.F90:289-312
+PMC_HD double air_mean_free_path(double temp, double pressure) {
+  double rhoair = (pressure * kAirMolecWeight) / (kUnivGas * temp);
+  double viscosd = (1.8325e-5 * (296.16 + 120.0) / (temp + 120.0)) * pow(temp / 296.16, 1.5);
+  double viscosk = viscosd / rhoair;
+  double gasspeed = sqrt(8.0 * kBoltzmann * temp * kAvogadro / (kPi * kAirMolecWeight));
+  return 2.0 * viscosk / gasspeed;
+}
+
+// slip-correction and accessible-surface constants, fractal.F90:43-53
+constexpr double kFracASlip = 1.142, kFracQSlip = 0.588, kFracBSlip = 0.999;
+constexpr double kFracScaleFactorSAcc = 1.0, kFracScaleExponentSAcc = 0.86;
+
+// fractal_surface_frac_dim, fractal.F90:177-191 (d_f above 3 is rejected
+// when the parameters are set)
+PMC_HD double surface_frac_dim(const Fractal& F) { return F.frac_dim <= 2.0 ? 3.0 : 6.0 / F.frac_dim; }
+// fractal_vol_to_accessible_surface, fractal.F90:199-216 (Naumann eq. 26)
+PMC_HD double accessible_surface(const Fractal& F, double v) {
+  double ds = surface_frac_dim(F);
+  double n = num_of_monomers(F, v);
+  return 4.0 * kPi * (F.prime_radius * F.prime_radius) * pow(n, ds / 3.0) *
+         ((ds - 2.0) * pow(kFracScaleFactorSAcc / n, 1.0 - kFracScaleExponentSAcc) - ds + 3.0);
+}
+// fractal_kirkwood_riseman, fractal.F90:223-231 (Naumann eq. 21)
+PMC_HD double kirkwood_riseman(const Fractal& F) {
+  return -0.06483 * (F.frac_dim * F.frac_dim) + 0.6353 * F.frac_dim - 0.4898;
+}
+// fractal_vol_to_mobility_rad_in_continuum, fractal.F90:239-249
+PMC_HD double mobility_rad_in_continuum(const Fractal& F, double v) { return kirkwood_riseman(F) * vol2rad(F, v); }
+// fractal_vol_to_effective_rad, fractal.F90:257-268 (Naumann eq. 28)
+PMC_HD double effective_rad(const Fractal& F, double v) {
+  return accessible_surface(F, v) / 4.0 / kPi / mobility_rad_in_continuum(F, v);
+}
+// fractal_slip_correct, fractal.F90:276-291, with the mean free path fp
+PMC_HD double slip_correct(double r_eff, double fp) {
+  return 1.0 + kFracASlip * fp / r_eff + kFracQSlip * fp / r_eff * exp(-kFracBSlip * r_eff / fp);
+}
+
+// fractal_vol_to_mobility_rad, fractal.F90:315-362: the mobility-equivalent
+// radius x solves C(R_eff) x^2 - R_mec x - R_mec Q fp exp(-B x / fp)
+// - R_mec A fp = 0 (Naumann eq. 30), by Newton's method from x = R_mec with
+// the reference's relative step tolerance 1e-14 and at most 10 steps.  fp is
+// air_mean_free_path(temp, pressure).  *ok is cleared where the reference
+// stops (no convergence before the 10th step, assert 728724732).
+PMC_HD double mobility_rad(const Fractal& F, double v, double fp, bool* ok) {
+  if (F.spherical) return vol2rad(F, v);
+  double rmec = mobility_rad_in_continuum(F, v);
+  double c_reff = slip_correct(effective_rad(F, v), fp);
+  double a1 = c_reff, a2 = -rmec, a3 = -rmec * kFracQSlip * fp, a4 = -kFracBSlip / fp;
+  double a5 = -rmec * kFracASlip * fp;
+  double x = rmec;
+  int step;
+  for (step = 1; step <= 10; step++) {
+    double e = exp(a4 * x);
+    double f = a1 * (x * x) + a2 * x + a3 * e + a5;
+    double df = 2.0 * a1 * x + a2 + a3 * a4 * e;
+    x = x - f / df;
+    if (fabs(f / df) / (fabs(x + f / df) + fabs(x)) < 1e-14) break;
+  }
+  if (!(step < 10)) *ok = false;
+  return x;
+}
+
 // interp_linear_disc, util.F90:663-683
 PMC_HD double interp_linear_disc(double x1, double xn, int n, int i) {
   if (x1 == xn) return x1;
@@ -135,14 +236,16 @@ PMC_HD bool weights_flat(const Weights& w) {
 
 // Air properties of kernel_brown_helper that depend only on the
 // environment, coag_kernel_brown.F90:143-151.
+// The particle shape (fractal_t) travels with the environment because every
+// kernel's per-particle terms need it; fp is util.F90's air mean free path
+// for the fractal mobility radius.
 struct BrownEnv {
   double temp, viscosd, gasfreepath;
-  // fractal_t (fractal.F90:56-63) for the free and continuum kernels;
-  // brown_env sets the spherical values of fractal_set_spherical
-  double frac_dim, prime_radius;
+  Fractal frac;
+  double fp;
 };
 
-PMC_HD BrownEnv brown_env(double temp, double pressure) {
+PMC_HD BrownEnv brown_env(double temp, double pressure, const Fractal& frac) {
   BrownEnv e;
   double rhoair = (pressure * kAirMolecWeight) / (kUnivGas * temp);
   e.viscosd = 1.8325e-05 * (416.16 / (temp + 120.0)) * pow(temp / 296.16, 1.5);
@@ -150,22 +253,23 @@ PMC_HD BrownEnv brown_env(double temp, double pressure) {
   double gasspeed = sqrt((8.0 * kBoltzmann * temp * kAvogadro) / (kPi * kAirMolecWeight));
   e.gasfreepath = 2.0 * viscosk / gasspeed;
   e.temp = temp;
-  e.frac_dim = 3.0;
-  e.prime_radius = 1e-8;
+  e.frac = frac;
+  e.fp = air_mean_free_path(temp, pressure);
   return e;
 }
 
-// The per-particle half of kernel_brown_helper, coag_kernel_brown.F90:163-189
-// (spherical particles: mobility radius = geometric radius).
+// The per-particle half of kernel_brown_helper, coag_kernel_brown.F90:163-189:
+// geometric radius and, for the diffusion terms, the mobility radius.
+// *ok is cleared if the fractal mobility radius does not converge.
 struct BrownPart {
   double rad, diffus, speedsq, deltasq;
 };
 
-PMC_HD BrownPart brown_part(const BrownEnv& e, double vol, double den) {
+PMC_HD BrownPart brown_part(const BrownEnv& e, double vol, double den, bool* ok) {
   BrownPart p;
   double temp = e.temp;
-  p.rad = vol2rad(vol);
-  double rme = vol2rad(vol);
+  p.rad = vol2rad(e.frac, vol);
+  double rme = mobility_rad(e.frac, vol, e.fp, ok);
   double knud = e.gasfreepath / rme;
   double cunning = 1.0 + knud * (1.249 + 0.42 * exp(-0.87 / knud));
   p.diffus = (kBoltzmann * temp * cunning) / (6.0 * kPi * rme * e.viscosd);
@@ -191,9 +295,9 @@ PMC_HD T brown_pair(T rad_i, T diffus_i, T speedsq_i, T deltasq_i, T rad_j, T di
 }
 
 // Full FP64 form in the reference's order, for k-bound tables and checks.
-PMC_HD double brown_kernel(const BrownEnv& e, double vi, double di, double vj, double dj) {
-  BrownPart a = brown_part(e, vi, di);
-  BrownPart b = brown_part(e, vj, dj);
+PMC_HD double brown_kernel(const BrownEnv& e, double vi, double di, double vj, double dj, bool* ok) {
+  BrownPart a = brown_part(e, vi, di, ok);
+  BrownPart b = brown_part(e, vj, dj, ok);
   double rad_sum = a.rad + b.rad;
   double diffus_sum = a.diffus + b.diffus;
   double tmp1 = rad_sum / (rad_sum + sqrt(a.deltasq + b.deltasq));
@@ -352,31 +456,31 @@ PMC_HD T sedi_pair(T r1, T w1, T r2, T w2) {
   return ec * T(kPi) * (rs * rs) * fabs(w1 - w2);
 }
 
-PMC_HD double sedi_kernel(double v1, double v2) {
-  double r1 = vol2rad(v1), r2 = vol2rad(v2);
-  return sedi_pair<double>(r1, fall_g(vol2rad(v1)), r2, fall_g(vol2rad(v2)));
+// kernel_sedi_helper, coag_kernel_sedi.F90:96-103: the collision
+// efficiency from the geometric radii, the fall speeds from the mobility radii
+PMC_HD double sedi_kernel(const BrownEnv& e, double v1, double v2, bool* ok) {
+  double r1 = vol2rad(e.frac, v1), r2 = vol2rad(e.frac, v2);
+  return sedi_pair<double>(r1, fall_g(mobility_rad(e.frac, v1, e.fp, ok)), r2,
+                           fall_g(mobility_rad(e.frac, v2, e.fp, ok)));
 }
 
-// fractal_vol_to_num_of_monomers (fractal.F90:84-100): N = (r / R0)^3
-PMC_HD double num_of_monomers(const BrownEnv& e, double v) {
-  double x = vol2rad(v) / e.prime_radius;
-  return x * x * x;
-}
-
-// kernel_brown_free_helper (coag_kernel_brown_free.F90): free molecular
-// regime, d1/d2 particle densities
+// kernel_brown_free_helper (coag_kernel_brown_free.F90:118-147): free
+// molecular regime, d1/d2 particle densities
 PMC_HD double brown_free_kernel(const BrownEnv& e, double v1, double d1, double v2, double d2) {
+  const Fractal& F = e.frac;
   double rho = (v1 / (v1 + v2)) * d1 + (v2 / (v1 + v2)) * d2;
-  double ni = num_of_monomers(e, v1), nj = num_of_monomers(e, v2);
-  double nif = pow(ni, 1.0 / e.frac_dim), njf = pow(nj, 1.0 / e.frac_dim);
+  double ni = num_of_monomers(F, v1), nj = num_of_monomers(F, v2);
+  double nif = pow(ni, 1.0 / F.frac_dim), njf = pow(nj, 1.0 / F.frac_dim);
   double s = nif + njf;
-  return sqrt(6.0 * kBoltzmann * e.temp * e.prime_radius / rho * (1.0 / ni + 1.0 / nj)) * (s * s);
+  return sqrt(6.0 * kBoltzmann * e.temp * F.prime_radius / rho * (1.0 / ni + 1.0 / nj)) * (s * s);
 }
 
-// kernel_brown_cont_helper (coag_kernel_brown_cont.F90): continuum regime
+// kernel_brown_cont_helper (coag_kernel_brown_cont.F90:115-144): continuum
+// regime
 PMC_HD double brown_cont_kernel(const BrownEnv& e, double v1, double v2) {
-  double nif = pow(num_of_monomers(e, v1), 1.0 / e.frac_dim);
-  double njf = pow(num_of_monomers(e, v2), 1.0 / e.frac_dim);
+  const Fractal& F = e.frac;
+  double nif = pow(num_of_monomers(F, v1), 1.0 / F.frac_dim);
+  double njf = pow(num_of_monomers(F, v2), 1.0 / F.frac_dim);
   return 2.0 * kBoltzmann * e.temp / 3.0 / kAirDynVisc * (1.0 / nif + 1.0 / njf) * (nif + njf);
 }
 
@@ -386,9 +490,10 @@ PMC_HD bool kernel_minmax(int kt, double v1, double v2, const BrownEnv& be, doub
                           double dmin, double dmax, double* kmin, double* kmax) {
   switch (kt) {
     case kKernelSedi: {
-      double k = sedi_kernel(v1, v2);
+      bool ok = true;
+      double k = sedi_kernel(be, v1, v2, &ok);
       *kmin = *kmax = k;
-      return k >= 0.0;
+      return k >= 0.0 && ok;
     }
     case kKernelAdditive: *kmin = *kmax = coeff * (v1 + v2); return true;
     case kKernelConstant: *kmin = *kmax = kBeta0; return true;
@@ -397,12 +502,12 @@ PMC_HD bool kernel_minmax(int kt, double v1, double v2, const BrownEnv& be, doub
     case kKernelBrownFree:
     case kKernelBrownCont: {
       // kernel_brown*_minmax: 3x3 density samples
-      bool first = true;
+      bool first = true, ok = true;
       for (int i = 1; i <= 3; i++)
         for (int j = 1; j <= 3; j++) {
           double d1 = interp_linear_disc(dmin, dmax, 3, i);
           double d2 = interp_linear_disc(dmin, dmax, 3, j);
-          double k = kt == kKernelBrown ? brown_kernel(be, v1, d1, v2, d2)
+          double k = kt == kKernelBrown ? brown_kernel(be, v1, d1, v2, d2, &ok)
                      : kt == kKernelBrownFree ? brown_free_kernel(be, v1, d1, v2, d2)
                                               : brown_cont_kernel(be, v1, v2);
           if (first) {
@@ -413,7 +518,7 @@ PMC_HD bool kernel_minmax(int kt, double v1, double v2, const BrownEnv& be, doub
             if (k > *kmax) *kmax = k;
           }
         }
-      return true;
+      return ok;
     }
   }
   return false;
@@ -424,8 +529,8 @@ PMC_HD bool kernel_minmax(int kt, double v1, double v2, const BrownEnv& be, doub
 PMC_HD bool kminmax_for_bin(int kt, const double* edges, int b1, int b2, const BrownEnv& be,
                             double coeff, double dmin, double dmax, double* kmin,
                             double* kmax) {
-  double v1lo = rad2vol(edges[b1]), v1hi = rad2vol(edges[b1 + 1]);
-  double v2lo = rad2vol(edges[b2]), v2hi = rad2vol(edges[b2 + 1]);
+  double v1lo = rad2vol(be.frac, edges[b1]), v1hi = rad2vol(be.frac, edges[b1 + 1]);
+  double v2lo = rad2vol(be.frac, edges[b2]), v2hi = rad2vol(be.frac, edges[b2 + 1]);
   bool ok = true;
   for (int i = 1; i <= 3; i++)
     for (int j = 1; j <= 3; j++) {
@@ -446,8 +551,8 @@ PMC_HD bool kminmax_for_bin(int kt, const double* edges, int b1, int b2, const B
 }
 
 // coag_num_conc_factor, coag_kernel.F90:346-377 (classes 0-based)
-PMC_HD double num_conc_factor(const Weights& w, double ri, double rj, int ci, int cj, int cij) {
-  double rij = vol2rad(rad2vol(ri) + rad2vol(rj));
+PMC_HD double num_conc_factor(const Weights& w, const Fractal& F, double ri, double rj, int ci, int cj, int cij) {
+  double rij = vol2rad(F, rad2vol(F, ri) + rad2vol(F, rj));
   double nci = num_conc_at_radius<double>(w, ci, ri);
   double ncj = num_conc_at_radius<double>(w, cj, rj);
   double ncij = num_conc_at_radius<double>(w, cij, rij);
@@ -459,11 +564,11 @@ PMC_HD double num_conc_factor(const Weights& w, double ri, double rj, int ci, in
 
 // coag_dest_class, coag_kernel.F90:382-416, including the reference's use of
 // centers(i_bin) for both radii (lines 402-403).  Bins/classes 0-based.
-PMC_HD int coag_dest_class(const Weights& w, const double* centers, int b1, int b2, int c1,
+PMC_HD int coag_dest_class(const Weights& w, const Fractal& F, const double* centers, int b1, int b2, int c1,
                            int c2) {
   double ri = centers[b1];
   double rj = centers[b1];
-  double rij = vol2rad(rad2vol(ri) + rad2vol(rj));
+  double rij = vol2rad(F, rad2vol(F, ri) + rad2vol(F, rj));
   double nci = num_conc_at_radius<double>(w, c1, rij);
   double ncj = num_conc_at_radius<double>(w, c2, rij);
   (void)b2;
@@ -471,7 +576,7 @@ PMC_HD int coag_dest_class(const Weights& w, const double* centers, int b1, int 
 }
 
 // max_coag_num_conc_factor, coag_kernel.F90:422-465 (5x5 radius samples)
-PMC_HD double max_num_conc_factor(const Weights& w, const double* edges, int b1, int b2, int c1,
+PMC_HD double max_num_conc_factor(const Weights& w, const Fractal& F, const double* edges, int b1, int b2, int c1,
                                   int c2, int cc) {
   double i0 = edges[b1], i1 = edges[b1 + 1], j0 = edges[b2], j1 = edges[b2 + 1];
   double fmax = 0.0;
@@ -479,7 +584,7 @@ PMC_HD double max_num_conc_factor(const Weights& w, const double* edges, int b1,
     for (int b = 1; b <= 5; b++) {
       double ri = interp_linear_disc(i0, i1, 5, a);
       double rj = interp_linear_disc(j0, j1, 5, b);
-      double f = num_conc_factor(w, ri, rj, c1, c2, cc);
+      double f = num_conc_factor(w, F, ri, rj, c1, c2, cc);
       if (f > fmax) fmax = f;
     }
   return fmax;

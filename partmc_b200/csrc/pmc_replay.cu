@@ -49,7 +49,7 @@ struct Seq {
 
   // ---- particle slots (aero_particle_array, aero_particle_array.F90:158-198)
   __device__ double vtot(int i) { return P->vtot[i - 1]; }
-  __device__ double radius(int i) { return vol2rad(P->vtot[i - 1]); }
+  __device__ double radius(int i) { return vol2rad(P->benv.frac, P->vtot[i - 1]); }
   __device__ void load(int i, Tp& t) {
     for (int s = 0; s < P->n_spec; s++) t.vol[s] = P->vol[vol_at(*P, i - 1, s)];
     load_meta(*P, i - 1, t.m);
@@ -180,7 +180,7 @@ struct Seq {
   __device__ bool state_add(const Tp& t) {
     double vt = 0.0;
     for (int s = 0; s < P->n_spec; s++) vt = vt + t.vol[s];
-    int b = in_bin(vol2rad(vt));
+    int b = in_bin(vol2rad(P->benv.frac, vt));
     if (t.m.grp < 1 || t.m.grp > P->n_group || t.m.cls < 1 || t.m.cls > P->n_class) return fail(kErrAssert);
     if (!array_add(t)) return false;
     if (b < 1 || b > nb) return fail(kErrOutOfGrid);
@@ -224,9 +224,10 @@ struct Seq {
       v2 = v2 + vb[s];
     }
     double kk = 0.0;
+    bool ok = true;
     switch (P->kernel_type) {
       case kKernelSedi:
-        kk = sedi_kernel(v1, v2);
+        kk = sedi_kernel(P->benv, v1, v2, &ok);
         if (kk < 0.0) return fail(kErrAssert);
         break;
       case kKernelAdditive: kk = P->coeff * (v1 + v2); break;
@@ -236,7 +237,7 @@ struct Seq {
           m1 = m1 + va[s] * P->density[s];
           m2 = m2 + vb[s] * P->density[s];
         }
-        kk = brown_kernel(P->benv, v1, m1 / v1, v2, m2 / v2);
+        kk = brown_kernel(P->benv, v1, m1 / v1, v2, m2 / v2, &ok);
         break;
       case kKernelBrownFree:
         for (int s = 0; s < P->n_spec; s++) {
@@ -248,8 +249,10 @@ struct Seq {
       case kKernelBrownCont: kk = brown_cont_kernel(P->benv, v1, v2); break;
       default: kk = 0.0;
     }
-    double ri = vol2rad(v1), rj = vol2rad(v2);
-    *k = kk * num_conc_factor(P->w, ri, rj, ci - 1, cj - 1, cij - 1);
+    if (!ok) return fail(kErrAssert);  // the fractal Newton loop did not converge
+    const Fractal& F = P->benv.frac;
+    double ri = vol2rad(F, v1), rj = vol2rad(F, v2);
+    *k = kk * num_conc_factor(P->w, F, ri, rj, ci - 1, cj - 1, cij - 1);
     return true;
   }
   __device__ void slot_vol(int i, double* v) {
@@ -260,7 +263,7 @@ struct Seq {
   __device__ bool coagulate(int p1, int p2, int c1, int c2, int cc) {
     if (P->id[p1 - 1] == P->id[p2 - 1]) return fail(kErrAssert);
     double r1 = radius(p1), r2 = radius(p2);
-    double rc = vol2rad(rad2vol(r1) + rad2vol(r2));
+    double rc = vol2rad(P->benv.frac, rad2vol(P->benv.frac, r1) + rad2vol(P->benv.frac, r2));
     double nc1 = num_conc_at_radius<double>(P->w, c1 - 1, r1);
     double nc2 = num_conc_at_radius<double>(P->w, c2 - 1, r2);
     double ncc = num_conc_at_radius<double>(P->w, cc - 1, rc);
@@ -377,7 +380,7 @@ struct Seq {
     double vt = 0.0;
     for (int s = 0; s < ns; s++) vt = vt + target.vol[s];
     int ct = target.m.cls;
-    double nc_target = num_conc_at_radius<double>(P->w, ct - 1, vol2rad(vt));
+    double nc_target = num_conc_at_radius<double>(P->w, ct - 1, vol2rad(P->benv.frac, vt));
     double nc_src_min = num_conc_at_radius<double>(P->w, cs - 1, G->edges[bs - 1]);
     double prm_max = nc_target / nc_src_min;
     if (!(prm_max <= 1.0)) return fail(kErrAssert);
@@ -514,7 +517,7 @@ struct Seq {
     t.m = nm;
     double vt = 0.0;
     for (int s = 0; s < P->n_spec; s++) vt = vt + t.vol[s];
-    int grp = rand_group(g, P->w, cc - 1, vol2rad(vt));
+    int grp = rand_group(g, P->w, cc - 1, vol2rad(P->benv.frac, vt));
     if (!rng_ok()) return false;
     if (grp == 0) return fail(kErrTimeout);
     t.m.grp = grp;
@@ -556,8 +559,8 @@ struct Seq {
     double nspt = k_max * P->del_t * (double)cn(bs, cs);
     double af = 1.0 / k_max;
     if (nspt < 1.0) return true;
-    double min_tv = rad2vol(G->edges[bt - 1]);
-    double max_sv = rad2vol(G->edges[bs]);
+    double min_tv = rad2vol(P->benv.frac, G->edges[bt - 1]);
+    double max_sv = rad2vol(P->benv.frac, G->edges[bs]);
     double max_new = min_tv + max_sv * nspt;
     if (max_new / min_tv > 1.5) return true;
     for (int e = cn(bt, ct); e >= 1; e--) {
@@ -584,8 +587,9 @@ struct Seq {
           int b2s = c1 == c2 ? b1 : 1;
           for (int b2 = b2s; b2 <= nb; b2++) {
             if (cn(b2, c2) == 0) continue;
-            int cc = coag_dest_class(P->w, G->centers, b1 - 1, b2 - 1, c1 - 1, c2 - 1) + 1;
-            double f_max = max_num_conc_factor(P->w, G->edges, b1 - 1, b2 - 1, c1 - 1, c2 - 1, cc - 1);
+            int cc = coag_dest_class(P->w, P->benv.frac, G->centers, b1 - 1, b2 - 1, c1 - 1, c2 - 1) + 1;
+            double f_max =
+                max_num_conc_factor(P->w, P->benv.frac, G->edges, b1 - 1, b2 - 1, c1 - 1, c2 - 1, cc - 1);
             double k_max = P->kmax_tab[(b1 - 1) + nb * (b2 - 1)] * f_max;
             bool done;
             if (!try_per_particle(k_max, b1, b2, c1, c2, cc, &done)) return false;

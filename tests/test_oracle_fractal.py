@@ -68,3 +68,49 @@ def test_surface_fractal_dimension():
     assert F.surface_frac_dim(F.Fractal(2.4)) == pytest.approx(2.5)
     with pytest.raises(ValueError):
         F.surface_frac_dim(F.Fractal(3.2))
+
+
+def test_c_oracle_radii_match_the_pinned_restatement():
+    """The C oracle's fractal_vol2rad and fractal_vol_to_mobility_rad (the
+    checker of the device path) against oracle/fractal.py, which the
+    reference's radii round trips pin, over the reference test's grid."""
+    from oracle import oracle as O
+    worst = 0.0
+    for r0 in (1e-10, 1e-9, 1e-8, 1e-7):
+        for f in (1.0, 1.43):
+            for df in (1.8, 2.0, 2.4, 2.8, 3.0):
+                fr = F.Fractal(df, r0, f)
+                for r in F.logspace(r0, r0 * 1e3, 25):
+                    v = F.rad2vol(fr, r)
+                    rg, rme = O.fractal_radius(v, df, r0, f, TEMP, PRESSURE)
+                    worst = max(worst, abs(rg / F.vol2rad(fr, v) - 1),
+                                abs(rme / F.vol_to_mobility_rad(fr, v, TEMP, PRESSURE) - 1))
+    assert worst < 1e-12, worst
+
+
+def test_c_oracle_fractal_kernels():
+    """Free-molecular and continuum kernels of clusters (d_f 2.4 and 1.8, the
+    shapes of test/fractal) against their formulas written out here, and the
+    Brownian and sedimentation kernels reduce to the spherical ones at
+    d_f = 3."""
+    from oracle import oracle as O
+    kB, visc = 1.3806505e-23, 1.78e-5
+    for df, r0, temp in ((2.4, 5e-10, 1800.0), (1.8, 2.5e-7, 300.0)):
+        v0 = 4.0 / 3.0 * math.pi * r0 ** 3
+        for n1, n2 in ((1.0, 1.0), (7.0, 300.0), (2e4, 5e5)):
+            v1, v2 = n1 * v0, n2 * v0
+            free = O.kernel_value_fractal(O.KERNEL_BROWN_FREE, v1, 4200.0, v2, 4200.0, df, r0, 1.0, temp)
+            want = math.sqrt(6 * kB * temp * r0 / 4200.0 * (1 / n1 + 1 / n2)) * (n1 ** (1 / df) + n2 ** (1 / df)) ** 2
+            assert free == pytest.approx(want, rel=1e-12)
+            cont = O.kernel_value_fractal(O.KERNEL_BROWN_CONT, v1, 4200.0, v2, 4200.0, df, r0, 1.0, temp)
+            a, b = n1 ** (1 / df), n2 ** (1 / df)
+            assert cont == pytest.approx(2 * kB * temp / 3 / visc * (1 / a + 1 / b) * (a + b), rel=1e-12)
+    for kt in (O.KERNEL_BROWN, O.KERNEL_SEDI):
+        v1, v2 = (1e-24, 3e-22) if kt == O.KERNEL_BROWN else (4e-15, 3e-14)
+        assert O.kernel_value_fractal(kt, v1, 1500.0, v2, 1500.0, 3.0, 1e-8) == O.kernel_value(kt, v1, 1500.0, v2,
+                                                                                                1500.0)
+    # the cluster shape reaches the transition-regime kernel (through the
+    # geometric and mobility radii)
+    k_sph = O.kernel_value(O.KERNEL_BROWN, 1e-24, 1500.0, 3e-22, 1500.0)
+    k_frac = O.kernel_value_fractal(O.KERNEL_BROWN, 1e-24, 1500.0, 3e-22, 1500.0, 1.8, 1e-9)
+    assert k_frac != k_sph and math.isfinite(k_frac)
