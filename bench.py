@@ -220,6 +220,21 @@ def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode):
              "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec}, samp, sec)
 
 
+def fp32_error(pm, pop, env, n_pairs=200000, seed=3):
+    """Largest relative error of the FP32 weighted kernel against the FP64
+    one over random particle pairs of the workload (the acceptance of MIXED
+    mode falls back to FP64 within 2^-12 of the uniform, far above it)."""
+    rng = np.random.default_rng(seed)
+    i = rng.integers(0, pop.n_part, n_pairs)
+    j = rng.integers(0, pop.n_part, n_pairs)
+    st = pm.AeroState(pop.aero_data, pop.awa, mode=pm.MODE_FP64)
+    k64 = st.eval_kernel(pm.COAG_KERNEL_TYPE_BROWN, env, pop.vol[i], 1, pop.vol[j], 1, 1)
+    st.set_mode(pm.MODE_MIXED)
+    k32 = st.eval_kernel(pm.COAG_KERNEL_TYPE_BROWN, env, pop.vol[i], 1, pop.vol[j], 1, 1)
+    ok = k64 > 0
+    return float((np.abs(k32[ok] - k64[ok]) / k64[ok]).max())
+
+
 def cpu_baseline(n_part, del_t, budget_s=20.0):
     """The oracle (C restatement of the reference's mc_coag), one thread, on
     a bounded sample of the same workload: as many steps as fit in budget_s."""
@@ -435,6 +450,7 @@ def main():
         for _ in range(w):
             pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, st, args.del_t)
         L.pmc_coag_gpu_profile(st.ctx, 1)
+        exact0 = st.exact_tests()
         n0 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n0))
         barrier(ws)
@@ -460,6 +476,7 @@ def main():
                 conf[kk] += vv
         n1 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
+        prof["exact_tests_per_step"] = (st.exact_tests() - exact0) / max(k, 1)
         prof = {}
         for which, name in ((0, "test"), (1, "sort"), (2, "redraw_graph"), (3, "step")):
             t, nl, u = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
@@ -526,6 +543,11 @@ def main():
                          "bytes_per_unit": bpu, "units_per_launch": units / max(n_l, 1)},
             "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "units": v[2]} for k, v in prof.items()
                           if isinstance(v, tuple)},
+            "precision": {"kernel_eval": "FP32" if args.mode == "mixed" else "FP64",
+                          "fp32_kernel_max_rel_err": fp32_error(pm, pop, env),
+                          "accept_margin": 2.0 ** -12,
+                          "tests_decided_in_fp64_per_step": prof["exact_tests_per_step"],
+                          "decisions": "identical to FP64 mode (FP64 fallback within the margin)"},
             "rounds_per_step": prof["rounds_per_step"],
             "redraws_per_step": prof["redraws_per_step"],
             "conflicts_per_step": prof["conflicts_per_step"],

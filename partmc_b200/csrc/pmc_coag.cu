@@ -14,6 +14,9 @@
 #include <memory>
 #include <string>
 #include <vector>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <type_traits>
 
@@ -394,24 +397,41 @@ __global__ void k_download(PopDev P, const long long* live_off, int n_slots, dou
   }
 }
 
-// the slots written since the last host sync, compacted in slot order
-// (off: exclusive scan of changed over the slots); their flags are cleared
-__global__ void k_gather_changed(PopDev P, const long long* off, int n_range, int* slot, int* alive, double* vol,
-                                 int* grp, int* cls, long long* id, int* nprim) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_range; i += gridDim.x * blockDim.x) {
-    if (!P.changed[i]) continue;
-    long long j = off[i];
-    slot[j] = i;
-    int a = P.alive[i];
-    alive[j] = a;
-    if (a) {
-      for (int s = 0; s < P.n_spec; s++) vol[j * P.n_spec + s] = P.vol[vol_at(P, i, s)];
-      grp[j] = P.grp[i];
-      cls[j] = P.cls[i];
-      id[j] = P.id[i];
-      nprim[j] = P.nprim[i];
+// Changed slots of [0, n_range) packed for the host copy, one record of
+// kSyncHead + 8 n_spec bytes each: {slot, alive, group, class, n_primary,
+// 0, id (8 bytes)} then the species volumes.  Each warp takes 32 slots,
+// reserves places for its changed ones with one atomic, and copies each
+// changed slot's volumes with one lane per species (coalesced); record order
+// is arbitrary (the host scatters by slot).  Clears the changed flags.
+constexpr int kSyncHead = 32;
+__global__ void k_pack_changed(PopDev P, int n_range, unsigned long long* count, unsigned char* out,
+                               int rec_bytes) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n_range; base += warps * 32) {
+    const int i = base + lane;
+    const bool ch = i < n_range && P.changed[i];
+    const unsigned m = __ballot_sync(0xffffffffu, ch);
+    if (!m) continue;
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(count, (unsigned long long)__popc(m));
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (ch) {
+      unsigned char* r = out + (size_t)(b + __popc(m & ((1u << lane) - 1u))) * rec_bytes;
+      const int a = P.alive[i];
+      int4 h = make_int4(i, a, a ? P.grp[i] : 0, a ? P.cls[i] : 0);
+      *(int4*)r = h;
+      *(int2*)(r + 16) = make_int2(a ? P.nprim[i] : 0, 0);
+      *(long long*)(r + 24) = a ? P.id[i] : 0;
+      P.changed[i] = 0;
     }
-    P.changed[i] = 0;
+    for (unsigned mm = m; mm; mm &= mm - 1) {
+      const int src = __ffs(mm) - 1;
+      const int si = base + src;
+      if (!P.alive[si]) continue;
+      double* v = (double*)(out + (size_t)(b + __popc(m & ((1u << src) - 1u))) * rec_bytes + kSyncHead);
+      for (int sp = lane; sp < P.n_spec; sp += 32) v[sp] = P.vol[vol_at(P, si, sp)];
+    }
   }
 }
 
@@ -690,6 +710,70 @@ struct PinnedBuf {
   }
 };
 
+// Persistent host workers for the scatter of pmc_coag_gpu_sync_host: run(n,
+// f) calls f(q, n) for q = 0..n-1 on n threads (the caller's among them) and
+// returns when all are done.
+class HostPool {
+ public:
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  void run(int n, const std::function<void(int, int)>& f) {
+    if (n <= 1) {
+      f(0, 1);
+      return;
+    }
+    while ((int)th_.size() < n - 1) {
+      int q = (int)th_.size() + 1;
+      th_.emplace_back([this, q] { loop(q); });
+    }
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      job_ = &f;
+      n_ = n;
+      left_ = n - 1;
+      gen_++;
+    }
+    cv_.notify_all();
+    f(0, n);
+    std::unique_lock<std::mutex> l(mu_);
+    done_.wait(l, [this] { return left_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void loop(int q) {
+    unsigned long long seen = 0;
+    for (;;) {
+      const std::function<void(int, int)>* f;
+      int n;
+      {
+        std::unique_lock<std::mutex> l(mu_);
+        cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        f = job_;
+        n = n_;
+      }
+      if (q < n) (*f)(q, n);
+      std::lock_guard<std::mutex> l(mu_);
+      if (q < n && --left_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int, int)>* job_ = nullptr;
+  int n_ = 0, left_ = 0;
+  unsigned long long gen_ = 0;
+  bool stop_ = false;
+};
+
 struct PopHost {
   PopDev h{};
   bool valid_sort = false;
@@ -795,6 +879,10 @@ struct Ctx {
   DevBuf<int> st_i;
   DevBuf<long long> st_l;
   PinnedBuf pin;  // host staging of the changed slots
+  DevBuf<unsigned char> st_rec;             // packed changed slots (k_pack_changed)
+  DevBuf<unsigned long long> st_cnt;        // their count
+  long long sync_guess = 0;                 // records copied with the count (the last sync's count)
+  std::unique_ptr<HostPool> pool;           // scatter workers
   long long h_total = 0;
   // stats of the last step
   long long last_redraws = 0, last_rounds = 0, last_kmax_warn = 0, exact_tests = 0;
@@ -2477,6 +2565,8 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.st_d.release();
   c.st_i.release();
   c.st_l.release();
+  c.st_rec.release();
+  c.st_cnt.release();
   c.pin.release();
   replay_free(c.replay);
   free_redraw_graph(c);
@@ -2910,61 +3000,55 @@ int pmc_coag_gpu_sync_host(pmc_coag_gpu_ctx* x, int pop, int cap, double* vol, i
   }
   int range = std::max(ph.mirror_slots, r.n_slots);
   if (range > ph.h.cap) range = ph.h.cap;
-  size_t t = (size_t)std::max(range, 1);  // room for every slot of the range
-  c.st_l.reserve(2 * t + 2);
-  c.st_d.reserve(t * ns);
-  c.st_i.reserve(5 * t);
-  long long total = range > 0 ? scan(c, ph.h.changed, range, c.st_l.p, true) : 0;
+  long long total = 0;
   if (range > 0) {
-    int* d_slot = c.st_i.p;
-    int* d_alive = d_slot + t;
-    int* d_grp = d_alive + t;
-    int* d_cls = d_grp + t;
-    int* d_np = d_cls + t;
-    long long* d_id = c.st_l.p + range + 1;
-    k_gather_changed<<<grid_for(range, 256), 256, 0, c.stream>>>(ph.h, c.st_l.p, range, d_slot, d_alive, c.st_d.p,
-                                                                d_grp, d_cls, d_id, d_np);
+    // pack the changed slots into records on the device (one kernel), then
+    // copy the count together with as many records as the last sync had
+    // (one stream sync when the guess holds), the rest if it did not
+    const int rec = kSyncHead + 8 * ns;
+    c.st_rec.reserve((size_t)range * rec);
+    c.st_cnt.reserve(1);
+    CK(cudaMemsetAsync(c.st_cnt.p, 0, sizeof(unsigned long long), c.stream));
+    k_pack_changed<<<grid_for(range, 256), 256, 0, c.stream>>>(ph.h, range, c.st_cnt.p, c.st_rec.p, rec);
     note_launch();
-    size_t tt = (size_t)std::max<long long>(total, 1);
-    size_t rec = sizeof(double) * ns + 5 * sizeof(int) + sizeof(long long);
-    c.pin.reserve(rec * tt);
-    double* h_vol = (double*)c.pin.p;
-    long long* h_id = (long long*)(h_vol + tt * ns);
-    int* h_i = (int*)(h_id + tt);
-    if (total > 0) {
-      CK(cudaMemcpyAsync(h_vol, c.st_d.p, sizeof(double) * total * ns, cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaMemcpyAsync(h_id, d_id, sizeof(long long) * total, cudaMemcpyDeviceToHost, c.stream));
-      for (int f = 0; f < 5; f++)
-        CK(cudaMemcpyAsync(h_i + (size_t)f * tt, c.st_i.p + (size_t)f * t, sizeof(int) * total,
-                           cudaMemcpyDeviceToHost, c.stream));
-    }
+    long long guess = std::min<long long>(range, c.sync_guess + c.sync_guess / 8 + 256);
+    c.pin.reserve(64 + (size_t)std::max<long long>(guess, 1) * rec);
+    unsigned long long* h_cnt = (unsigned long long*)c.pin.p;
+    unsigned char* h_rec = (unsigned char*)c.pin.p + 64;
+    CK(cudaMemcpyAsync(h_cnt, c.st_cnt.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(h_rec, c.st_rec.p, (size_t)guess * rec, cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    total = (long long)*h_cnt;
+    if (total > guess) {
+      std::vector<unsigned char> keep((size_t)guess * rec);
+      memcpy(keep.data(), h_rec, keep.size());
+      c.pin.reserve(64 + (size_t)total * rec);
+      h_rec = (unsigned char*)c.pin.p + 64;
+      memcpy(h_rec, keep.data(), keep.size());
+      CK(cudaMemcpyAsync(h_rec + (size_t)guess * rec, c.st_rec.p + (size_t)guess * rec,
+                         (size_t)(total - guess) * rec, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+    }
+    c.sync_guess = total;
     // scatter into the caller's slot-indexed arrays
-    const int* h_slot = h_i;
-    const int* h_alive = h_i + tt;
-    const int* h_grp = h_i + 2 * tt;
-    const int* h_cls = h_i + 3 * tt;
-    const int* h_np = h_i + 4 * tt;
-    auto work = [&](long long j0, long long j1) {
-      for (long long j = j0; j < j1; j++) {
-        int sl = h_slot[j];
-        alive[sl] = (uint8_t)h_alive[j];
-        if (!h_alive[j]) continue;
-        memcpy(vol + (size_t)sl * ns, h_vol + (size_t)j * ns, sizeof(double) * ns);
-        group[sl] = h_grp[j];
-        cls[sl] = h_cls[j];
-        id[sl] = h_id[j];
-        n_primary[sl] = h_np[j];
+    const std::function<void(int, int)> work = [&](int q, int nq) {
+      const long long j1 = total * (q + 1) / nq;
+      for (long long j = total * q / nq; j < j1; j++) {
+        const unsigned char* e = h_rec + (size_t)j * rec;
+        const int* hd = (const int*)e;
+        const int sl = hd[0];
+        alive[sl] = (uint8_t)hd[1];
+        if (!hd[1]) continue;
+        group[sl] = hd[2];
+        cls[sl] = hd[3];
+        n_primary[sl] = hd[4];
+        memcpy(&id[sl], e + 24, sizeof(long long));
+        memcpy(vol + (size_t)sl * ns, e + kSyncHead, sizeof(double) * ns);
       }
     };
-    int n_thr = total > 32768 ? (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency())) : 1;
-    if (n_thr <= 1) {
-      work(0, total);
-    } else {
-      std::vector<std::thread> th;
-      for (int q = 0; q < n_thr; q++) th.emplace_back(work, total * q / n_thr, total * (q + 1) / n_thr);
-      for (auto& w : th) w.join();
-    }
+    int n_thr = total > 16384 ? (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (!c.pool) c.pool.reset(new HostPool());
+    c.pool->run(n_thr, work);
   }
   ph.mirror_slots = r.n_slots;
   if (n_changed) *n_changed = (int)total;

@@ -9,7 +9,8 @@ reproduce the FP64 run particle for particle.  These tests check that on the
 benchmark's workload classes and record the FP32 kernel error per workload:
   - 20 species with nummass weights, Brownian, 60 s steps (the 1e6-particle
     benchmark workload, in miniature);
-  - the bimodal Brownian population with power weights (alpha = -1), 60 s;
+  - the bimodal Brownian population with power weights (alpha = -1), 600 s
+    steps (enough tests at 1e5 particles for the FP64 fallback to occur);
   - the additive kernel with flat weights at test/additive's 1 s steps;
   - the sedimentation kernel with flat weights at test/sedi's 5 s steps."""
 import numpy as np
@@ -28,8 +29,8 @@ def workloads():
     return {
         "brown_20spec_nummass": (aero_dist.brown_20spec(20000, seed=11), pm.COAG_KERNEL_TYPE_BROWN,
                                  pm.EnvState(288.0, 1e5), 60.0, 6),
-        "brown_bimodal_power": (aero_dist.brown_bimodal(20000, seed=12), pm.COAG_KERNEL_TYPE_BROWN,
-                                pm.EnvState(288.0, 1e5), 60.0, 10),
+        "brown_bimodal_power": (aero_dist.brown_bimodal(100000, seed=12), pm.COAG_KERNEL_TYPE_BROWN,
+                                pm.EnvState(288.0, 1e5), 600.0, 10),
         "additive_flat": (aero_dist.additive_exp(10000, seed=13), pm.COAG_KERNEL_TYPE_ADDITIVE,
                           pm.EnvState(288.0, 1e5, 1000.0), 1.0, 20),
         "sedi_flat": (sedi, pm.COAG_KERNEL_TYPE_SEDI, pm.EnvState(288.0, 1e5), 5.0, 12),
