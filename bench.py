@@ -476,13 +476,14 @@ def main():
                 conf[kk] += vv
         n1 = ctypes.c_int64()
         L.pmc_coag_gpu_launch_count(ctypes.byref(n1))
-        prof["exact_tests_per_step"] = (st.exact_tests() - exact0) / max(k, 1)
+        exact1 = st.exact_tests()
         prof = {}
         for which, name in ((0, "test"), (1, "sort"), (2, "redraw_graph"), (3, "step")):
             t, nl, u = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
             L.pmc_coag_gpu_profile_read(st.ctx, which, ctypes.byref(t), ctypes.byref(nl), ctypes.byref(u))
             prof[name] = (t.value, nl.value, u.value)
         L.pmc_coag_gpu_profile(st.ctx, 0)
+        prof["exact_tests_per_step"] = (exact1 - exact0) / max(k, 1)
         prof["rounds_per_step"] = rounds / max(k, 1)
         prof["redraws_per_step"] = redraws / max(k, 1)
         prof["conflicts_per_step"] = {kk: vv / max(k, 1) for kk, vv in conf.items()}

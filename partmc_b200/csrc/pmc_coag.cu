@@ -398,8 +398,9 @@ __global__ void k_download(PopDev P, const long long* live_off, int n_slots, dou
 }
 
 // Changed slots of [0, n_range) packed for the host copy, one record of
-// kSyncHead + 8 n_spec bytes each: {slot, alive, group, class, n_primary,
-// 0, id (8 bytes)} then the species volumes.  Each warp takes 32 slots,
+// rec_bytes = kSyncHead + 8 n_spec bytes rounded up to a multiple of 16 (the
+// header is stored as one 16-byte vector): {slot, alive, group, class,
+// n_primary, 0, id (8 bytes)} then the species volumes.  Each warp takes 32 slots,
 // reserves places for its changed ones with one atomic, and copies each
 // changed slot's volumes with one lane per species (coalesced); record order
 // is arbitrary (the host scatters by slot).  Clears the changed flags.
@@ -1254,6 +1255,9 @@ void set_params(Ctx& c, PopHost& ph) {
   h.dmax = *std::max_element(c.density.begin(), c.density.end());
   h.seed = ph.seed;
   h.pair_setup_valid = 0;  // the per-pair weight factors depend on the weights
+  // radii follow the particle shape from the first sort on, before any step
+  // sets the environment
+  h.benv.frac = c.frac;
   c.dirty = true;
 }
 
@@ -3005,7 +3009,7 @@ int pmc_coag_gpu_sync_host(pmc_coag_gpu_ctx* x, int pop, int cap, double* vol, i
     // pack the changed slots into records on the device (one kernel), then
     // copy the count together with as many records as the last sync had
     // (one stream sync when the guess holds), the rest if it did not
-    const int rec = kSyncHead + 8 * ns;
+    const int rec = (kSyncHead + 8 * ns + 15) & ~15;  // keeps every record's header 16-byte aligned
     c.st_rec.reserve((size_t)range * rec);
     c.st_cnt.reserve(1);
     CK(cudaMemsetAsync(c.st_cnt.p, 0, sizeof(unsigned long long), c.stream));

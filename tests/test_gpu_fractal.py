@@ -3,8 +3,9 @@
 1. Static parity with the oracle under three particle shapes: the kernel
    values of every kernel (FP64, 1e-12 relative; the Brownian and
    sedimentation kernels through the fractal mobility radius of
-   fractal.F90:315-362), the bin grid and every particle's bin (bit-exact,
-   radii from fractal_vol2rad), and the k_max table (1e-12).
+   fractal.F90:315-362), every particle's bin and the bin counts (exact,
+   radii from fractal_vol2rad; the grid edges to 1e-14), and the k_max
+   table (1e-12).
 2. The reference's own test/fractal cases (test_fractal_2.sh, _3.sh): the
    device runs both through the package API and must meet the reference's
    criterion against the reference's golden vectors, numeric_diff --by col
@@ -79,7 +80,10 @@ def test_fractal_bins_bit_exact(gpu_lib, shape):
     orc = oracle_for(pop, shape)
     orc.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
     orc.sort()
-    assert np.array_equal(edges, orc.bin_edges())
+    # the grid comes from the extreme radii, which the device computes with
+    # CUDA's pow and the oracle with the C library's: the edges may differ in
+    # the last bit; counts and bins are exact
+    assert np.allclose(edges, orc.bin_edges(), rtol=1e-14, atol=0.0)
     assert np.array_equal(counts, orc.bin_counts())
     assert np.array_equal(bins, orc.particle_bins())
     # the grid spans the fractal radii, not the spheres' (d_f < 3 spreads them)
@@ -102,7 +106,11 @@ def test_fractal_kmax_table(gpu_lib, shape, kt):
     orc.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group))
     orc.sort()
     _, k_cpu = orc.kmax_table(kt, ENV.temp, ENV.pressure, ENV.additive_kernel_coefficient)
-    rel = np.abs(k_gpu - k_cpu) / np.abs(k_cpu)
+    # clusters whose mobility radius exceeds 3.5 mm all fall at the capped
+    # terminal speed (fall_g), so their sedimentation kernel is 0 in both
+    nz = k_cpu != 0
+    assert np.array_equal(k_gpu[~nz], k_cpu[~nz])
+    rel = np.abs(k_gpu[nz] - k_cpu[nz]) / np.abs(k_cpu[nz])
     assert rel.max() < 1e-12, rel.max()
 
 
