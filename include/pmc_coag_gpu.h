@@ -240,6 +240,26 @@ int pmc_coag_gpu_replay_used(pmc_coag_gpu_ctx *ctx, int64_t *n_used);
 int pmc_coag_gpu_stats(pmc_coag_gpu_ctx *ctx, int64_t *kmax_violations,
                        int64_t *redraws, int64_t *rounds);
 
+/* Removal records (aero_state%aero_info_array, aero_info.F90:48-56), the
+ * output run_part writes when record_removals is set (run_part.F90:745,
+ * 995-1001).  After pmc_coag_gpu_set_record_removals(ctx, 1) every
+ * population logs each particle it removes, on the device: coagulation
+ * removals whose ID is lost (coagulate, coagulation.F90:928-985; other_id =
+ * the ID of the particle the coagulation made, or 0), the sources a
+ * per-particle coagulation removes (coagulation.F90:447-453; other_id = the
+ * target's ID), weight removals (aero_state_dup_particle,
+ * aero_state.F90:502-513) and halving removals (aero_state_halve,
+ * aero_state.F90:1753-1785).  pmc_coag_gpu_removals copies population
+ * pop's records into id/action/other_id (action: 2 coagulation, 3 halved, 4
+ * weight) and clears them, as run_part does after an output
+ * (aero_info_array_zero).  *n gets the record count; if it exceeds max_n the
+ * call returns PMC_ERR_CAPACITY and copies and clears nothing.  Records come
+ * in removal order in replay mode and in no particular order otherwise. */
+int pmc_coag_gpu_set_record_removals(pmc_coag_gpu_ctx *ctx, int enable);
+int pmc_coag_gpu_removals(pmc_coag_gpu_ctx *ctx, int pop, int64_t max_n,
+                          int64_t *id, int *action, int64_t *other_id,
+                          int64_t *n);
+
 /* Pair tests that MIXED mode decided in FP64, summed over the populations
  * since they were uploaded.  A test's FP32 acceptance probability is used
  * only where the uniform lies farther from it than a margin (2^-12) that

@@ -16,6 +16,7 @@ _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 KERNEL_SEDI, KERNEL_ADDITIVE, KERNEL_CONSTANT, KERNEL_BROWN, KERNEL_ZERO = 1, 2, 3, 4, 5
 KERNEL_BROWN_FREE, KERNEL_BROWN_CONT = 6, 7
 WEIGHT_NONE, WEIGHT_POWER, WEIGHT_MFA = 1, 2, 3
+INFO_NONE, INFO_DILUTION, INFO_COAG, INFO_HALVED, INFO_WEIGHT = 0, 1, 2, 3, 4  # aero_info.F90:19-28
 MAX_COMPONENT = 20
 
 # layout of orc_particle_meta (pmc_oracle.h)
@@ -123,6 +124,10 @@ def lib():
         L.orc_binomial_hist.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int64)]
         L.orc_set_fractal.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_set_record_removals.argtypes = [P, ctypes.c_int]
+        L.orc_removals.restype = ctypes.c_int64
+        L.orc_removals.argtypes = [P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ip,
+                                   ctypes.POINTER(ctypes.c_int64)]
         L.orc_fractal_radius.restype = ctypes.c_double
         L.orc_fractal_radius.argtypes = [ctypes.c_double] * 6 + [dp]
         L.orc_kernel_value_fractal.restype = ctypes.c_double
@@ -198,6 +203,21 @@ class Oracle:
         rc = lib().orc_set_fractal(self.ptr, frac_dim, prime_radius, vol_fill_factor)
         if rc:
             raise ValueError(f"orc_set_fractal failed: {rc}")
+
+    def set_record_removals(self, on=True):
+        lib().orc_set_record_removals(self.ptr, int(bool(on)))
+
+    def removals(self, max_n=1 << 22):
+        """Removal records since the last call, in removal order: dict of id,
+        action (aero_info.F90 codes) and other_id arrays; cleared."""
+        i64 = ctypes.POINTER(ctypes.c_int64)
+        ids = np.zeros(max_n, np.int64)
+        act = np.zeros(max_n, np.int32)
+        oth = np.zeros(max_n, np.int64)
+        n = lib().orc_removals(self.ptr, max_n, ids.ctypes.data_as(i64), _ip(act), oth.ctypes.data_as(i64))
+        if n < 0:
+            raise ValueError(f"{-n} removal records exceed max_n")
+        return {"id": ids[:n], "action": act[:n], "other_id": oth[:n]}
 
     def seed(self, s):
         lib().orc_set_seed(self.ptr, s)

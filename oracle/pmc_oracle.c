@@ -90,6 +90,11 @@ struct orc_state {
 
   int64_t next_id;
   int64_t kmax_warn;
+  /* aero_info_array (aero_info_array.F90): removal records, kept when on */
+  int rec_removals;
+  int64_t rm_n, rm_cap;
+  int64_t *rm_id, *rm_other;
+  int *rm_action;
   int64_t pp_targets; /* targets handled by the per-particle path (a counter for tests) */
 
   jmp_buf *fail;
@@ -1354,8 +1359,29 @@ static void array_add(orc_state *st, const double *v,
   st->meta[st->n_part - 1] = *m;
 }
 
-/* aero_state_remove_particle(_no_info / _with_info), aero_state.F90:382-446
- * (removal records are not kept) */
+/* aero_info_array_add_aero_info (aero_info_array.F90): one aero_info
+ * (aero_info.F90:48-56) of a removed particle, when records are kept */
+static void log_removal(orc_state *st, int64_t id, int action, int64_t other_id) {
+  if (!st->rec_removals) return;
+  if (st->rm_n == st->rm_cap) {
+    int64_t cap = st->rm_cap ? 2 * st->rm_cap : 1024;
+    int64_t *a = (int64_t *)realloc(st->rm_id, sizeof(int64_t) * cap);
+    if (a) st->rm_id = a;
+    int64_t *b = (int64_t *)realloc(st->rm_other, sizeof(int64_t) * cap);
+    if (b) st->rm_other = b;
+    int *c = (int *)realloc(st->rm_action, sizeof(int) * cap);
+    if (c) st->rm_action = c;
+    if (!a || !b || !c) orc_fail(st, ORC_ERR_NOMEM);
+    st->rm_cap = cap;
+  }
+  st->rm_id[st->rm_n] = id;
+  st->rm_action[st->rm_n] = action;
+  st->rm_other[st->rm_n] = other_id;
+  st->rm_n++;
+}
+
+/* aero_state_remove_particle(_no_info / _with_info), aero_state.F90:382-446;
+ * the callers log the removal first where the reference records it */
 static void state_remove(orc_state *st, int i) {
   if (st->valid_sort) {
     array_remove(st, i);
@@ -1401,6 +1427,7 @@ static void new_id(orc_state *st, orc_particle_meta *m) {
 static void state_dup(orc_state *st, int i, double n_mean, int rand_group) {
   int n_copies = orc_prob_round(st, n_mean);
   if (n_copies == 0) {
+    log_removal(st, st->meta[i - 1].id, ORC_INFO_WEIGHT, 0);
     state_remove(st, i);
   } else if (n_copies > 1) {
     for (int d = 1; d <= n_copies - 1; d++) {
@@ -1488,12 +1515,27 @@ static void coagulate(orc_state *st, int p1, int p2, int c1, int c2, int cc) {
   tpart ptc;
   int rm1, rm2, cn, l1, l2;
   coagulate_weighting(st, p1, p2, c1, c2, cc, &ptc, &rm1, &rm2, &cn, &l1, &l2);
+  /* aero_info_1/2 (coagulation.F90:900-920), recorded when the id is lost */
+  int64_t id1 = st->meta[p1 - 1].id, id2 = st->meta[p2 - 1].id;
+  int64_t other = cn ? ptc.m.id : 0;
   if (p2 > p1) {
-    if (rm2) state_remove(st, p2);
-    if (rm1) state_remove(st, p1);
+    if (rm2) {
+      if (l2) log_removal(st, id2, ORC_INFO_COAG, other);
+      state_remove(st, p2);
+    }
+    if (rm1) {
+      if (l1) log_removal(st, id1, ORC_INFO_COAG, other);
+      state_remove(st, p1);
+    }
   } else {
-    if (rm1) state_remove(st, p1);
-    if (rm2) state_remove(st, p2);
+    if (rm1) {
+      if (l1) log_removal(st, id1, ORC_INFO_COAG, other);
+      state_remove(st, p1);
+    }
+    if (rm2) {
+      if (l2) log_removal(st, id2, ORC_INFO_COAG, other);
+      state_remove(st, p2);
+    }
   }
   if (cn) state_add(st, ptc.vol, &ptc.m, 0);
 }
@@ -1658,7 +1700,11 @@ static void sample_source_particle(orc_state *st, const coag_env *env, int bs,
         double nc_i = orc_num_conc_at_radius(st, st->meta[ip - 1].weight_class,
                                              part_radius(st, ip));
         double pri = nc_target / nc_i;
-        if (orc_random(st) < pri / prm_max) state_remove(st, ip);
+        if (orc_random(st) < pri / prm_max) {
+          /* coagulation.F90:447-453 */
+          log_removal(st, st->meta[ip - 1].id, ORC_INFO_COAG, target->m.id);
+          state_remove(st, ip);
+        }
       }
     }
   }
@@ -1876,7 +1922,25 @@ void orc_destroy(orc_state *st) {
   rmap2_free(&st->size_class);
   rmap2_free(&st->group_class);
   free(st->dump);
+  free(st->rm_id);
+  free(st->rm_other);
+  free(st->rm_action);
   free(st);
+}
+
+void orc_set_record_removals(orc_state *st, int on) { st->rec_removals = on != 0; }
+
+int64_t orc_removals(orc_state *st, int64_t max_n, int64_t *id, int *action,
+                     int64_t *other_id) {
+  int64_t n = st->rm_n;
+  if (n > max_n) return -n;
+  for (int64_t k = 0; k < n; k++) {
+    id[k] = st->rm_id[k];
+    action[k] = st->rm_action[k];
+    other_id[k] = st->rm_other[k];
+  }
+  st->rm_n = 0;
+  return n;
 }
 
 void orc_set_next_id(orc_state *st, int64_t id) { st->next_id = id; }
@@ -2111,7 +2175,10 @@ static void state_double(orc_state *st, int g, int c) {
 static void state_halve(orc_state *st, int g, int c) {
   for (int i = st->n_part; i >= 1; i--) {
     if (st->meta[i - 1].weight_group == g && st->meta[i - 1].weight_class == c) {
-      if (orc_random(st) < 0.5) state_remove(st, i);
+      if (orc_random(st) < 0.5) {
+        log_removal(st, st->meta[i - 1].id, ORC_INFO_HALVED, 0);
+        state_remove(st, i);
+      }
     }
   }
   st->w_mag[(g - 1) + st->n_group * (c - 1)] *= 2.0;

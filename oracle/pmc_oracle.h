@@ -44,6 +44,15 @@ enum {
   ORC_KERNEL_BROWN_CONT = 7
 };
 
+/* removal actions, src/aero_info.F90:19-28 */
+enum {
+  ORC_INFO_NONE = 0,
+  ORC_INFO_DILUTION = 1,
+  ORC_INFO_COAG = 2,
+  ORC_INFO_HALVED = 3,
+  ORC_INFO_WEIGHT = 4
+};
+
 /* weight type codes, src/aero_weight.F90:24-30 */
 enum { ORC_WEIGHT_NONE = 1, ORC_WEIGHT_POWER = 2, ORC_WEIGHT_MFA = 3 };
 
@@ -131,6 +140,19 @@ int orc_check(const orc_state *st);
 int orc_kmax_table(orc_state *st, int kernel_type, double temp,
                    double pressure, double additive_coeff, double *kmin,
                    double *kmax);
+
+/* Keep removal records (aero_state%aero_info_array) from now on.  Records
+ * are appended in the reference's order of removals: coagulation removals
+ * whose ID is lost (coagulation.F90:928-985, other_id = the coagulated
+ * particle's ID or 0), per-particle source removals (:447-453, other_id =
+ * the target's ID), weight removals of aero_state_dup_particle and halving
+ * removals of aero_state_halve. */
+void orc_set_record_removals(orc_state *st, int on);
+/* Copy the records out (id, action, other_id) and clear them, as run_part
+ * does after an output (aero_info_array_zero); returns the count, or minus
+ * the count (nothing copied) if it exceeds max_n. */
+int64_t orc_removals(orc_state *st, int64_t max_n, int64_t *id, int *action,
+                     int64_t *other_id);
 
 /* Particle shape of aero_data (fractal_t, fractal.F90:59-66); d_f = 3 and
  * f = 1 are spherical particles, the default.  Invalidates the sort and the

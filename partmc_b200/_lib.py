@@ -71,6 +71,8 @@ SIGNATURES = {
     "pmc_coag_gpu_conflicts": (_I, [_P, _LP, _LP, _LP, _LP]),
     "pmc_coag_gpu_exact_tests": (_I, [_P, _LP]),
     "pmc_coag_gpu_set_fractal": (_I, [_P, _D, _D, _D]),
+    "pmc_coag_gpu_set_record_removals": (_I, [_P, _I]),
+    "pmc_coag_gpu_removals": (_I, [_P, _I, ctypes.c_int64, _LP, _IP, _LP, _LP]),
     "pmc_coag_gpu_bin_sort_noalloc": (_I, [_I, _P, _P, _I, _I, _D, _D, _P, _P, _P, _P, _P]),
 }
 

@@ -303,6 +303,28 @@ class AeroState:
               "pmc_coag_gpu_stats")
         return {"kmax_violations": a.value, "redraws": b.value, "rounds": c.value}
 
+    def set_record_removals(self, enable=True):
+        """Keep removal records (aero_info_array) on the device from now on."""
+        check(_lib.lib().pmc_coag_gpu_set_record_removals(self.ctx, int(bool(enable))),
+              "pmc_coag_gpu_set_record_removals")
+
+    def removals(self, pop=0, max_n=None):
+        """Removal records of population ``pop`` since the last call (dict of
+        id, action and other_id arrays; action codes of aero_info.F90:
+        2 coagulation, 3 halved, 4 weight), cleared on the device."""
+        n = ctypes.c_int64()
+        cap = max(1024, 2 * self.n_part(pop)) if max_n is None else int(max_n)
+        while True:
+            ids = np.zeros(cap, np.int64)
+            act = np.zeros(cap, np.int32)
+            oth = np.zeros(cap, np.int64)
+            rc = _lib.lib().pmc_coag_gpu_removals(self.ctx, pop, cap, lp(ids), ip(act), lp(oth), ctypes.byref(n))
+            if rc == _lib.PMC_ERR_CAPACITY and n.value > cap and max_n is None:
+                cap = n.value
+                continue
+            check(rc, "pmc_coag_gpu_removals")
+            return {"id": ids[:n.value], "action": act[:n.value], "other_id": oth[:n.value]}
+
     def exact_tests(self):
         """Pair tests that MIXED mode decided in FP64 (near the uniform or
         near k_max), summed over the populations since their upload."""

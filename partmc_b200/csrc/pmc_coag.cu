@@ -506,6 +506,7 @@ __global__ void k_halve(PopDev P, int g, int c, uint32_t call) {
     U4 r = philox4x32_10(U4{P.step, (call << 4) | kStreamHalve, (uint32_t)i, 0u}, (uint32_t)P.seed,
                          (uint32_t)(P.seed >> 32));
     if (u53(r.x, r.y) < 0.5) {
+      log_removal(P, P.id[i], kInfoHalved, 0);  // aero_state_halve records it (aero_state.F90:1768-1781)
       kill_slot(P, i);
       removed++;
     }
@@ -802,6 +803,7 @@ struct PopHost {
   int key_kt = 0, key_wver = -1;
   int wver = 0;  // bumped when this population's weights change
   double key_temp = 0, key_press = 0, key_coeff = 0;
+  long long rm_count = 0;  // removal records on the device at the last counter read
 };
 
 struct Ctx {
@@ -1271,6 +1273,7 @@ void init_pop(Ctx& c, PopHost& ph, int cap) {
   set_params(c, ph);
   alloc_slots(c, ph, cap);
   PopCtr z{};
+  ph.rm_count = 0;  // the population's removal records start empty
   z.next_id = 1;
   z.bmin = 1 << 30;
   z.bmax = -1;
@@ -2525,6 +2528,7 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
     free_list(ph.slot_allocs);
     free_list(ph.sort_allocs);
     free_list(ph.fixed_allocs);
+    if (ph.h.rm_log) cudaFree(ph.h.rm_log);
   }
   cudaFree(c.d_pops);
   cudaFree(c.d_ctrs);
@@ -2678,6 +2682,34 @@ int pmc_coag_gpu_upload_components(pmc_coag_gpu_ctx* x, int pop, int n_part, con
   GUARD_END
 }
 
+// Removal logs that record: room for the records kept so far plus the most
+// one step or rebalance can add (each removal frees a slot, and a step ends
+// with at most cap slots; twice that allows for slot growth within the
+// step).  Grows a log by copying its records into a larger buffer.
+void reserve_removal_logs(Ctx& c) {
+  for (auto& ph : c.pops) {
+    if (!ph.h.rm_on) continue;
+    long long need = ph.rm_count + 2LL * ph.h.cap + 1024;
+    if (ph.h.rm_cap >= need) continue;
+    long long cap = std::max(need, ph.h.rm_cap + ph.h.rm_cap / 2);
+    RemovalRec* p = nullptr;
+    if (cudaMalloc(&p, sizeof(RemovalRec) * (size_t)cap) != cudaSuccess) {
+      cudaGetLastError();
+      throw Fail(PMC_ERR_CAPACITY);
+    }
+    if (ph.h.rm_log) {
+      long long keep = std::min(ph.rm_count, ph.h.rm_cap);
+      if (keep > 0)
+        CK(cudaMemcpyAsync(p, ph.h.rm_log, sizeof(RemovalRec) * (size_t)keep, cudaMemcpyDeviceToDevice, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+      cudaFree(ph.h.rm_log);
+    }
+    ph.h.rm_log = p;
+    ph.h.rm_cap = cap;
+    c.dirty = true;
+  }
+}
+
 static int finish_step(Ctx& c, long long* samp, long long* coag) {
   long long s = 0, k = 0, warn = 0, exact = 0;
   int status = 0;
@@ -2690,6 +2722,11 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
     k += r.tot_coag;
     warn += r.kmax_warn;
     exact += r.exact_tests;
+    c.pops[p].rm_count = r.n_removed;
+    if (c.pops[p].h.rm_on && r.n_removed > c.pops[p].h.rm_cap) {
+      snprintf(g_last_assert, sizeof(g_last_assert), "removal log of population %d overflowed", p);
+      if (!status) status = PMC_ERR_CAPACITY;
+    }
     if (r.status && !status) status = r.status;
     if (r.bad_site) {
       static const char* site[] = {"", "pair test: list position", "pair test: slot", "event: slot",
@@ -2738,6 +2775,7 @@ int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* 
         ph.kmax_kt = kernel_type;
       }
     }
+    reserve_removal_logs(c);
     push_pops(c);
     long long s = 0, k = 0;
     int status;
@@ -2904,6 +2942,7 @@ int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx* x, int pop, const double* n_part_id
           changed = true;
         }
       }
+  if (allow_halving) reserve_removal_logs(c);  // halving records its removals
   if (allow_halving)
     for (int g = 1; g <= c.n_group; g++)
       for (int cl = 1; cl <= c.n_class; cl++) {
@@ -2926,7 +2965,9 @@ int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx* x, int pop, const double* n_part_id
     push_pops(c);
     CK(cudaStreamSynchronize(c.stream));
     PopCtr r = read_ctr(c, pop);
+    ph.rm_count = r.n_removed;
     if (r.status) return r.status;
+    if (ph.h.rm_on && r.n_removed > ph.h.rm_cap) return PMC_ERR_CAPACITY;
   }
   return PMC_OK;
   GUARD_END
@@ -3239,6 +3280,47 @@ int pmc_coag_gpu_exact_tests(pmc_coag_gpu_ctx* x, int64_t* n) {
   if (!x || !n) return PMC_ERR_INVALID_ARG;
   *n = x->c.exact_tests;
   return PMC_OK;
+}
+
+int pmc_coag_gpu_set_record_removals(pmc_coag_gpu_ctx* x, int enable) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  for (auto& ph : c.pops) ph.h.rm_on = enable ? 1 : 0;
+  reserve_removal_logs(c);
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  return PMC_OK;
+  GUARD_END
+}
+
+int pmc_coag_gpu_removals(pmc_coag_gpu_ctx* x, int pop, int64_t max_n, int64_t* id, int* action,
+                          int64_t* other_id, int64_t* n) {
+  if (!x || pop < 0 || pop >= x->c.n_pop || max_n < 0 || !n || (max_n > 0 && (!id || !action || !other_id)))
+    return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  PopCtr r = read_ctr(c, pop);
+  *n = r.n_removed;
+  ph.rm_count = r.n_removed;
+  if (r.n_removed > ph.h.rm_cap && ph.h.rm_on) return PMC_ERR_CAPACITY;  // records were dropped
+  if (r.n_removed > max_n) return PMC_ERR_CAPACITY;                     // nothing copied or cleared
+  if (r.n_removed > 0) {
+    std::vector<RemovalRec> h((size_t)r.n_removed);
+    CK(cudaMemcpyAsync(h.data(), ph.h.rm_log, sizeof(RemovalRec) * h.size(), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    for (size_t k = 0; k < h.size(); k++) {
+      id[k] = h[k].id;
+      action[k] = h[k].action;
+      other_id[k] = h[k].other_id;
+    }
+  }
+  r.n_removed = 0;
+  write_ctr(c, pop, r);
+  ph.rm_count = 0;
+  return PMC_OK;
+  GUARD_END
 }
 
 int pmc_coag_gpu_profile(pmc_coag_gpu_ctx* x, int enable) {

@@ -75,6 +75,7 @@ __device__ __forceinline__ void add_ll(long long* p, long long v) {
 }
 __device__ __forceinline__ void add_ll(int* p, long long v) { atomicAdd(p, (int)v); }
 
+
 // add_ll for counters that many threads of a launch bump: the converged
 // lanes that add to the same counter sum their values (|v| small) and one of
 // them adds the sum, so a warp makes one atomic per counter instead of 32

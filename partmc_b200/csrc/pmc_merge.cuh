@@ -285,6 +285,9 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
     if (m.rm1) P.touched[s1] = gen;
     if (m.rm2) P.touched[s2] = gen;
     if (!m.create) {
+      // coagulate (coagulation.F90:928-985) records a removal whose ID is lost
+      if (m.rm1 && m.lost1) log_removal(P, P.id[s1], kInfoCoag, 0);
+      if (m.rm2 && m.lost2) log_removal(P, P.id[s2], kInfoCoag, 0);
       if (m.rm1) kill_slot(P, s1);
       if (m.rm2) kill_slot(P, s2);
       int dlive = -(int)m.rm1 - (int)m.rm2;
@@ -307,9 +310,13 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
     coag_scalars(a, wi.x, b, wi.y, c);
     P.grp[dest] = m.new_group;
     P.cls[dest] = P.pair[p].cc + 1;
-    if (m.rm1 && !m.lost1) P.id[dest] = a.id;
-    else if (m.rm2 && !m.lost2) P.id[dest] = b.id;
-    else P.id[dest] = id_base[pop] + id_rank[e];
+    long long new_id;
+    if (m.rm1 && !m.lost1) new_id = a.id;
+    else if (m.rm2 && !m.lost2) new_id = b.id;
+    else new_id = id_base[pop] + id_rank[e];
+    P.id[dest] = new_id;
+    if (m.rm1 && m.lost1) log_removal(P, a.id, kInfoCoag, new_id);
+    if (m.rm2 && m.lost2) log_removal(P, b.id, kInfoCoag, new_id);
     P.nprim[dest] = c.nprim;
     P.lct[dest] = c.lct;
     P.gct[dest] = c.gct;
@@ -943,7 +950,7 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
           vt_b = vt;
           C_b = C;
         }
-        bool ok = true, first_k = false, rm_y_k = false, lost_x_k = false;
+        bool ok = true, first_k = false, rm_y_k = false, lost_x_k = false, lost_y_k = false;
         int group_k = 0;
         uint32_t used_k = 0;
         if (lane < n_ok) {
@@ -957,6 +964,7 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
           rm_y_k = first_k ? m.rm2 : m.rm1;
           lost_x_k = first_k ? m.lost1 : m.lost2;
           bool lost_y = first_k ? m.lost2 : m.lost1;
+          lost_y_k = rm_y_k && lost_y;
           ok = m.create && rm_x && m.new_group != 0 && !(lost_x_k && !(rm_y_k && !lost_y));
           group_k = m.new_group;
           used_k = g.used();
@@ -986,6 +994,7 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
           const bool first = __shfl_sync(kFull, first_k ? 1 : 0, k) != 0;
           const bool rm_y = __shfl_sync(kFull, rm_y_k ? 1 : 0, k) != 0;
           const bool lost_x = __shfl_sync(kFull, lost_x_k ? 1 : 0, k) != 0;
+          const bool lost_y = __shfl_sync(kFull, lost_y_k ? 1 : 0, k) != 0;
           const int new_group = __shfl_sync(kFull, group_k, k);
           const uint32_t used = __shfl_sync(kFull, used_k, k);
           const PScal ys = st.s;
@@ -1019,6 +1028,12 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
           coag_scalars(A, first ? ice_x : ice_y, B, first ? ice_y : ice_x, nm);
           nm.ncomp = n_out;
           nm.id = !lost_x ? cur.id : ys.id;
+          // the removals of this event whose ID is lost (coagulate,
+          // coagulation.F90:928-985): the walking particle's is always removed
+          if (lane == 0) {
+            if (lost_x) log_removal(P, cur.id, kInfoCoag, nm.id);
+            if (lost_y) log_removal(P, ys.id, kInfoCoag, nm.id);
+          }
           nm.grp = new_group;
           nm.cls = st.cc + 1;
           cc_ = lane < n_out ? (from_a ? xa : xb) : 0;
@@ -1421,6 +1436,9 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
     uint32_t gen = *P.gen_p;
     int dlive = 0;
     for (int z = 0; z < R.n_rm; z++) {
+      // sample_source_particle records each source it removes with the
+      // target's ID (coagulation.F90:447-453)
+      log_removal(P, P.id[R.rm[z]], kInfoCoag, P.id[R.target]);
       kill_slot(P, R.rm[z]);
       P.touched[R.rm[z]] = gen;
       dlive--;
@@ -1430,6 +1448,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
       int t = R.target;
       P.touched[t] = gen;
       if (R.n_copies == 0) {
+        log_removal(P, P.id[t], kInfoWeight, 0);  // aero_state_dup_particle (aero_state.F90:502-513)
         kill_slot(P, t);
         dlive--;
       } else {

@@ -198,7 +198,10 @@ struct Seq {
   __device__ bool state_dup(int i, double n_mean) {
     int nc = prob_round(g, n_mean);
     if (!rng_ok()) return false;
-    if (nc == 0) return state_remove(i);
+    if (nc == 0) {
+      log_removal(*P, P->id[i - 1], kInfoWeight, 0);
+      return state_remove(i);
+    }
     for (int d = 1; d <= nc - 1; d++) {
       Tp c;
       load(i, c);
@@ -307,11 +310,17 @@ struct Seq {
       else if (rm2 && !l2) ptc.m.id = b.m.id;
       else ptc.m.id = new_id();
     }
+    // aero_info of each removal whose ID is lost, in the order of removal
+    const long long id1 = P->id[p1 - 1], id2 = P->id[p2 - 1], other = cn_ ? ptc.m.id : 0;
     if (p2 > p1) {
+      if (rm2 && l2) log_removal(*P, id2, kInfoCoag, other);
       if (rm2 && !state_remove(p2)) return false;
+      if (rm1 && l1) log_removal(*P, id1, kInfoCoag, other);
       if (rm1 && !state_remove(p1)) return false;
     } else {
+      if (rm1 && l1) log_removal(*P, id1, kInfoCoag, other);
       if (rm1 && !state_remove(p1)) return false;
+      if (rm2 && l2) log_removal(*P, id2, kInfoCoag, other);
       if (rm2 && !state_remove(p2)) return false;
     }
     if (cn_) return state_add(ptc);
@@ -442,6 +451,7 @@ struct Seq {
           double pri = nc_target / nc_i;
           if (g.next() < pri / prm_max) {
             if (!rng_ok()) return false;
+            log_removal(*P, P->id[ip - 1], kInfoCoag, target.m.id);
             if (!state_remove(ip)) return false;
           }
         }

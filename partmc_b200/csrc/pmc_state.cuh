@@ -47,6 +47,16 @@ struct __align__(32) RecF {
 
 struct PopDev;
 
+// aero_info_t (aero_info.F90:48-56): the ID of a removed particle, the
+// action (aero_info.F90:19-28: kInfoCoag, kInfoHalved, kInfoWeight) and the
+// ID of the particle the coagulation produced (the target's ID for a
+// per-particle coagulation, 0 if none)
+struct RemovalRec {
+  long long id, other_id;
+  int action, pad;
+};
+enum : int { kInfoCoag = 2, kInfoHalved = 3, kInfoWeight = 4 };
+
 // index of species s of slot i, and of component k of slot i
 #define PMC_VOL_AT(n_spec, i, s) ((size_t)(i) * (size_t)(n_spec) + (size_t)(s))
 __host__ __device__ __forceinline__ size_t comp_at(long long i, int k) {
@@ -106,6 +116,7 @@ struct PopCtr {
   long long bad_index;     // the index that failed it
   long long walk_tests;    // pair tests made by walks in the current step
   long long exact_tests;   // FP32 pair tests decided in FP64 (f32_decides), since the context was made
+  long long n_removed;     // removal records appended since the host last read them
 };
 
 // sites of the device bounds checks (PopCtr::bad_site)
@@ -217,6 +228,13 @@ struct PopDev {
   uint32_t* touched;
 
   PopCtr* ctr;
+
+  // removal log (aero_state%aero_info_array) when rm_on: records
+  // [0, ctr->n_removed), at most rm_cap kept (the host sizes it before
+  // every step for the most removals a step can make)
+  RemovalRec* rm_log;
+  long long rm_cap;
+  int rm_on;
 };
 
 __host__ __device__ __forceinline__ size_t vol_at(const PopDev& P, long long i, int s) {
@@ -254,6 +272,23 @@ __device__ __forceinline__ void claim_slot(const PopDev& P, int s, unsigned long
 }
 __device__ __forceinline__ bool holds_slot(const PopDev& P, int s, unsigned long long ck, bool write) {
   return write ? (P.claim[s] == ck && P.rclaim[s] > ck) : P.claim[s] > ck;
+}
+
+// aero_state_remove_particle_with_info (aero_state.F90:408-422): append
+// the removal's aero_info to the population's log when records are kept.
+// Records past the log's capacity are counted but dropped (the host reports
+// that as PMC_ERR_CAPACITY).
+__device__ __forceinline__ void log_removal(const PopDev& P, long long id, int action, long long other_id) {
+  if (!P.rm_on) return;
+  const unsigned long long k = atomicAdd((unsigned long long*)&P.ctr->n_removed, 1ULL);
+  if ((long long)k < P.rm_cap) {
+    RemovalRec r;
+    r.id = id;
+    r.other_id = other_id;
+    r.action = action;
+    r.pad = 0;
+    P.rm_log[k] = r;
+  }
 }
 #endif
 

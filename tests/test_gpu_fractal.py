@@ -110,7 +110,11 @@ def test_fractal_kmax_table(gpu_lib, shape, kt):
     # terminal speed (fall_g), so their sedimentation kernel is 0 in both
     nz = k_cpu != 0
     assert np.array_equal(k_gpu[~nz], k_cpu[~nz])
-    rel = np.abs(k_gpu[nz] - k_cpu[nz]) / np.abs(k_cpu[nz])
+    # the sedimentation kernel's |w1 - w2| cancels where both speeds are near
+    # the cap: there the error is measured against a thousandth of the
+    # table's largest value instead of the entry
+    scale = np.maximum(np.abs(k_cpu[nz]), 1e-3 * np.abs(k_cpu).max())
+    rel = np.abs(k_gpu[nz] - k_cpu[nz]) / scale
     assert rel.max() < 1e-12, rel.max()
 
 

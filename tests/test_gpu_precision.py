@@ -58,7 +58,9 @@ def test_mixed_reproduces_fp64_particle_for_particle(gpu_lib, name):
     n_tests = sum(s for s, _ in c32)
     n_exact = st32.exact_tests()
     print(f"{name}: {n_tests} tests, {n_exact} decided in FP64 ({n_exact / max(n_tests, 1):.2e})")
-    assert 0 < n_exact < 0.05 * n_tests
+    assert n_exact < 0.05 * n_tests
+    if n_tests > 20000:  # expected about 10 or more: the fallback must have run
+        assert n_exact > 0
 
 
 @pytest.mark.parametrize("name", list(workloads()))

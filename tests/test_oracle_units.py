@@ -92,3 +92,32 @@ def test_sort_bookkeeping_consistent_after_steps():
         assert orc.check() == 0
     vol2, meta = orc.particles()
     assert len(np.unique(meta["id"])) == len(meta)
+
+
+def test_oracle_removal_records_account_for_every_id():
+    """The oracle's aero_info log over coagulation steps of three weightings
+    (flat additive; power weights with the per-particle path; nummass with 20
+    species) and a halving: every ID that existed is present afterwards or
+    removed with exactly one record (removal_check.py)."""
+    import removal_check as RCK
+    from partmc_b200 import aero_dist
+    cases = [(aero_dist.additive_exp(3000, seed=3), O.KERNEL_ADDITIVE, 60.0),
+             (aero_dist.brown_bimodal(3000, seed=4, modes=[(1e11, 0.005e-6, np.log10(1.5)),
+                                                           (1e8, 0.25e-6, np.log10(1.5))]), O.KERNEL_BROWN, 600.0),
+             (aero_dist.brown_20spec(3000, seed=5), O.KERNEL_BROWN, 600.0)]
+    for pop, kt, dt in cases:
+        o = O.Oracle(pop.aero_data.density, (pop.awa.type, pop.awa.magnitude, pop.awa.exponent), seed=9)
+        o.add_particles(pop.vol, O.make_meta(pop.n_part, group=pop.group, ids=np.arange(1, pop.n_part + 1)))
+        o.set_next_id(pop.n_part + 1)
+        o.set_record_removals(True)
+        for _ in range(3):
+            ids0, nid0 = o.particles()[1]["id"].copy(), o.next_id()
+            o.mc_coag(kt, 288.0, 1e5, 1000.0, dt)
+            rec = o.removals()
+            RCK.check_id_accounting(ids0, nid0, o.next_id(), o.particles()[1]["id"], rec)
+            assert len(rec["id"]) > 0
+        ids0, nid0 = o.particles()[1]["id"].copy(), o.next_id()
+        o.rebalance(np.full((o.n_group, o.n_class), o.n_part / 8.0), allow_doubling=False)
+        rec = o.removals()
+        assert (rec["action"] == RCK.INFO_HALVED).all() and len(rec["id"]) > 0
+        RCK.check_id_accounting(ids0, nid0, o.next_id(), o.particles()[1]["id"], rec)
