@@ -191,7 +191,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lb(ScanJobs jobs, unsigne
 // test sequence ((s + 1) / n_samp: the part of the pair done after it)
 __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const long long* n_samples,
                                 const int2* ev, const int* ev_gp, const int* gpair_local, const long long* work_off,
-                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len) {
+                                unsigned long long* ev_key, int2* ev_c, int* gp_c, float* ev_pos, int* ev_len,
+                                int4* ev_term) {
   long long n = *n_samples;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -204,6 +205,7 @@ __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const
       gp_c[e] = gp;
       ev_pos[e] = (float)((double)(s + 1) / (double)ns);
       ev_len[e] = 0;
+      ev_term[e] = no_term();
     }
 }
 
@@ -211,8 +213,9 @@ __global__ void k_compact_flags(const uint8_t* flag, const long long* off, const
 __global__ void k_compact_items(const uint8_t* it_flag, const long long* off, const long long* n_items,
                                 const unsigned long long* it_key, const int2* it_c, const int* it_gp,
                                 const float* it_pos, const int* it_len, const int* it_head, const uint8_t* it_done,
-                                const uint32_t* it_dec, unsigned long long* ev_key, int2* ev_c, int* gp_c,
-                                float* ev_pos, int* ev_len, int* ev_head, uint8_t* ev_done, uint32_t* dec) {
+                                const uint32_t* it_dec, const int4* it_term, unsigned long long* ev_key, int2* ev_c,
+                                int* gp_c, float* ev_pos, int* ev_len, int* ev_head, uint8_t* ev_done, uint32_t* dec,
+                                int4* ev_term) {
   long long n = *n_items;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -226,6 +229,7 @@ __global__ void k_compact_items(const uint8_t* it_flag, const long long* off, co
       ev_head[e] = it_head[i];
       ev_done[e] = it_done[i];
       dec[e] = it_dec[i];
+      ev_term[e] = it_term[i];
     }
 }
 
@@ -857,6 +861,7 @@ struct Ctx {
   DevBuf<int> it_gp, it_len, it_head;
   DevBuf<float> it_pos;
   DevBuf<uint32_t> it_dec, it_gused;
+  DevBuf<int4> it_term, ev_term;  // pending tests where chains stopped (kPendingTerm)
   DevBuf<long long> it_off;
   // chain events of a round (ChainPool), in chunks
   DevBuf<int> ch_y, ch_q;
@@ -1610,11 +1615,11 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
     k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
                               c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
                               c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
-                              c.it_done.p, c.it_dec.p, c.it_gused.p);
+                              c.it_done.p, c.it_dec.p, c.it_gused.p, c.it_term.p);
     auto kc = flat ? k_chain<KT, T, true> : k_chain<KT, T, false>;
     kc<<<grid_for(W, 128), 128, 0, st>>>(c.d_pops, c.gpair_pop.p, n_items, c.it_flag.p, c.it_key.p, c.it_c.p,
                                          c.it_gp.p, c.it_pos.p, c.it_dec.p, c.it_gused.p, pool, c.it_len.p,
-                                         c.it_head.p, c.it_done.p);
+                                         c.it_head.p, c.it_done.p, c.it_term.p);
   });
   note_launch();
   note_launch();
@@ -1889,13 +1894,14 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
     k_apply_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
                                                   c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
                                                   c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_done.p,
-                                                  c.ev_dest.p);
+                                                  c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
+                                                  c.ev_term.p, c.pop_pair_base.p);
     note_launch();
     // chains, one warp each
     k_apply_chain<<<grid_for(W, 32), 32, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, c.chain_list.p,
                                                     c.round_dev.p + 4, c.ev_key.p, c.ev_len.p, c.ev_app.p,
                                                     c.ev_head.p, c.ev_done.p, pool, c.gp_c.p, c.ev_pos.p,
-                                                    c.ev_dest.p);
+                                                    c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.dec_set.p, c.ev_term.p);
     note_launch();
   }
   if (Q > 0) {
@@ -1938,8 +1944,8 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
   scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.it_flag.p, W, Id, c.it_off.p, Ed}}, st);
   k_compact_items<<<grid_for(W, 256), 256, 0, st>>>(c.it_flag.p, c.it_off.p, Id, c.it_key.p, c.it_c.p, c.it_gp.p,
                                                     c.it_pos.p, c.it_len.p, c.it_head.p, c.it_done.p, c.it_dec.p,
-                                                    c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.ev_len.p,
-                                                    c.ev_head.p, c.ev_done.p, c.dec_set.p);
+                                                    c.it_term.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p,
+                                                    c.ev_len.p, c.ev_head.p, c.ev_done.p, c.dec_set.p, c.ev_term.p);
   note_launch();
   resolve_apply(c, st, W, Q);
 }
@@ -1955,6 +1961,7 @@ std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
           (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.chain_list.p, (long long)c.it_flag.p, (long long)c.it_key.p,
           (long long)c.it_c.p, (long long)c.it_gp.p, (long long)c.it_pos.p, (long long)c.it_len.p,
           (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_dec.p, (long long)c.it_gused.p, (long long)c.it_off.p,
+          (long long)c.it_term.p, (long long)c.ev_term.p,
           (long long)c.ch_y.p,
           (long long)c.ch_q.p, (long long)c.ch_pos.p, (long long)c.need_slot_set.p, (long long)c.need_id_set.p,
           (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p, (long long)c.rank_id_set.p,
@@ -1989,6 +1996,7 @@ void reserve_events(Ctx& c, long long W) {
   c.ev_key.reserve(w + 1); c.ev_c.reserve(w + 1); c.gp_c.reserve(w + 1); c.ev_pos.reserve(w + 1);
   c.ev_dest.reserve(w + 1); c.win_set.reserve(w + 1); c.dec_set.reserve(w + 1);
   c.ev_len.reserve(w + 1); c.ev_head.reserve(w + 1); c.ev_app.reserve(w + 1); c.ev_done.reserve(w + 1);
+  c.ev_term.reserve(w + 1);
   c.chain_list.reserve(w + 1);
   c.need_slot_set.reserve(w + 1); c.need_id_set.reserve(w + 1); c.ice_set.reserve(w + 1);
   c.rank_slot_set.reserve(w + 2); c.rank_id_set.reserve(w + 2);
@@ -2004,6 +2012,7 @@ bool events_fit(const Ctx& c, long long W) {
   return c.ev_key.n >= w + 1 && c.ev_c.n >= w + 1 && c.gp_c.n >= w + 1 && c.ev_pos.n >= w + 1 &&
          c.ev_dest.n >= w + 1 && c.win_set.n >= w + 1 && c.dec_set.n >= w + 1 && c.ev_len.n >= w + 1 &&
          c.ev_head.n >= w + 1 && c.ev_app.n >= w + 1 && c.ev_done.n >= w + 1 && c.chain_list.n >= w + 1 &&
+         c.ev_term.n >= w + 1 &&
          c.need_slot_set.n >= w + 1 &&
          c.need_id_set.n >= w + 1 && c.ice_set.n >= w + 1 && c.rank_slot_set.n >= w + 2 &&
          c.rank_id_set.n >= w + 2;
@@ -2015,7 +2024,7 @@ void reserve_round(Ctx& c, long long W) {
   size_t w = (size_t)std::max<long long>(W, 1);
   c.it_flag.reserve(w + 1); c.it_key.reserve(w + 1); c.it_c.reserve(w + 1); c.it_gp.reserve(w + 1);
   c.it_pos.reserve(w + 1); c.it_len.reserve(w + 1); c.it_head.reserve(w + 1); c.it_done.reserve(w + 1);
-  c.it_dec.reserve(w + 1); c.it_gused.reserve(w + 1);
+  c.it_dec.reserve(w + 1); c.it_gused.reserve(w + 1); c.it_term.reserve(w + 1);
   c.it_off.reserve(w + 2);
 }
 
@@ -2309,7 +2318,7 @@ void step_parallel(Ctx& c, int kt) {
     scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.flag.p, W, Wd, c.flag_off.p, c.round_dev.p + 1}});
     k_compact_flags<<<grid_for(W, 256), 256, 0, c.stream>>>(c.flag.p, c.flag_off.p, Wd, c.ev.p, c.ev_gp.p,
                                                            c.gpair_local.p, c.work_off.p, c.ev_key.p, c.ev_c.p,
-                                                           c.gp_c.p, c.ev_pos.p, c.ev_len.p);
+                                                           c.gp_c.p, c.ev_pos.p, c.ev_len.p, c.ev_term.p);
     note_launch();
     k_decide<<<grid_for(W, 256), 256, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.round_dev.p + 1, c.ev_key.p,
                                                     c.ev_c.p, c.gp_c.p, c.dec_set.p);
@@ -2549,6 +2558,8 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.it_pos.release();
   c.it_dec.release();
   c.it_gused.release();
+  c.it_term.release();
+  c.ev_term.release();
   c.ch_pos.release();
   c.it_flag.release();
   c.it_done.release();

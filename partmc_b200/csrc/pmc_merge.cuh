@@ -68,6 +68,28 @@ struct ChainReader {
   }
 };
 
+// A chain stops at an accepted test that is no absorb (or that the pool has
+// no room for).  That test has happened: dropping it and walking on afresh
+// in the next round would redraw its merge decision until an absorb came up,
+// which favours absorbs whenever the weights make some decisions keep the
+// walking particle (with flat weights every decision absorbs).  So the
+// stopping test is carried to the next round as a pending event with its
+// decision: its partner, pair (and whether the walker is in the pair's first
+// cell), decision and position, packed as {y, q | first << 30, decision,
+// position bits}; y = -1 for none.  An event whose dest_out is kPendingTerm
+// hands that test to the next round (k_items) instead of a walk.
+constexpr int kPendingTerm = -2;
+// The same holds for a chain cut short where a partner's claim failed: the
+// claim's kind (write or read) follows the event's decision, so the cut
+// depends on it, and walking on afresh would redraw that decision.  The
+// first event not applied is pending for the next round (kPendingChain),
+// its decision recomputed there from the chain's stream (event index in
+// the decision word) and the particles' values, which give the decision
+// the walk made whenever the partner is unchanged.
+constexpr int kPendingChain = -3;
+constexpr int kTermFirst = 1 << 30;
+__device__ __forceinline__ int4 no_term() { return make_int4(-1, 0, 0, 0); }
+
 __device__ __forceinline__ void kill_slot(const PopDev& P, int i) {
   P.alive[i] = 0;
   P.changed[i] = 1;
@@ -266,7 +288,9 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
                             const unsigned long long* ev_key, const int2* ev, const int* ev_gp,
                             const uint8_t* win, const uint32_t* dec, const long long* slot_rank,
                             const long long* id_rank, const int* slot_base, const long long* id_base,
-                            const double2* ice, const uint8_t* ev_done, int* dest_out) {
+                            const double2* ice, const uint8_t* ev_done, int* dest_out, unsigned long long* ev_key_w,
+                            int2* ev_w, int* gp_w, float* pos_w, uint32_t* dec_w, const int4* ev_term,
+                            const long long* pop_pair_base) {
   long long E = *n_events;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
        e += (long long)gridDim.x * blockDim.x) {
@@ -331,8 +355,23 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
     // with allow_resort=.false., aero_sorted.F90:427-440)
     P.touched[dest] = gen;
     int nbin = refresh_slot(P, dest);
-    if (nbin < 1 || nbin > P.grid->n_bin) set_status(P.ctr, kErrOutOfGrid);
-    else if (!(key_kind(ev_key[e]) == 1u && ev_done[e])) dest_out[e] = dest;  // a walk that ran to its end stops
+    if (nbin < 1 || nbin > P.grid->n_bin) {
+      set_status(P.ctr, kErrOutOfGrid);
+    } else if (ev_term[e].x >= 0) {
+      // a one-event chain that stopped at a pending test: the coagulated
+      // particle (in slot dest) meets that test in the next round
+      const int4 t = ev_term[e];
+      const int tq = t.y & (kTermFirst - 1);
+      const bool tfirst = (t.y & kTermFirst) != 0;
+      ev_key_w[e] = make_key((uint32_t)tq, 1u, (uint32_t)dest);
+      ev_w[e] = tfirst ? make_int2(dest, t.x) : make_int2(t.x, dest);
+      gp_w[e] = (int)(pop_pair_base[pop] + tq);
+      pos_w[e] = __int_as_float(t.w);
+      dec_w[e] = (uint32_t)t.z;
+      dest_out[e] = kPendingTerm;
+    } else if (!(key_kind(ev_key[e]) == 1u && ev_done[e])) {
+      dest_out[e] = dest;  // a walk that ran to its end stops
+    }
     if (m.rm1 && dest != s1) kill_slot(P, s1);
     if (m.rm2 && dest != s2) kill_slot(P, s2);
     int dlive = 1 - (int)m.rm1 - (int)m.rm2;
@@ -649,11 +688,12 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
                                                const int* gp_c, const float* ev_pos, const uint32_t* dec,
                                                uint8_t* it_flag, unsigned long long* it_key,
                                                int2* it_c, int* it_gp, float* it_pos, int* it_len, int* it_head,
-                                               uint8_t* it_done, uint32_t* it_dec, uint32_t* it_gused) {
+                                               uint8_t* it_done, uint32_t* it_dec, uint32_t* it_gused, int4* it_term) {
   long long n = *n_items;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
     it_flag[e] = 0;
+    it_term[e] = no_term();
     int gp = gp_c[e];
     if (gp < 0 || gp >= n_gpairs) {
       bad_index(pops[0].ctr, kBadEventSlot, gp);
@@ -662,10 +702,41 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     int pop = gpair_pop[gp];
     const PopDev& P = pops[pop];
     int walker = -1, p0 = 0;
+    uint32_t pend_dec = 0xffffffffu;  // a pending chain event's recomputed decision
     float pos0 = ev_pos[e];
     unsigned long long key = ev_key[e];
     int2 sl = ev_c[e];
-    if (win[e]) {
+    if (win[e] && (dest[e] == kPendingTerm || dest[e] == kPendingChain)) {
+      // the test where the previous round's chain stopped, with its decision:
+      // the walker was rewritten by its own chain, so only its death counts;
+      // a partner consumed in that round is no member now, and the walk goes
+      // on after the test
+      if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
+        bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+        continue;
+      }
+      const int x = (int)key_idx(key), y = x == sl.x ? sl.y : sl.x;
+      if (!P.alive[x]) continue;
+      if (P.touched[y] == *P.gen_p - 1u || !P.alive[y]) {
+        walker = x;
+        p0 = (int)key_pair(key);
+      } else if (dest[e] == kPendingChain) {
+        // the chain's event again, decided as the walk decided it
+        const int q = (int)key_pair(key);
+        if (q >= P.n_pairs) {
+          bad_index(P.ctr, kBadEventSlot, q);
+          continue;
+        }
+        const PairDesc d = P.pair_desc[q];
+        const PairState& S = P.pair[q];
+        Rng g = make_rng(P, kStreamChain, dec[e] + 1u, (uint32_t)x);
+        MergeDecision m = sl.x == x
+                              ? merge_decide_v(P, g, P.rad[x], P.vtot[x], P.rad[y], P.vtot[y], d.c1, d.c2, S.cc)
+                              : merge_decide_v(P, g, P.rad[y], P.vtot[y], P.rad[x], P.vtot[x], d.c1, d.c2, S.cc);
+        if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+        pend_dec = pack_decision(m, g.used());
+      }
+    } else if (win[e]) {
       walker = dest[e];
       p0 = gpair_local[gp];
       if (walker < 0) continue;
@@ -691,7 +762,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     }
     int len = 0, head = -1;
     bool done = false;
-    uint32_t dc = dec[e];
+    uint32_t dc = pend_dec != 0xffffffffu ? pend_dec : dec[e];
     if (walker >= 0) {
       WalkOut w;
       walk<KT, T, FLAT>(P, walker, p0, pos0, &w);
@@ -741,7 +812,7 @@ __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gp
                                                const uint8_t* it_flag, const unsigned long long* it_key,
                                                const int2* it_c, const int* it_gp, const float* it_pos,
                                                const uint32_t* it_dec, const uint32_t* it_gused, ChainPool pool,
-                                               int* it_len, int* it_head, uint8_t* it_done) {
+                                               int* it_len, int* it_head, uint8_t* it_done, int4* it_term) {
   long long n = *n_items;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
@@ -796,9 +867,12 @@ __global__ void __launch_bounds__(128) k_chain(const PopDev* pops, const int* gp
                               : merge_decide_v(P, gm, ry, vty, r, vt, d.c1, d.c2, S.cc);
       bool rm_x = first ? m.rm1 : m.rm2, rm_y = first ? m.rm2 : m.rm1;
       // the chain ends before an event that is no absorb, or when the pool
-      // is full; the walk resumes there in the next round
-      if (!(m.create && rm_x && m.new_group != 0) || !cw.append(pool, yy, qq | (rm_y ? kChainRemoves : 0), pos))
+      // is full; that event is pending for the next round (kPendingTerm)
+      if (!(m.create && rm_x && m.new_group != 0) || !cw.append(pool, yy, qq | (rm_y ? kChainRemoves : 0), pos)) {
+        if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+        it_term[e] = make_int4(yy, qq | (first ? kTermFirst : 0), (int)pack_decision(m, gm.used()), __float_as_int(pos));
         break;
+      }
       claim_slot(P, yy, claim_key(P, k2), rm_y);
       y = yy;
       q = qq;
@@ -848,7 +922,8 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
                                                     const long long* n_chain, const unsigned long long* ev_key,
                                                     const int* ev_len, const int* ev_app, const int* ev_head,
                                                     const uint8_t* ev_done, ChainPool pool, int* gp_c, float* ev_pos,
-                                                    int* dest_out) {
+                                                    int* dest_out, unsigned long long* ev_key_w, int2* ev_w,
+                                                    uint32_t* dec_w, const int4* ev_term) {
   constexpr unsigned kFull = 0xffffffffu;
   constexpr int kBatch = kApplyBatch;
   __shared__ ChainStage stage[kBatch];
@@ -1106,9 +1181,43 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
       add_ll(&P.ctr->tot_coag, (long long)done_ev);
       if (dlive) add_ll(&P.ctr->n_live, (long long)dlive);
       bool walk_done = ev_done[e] && done_ev == ev_len[e];
-      dest_out[e] = (walk_done || !on_grid) ? -1 : x;
-      gp_c[e] = (int)(pop_pair_base[pop] + last_q);
-      ev_pos[e] = last_pos;
+      const int4 t = ev_term[e];
+      if (on_grid && done_ev == ev_len[e] && t.x >= 0) {
+        // every event applied: the test where the chain stopped is pending
+        const int tq = t.y & (kTermFirst - 1);
+        const bool tfirst = (t.y & kTermFirst) != 0;
+        ev_key_w[e] = make_key((uint32_t)tq, 1u, (uint32_t)x);
+        ev_w[e] = tfirst ? make_int2(x, t.x) : make_int2(t.x, x);
+        gp_c[e] = (int)(pop_pair_base[pop] + tq);
+        ev_pos[e] = __int_as_float(t.w);
+        dec_w[e] = (uint32_t)t.z;
+        dest_out[e] = kPendingTerm;
+      } else if (on_grid && !stop && done_ev < ev_len[e]) {
+        // cut short where a partner's claim failed: that event is pending
+        ChainReader rd(ev_head[e]);
+        long long ix = -1;
+        for (int i = 0; i <= done_ev; i++) ix = rd.next(pool);
+        const int y = ix >= 0 ? pool.y[ix] : -1;
+        const int q = ix >= 0 ? (pool.q[ix] & kChainPairMask) : -1;
+        if (y >= 0 && y < P.cap && q >= 0 && q < P.n_pairs) {
+          const PairDesc d = P.pair_desc[q];
+          const bool first = C == d.b1 + nb * d.c1;
+          ev_key_w[e] = make_key((uint32_t)q, 1u, (uint32_t)x);
+          ev_w[e] = first ? make_int2(x, y) : make_int2(y, x);
+          gp_c[e] = (int)(pop_pair_base[pop] + q);
+          ev_pos[e] = pool.pos[ix];
+          dec_w[e] = (uint32_t)done_ev;
+          dest_out[e] = kPendingChain;
+        } else {
+          bad_index(P.ctr, kBadEventSlot, y);
+          dest_out[e] = -1;
+        }
+      } else {
+        // off the grid, or stopped by an error: no walk on
+        dest_out[e] = (walk_done || !on_grid || stop) ? -1 : x;
+        gp_c[e] = (int)(pop_pair_base[pop] + last_q);
+        ev_pos[e] = last_pos;
+      }
     }
     }
   }

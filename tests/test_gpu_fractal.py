@@ -112,10 +112,15 @@ def test_fractal_kmax_table(gpu_lib, shape, kt):
     assert np.array_equal(k_gpu[~nz], k_cpu[~nz])
     # the sedimentation kernel's |w1 - w2| cancels where both speeds are near
     # the cap: there the error is measured against a thousandth of the
-    # table's largest value instead of the entry
+    # table's largest value instead of the entry.  The fractal mobility
+    # radius is the root of a sum of nearly cancelling terms (Newton,
+    # fractal.F90:315-362), so the device's fused multiply-adds and the C
+    # library's separate roundings differ by more than in the spherical
+    # kernels: 1e-10 where the radius enters (Brownian, sedimentation)
     scale = np.maximum(np.abs(k_cpu[nz]), 1e-3 * np.abs(k_cpu).max())
     rel = np.abs(k_gpu[nz] - k_cpu[nz]) / scale
-    assert rel.max() < 1e-12, rel.max()
+    tol = 1e-10 if kt in (pm.COAG_KERNEL_TYPE_BROWN, pm.COAG_KERNEL_TYPE_SEDI) else 1e-12
+    assert rel.max() < tol, rel.max()
 
 
 def test_set_fractal_rejects_the_reference_stops(gpu_lib):

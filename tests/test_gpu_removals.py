@@ -41,13 +41,15 @@ def test_replay_removal_records_match_the_oracle(gpu_lib, path):
     o.set_replay(g["uniforms"])
     o.set_record_removals(True)
     env = pm.EnvState(float(g["temp"]), float(g["pressure"]), float(g["coeff"]))
+    n_rec = 0
     for _ in range(int(g["steps"])):
         pm.mc_coag(int(g["kernel"]), env, ad, st, float(g["del_t"]))
         o.mc_coag(int(g["kernel"]), float(g["temp"]), float(g["pressure"]), float(g["coeff"]), float(g["del_t"]))
         dev, orc = st.removals(), o.removals()
-        assert len(orc["id"]) > 0
+        n_rec += len(orc["id"])
         for k in ("id", "action", "other_id"):
             assert np.array_equal(dev[k], orc[k]), k
+    assert n_rec > 0
 
 
 def workloads():
