@@ -260,17 +260,23 @@ __global__ void k_build_ops(const PopDev* pops, const int* gpair_pop, const int*
 
 // redo list of lost target operations (order of q kept); a redo keeps its
 // place in the loop order (its key)
-__global__ void k_build_redo(const int* op_pop, const int* op_pair, const int* op_slot,
+__global__ void k_build_redo(const PopDev* pops, const int* op_pop, const int* op_pair, const int* op_slot,
                              const int* op_k, const unsigned long long* op_key, const int* lost,
-                             const long long* lost_off, long long Q, int* r_pop, int* r_pair, int* r_slot,
+                             const long long* lost_off, const long long* n_ops, int* r_pop, int* r_pair, int* r_slot,
                              int* r_k, unsigned long long* r_key) {
+  const long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
     if (!lost[q]) continue;
     long long j = lost_off[q];
+    const PopDev& P = pops[op_pop[q]];
+    const int t = op_slot[q];
     r_pop[j] = op_pop[q];
     r_pair[j] = op_pair[q];
-    r_slot[j] = op_slot[q];
+    // a target that an earlier operation or event of the round consumed
+    // (removed or rewrote) walks on from there instead: its redo is void
+    const bool consumed = t < 0 || t >= P.cap || !P.alive[t] || P.touched[t] == *P.gen_p;
+    r_slot[j] = consumed ? -1 : t;
     r_k[j] = op_k[q] + (1 << 24);  // fresh random stream for the redo
     r_key[j] = op_key[q];
   }
@@ -862,6 +868,13 @@ struct Ctx {
   DevBuf<float> it_pos;
   DevBuf<uint32_t> it_dec, it_gused;
   DevBuf<int4> it_term, ev_term;  // pending tests where chains stopped (kPendingTerm)
+  // walkers made by target operations (slot, global pair), read by the next
+  // round's k_items; their count is round_dev[5]
+  DevBuf<int> ppw_slot, ppw_gp;      // written by this round's k_pp_apply
+  DevBuf<int> ppw_slot_in, ppw_gp_in;  // read by this round's k_items (the round before's)
+  long long ppw_cap = 0;
+  long long op_cap = 0;   // room in the target-operation arrays this round
+  bool pp_step = false;   // the step has target operations (per-particle path)
   DevBuf<long long> it_off;
   // chain events of a round (ChainPool), in chunks
   DevBuf<int> ch_y, ch_q;
@@ -1188,6 +1201,7 @@ void alloc_sort(Ctx& c, PopHost& ph) {
     int* d_list = dalloc<int>(o, list.size());
     h.cp_cum = dalloc<double>(o, (size_t)off[h.n_cells] + h.n_cells);
     h.cp_ent = dalloc<int4>(o, std::max(off[h.n_cells], 1));
+    h.cp_nstop = dalloc<int>(o, std::max(off[h.n_cells], 1));
     h.cp_tab = dalloc<int>(o, (size_t)h.n_cells * kWalkTab);
     CK(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, c.stream));
@@ -1613,6 +1627,8 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
     using T = decltype(tt);
     auto k = flat ? k_items<KT, T, true> : k_items<KT, T, false>;
     k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
+                              c.round_dev.p + 6, c.ppw_slot_in.p, c.ppw_gp_in.p, c.op_pop.p, c.op_pair.p,
+                              c.op_slot.p, c.op_k.p, c.op_key.p, c.n_dev.p, c.op_cap,
                               c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
                               c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
                               c.it_done.p, c.it_dec.p, c.it_gused.p, c.it_term.p);
@@ -1820,11 +1836,17 @@ __global__ void k_round_begin(uint32_t* d_round, long long* round_dev, int* per_
   if (threadIdx.x == 0) {
     d_round[0] += 1u;
     d_round[1] += 1u;
-    round_dev[2] = round_dev[1];
+    // this round's items: the events of the round before, then the walkers
+    // its target operations made
+    round_dev[6] = round_dev[1];
+    round_dev[7] = round_dev[5];
+    round_dev[2] = round_dev[1] + round_dev[5];
     round_dev[0] = 0;
     round_dev[1] = 0;
     round_dev[3] = 0;
     round_dev[4] = 0;
+    round_dev[5] = 0;
+    round_dev[8] = 0;
   }
   for (int k = threadIdx.x; k < n_per_pop; k += blockDim.x) per_pop[k] = 0;
 }
@@ -1866,12 +1888,13 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
     scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}},
                     st);
   }
+  // Q bounds the round's target operations; their count is n_dev[0] (the
+  // redone ones, then those that walks appended)
   if (Q > 0) {
-    set_n_dev(c, Q);
     k_pp_resolve<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.op_key.p, c.n_dev.p, c.pp_res.p,
                                                    c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
     note_launch();
-    scan_multi<int>(c, {{c.need_slot_pp.p, Q, nullptr, c.rank_slot_pp.p}, {c.need_id_pp.p, Q, nullptr, c.rank_id_pp.p}},
+    scan_multi<int>(c, {{c.need_slot_pp.p, Q, c.n_dev.p, c.rank_slot_pp.p}, {c.need_id_pp.p, Q, c.n_dev.p, c.rank_id_pp.p}},
                     st);
     k_count_per_pop<<<grid_for(Q, 256), 256, 0, st>>>(c.need_slot_pp.p, c.n_dev.p, c.op_pop.p,
                                                       c.per_pop_i.p + 2 * c.n_pop);
@@ -1907,9 +1930,10 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   if (Q > 0) {
     k_pp_apply<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
                                                  c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p, c.slot_base_pp.p,
-                                                 c.id_base_pp.p);
+                                                 c.id_base_pp.p, c.pop_pair_base.p, c.ppw_slot.p, c.ppw_gp.p,
+                                                 c.round_dev.p + 5, c.ppw_cap);
     note_launch();
-    scan_multi<int>(c, {ScanArg<int>{c.lost_pp.p, Q, nullptr, c.lost_off.p}}, st);
+    scan_multi<int>(c, {ScanArg<int>{c.lost_pp.p, Q, c.n_dev.p, c.lost_off.p, c.round_dev.p + 8}}, st);
   }
 }
 
@@ -1926,19 +1950,21 @@ struct RoundBounds {
 // sort, items, their events in item order, then resolve and apply.  With
 // Q > 0 (host loop only) the round's per-particle redo operations claim
 // alongside.
-void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long Q) {
+// Qn: the round's redone target operations (host loop only); with
+// per-particle pairs in the step, walks append more (at most one per item),
+// so the operations are bounded by Qb = Qn + W and counted on the device.
+void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long Qn) {
   long long W = b.W;
+  const long long Q = c.pp_step ? Qn + W : Qn;
   launch_sort(c, st, b.max_chunks, b.max_cells);
   {
     dim3 g(b.max_cells, c.n_pop);
     k_walk_rates<<<g, 128, 0, st>>>(c.d_pops);
     note_launch();
   }
+  if (Q > 0) set_n_dev(c, Qn);
   launch_items_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
-  if (Q > 0) {
-    set_n_dev(c, Q);
-    launch_pp(c, b.kt, Q);
-  }
+  if (Q > 0) launch_pp(c, b.kt, Q);
   const long long* Id = c.round_dev.p + 2;
   long long* Ed = c.round_dev.p + 1;
   scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.it_flag.p, W, Id, c.it_off.p, Ed}}, st);
@@ -1961,7 +1987,7 @@ std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
           (long long)c.ev_app.p, (long long)c.ev_done.p, (long long)c.chain_list.p, (long long)c.it_flag.p, (long long)c.it_key.p,
           (long long)c.it_c.p, (long long)c.it_gp.p, (long long)c.it_pos.p, (long long)c.it_len.p,
           (long long)c.it_head.p, (long long)c.it_done.p, (long long)c.it_dec.p, (long long)c.it_gused.p, (long long)c.it_off.p,
-          (long long)c.it_term.p, (long long)c.ev_term.p,
+          (long long)c.it_term.p, (long long)c.ev_term.p, (long long)c.ppw_slot.p, (long long)c.ppw_gp.p,
           (long long)c.ch_y.p,
           (long long)c.ch_q.p, (long long)c.ch_pos.p, (long long)c.need_slot_set.p, (long long)c.need_id_set.p,
           (long long)c.win_set.p, (long long)c.dec_set.p, (long long)c.rank_slot_set.p, (long long)c.rank_id_set.p,
@@ -2189,7 +2215,10 @@ void step_parallel(Ctx& c, int kt) {
   c.id_base_set.reserve(c.n_pop);
   c.id_base_pp.reserve(c.n_pop);
   c.n_dev.reserve(4 + 2 * (size_t)c.n_pop);
-  c.round_dev.reserve(5);
+  // round_dev: [0] losers, [1] events, [2] items, [3] chain chunks, [4] chains,
+  // [5] walkers of target operations, [6] items that are events, [7] items
+  // that are such walkers, [8] target operations that lost a claim
+  c.round_dev.reserve(10);
   int max_pairs = 1, nb_max = 1, max_cap = 1;
   for (int k = 0; k < c.n_pop; k++) {
     max_pairs = std::max(max_pairs, c.pops[k].h.n_pairs);
@@ -2271,6 +2300,14 @@ void step_parallel(Ctx& c, int kt) {
     }
     W = hw[0];
     Q = hw[1];
+    // a step with target operations runs its later rounds from the host,
+    // where walks that reach a per-particle pair's target cell stop for one
+    c.pp_step = Q > 0;
+    for (int k = 0; k < c.n_pop; k++)
+      if (c.pops[k].h.walk_stops != (c.pp_step ? 1 : 0)) {
+        c.pops[k].h.walk_stops = c.pp_step ? 1 : 0;
+        c.dirty = true;
+      }
     if (c.n_pop == 1) {
       hw[3] = W;
       hw[4] = Q;
@@ -2290,12 +2327,18 @@ void step_parallel(Ctx& c, int kt) {
   {
     size_t w = (size_t)W;
     c.flag.reserve(w + 1); c.ev.reserve(w + 1); c.flag_off.reserve(w + 2); c.ev_gp.reserve(w + 1);
-    reserve_events(c, W);
+    // the walkers that target operations make (the target and its copies)
+    // join a later round's items and events
+    reserve_events(c, W + kMaxCopies * Q);
+    c.ppw_cap = kMaxCopies * (Q + 1);
+    c.ppw_slot.reserve((size_t)c.ppw_cap);
+    c.ppw_gp.reserve((size_t)c.ppw_cap);
+    c.op_cap = Q;
     c.need_slot_pp.reserve(Q + 1); c.need_id_pp.reserve(Q + 1); c.win_pp.reserve(Q + 1); c.lost_pp.reserve(Q + 1);
     c.lost_off.reserve(Q + 2); c.rank_slot_pp.reserve(Q + 2); c.rank_id_pp.reserve(Q + 2);
   }
   if (c.dirty) push_pops(c);
-  CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 5, c.stream));
+  CK(cudaMemsetAsync(c.round_dev.p, 0, sizeof(long long) * 10, c.stream));
   CK(cudaMemsetAsync(c.per_pop_i.p, 0, sizeof(int) * 4 * c.n_pop, c.stream));
   if (W > 0) {
     ProfScope ps(c, 0, W);
@@ -2328,16 +2371,21 @@ void step_parallel(Ctx& c, int kt) {
 
   // ---- later rounds: retries, walks and per-particle redo operations
   long long redraws = 0, E = 0, pp_lost = 0;
+  long long last_qb = Q;  // bound of the last round's target operations (0: it had none)
   int round = 0;
   bool graph_tried = false;
   for (;;) {
     // one read-back at the end of each host round
-    long long losers = 0;
+    long long losers = 0, ppw = 0;
     CK(cudaMemcpyAsync(&losers, c.round_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(&E, c.round_dev.p + 1, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-    long long Qr = round == 0 ? Q : pp_lost;
+    CK(cudaMemcpyAsync(&ppw, c.round_dev.p + 5, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    long long Qr = 0;
     pp_lost = 0;
-    if (Qr > 0) CK(cudaMemcpyAsync(&pp_lost, c.lost_off.p + Qr, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    if (last_qb > 0) {
+      CK(cudaMemcpyAsync(&pp_lost, c.round_dev.p + 8, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(&Qr, c.n_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    }
     CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
     unsigned long long scan_err = 0;
     CK(cudaMemcpyAsync(&scan_err, c.scan_err.p, sizeof(scan_err), cudaMemcpyDeviceToHost, c.stream));
@@ -2353,7 +2401,7 @@ void step_parallel(Ctx& c, int kt) {
     c.last_events += E;
     c.last_ops += Qr;
     round++;
-    if (E == 0 && pp_lost == 0) break;
+    if (E == 0 && pp_lost == 0 && ppw == 0) break;
     if (round >= c.max_rounds) {
       std::vector<PopCtr>& r = read_ctrs(c);
       for (int k = 0; k < c.n_pop; k++)
@@ -2361,10 +2409,15 @@ void step_parallel(Ctx& c, int kt) {
       write_ctrs(c);
       break;
     }
+    // this round's target operations: the redone ones, and with per-particle
+    // pairs in the step at most one more per item (a walk that stops there)
+    const long long Qb = pp_lost + (c.pp_step ? E + ppw : 0);
     // room for this round's new slots: at most one per item, and
     // kMaxCopies - 1 per target operation
-    ensure_room(c, E + (kMaxCopies - 1) * pp_lost);
-    if (!graph_tried && c.use_graph && pp_lost == 0) {
+    ensure_room(c, E + ppw + (kMaxCopies - 1) * Qb);
+    // a round's items (events and walkers) each make at most one event
+    if (!events_fit(c, E + ppw)) throw Fail(PMC_ERR_CAPACITY);
+    if (!graph_tried && c.use_graph && !c.pp_step && pp_lost == 0 && ppw == 0) {
       graph_tried = true;
       GraphRun g = run_round_graph(c, kt, flat, n_gpairs, E);
       if (g.rounds >= 0) {
@@ -2389,33 +2442,46 @@ void step_parallel(Ctx& c, int kt) {
       }
     }
     // one host-driven round
-    reserve_round(c, E);
+    reserve_round(c, E + ppw);
     long long Qn = pp_lost;
     if (Qn > 0) {
-      c.r_pop.reserve(Qn); c.r_pair.reserve(Qn); c.r_slot.reserve(Qn); c.r_k.reserve(Qn); c.r_key.reserve(Qn);
-      k_build_redo<<<grid_for(Qr, 256), 256, 0, c.stream>>>(c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
-                                                            c.op_key.p, c.lost_pp.p, c.lost_off.p, Qr, c.r_pop.p,
-                                                            c.r_pair.p, c.r_slot.p, c.r_k.p, c.r_key.p);
+      c.r_pop.reserve(Qb); c.r_pair.reserve(Qb); c.r_slot.reserve(Qb); c.r_k.reserve(Qb); c.r_key.reserve(Qb);
+      k_build_redo<<<grid_for(last_qb, 256), 256, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p,
+                                                                 c.op_k.p, c.op_key.p, c.lost_pp.p, c.lost_off.p,
+                                                                 c.n_dev.p, c.r_pop.p, c.r_pair.p, c.r_slot.p,
+                                                                 c.r_k.p, c.r_key.p);
       note_launch();
       std::swap(c.op_pop, c.r_pop); std::swap(c.op_pair, c.r_pair); std::swap(c.op_slot, c.r_slot);
       std::swap(c.op_k, c.r_k); std::swap(c.op_key, c.r_key);
-      c.pp_res.reserve(Qn);
-      c.pp_vol.reserve((size_t)Qn * c.n_spec);
-      c.need_slot_pp.reserve(Qn + 1); c.need_id_pp.reserve(Qn + 1); c.win_pp.reserve(Qn + 1);
-      c.lost_pp.reserve(Qn + 1); c.lost_off.reserve(Qn + 2); c.rank_slot_pp.reserve(Qn + 2);
-      c.rank_id_pp.reserve(Qn + 2);
+    } else if (Qb > 0) {
+      c.op_pop.reserve(Qb); c.op_pair.reserve(Qb); c.op_slot.reserve(Qb); c.op_k.reserve(Qb); c.op_key.reserve(Qb);
     }
+    if (Qb > 0) {
+      c.pp_res.reserve(Qb);
+      c.pp_vol.reserve((size_t)Qb * c.n_spec);
+      c.need_slot_pp.reserve(Qb + 1); c.need_id_pp.reserve(Qb + 1); c.win_pp.reserve(Qb + 1);
+      c.lost_pp.reserve(Qb + 1); c.lost_off.reserve(Qb + 2); c.rank_slot_pp.reserve(Qb + 2);
+      c.rank_id_pp.reserve(Qb + 2);
+    }
+    c.op_cap = Qb;
+    // the walkers the last round's operations made are this round's to read;
+    // this round's operations write theirs into the other pair of arrays
+    std::swap(c.ppw_slot, c.ppw_slot_in);
+    std::swap(c.ppw_gp, c.ppw_gp_in);
+    c.ppw_cap = kMaxCopies * (Qb + 1);
+    c.ppw_slot.reserve((size_t)c.ppw_cap);
+    c.ppw_gp.reserve((size_t)c.ppw_cap);
     // the round's sort covers the current slots exactly
     prepare_chunks(c);
     int mc = 1;
     for (int k = 0; k < c.n_pop; k++) mc = std::max(mc, c.pops[k].h.n_chunks);
     if (c.dirty) push_pops(c);
-    RoundBounds b{kt, flat, n_gpairs, E, mc, max_cells_of(c)};
+    RoundBounds b{kt, flat, n_gpairs, E + ppw, mc, max_cells_of(c)};
     k_round_begin<<<1, 128, 0, c.stream>>>(c.d_round, c.round_dev.p, c.per_pop_i.p, 4 * c.n_pop);
     note_launch();
     c.claim_gen++;  // as k_round_begin on the device
     enqueue_round_body(c, c.stream, b, Qn);
-    pp_lost = Qn;  // read back as this round's operations at the top of the loop
+    last_qb = Qb;
   }
   c.last_redraws = redraws;
   c.last_rounds = round;

@@ -495,18 +495,16 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
   double k_max = P.kmax_tab[b1 + nb * b2] * S.f_max;
   S.k_max = k_max;
   S.inv_k_max = 1.0 / k_max;
-  if (n1 == 0 || n2 == 0) {
-    S.path = kPathSkip;
-    nwork_set[gp] = nwork_pp[gp] = 0;
-    return;
-  }
   // try_per_particle_coag eligibility (coagulation.F90:191-217): the weight
-  // conditions were settled by k_pair_setup; the cell-count ones are here
+  // conditions were settled by k_pair_setup; the cell-count ones are here.
+  // A pair whose target cell is empty now but whose source cell is not is
+  // marked too: particles that reach the target cell during the step are
+  // its targets when the pair's turn comes (walks stop there).
   if (use_particle_path && P.mono_dec && S.pp_ok) {
     int ns = P.cell_count[S.bs + nb * S.cs];
     double nspt = k_max * P.del_t * (double)ns;
     double max_new = S.pp_min_tv + S.pp_max_sv * nspt;
-    if (nspt >= 1.0 && !(max_new / S.pp_min_tv > 1.5)) {
+    if (ns > 0 && nspt >= 1.0 && !(max_new / S.pp_min_tv > 1.5)) {
       S.path = kPathParticle;
       S.nspt = nspt;
       int nt = P.cell_count[S.bt + nb * S.ct];
@@ -514,6 +512,11 @@ __global__ void k_pairs(const PopDev* pops, const long long* pop_pair_base, long
       nwork_pp[gp] = nt;
       return;
     }
+  }
+  if (n1 == 0 || n2 == 0) {
+    S.path = kPathSkip;
+    nwork_set[gp] = nwork_pp[gp] = 0;
+    return;
   }
   // per_set_coag / compute_n_samp
   double n_possible = same ? (double)n1 * ((double)n2 - 1.0) / 2.0 : (double)n1 * (double)n2;

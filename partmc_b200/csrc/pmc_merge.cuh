@@ -429,6 +429,7 @@ struct WalkOut {
   uint32_t dec = 0;         // merge decision of the first event
   bool cont = false;        // the first event is an absorb: k_chain carries the walk on
   uint32_t g_used = 0;      // index of the walk's next test after the first event
+  bool stop = false;        // the walk reached a per-particle pair (q) whose target cell is its cell
 };
 
 // true if this round's claim on slot y is the chain of walker x
@@ -456,6 +457,7 @@ struct Stretch {
   const int* tab;
   int C, end, j;
   double at, total;
+  int stop;  // the stop (cp_nstop) that ends the stretch, or -1: it runs to the cell's last pair
 };
 
 // the stretch of cell C from (pair p0, position pos0 in it) on.  The first
@@ -481,11 +483,17 @@ __device__ __forceinline__ void walk_stretch(const PopDev& P, int C, int p0, flo
   a += cnt;
   double at = cum[a];
   if (a < end && P.cp_list[a] == p0) at += (cum[a + 1] - cum[a]) * (double)pos0;
+  // the stretch ends at the first stop after the start; a walk that starts
+  // at the end of a pair (its target operation there is done) looks past it
+  const int sa = (a < end && P.cp_list[a] == p0 && pos0 >= 1.0f) ? a + 1 : a;
+  const int stop = (P.walk_stops && sa < end) ? P.cp_nstop[sa] : end;
   s->cum = cum;
   s->tab = P.cp_tab + (size_t)C * kWalkTab;
   s->C = C;
+  s->stop = stop < end ? stop : -1;
+  if (stop < end) end = stop;
   s->end = end;
-  s->j = a < end ? a : end - 1;
+  s->j = a < end ? a : (end > P.cp_off[C] ? end - 1 : end);
   s->at = at;
   s->total = cum[end];
 }
@@ -601,6 +609,10 @@ __device__ __forceinline__ int walk_next(const PopDev& P, int x, Stretch& s, uin
     double at = s.at - log(u53(u.x, u.y));
     if (!(at < s.total)) {
       s.at = at;
+      if (s.stop >= 0) {  // a per-particle pair that takes the particle as a target
+        *q = P.cp_list[s.stop];
+        return 3;
+      }
       return 0;  // no test left in the cell's later pairs
     }
     if (t >= (1u << 26)) {  // far past any mean the step can ask for
@@ -639,6 +651,10 @@ __device__ void walk(const PopDev& P, int x, int p0, float pos0, WalkOut* out) {
   double ry, vty;
   int r = walk_next<KT, T, FLAT>(P, x, s, t_next, qxd, qxf, false, &n_tests, &y, &pos, &q, &first, &ry, &vty);
   if (r == 0) out->done = true;
+  if (r == 3) {
+    out->stop = true;
+    out->q = q;
+  }
   if (r == 1) {
     const PairDesc d = P.pair_desc[q];
     const PairState& S = P.pair[q];
@@ -667,6 +683,44 @@ __device__ void walk(const PopDev& P, int x, int p0, float pos0, WalkOut* out) {
   }
 }
 
+// A chain's event i again, for the pending event of a chain cut short: the
+// decision the walk made, from the chain's stream and the particles' values
+// (0xffffffff for a bad pair index)
+__device__ __noinline__ uint32_t chain_event_decision(const PopDev& P, unsigned long long key, int2 sl, int x, int y,
+                                                      uint32_t i) {
+  const int q = (int)key_pair(key);
+  if (q >= P.n_pairs) {
+    bad_index(P.ctr, kBadEventSlot, q);
+    return 0xffffffffu;
+  }
+  const PairDesc d = P.pair_desc[q];
+  const PairState& S = P.pair[q];
+  Rng g = make_rng(P, kStreamChain, i + 1u, (uint32_t)x);
+  MergeDecision m = sl.x == x ? merge_decide_v(P, g, P.rad[x], P.vtot[x], P.rad[y], P.vtot[y], d.c1, d.c2, S.cc)
+                              : merge_decide_v(P, g, P.rad[y], P.vtot[y], P.rad[x], P.vtot[x], d.c1, d.c2, S.cc);
+  if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
+  return pack_decision(m, g.used());
+}
+
+// A target operation for particle x at per-particle pair q (its walk reached
+// the pair with x in the pair's target cell), appended to the round's
+// operations after the redone ones; it runs in this round.  Its key puts it
+// after the pair's own operations.
+__device__ __noinline__ void add_target_op(const PopDev& P, int pop, int q, int x, int* op_pop, int* op_pair,
+                                              int* op_slot, int* op_k, unsigned long long* op_key, long long* n_ops,
+                                              long long op_cap) {
+  const unsigned long long k = atomicAdd((unsigned long long*)n_ops, 1ULL);
+  if ((long long)k >= op_cap) {
+    set_status(P.ctr, kErrCapacity);
+    return;
+  }
+  op_pop[k] = pop;
+  op_pair[k] = q;
+  op_slot[k] = x;
+  op_k[k] = 0x40000000 | x;  // its own stream: round-0 operations count from 0, redos add 1 << 24
+  op_key[k] = make_key((uint32_t)q, 1u, (uint32_t)x);
+}
+
 // The work of a later round, one thread per event e of the round before:
 //   - a winner that created or changed a particle (dest[e] >= 0): that
 //     particle walks from the event's pair and position (for a chain, its
@@ -683,17 +737,46 @@ __device__ void walk(const PopDev& P, int x, int p0, float pos0, WalkOut* out) {
 template <int KT, class T, bool FLAT>
 __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gpair_pop, const int* gpair_local,
                                                const long long* pop_pair_base, int n_gpairs, const long long* n_items,
+                                               const long long* n_items_ev, const int* ppw_slot, const int* ppw_gp,
+                                               int* op_pop, int* op_pair, int* op_slot, int* op_k,
+                                               unsigned long long* op_key, long long* n_ops, long long op_cap,
                                                const uint8_t* win, const int* dest,
                                                const unsigned long long* ev_key, const int2* ev_c,
                                                const int* gp_c, const float* ev_pos, const uint32_t* dec,
                                                uint8_t* it_flag, unsigned long long* it_key,
                                                int2* it_c, int* it_gp, float* it_pos, int* it_len, int* it_head,
                                                uint8_t* it_done, uint32_t* it_dec, uint32_t* it_gused, int4* it_term) {
-  long long n = *n_items;
+  long long n = *n_items, n_ev = *n_items_ev;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
     it_flag[e] = 0;
     it_term[e] = no_term();
+    if (e >= n_ev) {
+      // a particle that a target operation of the round before made or
+      // changed walks from the end of that operation's pair
+      const int gp = ppw_gp[e - n_ev], x = ppw_slot[e - n_ev];
+      if (gp < 0 || gp >= n_gpairs) {
+        bad_index(pops[0].ctr, kBadEventSlot, gp);
+        continue;
+      }
+      const int pop = gpair_pop[gp];
+      const PopDev& P = pops[pop];
+      WalkOut w;
+      walk<KT, T, FLAT>(P, x, gpair_local[gp], 1.0f, &w);
+      if (w.stop) add_target_op(P, pop, w.q, x, op_pop, op_pair, op_slot, op_k, op_key, n_ops, op_cap);
+      if (!w.found) continue;
+      it_flag[e] = 1;
+      it_key[e] = make_key((uint32_t)w.q, 1u, (uint32_t)x);
+      it_c[e] = w.first_cell1 ? make_int2(x, w.y) : make_int2(w.y, x);
+      it_gp[e] = (int)(pop_pair_base[pop] + w.q);
+      it_pos[e] = w.pos;
+      it_len[e] = w.cont ? -1 : 0;
+      it_head[e] = -1;
+      it_done[e] = w.done ? 1 : 0;
+      it_dec[e] = w.dec;
+      it_gused[e] = w.g_used;
+      continue;
+    }
     int gp = gp_c[e];
     if (gp < 0 || gp >= n_gpairs) {
       bad_index(pops[0].ctr, kBadEventSlot, gp);
@@ -721,20 +804,8 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
         walker = x;
         p0 = (int)key_pair(key);
       } else if (dest[e] == kPendingChain) {
-        // the chain's event again, decided as the walk decided it
-        const int q = (int)key_pair(key);
-        if (q >= P.n_pairs) {
-          bad_index(P.ctr, kBadEventSlot, q);
-          continue;
-        }
-        const PairDesc d = P.pair_desc[q];
-        const PairState& S = P.pair[q];
-        Rng g = make_rng(P, kStreamChain, dec[e] + 1u, (uint32_t)x);
-        MergeDecision m = sl.x == x
-                              ? merge_decide_v(P, g, P.rad[x], P.vtot[x], P.rad[y], P.vtot[y], d.c1, d.c2, S.cc)
-                              : merge_decide_v(P, g, P.rad[y], P.vtot[y], P.rad[x], P.vtot[x], d.c1, d.c2, S.cc);
-        if (m.new_group == 0) set_status(P.ctr, kErrTimeout);
-        pend_dec = pack_decision(m, g.used());
+        pend_dec = chain_event_decision(P, key, sl, x, y, dec[e]);
+        if (pend_dec == 0xffffffffu) continue;
       }
     } else if (win[e]) {
       walker = dest[e];
@@ -766,6 +837,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     if (walker >= 0) {
       WalkOut w;
       walk<KT, T, FLAT>(P, walker, p0, pos0, &w);
+      if (w.stop) add_target_op(P, pop, w.q, walker, op_pop, op_pair, op_slot, op_k, op_key, n_ops, op_cap);
       if (!w.found) continue;
       key = make_key((uint32_t)w.q, 1u, (uint32_t)walker);
       sl = w.first_cell1 ? make_int2(walker, w.y) : make_int2(w.y, walker);
@@ -1227,6 +1299,10 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
 // pairs (loop order) of k_max * del_t * members of the pair's other cell;
 // pairs on the per-particle path add nothing.  One block per cell, its
 // threads over the cell's pairs, a block-wide scan in a fixed order.
+// P.walk_stops: 1 when the step has target operations (its later rounds run
+// from the host and take the operations that walks stop for); with 0,
+// per-particle pairs (whose target cells were all empty at the step's start)
+// are walked at the per-set rate like any pair.
 __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int c = blockIdx.x;
@@ -1237,6 +1313,7 @@ __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
   __shared__ double wsum[4];
   __shared__ double carry;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int stops = P.walk_stops;
   if (threadIdx.x == 0) carry = 0.0;
   __syncthreads();
   for (int base = lo; base < hi; base += blockDim.x) {
@@ -1250,7 +1327,12 @@ __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
       int O = cell1 == c ? cell2 : cell1;
       int n_o = P.cell_count[O];
       P.cp_ent[j] = make_int4(q, O | (cell1 == c ? (1 << 30) : 0), P.cell_start[O], n_o);
-      if (S.path != kPathParticle) {
+      // per-set pairs, and per-particle pairs seen from their source cell: a
+      // particle that arrives in the cell meets the other cell's members at
+      // the per-set rate.  Seen from its target cell a per-particle pair is a
+      // stop (no rate, cp_nstop): a particle that arrives there is one of
+      // its targets, and its walk ends at the pair in a target operation
+      if (!(stops && S.path == kPathParticle && c == S.bt + nb * S.ct)) {
         double l = S.k_max * P.del_t * (double)n_o;
         if (l > 0.0) lam = l;
       }
@@ -1271,6 +1353,15 @@ __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
   }
   const double total = carry;
   if (threadIdx.x == 0) cum[hi - lo] = total;
+  if (threadIdx.x == 0 && stops) {
+    // per entry, the first stop at or after it (hi: none)
+    int nxt = hi;
+    for (int j = hi - 1; j >= lo; j--) {
+      const PairState& S = P.pair[P.cp_list[j]];
+      if (stops && S.path == kPathParticle && c == S.bt + nb * S.ct) nxt = j;
+      P.cp_nstop[j] = nxt;
+    }
+  }
   // the bucket table: the last entry whose stretch starts at or before each
   // bucket's start (cum is visible to the block after the barrier above)
   if (threadIdx.x < kWalkTab) {
@@ -1328,7 +1419,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     R.merged = 0;
     R.n_copies = 1;
     R.n_rm = 0;
-    if (!P.alive[t]) continue;
+    if (t < 0 || t >= P.cap || !P.alive[t]) continue;  // t = -1: a redo voided by k_build_redo
     const PairState& S = P.pair[p];
     const GridDev& G = *P.grid;
     int nb = G.n_bin;
@@ -1530,7 +1621,8 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
 __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long long* n_ops,
                            const PPResult* res, const double* res_vol, const uint8_t* win,
                            const long long* slot_rank, const long long* id_rank,
-                           const int* slot_base, const long long* id_base) {
+                           const int* slot_base, const long long* id_base, const long long* pop_pair_base,
+                           int* ppw_slot, int* ppw_gp, long long* ppw_n, long long ppw_cap) {
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
@@ -1561,8 +1653,21 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
         kill_slot(P, t);
         dlive--;
       } else {
+        // the changed target and its copies take part in the rest of the
+        // step: they walk from the end of this pair in the next round
+        const int wgp = (int)(pop_pair_base[pop] + R.p);
+        auto add_walker = [&](int slot) {
+          const unsigned long long k = atomicAdd((unsigned long long*)ppw_n, 1ULL);
+          if ((long long)k < ppw_cap) {
+            ppw_slot[k] = slot;
+            ppw_gp[k] = wgp;
+          } else {
+            set_status(P.ctr, kErrCapacity);
+          }
+        };
         store_particle(P, t, v, R.meta);
         refresh_slot(P, t);
+        add_walker(t);
         for (int z = 1; z < R.n_copies; z++) {
           int dest = slot_base[pop] + (int)slot_rank[q] + (z - 1);
           if (dest >= P.cap) {
@@ -1575,6 +1680,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
           store_particle(P, dest, v, cm);
           refresh_slot(P, dest);
           P.touched[dest] = gen;
+          add_walker(dest);
           dlive++;
         }
       }

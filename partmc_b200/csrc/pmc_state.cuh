@@ -206,6 +206,11 @@ struct PopDev {
   // with the rates, per entry j of the lists: {pair, other cell (bit 30 set
   // if this cell is the pair's first), the other cell's start and members}
   int4* cp_ent;        // [cp_off[n_cells]]
+  // per entry j of a cell's list, the first entry at or after j whose pair is
+  // on the per-particle path with this cell as its target cell (a walk stops
+  // there for a target operation); the cell's end if none
+  int* cp_nstop;       // [cp_off[n_cells]], valid when walk_stops
+  int walk_stops;      // the step has target operations: walks stop at per-particle pairs
   // per cell, kWalkTab buckets of its stretch of tests: entry b is the last
   // j of the cell with cp_cum[j] <= b / kWalkTab of the cell's total
   int* cp_tab;         // [n_cells * kWalkTab]
