@@ -407,31 +407,34 @@ __global__ void k_download(PopDev P, const long long* live_off, int n_slots, dou
   }
 }
 
-// Changed slots of [0, n_range) packed for the host copy, one record of
-// rec_bytes = kSyncHead + 8 n_spec bytes rounded up to a multiple of 16 (the
-// header is stored as one 16-byte vector): {slot, alive, group, class,
-// n_primary, 0, id (8 bytes)} then the species volumes.  Each warp takes 32 slots,
-// reserves places for its changed ones with one atomic, and copies each
-// changed slot's volumes with one lane per species (coalesced); record order
-// is arbitrary (the host scatters by slot).  Clears the changed flags.
+// Changed slots of [lo, hi) packed for the host copy, one record of
+// rec_bytes = kSyncHead + 8 n_spec bytes rounded up to a multiple of 16:
+// {slot, alive, group, class, n_primary, 0, id (8 bytes)} then the species
+// volumes.  Each warp takes 32 slots and reserves places for its changed
+// ones with one atomic; it assembles their records in shared memory (one
+// lane per species for the volumes) and writes them out as consecutive
+// 16-byte words, so that a write into host memory goes over the bus in full
+// lines.  Record order is arbitrary (the host scatters by slot).  Clears the
+// changed flags.
 constexpr int kSyncHead = 32;
-__global__ void k_pack_changed(PopDev P, int n_range, unsigned long long* count, unsigned char* out,
+__global__ void k_pack_changed(PopDev P, int lo, int hi, unsigned long long* count, unsigned char* out,
                                int rec_bytes) {
+  extern __shared__ int4 pack_stage[];  // [warps of the block][32 records]
   const int lane = threadIdx.x & 31;
+  unsigned char* my = (unsigned char*)pack_stage + (size_t)(threadIdx.x >> 5) * 32 * rec_bytes;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n_range; base += warps * 32) {
+  for (int base = lo + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < hi; base += warps * 32) {
     const int i = base + lane;
-    const bool ch = i < n_range && P.changed[i];
+    const bool ch = i < hi && P.changed[i];
     const unsigned m = __ballot_sync(0xffffffffu, ch);
     if (!m) continue;
     unsigned long long b = 0;
     if (lane == 0) b = atomicAdd(count, (unsigned long long)__popc(m));
     b = __shfl_sync(0xffffffffu, b, 0);
     if (ch) {
-      unsigned char* r = out + (size_t)(b + __popc(m & ((1u << lane) - 1u))) * rec_bytes;
+      unsigned char* r = my + (size_t)__popc(m & ((1u << lane) - 1u)) * rec_bytes;
       const int a = P.alive[i];
-      int4 h = make_int4(i, a, a ? P.grp[i] : 0, a ? P.cls[i] : 0);
-      *(int4*)r = h;
+      *(int4*)r = make_int4(i, a, a ? P.grp[i] : 0, a ? P.cls[i] : 0);
       *(int2*)(r + 16) = make_int2(a ? P.nprim[i] : 0, 0);
       *(long long*)(r + 24) = a ? P.id[i] : 0;
       P.changed[i] = 0;
@@ -440,9 +443,15 @@ __global__ void k_pack_changed(PopDev P, int n_range, unsigned long long* count,
       const int src = __ffs(mm) - 1;
       const int si = base + src;
       if (!P.alive[si]) continue;
-      double* v = (double*)(out + (size_t)(b + __popc(m & ((1u << src) - 1u))) * rec_bytes + kSyncHead);
+      double* v = (double*)(my + (size_t)__popc(m & ((1u << src) - 1u)) * rec_bytes + kSyncHead);
       for (int sp = lane; sp < P.n_spec; sp += 32) v[sp] = P.vol[vol_at(P, si, sp)];
     }
+    __syncwarp();
+    const int n16 = __popc(m) * (rec_bytes / 16);
+    int4* d = (int4*)(out + (size_t)b * rec_bytes);
+    const int4* sm = (const int4*)my;
+    for (int k = lane; k < n16; k += 32) d[k] = sm[k];
+    __syncwarp();
   }
 }
 
@@ -722,6 +731,31 @@ struct PinnedBuf {
   }
 };
 
+// page-locked host memory that the device writes directly (mapped into the
+// device's address space), grown on demand
+struct MappedBuf {
+  void* p = nullptr;    // host address
+  void* dev = nullptr;  // device address of the same memory
+  size_t bytes = 0;
+  void reserve(size_t b) {
+    if (b <= bytes) return;
+    release();
+    size_t want = std::max<size_t>(b + b / 4, 1 << 20);
+    if (cudaHostAlloc(&p, want, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&dev, p, 0) != cudaSuccess) {
+      cudaGetLastError();
+      release();
+      throw Fail(PMC_ERR_CAPACITY);
+    }
+    bytes = want;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = dev = nullptr;
+    bytes = 0;
+  }
+};
+
 // Persistent host workers for the scatter of pmc_coag_gpu_sync_host: run(n,
 // f) calls f(q, n) for q = 0..n-1 on n threads (the caller's among them) and
 // returns when all are done.
@@ -900,9 +934,9 @@ struct Ctx {
   DevBuf<int> st_i;
   DevBuf<long long> st_l;
   PinnedBuf pin;  // host staging of the changed slots
-  DevBuf<unsigned char> st_rec;             // packed changed slots (k_pack_changed)
+  MappedBuf map;  // packed changed slots, written by the device into host memory
+  cudaEvent_t sync_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // chunks of a host sync
   DevBuf<unsigned long long> st_cnt;        // their count
-  long long sync_guess = 0;                 // records copied with the count (the last sync's count)
   std::unique_ptr<HostPool> pool;           // scatter workers
   long long h_total = 0;
   // stats of the last step
@@ -2650,9 +2684,11 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.st_d.release();
   c.st_i.release();
   c.st_l.release();
-  c.st_rec.release();
   c.st_cnt.release();
   c.pin.release();
+  c.map.release();
+  for (auto& ev : c.sync_ev)
+    if (ev) cudaEventDestroy(ev);
   replay_free(c.replay);
   free_redraw_graph(c);
   c.graph_stats.release();
@@ -3124,53 +3160,59 @@ int pmc_coag_gpu_sync_host(pmc_coag_gpu_ctx* x, int pop, int cap, double* vol, i
   if (range > ph.h.cap) range = ph.h.cap;
   long long total = 0;
   if (range > 0) {
-    // pack the changed slots into records on the device (one kernel), then
-    // copy the count together with as many records as the last sync had
-    // (one stream sync when the guess holds), the rest if it did not
+    // pack the changed slots into records that the device writes straight
+    // into page-locked host memory (room for every slot of the range), so
+    // the records cross the bus while the kernel runs.  The range goes in
+    // up to four chunks: after each, a copy of the running record count and
+    // an event, so the host scatters one chunk's records while the device
+    // packs the next
     const int rec = (kSyncHead + 8 * ns + 15) & ~15;  // keeps every record's header 16-byte aligned
-    c.st_rec.reserve((size_t)range * rec);
+    c.map.reserve((size_t)range * rec);
     c.st_cnt.reserve(1);
-    CK(cudaMemsetAsync(c.st_cnt.p, 0, sizeof(unsigned long long), c.stream));
-    k_pack_changed<<<grid_for(range, 256), 256, 0, c.stream>>>(ph.h, range, c.st_cnt.p, c.st_rec.p, rec);
-    note_launch();
-    long long guess = std::min<long long>(range, c.sync_guess + c.sync_guess / 8 + 256);
-    c.pin.reserve(64 + (size_t)std::max<long long>(guess, 1) * rec);
+    c.pin.reserve(64);
+    for (auto& ev : c.sync_ev)
+      if (!ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    const int n_chunk = range >= (1 << 18) ? 4 : 1;
+    const int wpb = std::max(1, std::min(4, (int)(48 * 1024 / (32 * rec))));  // warps per block
+    const size_t smem = (size_t)wpb * 32 * rec;
     unsigned long long* h_cnt = (unsigned long long*)c.pin.p;
-    unsigned char* h_rec = (unsigned char*)c.pin.p + 64;
-    CK(cudaMemcpyAsync(h_cnt, c.st_cnt.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(h_rec, c.st_rec.p, (size_t)guess * rec, cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
-    total = (long long)*h_cnt;
-    if (total > guess) {
-      std::vector<unsigned char> keep((size_t)guess * rec);
-      memcpy(keep.data(), h_rec, keep.size());
-      c.pin.reserve(64 + (size_t)total * rec);
-      h_rec = (unsigned char*)c.pin.p + 64;
-      memcpy(h_rec, keep.data(), keep.size());
-      CK(cudaMemcpyAsync(h_rec + (size_t)guess * rec, c.st_rec.p + (size_t)guess * rec,
-                         (size_t)(total - guess) * rec, cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaStreamSynchronize(c.stream));
+    const unsigned char* h_rec = (const unsigned char*)c.map.p;
+    CK(cudaMemsetAsync(c.st_cnt.p, 0, sizeof(unsigned long long), c.stream));
+    for (int k = 0; k < n_chunk; k++) {
+      const int lo = (int)((long long)range * k / n_chunk), hi = (int)((long long)range * (k + 1) / n_chunk);
+      k_pack_changed<<<grid_for(hi - lo, 32 * wpb), 32 * wpb, smem, c.stream>>>(ph.h, lo, hi, c.st_cnt.p,
+                                                                                (unsigned char*)c.map.dev, rec);
+      note_launch();
+      CK(cudaMemcpyAsync(h_cnt + k, c.st_cnt.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaEventRecord(c.sync_ev[k], c.stream));
     }
-    c.sync_guess = total;
-    // scatter into the caller's slot-indexed arrays
-    const std::function<void(int, int)> work = [&](int q, int nq) {
-      const long long j1 = total * (q + 1) / nq;
-      for (long long j = total * q / nq; j < j1; j++) {
-        const unsigned char* e = h_rec + (size_t)j * rec;
-        const int* hd = (const int*)e;
-        const int sl = hd[0];
-        alive[sl] = (uint8_t)hd[1];
-        if (!hd[1]) continue;
-        group[sl] = hd[2];
-        cls[sl] = hd[3];
-        n_primary[sl] = hd[4];
-        memcpy(&id[sl], e + 24, sizeof(long long));
-        memcpy(vol + (size_t)sl * ns, e + kSyncHead, sizeof(double) * ns);
-      }
-    };
-    int n_thr = total > 16384 ? (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    // scatter each chunk's records into the caller's slot-indexed arrays
+    long long j0 = 0;
+    const int n_thr = (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
     if (!c.pool) c.pool.reset(new HostPool());
-    c.pool->run(n_thr, work);
+    for (int k = 0; k < n_chunk; k++) {
+      CK(cudaEventSynchronize(c.sync_ev[k]));
+      const long long j1 = (long long)h_cnt[k];
+      const long long nk = j1 - j0;
+      const std::function<void(int, int)> work = [&](int q, int nq) {
+        const long long a1 = j0 + nk * (q + 1) / nq;
+        for (long long j = j0 + nk * q / nq; j < a1; j++) {
+          const unsigned char* e = h_rec + (size_t)j * rec;
+          const int* hd = (const int*)e;
+          const int sl = hd[0];
+          alive[sl] = (uint8_t)hd[1];
+          if (!hd[1]) continue;
+          group[sl] = hd[2];
+          cls[sl] = hd[3];
+          n_primary[sl] = hd[4];
+          memcpy(&id[sl], e + 24, sizeof(long long));
+          memcpy(vol + (size_t)sl * ns, e + kSyncHead, sizeof(double) * ns);
+        }
+      };
+      c.pool->run(nk > 4096 ? n_thr : 1, work);
+      j0 = j1;
+    }
+    total = j0;
   }
   ph.mirror_slots = r.n_slots;
   if (n_changed) *n_changed = (int)total;
