@@ -303,6 +303,41 @@ def aggregate(d, samp, sec, ws):
     return d
 
 
+def run_ic_sample(pm, pop, n_part, ws, reps=3):
+    import torch
+    from partmc_b200 import aero_dist
+    rng = np.random.default_rng(3)
+    sig = rng.uniform(1.5, 2.0, size=3)
+    n_spec = pop.aero_data.n_spec
+    frac = np.full(n_spec, 1.0 / n_spec)
+    modes = [pm.AeroMode(pm.AERO_MODE_TYPE_LOG_NORMAL, d / 2.0, np.log10(sig[k]), nc, vol_frac=frac,
+                         vol_frac_std=0.1 * frac)
+             for k, (d, nc) in enumerate(((0.02e-6, 1e10), (0.1e-6, 1e9), (0.5e-6, 1e8)))]
+    dev_s, host_s, n_dev = [], [], 0
+    for k in range(reps):
+        st = pm.AeroState(pop.aero_data, pm.AeroWeightArray.nummass(), seed=40 + k)
+        st.set_n_part_ideal(n_part)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_dev = st.add_aero_dist_sample(pm.AeroDist(modes))
+        torch.cuda.synchronize()
+        dev_s.append(time.perf_counter() - t0)
+        del st
+        st = pm.AeroState(pop.aero_data, pop.awa, seed=40 + k)
+        t0 = time.perf_counter()
+        hp = aero_dist.brown_20spec(n_part, seed=40 + k)
+        st.add_particles(hp.vol, hp.group)
+        torch.cuda.synchronize()
+        host_s.append(time.perf_counter() - t0)
+        del st
+    return {"particles": n_dev, "device_ms": 1e3 * float(np.median(dev_s)),
+            "host_numpy_and_upload_ms": 1e3 * float(np.median(host_s)),
+            "particles_per_s": n_dev / float(np.median(dev_s)),
+            "what": "pmc_coag_gpu_add_dist_sample of three log-normal modes, 20 species with fraction "
+                    "deviations, nummass weights prepared for the ideal count, wall clock with a device "
+                    "synchronize; against numpy sampling on the host plus upload"}
+
+
 def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     """Secondary lines: the plain FP64 step, the batched forms and the two
     end-to-end measurements through the C ABI."""
@@ -386,6 +421,38 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     torch.cuda.synchronize()
     res_s = time.perf_counter() - t0
     del mirror, str_
+
+    # the same resident path in FP64 mode, for an end-to-end figure at
+    # matched precision
+    str64 = new_state(pm.MODE_FP64)
+    mirror = pm.HostMirror(str64, alloc=lambda shape, dt: pinned(shape, torch.from_numpy(np.empty(0, dt)).dtype))
+    mirror.sync()
+    for _ in range(args.warmup):
+        pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, str64, args.del_t)
+        mirror.sync()
+    barrier(ws)
+    torch.cuda.synchronize()
+    r64_samp, r64_d2h = 0, 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        a, _ = pm.mc_coag(pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, str64, args.del_t)
+        n_changed, _ = mirror.sync()
+        r64_samp += a
+        r64_d2h += 8 + n_changed * rec
+    torch.cuda.synchronize()
+    r64_s = time.perf_counter() - t0
+    del mirror, str64
+    out["e2e_fp64"] = aggregate({"unit": "pair-tests/s", "h2d_bytes_per_step": 16,
+                                 "d2h_bytes_per_step": int(r64_d2h / max(args.steps, 1)),
+                                 "path": "as e2e, FP64 mode",
+                                 "ms_per_step": 1e3 * r64_s / max(args.steps, 1)}, r64_samp, r64_s, ws)
+
+    # the initial condition on the device: the benchmark's three log-normal
+    # modes (20 species, fraction deviations 0.1 of each fraction) sampled
+    # into an empty nummass state with an ideal of n_part particles
+    # (aero_state_add_aero_dist_sample), against drawing the population in
+    # numpy on the host and uploading it
+    out["ic_sample"] = run_ic_sample(pm, pop, args.n_part, ws)
 
     # serving (cfg 5): Poisson arrivals at 50 jobs/s, 1e3..1e6 particles,
     # additive / Brownian / sedimentation, 10..200 steps each of the step

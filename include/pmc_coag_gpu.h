@@ -50,8 +50,14 @@ extern "C" {
 #define PMC_KERNEL_CONSTANT 3
 #define PMC_KERNEL_BROWN 4
 #define PMC_KERNEL_ZERO 5
-#define PMC_KERNEL_BROWN_FREE 6  /* coag_kernel_brown_free.F90, spherical fractal parameters */
-#define PMC_KERNEL_BROWN_CONT 7  /* coag_kernel_brown_cont.F90, spherical fractal parameters */
+#define PMC_KERNEL_BROWN_FREE 6  /* coag_kernel_brown_free.F90, with the context's fractal parameters */
+#define PMC_KERNEL_BROWN_CONT 7  /* coag_kernel_brown_cont.F90, with the context's fractal parameters */
+
+/* aerosol mode types, aero_mode.F90:31-37 */
+#define PMC_AERO_MODE_LOG_NORMAL 1
+#define PMC_AERO_MODE_EXP 2
+#define PMC_AERO_MODE_MONO 3
+#define PMC_AERO_MODE_SAMPLED 4
 
 /* weight types, aero_weight.F90:24-30 */
 #define PMC_WEIGHT_NONE 1
@@ -185,6 +191,58 @@ int pmc_coag_gpu_set_weight_pop(pmc_coag_gpu_ctx *ctx, int pop,
 int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx *ctx, int pop,
                            const double *n_part_ideal, int allow_doubling,
                            int allow_halving);
+
+/* aero_state_add_aero_dist_sample (aero_state.F90:758-831) on the device:
+ * add a Poisson sample of a distribution of n_mode modes to population
+ * `pop`, with the given sample proportion, characteristic factor and
+ * creation time.  For every weight group and then every mode, in the
+ * reference's order, the mode's expected number of computational particles
+ * is sample_prop * aero_mode_number (aero_mode.F90:495-546) under the weight
+ * of (group, class); the class is the mode's source when the context has
+ * more than one class, else 1 (aero_state_weight_class_for_source,
+ * aero_state.F90:263-282).  With n_part_ideal (n_group x n_class, the
+ * layout of the weights; NULL skips this) the weight is first prepared as
+ * aero_state_prepare_weight_for_add does (:704-752): if the members of
+ * (group, class) plus the expected new ones fall outside [ideal/2, 2 ideal],
+ * the weight is scaled to bring them to ideal, halving (a uniform random
+ * subset removed, recorded as AERO_INFO_HALVED) or doubling (each member
+ * copied to prob_round(1/ratio) particles) the members as
+ * aero_state_scale_weight does (:1859-1922) when allow_halving /
+ * allow_doubling permit it or the group is empty.  Each particle's radius
+ * comes from aero_mode_sample_radius (aero_mode.F90:550-630; log-normal
+ * draws truncated at min(1 / (characteristic_factor * mean), 0.32)), its
+ * volume from the context's particle shape (aero_data_rad2vol), its species
+ * volumes from aero_mode_sample_vols (:633-665); it gets a new ID, one
+ * component (source, create_time) and one primary particle.
+ * Mode arrays, one entry per mode: mode_type (PMC_AERO_MODE_*),
+ * char_radius (m), log10_std (log10 of the geometric standard deviation;
+ * log-normal modes, may be NULL otherwise), num_conc (m^-3), vol_frac and
+ * vol_frac_std (n_mode x n_spec, mode-major; vol_frac_std may be NULL for
+ * all zero), source (1-based; NULL: mode m has source m + 1, one source per
+ * named mode as aero_mode_read assigns them).  Sampled modes: n_sample[m]
+ * intervals, their n_sample[m] + 1 radius edges (m) concatenated over the
+ * sampled modes in sample_radius, their number concentrations (m^-3)
+ * concatenated in sample_num_conc; n_sample may be NULL when no mode is
+ * sampled.  n_part_add (may be NULL) receives the number of particles
+ * added.  Exponential modes need flat weights (die_msg(822252601) in the
+ * reference).  The draws come from the population's counter-based stream,
+ * keyed by its seed, its step count and the call. */
+int pmc_coag_gpu_add_dist_sample(pmc_coag_gpu_ctx *ctx, int pop, int n_mode,
+                                 const int *mode_type,
+                                 const double *char_radius,
+                                 const double *log10_std,
+                                 const double *num_conc,
+                                 const double *vol_frac,
+                                 const double *vol_frac_std,
+                                 const int *source, const int *n_sample,
+                                 const double *sample_radius,
+                                 const double *sample_num_conc,
+                                 double sample_prop,
+                                 double characteristic_factor,
+                                 double create_time,
+                                 const double *n_part_ideal,
+                                 int allow_doubling, int allow_halving,
+                                 int64_t *n_part_add);
 
 /* Size distributions of population `pop` without a download: the
  * reference's aero_state diameter histograms (extract_aero_size.F90:132-138,

@@ -29,6 +29,10 @@ from .exact import rad2vol, vol2rad
 
 MODE_LOG_NORMAL, MODE_EXP, MODE_MONO, MODE_SAMPLED = 1, 2, 3, 4  # aero_mode.F90:31-37
 WEIGHT_NONE, WEIGHT_POWER, WEIGHT_MFA = 0, 1, 2
+# rand_normal divides by 2.0**.5 (rand.F90:465, :478), a default-kind (single
+# precision) constant
+SQRT2_SINGLE = float(np.float32(math.sqrt(2.0)))
+INFO_HALVED, INFO_WEIGHT = 3, 4  # aero_info.F90:19-28
 
 
 class Weight:
@@ -103,11 +107,11 @@ def mode_number(mode, w):
 
 def rand_normal(rng, mean, std, prob_threshold=None):
     """rand_normal, rand.F90:410-487 (Box-Muller form): redraw while
-    1 - |erf(z0 / sqrt 2)| < prob_threshold."""
+    1 - |erf(z0 / 2.0**.5)| < prob_threshold."""
     while True:
         u1, u2 = 1.0 - rng.random(), rng.random()  # u1 in (0, 1]
         z0 = math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
-        if prob_threshold is None or 1.0 - abs(math.erf(z0 / math.sqrt(2.0))) >= prob_threshold:
+        if prob_threshold is None or 1.0 - abs(math.erf(z0 / SQRT2_SINGLE)) >= prob_threshold:
             return std * z0 + mean
 
 
@@ -182,3 +186,119 @@ def add_dist_sample(rng, modes, weights, sample_prop, characteristic_factor=1.0)
     n_spec = len(modes[0].vol_frac) if modes else 1
     return (np.array(vols).reshape(-1, n_spec), np.array(groups, dtype=np.int32),
             np.array(mode_of, dtype=np.int32))
+
+
+def prob_round(rng, val):
+    """prob_round, rand.F90:214-227: floor or ceiling with mean val."""
+    c = math.ceil(val)
+    return int(math.floor(val)) if rng.random() < c - val else int(c)
+
+
+class SampleState:
+    """The parts of aero_state_t (aero_state.F90:69-84) the sampler touches:
+    per particle the species volumes, 1-based weight group and class,
+    component source, creation time and ID; the weights per (group, class)
+    as a nested list weights[g-1][c-1]; n_part_ideal (n_group, n_class) or
+    None; the removal records (id, action)."""
+
+    def __init__(self, n_spec, weights, n_part_ideal=None, next_id=1):
+        self.n_spec = n_spec
+        self.weights = weights
+        self.n_group, self.n_class = len(weights), len(weights[0])
+        self.n_part_ideal = None if n_part_ideal is None else np.asarray(n_part_ideal, dtype=np.float64)
+        self.vols, self.group, self.cls, self.source, self.ctime, self.id = [], [], [], [], [], []
+        self.next_id = next_id
+        self.removed = []
+
+    def add(self, vols, g, c, source, create_time):
+        self.vols.append(np.asarray(vols, dtype=np.float64))
+        self.group.append(g)
+        self.cls.append(c)
+        self.source.append(source)
+        self.ctime.append(create_time)
+        self.id.append(self.next_id)
+        self.next_id += 1
+
+    def members(self, g, c):
+        return [i for i in range(len(self.id)) if self.group[i] == g and self.cls[i] == c]
+
+    def remove(self, idx, action):
+        for i in sorted(idx, reverse=True):
+            self.removed.append((self.id[i], action))
+            for a in (self.vols, self.group, self.cls, self.source, self.ctime, self.id):
+                del a[i]
+
+    def arrays(self):
+        return (np.array(self.vols).reshape(-1, self.n_spec), np.array(self.group, dtype=np.int32),
+                np.array(self.cls, dtype=np.int32), np.array(self.source, dtype=np.int32),
+                np.array(self.id, dtype=np.int64))
+
+
+def scale_weight(rng, st, g, c, ratio, allow_doubling, allow_halving):
+    """aero_state_scale_weight, aero_state.F90:1859-1922.  The halving branch
+    removes prob_round(n (1 - 1/ratio)) members; the reference picks them
+    one at a time uniformly from the shrinking list, which is a uniform
+    subset of that size, drawn here at once.  The doubling branch ends each
+    member as prob_round(1/ratio) particles (aero_state_dup_particle,
+    :488-539)."""
+    mem = st.members(g, c)
+    n = len(mem)
+    w = st.weights[g - 1][c - 1]
+    if ratio > 1.0 and (allow_halving or n == 0):
+        w.magnitude *= ratio
+        n_remove = prob_round(rng, n * (1.0 - 1.0 / ratio))
+        if n_remove > 0:
+            st.remove(list(rng.choice(mem, n_remove, replace=False)), INFO_HALVED)
+    elif ratio < 1.0 and (allow_doubling or n == 0):
+        w.magnitude *= ratio
+        gone = []
+        for i in reversed(mem):
+            k = prob_round(rng, 1.0 / ratio)
+            if k == 0:
+                gone.append(i)
+            for _ in range(k - 1):
+                st.add(st.vols[i], st.group[i], st.cls[i], st.source[i], st.ctime[i])
+        st.remove(gone, INFO_WEIGHT)
+
+
+def prepare_weight_for_add(rng, st, g, c, n_add, allow_doubling, allow_halving):
+    """aero_state_prepare_weight_for_add, aero_state.F90:704-752 (one
+    process)."""
+    n_new = len(st.members(g, c)) + n_add
+    if n_new == 0.0:
+        return
+    ideal = st.n_part_ideal[g - 1, c - 1]
+    if n_new < ideal / 2.0 or n_new > ideal * 2.0:
+        scale_weight(rng, st, g, c, n_new / ideal, allow_doubling, allow_halving)
+
+
+def add_aero_dist_sample(rng, st, modes, sample_prop, characteristic_factor=1.0, create_time=0.0,
+                         allow_doubling=True, allow_halving=True, sources=None, rad2vol_fn=rad2vol):
+    """aero_state_add_aero_dist_sample, aero_state.F90:758-831, over a
+    SampleState: for every group and mode, the weight prepared for the
+    expected count (when n_part_ideal is set), then Poisson(sample_prop *
+    aero_mode_number) particles.  The class is the mode's source when there
+    is more than one class (aero_state_weight_class_for_source,
+    aero_state.F90:263-282); sources default to mode index + 1.
+    rad2vol_fn is aero_data_rad2vol (the particle shape).  Returns the
+    number of particles added."""
+    added = 0
+    for g in range(1, st.n_group + 1):
+        for m, mode in enumerate(modes):
+            src = m + 1 if sources is None else sources[m]
+            c = src if st.n_class > 1 else 1
+            w = st.weights[g - 1][c - 1]
+            n_avg = sample_prop * mode_number(mode, w)
+            if st.n_part_ideal is not None:
+                prepare_weight_for_add(rng, st, g, c, n_avg, allow_doubling, allow_halving)
+            if n_avg == 0.0:
+                continue
+            w = st.weights[g - 1][c - 1]
+            n_avg = sample_prop * mode_number(mode, w)
+            n = int(rng.poisson(n_avg))
+            size_factor = min(1.0 / (characteristic_factor * n_avg), 0.32)
+            added += n
+            for _ in range(n):
+                r = sample_radius(rng, mode, w, size_factor)
+                st.add(sample_vols(rng, mode, float(rad2vol_fn(r))), g, c, src, create_time)
+    return added

@@ -22,7 +22,7 @@ UNITS = [
     ("pmc_noalloc.cu", []),
 ]
 HEADERS = ["pmc_physics.cuh", "pmc_state.cuh", "pmc_kernels.cuh", "pmc_merge.cuh", "pmc_particle.cuh",
-           "pmc_replay.cuh"]
+           "pmc_replay.cuh", "pmc_sample.cuh"]
 
 
 def _nvcc():

@@ -31,6 +31,12 @@ AERO_WEIGHT_TYPE_MFA = 3
 
 MAX_AERO_COMPONENT_SIZE = 20
 
+# aero_mode.F90:31-37
+AERO_MODE_TYPE_LOG_NORMAL = 1
+AERO_MODE_TYPE_EXP = 2
+AERO_MODE_TYPE_MONO = 3
+AERO_MODE_TYPE_SAMPLED = 4
+
 
 class Fractal:
     """Particle shape (fractal_t, fractal.F90:59-66): volume fractal dimension,
@@ -114,6 +120,34 @@ class AeroWeightArray:
         return 1.0 / inv
 
 
+class AeroMode:
+    """aero_mode_t (aero_mode.F90:40-66): type, characteristic radius (m),
+    log10 of the geometric standard deviation, number concentration
+    (m^-3), species volume fractions and their standard deviations, the
+    source, and for sampled modes the radius edges (m) and the number
+    concentration (m^-3) of each interval."""
+
+    def __init__(self, type, char_radius=0.0, log10_std_dev_radius=0.0, num_conc=0.0, vol_frac=(1.0,),
+                 vol_frac_std=None, source=None, sample_radius=None, sample_num_conc=None):
+        self.type = int(type)
+        self.char_radius = float(char_radius)
+        self.log10_std_dev_radius = float(log10_std_dev_radius)
+        self.num_conc = float(num_conc)
+        self.vol_frac = np.asarray(vol_frac, dtype=np.float64)
+        self.vol_frac_std = (np.zeros_like(self.vol_frac) if vol_frac_std is None
+                             else np.asarray(vol_frac_std, dtype=np.float64))
+        self.source = source
+        self.sample_radius = None if sample_radius is None else np.asarray(sample_radius, dtype=np.float64)
+        self.sample_num_conc = None if sample_num_conc is None else np.asarray(sample_num_conc, dtype=np.float64)
+
+
+class AeroDist:
+    """aero_dist_t (aero_dist.F90:33-36): a list of modes."""
+
+    def __init__(self, modes):
+        self.mode = list(modes)
+
+
 class EnvState:
     def __init__(self, temp=288.0, pressure=1e5, additive_kernel_coefficient=1000.0):
         self.temp = float(temp)
@@ -180,6 +214,52 @@ class AeroState:
         if self.n_pop == 1:
             self.awa = AeroWeightArray(self.awa.type, mag, self.awa.exponent)
         return mag
+
+    def set_n_part_ideal(self, n_part):
+        """aero_state_set_n_part_ideal (aero_state.F90:241-258): the ideal
+        number of computational particles, split evenly over the weight
+        groups and classes."""
+        self.n_part_ideal = np.full(self.awa.magnitude.shape, float(n_part) / self.awa.magnitude.size)
+
+    def add_aero_dist_sample(self, aero_dist, sample_prop=1.0, characteristic_factor=1.0, create_time=0.0,
+                             allow_doubling=True, allow_halving=True, pop=0):
+        """aero_state_add_aero_dist_sample (aero_state.F90:758-831) on the
+        device (pmc_coag_gpu_add_dist_sample): a Poisson sample of the modes
+        of ``aero_dist`` added to population ``pop``, the weights prepared
+        for the ideal particle count when set_n_part_ideal was called.
+        Returns the number of particles added."""
+        modes = aero_dist.mode
+        n_mode = len(modes)
+        n_spec = self.aero_data.n_spec
+        typ = np.array([m.type for m in modes], dtype=np.int32)
+        rad = np.array([m.char_radius for m in modes], dtype=np.float64)
+        std = np.array([m.log10_std_dev_radius for m in modes], dtype=np.float64)
+        nc = np.array([m.num_conc for m in modes], dtype=np.float64)
+        vf = np.zeros((max(n_mode, 1), n_spec))
+        vfs = np.zeros((max(n_mode, 1), n_spec))
+        for k, m in enumerate(modes):
+            if m.vol_frac.size != n_spec or m.vol_frac_std.size != n_spec:
+                raise ValueError("vol_frac and vol_frac_std need one entry per species")
+            vf[k], vfs[k] = m.vol_frac, m.vol_frac_std
+        src = np.array([k + 1 if m.source is None else int(m.source) for k, m in enumerate(modes)], dtype=np.int32)
+        ns = np.array([0 if m.type != AERO_MODE_TYPE_SAMPLED else m.sample_num_conc.size for m in modes],
+                      dtype=np.int32)
+        sr = [m.sample_radius for m in modes if m.type == AERO_MODE_TYPE_SAMPLED]
+        sn = [m.sample_num_conc for m in modes if m.type == AERO_MODE_TYPE_SAMPLED]
+        sr = np.ascontiguousarray(np.concatenate(sr) if sr else np.zeros(1))
+        sn = np.ascontiguousarray(np.concatenate(sn) if sn else np.zeros(1))
+        ideal = getattr(self, "n_part_ideal", None)
+        ideal_flat = None if ideal is None else np.ascontiguousarray(np.asarray(ideal).ravel(order="F"))
+        n_add = ctypes.c_int64(0)
+        check(_lib.lib().pmc_coag_gpu_add_dist_sample(
+            self.ctx, pop, n_mode, ip(typ), dp(rad), dp(std), dp(nc), dp(np.ascontiguousarray(vf)),
+            dp(np.ascontiguousarray(vfs)), ip(src), ip(ns), dp(sr), dp(sn), float(sample_prop),
+            float(characteristic_factor), float(create_time), None if ideal_flat is None else dp(ideal_flat),
+            int(bool(allow_doubling)), int(bool(allow_halving)), ctypes.byref(n_add)),
+            "pmc_coag_gpu_add_dist_sample")
+        if self.n_pop == 1:
+            self.awa = AeroWeightArray(self.awa.type, self.weight_magnitudes(pop), self.awa.exponent)
+        return int(n_add.value)
 
     def size_dist(self, n_bin, d_min, d_max, pop=0):
         """Number and per-species mass distributions on a log diameter grid

@@ -24,6 +24,7 @@
 #include "pmc_kernels.cuh"
 #include "pmc_merge.cuh"
 #include "pmc_replay.cuh"
+#include "pmc_sample.cuh"
 
 using namespace pmc;
 
@@ -484,34 +485,7 @@ __global__ void k_double(PopDev P, int n, const uint8_t* flag, const long long* 
       set_status(P.ctr, kErrCapacity);
       continue;
     }
-    for (int s = 0; s < P.n_spec; s++) P.vol[vol_at(P, d, s)] = P.vol[vol_at(P, i, s)];
-    P.vtot[d] = P.vtot[i];
-    P.mass[d] = P.mass[i];
-    P.rad[d] = P.rad[i];
-    P.grp[d] = P.grp[i];
-    P.cls[d] = P.cls[i];
-    P.id[d] = id0 + off[i];
-    P.nprim[d] = P.nprim[i];
-    P.ncomp[d] = P.ncomp[i];
-    for (int k = 0; k < P.ncomp[i]; k++) {
-      P.csrc[comp_at(d, k)] = P.csrc[comp_at(i, k)];
-      P.ctime[comp_at(d, k)] = P.ctime[comp_at(i, k)];
-    }
-    P.lct[d] = P.lct[i];
-    P.gct[d] = P.gct[i];
-    P.imf[d] = P.imf[i];
-    P.den_ice[d] = P.den_ice[i];
-    P.phi[d] = P.phi[i];
-    P.hyst[d] = P.hyst[i];
-    P.frozen[d] = P.frozen[i];
-    P.cell[d] = P.cell[i];
-    P.recd[d] = P.recd[i];
-    P.recf[d] = P.recf[i];
-    P.claim[d] = ~0ULL;
-    P.rclaim[d] = ~0ULL;
-    P.touched[d] = ~0u;
-    P.alive[d] = 1;
-    P.changed[d] = 1;
+    copy_particle(P, i, d, id0 + off[i]);
   }
 }
 
@@ -839,6 +813,7 @@ struct PopHost {
   bool mirror_full = true;
   int mirror_slots = 0;
   uint32_t rebalance_calls = 0;  // halving draws: one stream per call
+  uint32_t sample_calls = 0;     // initial-condition samples: one stream per call
   Weights w{};
   int chunk_hist_cap = 0;
   // per-slot radius/bin/record caches are valid for this grid, kernel,
@@ -875,6 +850,10 @@ struct Ctx {
   std::vector<long long> rg_seen;  // the key of the previous step's later rounds
   long long rg_nodes = 0, rg_builds = 0;
   DevBuf<long long> graph_stats;
+  // initial-condition sampler: staging of the modes, copy counts, radix select
+  DevBuf<double> sample_buf;
+  DevBuf<int> dup_n;
+  DevBuf<unsigned char> select_buf;
   size_t sort_smem = 0;  // dynamic shared memory the sort grid was sized for
   int sort_blocks = 0;   // co-resident sort blocks at that size
   // per-round buffers
@@ -2692,6 +2671,9 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   replay_free(c.replay);
   free_redraw_graph(c);
   c.graph_stats.release();
+  c.sample_buf.release();
+  c.dup_n.release();
+  c.select_buf.release();
   cudaStreamDestroy(c.cap_stream);
   cudaStreamDestroy(c.stream);
   delete x;
@@ -3082,6 +3064,281 @@ int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx* x, int pop, const double* n_part_id
     if (r.status) return r.status;
     if (ph.h.rm_on && r.n_removed > ph.h.rm_cap) return PMC_ERR_CAPACITY;
   }
+  return PMC_OK;
+  GUARD_END
+}
+
+// ---------------------------------------------------------------------------
+// aero_state_add_aero_dist_sample (aero_state.F90:758-831) on the device
+
+// One mode of the caller's distribution (aero_mode_t, aero_mode.F90:40-66)
+struct HostMode {
+  int type = 0;
+  double char_radius = 0, log10_std = 0, num_conc = 0;
+  int source = 1;
+  int n_sample = 0;
+  const double* sample_radius = nullptr;  // [n_sample + 1] (host)
+  const double* sample_nc = nullptr;      // [n_sample] (host)
+  long long r_off = 0;                    // offset of sample_radius in the device copy
+};
+
+// aero_mode_weighted_sampled_num_conc (aero_mode.F90:457-491).  Under a
+// power weight of exponent 0 the reference's expression is 0/0; its limit,
+// the unweighted concentration, is used.
+static void weighted_sampled_num_conc(const HostMode& m, int w_type, double expo, std::vector<double>& out) {
+  out.resize(m.n_sample);
+  for (int i = 0; i < m.n_sample; i++) {
+    if (w_type == kWeightNone || expo == 0.0) {
+      out[i] = m.sample_nc[i];
+      continue;
+    }
+    double x0 = log(m.sample_radius[i]), x1 = log(m.sample_radius[i + 1]);
+    out[i] = m.sample_nc[i] / expo * (exp(-expo * x0) - exp(-expo * x1)) / (x1 - x0);
+  }
+}
+
+// log10 of the weighted mode's median radius, x_mean_prime
+// (aero_mode.F90:510-513, :574-577)
+static double x_mean_prime(const HostMode& m, int w_type, double expo) {
+  double x = log10(m.char_radius);
+  if (w_type == kWeightNone) return x;
+  return x - expo * (m.log10_std * m.log10_std) * log(10.0);
+}
+
+// aero_mode_number (aero_mode.F90:495-546): the mean number of computational
+// particles per unit sample proportion under weight (w_type, mag, expo);
+// wnc receives a sampled mode's weighted interval concentrations
+static double mode_number(const HostMode& m, int w_type, double mag, double expo, std::vector<double>& wnc) {
+  switch (m.type) {
+    case kModeLogNormal: {
+      if (w_type == kWeightNone) return m.num_conc / mag;
+      double x = log10(m.char_radius), xp = x_mean_prime(m, w_type, expo);
+      return m.num_conc / mag * exp((xp * xp - x * x) / (2.0 * (m.log10_std * m.log10_std)));
+    }
+    case kModeExp:
+      if (w_type != kWeightNone) throw Fail(PMC_ERR_INVALID_ARG);  // die_msg(822252601)
+      return m.num_conc / mag;
+    case kModeMono:
+      return m.num_conc / (w_type == kWeightNone ? mag : mag * fast_pow<double>(m.char_radius, expo));
+    case kModeSampled: {
+      weighted_sampled_num_conc(m, w_type, expo, wnc);
+      double s = 0.0;
+      for (double v : wnc) s = s + v;
+      return s / mag;
+    }
+  }
+  throw Fail(PMC_ERR_INVALID_ARG);
+}
+
+// aero_state_scale_weight (aero_state.F90:1859-1922) for (g, cl) of
+// population k holding n members: returns the members after the call
+static long long scale_weight_members(Ctx& c, int k, int g, int cl, long long n, double ratio, bool allow_doubling,
+                                      bool allow_halving, Rng& hr, uint32_t call) {
+  PopHost& ph = c.pops[k];
+  if (ratio > 1.0 && (allow_halving || n == 0)) {
+    scale_weight(c, k, g, cl, ratio);
+    long long n_remove = prob_round(hr, (double)n * (1.0 - 1.0 / ratio));
+    if (n_remove <= 0) return n;
+    reserve_removal_logs(c);  // the removals are recorded (AERO_INFO_HALVED)
+    if (c.dirty) push_pops(c);
+    c.select_buf.reserve(sizeof(SelectState));
+    SelectState* S = (SelectState*)c.select_buf.p;
+    CK(cudaMemsetAsync(S, 0, sizeof(SelectState), c.stream));
+    CK(cudaMemcpyAsync(&S->need, &n_remove, sizeof(long long), cudaMemcpyHostToDevice, c.stream));
+    PopCtr r = read_ctr(c, k);
+    int grid = grid_for(r.n_slots, 256);
+    for (int shift = 48; shift >= 0; shift -= 16) {
+      k_select_hist<<<grid, 256, 0, c.stream>>>(ph.h, g, cl, call, S, shift);
+      note_launch();
+      k_select_pick<<<1, 1024, 0, c.stream>>>(S, shift);
+      note_launch();
+    }
+    k_select_remove<<<grid, 256, 0, c.stream>>>(ph.h, g, cl, call, S);
+    note_launch();
+    // the records kept so far, for a later growth of the log
+    ph.rm_count = read_ctr(c, k).n_removed;
+    return n - n_remove;
+  }
+  if (ratio < 1.0 && (allow_doubling || n == 0)) {
+    scale_weight(c, k, g, cl, ratio);
+    if (n == 0) return 0;
+    if (c.dirty) push_pops(c);
+    PopCtr r = read_ctr(c, k);
+    size_t ns = (size_t)r.n_slots;
+    c.dup_n.reserve(ns + 1);
+    c.st_l.reserve(ns + 1);
+    k_dup_count<<<grid_for(ns, 256), 256, 0, c.stream>>>(ph.h, r.n_slots, g, cl, 1.0 / ratio, call, c.dup_n.p);
+    note_launch();
+    long long copies = scan(c, c.dup_n.p, (long long)ns, c.st_l.p, true);
+    if (copies > 0) {
+      long long need = (long long)r.n_slots + copies;
+      if (need > (1LL << 31) - 1) throw Fail(PMC_ERR_CAPACITY);
+      if (need > ph.h.cap) {
+        relayout(c, k, (int)std::min<long long>(need * 3 / 2 + 1024, (1LL << 31) - 1), false);
+        push_pops(c);
+      }
+      k_dup_write<<<grid_for(ns, 256), 256, 0, c.stream>>>(ph.h, r.n_slots, c.dup_n.p, c.st_l.p, r.next_id);
+      note_launch();
+      r.n_slots += (int)copies;
+      r.n_live += (int)copies;
+      r.next_id += copies;
+      write_ctr(c, k, r);
+    }
+    return n + copies;
+  }
+  return n;
+}
+
+int pmc_coag_gpu_add_dist_sample(pmc_coag_gpu_ctx* x, int pop, int n_mode, const int* mode_type,
+                                 const double* char_radius, const double* log10_std, const double* num_conc,
+                                 const double* vol_frac, const double* vol_frac_std, const int* source,
+                                 const int* n_sample, const double* sample_radius, const double* sample_num_conc,
+                                 double sample_prop, double characteristic_factor, double create_time,
+                                 const double* n_part_ideal, int allow_doubling, int allow_halving,
+                                 int64_t* n_part_add) {
+  if (n_part_add) *n_part_add = 0;
+  if (!x || pop < 0 || pop >= x->c.n_pop || n_mode < 0) return PMC_ERR_INVALID_ARG;
+  if (n_mode > 0 && (!mode_type || !char_radius || !num_conc || !vol_frac)) return PMC_ERR_INVALID_ARG;
+  if (!(sample_prop >= 0.0) || !(characteristic_factor > 0.0)) return PMC_ERR_INVALID_ARG;
+  Ctx& c = x->c;
+  // the modes, checked as aero_mode_read and the samplers check them
+  std::vector<HostMode> modes(n_mode);
+  long long r_tot = 0, nc_tot = 0;
+  for (int m = 0; m < n_mode; m++) {
+    HostMode& h = modes[m];
+    h.type = mode_type[m];
+    h.char_radius = char_radius[m];
+    h.log10_std = log10_std ? log10_std[m] : 0.0;
+    h.num_conc = num_conc[m];
+    h.source = source ? source[m] : m + 1;
+    if (h.type < kModeLogNormal || h.type > kModeSampled || !(h.num_conc >= 0.0) || h.source < 1)
+      return PMC_ERR_INVALID_ARG;
+    if (c.n_class > 1 && h.source > c.n_class) return PMC_ERR_INVALID_ARG;  // assert(765048788)
+    if (h.type == kModeLogNormal && (!log10_std || !(h.log10_std > 0.0) || !(h.char_radius > 0.0)))
+      return PMC_ERR_INVALID_ARG;
+    if ((h.type == kModeExp || h.type == kModeMono) && !(h.char_radius > 0.0)) return PMC_ERR_INVALID_ARG;
+    if (h.type == kModeSampled) {
+      if (!n_sample || !sample_radius || !sample_num_conc || n_sample[m] < 1) return PMC_ERR_INVALID_ARG;
+      h.n_sample = n_sample[m];
+      h.sample_radius = sample_radius + r_tot;
+      h.sample_nc = sample_num_conc + nc_tot;
+      h.r_off = r_tot;
+      for (int i = 0; i <= h.n_sample; i++)
+        if (!(h.sample_radius[i] > 0.0) || (i > 0 && !(h.sample_radius[i] > h.sample_radius[i - 1])))
+          return PMC_ERR_INVALID_ARG;
+      for (int i = 0; i < h.n_sample; i++)
+        if (!(h.sample_nc[i] >= 0.0)) return PMC_ERR_INVALID_ARG;
+      r_tot += h.n_sample + 1;
+      nc_tot += h.n_sample;
+    }
+    for (int s = 0; s < c.n_spec; s++) {
+      double f = vol_frac[m * c.n_spec + s], sd = vol_frac_std ? vol_frac_std[m * c.n_spec + s] : 0.0;
+      if (!(f >= 0.0) || !(sd >= 0.0)) return PMC_ERR_INVALID_ARG;
+    }
+  }
+  GUARD_BEGIN
+  PopHost& ph = c.pops[pop];
+  const uint32_t call = ph.sample_calls++;
+  Rng hr(ph.seed, ph.step, sample_ctr(call, kSubHost), 0u);
+  // device copies: fractions and their deviations per mode, the sampled
+  // modes' radius edges, one weighted-concentration array per batch
+  const int ns = c.n_spec;
+  size_t n_vf = (size_t)n_mode * ns;
+  std::vector<double> hbuf(2 * n_vf + (size_t)r_tot + (size_t)nc_tot * c.n_group + 1, 0.0);
+  for (size_t i = 0; i < n_vf; i++) {
+    hbuf[i] = vol_frac[i];
+    hbuf[n_vf + i] = vol_frac_std ? vol_frac_std[i] : 0.0;
+  }
+  if (r_tot) std::memcpy(&hbuf[2 * n_vf], sample_radius, sizeof(double) * (size_t)r_tot);
+  c.sample_buf.reserve(hbuf.size());
+  double* d_vf = c.sample_buf.p;
+  double* d_sr = d_vf + 2 * n_vf;
+  double* d_wnc = d_sr + r_tot;
+  std::vector<int> cnt = count_group_class(c, pop);
+  long long wnc_used = 0, added = 0;
+  uint32_t idx = 0;
+  std::vector<double> wnc;
+  for (int g = 1; g <= c.n_group; g++)
+    for (int m = 0; m < n_mode; m++) {
+      const HostMode& h = modes[m];
+      int cl = c.n_class > 1 ? h.source : 1;  // aero_state_weight_class_for_source, aero_state.F90:263-282
+      int kc = (g - 1) + c.n_group * (cl - 1);
+      int kw = (g - 1) + kMaxGroup * (cl - 1);
+      const Weights& W0 = ph.own_w ? ph.w : c.w;
+      double n_avg = sample_prop * mode_number(h, W0.type[kw], W0.mag[kw], W0.expo[kw], wnc);
+      if (n_part_ideal) {
+        // aero_state_prepare_weight_for_add (aero_state.F90:704-752)
+        double n_new = (double)cnt[kc] + n_avg;
+        double ideal = n_part_ideal[kc];
+        if (n_new != 0.0 && (n_new < ideal / 2.0 || n_new > ideal * 2.0))
+          cnt[kc] = (int)scale_weight_members(c, pop, g, cl, cnt[kc], n_new / ideal, allow_doubling != 0,
+                                              allow_halving != 0, hr, call);
+      }
+      if (n_avg == 0.0) continue;
+      const Weights& W = ph.own_w ? ph.w : c.w;
+      int wt = W.type[kw];
+      double mag = W.mag[kw], expo = W.expo[kw];
+      n_avg = sample_prop * mode_number(h, wt, mag, expo, wnc);
+      int n = rand_poisson(hr, n_avg);
+      if (n < 0) throw Fail(PMC_ERR_CAPACITY);
+      double size_factor = std::min(1.0 / (characteristic_factor * n_avg), 0.32);
+      added += n;
+      if (n == 0) continue;
+      PopCtr r = read_ctr(c, pop);
+      long long need = (long long)r.n_slots + n;
+      if (need > (1LL << 31) - 1) throw Fail(PMC_ERR_CAPACITY);
+      if (need > ph.h.cap) relayout(c, pop, (int)std::min<long long>(need * 3 / 2 + 1024, (1LL << 31) - 1), false);
+      SampleBatch B{};
+      B.n = n;
+      B.type = h.type;
+      B.group = g;
+      B.cls = cl;
+      B.w_type = wt;
+      B.w_mag = mag;
+      B.w_expo = expo;
+      B.log10_std = h.log10_std;
+      B.x_mean = h.type == kModeLogNormal ? x_mean_prime(h, wt, expo) : 0.0;
+      B.threshold = size_factor;
+      B.char_radius = h.char_radius;
+      B.char_vol = rad2vol(c.frac, h.char_radius);
+      B.n_sample = h.n_sample;
+      B.sample_radius = d_sr + h.r_off;
+      if (h.type == kModeSampled) {
+        std::memcpy(&hbuf[2 * n_vf + r_tot + wnc_used], wnc.data(), sizeof(double) * wnc.size());
+        B.wnc = d_wnc + wnc_used;
+        wnc_used += (long long)wnc.size();
+      }
+      B.vol_frac = d_vf + (size_t)m * ns;
+      B.vol_frac_std = d_vf + n_vf + (size_t)m * ns;
+      B.any_std = 0;
+      for (int s = 0; s < ns; s++)
+        if (hbuf[n_vf + (size_t)m * ns + s] > 0.0) B.any_std = 1;
+      B.source = h.source;
+      B.create_time = create_time;
+      // the whole staging array is copied before every batch: it is small,
+      // and the batch's weighted concentrations were just written into it
+      CK(cudaMemcpyAsync(c.sample_buf.p, hbuf.data(), sizeof(double) * hbuf.size(), cudaMemcpyHostToDevice,
+                         c.stream));
+      if (c.dirty) push_pops(c);
+      k_sample_batch<<<grid_for(n, 256), 256, 0, c.stream>>>(ph.h, B, r.n_slots, r.next_id, call, idx);
+      note_launch();
+      idx += (uint32_t)n;
+      r.n_slots += n;
+      r.n_live += n;
+      r.next_id += n;
+      write_ctr(c, pop, r);
+      cnt[kc] += n;
+    }
+  ph.valid_sort = false;
+  ph.caches_valid = false;
+  c.replay.valid = false;
+  push_pops(c);
+  CK(cudaStreamSynchronize(c.stream));
+  PopCtr r = read_ctr(c, pop);
+  ph.rm_count = r.n_removed;
+  if (n_part_add) *n_part_add = added;
+  if (r.status) return r.status;
+  if (ph.h.rm_on && r.n_removed > ph.h.rm_cap) return PMC_ERR_CAPACITY;
   return PMC_OK;
   GUARD_END
 }

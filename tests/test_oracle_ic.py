@@ -153,3 +153,95 @@ def test_sampled_distribution_matches_the_mode_under_any_weighting(alpha):
         -(np.log(centers) - math.log(2.0 * mode.char_radius)) ** 2 / (2.0 * ln_sigma ** 2))
     assert abs(len(r) - 10000) < 5 * math.sqrt(10000)
     assert E.rel_err_by_col(exact, h)[0] < 0.1
+
+
+def _state(n, weights, ideal=None, seed=0):
+    """a SampleState holding n log-normal particles in group 1, class 1"""
+    rng = np.random.default_rng(seed)
+    st = S.SampleState(1, weights, ideal)
+    for r in 10.0 ** rng.normal(-7.0, 0.2, n):
+        st.add([S.rad2vol(r)], 1, 1, 1, 0.0)
+    return st
+
+
+def test_scale_weight_halving_removes_a_uniform_subset_of_exact_size():
+    """aero_state_scale_weight, ratio > 1: prob_round(n (1 - 1/ratio))
+    members removed, each recorded as halved, the weight scaled by ratio;
+    the removed members are a uniform subset (their sizes follow the
+    population's)."""
+    n, ratio = 4000, 2.5
+    kept_small = []
+    for seed in range(6):
+        st = _state(n, [[S.Weight(S.WEIGHT_POWER, 3.0, -1.0)]], seed=seed)
+        v0 = np.array(st.vols)[:, 0]
+        S.scale_weight(np.random.default_rng(100 + seed), st, 1, 1, ratio, False, True)
+        left = len(st.id)
+        assert n - left in (math.floor(n * (1 - 1 / ratio)), math.ceil(n * (1 - 1 / ratio)))
+        assert len(st.removed) == n - left and all(a == S.INFO_HALVED for _, a in st.removed)
+        assert st.weights[0][0].magnitude == 3.0 * ratio
+        kept_small.append(np.mean(np.array(st.vols)[:, 0] < np.median(v0)))
+    # half of the population is below the median: a uniform subset keeps half of those
+    assert abs(np.mean(kept_small) - 0.5) < 4 * math.sqrt(0.25 / (6 * n / ratio))
+
+
+def test_scale_weight_doubling_copies_each_member():
+    """aero_state_scale_weight, ratio < 1: each member ends as
+    prob_round(1/ratio) particles (aero_state_dup_particle), copies with
+    new IDs and the member's volumes."""
+    n, ratio = 3000, 0.3
+    st = _state(n, [[S.Weight(S.WEIGHT_POWER, 3.0, -1.0)]], seed=1)
+    ids0 = list(st.id)
+    S.scale_weight(np.random.default_rng(5), st, 1, 1, ratio, True, False)
+    m = len(st.id)
+    assert abs(m / n - 1 / ratio) < 4 * math.sqrt((1 / 3) * (2 / 3) / n)
+    assert st.id[:n] == ids0 and len(set(st.id)) == m
+    vols = np.array(st.vols)[:, 0]
+    _, k = np.unique(vols, return_counts=True)
+    assert set(k) <= {3, 4}
+    assert st.weights[0][0].magnitude == 3.0 * ratio
+
+
+def test_prepare_weight_for_an_empty_state_sets_the_magnitude():
+    """With no particles, the weight is scaled by n_add / ideal whatever
+    allow_doubling / allow_halving say (aero_state.F90:1890, :1910)."""
+    mode = S.Mode(S.MODE_LOG_NORMAL, char_radius=5e-8, log10_std=0.2, num_conc=1e10)
+    for allow in (False, True):
+        st = S.SampleState(1, [[S.Weight(S.WEIGHT_POWER, 1.0, -3.0)]], [[5000.0]])
+        n_avg = S.mode_number(mode, st.weights[0][0])
+        S.add_aero_dist_sample(np.random.default_rng(3), st, [mode], 1.0, allow_doubling=allow,
+                               allow_halving=allow)
+        assert st.weights[0][0].magnitude == 1.0 * (n_avg / 5000.0)
+        assert abs(len(st.id) - 5000) < 5 * math.sqrt(5000)
+
+
+def combined_num_conc(weights, cls, r):
+    """aero_weight_array_num_conc_at_radius: harmonic combination of the
+    groups' weights of class cls (1-based) at r"""
+    return 1.0 / sum(1.0 / w[cls - 1].num_conc_at_radius(r) for w in weights)
+
+
+def test_multi_mode_sample_with_halving_estimates_every_mode_without_bias():
+    """Three modes under two weight groups (flat and r^-3) with an ideal of
+    2000 particles: the second and third modes push the groups past twice
+    the ideal, so aero_state_prepare_weight_for_add halves them.  Summing
+    each particle's combined number concentration per source still gives
+    every mode's number concentration (an unbiased estimate)."""
+    modes = [S.Mode(S.MODE_LOG_NORMAL, char_radius=2e-8, log10_std=0.2, num_conc=3e9),
+             S.Mode(S.MODE_LOG_NORMAL, char_radius=1.2e-7, log10_std=0.25, num_conc=5e9),
+             S.Mode(S.MODE_MONO, char_radius=3e-7, num_conc=2e8)]
+    est = []
+    n_halved = 0
+    for seed in range(24):
+        st = S.SampleState(1, [[S.Weight(S.WEIGHT_NONE, 1.0, 0.0)], [S.Weight(S.WEIGHT_POWER, 1.0, -3.0)]],
+                           [[1000.0], [1000.0]])
+        S.add_aero_dist_sample(np.random.default_rng(seed), st, modes, 1.0)
+        n_halved += len(st.removed)
+        vols, grp, cls, src, _ = st.arrays()
+        r = S.vol2rad(vols[:, 0])
+        nc = combined_num_conc(st.weights, 1, r)
+        est.append([nc[src == k + 1].sum() for k in range(3)])
+    assert n_halved > 0
+    est = np.array(est)
+    truth = np.array([m.num_conc for m in modes])
+    z = np.abs(est.mean(0) - truth) / (est.std(0, ddof=1) / math.sqrt(len(est)))
+    assert z.max() < 4.5, z
