@@ -313,7 +313,7 @@ def run_ic_sample(pm, pop, n_part, ws, reps=3):
     modes = [pm.AeroMode(pm.AERO_MODE_TYPE_LOG_NORMAL, d / 2.0, np.log10(sig[k]), nc, vol_frac=frac,
                          vol_frac_std=0.1 * frac)
              for k, (d, nc) in enumerate(((0.02e-6, 1e10), (0.1e-6, 1e9), (0.5e-6, 1e8)))]
-    dev_s, host_s, n_dev = [], [], 0
+    dev_s, host_s, n_dev, n_host = [], [], 0, 0
     for k in range(reps):
         st = pm.AeroState(pop.aero_data, pm.AeroWeightArray.nummass(), seed=40 + k)
         st.set_n_part_ideal(n_part)
@@ -327,12 +327,14 @@ def run_ic_sample(pm, pop, n_part, ws, reps=3):
         t0 = time.perf_counter()
         hp = aero_dist.brown_20spec(n_part, seed=40 + k)
         st.add_particles(hp.vol, hp.group)
+        n_host = hp.n_part
         torch.cuda.synchronize()
         host_s.append(time.perf_counter() - t0)
         del st
     return {"particles": n_dev, "device_ms": 1e3 * float(np.median(dev_s)),
-            "host_numpy_and_upload_ms": 1e3 * float(np.median(host_s)),
             "particles_per_s": n_dev / float(np.median(dev_s)),
+            "host_particles": int(n_host), "host_numpy_and_upload_ms": 1e3 * float(np.median(host_s)),
+            "host_particles_per_s": n_host / float(np.median(host_s)),
             "what": "pmc_coag_gpu_add_dist_sample of three log-normal modes, 20 species with fraction "
                     "deviations, nummass weights prepared for the ideal count, wall clock with a device "
                     "synchronize; against numpy sampling on the host plus upload"}

@@ -3255,6 +3255,42 @@ int pmc_coag_gpu_add_dist_sample(pmc_coag_gpu_ctx* x, int pop, int n_mode, const
   double* d_sr = d_vf + 2 * n_vf;
   double* d_wnc = d_sr + r_tot;
   std::vector<int> cnt = count_group_class(c, pop);
+  {
+    // room for the whole call at once: the batches' expected counts, with
+    // the weight preparation run on expected values, plus a margin of 8
+    // standard deviations (a larger draw grows the slots below)
+    Weights w = ph.own_w ? ph.w : c.w;
+    std::vector<double> est(cnt.begin(), cnt.end());
+    double slots = 0.0, var = 0.0;
+    std::vector<double> tmp;
+    for (int g = 1; g <= c.n_group; g++)
+      for (int m = 0; m < n_mode; m++) {
+        int cl = c.n_class > 1 ? modes[m].source : 1;
+        int kc = (g - 1) + c.n_group * (cl - 1), kw = (g - 1) + kMaxGroup * (cl - 1);
+        double n_avg = sample_prop * mode_number(modes[m], w.type[kw], w.mag[kw], w.expo[kw], tmp);
+        if (n_part_ideal) {
+          double n_new = est[kc] + n_avg, ideal = n_part_ideal[kc];
+          if (n_new != 0.0 && (n_new < ideal / 2.0 || n_new > ideal * 2.0)) {
+            double ratio = n_new / ideal;
+            bool halve = ratio > 1.0 && (allow_halving || est[kc] == 0.0);
+            bool dbl = ratio < 1.0 && (allow_doubling || est[kc] == 0.0);
+            if (halve || dbl) {
+              if (dbl) slots += est[kc] * (1.0 / ratio - 1.0);
+              est[kc] /= ratio;
+              w.mag[kw] *= ratio;
+            }
+          }
+        }
+        if (n_avg == 0.0) continue;
+        n_avg = sample_prop * mode_number(modes[m], w.type[kw], w.mag[kw], w.expo[kw], tmp);
+        est[kc] += n_avg;
+        slots += n_avg;
+        var += n_avg;
+      }
+    PopCtr r = read_ctr(c, pop);
+    double need = (double)r.n_slots + slots + 8.0 * std::sqrt(var) + 1024.0;
+    if (need > (double)ph.h.cap && need < (double)((1LL << 31) - 1)) relayout(c, pop, (int)need, false);
+  }
   long long wnc_used = 0, added = 0;
   uint32_t idx = 0;
   std::vector<double> wnc;

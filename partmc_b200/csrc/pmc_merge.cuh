@@ -751,89 +751,80 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
        e += (long long)gridDim.x * blockDim.x) {
     it_flag[e] = 0;
     it_term[e] = no_term();
+    int gp, walker = -1, p0 = 0;
+    float pos0 = 1.0f;
+    unsigned long long key = 0;
+    int2 sl = make_int2(-1, -1);
+    uint32_t dc = 0;
     if (e >= n_ev) {
       // a particle that a target operation of the round before made or
       // changed walks from the end of that operation's pair
-      const int gp = ppw_gp[e - n_ev], x = ppw_slot[e - n_ev];
+      gp = ppw_gp[e - n_ev];
       if (gp < 0 || gp >= n_gpairs) {
         bad_index(pops[0].ctr, kBadEventSlot, gp);
         continue;
       }
-      const int pop = gpair_pop[gp];
-      const PopDev& P = pops[pop];
-      WalkOut w;
-      walk<KT, T, FLAT>(P, x, gpair_local[gp], 1.0f, &w);
-      if (w.stop) add_target_op(P, pop, w.q, x, op_pop, op_pair, op_slot, op_k, op_key, n_ops, op_cap);
-      if (!w.found) continue;
-      it_flag[e] = 1;
-      it_key[e] = make_key((uint32_t)w.q, 1u, (uint32_t)x);
-      it_c[e] = w.first_cell1 ? make_int2(x, w.y) : make_int2(w.y, x);
-      it_gp[e] = (int)(pop_pair_base[pop] + w.q);
-      it_pos[e] = w.pos;
-      it_len[e] = w.cont ? -1 : 0;
-      it_head[e] = -1;
-      it_done[e] = w.done ? 1 : 0;
-      it_dec[e] = w.dec;
-      it_gused[e] = w.g_used;
-      continue;
-    }
-    int gp = gp_c[e];
-    if (gp < 0 || gp >= n_gpairs) {
-      bad_index(pops[0].ctr, kBadEventSlot, gp);
-      continue;
-    }
-    int pop = gpair_pop[gp];
-    const PopDev& P = pops[pop];
-    int walker = -1, p0 = 0;
-    uint32_t pend_dec = 0xffffffffu;  // a pending chain event's recomputed decision
-    float pos0 = ev_pos[e];
-    unsigned long long key = ev_key[e];
-    int2 sl = ev_c[e];
-    if (win[e] && (dest[e] == kPendingTerm || dest[e] == kPendingChain)) {
-      // the test where the previous round's chain stopped, with its decision:
-      // the walker was rewritten by its own chain, so only its death counts;
-      // a partner consumed in that round is no member now, and the walk goes
-      // on after the test
-      if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
-        bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
-        continue;
-      }
-      const int x = (int)key_idx(key), y = x == sl.x ? sl.y : sl.x;
-      if (!P.alive[x]) continue;
-      if (P.touched[y] == *P.gen_p - 1u || !P.alive[y]) {
-        walker = x;
-        p0 = (int)key_pair(key);
-      } else if (dest[e] == kPendingChain) {
-        pend_dec = chain_event_decision(P, key, sl, x, y, dec[e]);
-        if (pend_dec == 0xffffffffu) continue;
-      }
-    } else if (win[e]) {
-      walker = dest[e];
+      walker = ppw_slot[e - n_ev];
       p0 = gpair_local[gp];
-      if (walker < 0) continue;
     } else {
-      if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
-        bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+      gp = gp_c[e];
+      if (gp < 0 || gp >= n_gpairs) {
+        bad_index(pops[0].ctr, kBadEventSlot, gp);
         continue;
       }
-      uint32_t gen_prev = *P.gen_p - 1u;
-      bool c1 = P.touched[sl.x] == gen_prev || !P.alive[sl.x];
-      bool c2 = P.touched[sl.y] == gen_prev || !P.alive[sl.y];
-      if (key_kind(key) == 0u) {
-        if (c1 || c2) continue;
-      } else {
-        int x = (int)key_idx(key);
-        bool cx = x == sl.x ? c1 : c2, cy = x == sl.x ? c2 : c1;
-        if (cx) continue;
-        if (cy) {
+      const PopDev& P = pops[gpair_pop[gp]];
+      uint32_t pend_dec = 0xffffffffu;  // a pending chain event's recomputed decision
+      pos0 = ev_pos[e];
+      key = ev_key[e];
+      sl = ev_c[e];
+      if (win[e] && (dest[e] == kPendingTerm || dest[e] == kPendingChain)) {
+        // the test where the previous round's chain stopped, with its
+        // decision: the walker was rewritten by its own chain, so only its
+        // death counts; a partner consumed in that round is no member now,
+        // and the walk goes on after the test
+        if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
+          bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+          continue;
+        }
+        const int x = (int)key_idx(key), y = x == sl.x ? sl.y : sl.x;
+        if (!P.alive[x]) continue;
+        if (P.touched[y] == *P.gen_p - 1u || !P.alive[y]) {
           walker = x;
           p0 = (int)key_pair(key);
+        } else if (dest[e] == kPendingChain) {
+          pend_dec = chain_event_decision(P, key, sl, x, y, dec[e]);
+          if (pend_dec == 0xffffffffu) continue;
+        }
+      } else if (win[e]) {
+        walker = dest[e];
+        p0 = gpair_local[gp];
+        if (walker < 0) continue;
+      } else {
+        if (sl.x < 0 || sl.x >= P.cap || sl.y < 0 || sl.y >= P.cap) {
+          bad_index(P.ctr, kBadEventSlot, sl.x < 0 || sl.x >= P.cap ? sl.x : sl.y);
+          continue;
+        }
+        uint32_t gen_prev = *P.gen_p - 1u;
+        bool c1 = P.touched[sl.x] == gen_prev || !P.alive[sl.x];
+        bool c2 = P.touched[sl.y] == gen_prev || !P.alive[sl.y];
+        if (key_kind(key) == 0u) {
+          if (c1 || c2) continue;
+        } else {
+          int x = (int)key_idx(key);
+          bool cx = x == sl.x ? c1 : c2, cy = x == sl.x ? c2 : c1;
+          if (cx) continue;
+          if (cy) {
+            walker = x;
+            p0 = (int)key_pair(key);
+          }
         }
       }
+      dc = pend_dec != 0xffffffffu ? pend_dec : dec[e];
     }
+    const int pop = gpair_pop[gp];
+    const PopDev& P = pops[pop];
     int len = 0, head = -1;
     bool done = false;
-    uint32_t dc = pend_dec != 0xffffffffu ? pend_dec : dec[e];
     if (walker >= 0) {
       WalkOut w;
       walk<KT, T, FLAT>(P, walker, p0, pos0, &w);
