@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--del-t", type=float, default=60.0)
     ap.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes instead of searching them on a copy of each workload")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batch-pops", type=int, default=256)
     ap.add_argument("--batch-same", type=int, default=8)
@@ -168,7 +170,22 @@ def workload(n_part, seed):
     return aero_dist.brown_20spec(n_part, seed=seed)
 
 
-def run_batched(pm, n_pop, steps, warmup, del_t, mode, seed=5):
+def tune_shapes(make_state, step, max_steps=64):
+    """The autotuner's launch shapes for a workload, searched on a copy of
+    it (untimed), so that the timed state starts from the workload itself.
+    Returns (shapes, scores in ms per candidate)."""
+    st = make_state()
+    st.autotune()
+    for _ in range(max_steps):
+        if not st.tune_state()[0]:
+            break
+        step(st)
+    _, shapes, scores = st.tune_state()
+    st.close()
+    return shapes, scores
+
+
+def run_batched(pm, n_pop, steps, warmup, del_t, mode, seed=5, autotune=True):
     """Batched form: n_pop independent populations (log-uniform 1e3..1e5
     particles, per-population T, p and mode parameters, power weighting) in
     one context; every launch covers all populations.  Returns aggregate
@@ -177,10 +194,21 @@ def run_batched(pm, n_pop, steps, warmup, del_t, mode, seed=5):
     from partmc_b200 import aero_dist
     pops, temps, press = aero_dist.batched_bimodal(n_pop=n_pop, seed=seed)
     ad = pops[0].aero_data
-    st = pm.AeroState(ad, pops[0].awa, mode=mode, n_pop=n_pop)
-    for k, p in enumerate(pops):
-        st.set_weight_pop(k, p.awa)
-        st.add_particles(p.vol, p.group, pop=k)
+
+    def make():
+        st = pm.AeroState(ad, pops[0].awa, mode=mode, n_pop=n_pop)
+        for k, p in enumerate(pops):
+            st.set_weight_pop(k, p.awa)
+            st.add_particles(p.vol, p.group, pop=k)
+        return st
+
+    shapes = None
+    if autotune:
+        shapes, _ = tune_shapes(make, lambda s: pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, s,
+                                                                  del_t))
+    st = make()
+    if shapes:
+        st.set_tune(shapes)
     for _ in range(warmup):
         pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, st, del_t)
     torch.cuda.synchronize()
@@ -193,20 +221,31 @@ def run_batched(pm, n_pop, steps, warmup, del_t, mode, seed=5):
     n_part = int(sum(p.n_part for p in pops))
     return ({"unit": "pair-tests/s", "populations": n_pop, "particles": n_part,
              "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec,
-             "rounds_last_step": st.stats()["rounds"]}, samp, sec)
+             "rounds_last_step": st.stats()["rounds"], "launch_shapes": shapes}, samp, sec)
 
 
-def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode):
+def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode, autotune=True):
     """n_pop independent copies (different seeds and samples) of the 1e6
     particle workload advanced together in one batched context."""
     import torch
     pops = [workload(n_part, seed=200 + k) for k in range(n_pop)]
-    st = pm.AeroState(pops[0].aero_data, pops[0].awa, mode=mode, n_pop=n_pop)
-    for k, p in enumerate(pops):
-        # same densities (seeded); the weights depend on the sample
-        st.set_weight_pop(k, p.awa)
-        st.add_particles(p.vol, p.group, pop=k)
     temps, press = np.full(n_pop, 288.0), np.full(n_pop, 1e5)
+
+    def make():
+        st = pm.AeroState(pops[0].aero_data, pops[0].awa, mode=mode, n_pop=n_pop)
+        for k, p in enumerate(pops):
+            # same densities (seeded); the weights depend on the sample
+            st.set_weight_pop(k, p.awa)
+            st.add_particles(p.vol, p.group, pop=k)
+        return st
+
+    shapes = None
+    if autotune:
+        shapes, _ = tune_shapes(make, lambda s: pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, s,
+                                                                  del_t))
+    st = make()
+    if shapes:
+        st.set_tune(shapes)
     for _ in range(warmup):
         pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_BROWN, temps, press, 0.0, st, del_t)
     torch.cuda.synchronize()
@@ -217,7 +256,8 @@ def run_batched_same(pm, n_pop, n_part, steps, warmup, del_t, mode):
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     return ({"unit": "pair-tests/s", "populations": n_pop, "particles_each": n_part,
-             "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec}, samp, sec)
+             "ms_per_step": 1e3 * sec / steps, "sim_s_per_s": n_pop * steps * del_t / sec,
+             "launch_shapes": shapes}, samp, sec)
 
 
 def fp32_error(pm, pop, env, n_pairs=200000, seed=3):
@@ -295,6 +335,21 @@ def run_reference(args, ws, rank):
     print(json.dumps(line))
 
 
+def step_phases(prof, steps):
+    """Where a step's device time goes, from the CUDA events around the
+    phases: round 0 (sort, pair set-up, tests, resolve, apply, host
+    read-backs between them) and the later rounds (the conditional graph of
+    retries, walks and chains).  The later rounds are bound by the
+    dependent loads of their slowest walk or chain, not by HBM; their
+    per-kernel shares come from the ncu launch list."""
+    step_ms = prof["step"][0] / max(steps, 1)
+    later_ms = prof["redraw_graph"][0] / max(steps, 1)
+    return {"round0_ms": step_ms - later_ms, "later_rounds_ms": later_ms,
+            "later_rounds_share": later_ms / step_ms if step_ms > 0 else 0.0,
+            "later_rounds_bound": "latency (dependent loads of walks and chains)",
+            "test_ms": prof["test"][0] / max(steps, 1), "sort_ms": prof["sort"][0] / max(steps, 1)}
+
+
 def aggregate(d, samp, sec, ws):
     """Whole-job form of a per-rank measurement: summed work over the
     slowest rank's time."""
@@ -351,9 +406,11 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     del st64
     out["fp64_plain"] = aggregate({"unit": "pair-tests/s", "ms_per_step": ms64 / k64}, samp64, ms64 / 1e3, ws)
     kb = max(3, args.steps // 2)
-    b, samp_b, sec_b = run_batched(pm, args.batch_pops, kb, args.warmup, args.del_t, mode)
+    b, samp_b, sec_b = run_batched(pm, args.batch_pops, kb, args.warmup, args.del_t, mode,
+                                   autotune=not args.no_autotune)
     out["batched"] = aggregate(b, samp_b, sec_b, ws)
-    b, samp_b, sec_b = run_batched_same(pm, args.batch_same, args.n_part, kb, args.warmup, args.del_t, mode)
+    b, samp_b, sec_b = run_batched_same(pm, args.batch_same, args.n_part, kb, args.warmup, args.del_t, mode,
+                                        autotune=not args.no_autotune)
     out["batched_1e6"] = aggregate(b, samp_b, sec_b, ws)
 
     # end to end through the C ABI with host buffers, the way a drop-in
@@ -506,11 +563,23 @@ def main():
     pop = workload(args.n_part, seed=1 + rank)
     env = pm.EnvState(288.0, 1e5)
 
+    shapes = {}
+
     def new_state(m):
         st = pm.AeroState(pop.aero_data, pop.awa, seed=1000 + rank, mode=m)
         st.set_graphs(not args.no_graphs)
         st.add_particles(pop.vol, pop.group)
+        if m in shapes:
+            st.set_tune(shapes[m][0])
         return st
+
+    # the autotuner's launch shapes for the workload in each mode, searched on
+    # a copy of it before anything is timed
+    if not args.no_autotune:
+        for m in (mode, pm.MODE_FP64):
+            if m not in shapes:
+                shapes[m] = tune_shapes(lambda: new_state(m), lambda s: pm.mc_coag(
+                    pm.COAG_KERNEL_TYPE_BROWN, env, pop.aero_data, s, args.del_t))
 
     # L2 flush buffer (larger than the 126 MB L2), written between timed steps
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -618,6 +687,11 @@ def main():
                           "accept_margin": 2.0 ** -12,
                           "tests_decided_in_fp64_per_step": prof["exact_tests_per_step"],
                           "decisions": "identical to FP64 mode (FP64 fallback within the margin)"},
+            "step_phases": step_phases(prof, args.steps),
+            "autotune": ({"launch_shapes": shapes[mode][0], "scores_ms": shapes[mode][1],
+                          "how": "coordinate search over threads per block at five launch sites, 3 steps per "
+                                 "candidate on a copy of the workload, untimed (pmc_coag_gpu_autotune)"}
+                         if mode in shapes else None),
             "rounds_per_step": prof["rounds_per_step"],
             "redraws_per_step": prof["redraws_per_step"],
             "conflicts_per_step": prof["conflicts_per_step"],

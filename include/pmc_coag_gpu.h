@@ -192,6 +192,33 @@ int pmc_coag_gpu_rebalance(pmc_coag_gpu_ctx *ctx, int pop,
                            const double *n_part_ideal, int allow_doubling,
                            int allow_halving);
 
+/* Autotuning of the step's launch shapes (no counterpart in the reference).
+ * Five launch sites have a threads-per-block choice: the pair tests, the
+ * merge decisions and claim resolution, the walks, the chains, and the
+ * apply.  pmc_coag_gpu_autotune(ctx, 1) makes the context's next steps
+ * (ordinary pmc_coag_gpu_step / _step_batch calls) a coordinate search over
+ * those choices: each site in turn tries its PMC_TUNE_CANDIDATES shapes for
+ * PMC_TUNE_REPS steps each and keeps the best before moving on.  A shape's
+ * score is the device time of the site's launches (CUDA events on the
+ * library's stream) per million pair tests of its steps; during the search
+ * the later rounds run from the host loop instead of the CUDA graph, so
+ * that each launch can be timed.  The search takes PMC_TUNE_SITES *
+ * PMC_TUNE_CANDIDATES * PMC_TUNE_REPS steps.  The particles do not depend
+ * on the shapes or on the loop, so these steps are the caller's own.
+ * pmc_coag_gpu_tune_state reports whether the search is still running, the
+ * shapes in use (threads[PMC_TUNE_SITES]) and the scores
+ * (ms[site * PMC_TUNE_CANDIDATES + candidate], 0 where not yet measured);
+ * either pointer may be NULL.  pmc_coag_gpu_set_tune sets shapes
+ * found earlier (each must be one of the site's candidates: 64, 128 or 256
+ * threads, 32, 64 or 128 for the chains) and stops a search. */
+#define PMC_TUNE_SITES 5
+#define PMC_TUNE_CANDIDATES 3
+#define PMC_TUNE_REPS 3
+int pmc_coag_gpu_autotune(pmc_coag_gpu_ctx *ctx, int enable);
+int pmc_coag_gpu_tune_state(pmc_coag_gpu_ctx *ctx, int *tuning, int *threads,
+                            float *ms);
+int pmc_coag_gpu_set_tune(pmc_coag_gpu_ctx *ctx, const int *threads);
+
 /* aero_state_add_aero_dist_sample (aero_state.F90:758-831) on the device:
  * add a Poisson sample of a distribution of n_mode modes to population
  * `pop`, with the given sample proportion, characteristic factor and

@@ -55,6 +55,9 @@ SIGNATURES = {
     "pmc_coag_gpu_set_graphs": (_I, [_P, _I]),
     "pmc_coag_gpu_set_seed": (_I, [_P, _I, ctypes.c_uint64]),
     "pmc_coag_gpu_rebalance": (_I, [_P, _I, _DP, _I, _I]),
+    "pmc_coag_gpu_autotune": (_I, [_P, _I]),
+    "pmc_coag_gpu_tune_state": (_I, [_P, _IP, _IP, ctypes.POINTER(ctypes.c_float)]),
+    "pmc_coag_gpu_set_tune": (_I, [_P, _IP]),
     "pmc_coag_gpu_add_dist_sample": (_I, [_P, _I, _I, _IP, _DP, _DP, _DP, _DP, _DP, _IP, _IP, _DP, _DP, _D, _D, _D,
                                           _DP, _I, _I, _LP]),
     "pmc_coag_gpu_get_weight": (_I, [_P, _I, _DP]),

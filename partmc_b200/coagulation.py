@@ -215,6 +215,32 @@ class AeroState:
             self.awa = AeroWeightArray(self.awa.type, mag, self.awa.exponent)
         return mag
 
+    TUNE_SITES = ("test", "resolve", "items", "chain", "apply")
+
+    def autotune(self, enable=True):
+        """Make the next steps a search over the step's launch shapes
+        (pmc_coag_gpu_autotune); tune_state() tells when it is done."""
+        check(_lib.lib().pmc_coag_gpu_autotune(self.ctx, int(bool(enable))), "pmc_coag_gpu_autotune")
+
+    def tune_state(self):
+        """(tuning, {site: threads per block}, {site: [ms per candidate]})."""
+        n = len(self.TUNE_SITES)
+        tuning = ctypes.c_int()
+        threads = np.zeros(n, dtype=np.int32)
+        ms = np.zeros(3 * n, dtype=np.float32)
+        check(_lib.lib().pmc_coag_gpu_tune_state(self.ctx, ctypes.byref(tuning), ip(threads),
+                                                  ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+              "pmc_coag_gpu_tune_state")
+        return (bool(tuning.value), dict(zip(self.TUNE_SITES, threads.tolist())),
+                {k: ms[3 * i:3 * i + 3].tolist() for i, k in enumerate(self.TUNE_SITES)})
+
+    def set_tune(self, threads):
+        """Launch shapes found earlier: {site: threads per block}."""
+        _, cur, _ = self.tune_state()
+        cur.update(threads)
+        a = np.array([cur[k] for k in self.TUNE_SITES], dtype=np.int32)
+        check(_lib.lib().pmc_coag_gpu_set_tune(self.ctx, ip(a)), "pmc_coag_gpu_set_tune")
+
     def set_n_part_ideal(self, n_part):
         """aero_state_set_n_part_ideal (aero_state.F90:241-258): the ideal
         number of computational particles, split evenly over the weight

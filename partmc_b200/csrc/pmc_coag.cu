@@ -825,6 +825,44 @@ struct PopHost {
   long long rm_count = 0;  // removal records on the device at the last counter read
 };
 
+// Launch shapes of the step that the autotuner chooses: threads per block
+// at five launch sites.  Every kernel there walks its work with a
+// grid-stride loop and keeps no per-block state, every draw is keyed by
+// index and every counter is a sum, so the particles do not depend on these
+// shapes, and tuning runs on the caller's own steps.
+enum TuneSite : int { kTuneTest, kTuneResolve, kTuneItems, kTuneChain, kTuneApply, kTuneSites };
+constexpr int kTuneCands = 3;
+// candidates per site (within each kernel's __launch_bounds__)
+constexpr int kTuneCand[kTuneSites][kTuneCands] = {
+    {64, 128, 256},  // k_test: one pair test per thread
+    {64, 128, 256},  // k_decide and k_resolve_set: one event per thread
+    {64, 128, 256},  // k_items: one walk per thread
+    {32, 64, 128},   // k_chain: one chain per thread
+    {64, 128, 256},  // k_apply_move and k_apply_set: one event per thread
+};
+constexpr int kTuneReps = 3;  // steps per candidate
+struct Tune {
+  int threads[kTuneSites] = {256, 256, 256, 128, 256};
+};
+// Coordinate search, one site at a time.  While it runs the later rounds
+// are launched from the host loop (the same particles as the graph), so
+// that every launch of the site being searched can be bracketed by CUDA
+// events.  A candidate's score is the device time of the site's launches
+// over its kTuneReps steps divided by those steps' pair tests: the site's
+// cost per unit of work, which does not drift with the state as the whole
+// step's time does.  The site keeps its best candidate before the next site
+// is searched.
+struct Tuner {
+  bool on = false;
+  int site = 0, cand = 0, rep = 0, best = 0;
+  float best_ms = 0.f;           // best score (ms per million pair tests)
+  double cand_ms = 0.0;          // the candidate's site time so far (ms)
+  long long cand_tests = 0;      // and its steps' pair tests
+  float site_ms[kTuneSites][kTuneCands] = {};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;  // this step's launches of the site
+  std::vector<cudaEvent_t> spare;
+};
+
 struct Ctx {
   int n_pop = 1, n_spec = 1, n_group = 1, n_class = 1, i_water = 0;
   std::vector<double> density;
@@ -850,6 +888,8 @@ struct Ctx {
   std::vector<long long> rg_seen;  // the key of the previous step's later rounds
   long long rg_nodes = 0, rg_builds = 0;
   DevBuf<long long> graph_stats;
+  Tune tune;
+  Tuner tuner;
   // initial-condition sampler: staging of the modes, copy counts, radix select
   DevBuf<double> sample_buf;
   DevBuf<int> dup_n;
@@ -1603,18 +1643,49 @@ void with_kt(const Ctx& c, int kt, F&& f) {
   }
 }
 
+// Brackets the launches of one tunable site with CUDA events while the
+// autotuner searches that site; otherwise does nothing.
+struct TuneScope {
+  Ctx& c;
+  cudaEvent_t e0 = nullptr;
+  cudaStream_t st;
+  static cudaEvent_t event(Ctx& c) {
+    if (!c.tuner.spare.empty()) {
+      cudaEvent_t e = c.tuner.spare.back();
+      c.tuner.spare.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    CK(cudaEventCreate(&e));
+    return e;
+  }
+  TuneScope(Ctx& c_, int site, cudaStream_t st_) : c(c_), st(st_) {
+    if (!c.tuner.on || c.tuner.site != site) return;
+    e0 = event(c);
+    CK(cudaEventRecord(e0, st));
+  }
+  ~TuneScope() {
+    if (!e0) return;
+    cudaEvent_t e1 = event(c);
+    cudaEventRecord(e1, st);
+    c.tuner.pending.push_back({e0, e1});
+  }
+};
+
 void launch_test_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaStream_t st) {
-  // sized from the round's sample count
-  int blocks = (int)std::min<long long>(148 * 8, std::max<long long>(1, (W + 255) / 256));
+  TuneScope ts(c, kTuneTest, st);
+  // sized from the round's sample count, at most 8 x 256 threads per SM
+  const int tb = c.tune.threads[kTuneTest];
+  int blocks = (int)std::min<long long>((long long)c.n_sm * 8 * 256 / tb, std::max<long long>(1, (W + tb - 1) / tb));
   with_kt(c, kt, [&](auto ktc, auto tt) {
     constexpr int KT = decltype(ktc)::value;
     using T = decltype(tt);
     if (flat)
-      k_test<KT, T, true><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
-                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
+      k_test<KT, T, true><<<blocks, tb, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
+                                                 c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
     else
-      k_test<KT, T, false><<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
-                                                   c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
+      k_test<KT, T, false><<<blocks, tb, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.work_off.p, n_gpairs,
+                                                  c.work_off.p + n_gpairs, c.flag.p, c.ev.p, c.ev_gp.p);
   });
   note_launch();
 }
@@ -1632,23 +1703,30 @@ ChainPool chain_pool(Ctx& c) {
 // a later round's items: the events of the round before, n_items =
 // round_dev[2] on the device, W bounds it
 void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaStream_t st) {
-  int blocks = grid_for(W, 256);
+  const int ti = c.tune.threads[kTuneItems], tc = c.tune.threads[kTuneChain];
+  int blocks = grid_for(W, ti);
   const long long* n_items = c.round_dev.p + 2;
   ChainPool pool = chain_pool(c);
   with_kt(c, kt, [&](auto ktc, auto tt) {
     constexpr int KT = decltype(ktc)::value;
     using T = decltype(tt);
     auto k = flat ? k_items<KT, T, true> : k_items<KT, T, false>;
-    k<<<blocks, 256, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
-                              c.round_dev.p + 6, c.ppw_slot_in.p, c.ppw_gp_in.p, c.op_pop.p, c.op_pair.p,
-                              c.op_slot.p, c.op_k.p, c.op_key.p, c.n_dev.p, c.op_cap,
-                              c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
-                              c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
-                              c.it_done.p, c.it_dec.p, c.it_gused.p, c.it_term.p);
+    {
+      TuneScope ts_items(c, kTuneItems, st);
+      k<<<blocks, ti, 0, st>>>(c.d_pops, c.gpair_pop.p, c.gpair_local.p, c.pop_pair_base.p, n_gpairs, n_items,
+                                c.round_dev.p + 6, c.ppw_slot_in.p, c.ppw_gp_in.p, c.op_pop.p, c.op_pair.p,
+                                c.op_slot.p, c.op_k.p, c.op_key.p, c.n_dev.p, c.op_cap,
+                                c.win_set.p, c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
+                                c.it_flag.p, c.it_key.p, c.it_c.p, c.it_gp.p, c.it_pos.p, c.it_len.p, c.it_head.p,
+                                c.it_done.p, c.it_dec.p, c.it_gused.p, c.it_term.p);
+    }
     auto kc = flat ? k_chain<KT, T, true> : k_chain<KT, T, false>;
-    kc<<<grid_for(W, 128), 128, 0, st>>>(c.d_pops, c.gpair_pop.p, n_items, c.it_flag.p, c.it_key.p, c.it_c.p,
-                                         c.it_gp.p, c.it_pos.p, c.it_dec.p, c.it_gused.p, pool, c.it_len.p,
-                                         c.it_head.p, c.it_done.p, c.it_term.p);
+    {
+      TuneScope ts_chain(c, kTuneChain, st);
+      kc<<<grid_for(W, tc), tc, 0, st>>>(c.d_pops, c.gpair_pop.p, n_items, c.it_flag.p, c.it_key.p, c.it_c.p,
+                                           c.it_gp.p, c.it_pos.p, c.it_dec.p, c.it_gused.p, pool, c.it_len.p,
+                                           c.it_head.p, c.it_done.p, c.it_term.p);
+    }
   });
   note_launch();
   note_launch();
@@ -1893,10 +1971,14 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   long long* Ed = c.round_dev.p + 1;
   ChainPool pool = chain_pool(c);
   if (W > 0) {
-    k_resolve_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
-                                                    c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p,
-                                                    c.round_dev.p, c.ev_len.p, c.ev_head.p, c.ev_app.p, pool,
-                                                    c.chain_list.p, c.round_dev.p + 4);
+    const int tr = c.tune.threads[kTuneResolve];
+    {
+      TuneScope ts(c, kTuneResolve, st);
+      k_resolve_set<<<grid_for(W, tr), tr, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+                                                      c.need_slot_set.p, c.need_id_set.p, c.win_set.p, c.dec_set.p,
+                                                      c.round_dev.p, c.ev_len.p, c.ev_head.p, c.ev_app.p, pool,
+                                                      c.chain_list.p, c.round_dev.p + 4);
+    }
     note_launch();
     scan_multi<int>(c, {{c.need_slot_set.p, W, Ed, c.rank_slot_set.p}, {c.need_id_set.p, W, Ed, c.rank_id_set.p}},
                     st);
@@ -1922,17 +2004,21 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   note_launch();
   if (W > 0) {
     // part 1, one thread per event: species and components
-    k_apply_move<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
-                                                        c.win_set.p, c.dec_set.p, c.rank_slot_set.p,
-                                                        c.slot_base_set.p, c.ice_set.p);
-    note_launch();
-    // part 2, one thread per event: removals, scalar fields, caches
-    k_apply_set<<<grid_for(W, 256), 256, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
-                                                  c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
-                                                  c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_done.p,
-                                                  c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
-                                                  c.ev_term.p, c.pop_pair_base.p);
-    note_launch();
+    const int ta = c.tune.threads[kTuneApply];
+    {
+      TuneScope ts(c, kTuneApply, st);
+      k_apply_move<<<grid_for(W, ta), ta, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+                                                          c.win_set.p, c.dec_set.p, c.rank_slot_set.p,
+                                                          c.slot_base_set.p, c.ice_set.p);
+      note_launch();
+      // part 2, one thread per event: removals, scalar fields, caches
+      k_apply_set<<<grid_for(W, ta), ta, 0, st>>>(c.d_pops, c.gpair_pop.p, Ed, c.ev_key.p, c.ev_c.p, c.gp_c.p,
+                                                    c.win_set.p, c.dec_set.p, c.rank_slot_set.p, c.rank_id_set.p,
+                                                    c.slot_base_set.p, c.id_base_set.p, c.ice_set.p, c.ev_done.p,
+                                                    c.ev_dest.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p, c.dec_set.p,
+                                                    c.ev_term.p, c.pop_pair_base.p);
+      note_launch();
+    }
     // chains, one warp each
     k_apply_chain<<<grid_for(W, 32), 32, 0, st>>>(c.d_pops, c.gpair_pop.p, c.pop_pair_base.p, c.chain_list.p,
                                                     c.round_dev.p + 4, c.ev_key.p, c.ev_len.p, c.ev_app.p,
@@ -1992,7 +2078,8 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
 // everything the captured launches depend on: sizes and device addresses
 std::vector<long long> round_graph_key(const Ctx& c, const RoundBounds& b) {
   return {c.n_pop, b.kt, b.flat, b.n_gpairs, b.W, b.max_chunks, b.max_cells, c.sort_blocks, (long long)c.sort_smem,
-          c.max_rounds, c.mode, c.ch_chunks,
+          c.max_rounds, c.mode, c.ch_chunks, c.tune.threads[kTuneItems], c.tune.threads[kTuneChain],
+          c.tune.threads[kTuneResolve], c.tune.threads[kTuneApply],
           (long long)c.d_pops, (long long)c.d_round, (long long)c.d_ctrs, (long long)c.round_dev.p,
           (long long)c.per_pop_i.p, (long long)c.pop_pair_base.p, (long long)c.gpair_pop.p,
           (long long)c.gpair_local.p, (long long)c.ev_key.p, (long long)c.ev_c.p, (long long)c.gp_c.p,
@@ -2376,8 +2463,10 @@ void step_parallel(Ctx& c, int kt) {
                                                            c.gpair_local.p, c.work_off.p, c.ev_key.p, c.ev_c.p,
                                                            c.gp_c.p, c.ev_pos.p, c.ev_len.p, c.ev_term.p);
     note_launch();
-    k_decide<<<grid_for(W, 256), 256, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.round_dev.p + 1, c.ev_key.p,
-                                                    c.ev_c.p, c.gp_c.p, c.dec_set.p);
+    const int td = c.tune.threads[kTuneResolve];
+    TuneScope ts(c, kTuneResolve, c.stream);
+    k_decide<<<grid_for(W, td), td, 0, c.stream>>>(c.d_pops, c.gpair_pop.p, c.round_dev.p + 1, c.ev_key.p, c.ev_c.p,
+                                                   c.gp_c.p, c.dec_set.p);
     note_launch();
   }
   resolve_apply(c, c.stream, W, Q);
@@ -2430,7 +2519,7 @@ void step_parallel(Ctx& c, int kt) {
     ensure_room(c, E + ppw + (kMaxCopies - 1) * Qb);
     // a round's items (events and walkers) each make at most one event
     if (!events_fit(c, E + ppw)) throw Fail(PMC_ERR_CAPACITY);
-    if (!graph_tried && c.use_graph && !c.pp_step && pp_lost == 0 && ppw == 0) {
+    if (!graph_tried && c.use_graph && !c.tuner.on && !c.pp_step && pp_lost == 0 && ppw == 0) {
       graph_tried = true;
       GraphRun g = run_round_graph(c, kt, flat, n_gpairs, E);
       if (g.rounds >= 0) {
@@ -2674,6 +2763,11 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   c.sample_buf.release();
   c.dup_n.release();
   c.select_buf.release();
+  for (auto& pr : c.tuner.pending) {
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  for (auto e : c.tuner.spare) cudaEventDestroy(e);
   cudaStreamDestroy(c.cap_stream);
   cudaStreamDestroy(c.stream);
   delete x;
@@ -2844,6 +2938,82 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
   return status;
 }
 
+// the autotuner around one step: the candidate's shape before it; after it
+// (finish_step has synchronised the stream) the device time of the site's
+// launches and the step's pair tests
+static void tune_before(Ctx& c) {
+  Tuner& t = c.tuner;
+  c.tune.threads[t.site] = kTuneCand[t.site][t.cand];
+}
+
+static void tune_after(Ctx& c, long long tests) {
+  Tuner& t = c.tuner;
+  for (auto& pr : t.pending) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    t.cand_ms += ms;
+    t.spare.push_back(pr.first);
+    t.spare.push_back(pr.second);
+  }
+  t.pending.clear();
+  t.cand_tests += tests;
+  if (++t.rep < kTuneReps) return;
+  const float score = (float)(t.cand_ms / (double)std::max(t.cand_tests, 1LL) * 1e6);
+  t.site_ms[t.site][t.cand] = score;
+  if (t.cand == 0 || score < t.best_ms) {
+    t.best_ms = score;
+    t.best = t.cand;
+  }
+  t.rep = 0;
+  t.cand_ms = 0.0;
+  t.cand_tests = 0;
+  if (++t.cand < kTuneCands) return;
+  c.tune.threads[t.site] = kTuneCand[t.site][t.best];
+  t.cand = 0;
+  if (++t.site < kTuneSites) return;
+  t.on = false;
+}
+
+int pmc_coag_gpu_autotune(pmc_coag_gpu_ctx* x, int enable) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  Tuner& t = x->c.tuner;
+  t.on = enable != 0;
+  t.site = t.cand = t.rep = t.best = 0;
+  t.best_ms = 0.f;
+  t.cand_ms = 0.0;
+  t.cand_tests = 0;
+  for (auto& pr : t.pending) {
+    t.spare.push_back(pr.first);
+    t.spare.push_back(pr.second);
+  }
+  t.pending.clear();
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_tune_state(pmc_coag_gpu_ctx* x, int* tuning, int* threads, float* ms) {
+  if (!x) return PMC_ERR_INVALID_ARG;
+  const Ctx& c = x->c;
+  if (tuning) *tuning = c.tuner.on ? 1 : 0;
+  if (threads)
+    for (int k = 0; k < kTuneSites; k++) threads[k] = c.tune.threads[k];
+  if (ms)
+    for (int k = 0; k < kTuneSites; k++)
+      for (int j = 0; j < kTuneCands; j++) ms[k * kTuneCands + j] = c.tuner.site_ms[k][j];
+  return PMC_OK;
+}
+
+int pmc_coag_gpu_set_tune(pmc_coag_gpu_ctx* x, const int* threads) {
+  if (!x || !threads) return PMC_ERR_INVALID_ARG;
+  for (int k = 0; k < kTuneSites; k++) {
+    bool ok = false;
+    for (int j = 0; j < kTuneCands; j++) ok = ok || threads[k] == kTuneCand[k][j];
+    if (!ok) return PMC_ERR_INVALID_ARG;
+  }
+  for (int k = 0; k < kTuneSites; k++) x->c.tune.threads[k] = threads[k];
+  x->c.tuner.on = false;
+  return PMC_OK;
+}
+
 int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* temp,
                             const double* pressure, double additive_coeff, double del_t, int n_steps,
                             int64_t* tot_n_samp, int64_t* tot_n_coag) {
@@ -2879,8 +3049,10 @@ int pmc_coag_gpu_step_batch(pmc_coag_gpu_ctx* x, int kernel_type, const double* 
     } else {
       ProfScope ps(c, 3, 1);
       c.replay.valid = false;  // the parallel step reorders and rewrites slots
+      if (c.tuner.on) tune_before(c);
       step_parallel(c, kernel_type);
       status = finish_step(c, &s, &k);
+      if (c.tuner.on && status == 0) tune_after(c, s);
     }
     S += s;
     K += k;

@@ -528,16 +528,28 @@ __device__ __forceinline__ int walk_pair(const Stretch& s, double at) {
   return a;
 }
 
-// One walk test of particle x (records qxd/qxf) at running position at of
+// Partner draws of a chain's test t after the first: the walk stream's
+// block (x, t + r * 2^26) for the r-th redraw (t stays below 2^26).
+constexpr uint32_t kChainRedraws = 64;
+__device__ __forceinline__ uint32_t walk_redraw(const PopDev& P, int x, uint32_t t, uint32_t r) {
+  return walk_draws(P, x, t | (r << 26)).x;
+}
+
+// One walk test t of particle x (records qxd/qxf) at running position at of
 // its stretch, in entry j: the partner drawn from the other cell's members
 // and the accept test.  The pair's fields and the partner slot are loaded
-// together, then the partner's state.  Returns 0 for no test (no member,
-// itself, a dead or moved member, or one this chain absorbed), 1 for a
-// rejected test, 2 for an accepted one, -1 for a failed bounds check.
+// together, then the partner's state.  In a chain, a partner that the chain
+// has absorbed already is drawn again: the reference draws a pair's samples
+// from the members left when each sample runs, after the earlier samples'
+// merges, and exits the pair when a cell is empty (per_set_coag,
+// coagulation.F90:628-638); a test whose kChainRedraws draws all land on
+// absorbed members counts as that exit.  Returns 0 for no test (no member,
+// itself, a dead or moved member, the exit), 1 for a rejected test, 2 for an
+// accepted one, -1 for a failed bounds check.
 template <int KT, class T, bool FLAT>
-__device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& s, int j, double at, uint32_t pick,
-                                         uint32_t accu, const RecD& qxd, const RecF& qxf, bool chain, int* y_out,
-                                         float* pos_out, int* q_out, bool* first_out, double* ry_out,
+__device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& s, int j, double at, uint32_t t,
+                                         uint32_t pick, uint32_t accu, const RecD& qxd, const RecF& qxf, bool chain,
+                                         int* y_out, float* pos_out, int* q_out, bool* first_out, double* ry_out,
                                          double* vty_out) {
   const double c0 = s.cum[j], c1 = s.cum[j + 1];
   const int4 ent = P.cp_ent[j];
@@ -552,7 +564,15 @@ __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& 
   const bool first = (ent.y >> 30) & 1;
   int i = (int)(u32d(pick) * (double)n_o);
   if (i >= n_o) i = n_o - 1;
-  const int y = P.list[o_start + i];
+  int y = P.list[o_start + i];
+  if (chain) {
+    for (uint32_t r = 1; y >= 0 && y < P.cap && claimed_by_walk(P, y, x); r++) {
+      if (r >= kChainRedraws) return 0;
+      i = (int)(u32d(walk_redraw(P, x, t, r)) * (double)n_o);
+      if (i >= n_o) i = n_o - 1;
+      y = P.list[o_start + i];
+    }
+  }
   const PairDesc d = P.pair_desc[q];
   const PairState& S = P.pair[q];
   const double inv_k_max = S.inv_k_max, fflat = S.fflat;
@@ -565,7 +585,6 @@ __device__ __forceinline__ int walk_test(const PopDev& P, int x, const Stretch& 
   const int cell_y = P.cell[y];
   const double ry = P.rad[y], vty = P.vtot[y];  // for the merge decision if the test accepts
   if (y == x || !alive || cell_y != O) return 0;
-  if (chain && claimed_by_walk(P, y, x)) return 0;  // absorbed earlier in this chain
   const double u = u32d(accu);
   bool acc;
   if constexpr (sizeof(T) == 8) {
@@ -622,7 +641,7 @@ __device__ __forceinline__ int walk_next(const PopDev& P, int x, Stretch& s, uin
     int j = walk_pair(s, at);
     s.j = j;
     s.at = at;
-    int r = walk_test<KT, T, FLAT>(P, x, s, j, at, u.z, u.w, qxd, qxf, chain, y, pos, q, first, ry, vty);
+    int r = walk_test<KT, T, FLAT>(P, x, s, j, at, t, u.z, u.w, qxd, qxf, chain, y, pos, q, first, ry, vty);
     if (r < 0) return -1;
     if (r == 0) continue;
     (*n_tests)++;
