@@ -29,13 +29,10 @@ sys.path.insert(0, HERE)
 B_TEST = 56  # algorithmic bytes per pair test: two cell-list entries and two 24-byte records
 B_SORT = 8  # per slot: its cell key read, its cell-list entry written
 # DRAM traffic per unit (dram__bytes_read.sum + dram__bytes_write.sum) from
-# ncu captures of one launch at this workload: k_test read 46.91 MB and wrote
-# 1.12 MB for about 209,000 tests; k_sort_all read 4.04 MB and wrote none for
+# ncu captures of one launch at this workload: k_test read 27.29 MB and wrote
+# 1.5 kB for about 209,000 tests; k_sort_all read 4.04 MB and wrote none for
 # 1e6 slots.  The roofline's traffic scales these by the units of a launch.
-# The k_test capture predates the pass that now draws the accepted samples'
-# merge decisions (k_decide): it includes their reads, so for the current
-# kernel it is an upper bound.
-DRAM_TEST = (46.91e6 + 1.12e6) / 209000
+DRAM_TEST = (27.29e6 + 1.5e3) / 209000
 DRAM_SORT = 4.04e6 / 1e6
 
 
