@@ -216,12 +216,12 @@ __global__ void k_compact_items(const uint8_t* it_flag, const long long* off, co
                                 const float* it_pos, const int* it_len, const int* it_head, const uint8_t* it_done,
                                 const uint32_t* it_dec, const int4* it_term, unsigned long long* ev_key, int2* ev_c,
                                 int* gp_c, float* ev_pos, int* ev_len, int* ev_head, uint8_t* ev_done, uint32_t* dec,
-                                int4* ev_term) {
+                                int4* ev_term, const long long* grouped) {
   long long n = *n_items;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     if (it_flag[i]) {
-      long long e = off[i];
+      long long e = grouped ? grouped[i] : off[i];
       ev_key[e] = it_key[i];
       ev_c[e] = it_c[i];
       gp_c[e] = it_gp[i];
@@ -482,7 +482,7 @@ __global__ void k_double(PopDev P, int n, const uint8_t* flag, const long long* 
     if (!flag[i]) continue;
     int d = n + (int)off[i];
     if (d >= P.cap) {
-      set_status(P.ctr, kErrCapacity);
+      cap_fail(P.ctr, kCapDupSlot);
       continue;
     }
     copy_particle(P, i, d, id0 + off[i]);
@@ -648,6 +648,8 @@ __global__ void k_eval_kernel(PopDev P, int n, const double* v1, const int* c1, 
 
 char g_last_error[512];
 char g_last_assert[256];  // site and index of the last failed device bounds check
+char g_last_capacity[256];  // which limit the last PMC_ERR_CAPACITY hit
+[[noreturn]] void cap_throw(const char* why);
 // kernel launches issued by this library (for the benchmark's launch count)
 long long g_launches = 0;
 inline void note_launch() { ++g_launches; }
@@ -656,6 +658,12 @@ struct Fail {
   int code;
   explicit Fail(int c) : code(c) {}
 };
+
+void cap_throw(const char* why) {
+  cudaGetLastError();  // a failed allocation leaves an error behind
+  snprintf(g_last_capacity, sizeof(g_last_capacity), "capacity exceeded: %s", why);
+  throw Fail(PMC_ERR_CAPACITY);
+}
 
 template <class T>
 struct DevBuf {
@@ -671,7 +679,7 @@ struct DevBuf {
     n = 0;
     if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) {
       p = nullptr;
-      throw Fail(PMC_ERR_CAPACITY);
+      cap_throw("device memory: an allocation failed");
     }
     n = want;
   }
@@ -694,7 +702,7 @@ struct PinnedBuf {
     size_t want = std::max<size_t>(b + b / 4, 1 << 20);
     if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) {
       p = nullptr;
-      throw Fail(PMC_ERR_CAPACITY);
+      cap_throw("page-locked host memory: an allocation failed");
     }
     bytes = want;
   }
@@ -719,7 +727,7 @@ struct MappedBuf {
         cudaHostGetDevicePointer(&dev, p, 0) != cudaSuccess) {
       cudaGetLastError();
       release();
-      throw Fail(PMC_ERR_CAPACITY);
+      cap_throw("mapped host memory: an allocation failed");
     }
     bytes = want;
   }
@@ -890,6 +898,13 @@ struct Ctx {
   DevBuf<long long> graph_stats;
   Tune tune;
   Tuner tuner;
+  // removal pool of the round's target operations
+  DevBuf<int> pp_rm_n, pp_rm_pool;
+  // a batched round's lists grouped by population (group_by_pop)
+  DevBuf<int> grp_hist, item_pop, g_pop, g_pair, g_slot, g_k;
+  DevBuf<long long> grp_off, grp_dest;
+  DevBuf<unsigned long long> g_key;
+  DevBuf<long long> pp_rm_off, pp_rm_tot;
   // initial-condition sampler: staging of the modes, copy counts, radix select
   DevBuf<double> sample_buf;
   DevBuf<int> dup_n;
@@ -998,7 +1013,8 @@ void free_list(std::vector<void*>& v) {
 template <class T>
 T* dalloc(std::vector<void*>& owner, size_t n) {
   void* p = nullptr;
-  if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) throw Fail(PMC_ERR_CAPACITY);
+  if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess)
+    cap_throw("device memory: an allocation failed");
   owner.push_back(p);
   return (T*)p;
 }
@@ -1085,7 +1101,7 @@ void scan_multi(Ctx& c, std::initializer_list<ScanArg<T>> args, cudaStream_t st 
     k++;
   }
   if (k == 0) return;
-  if (nb > (1LL << 30)) throw Fail(PMC_ERR_CAPACITY);
+  if (nb > (1LL << 30)) cap_throw("scan longer than its tile limit");
   c.scan_status.reserve((size_t)kScanMaxJobs * nb);
   if (c.scan_status.n > c.scan_status_n) {  // fresh memory: clear it once
     CK(cudaMemsetAsync(c.scan_status.p, 0, sizeof(unsigned long long) * c.scan_status.n, st));
@@ -1223,7 +1239,7 @@ void alloc_sort(Ctx& c, PopHost& ph) {
           ph.pair_desc.push_back(d);
         }
   h.n_pairs = (int)ph.pair_desc.size();
-  if (h.n_pairs >= (1 << 20)) throw Fail(PMC_ERR_CAPACITY);  // pair numbers in keys and random streams
+  if (h.n_pairs >= (1 << 20)) cap_throw("more than 2^20 bin pairs");  // pair numbers in keys and random streams
   // the pairs of each cell in loop order, for walks
   {
     std::vector<int> off(h.n_cells + 1, 0), list;
@@ -1452,7 +1468,7 @@ size_t size_sort(Ctx& c, int max_cells) {
   if (smem != c.sort_smem) {
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_all, kSortThreads, smem));
-    if (per_sm < 1) throw Fail(PMC_ERR_CAPACITY);
+    if (per_sm < 1) cap_throw("the sort does not fit one block per multiprocessor");
     c.sort_blocks = per_sm * c.n_sm;
     c.sort_smem = smem;
   }
@@ -1604,7 +1620,7 @@ void sort_pops(Ctx& c, bool decide_grid) {
       if (need) {
         double gmin = rmin / 10.0, gmax = rmax * 10.0;
         int n_bin = (int)ceil((log10(gmax) - log10(gmin)) * 10.0);
-        if (n_bin > kMaxBin) throw Fail(PMC_ERR_CAPACITY);
+        if (n_bin > kMaxBin) cap_throw("more than 256 bins");
         make_grid(c, ph, n_bin, gmin, gmax);
       }
       // a new grid or a population without a valid sort: all bins change
@@ -1732,12 +1748,136 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
   note_launch();
 }
 
-void launch_pp(Ctx& c, int kt, long long Q) {
+// Stable grouping by population of a batched context's per-round lists.
+// Slot and ID ranks come from one scan over a list, and the per-population
+// bases of k_alloc_bases assume that each population's entries lie together
+// and in population order.  Round 0's samples and target operations are
+// built that way; later rounds add entries from every population at the end
+// (the walkers of target operations, and the target operations that walks
+// add).  Entry i with population pop_of[i] >= 0 (negative: not kept) goes to
+// dest[i]: all of population 0 first, then 1, ..., each in list order.
+// Tiles of kGrpTile entries: per tile and population a count (hist, laid
+// out population-major so that one scan gives every (population, tile) its
+// start), then each entry's rank within its tile.
+constexpr int kGrpTile = 256;
+
+__global__ void __launch_bounds__(kGrpTile) k_grp_hist(const long long* n, const int* pop_of, int n_pop, int n_tiles,
+                                                       int* hist, PopCtr* ctr0) {
+  const long long N = *n;
+  const long long i = blockIdx.x * (long long)kGrpTile + threadIdx.x;
+  if (i >= N) return;
+  const int p = pop_of[i];
+  if (p < 0) return;
+  if (p >= n_pop || blockIdx.x >= (unsigned)n_tiles) {
+    bad_index(ctr0, kBadEventSlot, p);
+    return;
+  }
+  atomicAdd(&hist[(size_t)p * n_tiles + blockIdx.x], 1);
+}
+
+__global__ void __launch_bounds__(kGrpTile) k_grp_rank(const long long* n, const int* pop_of, int n_tiles,
+                                                       const long long* off, long long* dest) {
+  __shared__ int wpop[kGrpTile / 32][32], wcnt[kGrpTile / 32][32];
+  const long long N = *n;
+  const long long i = blockIdx.x * (long long)kGrpTile + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = i < N ? pop_of[i] : -1;
+  const unsigned same = __match_any_sync(0xffffffffu, p);
+  const int rank = __popc(same & ((1u << lane) - 1u));
+  // one entry per distinct population of the warp: its count there
+  wpop[w][lane] = -1;
+  wcnt[w][lane] = 0;
+  __syncthreads();
+  // the lowest lane of each group writes at its own lane index
+  if (rank == 0) {
+    wpop[w][lane] = p;
+    wcnt[w][lane] = __popc(same);
+  }
+  __syncthreads();
+  if (p < 0) return;
+  int before = 0;
+  for (int v = 0; v < w; v++)
+    for (int l = 0; l < 32; l++)
+      if (wpop[v][l] == p) before += wcnt[v][l];
+  dest[i] = off[(size_t)p * n_tiles + blockIdx.x] + before + rank;
+}
+
+__global__ void k_scatter_ops(const long long* n_ops, const long long* dest, const int* pop, const int* pair,
+                              const int* slot, const int* k, const unsigned long long* key, int* pop_o, int* pair_o,
+                              int* slot_o, int* k_o, unsigned long long* key_o) {
+  const long long Q = *n_ops;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q; q += (long long)gridDim.x * blockDim.x) {
+    const long long d = dest[q];
+    pop_o[d] = pop[q];
+    pair_o[d] = pair[q];
+    slot_o[d] = slot[q];
+    k_o[d] = k[q];
+    key_o[d] = key[q];
+  }
+}
+
+// the population of each kept item of a later round (-1 for an item that
+// made no event)
+__global__ void k_item_pops(const long long* n_items, const uint8_t* it_flag, const int* it_gp, const int* gpair_pop,
+                            int n_gpairs, int* pop_of) {
+  const long long n = *n_items;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int gp = it_gp[i];
+    pop_of[i] = (it_flag[i] && gp >= 0 && gp < n_gpairs) ? gpair_pop[gp] : -1;
+  }
+}
+
+// dest for the entries of a list of at most bound entries (count *n on the
+// device), grouped by population (k_grp_hist, k_grp_rank)
+void group_by_pop(Ctx& c, const long long* n, long long bound, const int* pop_of, long long* dest, cudaStream_t st) {
+  const int n_tiles = (int)std::max<long long>(1, (bound + kGrpTile - 1) / kGrpTile);
+  const long long nh = (long long)n_tiles * c.n_pop;
+  c.grp_hist.reserve((size_t)nh);
+  c.grp_off.reserve((size_t)nh + 1);
+  CK(cudaMemsetAsync(c.grp_hist.p, 0, sizeof(int) * (size_t)nh, st));
+  k_grp_hist<<<n_tiles, kGrpTile, 0, st>>>(n, pop_of, c.n_pop, n_tiles, c.grp_hist.p, c.d_ctrs);
+  note_launch();
+  scan_multi<int>(c, {ScanArg<int>{c.grp_hist.p, nh, nullptr, c.grp_off.p}}, st);
+  k_grp_rank<<<n_tiles, kGrpTile, 0, st>>>(n, pop_of, n_tiles, c.grp_off.p, dest);
+  note_launch();
+}
+
+// The round's target operations (at most Q, counted on the device): the
+// bound on each one's removals, scanned into its place in the removal pool
+// (one read-back sizes the pool), then the operations themselves.  Steps
+// with target operations run their rounds from the host, so the read-back
+// never falls inside a graph.
+void launch_pp(Ctx& c, int kt, long long Q, bool grouped) {
   int blocks = grid_for(Q, 128);
+  if (!grouped && c.n_pop > 1) {
+    c.grp_dest.reserve((size_t)Q + 1);
+    c.g_pop.reserve(Q); c.g_pair.reserve(Q); c.g_slot.reserve(Q); c.g_k.reserve(Q); c.g_key.reserve(Q);
+    group_by_pop(c, c.n_dev.p + 0, Q, c.op_pop.p, c.grp_dest.p, c.stream);
+    k_scatter_ops<<<grid_for(Q, 256), 256, 0, c.stream>>>(c.n_dev.p + 0, c.grp_dest.p, c.op_pop.p, c.op_pair.p,
+                                                          c.op_slot.p, c.op_k.p, c.op_key.p, c.g_pop.p, c.g_pair.p,
+                                                          c.g_slot.p, c.g_k.p, c.g_key.p);
+    note_launch();
+    std::swap(c.op_pop, c.g_pop); std::swap(c.op_pair, c.g_pair); std::swap(c.op_slot, c.g_slot);
+    std::swap(c.op_k, c.g_k); std::swap(c.op_key, c.g_key);
+  }
+  c.pp_rm_n.reserve((size_t)Q + 1);
+  c.pp_rm_off.reserve((size_t)Q + 2);
+  c.pp_rm_tot.reserve(1);
+  k_pp_count<<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
+                                           c.n_dev.p + 0, c.pp_rm_n.p);
+  note_launch();
+  CK(cudaMemsetAsync(c.pp_rm_tot.p, 0, sizeof(long long), c.stream));
+  scan_multi<int>(c, {ScanArg<int>{c.pp_rm_n.p, Q, c.n_dev.p + 0, c.pp_rm_off.p, c.pp_rm_tot.p}});
+  long long tot = 0;
+  CK(cudaMemcpyAsync(&tot, c.pp_rm_tot.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  check_scan_err(c);
+  c.pp_rm_pool.reserve((size_t)std::max(tot, 1LL));
   with_kt(c, kt, [&](auto ktc, auto) {
     constexpr int KT = decltype(ktc)::value;
     k_pp_ops<KT><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
-                                               c.op_key.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p);
+                                               c.op_key.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p, c.pp_rm_off.p,
+                                               c.pp_rm_pool.p);
   });
   note_launch();
 }
@@ -1881,6 +2021,7 @@ __global__ void k_step_reset(PopCtr* ctrs, int n_pop) {
   ctrs[k].status = 0;
   ctrs[k].bad_site = 0;
   ctrs[k].bad_index = 0;
+  ctrs[k].cap_site = 0;
 }
 
 __global__ void k_fill_claims(const PopDev* pops) {
@@ -1987,7 +2128,7 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   // redone ones, then those that walks appended)
   if (Q > 0) {
     k_pp_resolve<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.op_key.p, c.n_dev.p, c.pp_res.p,
-                                                   c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
+                                                   c.pp_rm_pool.p, c.win_pp.p, c.need_slot_pp.p, c.need_id_pp.p, c.lost_pp.p);
     note_launch();
     scan_multi<int>(c, {{c.need_slot_pp.p, Q, c.n_dev.p, c.rank_slot_pp.p}, {c.need_id_pp.p, Q, c.n_dev.p, c.rank_id_pp.p}},
                     st);
@@ -2028,7 +2169,7 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   }
   if (Q > 0) {
     k_pp_apply<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
-                                                 c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p, c.slot_base_pp.p,
+                                                 c.pp_rm_pool.p, c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p, c.slot_base_pp.p,
                                                  c.id_base_pp.p, c.pop_pair_base.p, c.ppw_slot.p, c.ppw_gp.p,
                                                  c.round_dev.p + 5, c.ppw_cap);
     note_launch();
@@ -2063,14 +2204,28 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
   }
   if (Q > 0) set_n_dev(c, Qn);
   launch_items_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
-  if (Q > 0) launch_pp(c, b.kt, Q);
+  if (Q > 0) launch_pp(c, b.kt, Q, false);
   const long long* Id = c.round_dev.p + 2;
   long long* Ed = c.round_dev.p + 1;
   scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.it_flag.p, W, Id, c.it_off.p, Ed}}, st);
+  // a batched step with target operations: the walkers they made join the
+  // items after the events, from every population, so the events are
+  // grouped by population for the allocation (group_by_pop)
+  const long long* grouped = nullptr;
+  if (c.pp_step && c.n_pop > 1) {
+    c.item_pop.reserve((size_t)W + 1);
+    c.grp_dest.reserve((size_t)W + 1);
+    k_item_pops<<<grid_for(W, 256), 256, 0, st>>>(Id, c.it_flag.p, c.it_gp.p, c.gpair_pop.p, b.n_gpairs,
+                                                  c.item_pop.p);
+    note_launch();
+    group_by_pop(c, Id, W, c.item_pop.p, c.grp_dest.p, st);
+    grouped = c.grp_dest.p;
+  }
   k_compact_items<<<grid_for(W, 256), 256, 0, st>>>(c.it_flag.p, c.it_off.p, Id, c.it_key.p, c.it_c.p, c.it_gp.p,
                                                     c.it_pos.p, c.it_len.p, c.it_head.p, c.it_done.p, c.it_dec.p,
                                                     c.it_term.p, c.ev_key.p, c.ev_c.p, c.gp_c.p, c.ev_pos.p,
-                                                    c.ev_len.p, c.ev_head.p, c.ev_done.p, c.dec_set.p, c.ev_term.p);
+                                                    c.ev_len.p, c.ev_head.p, c.ev_done.p, c.dec_set.p, c.ev_term.p,
+                                                    grouped);
   note_launch();
   resolve_apply(c, st, W, Q);
 }
@@ -2413,7 +2568,7 @@ void step_parallel(Ctx& c, int kt) {
       hw[4] = Q;
     }
     // sample numbers fit in a key's 31 bits below the walk flag of the merge stream
-    if (W + Q + 1 >= 0x7fffffffLL) throw Fail(PMC_ERR_CAPACITY);
+    if (W + Q + 1 >= 0x7fffffffLL) cap_throw("more than 2^31 samples in one step");
   }
   // capacity for the worst case of this round: every sample creates a
   // particle and every target operation makes kMaxCopies - 1 copies
@@ -2452,7 +2607,7 @@ void step_parallel(Ctx& c, int kt) {
     c.pp_res.reserve(Q);
     c.pp_vol.reserve((size_t)Q * c.n_spec);
     set_n_dev(c, Q);
-    launch_pp(c, kt, Q);
+    launch_pp(c, kt, Q, true);  // built in population order
   }
   // accepted samples in sample order; the sample count is work_off[n_gpairs]
   // and the event count E goes to round_dev[1], both on the device
@@ -2518,7 +2673,7 @@ void step_parallel(Ctx& c, int kt) {
     // kMaxCopies - 1 per target operation
     ensure_room(c, E + ppw + (kMaxCopies - 1) * Qb);
     // a round's items (events and walkers) each make at most one event
-    if (!events_fit(c, E + ppw)) throw Fail(PMC_ERR_CAPACITY);
+    if (!events_fit(c, E + ppw)) cap_throw("a round's events past the event arrays");
     if (!graph_tried && c.use_graph && !c.tuner.on && !c.pp_step && pp_lost == 0 && ppw == 0) {
       graph_tried = true;
       GraphRun g = run_round_graph(c, kt, flat, n_gpairs, E);
@@ -2605,7 +2760,7 @@ const char* pmc_coag_gpu_status_string(int s) {
     case PMC_OK: return "ok";
     case PMC_ERR_INVALID_ARG: return "invalid argument";
     case PMC_ERR_OUT_OF_GRID: return "particle outside of bin_grid: try reducing the timestep del_t";
-    case PMC_ERR_CAPACITY: return "capacity exceeded";
+    case PMC_ERR_CAPACITY: return g_last_capacity[0] ? g_last_capacity : "capacity exceeded";
     case PMC_ERR_CUDA: return g_last_error[0] ? g_last_error : "CUDA error";
     case PMC_ERR_TIMEOUT: return "bounded device loop ran out of iterations";
     case PMC_ERR_RNG_EXHAUSTED: return "replay stream exhausted";
@@ -2761,6 +2916,14 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   free_redraw_graph(c);
   c.graph_stats.release();
   c.sample_buf.release();
+  c.pp_rm_n.release();
+  for (auto* b : {&c.grp_hist, &c.item_pop, &c.g_pop, &c.g_pair, &c.g_slot, &c.g_k}) b->release();
+  c.grp_off.release();
+  c.grp_dest.release();
+  c.g_key.release();
+  c.pp_rm_pool.release();
+  c.pp_rm_off.release();
+  c.pp_rm_tot.release();
   c.dup_n.release();
   c.select_buf.release();
   for (auto& pr : c.tuner.pending) {
@@ -2917,6 +3080,18 @@ static int finish_step(Ctx& c, long long* samp, long long* coag) {
       if (!status) status = PMC_ERR_CAPACITY;
     }
     if (r.status && !status) status = r.status;
+    if (r.status == kErrCapacity && r.cap_site) {
+      static const char* site[] = {"", "an event's new particle past the slot arrays",
+                                   "the round's target-operation list is full",
+                                   "a target operation's removals past its share of the pool",
+                                   "more dup copies than one target operation holds",
+                                   "a target operation's copy past the slot arrays",
+                                   "the walker list of target operations is full",
+                                   "a sampled particle past the slot arrays",
+                                   "a doubled or dup copy past the slot arrays"};
+      snprintf(g_last_capacity, sizeof(g_last_capacity), "capacity exceeded: %s (population %d)",
+               r.cap_site < 9 ? site[r.cap_site] : "?", p);
+    }
     if (r.bad_site) {
       static const char* site[] = {"", "pair test: list position", "pair test: slot", "event: slot",
                                    "sort scatter: list position", "sort: chunk histogram size",

@@ -57,6 +57,12 @@ enum Stream : uint32_t {
 
 __device__ __forceinline__ void set_status(PopCtr* c, int code) { atomicCAS(&c->status, 0, code); }
 
+// a capacity limit hit on the device: the status and the first site
+__device__ __forceinline__ void cap_fail(PopCtr* c, int site) {
+  atomicCAS(&c->cap_site, 0, site);
+  set_status(c, kErrCapacity);
+}
+
 // a failed bounds check: record the first site and index, flag the step
 __device__ __noinline__ void bad_index(PopCtr* c, int site, long long idx) {
   if (atomicCAS(&c->bad_site, 0, site) == 0) c->bad_index = idx;

@@ -320,7 +320,7 @@ __global__ void k_apply_set(const PopDev* pops, const int* gpair_pop, const long
     }
     int dest = event_dest(m, s1, s2, slot_base[pop], m.rm1 || m.rm2 ? 0 : slot_rank[e]);
     if (dest >= P.cap) {
-      set_status(P.ctr, kErrCapacity);
+      cap_fail(P.ctr, kCapEventDest);
       continue;
     }
     if (dest < 0) {
@@ -730,7 +730,7 @@ __device__ __noinline__ void add_target_op(const PopDev& P, int pop, int q, int 
                                               long long op_cap) {
   const unsigned long long k = atomicAdd((unsigned long long*)n_ops, 1ULL);
   if ((long long)k >= op_cap) {
-    set_status(P.ctr, kErrCapacity);
+    cap_fail(P.ctr, kCapTargetOps);
     return;
   }
   op_pop[k] = pop;
@@ -1390,17 +1390,16 @@ __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
 // Per-particle (accelerated) path, phase 1: run sample_source_particle and
 // the target update of coag_target_with_source for one target, store the
 // result, and claim the target and every removed source.
-constexpr int kMaxRemove = 64;  // removals stored per target operation
-constexpr int kMaxCopies = 8;   // dup copies per target operation
+constexpr int kMaxCopies = 8;  // dup copies per target operation (the growth limit keeps them at 2 or less)
 
 struct PPResult {
   int target, p;        // target slot, pair (local)
   int n_samp, n_coag;   // counted into tot_n_samp / tot_n_coag when the operation is applied
   int merged;           // n_coag > 0
   int n_copies;         // prob_round(old_nc / new_nc); 0 removes the target
-  int n_rm;
+  int n_rm;             // sources it removes: rm_pool[rm_off .. rm_off + n_rm)
   int copy_group[kMaxCopies];
-  int rm[kMaxRemove];
+  long long rm_off;
   PMeta meta;           // new target metadata
 };
 
@@ -1411,10 +1410,51 @@ __device__ double pp_kernel(const PopDev& P, const RecD& qs, const RecD& qt, int
   return pair_kernel<KT, double, false>(P, a, b, cs, ct, ct, 0.0, P.coeff);
 }
 
+// The first draws of a target operation: the number of removal samples,
+// which bounds the sources it can remove (sample_source_particle,
+// coagulation.F90:397).  k_pp_count stores that bound per operation;
+// its scan places every operation's removals in one pool, so an operation
+// can remove any number of sources.  Returns -1 for an operation that
+// draws nothing (void, dead target, empty source cell).
+__device__ __forceinline__ int pp_remove_bound(const PopDev& P, int p, int t, int k, Rng* g_out, int* n_extra,
+                                               double* prm_out) {
+  if (t < 0 || t >= P.cap || !P.alive[t]) return -1;
+  const PairState& S = P.pair[p];
+  const GridDev& G = *P.grid;
+  int nb = G.n_bin;
+  int src_cell = S.bs + nb * S.cs;
+  if (P.cell_count[src_cell] == 0) return -1;
+  double nc_target = P.recd[t].nc;
+  double nc_src_min = num_conc_at_radius<double>(P.w, S.cs, G.edges[S.bs]);
+  double prm_max = nc_target / nc_src_min;
+  if (!(prm_max <= 1.0)) return -2;
+  Rng g = make_rng(P, kStreamPart, (uint32_t)p, (uint32_t)k);
+  int n_remove = rand_poisson(g, prm_max * S.nspt);
+  *n_extra = rand_poisson(g, (1.0 - prm_max) * S.nspt);
+  *g_out = g;
+  *prm_out = prm_max;
+  return n_remove;
+}
+
+__global__ void k_pp_count(const PopDev* pops, const int* op_pop, const int* op_pair, const int* op_slot,
+                           const int* op_k, const long long* n_ops, int* rm_n) {
+  long long Q = *n_ops;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
+       q += (long long)gridDim.x * blockDim.x) {
+    const PopDev& P = pops[op_pop[q]];
+    Rng g(0, 0, 0, 0);
+    int n_extra = 0;
+    double prm = 0.0;
+    int n = pp_remove_bound(P, op_pair[q], op_slot[q], op_k[q], &g, &n_extra, &prm);
+    rm_n[q] = n > 0 ? n : 0;
+  }
+}
+
 template <int KT>
 __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pair,
                          const int* op_slot, const int* op_k, const unsigned long long* op_key,
-                         const long long* n_ops, PPResult* res, double* res_vol) {
+                         const long long* n_ops, PPResult* res, double* res_vol, const long long* rm_off,
+                         int* rm_pool) {
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
@@ -1429,6 +1469,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     R.merged = 0;
     R.n_copies = 1;
     R.n_rm = 0;
+    R.rm_off = rm_off[q];
     if (t < 0 || t >= P.cap || !P.alive[t]) continue;  // t = -1: a redo voided by k_build_redo
     const PairState& S = P.pair[p];
     const GridDev& G = *P.grid;
@@ -1487,6 +1528,14 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
       int ie = rand_int(g, n_src);
       int e = src_start + ie - 1;
       int si = P.list[e];
+      // a source this operation removed already has left the bin in the
+      // reference, whose later samples draw from the sources left
+      // (coagulation.F90:428-430): draw again
+      for (int r = 0; r < 64 && R.n_rm > 0 && P.claim[si] == claim_key(P, prio); r++) {
+        ie = rand_int(g, n_src);
+        e = src_start + ie - 1;
+        si = P.list[e];
+      }
       RecD qs = P.recd[si];
       double k = pp_kernel<KT>(P, qs, qt, cs, ct);
       double pc = k * S.inv_k_max;
@@ -1510,13 +1559,13 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
           double pri = nc_target / qs.nc;
           if (g.next() < pri / prm_max) {
             bool dup = false;
-            for (int z = 0; z < R.n_rm; z++) dup = dup || (R.rm[z] == si);
+            for (int z = 0; z < R.n_rm; z++) dup = dup || (rm_pool[R.rm_off + z] == si);
             if (!dup) {
-              if (R.n_rm < kMaxRemove) {
-                R.rm[R.n_rm++] = si;
+              if (R.n_rm < n_remove) {  // at most one per removal sample: the pool holds n_remove
+                rm_pool[R.rm_off + R.n_rm++] = si;
                 atomicMin(&P.claim[si], claim_key(P, prio));
               } else {
-                set_status(P.ctr, kErrCapacity);
+                cap_fail(P.ctr, kCapRemovals);
               }
             }
           }
@@ -1595,7 +1644,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     double new_nc = num_conc_at_radius<double>(P.w, cc, rnew);
     int n_copies = prob_round(g, old_nc / new_nc);
     if (n_copies > kMaxCopies) {
-      set_status(P.ctr, kErrCapacity);
+      cap_fail(P.ctr, kCapCopies);
       n_copies = kMaxCopies;
     }
     for (int z = 1; z < n_copies; z++) R.copy_group[z] = rand_group(g, P.w, cc, rnew);
@@ -1608,7 +1657,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
 
 // phase 2a: winners and allocation needs of the target operations
 __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsigned long long* op_key,
-                             const long long* n_ops, const PPResult* res, uint8_t* win,
+                             const long long* n_ops, const PPResult* res, const int* rm_pool, uint8_t* win,
                              int* need_slot, int* need_id, int* lost) {
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
@@ -1618,7 +1667,7 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
     unsigned long long prio = op_key[q];
     bool ok = true;
     if (R.merged) ok = ok && holds_slot(P, R.target, claim_key(P, prio), true);
-    for (int z = 0; z < R.n_rm; z++) ok = ok && holds_slot(P, R.rm[z], claim_key(P, prio), true);
+    for (int z = 0; z < R.n_rm; z++) ok = ok && holds_slot(P, rm_pool[R.rm_off + z], claim_key(P, prio), true);
     win[q] = ok ? 1 : 0;
     lost[q] = ok ? 0 : 1;
     int extra = (ok && R.merged && R.n_copies > 1) ? R.n_copies - 1 : 0;
@@ -1629,7 +1678,7 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
 
 // phase 2b: apply the winning target operations
 __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long long* n_ops,
-                           const PPResult* res, const double* res_vol, const uint8_t* win,
+                           const PPResult* res, const double* res_vol, const int* rm_pool, const uint8_t* win,
                            const long long* slot_rank, const long long* id_rank,
                            const int* slot_base, const long long* id_base, const long long* pop_pair_base,
                            int* ppw_slot, int* ppw_gp, long long* ppw_n, long long ppw_cap) {
@@ -1649,9 +1698,10 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
     for (int z = 0; z < R.n_rm; z++) {
       // sample_source_particle records each source it removes with the
       // target's ID (coagulation.F90:447-453)
-      log_removal(P, P.id[R.rm[z]], kInfoCoag, P.id[R.target]);
-      kill_slot(P, R.rm[z]);
-      P.touched[R.rm[z]] = gen;
+      const int sz = rm_pool[R.rm_off + z];
+      log_removal(P, P.id[sz], kInfoCoag, P.id[R.target]);
+      kill_slot(P, sz);
+      P.touched[sz] = gen;
       dlive--;
     }
     if (R.merged) {
@@ -1672,7 +1722,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
             ppw_slot[k] = slot;
             ppw_gp[k] = wgp;
           } else {
-            set_status(P.ctr, kErrCapacity);
+            cap_fail(P.ctr, kCapWalkers);
           }
         };
         store_particle(P, t, v, R.meta);
@@ -1681,7 +1731,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
         for (int z = 1; z < R.n_copies; z++) {
           int dest = slot_base[pop] + (int)slot_rank[q] + (z - 1);
           if (dest >= P.cap) {
-            set_status(P.ctr, kErrCapacity);
+            cap_fail(P.ctr, kCapCopySlot);
             break;
           }
           PMeta cm = R.meta;

@@ -150,7 +150,7 @@ __global__ void k_sample_batch(PopDev P, SampleBatch B, int slot0, long long id0
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < B.n; j += gridDim.x * blockDim.x) {
     int d = slot0 + j;
     if (d >= P.cap) {
-      set_status(P.ctr, kErrCapacity);
+      cap_fail(P.ctr, kCapSampleSlot);
       continue;
     }
     Rng g(P.seed, P.step, sample_ctr(call, kSubParticle), idx0 + (uint32_t)j);
@@ -331,7 +331,7 @@ __global__ void k_dup_write(PopDev P, int n, const int* n_copies, const long lon
       long long o = off[i] + j;
       int d = n + (int)o;
       if (d >= P.cap) {
-        set_status(P.ctr, kErrCapacity);
+        cap_fail(P.ctr, kCapDupSlot);
         break;
       }
       copy_particle(P, i, d, id0 + o);

@@ -117,6 +117,21 @@ struct PopCtr {
   long long walk_tests;    // pair tests made by walks in the current step
   long long exact_tests;   // FP32 pair tests decided in FP64 (f32_decides), since the context was made
   long long n_removed;     // removal records appended since the host last read them
+  int cap_site;            // first capacity limit a kernel hit (kCap*), 0 if none
+  int cap_pad;
+};
+
+// sites of the device capacity limits (PopCtr::cap_site)
+enum : int {
+  kCapNone = 0,
+  kCapEventDest = 1,   // an event's new particle past the slot arrays
+  kCapTargetOps = 2,   // the round's target-operation list is full
+  kCapRemovals = 3,    // a target operation's removals past its share of the pool
+  kCapCopies = 4,      // more dup copies than one target operation holds
+  kCapCopySlot = 5,    // a target operation's copy past the slot arrays
+  kCapWalkers = 6,     // the walker list of target operations is full
+  kCapSampleSlot = 7,  // a sampled particle past the slot arrays
+  kCapDupSlot = 8,     // a doubled or dup copy past the slot arrays
 };
 
 // sites of the device bounds checks (PopCtr::bad_site)
