@@ -50,7 +50,7 @@ def parse():
                     help="keep the default launch shapes instead of searching them on a copy of each workload")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batch-pops", type=int, default=256)
-    ap.add_argument("--batch-same", type=int, default=8)
+    ap.add_argument("--batch-same", type=int, default=16)
     ap.add_argument("--serve-jobs", type=int, default=200)
     ap.add_argument("--no-graphs", action="store_true",
                     help="later rounds from the host loop instead of the CUDA graph (for launch lists)")

@@ -1843,10 +1843,11 @@ void group_by_pop(Ctx& c, const long long* n, long long bound, const int* pop_of
 }
 
 // The round's target operations (at most Q, counted on the device): the
-// bound on each one's removals, scanned into its place in the removal pool
-// (one read-back sizes the pool), then the operations themselves.  Steps
-// with target operations run their rounds from the host, so the read-back
-// never falls inside a graph.
+// bound on each one's removals, scanned into its place in the removal pool,
+// then the operations themselves.  An operation whose place runs past the
+// pool loses, as one that lost a claim does, and is redone in the next
+// round; the host reads the round's total with its other counts and grows
+// the pool before that round.
 void launch_pp(Ctx& c, int kt, long long Q, bool grouped) {
   int blocks = grid_for(Q, 128);
   if (!grouped && c.n_pop > 1) {
@@ -1866,18 +1867,13 @@ void launch_pp(Ctx& c, int kt, long long Q, bool grouped) {
   k_pp_count<<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
                                            c.n_dev.p + 0, c.pp_rm_n.p);
   note_launch();
-  CK(cudaMemsetAsync(c.pp_rm_tot.p, 0, sizeof(long long), c.stream));
   scan_multi<int>(c, {ScanArg<int>{c.pp_rm_n.p, Q, c.n_dev.p + 0, c.pp_rm_off.p, c.pp_rm_tot.p}});
-  long long tot = 0;
-  CK(cudaMemcpyAsync(&tot, c.pp_rm_tot.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-  CK(cudaStreamSynchronize(c.stream));
-  check_scan_err(c);
-  c.pp_rm_pool.reserve((size_t)std::max(tot, 1LL));
+  c.pp_rm_pool.reserve(1);
   with_kt(c, kt, [&](auto ktc, auto) {
     constexpr int KT = decltype(ktc)::value;
     k_pp_ops<KT><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
                                                c.op_key.p, c.n_dev.p + 0, c.pp_res.p, c.pp_vol.p, c.pp_rm_off.p,
-                                               c.pp_rm_pool.p);
+                                               c.pp_rm_pool.p, (long long)c.pp_rm_pool.n);
   });
   note_launch();
 }
@@ -2639,9 +2635,11 @@ void step_parallel(Ctx& c, int kt) {
     CK(cudaMemcpyAsync(&ppw, c.round_dev.p + 5, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     long long Qr = 0;
     pp_lost = 0;
+    long long rm_tot = 0;
     if (last_qb > 0) {
       CK(cudaMemcpyAsync(&pp_lost, c.round_dev.p + 8, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
       CK(cudaMemcpyAsync(&Qr, c.n_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(&rm_tot, c.pp_rm_tot.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     }
     CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
     unsigned long long scan_err = 0;
@@ -2652,6 +2650,9 @@ void step_parallel(Ctx& c, int kt) {
       throw Fail(PMC_ERR_TIMEOUT);
     }
     for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] += per_pop[0 * c.n_pop + k] + per_pop[2 * c.n_pop + k];
+    // room in the removal pool for the redone operations (they draw anew,
+    // so with a margin)
+    if (rm_tot > (long long)c.pp_rm_pool.n) c.pp_rm_pool.reserve((size_t)(rm_tot + rm_tot / 2 + 1024));
     redraws += losers + pp_lost;
     c.last_set_losers += losers;
     c.last_pp_lost += pp_lost;

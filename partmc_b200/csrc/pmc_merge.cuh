@@ -1398,6 +1398,7 @@ struct PPResult {
   int merged;           // n_coag > 0
   int n_copies;         // prob_round(old_nc / new_nc); 0 removes the target
   int n_rm;             // sources it removes: rm_pool[rm_off .. rm_off + n_rm)
+  int nofit;            // its removals did not fit the round's pool: it loses and is redone
   int copy_group[kMaxCopies];
   long long rm_off;
   PMeta meta;           // new target metadata
@@ -1454,7 +1455,7 @@ template <int KT>
 __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pair,
                          const int* op_slot, const int* op_k, const unsigned long long* op_key,
                          const long long* n_ops, PPResult* res, double* res_vol, const long long* rm_off,
-                         int* rm_pool) {
+                         int* rm_pool, long long rm_cap) {
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
@@ -1469,6 +1470,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     R.merged = 0;
     R.n_copies = 1;
     R.n_rm = 0;
+    R.nofit = 0;
     R.rm_off = rm_off[q];
     if (t < 0 || t >= P.cap || !P.alive[t]) continue;  // t = -1: a redo voided by k_build_redo
     const PairState& S = P.pair[p];
@@ -1492,6 +1494,10 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
     int n_extra = rand_poisson(g, (1.0 - prm_max) * S.nspt);
     if (n_remove < 0 || n_extra < 0) {
       set_status(P.ctr, kErrTimeout);
+      continue;
+    }
+    if (R.rm_off + n_remove > rm_cap) {
+      R.nofit = 1;  // no draws, no claims: redone next round with a larger pool
       continue;
     }
     int n_total = n_remove + n_extra;
@@ -1665,7 +1671,7 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
     const PopDev& P = pops[op_pop[q]];
     const PPResult& R = res[q];
     unsigned long long prio = op_key[q];
-    bool ok = true;
+    bool ok = !R.nofit;
     if (R.merged) ok = ok && holds_slot(P, R.target, claim_key(P, prio), true);
     for (int z = 0; z < R.n_rm; z++) ok = ok && holds_slot(P, rm_pool[R.rm_off + z], claim_key(P, prio), true);
     win[q] = ok ? 1 : 0;
