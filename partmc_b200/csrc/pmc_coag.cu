@@ -2166,7 +2166,7 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
   if (Q > 0) {
     k_pp_apply<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
                                                  c.pp_rm_pool.p, c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p, c.slot_base_pp.p,
-                                                 c.id_base_pp.p, c.pop_pair_base.p, c.ppw_slot.p, c.ppw_gp.p,
+                                                 c.id_base_pp.p, c.pop_pair_base.p, c.op_k.p, c.ppw_slot.p, c.ppw_gp.p,
                                                  c.round_dev.p + 5, c.ppw_cap);
     note_launch();
     scan_multi<int>(c, {ScanArg<int>{c.lost_pp.p, Q, c.n_dev.p, c.lost_off.p, c.round_dev.p + 8}}, st);

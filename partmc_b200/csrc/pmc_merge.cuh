@@ -1687,7 +1687,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
                            const PPResult* res, const double* res_vol, const int* rm_pool, const uint8_t* win,
                            const long long* slot_rank, const long long* id_rank,
                            const int* slot_base, const long long* id_base, const long long* pop_pair_base,
-                           int* ppw_slot, int* ppw_gp, long long* ppw_n, long long ppw_cap) {
+                           const int* op_k, int* ppw_slot, int* ppw_gp, long long* ppw_n, long long ppw_cap) {
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
@@ -1749,6 +1749,20 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
           add_walker(dest);
           dlive++;
         }
+      }
+    } else if ((op_k[q] & 0x40000000) && R.target >= 0 && R.target < P.cap && P.alive[R.target] &&
+               P.touched[R.target] != gen) {
+      // a walk that stopped here for this operation, which changed nothing,
+      // goes on from the end of the pair: the reference's target stays in
+      // its bin for the step's later pairs.  A target that an event of this
+      // round rewrote walks on from that event instead (one walker per
+      // particle: two would draw the same tests and make the same event)
+      const unsigned long long k = atomicAdd((unsigned long long*)ppw_n, 1ULL);
+      if ((long long)k < ppw_cap) {
+        ppw_slot[k] = R.target;
+        ppw_gp[k] = (int)(pop_pair_base[pop] + R.p);
+      } else {
+        cap_fail(P.ctr, kCapWalkers);
       }
     }
     if (dlive) add_ll(&P.ctr->n_live, (long long)(dlive));
