@@ -222,6 +222,7 @@ __global__ void k_compact_items(const uint8_t* it_flag, const long long* off, co
        i += (long long)gridDim.x * blockDim.x)
     if (it_flag[i]) {
       long long e = grouped ? grouped[i] : off[i];
+      if (e < 0) continue;
       ev_key[e] = it_key[i];
       ev_c[e] = it_c[i];
       gp_c[e] = it_gp[i];
@@ -903,6 +904,10 @@ struct Ctx {
   // a batched round's lists grouped by population (group_by_pop)
   DevBuf<int> grp_hist, item_pop, g_pop, g_pair, g_slot, g_k;
   DevBuf<long long> grp_off, grp_dest;
+  // walkers of the round's operations, one place per operation and copy
+  DevBuf<int> wk_slot, wk_gp;
+  DevBuf<uint8_t> wk_flag;
+  DevBuf<long long> wk_off;
   DevBuf<unsigned long long> g_key;
   DevBuf<long long> pp_rm_off, pp_rm_tot;
   // initial-condition sampler: staging of the modes, copy counts, radix select
@@ -1748,6 +1753,10 @@ void launch_items_kt(Ctx& c, int kt, bool flat, int n_gpairs, long long W, cudaS
   note_launch();
 }
 
+__global__ void k_ops_span(long long* n_ops, long long n_redo, const long long* n_items) {
+  n_ops[0] = n_redo + *n_items;
+}
+
 // Stable grouping by population of a batched context's per-round lists.
 // Slot and ID ranks come from one scan over a list, and the per-population
 // bases of k_alloc_bases assume that each population's entries lie together
@@ -1794,7 +1803,10 @@ __global__ void __launch_bounds__(kGrpTile) k_grp_rank(const long long* n, const
     wcnt[w][lane] = __popc(same);
   }
   __syncthreads();
-  if (p < 0) return;
+  if (p < 0) {
+    if (i < N) dest[i] = -1;  // not kept
+    return;
+  }
   int before = 0;
   for (int v = 0; v < w; v++)
     for (int l = 0; l < 32; l++)
@@ -1808,6 +1820,7 @@ __global__ void k_scatter_ops(const long long* n_ops, const long long* dest, con
   const long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q; q += (long long)gridDim.x * blockDim.x) {
     const long long d = dest[q];
+    if (d < 0) continue;  // a place without an operation: dropped
     pop_o[d] = pop[q];
     pair_o[d] = pair[q];
     slot_o[d] = slot[q];
@@ -1850,7 +1863,9 @@ void group_by_pop(Ctx& c, const long long* n, long long bound, const int* pop_of
 // the pool before that round.
 void launch_pp(Ctx& c, int kt, long long Q, bool grouped) {
   int blocks = grid_for(Q, 128);
-  if (!grouped && c.n_pop > 1) {
+  if (!grouped) {
+    // a later round's list: the redone operations, then one place per item
+    // (population -1 where the item made none); grouping also drops those
     c.grp_dest.reserve((size_t)Q + 1);
     c.g_pop.reserve(Q); c.g_pair.reserve(Q); c.g_slot.reserve(Q); c.g_k.reserve(Q); c.g_key.reserve(Q);
     group_by_pop(c, c.n_dev.p + 0, Q, c.op_pop.p, c.grp_dest.p, c.stream);
@@ -1858,6 +1873,9 @@ void launch_pp(Ctx& c, int kt, long long Q, bool grouped) {
                                                           c.op_slot.p, c.op_k.p, c.op_key.p, c.g_pop.p, c.g_pair.p,
                                                           c.g_slot.p, c.g_k.p, c.g_key.p);
     note_launch();
+    // the operations kept: the scan's total
+    const long long nh = (long long)std::max<long long>(1, (Q + kGrpTile - 1) / kGrpTile) * c.n_pop;
+    CK(cudaMemcpyAsync(c.n_dev.p, c.grp_off.p + nh, sizeof(long long), cudaMemcpyDeviceToDevice, c.stream));
     std::swap(c.op_pop, c.g_pop); std::swap(c.op_pair, c.g_pair); std::swap(c.op_slot, c.g_slot);
     std::swap(c.op_k, c.g_k); std::swap(c.op_key, c.g_key);
   }
@@ -2164,10 +2182,19 @@ void resolve_apply(Ctx& c, cudaStream_t st, long long W, long long Q) {
     note_launch();
   }
   if (Q > 0) {
+    const size_t nw = (size_t)Q * kMaxCopies;
+    c.wk_slot.reserve(nw); c.wk_gp.reserve(nw); c.wk_flag.reserve(nw); c.wk_off.reserve(nw + 1);
     k_pp_apply<<<grid_for(Q, 256), 256, 0, st>>>(c.d_pops, c.op_pop.p, c.n_dev.p, c.pp_res.p, c.pp_vol.p,
-                                                 c.pp_rm_pool.p, c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p, c.slot_base_pp.p,
-                                                 c.id_base_pp.p, c.pop_pair_base.p, c.op_k.p, c.ppw_slot.p, c.ppw_gp.p,
-                                                 c.round_dev.p + 5, c.ppw_cap);
+                                                 c.pp_rm_pool.p, c.win_pp.p, c.rank_slot_pp.p, c.rank_id_pp.p,
+                                                 c.slot_base_pp.p, c.id_base_pp.p, c.pop_pair_base.p, c.op_k.p,
+                                                 c.wk_slot.p, c.wk_gp.p, c.wk_flag.p);
+    note_launch();
+    k_walkers_span<<<1, 1, 0, st>>>(c.n_dev.p, c.round_dev.p + 9);
+    note_launch();
+    scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.wk_flag.p, (long long)nw, c.round_dev.p + 9, c.wk_off.p,
+                                             c.round_dev.p + 5}}, st);
+    k_compact_walkers<<<grid_for((long long)nw, 256), 256, 0, st>>>(c.round_dev.p + 9, c.wk_flag.p, c.wk_off.p,
+                                                                    c.wk_slot.p, c.wk_gp.p, c.ppw_slot.p, c.ppw_gp.p);
     note_launch();
     scan_multi<int>(c, {ScanArg<int>{c.lost_pp.p, Q, c.n_dev.p, c.lost_off.p, c.round_dev.p + 8}}, st);
   }
@@ -2200,7 +2227,11 @@ void enqueue_round_body(Ctx& c, cudaStream_t st, const RoundBounds& b, long long
   }
   if (Q > 0) set_n_dev(c, Qn);
   launch_items_kt(c, b.kt, b.flat, b.n_gpairs, W, st);
-  if (Q > 0) launch_pp(c, b.kt, Q, false);
+  if (Q > 0) {
+    k_ops_span<<<1, 1, 0, st>>>(c.n_dev.p, Qn, c.round_dev.p + 2);  // redone ones + one place per item
+    note_launch();
+    launch_pp(c, b.kt, Q, false);
+  }
   const long long* Id = c.round_dev.p + 2;
   long long* Ed = c.round_dev.p + 1;
   scan_multi<uint8_t>(c, {ScanArg<uint8_t>{c.it_flag.p, W, Id, c.it_off.p, Ed}}, st);
@@ -2921,6 +2952,10 @@ int pmc_coag_gpu_destroy(pmc_coag_gpu_ctx* x) {
   for (auto* b : {&c.grp_hist, &c.item_pop, &c.g_pop, &c.g_pair, &c.g_slot, &c.g_k}) b->release();
   c.grp_off.release();
   c.grp_dest.release();
+  c.wk_slot.release();
+  c.wk_gp.release();
+  c.wk_flag.release();
+  c.wk_off.release();
   c.g_key.release();
   c.pp_rm_pool.release();
   c.pp_rm_off.release();

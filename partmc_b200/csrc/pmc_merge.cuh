@@ -722,14 +722,15 @@ __device__ __noinline__ uint32_t chain_event_decision(const PopDev& P, unsigned 
 }
 
 // A target operation for particle x at per-particle pair q (its walk reached
-// the pair with x in the pair's target cell), appended to the round's
-// operations after the redone ones; it runs in this round.  Its key puts it
-// after the pair's own operations.
+// the pair with x in the pair's target cell), at place k of the round's
+// operations: after the redone ones, at the item's own index, so that the
+// list's order does not depend on scheduling (the places of items without
+// one hold population -1 and are dropped when the list is grouped).  It runs
+// in this round; its key puts it after the pair's own operations.
 __device__ __noinline__ void add_target_op(const PopDev& P, int pop, int q, int x, int* op_pop, int* op_pair,
-                                              int* op_slot, int* op_k, unsigned long long* op_key, long long* n_ops,
+                                              int* op_slot, int* op_k, unsigned long long* op_key, long long k,
                                               long long op_cap) {
-  const unsigned long long k = atomicAdd((unsigned long long*)n_ops, 1ULL);
-  if ((long long)k >= op_cap) {
+  if (k >= op_cap) {
     cap_fail(P.ctr, kCapTargetOps);
     return;
   }
@@ -766,10 +767,12 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
                                                int2* it_c, int* it_gp, float* it_pos, int* it_len, int* it_head,
                                                uint8_t* it_done, uint32_t* it_dec, uint32_t* it_gused, int4* it_term) {
   long long n = *n_items, n_ev = *n_items_ev;
+  const long long op_base = op_cap > 0 ? *n_ops : 0;  // the redone operations come first
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
     it_flag[e] = 0;
     it_term[e] = no_term();
+    if (op_cap > 0 && op_base + e < op_cap) op_pop[op_base + e] = -1;
     int gp, walker = -1, p0 = 0;
     float pos0 = 1.0f;
     unsigned long long key = 0;
@@ -847,7 +850,7 @@ __global__ void __launch_bounds__(256) k_items(const PopDev* pops, const int* gp
     if (walker >= 0) {
       WalkOut w;
       walk<KT, T, FLAT>(P, walker, p0, pos0, &w);
-      if (w.stop) add_target_op(P, pop, w.q, walker, op_pop, op_pair, op_slot, op_k, op_key, n_ops, op_cap);
+      if (w.stop) add_target_op(P, pop, w.q, walker, op_pop, op_pair, op_slot, op_k, op_key, op_base + e, op_cap);
       if (!w.found) continue;
       key = make_key((uint32_t)w.q, 1u, (uint32_t)walker);
       sl = w.first_cell1 ? make_int2(walker, w.y) : make_int2(w.y, walker);
@@ -1683,14 +1686,31 @@ __global__ void k_pp_resolve(const PopDev* pops, const int* op_pop, const unsign
 }
 
 // phase 2b: apply the winning target operations
+// walker places of the round's operations, compacted in order
+__global__ void k_walkers_span(const long long* n_ops, long long* n_places) { *n_places = *n_ops * kMaxCopies; }
+
+__global__ void k_compact_walkers(const long long* n_places, const uint8_t* flag, const long long* off,
+                                  const int* wk_slot, const int* wk_gp, int* ppw_slot, int* ppw_gp) {
+  const long long n = *n_places;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (flag[i]) {
+      ppw_slot[off[i]] = wk_slot[i];
+      ppw_gp[off[i]] = wk_gp[i];
+    }
+}
+
 __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long long* n_ops,
                            const PPResult* res, const double* res_vol, const int* rm_pool, const uint8_t* win,
                            const long long* slot_rank, const long long* id_rank,
                            const int* slot_base, const long long* id_base, const long long* pop_pair_base,
-                           const int* op_k, int* ppw_slot, int* ppw_gp, long long* ppw_n, long long ppw_cap) {
+                           const int* op_k, int* wk_slot, int* wk_gp, uint8_t* wk_flag) {
+  // the walkers an operation makes (its target, then its copies) go to the
+  // operation's own kMaxCopies places, compacted afterwards in operation
+  // order, so that the next round's items do not depend on scheduling
   long long Q = *n_ops;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Q;
        q += (long long)gridDim.x * blockDim.x) {
+    for (int z = 0; z < kMaxCopies; z++) wk_flag[q * kMaxCopies + z] = 0;
     if (!win[q]) continue;
     int pop = op_pop[q];
     const PopDev& P = pops[pop];
@@ -1722,18 +1742,15 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
         // the changed target and its copies take part in the rest of the
         // step: they walk from the end of this pair in the next round
         const int wgp = (int)(pop_pair_base[pop] + R.p);
-        auto add_walker = [&](int slot) {
-          const unsigned long long k = atomicAdd((unsigned long long*)ppw_n, 1ULL);
-          if ((long long)k < ppw_cap) {
-            ppw_slot[k] = slot;
-            ppw_gp[k] = wgp;
-          } else {
-            cap_fail(P.ctr, kCapWalkers);
-          }
+        auto add_walker = [&](int slot, int z) {
+          const long long k = q * kMaxCopies + z;
+          wk_slot[k] = slot;
+          wk_gp[k] = wgp;
+          wk_flag[k] = 1;
         };
         store_particle(P, t, v, R.meta);
         refresh_slot(P, t);
-        add_walker(t);
+        add_walker(t, 0);
         for (int z = 1; z < R.n_copies; z++) {
           int dest = slot_base[pop] + (int)slot_rank[q] + (z - 1);
           if (dest >= P.cap) {
@@ -1746,7 +1763,7 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
           store_particle(P, dest, v, cm);
           refresh_slot(P, dest);
           P.touched[dest] = gen;
-          add_walker(dest);
+          add_walker(dest, z);
           dlive++;
         }
       }
@@ -1757,13 +1774,10 @@ __global__ void k_pp_apply(const PopDev* pops, const int* op_pop, const long lon
       // its bin for the step's later pairs.  A target that an event of this
       // round rewrote walks on from that event instead (one walker per
       // particle: two would draw the same tests and make the same event)
-      const unsigned long long k = atomicAdd((unsigned long long*)ppw_n, 1ULL);
-      if ((long long)k < ppw_cap) {
-        ppw_slot[k] = R.target;
-        ppw_gp[k] = (int)(pop_pair_base[pop] + R.p);
-      } else {
-        cap_fail(P.ctr, kCapWalkers);
-      }
+      const long long k = q * kMaxCopies;
+      wk_slot[k] = R.target;
+      wk_gp[k] = (int)(pop_pair_base[pop] + R.p);
+      wk_flag[k] = 1;
     }
     if (dlive) add_ll(&P.ctr->n_live, (long long)(dlive));
   }

@@ -81,7 +81,9 @@ def test_batched_per_particle_rounds_keep_every_population_consistent(gpu_lib):
     the later rounds.  Each population's slots and IDs are allocated from
     its own range (the operations and events are grouped by population
     first), so after every step each member's live count matches its slots
-    and its IDs are unique."""
+    and its IDs are unique.  Every list of a round is built in an order that
+    does not depend on scheduling, so a second run with the same seeds gives
+    the same particles bit for bit."""
     import reference_cases as RC
     from oracle import ic_sampler as S
     from oracle import oracle as O
@@ -92,16 +94,23 @@ def test_batched_per_particle_rounds_keep_every_population_consistent(gpu_lib):
     n_pop = 64
     awa = pm.AeroWeightArray(np.array([[O.WEIGHT_POWER], [O.WEIGHT_POWER]]),
                              np.array([[ws[0].magnitude], [ws[1].magnitude]]), np.array([[0.0], [-3.0]]))
-    st = pm.AeroState(pm.AeroData([1000.0]), awa, mode=pm.MODE_FP64, n_pop=n_pop,
-                      seeds=np.arange(900, 900 + n_pop, dtype=np.uint64))
-    for k in range(n_pop):
-        vols, grp, _ = S.add_dist_sample(np.random.default_rng(100 + k), [mode], ws, 1.0)
-        st.add_particles(vols, grp + 1, pop=k)
-    ops = 0
-    for _ in range(4):
-        pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_SEDI, 288.0, 1e5, 0.0, st, 5.0)
-        ops += st.conflicts()["target_ops"]
-        for k in range(n_pop):
-            p = st.particles(pop=k)  # the download checks the live count against the slots
-            assert len(np.unique(p["id"])) == len(p["id"]) == st.n_part(pop=k)
-    assert ops > 0
+    inits = [S.add_dist_sample(np.random.default_rng(100 + k), [mode], ws, 1.0) for k in range(n_pop)]
+    finals = []
+    for run in range(2):
+        st = pm.AeroState(pm.AeroData([1000.0]), awa, mode=pm.MODE_FP64, n_pop=n_pop,
+                          seeds=np.arange(900, 900 + n_pop, dtype=np.uint64))
+        for k, (vols, grp, _) in enumerate(inits):
+            st.add_particles(vols, grp + 1, pop=k)
+        ops = 0
+        for _ in range(4):
+            pm.mc_coag_batch(pm.COAG_KERNEL_TYPE_SEDI, 288.0, 1e5, 0.0, st, 5.0)
+            ops += st.conflicts()["target_ops"]
+            for k in range(n_pop):
+                p = st.particles(pop=k)  # the download checks the live count against the slots
+                assert len(np.unique(p["id"])) == len(p["id"]) == st.n_part(pop=k)
+        assert ops > 0
+        finals.append([st.particles(pop=k) for k in range(n_pop)])
+        st.close()
+    for a, b in zip(*finals):
+        for key in ("vol", "id", "weight_group"):
+            assert np.array_equal(a[key], b[key]), key
