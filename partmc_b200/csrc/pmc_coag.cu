@@ -1886,7 +1886,23 @@ void launch_pp(Ctx& c, int kt, long long Q, bool grouped) {
                                            c.n_dev.p + 0, c.pp_rm_n.p);
   note_launch();
   scan_multi<int>(c, {ScanArg<int>{c.pp_rm_n.p, Q, c.n_dev.p + 0, c.pp_rm_off.p, c.pp_rm_tot.p}});
-  c.pp_rm_pool.reserve(1);
+  // every operation's removals fit the pool: one that did not would lose
+  // and draw anew a round later, so the pool's size (in a batch, the other
+  // populations' removals) would decide the particles.  One read-back; the
+  // steps that have target operations run their rounds from the host.
+  {
+    long long rm_tot = 0;
+    unsigned long long scan_err = 0;
+    CK(cudaMemcpyAsync(&rm_tot, c.pp_rm_tot.p, sizeof(rm_tot), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&scan_err, c.scan_err.p, sizeof(scan_err), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (scan_err) {
+      CK(cudaMemsetAsync(c.scan_err.p, 0, sizeof(scan_err), c.stream));
+      throw Fail(PMC_ERR_TIMEOUT);
+    }
+    if (rm_tot < 0 || rm_tot >= (1LL << 31)) cap_throw("more than 2^31 removals in one round");
+    if (rm_tot + 1 > (long long)c.pp_rm_pool.n) c.pp_rm_pool.reserve((size_t)(rm_tot + rm_tot / 2 + 1024));
+  }
   with_kt(c, kt, [&](auto ktc, auto) {
     constexpr int KT = decltype(ktc)::value;
     k_pp_ops<KT><<<blocks, 128, 0, c.stream>>>(c.d_pops, c.op_pop.p, c.op_pair.p, c.op_slot.p, c.op_k.p,
@@ -2582,17 +2598,21 @@ void step_parallel(Ctx& c, int kt) {
     }
     W = hw[0];
     Q = hw[1];
-    // a step with target operations runs its later rounds from the host,
-    // where walks that reach a per-particle pair's target cell stop for one
-    c.pp_step = Q > 0;
-    for (int k = 0; k < c.n_pop; k++)
-      if (c.pops[k].h.walk_stops != (c.pp_step ? 1 : 0)) {
-        c.pops[k].h.walk_stops = c.pp_step ? 1 : 0;
-        c.dirty = true;
-      }
     if (c.n_pop == 1) {
       hw[3] = W;
       hw[4] = Q;
+    }
+    // a step with target operations runs its later rounds from the host,
+    // where walks that reach a per-particle pair's target cell stop for one;
+    // a population's walks stop when it has target operations of its own,
+    // so it steps the same alone and in a batch
+    c.pp_step = Q > 0;
+    for (int k = 0; k < c.n_pop; k++) {
+      const int stops = hw[3 + 2 * k + 1] > 0 ? 1 : 0;
+      if (c.pops[k].h.walk_stops != stops) {
+        c.pops[k].h.walk_stops = stops;
+        c.dirty = true;
+      }
     }
     // sample numbers fit in a key's 31 bits below the walk flag of the merge stream
     if (W + Q + 1 >= 0x7fffffffLL) cap_throw("more than 2^31 samples in one step");
@@ -2666,11 +2686,9 @@ void step_parallel(Ctx& c, int kt) {
     CK(cudaMemcpyAsync(&ppw, c.round_dev.p + 5, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     long long Qr = 0;
     pp_lost = 0;
-    long long rm_tot = 0;
     if (last_qb > 0) {
       CK(cudaMemcpyAsync(&pp_lost, c.round_dev.p + 8, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
       CK(cudaMemcpyAsync(&Qr, c.n_dev.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
-      CK(cudaMemcpyAsync(&rm_tot, c.pp_rm_tot.p, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
     }
     CK(cudaMemcpyAsync(per_pop.data(), c.per_pop_i.p, sizeof(int) * 4 * c.n_pop, cudaMemcpyDeviceToHost, c.stream));
     unsigned long long scan_err = 0;
@@ -2681,9 +2699,6 @@ void step_parallel(Ctx& c, int kt) {
       throw Fail(PMC_ERR_TIMEOUT);
     }
     for (int k = 0; k < c.n_pop; k++) c.n_slots_host[k] += per_pop[0 * c.n_pop + k] + per_pop[2 * c.n_pop + k];
-    // room in the removal pool for the redone operations (they draw anew,
-    // so with a margin)
-    if (rm_tot > (long long)c.pp_rm_pool.n) c.pp_rm_pool.reserve((size_t)(rm_tot + rm_tot / 2 + 1024));
     redraws += losers + pp_lost;
     c.last_set_losers += losers;
     c.last_pp_lost += pp_lost;

@@ -1401,7 +1401,7 @@ struct PPResult {
   int merged;           // n_coag > 0
   int n_copies;         // prob_round(old_nc / new_nc); 0 removes the target
   int n_rm;             // sources it removes: rm_pool[rm_off .. rm_off + n_rm)
-  int nofit;            // its removals did not fit the round's pool: it loses and is redone
+  int nofit;            // its removals did not fit the pool (the host sizes it to fit): it loses
   int copy_group[kMaxCopies];
   long long rm_off;
   PMeta meta;           // new target metadata
@@ -1500,7 +1500,7 @@ __global__ void k_pp_ops(const PopDev* pops, const int* op_pop, const int* op_pa
       continue;
     }
     if (R.rm_off + n_remove > rm_cap) {
-      R.nofit = 1;  // no draws, no claims: redone next round with a larger pool
+      R.nofit = 1;  // no draws, no claims; the host sized the pool from the round's total, so a guard only
       continue;
     }
     int n_total = n_remove + n_extra;

@@ -83,7 +83,7 @@ def test_batched_per_particle_rounds_keep_every_population_consistent(gpu_lib):
     first), so after every step each member's live count matches its slots
     and its IDs are unique.  Every list of a round is built in an order that
     does not depend on scheduling, so a second run with the same seeds gives
-    the same particles bit for bit."""
+    the same particles bit for bit, and a member ends as it would alone."""
     import reference_cases as RC
     from oracle import ic_sampler as S
     from oracle import oracle as O
@@ -114,3 +114,12 @@ def test_batched_per_particle_rounds_keep_every_population_consistent(gpu_lib):
     for a, b in zip(*finals):
         for key in ("vol", "id", "weight_group"):
             assert np.array_equal(a[key], b[key]), key
+    # and each member as it would run alone
+    for k in (0, 17, 63):
+        alone = pm.AeroState(pm.AeroData([1000.0]), awa, seed=900 + k, mode=pm.MODE_FP64)
+        alone.add_particles(inits[k][0], inits[k][1] + 1)
+        for _ in range(4):
+            pm.mc_coag(pm.COAG_KERNEL_TYPE_SEDI, pm.EnvState(288.0, 1e5), pm.AeroData([1000.0]), alone, 5.0)
+        a = alone.particles()
+        for key in ("vol", "id", "weight_group"):
+            assert np.array_equal(a[key], finals[0][k][key]), (k, key)
