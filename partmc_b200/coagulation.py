@@ -192,7 +192,10 @@ class AeroState:
 
     def __del__(self):
         if getattr(self, "ctx", None):
-            _lib.lib().pmc_coag_gpu_destroy(self.ctx)
+            try:
+                _lib.lib().pmc_coag_gpu_destroy(self.ctx)
+            except (TypeError, AttributeError):
+                pass  # interpreter shutdown: the module's globals are gone; the process's exit frees the device memory
             self.ctx = None
 
     def close(self):
