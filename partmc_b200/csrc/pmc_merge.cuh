@@ -1312,10 +1312,11 @@ __global__ void __launch_bounds__(32) k_apply_chain(const PopDev* pops, const in
 // pairs (loop order) of k_max * del_t * members of the pair's other cell;
 // pairs on the per-particle path add nothing.  One block per cell, its
 // threads over the cell's pairs, a block-wide scan in a fixed order.
-// P.walk_stops: 1 when the step has target operations (its later rounds run
-// from the host and take the operations that walks stop for); with 0,
-// per-particle pairs (whose target cells were all empty at the step's start)
-// are walked at the per-set rate like any pair.
+// P.walk_stops: 1 when the population's round 0 has target operations (the
+// step's later rounds then run from the host and take the operations that
+// walks stop for); with 0, its per-particle pairs (whose target cells were
+// all empty at the step's start) are walked at the per-set rate like any
+// pair.
 __global__ void __launch_bounds__(128) k_walk_rates(const PopDev* pops) {
   const PopDev& P = pops[blockIdx.y];
   int c = blockIdx.x;

@@ -225,7 +225,7 @@ struct PopDev {
   // on the per-particle path with this cell as its target cell (a walk stops
   // there for a target operation); the cell's end if none
   int* cp_nstop;       // [cp_off[n_cells]], valid when walk_stops
-  int walk_stops;      // the step has target operations: walks stop at per-particle pairs
+  int walk_stops;      // round 0 gave this population target operations: walks stop at per-particle pairs
   // per cell, kWalkTab buckets of its stretch of tests: entry b is the last
   // j of the cell with cp_cum[j] <= b / kWalkTab of the cell's total
   int* cp_tab;         // [n_cells * kWalkTab]
