@@ -521,8 +521,15 @@ def run_extras(args, pm, torch, pop, env, new_state, timed_steps, mode, ws):
     serve.warm_up(srv)
     sm = serve.run(jobs, srv)
     del srv
-    out["serving"] = aggregate(dict(sm, unit="pair-tests/s", rate_jobs_per_s=50.0), sm["pair_tests_per_s"] * sm["wall_s"],
-                               sm["wall_s"], ws)
+    # each kernel at the step length of the reference's own test for it: at
+    # 60 s an additive job (total volume fraction 4.2e-6, beta1 = 1000 1/s:
+    # number decays as exp(-t / 240 s)) would coagulate to a few particles
+    # within its steps
+    del_t_s = {"additive": serve.DEL_T[pm.COAG_KERNEL_TYPE_ADDITIVE],
+               "brownian": serve.DEL_T[pm.COAG_KERNEL_TYPE_BROWN],
+               "sedimentation": serve.DEL_T[pm.COAG_KERNEL_TYPE_SEDI]}
+    out["serving"] = aggregate(dict(sm, unit="pair-tests/s", rate_jobs_per_s=50.0, del_t_s=del_t_s),
+                               sm["pair_tests_per_s"] * sm["wall_s"], sm["wall_s"], ws)
 
     out["e2e"] = aggregate({"unit": "pair-tests/s", "h2d_bytes_per_step": 16,
                             "d2h_bytes_per_step": int(res_d2h / max(args.steps, 1)),
